@@ -1,0 +1,84 @@
+"""ctypes binding of lib/libblgpu.so (the C ABI declared in include/blgpu.h).
+
+The library is the only compute path: if it is missing or fails to load the
+import raises, there is no CPU fallback.
+"""
+import ctypes
+import os
+
+from ._build import LIB_PATH
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("nu", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("dpdx", ctypes.c_double), ("dpdz", ctypes.c_double),
+        ("rk_scheme", ctypes.c_int), ("les_model", ctypes.c_int),
+        ("precision", ctypes.c_int), ("poisson", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+FP64 = 0
+MIXED = 1
+POISSON_NATIVE = 0
+POISSON_CUFFT = 1
+
+_SIGS = {
+    "blgpu_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
+    "blgpu_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "blgpu_set_grid": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p]),
+    "blgpu_set_boundary": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 6),
+    "blgpu_set_inflow_modes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [c_double_p] * 5),
+    "blgpu_set_nu_t": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "blgpu_upload_state": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, ctypes.c_double]),
+    "blgpu_download_state": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 5),
+    "blgpu_compute_dt": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "blgpu_set_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "blgpu_get_time": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),
+    "blgpu_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_time_step": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_compute_rhs": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 6),
+    "blgpu_apply_bc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_projection": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_get_rhs_p": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "blgpu_max_divergence": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "blgpu_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_device_bytes": (ctypes.c_longlong, [ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def exported_symbols():
+    """Names of the C-ABI entry points this binding declares."""
+    return sorted(_SIGS)
+
+
+def load():
+    """Load libblgpu.so; raises OSError when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("libblgpu.so not built (%s); run __graft_entry__.build()" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class BlgpuError(RuntimeError):
+    pass
+
+
+def check(rc, ctx=None):
+    if rc != 0:
+        msg = load().blgpu_last_error(ctx)
+        raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))

@@ -1,0 +1,160 @@
+"""Host mirror of the reference's step-path subroutines, over the C ABI.
+
+Method names follow the Fortran subroutines they replace
+(time_integration.f90, projection.f90, boundary_conditions.f90,
+equations.f90); arrays are numpy arrays in the reference's Fortran layout
+and bounds:  U(nx,nyg,nzg), V(nxg,ny,nzg), W(nxg,nyg,nz), P(nxg,nyg,nzg).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FP64, MIXED, POISSON_NATIVE, check
+
+
+def _p(a):
+    return a.ctypes.data_as(_lib.c_double_p)
+
+
+def _f64(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+class Solver:
+    """One box on one GPU (a blgpu context)."""
+
+    def __init__(self, nx, ny, nz, nu, cfl, dpdx=0.0, dpdz=0.0, rk_scheme=3, les_model=0,
+                 precision=FP64, poisson=POISSON_NATIVE, device=0):
+        self.lib = _lib.load()
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.nxg, self.nyg, self.nzg = self.nx + 1, self.ny + 1, self.nz + 1
+        cfg = _lib.Config(self.nx, self.ny, self.nz, float(nu), float(cfl), float(dpdx), float(dpdz),
+                          int(rk_scheme), int(les_model), int(precision), int(poisson), int(device))
+        h = ctypes.c_void_p()
+        check(self.lib.blgpu_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.ctx = h
+        self.cfg = cfg
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.blgpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, rc):
+        check(rc, self.ctx)
+
+    # -- set-up (initialization.f90) ---------------------------------------
+    def set_grid(self, x, y, z):
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        assert x.size == self.nx and y.size == self.ny and z.size == self.nz
+        self._ck(self.lib.blgpu_set_grid(self.ctx, _p(x), _p(y), _p(z)))
+
+    def set_boundary(self, U_inlet, V_inlet, W_inlet, U_top, V_top, W_top):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (U_inlet, V_inlet, W_inlet, U_top, V_top, W_top)]
+        want = [self.nyg, self.ny, self.nyg, self.nx, self.nxg, self.nxg]
+        for a, n in zip(arrs, want):
+            assert a.size == n, (a.size, n)
+        self._bc_keep = arrs
+        self._ck(self.lib.blgpu_set_boundary(self.ctx, *[_p(a) for a in arrs]))
+
+    def set_inflow_modes(self, zmode, tmode, qu, qv, qw):
+        zmode = np.ascontiguousarray(zmode, dtype=np.float64)
+        tmode = np.ascontiguousarray(tmode, dtype=np.float64)
+        n, m = zmode.size, tmode.size
+        qs = []
+        for q, ny_ in ((qu, self.nyg), (qv, self.ny), (qw, self.nyg)):
+            q = np.asfortranarray(np.asarray(q, dtype=np.complex128).reshape(ny_, n, m, order="F"))
+            qs.append(np.ascontiguousarray(q.ravel(order="F")).view(np.float64))
+        self._ck(self.lib.blgpu_set_inflow_modes(self.ctx, n, m, _p(zmode), _p(tmode), *[_p(q) for q in qs]))
+
+    def set_nu_t(self, nu_t):
+        a = _f64(nu_t)
+        assert a.shape == (self.nxg, self.nyg, self.nzg)
+        self._ck(self.lib.blgpu_set_nu_t(self.ctx, _p(a)))
+
+    # -- state ------------------------------------------------------------
+    def upload_state(self, U, V, W, t=0.0):
+        U, V, W = _f64(U), _f64(V), _f64(W)
+        assert U.shape == (self.nx, self.nyg, self.nzg)
+        assert V.shape == (self.nxg, self.ny, self.nzg)
+        assert W.shape == (self.nxg, self.nyg, self.nz)
+        self._ck(self.lib.blgpu_upload_state(self.ctx, _p(U), _p(V), _p(W), float(t)))
+
+    def download_state(self):
+        U = np.zeros((self.nx, self.nyg, self.nzg), order="F")
+        V = np.zeros((self.nxg, self.ny, self.nzg), order="F")
+        W = np.zeros((self.nxg, self.nyg, self.nz), order="F")
+        P = np.zeros((self.nxg, self.nyg, self.nzg), order="F")
+        t = ctypes.c_double()
+        self._ck(self.lib.blgpu_download_state(self.ctx, _p(U), _p(V), _p(W), _p(P), ctypes.byref(t)))
+        return U, V, W, P, t.value
+
+    # -- the step path ------------------------------------------------------
+    def compute_dt(self):
+        dt = ctypes.c_double()
+        self._ck(self.lib.blgpu_compute_dt(self.ctx, ctypes.byref(dt)))
+        return dt.value
+
+    def set_dt(self, dt):
+        self._ck(self.lib.blgpu_set_dt(self.ctx, float(dt)))
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.lib.blgpu_get_time(self.ctx, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def time_step(self):
+        """compute_time_step_{Euler,RK2,RK3} with the current dt."""
+        self._ck(self.lib.blgpu_time_step(self.ctx))
+
+    compute_time_step = time_step
+
+    def advance(self, nsteps=1):
+        """nsteps of the main loop body: compute_dt + time step (CUDA graph)."""
+        self._ck(self.lib.blgpu_advance(self.ctx, int(nsteps)))
+
+    def sync(self):
+        self._ck(self.lib.blgpu_sync(self.ctx))
+
+    def compute_rhs(self, U, V, W):
+        """compute_rhs_u/v/w: returns the compact interior arrays."""
+        U, V, W = _f64(U), _f64(V), _f64(W)
+        nx, ny, nz, nxg, nyg, nzg = self.nx, self.ny, self.nz, self.nxg, self.nyg, self.nzg
+        ru = np.zeros((nx - 2, nyg - 2, nzg - 2), order="F")
+        rv = np.zeros((nxg - 2, ny - 2, nzg - 2), order="F")
+        rw = np.zeros((nxg - 2, nyg - 2, nz - 2), order="F")
+        self._ck(self.lib.blgpu_compute_rhs(self.ctx, _p(U), _p(V), _p(W), _p(ru), _p(rv), _p(rw)))
+        return ru, rv, rw
+
+    def apply_boundary_conditions(self, rk_step):
+        self._ck(self.lib.blgpu_apply_bc(self.ctx, int(rk_step)))
+
+    def compute_projection_step(self, rk_step):
+        self._ck(self.lib.blgpu_projection(self.ctx, int(rk_step)))
+
+    def rhs_p(self):
+        r = np.zeros((self.nxg - 2, self.nyg - 2, self.nzg - 1), order="F")
+        self._ck(self.lib.blgpu_get_rhs_p(self.ctx, _p(r)))
+        return r
+
+    def check_divergence(self):
+        d = ctypes.c_double()
+        self._ck(self.lib.blgpu_max_divergence(self.ctx, ctypes.byref(d)))
+        return d.value
+
+    def device_bytes(self):
+        return int(self.lib.blgpu_device_bytes(self.ctx))

@@ -1,0 +1,857 @@
+// capi.cu -- the C ABI (include/blgpu.h): context, device memory, host<->box
+// layout conversion, step orchestration and CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/blgpu.h"
+#include "kernels.cuh"
+
+namespace blgpu {
+
+static thread_local std::string g_last_error = "";
+
+int fail_cuda(cudaError_t e, const char *what, const char *file, int line);
+
+}  // namespace blgpu
+
+using namespace blgpu;
+
+struct blgpu_ctx {
+  blgpu_config cfg{};
+  int nx = 0, ny = 0, nz = 0, nxg = 0, nyg = 0, nzg = 0, px = 0, py = 0;
+  long long plane = 0, boxn = 0;
+  bool fp64 = true;
+  size_t esz = 8;
+  cudaStream_t st = nullptr;
+  bool have_grid = false, have_bc = false, have_state = false;
+  std::string err;
+  // host copies (1-based where the Fortran is)
+  std::vector<double> x, y, z, xg, yg, zg, w0, w1, kxx, kzz, dd, dl, du;
+  double dxmin = 0, dymin = 0, dzmin = 0, dtvis = 0, length_y = 0, qy = 0;
+  double rk_t[4] = {0.0, 8.0 / 15.0, 2.0 / 3.0, 1.0};
+  // device allocations
+  std::vector<void *> allocs;
+  long long bytes = 0;
+  double *d_geo = nullptr;  // all FP64 metric tables in one block
+  float *f_geo = nullptr;   // FP32 copies
+  double *d_spec = nullptr; // dd, dl, du, kxx, kzz
+  double *d_bc = nullptr;   // inflow/top vectors
+  double *d_modes = nullptr;
+  Geo geo{};
+  MetT<double> m64{};
+  MetT<float> m32{};
+  BcData bc{};
+  Spec spec{};
+  void *S[3][3] = {};  // state buffers [buffer][u,v,w]
+  void *F1[3] = {};
+  void *P = nullptr, *nut = nullptr, *rhs_p = nullptr, *R = nullptr, *C = nullptr;
+  double *piv = nullptr, *dcsum = nullptr, *dcrow = nullptr, *dcout = nullptr, *qx_part = nullptr;
+  Scalars *sc = nullptr;
+  unsigned long long *d_maxdiv = nullptr;
+  void *tw = nullptr, *post = nullptr, *ztab = nullptr;
+  FftPlan<double> pl64{};
+  FftPlan<float> pl32{};
+  int cur = 0, old = 1;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  int graph_next[3] = {0, 0, 0};
+};
+
+namespace blgpu {
+
+int fail_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "CUDA error %s (%s) at %s:%d in %s", cudaGetErrorName(e), cudaGetErrorString(e), file,
+           line, what);
+  g_last_error = buf;
+  return BLGPU_ECUDA;
+}
+
+}  // namespace blgpu
+
+static int set_err(blgpu_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  g_last_error = buf;
+  return code;
+}
+
+static int check_cuda(blgpu_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return BLGPU_OK;
+  return set_err(c, BLGPU_ECUDA, "CUDA error %s (%s) in %s", cudaGetErrorName(e), cudaGetErrorString(e), what);
+}
+
+#define CK(expr)                                           \
+  do {                                                     \
+    int _r = check_cuda(ctx, (expr), #expr);               \
+    if (_r) return _r;                                     \
+  } while (0)
+
+static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return set_err(ctx, BLGPU_ECUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  ctx->allocs.push_back(*p);
+  ctx->bytes += (long long)bytes;
+  e = cudaMemset(*p, 0, bytes);
+  if (e != cudaSuccess) return set_err(ctx, BLGPU_ECUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+  return BLGPU_OK;
+}
+
+static void drop_graphs(blgpu_ctx *ctx) {
+  for (int r = 0; r < 3; ++r)
+    if (ctx->graph[r]) {
+      cudaGraphExecDestroy(ctx->graph[r]);
+      ctx->graph[r] = nullptr;
+    }
+}
+
+static std::vector<int> factorize(int n) {
+  std::vector<int> f;
+  int r = n;
+  while (r % 4 == 0) { f.push_back(4); r /= 4; }
+  while (r % 2 == 0) { f.push_back(2); r /= 2; }
+  for (int p = 3; r > 1; p += 2)
+    while (r % p == 0) { f.push_back(p); r /= p; }
+  return f;
+}
+
+extern "C" {
+
+const char *blgpu_last_error(const blgpu_ctx *ctx) {
+  if (ctx && !ctx->err.empty()) return ctx->err.c_str();
+  return g_last_error.c_str();
+}
+
+int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
+  if (!cfg || !out) return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: null argument");
+  *out = nullptr;
+  if (cfg->nx < 5 || cfg->ny < 4 || cfg->nz < 5)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: grid %dx%dx%d too small (need nx>=5, ny>=4, nz>=5)",
+                   cfg->nx, cfg->ny, cfg->nz);
+  if (cfg->rk_scheme < 1 || cfg->rk_scheme > 3)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: RKscheme %d not in {1,2,3}", cfg->rk_scheme);
+  if (cfg->precision != BLGPU_FP64 && cfg->precision != BLGPU_MIXED)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown precision %d", cfg->precision);
+  if (cfg->poisson != BLGPU_POISSON_NATIVE)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: poisson backend %d not available", cfg->poisson);
+  if (!(cfg->nu > 0)) return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: nu must be > 0");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return set_err(nullptr, BLGPU_ECUDA, "blgpu_create: no CUDA device (%s)", cudaGetErrorString(e));
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: device %d out of range", cfg->device);
+  blgpu_ctx *ctx = new blgpu_ctx();
+  ctx->cfg = *cfg;
+  ctx->nx = cfg->nx; ctx->ny = cfg->ny; ctx->nz = cfg->nz;
+  ctx->nxg = cfg->nx + 1; ctx->nyg = cfg->ny + 1; ctx->nzg = cfg->nz + 1;
+  ctx->px = (ctx->nxg + 31) / 32 * 32;
+  ctx->py = ctx->nyg;
+  ctx->plane = (long long)ctx->px * ctx->py;
+  ctx->boxn = ctx->plane * ctx->nzg;
+  ctx->fp64 = cfg->precision == BLGPU_FP64;
+  ctx->esz = ctx->fp64 ? 8 : 4;
+  int rc;
+#define TRY(x) do { rc = (x); if (rc) { g_last_error = ctx->err; blgpu_destroy(ctx); return rc; } } while (0)
+  TRY(check_cuda(ctx, cudaSetDevice(cfg->device), "cudaSetDevice"));
+  TRY(check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking), "cudaStreamCreate"));
+  const size_t box = (size_t)ctx->boxn * ctx->esz;
+  for (int b = 0; b < 3; ++b)
+    for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->S[b][q], box));
+  for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->F1[q], box));
+  TRY(dalloc(ctx, &ctx->P, box));
+  TRY(dalloc(ctx, &ctx->rhs_p, box));
+  if (cfg->les_model) TRY(dalloc(ctx, &ctx->nut, box));
+  Spec &s = ctx->spec;
+  s.N = ctx->nx - 2;
+  s.M = ctx->nz - 2;
+  s.NM = ctx->ny - 1;
+  s.MH = s.M / 2 + 1;
+  s.rx = (s.N + 31) / 32 * 32;
+  TRY(dalloc(ctx, &ctx->R, (size_t)s.NM * s.M * s.rx * ctx->esz));
+  TRY(dalloc(ctx, &ctx->C, (size_t)s.NM * s.MH * s.rx * ctx->esz * 2));
+  TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->dcsum, (size_t)s.NM * s.M * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->dcrow, (size_t)s.NM * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->dcout, (size_t)s.NM * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->sc, sizeof(Scalars)));
+  TRY(dalloc(ctx, (void **)&ctx->d_maxdiv, sizeof(unsigned long long)));
+  // transform tables
+  {
+    const int N = s.N, M = s.M;
+    std::vector<double> tw(2 * N), post(2 * N), zt(2 * M);
+    for (int t = 0; t < N; ++t) {
+      double a = -2.0 * M_PI * (double)t / (double)N;
+      tw[2 * t] = cos(a);
+      tw[2 * t + 1] = sin(a);
+      double b = -M_PI * (double)t / (2.0 * (double)N);
+      post[2 * t] = cos(b);
+      post[2 * t + 1] = sin(b);
+    }
+    for (int m = 0; m < M; ++m) {
+      double a = 2.0 * M_PI * (double)m / (double)M;
+      zt[2 * m] = cos(a);
+      zt[2 * m + 1] = sin(a);
+    }
+    const size_t es2 = 2 * ctx->esz;
+    TRY(dalloc(ctx, &ctx->tw, N * es2));
+    TRY(dalloc(ctx, &ctx->post, N * es2));
+    TRY(dalloc(ctx, &ctx->ztab, M * es2));
+    if (ctx->fp64) {
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, tw.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->post, post.data(), N * es2, cudaMemcpyHostToDevice), "post"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, zt.data(), M * es2, cudaMemcpyHostToDevice), "ztab"));
+    } else {
+      std::vector<float> a(tw.begin(), tw.end()), b(post.begin(), post.end()), c(zt.begin(), zt.end());
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, a.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->post, b.data(), N * es2, cudaMemcpyHostToDevice), "post"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, c.data(), M * es2, cudaMemcpyHostToDevice), "ztab"));
+    }
+    std::vector<int> f = factorize(N);
+    if (f.size() > 24) TRY(set_err(ctx, BLGPU_EINVAL, "DCT length %d has too many factors", N));
+    ctx->pl64.n = ctx->pl32.n = N;
+    ctx->pl64.nst = ctx->pl32.nst = (int)f.size();
+    for (size_t q = 0; q < f.size(); ++q) ctx->pl64.rad[q] = ctx->pl32.rad[q] = f[q];
+    ctx->pl64.tw = (const double2 *)ctx->tw;
+    ctx->pl64.post = (const double2 *)ctx->post;
+    ctx->pl32.tw = (const float2 *)ctx->tw;
+    ctx->pl32.post = (const float2 *)ctx->post;
+    const size_t sm = dct_smem_bytes(N, (int)ctx->esz, dct_lines_per_cta(N, (int)ctx->esz));
+    int dev_sm = 0;
+    cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg->device);
+    if ((long long)sm > dev_sm) TRY(set_err(ctx, BLGPU_EINVAL, "nx=%d needs %zu B shared memory per CTA", ctx->nx, sm));
+  }
+  {
+    Scalars h{};
+    TRY(check_cuda(ctx, cudaMemcpy(ctx->sc, &h, sizeof h, cudaMemcpyHostToDevice), "scalars"));
+  }
+#undef TRY
+  *out = ctx;
+  return BLGPU_OK;
+}
+
+int blgpu_destroy(blgpu_ctx *ctx) {
+  if (!ctx) return BLGPU_OK;
+  if (ctx->cfg.device >= 0) cudaSetDevice(ctx->cfg.device);
+  for (int r = 0; r < 3; ++r)
+    if (ctx->graph[r]) cudaGraphExecDestroy(ctx->graph[r]);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+  return BLGPU_OK;
+}
+
+long long blgpu_device_bytes(const blgpu_ctx *ctx) { return ctx ? ctx->bytes : 0; }
+
+int blgpu_set_grid(blgpu_ctx *ctx, const double *x, const double *y, const double *z) {
+  if (!ctx || !x || !y || !z) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_grid: null argument");
+  const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+  for (int i = 1; i < nx; ++i)
+    if (!(x[i] > x[i - 1])) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_grid: x not increasing at %d", i + 1);
+  for (int j = 1; j < ny; ++j)
+    if (!(y[j] > y[j - 1])) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_grid: y not increasing at %d", j + 1);
+  for (int k = 1; k < nz; ++k)
+    if (!(z[k] > z[k - 1])) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_grid: z not increasing at %d", k + 1);
+  CK(cudaSetDevice(ctx->cfg.device));
+  // initialization.f90:174-222 (faces -> centres -> ghost-padded centres)
+  auto build = [](const double *f, int n, std::vector<double> &F, std::vector<double> &G) {
+    F.assign(n + 1, 0.0);
+    for (int i = 1; i <= n; ++i) F[i] = f[i - 1];
+    const int nm = n - 1;
+    std::vector<double> m(nm + 1);
+    for (int i = 1; i <= nm; ++i) m[i] = 0.5 * (F[i] + F[i + 1]);
+    G.assign(nm + 3, 0.0);
+    for (int i = 1; i <= nm; ++i) G[i + 1] = m[i];
+    G[1] = m[1] - 2.0 * (m[1] - F[1]);
+    G[nm + 2] = m[nm] + 2.0 * (F[n] - m[nm]);
+  };
+  build(x, nx, ctx->x, ctx->xg);
+  build(y, ny, ctx->y, ctx->yg);
+  build(z, nz, ctx->z, ctx->zg);
+  auto minsp = [](const std::vector<double> &G, int ng) {
+    double mn = INFINITY;
+    for (int i = 2; i <= ng; ++i) mn = std::min(mn, G[i] - G[i - 1]);
+    return mn;
+  };
+  ctx->dxmin = minsp(ctx->xg, ctx->nxg);
+  ctx->dymin = minsp(ctx->yg, ctx->nyg);
+  ctx->dzmin = minsp(ctx->zg, ctx->nzg);
+  const double nu = ctx->cfg.nu, cfla = fabs(ctx->cfg.cfl);
+  ctx->dtvis = std::min(std::min(cfla * (ctx->dxmin * ctx->dxmin) / nu, cfla * (ctx->dymin * ctx->dymin) / nu),
+                        cfla * (ctx->dzmin * ctx->dzmin) / nu);
+  // weights (initialization.f90:482-484)
+  ctx->w0.assign(ny + 2, 0.0);
+  ctx->w1.assign(ny + 2, 0.0);
+  for (int j = 1; j <= ny; ++j) {
+    ctx->w0[j] = (ctx->yg[j + 1] - ctx->y[j]) / (ctx->yg[j + 1] - ctx->yg[j]);
+    ctx->w1[j] = 1.0 - ctx->w0[j];
+  }
+  // Dyy rows j = 2..nyg-1 (initialization.f90:395-425), stored by b = j-2
+  const Spec &s = ctx->spec;
+  ctx->dd.assign(s.NM, 0.0);
+  ctx->dl.assign(s.NM, 0.0);
+  ctx->du.assign(s.NM, 0.0);
+  for (int j = 2; j <= ctx->nyg - 1; ++j) {
+    const double *Y = ctx->y.data(), *YG = ctx->yg.data();
+    double a = 1.0 / (Y[j] - Y[j - 1]) / (YG[j + 1] - YG[j]);
+    double b = 1.0 / (Y[j] - Y[j - 1]) * (-1.0 / (YG[j + 1] - YG[j]) - 1.0 / (YG[j] - YG[j - 1]));
+    double c = 1.0 / (Y[j] - Y[j - 1]) / (YG[j] - YG[j - 1]);
+    double d = b;
+    if (j == 2) d = b + c;
+    if (j == ctx->nyg - 1) d = a + b;
+    ctx->dd[j - 2] = d;
+    ctx->dl[j - 2] = c;
+    ctx->du[j - 2] = a;
+  }
+  // modified wavenumbers (initialization.f90:329-344); dx = dxmin, dz = dzmin
+  const double pi = 4.0 * atan(1.0);
+  ctx->kxx.assign(s.N, 0.0);
+  for (int i = 0; i < s.N; ++i)
+    ctx->kxx[i] = 2.0 * (cos(pi * (double)i / (double)s.N) - 1.0) / (ctx->dxmin * ctx->dxmin);
+  ctx->kzz.assign(s.MH, 0.0);
+  const int half = (int)ceil((double)s.M / 2.0);
+  for (int k = 0; k < s.MH; ++k) {
+    if (k <= half)
+      ctx->kzz[k] = 2.0 * (cos(2.0 * pi * (double)k / (double)s.M) - 1.0) / (ctx->dzmin * ctx->dzmin);
+    else
+      ctx->kzz[k] = 2.0 * (cos(2.0 * pi * (double)(-s.M + k) / (double)s.M) - 1.0) / (ctx->dzmin * ctx->dzmin);
+  }
+  // length_y of the mass balance (boundary_conditions.f90:242-246)
+  ctx->length_y = 0.0;
+  for (int j = 2; j <= ctx->nyg - 1; ++j) ctx->length_y = ctx->length_y + ctx->y[j] - ctx->y[j - 1];
+  // metric tables: per axis F, C, rF, rC (1-based), then raw grids and weights
+  const int nxt = ctx->nxg + 2, nyt = ctx->nyg + 2, nzt = ctx->nzg + 2;
+  auto axis = [](const std::vector<double> &Fv, int n, const std::vector<double> &G, int ng, int len,
+                 std::vector<double> &out) {
+    std::vector<double> F(len, 1.0), C(len, 1.0);
+    for (int i = 2; i <= n; ++i) F[i] = Fv[i] - Fv[i - 1];
+    for (int i = 1; i <= ng - 1; ++i) C[i] = G[i + 1] - G[i];
+    for (int i = 0; i < len; ++i) out.push_back(F[i]);
+    for (int i = 0; i < len; ++i) out.push_back(C[i]);
+    for (int i = 0; i < len; ++i) out.push_back(1.0 / F[i]);
+    for (int i = 0; i < len; ++i) out.push_back(1.0 / C[i]);
+  };
+  std::vector<double> h;
+  axis(ctx->x, nx, ctx->xg, ctx->nxg, nxt, h);
+  axis(ctx->y, ny, ctx->yg, ctx->nyg, nyt, h);
+  axis(ctx->z, nz, ctx->zg, ctx->nzg, nzt, h);
+  const size_t off_w = h.size();
+  for (int j = 0; j < nyt; ++j) h.push_back(j < (int)ctx->w0.size() ? ctx->w0[j] : 0.0);
+  for (int j = 0; j < nyt; ++j) h.push_back(j < (int)ctx->w1.size() ? ctx->w1[j] : 0.0);
+  const size_t off_raw = h.size();
+  auto pushv = [&](const std::vector<double> &v, int len) {
+    for (int i = 0; i < len; ++i) h.push_back(i < (int)v.size() ? v[i] : 0.0);
+  };
+  pushv(ctx->x, nxt); pushv(ctx->xg, nxt); pushv(ctx->y, nyt); pushv(ctx->yg, nyt); pushv(ctx->z, nzt); pushv(ctx->zg, nzt);
+  if (!ctx->d_geo) {
+    int rc = dalloc(ctx, (void **)&ctx->d_geo, h.size() * sizeof(double));
+    if (rc) return rc;
+    rc = dalloc(ctx, (void **)&ctx->f_geo, h.size() * sizeof(float));
+    if (rc) return rc;
+    rc = dalloc(ctx, (void **)&ctx->d_spec, (size_t)(3 * s.NM + s.N + s.MH) * sizeof(double));
+    if (rc) return rc;
+    rc = dalloc(ctx, (void **)&ctx->qx_part, (size_t)bc_x_parts(Geo{0, 0, 0, 0, ctx->nyg, ctx->nzg}) * sizeof(double) + 64);
+    if (rc) return rc;
+  }
+  std::vector<float> hf(h.begin(), h.end());
+  CK(cudaMemcpy(ctx->d_geo, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->f_geo, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  std::vector<double> sp;
+  sp.insert(sp.end(), ctx->dd.begin(), ctx->dd.end());
+  sp.insert(sp.end(), ctx->dl.begin(), ctx->dl.end());
+  sp.insert(sp.end(), ctx->du.begin(), ctx->du.end());
+  sp.insert(sp.end(), ctx->kxx.begin(), ctx->kxx.end());
+  sp.insert(sp.end(), ctx->kzz.begin(), ctx->kzz.end());
+  CK(cudaMemcpy(ctx->d_spec, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // views
+  Geo &g = ctx->geo;
+  g.nx = nx; g.ny = ny; g.nz = nz; g.nxg = ctx->nxg; g.nyg = ctx->nyg; g.nzg = ctx->nzg;
+  g.px = ctx->px; g.py = ctx->py; g.plane = ctx->plane;
+  const double *D = ctx->d_geo;
+  g.ax = Axis{D, D + nxt, D + 2 * nxt, D + 3 * nxt};
+  D += 4 * nxt;
+  g.ay = Axis{D, D + nyt, D + 2 * nyt, D + 3 * nyt};
+  D += 4 * nyt;
+  g.az = Axis{D, D + nzt, D + 2 * nzt, D + 3 * nzt};
+  g.w0 = ctx->d_geo + off_w;
+  g.w1 = g.w0 + nyt;
+  const double *Rw = ctx->d_geo + off_raw;
+  g.x = Rw; g.xg = Rw + nxt; g.y = Rw + 2 * nxt; g.yg = g.y + nyt; g.z = g.yg + nyt; g.zg = g.z + nzt;
+  g.nu = nu; g.dpdx = ctx->cfg.dpdx; g.dpdz = ctx->cfg.dpdz;
+  auto met = [&](auto *B, auto &m, auto cast) {
+    auto *p = B;
+    m.xF = p; m.xC = p + nxt; m.xrF = p + 2 * nxt; m.xrC = p + 3 * nxt; p += 4 * nxt;
+    m.yF = p; m.yC = p + nyt; m.yrF = p + 2 * nyt; m.yrC = p + 3 * nyt; p += 4 * nyt;
+    m.zF = p; m.zC = p + nzt; m.zrF = p + 2 * nzt; m.zrC = p + 3 * nzt;
+    m.w0 = B + off_w; m.w1 = B + off_w + nyt;
+    m.nu = cast(nu); m.dpdx = cast(ctx->cfg.dpdx); m.dpdz = cast(ctx->cfg.dpdz);
+  };
+  met(ctx->d_geo, ctx->m64, [](double v) { return v; });
+  met(ctx->f_geo, ctx->m32, [](double v) { return (float)v; });
+  drop_graphs(ctx);
+  ctx->have_grid = true;
+  return BLGPU_OK;
+}
+
+int blgpu_set_boundary(blgpu_ctx *ctx, const double *U_inlet, const double *V_inlet, const double *W_inlet,
+                       const double *U_top, const double *V_top, const double *W_top) {
+  if (!ctx || !U_inlet || !V_inlet || !W_inlet || !U_top || !V_top || !W_top)
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_boundary: null argument");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const int nyg = ctx->nyg, ny = ctx->ny, nx = ctx->nx, nxg = ctx->nxg;
+  // 1-based vectors: [0]=unused
+  std::vector<double> h;
+  auto push = [&](const double *v, int n) {
+    h.push_back(0.0);
+    for (int i = 0; i < n; ++i) h.push_back(v[i]);
+    h.push_back(0.0);
+  };
+  push(U_inlet, nyg); push(V_inlet, ny); push(W_inlet, nyg); push(U_top, nx); push(V_top, nxg); push(W_top, nxg);
+  if (!ctx->d_bc) {
+    int rc = dalloc(ctx, (void **)&ctx->d_bc, h.size() * sizeof(double));
+    if (rc) return rc;
+  }
+  CK(cudaMemcpy(ctx->d_bc, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const double *p = ctx->d_bc;
+  ctx->bc.U_inlet = p; p += nyg + 2;
+  ctx->bc.V_inlet = p; p += ny + 2;
+  ctx->bc.W_inlet = p; p += nyg + 2;
+  ctx->bc.U_top = p; p += nx + 2;
+  ctx->bc.V_top = p; p += nxg + 2;
+  ctx->bc.W_top = p;
+  // Qy of the mass balance: V(i,1,k) = 0 and V(i,ny,k) = V_top(i) when it is
+  // evaluated (boundary_conditions.f90:230-253), so it is a constant of the run
+  if (ctx->have_grid) {
+    double qy = 0.0;
+    for (int i = 2; i <= ctx->nxg - 2; ++i) {
+      double s = 0.0;
+      for (int k = 2; k <= ctx->nzg - 2; ++k) s += (0.0 - V_top[i - 1]) * (ctx->x[i] - ctx->x[i - 1]);
+      qy = qy + s;
+    }
+    ctx->qy = qy;
+  } else {
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_set_boundary: call blgpu_set_grid first");
+  }
+  drop_graphs(ctx);
+  ctx->have_bc = true;
+  return BLGPU_OK;
+}
+
+int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const double *zmode, const double *tmode,
+                           const double *qu, const double *qv, const double *qw) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (n_modes < 0 || m_modes < 0) return set_err(ctx, BLGPU_EINVAL, "negative mode count");
+  CK(cudaSetDevice(ctx->cfg.device));
+  ctx->bc.n_modes = 0;
+  ctx->bc.m_modes = 0;
+  if (n_modes == 0 || m_modes == 0) return BLGPU_OK;
+  if (!zmode || !tmode || !qu || !qv || !qw) return set_err(ctx, BLGPU_EINVAL, "null mode array");
+  const size_t nq = (size_t)n_modes * m_modes;
+  std::vector<double> h;
+  h.insert(h.end(), zmode, zmode + n_modes);
+  h.insert(h.end(), tmode, tmode + m_modes);
+  if (h.size() & 1) h.push_back(0.0);  // keep the complex arrays 16-byte aligned
+  const size_t oq = h.size();
+  h.insert(h.end(), qu, qu + 2 * nq * ctx->nyg);
+  const size_t ov = h.size();
+  h.insert(h.end(), qv, qv + 2 * nq * ctx->ny);
+  const size_t ow = h.size();
+  h.insert(h.end(), qw, qw + 2 * nq * ctx->nyg);
+  void *p = nullptr;
+  int rc = dalloc(ctx, &p, h.size() * sizeof(double));
+  if (rc) return rc;
+  ctx->d_modes = (double *)p;
+  CK(cudaMemcpy(p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->bc.zmode = ctx->d_modes;
+  ctx->bc.tmode = ctx->d_modes + n_modes;
+  ctx->bc.qu = (const double2 *)(ctx->d_modes + oq);
+  ctx->bc.qv = (const double2 *)(ctx->d_modes + ov);
+  ctx->bc.qw = (const double2 *)(ctx->d_modes + ow);
+  ctx->bc.n_modes = n_modes;
+  ctx->bc.m_modes = m_modes;
+  drop_graphs(ctx);
+  return BLGPU_OK;
+}
+
+}  // extern "C"
+
+// ---- host <-> box layout ----
+template <typename T>
+static void to_box(const blgpu_ctx *c, const double *a, int n1, int n2, int n3, std::vector<T> &box) {
+  box.assign((size_t)c->boxn, (T)0);
+  for (int k = 0; k < n3; ++k)
+    for (int j = 0; j < n2; ++j) {
+      const double *src = a + ((size_t)k * n2 + j) * n1;
+      T *dst = box.data() + ((size_t)k * c->py + j) * c->px;
+      for (int i = 0; i < n1; ++i) dst[i] = (T)src[i];
+    }
+}
+
+template <typename T>
+static void from_box(const blgpu_ctx *c, const std::vector<T> &box, int n1, int n2, int n3, double *a) {
+  for (int k = 0; k < n3; ++k)
+    for (int j = 0; j < n2; ++j) {
+      double *dst = a + ((size_t)k * n2 + j) * n1;
+      const T *src = box.data() + ((size_t)k * c->py + j) * c->px;
+      for (int i = 0; i < n1; ++i) dst[i] = (double)src[i];
+    }
+}
+
+static int upload_field(blgpu_ctx *ctx, void *dst, const double *a, int n1, int n2, int n3) {
+  if (ctx->fp64) {
+    std::vector<double> b;
+    to_box(ctx, a, n1, n2, n3, b);
+    CK(cudaMemcpy(dst, b.data(), b.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> b;
+    to_box(ctx, a, n1, n2, n3, b);
+    CK(cudaMemcpy(dst, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return BLGPU_OK;
+}
+
+static int download_field(blgpu_ctx *ctx, const void *src, double *a, int n1, int n2, int n3) {
+  if (ctx->fp64) {
+    std::vector<double> b((size_t)ctx->boxn);
+    CK(cudaMemcpy(b.data(), src, b.size() * 8, cudaMemcpyDeviceToHost));
+    from_box(ctx, b, n1, n2, n3, a);
+  } else {
+    std::vector<float> b((size_t)ctx->boxn);
+    CK(cudaMemcpy(b.data(), src, b.size() * 4, cudaMemcpyDeviceToHost));
+    from_box(ctx, b, n1, n2, n3, a);
+  }
+  return BLGPU_OK;
+}
+
+extern "C" {
+
+int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t) {
+  if (!ctx || !nu_t) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_nu_t: null argument");
+  if (!ctx->nut) return set_err(ctx, BLGPU_ESTATE, "blgpu_set_nu_t: context created with LES=0");
+  CK(cudaSetDevice(ctx->cfg.device));
+  return upload_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);
+}
+
+int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t) {
+  if (!ctx || !U || !V || !W) return set_err(ctx, BLGPU_EINVAL, "blgpu_upload_state: null argument");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->cur = 0;
+  ctx->old = 1;
+  for (int b : {ctx->cur, ctx->old}) {
+    int rc = upload_field(ctx, ctx->S[b][0], U, ctx->nx, ctx->nyg, ctx->nzg);
+    if (!rc) rc = upload_field(ctx, ctx->S[b][1], V, ctx->nxg, ctx->ny, ctx->nzg);
+    if (!rc) rc = upload_field(ctx, ctx->S[b][2], W, ctx->nxg, ctx->nyg, ctx->nz);
+    if (rc) return rc;
+  }
+  Scalars h{};
+  CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
+  h.t = t;
+  h.to = t;
+  h.lmax[0] = h.lmax[1] = h.lmax[2] = 0ull;
+  CK(cudaMemcpy(ctx->sc, &h, sizeof h, cudaMemcpyHostToDevice));
+  ctx->have_state = true;
+  return BLGPU_OK;
+}
+
+int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double *P, double *t) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_download_state: no state uploaded");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  int rc = 0;
+  if (U && !rc) rc = download_field(ctx, ctx->S[ctx->cur][0], U, ctx->nx, ctx->nyg, ctx->nzg);
+  if (V && !rc) rc = download_field(ctx, ctx->S[ctx->cur][1], V, ctx->nxg, ctx->ny, ctx->nzg);
+  if (W && !rc) rc = download_field(ctx, ctx->S[ctx->cur][2], W, ctx->nxg, ctx->nyg, ctx->nz);
+  if (P && !rc) rc = download_field(ctx, ctx->P, P, ctx->nxg, ctx->nyg, ctx->nzg);
+  if (rc) return rc;
+  if (t) {
+    Scalars h{};
+    CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
+    *t = h.t;
+  }
+  return BLGPU_OK;
+}
+
+int blgpu_set_dt(blgpu_ctx *ctx, double dt) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(&ctx->sc->dt, &dt, sizeof dt, cudaMemcpyHostToDevice));
+  return BLGPU_OK;
+}
+
+int blgpu_get_time(blgpu_ctx *ctx, double *t, double *dt) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  Scalars h{};
+  CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
+  if (t) *t = h.t;
+  if (dt) *dt = h.dt;
+  return BLGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// step orchestration (all enqueued on ctx->st; capturable)
+// ---------------------------------------------------------------------------
+template <typename T>
+static void enq_bc(blgpu_ctx *ctx, int b, int o, int rk_step) {
+  T **S = reinterpret_cast<T **>(ctx->S[b]);
+  T **So = reinterpret_cast<T **>(ctx->S[o]);
+  launch_bc<T>(ctx->geo, ctx->bc, S[0], S[1], S[2], So[0], So[1], So[2], ctx->sc, ctx->rk_t[rk_step], ctx->qx_part,
+               ctx->qy, ctx->length_y, ctx->st);
+}
+
+template <typename T>
+static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
+  T **S = reinterpret_cast<T **>(ctx->S[b]);
+  typedef typename vec2<T>::type T2;
+  const Spec &s = ctx->spec;
+  const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
+  const bool mixed = !ctx->fp64;
+  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, mixed ? ctx->dcsum : nullptr, ctx->st);
+  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->st);
+  const double *sp = ctx->d_spec;
+  launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp, sp + s.NM, sp + 2 * s.NM, sp + 3 * s.NM, sp + 3 * s.NM + s.N,
+                   mixed ? ctx->dcsum : nullptr, ctx->dcrow, mixed ? ctx->dcout : nullptr, ctx->st);
+  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->st);
+  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->st);
+  const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
+  launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->dcout : nullptr, S[0], S[1], S[2],
+                    (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->st);
+}
+
+template <typename T>
+static void enq_rhs(blgpu_ctx *ctx, int mode, int in, int o, int outb, double c1, double c2) {
+  T **Si = reinterpret_cast<T **>(ctx->S[in]);
+  T **So = reinterpret_cast<T **>(ctx->S[o]);
+  T **Sn = reinterpret_cast<T **>(ctx->S[outb]);
+  T **F = reinterpret_cast<T **>(ctx->F1);
+  const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
+  launch_rhs_rk<T>(ctx->geo, m, mode, ctx->cfg.les_model != 0, Si[0], Si[1], Si[2], (const T *)ctx->nut, So[0], So[1],
+                   So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->st);
+}
+
+// One time step from buffer a.  Returns the index of the new state buffer.
+template <typename T>
+static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
+  const int b = (a + 1) % 3, c = (a + 2) % 3;
+  if (with_dt && ctx->cfg.cfl > 0) {
+    T **S = reinterpret_cast<T **>(ctx->S[a]);
+    launch_dt<T>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+  }
+  launch_set_time(ctx->sc, 0, 0.0, ctx->st);
+  auto sub = [&](int mode, int in, int outb, double c1, double c2, double tc, int rk_step) {
+    enq_rhs<T>(ctx, mode, in, a, outb, c1, c2);
+    launch_set_time(ctx->sc, 1, tc, ctx->st);
+    enq_bc<T>(ctx, outb, a, rk_step);
+    enq_projection<T>(ctx, outb, rk_step);
+    enq_bc<T>(ctx, outb, a, rk_step);
+  };
+  switch (ctx->cfg.rk_scheme) {
+    case 3:  // time_integration.f90:305-465, initialization.f90:517-530
+      sub(1, a, b, 8.0 / 15.0, 0.0, 8.0 / 15.0, 1);
+      sub(2, b, c, 1.0 / 4.0, 5.0 / 12.0, 2.0 / 3.0, 2);
+      sub(3, c, b, 1.0 / 4.0, 3.0 / 4.0, 1.0, 3);
+      return b;
+    case 2:  // time_integration.f90:145-300, initialization.f90:504-513
+      sub(1, a, b, 1.0 / 2.0, 0.0, 1.0 / 2.0, 1);
+      sub(2, b, c, 0.0, 1.0, 1.0, 2);
+      return c;
+    default:  // Euler, time_integration.f90:24-114 (rk_step = 3)
+      sub(1, a, b, 1.0, 0.0, 1.0, 3);
+      return b;
+  }
+}
+
+static int step_once(blgpu_ctx *ctx, bool with_dt) {
+  int nb = ctx->fp64 ? enq_step<double>(ctx, ctx->cur, with_dt) : enq_step<float>(ctx, ctx->cur, with_dt);
+  ctx->old = ctx->cur;
+  ctx->cur = nb;
+  return BLGPU_OK;
+}
+
+extern "C" {
+
+int blgpu_time_step(blgpu_ctx *ctx) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_time_step: grid, boundary and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  step_once(ctx, false);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_advance(blgpu_ctx *ctx, int nsteps) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (nsteps < 0) return set_err(ctx, BLGPU_EINVAL, "blgpu_advance: nsteps < 0");
+  if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_advance: grid, boundary and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  for (int n = 0; n < nsteps; ++n) {
+    const int a = ctx->cur;
+    if (!ctx->graph[a]) {
+      cudaGraph_t gr = nullptr;
+      CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeRelaxed));
+      const int nb = ctx->fp64 ? enq_step<double>(ctx, a, true) : enq_step<float>(ctx, a, true);
+      cudaError_t e = cudaStreamEndCapture(ctx->st, &gr);
+      if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&ctx->graph[a], gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) return check_cuda(ctx, e, "cudaGraphInstantiate");
+      ctx->graph_next[a] = nb;
+    }
+    CK(cudaGraphLaunch(ctx->graph[a], ctx->st));
+    ctx->old = a;
+    ctx->cur = ctx->graph_next[a];
+  }
+  CK(cudaGetLastError());
+  return BLGPU_OK;
+}
+
+int blgpu_sync(blgpu_ctx *ctx) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_compute_dt(blgpu_ctx *ctx, double *dt) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_compute_dt: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->cfg.cfl < 0) {
+    double v = -ctx->cfg.cfl;
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(&ctx->sc->dt, &v, sizeof v, cudaMemcpyHostToDevice));
+  } else if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_dt<double>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_dt<float>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  if (dt) CK(cudaMemcpy(dt, &ctx->sc->dt, sizeof(double), cudaMemcpyDeviceToHost));
+  return BLGPU_OK;
+}
+
+int blgpu_compute_rhs(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double *rhs_u,
+                      double *rhs_v, double *rhs_w) {
+  if (!ctx || !U || !V || !W) return set_err(ctx, BLGPU_EINVAL, "blgpu_compute_rhs: null argument");
+  if (!ctx->have_grid) return set_err(ctx, BLGPU_ESTATE, "blgpu_compute_rhs: no grid");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  // scratch buffer: the one that is neither the current state nor Uo
+  const int sb = 3 - ctx->cur - ctx->old;
+  int rc = upload_field(ctx, ctx->S[sb][0], U, ctx->nx, ctx->nyg, ctx->nzg);
+  if (!rc) rc = upload_field(ctx, ctx->S[sb][1], V, ctx->nxg, ctx->ny, ctx->nzg);
+  if (!rc) rc = upload_field(ctx, ctx->S[sb][2], W, ctx->nxg, ctx->nyg, ctx->nz);
+  if (rc) return rc;
+  if (ctx->fp64) enq_rhs<double>(ctx, 0, sb, sb, sb, 0.0, 0.0);
+  else enq_rhs<float>(ctx, 0, sb, sb, sb, 0.0, 0.0);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz, nxg = ctx->nxg, nyg = ctx->nyg, nzg = ctx->nzg;
+  std::vector<double> full;
+  auto grab = [&](int q, double *out, int i1, int j1, int k1) -> int {
+    // interior (2:i1, 2:j1, 2:k1) of component q, compact
+    if (!out) return BLGPU_OK;
+    full.assign((size_t)nxg * nyg * nzg, 0.0);
+    int r = download_field(ctx, ctx->F1[q], full.data(), nxg, nyg, nzg);
+    if (r) return r;
+    const int e1 = i1 - 1, e2 = j1 - 1;
+    for (int k = 2; k <= k1; ++k)
+      for (int j = 2; j <= j1; ++j)
+        for (int i = 2; i <= i1; ++i)
+          out[((size_t)(k - 2) * e2 + (j - 2)) * e1 + (i - 2)] = full[((size_t)(k - 1) * nyg + (j - 1)) * nxg + (i - 1)];
+    return BLGPU_OK;
+  };
+  rc = grab(0, rhs_u, nx - 1, nyg - 1, nzg - 1);
+  if (!rc) rc = grab(1, rhs_v, nxg - 1, ny - 1, nzg - 1);
+  if (!rc) rc = grab(2, rhs_w, nxg - 1, nyg - 1, nz - 1);
+  return rc;
+}
+
+int blgpu_apply_bc(blgpu_ctx *ctx, int rk_step) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (rk_step < 1 || rk_step > 3) return set_err(ctx, BLGPU_EINVAL, "blgpu_apply_bc: rk_step %d", rk_step);
+  if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_apply_bc: grid, boundary and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) enq_bc<double>(ctx, ctx->cur, ctx->old, rk_step);
+  else enq_bc<float>(ctx, ctx->cur, ctx->old, rk_step);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_projection(blgpu_ctx *ctx, int rk_step) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_projection: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) enq_projection<double>(ctx, ctx->cur, rk_step);
+  else enq_projection<float>(ctx, ctx->cur, rk_step);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_get_rhs_p(blgpu_ctx *ctx, double *rhs_p) {
+  if (!ctx || !rhs_p) return set_err(ctx, BLGPU_EINVAL, "blgpu_get_rhs_p: null argument");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  const int nxg = ctx->nxg, nyg = ctx->nyg, nzg = ctx->nzg;
+  std::vector<double> full((size_t)nxg * nyg * nzg);
+  int rc = download_field(ctx, ctx->rhs_p, full.data(), nxg, nyg, nzg);
+  if (rc) return rc;
+  const int e1 = nxg - 2, e2 = nyg - 2;
+  for (int k = 2; k <= nzg; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i)
+        rhs_p[((size_t)(k - 2) * e2 + (j - 2)) * e1 + (i - 2)] =
+            (k == nzg) ? 0.0 : full[((size_t)(k - 1) * nyg + (j - 1)) * nxg + (i - 1)];
+  return BLGPU_OK;
+}
+
+int blgpu_max_divergence(blgpu_ctx *ctx, double *max_div) {
+  if (!ctx || !max_div) return set_err(ctx, BLGPU_EINVAL, "blgpu_max_divergence: null argument");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_max_divergence: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaMemsetAsync(ctx->d_maxdiv, 0, sizeof(unsigned long long), ctx->st));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_maxdiv<double>(ctx->geo, S[0], S[1], S[2], ctx->d_maxdiv, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_maxdiv<float>(ctx->geo, S[0], S[1], S[2], ctx->d_maxdiv, ctx->st);
+  }
+  CK(cudaGetLastError());
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, ctx->d_maxdiv, sizeof bits, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  double v;
+  memcpy(&v, &bits, sizeof v);
+  *max_div = v;
+  return BLGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+// kernels.cuh -- launcher declarations shared by the kernel and host files.
+#pragma once
+#include "common.cuh"
+
+namespace blgpu {
+
+// metric tables in the storage precision T (1-based, see Axis)
+template <typename T> struct MetT {
+  const T *xF, *xC, *xrF, *xrC;
+  const T *yF, *yC, *yrF, *yrC;
+  const T *zF, *zC, *zrF, *zrC;
+  const T *w0, *w1;
+  T nu, dpdx, dpdz;
+};
+
+// boundary data (FP64, 1-based like the Fortran vectors)
+struct BcData {
+  const double *U_inlet, *V_inlet, *W_inlet;  // (nyg) (ny) (nyg)
+  const double *U_top, *V_top, *W_top;        // (nx) (nxg) (nxg)
+  int n_modes, m_modes;
+  const double *zmode, *tmode;                // (n) (m)
+  const double2 *qu, *qv, *qw;                // (nyg|ny, n, m) complex
+  const double *ut, *vt, *wt;                 // optional precomputed inflow perturbation planes
+};
+
+// ---- stencil.cu ----
+template <typename T>
+void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *U, const T *V, const T *W,
+                   const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
+                   const Scalars *sc, double c1, double c2, cudaStream_t st);
+template <typename T>
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
+                    const Scalars *sc, int save_p, cudaStream_t st);
+int bc_x_parts(const Geo &g);
+template <typename T>
+void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
+               Scalars *sc, double rkt, double *qx_part, double qy, double length_y, cudaStream_t st);
+template <typename T>
+void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
+               cudaStream_t st);
+void launch_set_time(Scalars *sc, int phase, double coef, cudaStream_t st);
+template <typename T>
+void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st);
+
+// ---- spectral.cu ----
+// Transform plan of one axis length n (device tables)
+template <typename T> struct FftPlan {
+  int n;
+  int nst;            // number of stages
+  int rad[24];        // radices, applied in order
+  const typename vec2<T>::type *tw;    // W_n^t = exp(-2 pi i t / n), t = 0..n-1
+  const typename vec2<T>::type *post;  // exp(-i pi k / (2n)), k = 0..n-1 (DCT twiddle)
+};
+
+struct Spec {  // spectral layout of the Poisson solve
+  int N;      // nxp = nx-2 (DCT length)
+  int M;      // nzp = nz-2 (DFT length)
+  int NM;     // nm  = ny-1 (unknowns per mode)
+  int MH;     // M/2 + 1 (stored z wavenumbers)
+  int rx;     // row pitch of the spectral arrays (>= N, multiple of 32)
+};
+
+template <typename T>
+void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
+                    double *dc_sum, cudaStream_t st);
+template <typename T>
+void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
+                  cudaStream_t st);
+template <typename T>
+void launch_thomas(const Spec &s, typename vec2<T>::type *C, double *piv, const double *dd, const double *dl,
+                   const double *du, const double *kxx, const double *kzz, const double *dc_lines,
+                   double *dc_rows, double *dc_out, cudaStream_t st);
+template <typename T>
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, cudaStream_t st);
+size_t dct_smem_bytes(int n, int elem_bytes, int lines);
+int dct_lines_per_cta(int n, int elem_bytes);
+
+}  // namespace blgpu

@@ -1,0 +1,560 @@
+// stencil.cu -- finite-difference kernels of the step path (compiled with
+// -fmad=false so the FP64 instantiation evaluates every expression in the
+// order and rounding of the Fortran source, with no fused multiply-adds).
+//
+//   k_rhs_rk      RHS of u, v, w (equations.f90:24-415) fused with the RK
+//                 substep update (time_integration.f90:351-458)
+//   k_project     project_velocity (projection.f90:355-386) fused with the
+//                 pressure save of solve_poisson_equation (projection.f90:75-85)
+//   k_bc_*        apply_boundary_conditions_gpu (boundary_conditions.f90:127-262)
+//   k_dt_*        compute_dt (time_integration.f90:528-591)
+//   k_maxdiv      check_divergence (projection.f90:391-413)
+#include "kernels.cuh"
+
+namespace blgpu {
+
+// ---------------------------------------------------------------------------
+// division policy: the FP64 path divides exactly where the source divides;
+// the FP32 path multiplies by the reciprocal table instead.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double qdiv(double a, double b, double) { return a / b; }
+__device__ __forceinline__ float qdiv(float a, float, float rb) { return a * rb; }
+
+template <typename T> struct Ld {
+  const T *__restrict__ p;
+  long long sx, sy, sz;  // strides: 1, px, plane
+  __device__ __forceinline__ T operator()(long long c, int di, int dj, int dk) const {
+    return __ldg(p + c + di + dj * sy + dk * sz);
+  }
+};
+
+// RHS of u at (i,j,k), equations.f90:53-91 (DNS) / :98-129 (LES)
+template <typename T, bool LES>
+__device__ __forceinline__ T rhs_u_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
+                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+  const T h = (T)0.5;
+  T uc = U(c, 0, 0, 0), ue = U(c, 1, 0, 0), uw = U(c, -1, 0, 0);
+  T un = U(c, 0, 1, 0), us = U(c, 0, -1, 0), ut = U(c, 0, 0, 1), ub = U(c, 0, 0, -1);
+  T a = h * (uc + ue), b = h * (uw + uc);
+  T r = -qdiv(a * a - b * b, m.xC[i], m.xrC[i]);
+  T t1 = (m.w0[j] * uc + m.w1[j] * un) * h * (V(c, 0, 0, 0) + V(c, 1, 0, 0));
+  T t2 = (m.w0[j - 1] * us + m.w1[j - 1] * uc) * h * (V(c, 0, -1, 0) + V(c, 1, -1, 0));
+  r = r - qdiv(t1 - t2, m.yF[j], m.yrF[j]);
+  T t3 = h * (uc + ut) * h * (W(c, 0, 0, 0) + W(c, 1, 0, 0));
+  T t4 = h * (ub + uc) * h * (W(c, 0, 0, -1) + W(c, 1, 0, -1));
+  r = r - qdiv(t3 - t4, m.zF[k], m.zrF[k]);
+  if (!LES) {
+    T vx = qdiv(m.xrF[i + 1] * (ue - uc) - m.xrF[i] * (uc - uw), m.xC[i], m.xrC[i]);
+    T vy = qdiv(qdiv(un - uc, m.yC[j], m.yrC[j]) - qdiv(uc - us, m.yC[j - 1], m.yrC[j - 1]), m.yF[j], m.yrF[j]);
+    T vz = qdiv(m.zrC[k] * (ut - uc) - m.zrC[k - 1] * (uc - ub), m.zF[k], m.zrF[k]);
+    r = r + m.dpdx + m.nu * (vx + vy + vz);
+  } else {
+    const T q = (T)0.25;
+    T n0 = N(c, 0, 0, 0), nE = N(c, 1, 0, 0);
+    T nu_x1 = m.nu + n0, nu_x2 = m.nu + nE;
+    T nu_y1 = m.nu + h * (m.w0[j - 1] * N(c, 0, -1, 0) + m.w1[j - 1] * n0 + m.w0[j - 1] * N(c, 1, -1, 0) + m.w1[j - 1] * nE);
+    T nu_y2 = m.nu + h * (m.w0[j] * n0 + m.w1[j] * N(c, 0, 1, 0) + m.w0[j] * nE + m.w1[j] * N(c, 1, 1, 0));
+    T nu_z1 = m.nu + q * (n0 + N(c, 0, 0, -1) + nE + N(c, 1, 0, -1));
+    T nu_z2 = m.nu + q * (n0 + N(c, 0, 0, 1) + nE + N(c, 1, 0, 1));
+    T t2p = qdiv(un - uc, m.yC[j], m.yrC[j]);
+    T t2m = qdiv(uc - us, m.yC[j - 1], m.yrC[j - 1]);
+    r = r + m.dpdx +
+        qdiv(qdiv(nu_x2, m.xF[i + 1], m.xrF[i + 1]) * (ue - uc) - qdiv(nu_x1, m.xF[i], m.xrF[i]) * (uc - uw), m.xC[i], m.xrC[i]) +
+        qdiv(nu_y2 * t2p - nu_y1 * t2m, m.yF[j], m.yrF[j]) +
+        qdiv(qdiv(nu_z2, m.zC[k], m.zrC[k]) * (ut - uc) - qdiv(nu_z1, m.zC[k - 1], m.zrC[k - 1]) * (uc - ub), m.zF[k], m.zrF[k]);
+  }
+  return r;
+}
+
+// RHS of v at (i,j,k), equations.f90:188-227 (DNS) / :238-266 (LES)
+template <typename T, bool LES>
+__device__ __forceinline__ T rhs_v_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
+                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+  const T h = (T)0.5;
+  T vc = V(c, 0, 0, 0), ve = V(c, 1, 0, 0), vw = V(c, -1, 0, 0);
+  T vn = V(c, 0, 1, 0), vs = V(c, 0, -1, 0), vt = V(c, 0, 0, 1), vb = V(c, 0, 0, -1);
+  T a = h * (vc + vn), b = h * (vs + vc);
+  T r = -qdiv(a * a - b * b, m.yC[j], m.yrC[j]);
+  T t1 = (m.w0[j] * U(c, 0, 0, 0) + m.w1[j] * U(c, 0, 1, 0)) * h * (vc + ve);
+  T t2 = (m.w0[j] * U(c, -1, 0, 0) + m.w1[j] * U(c, -1, 1, 0)) * h * (vw + vc);
+  r = r - qdiv(t1 - t2, m.xF[i], m.xrF[i]);
+  T t3 = h * (vc + vt) * (m.w0[j] * W(c, 0, 0, 0) + m.w1[j] * W(c, 0, 1, 0));
+  T t4 = h * (vb + vc) * (m.w0[j] * W(c, 0, 0, -1) + m.w1[j] * W(c, 0, 1, -1));
+  r = r - qdiv(t3 - t4, m.zF[k], m.zrF[k]);
+  if (!LES) {
+    T vx = qdiv(m.xrC[i] * (ve - vc) - m.xrC[i - 1] * (vc - vw), m.xF[i], m.xrF[i]);
+    T vy = qdiv(m.yrF[j + 1] * (vn - vc) - m.yrF[j] * (vc - vs), m.yC[j], m.yrC[j]);
+    T vz = qdiv(m.zrC[k] * (vt - vc) - m.zrC[k - 1] * (vc - vb), m.zF[k], m.zrF[k]);
+    r = r + m.nu * (vx + vy + vz);
+  } else {
+    T n0 = N(c, 0, 0, 0), nN = N(c, 0, 1, 0);
+    T nu_x1 = m.nu + h * (m.w0[j] * N(c, -1, 0, 0) + m.w1[j] * N(c, -1, 1, 0) + m.w0[j] * n0 + m.w1[j] * nN);
+    T nu_x2 = m.nu + h * (m.w0[j] * n0 + m.w1[j] * nN + m.w0[j] * N(c, 1, 0, 0) + m.w1[j] * N(c, 1, 1, 0));
+    T nu_y1 = m.nu + n0, nu_y2 = m.nu + nN;
+    T nu_z1 = m.nu + h * (m.w0[j] * N(c, 0, 0, -1) + m.w1[j] * N(c, 0, 1, -1) + m.w0[j] * n0 + m.w1[j] * nN);
+    T nu_z2 = m.nu + h * (m.w0[j] * n0 + m.w1[j] * nN + m.w0[j] * N(c, 0, 0, 1) + m.w1[j] * N(c, 0, 1, 1));
+    r = r + m.xrF[i] * (qdiv(nu_x2, m.xC[i], m.xrC[i]) * (ve - vc) - qdiv(nu_x1, m.xC[i - 1], m.xrC[i - 1]) * (vc - vw)) +
+        m.yrC[j] * (qdiv(nu_y2, m.yF[j + 1], m.yrF[j + 1]) * (vn - vc) - qdiv(nu_y1, m.yF[j], m.yrF[j]) * (vc - vs)) +
+        m.zrF[k] * (qdiv(nu_z2, m.zC[k], m.zrC[k]) * (vt - vc) - qdiv(nu_z1, m.zC[k - 1], m.zrC[k - 1]) * (vc - vb));
+  }
+  return r;
+}
+
+// RHS of w at (i,j,k), equations.f90:328-363 (DNS) / :383-401 (LES)
+template <typename T, bool LES>
+__device__ __forceinline__ T rhs_w_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
+                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+  const T h = (T)0.5;
+  T wc = W(c, 0, 0, 0), we = W(c, 1, 0, 0), ww = W(c, -1, 0, 0);
+  T wn = W(c, 0, 1, 0), ws = W(c, 0, -1, 0), wt = W(c, 0, 0, 1), wb = W(c, 0, 0, -1);
+  T a = h * (wc + wt), b = h * (wb + wc);
+  T r = -qdiv(a * a - b * b, m.zC[k], m.zrC[k]);
+  T t1 = h * (U(c, 0, 0, 0) + U(c, 0, 0, 1)) * h * (wc + we);
+  T t2 = h * (U(c, -1, 0, 0) + U(c, -1, 0, 1)) * h * (ww + wc);
+  r = r - qdiv(t1 - t2, m.xF[i], m.xrF[i]);
+  T t3 = h * (V(c, 0, 0, 0) + V(c, 0, 0, 1)) * (m.w0[j] * wc + m.w1[j] * wn);
+  T t4 = h * (V(c, 0, -1, 0) + V(c, 0, -1, 1)) * (m.w0[j - 1] * ws + m.w1[j - 1] * wc);
+  r = r - qdiv(t3 - t4, m.yF[j], m.yrF[j]);
+  if (!LES) {
+    T vx = qdiv(m.xrC[i] * (we - wc) - m.xrC[i - 1] * (wc - ww), m.xF[i], m.xrF[i]);
+    T vy = qdiv(qdiv(wn - wc, m.yC[j], m.yrC[j]) - qdiv(wc - ws, m.yC[j - 1], m.yrC[j - 1]), m.yF[j], m.yrF[j]);
+    T vz = qdiv(m.zrF[k + 1] * (wt - wc) - m.zrF[k] * (wc - wb), m.zC[k], m.zrC[k]);
+    r = r + m.dpdz + m.nu * (vx + vy + vz);
+  } else {
+    const T q = (T)0.25;
+    T n0 = N(c, 0, 0, 0), nT = N(c, 0, 0, 1);
+    T nu_x1 = m.nu + q * (n0 + nT + N(c, -1, 0, 0) + N(c, -1, 0, 1));
+    T nu_x2 = m.nu + q * (n0 + nT + N(c, 1, 0, 0) + N(c, 1, 0, 1));
+    T nu_y1 = m.nu + h * (m.w0[j - 1] * N(c, 0, -1, 0) + m.w1[j - 1] * n0 + m.w0[j - 1] * N(c, 0, -1, 1) + m.w1[j - 1] * nT);
+    T nu_y2 = m.nu + h * (m.w0[j] * n0 + m.w1[j] * N(c, 0, 1, 0) + m.w0[j] * nT + m.w1[j] * N(c, 0, 1, 1));
+    T nu_z1 = m.nu + n0, nu_z2 = m.nu + nT;
+    T t2p = qdiv(wn - wc, m.yC[j], m.yrC[j]);
+    T t2m = qdiv(wc - ws, m.yC[j - 1], m.yrC[j - 1]);
+    r = r + m.dpdz +
+        qdiv(qdiv(nu_x2, m.xC[i], m.xrC[i]) * (we - wc) - qdiv(nu_x1, m.xC[i - 1], m.xrC[i - 1]) * (wc - ww), m.xF[i], m.xrF[i]) +
+        qdiv(nu_y2 * t2p - nu_y1 * t2m, m.yF[j], m.yrF[j]) +
+        qdiv(qdiv(nu_z2, m.zF[k + 1], m.zrF[k + 1]) * (wt - wc) - qdiv(nu_z1, m.zF[k], m.zrF[k]) * (wc - wb), m.zC[k], m.zrC[k]);
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// RHS + RK update.  MODE 0: store the RHS only (compute_rhs_u/v/w).
+// MODE 1: U = Uo + (dt*c1)*F, F stored as F1 (first substep; Euler).
+// MODE 2: U = Uo + dt*(c1*F1 + c2*F)        (RK3 s2, RK2 s2).
+// MODE 3: U = Uo + dt*(c1*F1 + c2*F)        (RK3 s3, where rk_coef(3,2)=0 so
+//         the F2 term contributes exactly zero and F2 is never stored).
+// Threads cover the union of the three interior ranges, i=2..nx, j=2..ny,
+// k=2..nz, each thread marching through a chunk of k-planes.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE, bool LES>
+__global__ void __launch_bounds__(256) k_rhs_rk(Geo g, MetT<T> m, const T *__restrict__ U, const T *__restrict__ V,
+                                                const T *__restrict__ W, const T *__restrict__ nut,
+                                                const T *__restrict__ Uo, const T *__restrict__ Vo,
+                                                const T *__restrict__ Wo, T *__restrict__ F1u, T *__restrict__ F1v,
+                                                T *__restrict__ F1w, T *__restrict__ Un, T *__restrict__ Vn,
+                                                T *__restrict__ Wn, const Scalars *__restrict__ sc, double c1,
+                                                double c2, int kchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (i > g.nx || j > g.ny) return;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  const Ld<T> LU{U, 1, g.px, g.plane}, LV{V, 1, g.px, g.plane}, LW{W, 1, g.px, g.plane}, LN{nut, 1, g.px, g.plane};
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  // coefficient products in FP64, exactly as the source multiplies them
+  const T cdt1 = (T)(dt * c1);
+  const T tdt = (T)dt, tc1 = (T)c1, tc2 = (T)c2;
+  const bool du = (i <= g.nx - 1), dv = (j <= g.ny - 1);
+  for (int k = k0; k <= k1; ++k) {
+    const long long c = bidx(g, i, j, k);
+    if (du) {
+      T f = (i == g.nx - 1) ? (T)0 : rhs_u_at<T, LES>(g, m, LU, LV, LW, LN, c, i, j, k);
+      if (MODE == 0) F1u[c] = f;
+      else if (MODE == 1) { F1u[c] = f; Un[c] = Uo[c] + cdt1 * f; }
+      else Un[c] = Uo[c] + tdt * (tc1 * F1u[c] + tc2 * f);
+    }
+    if (dv) {
+      T f = (i == g.nx) ? (T)0 : rhs_v_at<T, LES>(g, m, LU, LV, LW, LN, c, i, j, k);
+      if (MODE == 0) F1v[c] = f;
+      else if (MODE == 1) { F1v[c] = f; Vn[c] = Vo[c] + cdt1 * f; }
+      else Vn[c] = Vo[c] + tdt * (tc1 * F1v[c] + tc2 * f);
+    }
+    if (k <= g.nz - 1) {
+      T f = (i == g.nx) ? (T)0 : rhs_w_at<T, LES>(g, m, LU, LV, LW, LN, c, i, j, k);
+      if (MODE == 0) F1w[c] = f;
+      else if (MODE == 1) { F1w[c] = f; Wn[c] = Wo[c] + cdt1 * f; }
+      else Wn[c] = Wo[c] + tdt * (tc1 * F1w[c] + tc2 * f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// project_velocity (projection.f90:359-384) + pressure save at rk_step 1
+// (projection.f90:75-78, P(2:nxg-1,2:nyg-1,2:nzg-1) = rhs_p/(dt*rk2_coef(1,1))).
+// p holds rhs_p in the box layout (i=2..nx, j=2..ny, k=2..nz valid).
+// dc (mixed form only): per-row constant of the zero wavenumber, kept in FP64.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_project(Geo g, MetT<T> m, const T *__restrict__ p, const double *__restrict__ dc,
+                                                 T *__restrict__ U, T *__restrict__ V, T *__restrict__ W,
+                                                 T *__restrict__ P, const Scalars *__restrict__ sc, int save_p,
+                                                 int kchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (i > g.nx || j > g.ny) return;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  const double den = save_p ? sc->dt * 0.5 : 1.0;  // dt*rk2_coef(1,1)
+  for (int k = k0; k <= k1; ++k) {
+    const long long c = bidx(g, i, j, k);
+    const T pc = __ldg(p + c);
+    if (i <= g.nx - 1) U[c] = U[c] - qdiv(__ldg(p + c + 1) - pc, m.xC[i], m.xrC[i]);
+    if (j <= g.ny - 1) {
+      T d = __ldg(p + c + g.px) - pc;
+      if (dc) d = (T)((double)d + (dc[j + 1 - 2] - dc[j - 2]));
+      V[c] = V[c] - qdiv(d, m.yC[j], m.yrC[j]);
+    }
+    if (k <= g.nz - 1) W[c] = W[c] - qdiv(__ldg(p + c + g.plane) - pc, m.zC[k], m.zrC[k]);
+    if (save_p) {
+      double pv = (double)pc;
+      if (dc) pv += dc[j - 2];
+      P[c] = (T)(pv / den);
+    }
+  }
+}
+
+// P ghost planes, projection.f90:78-83 (three ordered phases)
+template <typename T>
+__global__ void k_p_ghost(Geo g, T *__restrict__ P, int phase) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (phase == 0) {  // P(1,:,:)=P(2,:,:); P(nxg,:,:)=P(nxg-1,:,:) over (j,k)
+    if (a > g.nyg || b > g.nzg) return;
+    P[bidx(g, 1, a, b)] = P[bidx(g, 2, a, b)];
+    P[bidx(g, g.nxg, a, b)] = P[bidx(g, g.nxg - 1, a, b)];
+  } else if (phase == 1) {  // over (i,k)
+    if (a > g.nxg || b > g.nzg) return;
+    P[bidx(g, a, 1, b)] = P[bidx(g, a, 2, b)];
+    P[bidx(g, a, g.nyg, b)] = P[bidx(g, a, g.nyg - 1, b)];
+  } else {  // over (i,j)
+    if (a > g.nxg || b > g.nyg) return;
+    P[bidx(g, a, b, 1)] = P[bidx(g, a, b, 2)];
+    P[bidx(g, a, b, g.nzg)] = P[bidx(g, a, b, g.nzg - 1)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions, boundary_conditions.f90:127-262, in four ordered
+// launches: (1) inflow + convective outflow planes (+ the x mass-flux
+// partial sums), (2) z periodicity, (3) top and wall, (4) mass correction.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mode_sum(const double2 *__restrict__ q, int ld, int j, int nm, int mm,
+                                           const double *__restrict__ zmode, const double *__restrict__ tmode,
+                                           double zz, double t) {
+  // sum_n sum_m Re(q(j,n,m) exp(i(zmode_n z - tmode_m t)))  (:143-150)
+  double acc = 0.0;
+  for (int n = 0; n < nm; ++n)
+    for (int mi = 0; mi < mm; ++mi) {
+      double2 qq = q[((long long)mi * nm + n) * ld + (j - 1)];
+      double th = zmode[n] * zz - tmode[mi] * t;
+      double s, co;
+      sincos(th, &s, &co);
+      acc = acc + (qq.x * co - qq.y * s);
+    }
+  return acc;
+}
+
+template <typename T>
+__global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W,
+                       const T *__restrict__ Uo, const T *__restrict__ Vo, const T *__restrict__ Wo,
+                       const Scalars *__restrict__ sc, double rkt, double *__restrict__ qx_part) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;  // 1..nyg
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;  // 1..nzg
+  double q = 0.0;
+  if (j <= g.nyg && k <= g.nzg) {
+    const double t = sc->t, dt = sc->dt;
+    const int nx = g.nx, nxg = g.nxg;
+    // inflow (:182-190), with the temporal modes of :137-180
+    double ut = 0.0, vt = 0.0, wt = 0.0;
+    if (bc.n_modes > 0) {
+      ut = mode_sum(bc.qu, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+      if (j <= g.ny) vt = mode_sum(bc.qv, g.ny, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+      if (k <= g.nz) wt = mode_sum(bc.qw, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.z[k], t);
+    } else if (bc.ut) {
+      ut = bc.ut[(long long)(k - 1) * g.nyg + (j - 1)];
+      if (j <= g.ny) vt = bc.vt[(long long)(k - 1) * g.ny + (j - 1)];
+      if (k <= g.nz) wt = bc.wt[(long long)(k - 1) * g.nyg + (j - 1)];
+    }
+    const T u1 = (T)(bc.U_inlet[j] + ut);
+    U[bidx(g, 1, j, k)] = u1;
+    if (k <= g.nz) W[bidx(g, 1, j, k)] = (T)(bc.W_inlet[j] + wt);
+    if (j <= g.ny) V[bidx(g, 1, j, k)] = (T)(bc.V_inlet[j] + vt);
+    // outflow (:193-201): rk_t(rk_step)*dt*Uc*(Uo(nx-1)-Uo(nx-2))/(x(nx-1)-x(nx-2))
+    const double cc = rkt * dt * bc.U_top[nx];
+    {
+      long long a = bidx(g, nx - 1, j, k);
+      T uo1 = Uo[a], uo2 = Uo[a - 1];
+      const T un = (T)((double)uo1 - cc * (double)(uo1 - uo2) / g.ax.F[nx - 1]);
+      U[a] = un;
+      U[a + 1] = un;
+      if (j >= 2 && j <= g.nyg - 1 && k >= 2 && k <= g.nzg - 2)
+        q = ((double)u1 - (double)un) * g.ay.F[j];
+    }
+    if (j <= g.ny) {
+      long long a = bidx(g, nxg - 1, j, k);
+      T vo1 = Vo[a], vo2 = Vo[a - 1];
+      const T vn = (T)((double)vo1 - cc * (double)(vo1 - vo2) / g.ax.C[nxg - 2]);
+      V[a] = vn;
+      V[a + 1] = vn;
+    }
+    if (k <= g.nz) {
+      long long a = bidx(g, nxg - 1, j, k);
+      T wo1 = Wo[a], wo2 = Wo[a - 1];
+      const T wn = (T)((double)wo1 - cc * (double)(wo1 - wo2) / g.ax.C[nxg - 2]);
+      W[a] = wn;
+      W[a + 1] = wn;
+    }
+  }
+  // deterministic block reduction of the x mass-flux partials (:242-246)
+  __shared__ double red[256];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  red[tid] = q;
+  __syncthreads();
+  for (int s = (blockDim.x * blockDim.y) / 2; s > 0; s >>= 1) {
+    if (tid < s) red[tid] += red[tid + s];
+    __syncthreads();
+  }
+  if (tid == 0) qx_part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
+template <typename T>
+__global__ void k_bc_z(Geo g, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W) {
+  // :204-216
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (i > g.nxg || j > g.nyg) return;
+  const long long P = g.plane;
+  const long long c1 = bidx(g, i, j, 1);
+  const int nzg = g.nzg, nz = g.nz;
+  if (i <= g.nx) {
+    U[c1] = U[c1 + (nzg - 3) * P];
+    U[c1 + (nzg - 2) * P] = U[c1 + 1 * P];
+    U[c1 + (nzg - 1) * P] = U[c1 + 2 * P];
+  }
+  if (j <= g.ny) {
+    V[c1] = V[c1 + (nzg - 3) * P];
+    V[c1 + (nzg - 2) * P] = V[c1 + 1 * P];
+    V[c1 + (nzg - 1) * P] = V[c1 + 2 * P];
+  }
+  W[c1] = W[c1 + (nz - 2) * P];
+  W[c1 + (nz - 1) * P] = W[c1 + 1 * P];
+}
+
+template <typename T>
+__global__ void k_bc_y(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W) {
+  // top (:219-227) then wall (:230-237)
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (i > g.nxg || k > g.nzg) return;
+  if (i <= g.nx) U[bidx(g, i, g.nyg, k)] = (T)bc.U_top[i];
+  V[bidx(g, i, g.ny, k)] = (T)bc.V_top[i];
+  if (k <= g.nz) W[bidx(g, i, g.nyg, k)] = (T)bc.W_top[i];
+  if (i <= g.nx) U[bidx(g, i, 1, k)] = -U[bidx(g, i, 2, k)];
+  V[bidx(g, i, 1, k)] = (T)0;
+  if (k <= g.nz) W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
+}
+
+template <typename T>
+__global__ void k_bc_mass(Geo g, T *__restrict__ U, const double *__restrict__ qx_part, int nparts, double qy,
+                          double length_y, Scalars *__restrict__ sc) {
+  // :240-260.  Every block sums the partials in the same fixed order.
+  __shared__ double s_du;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    double qx = 0.0;
+    for (int p = 0; p < nparts; ++p) qx += qx_part[p];
+    double du = (qx + qy) / length_y / (double)(g.nzg - 3);
+    s_du = du;
+    if (blockIdx.x == 0 && blockIdx.y == 0) sc->dU = du;
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (j > g.nyg || k > g.nzg) return;
+  long long a = bidx(g, g.nx - 1, j, k);
+  const T v = (T)((double)U[a] + s_du);
+  U[a] = v;
+  U[a + 1] = v;
+}
+
+// ---------------------------------------------------------------------------
+// compute_dt: max over i=2..nxg-1, j=2..nyg-1, k=2..nzg-1 of spacing/|vel|
+// (time_integration.f90:546-556).  All ratios are >= 0 (or +Inf), so the
+// maximum of their IEEE bit patterns is their maximum and atomicMax is exact
+// and order independent.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ U, const T *__restrict__ V,
+                                                   const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  double mu = 0.0, mv = 0.0, mw = 0.0;
+  if (i <= g.nxg - 1 && j <= g.nyg - 1) {
+    const int k0 = blockIdx.z * kchunk + 2;
+    const int k1 = min(k0 + kchunk - 1, g.nzg - 1);
+    const double cu = g.ax.C[i], cv = g.ay.C[j];
+    for (int k = k0; k <= k1; ++k) {
+      long long c = bidx(g, i, j, k);
+      mu = fmax(mu, cu / fabs((double)__ldg(U + c)));
+      mv = fmax(mv, cv / fabs((double)__ldg(V + c)));
+      mw = fmax(mw, g.az.C[k] / fabs((double)__ldg(W + c)));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
+    atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
+    atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
+  }
+}
+
+// time_integration.f90:560-575 (dt = min(dt_conv, dt_vis)); also arms the
+// accumulators for the next call and records to = t for the RK substeps.
+__global__ void k_dt_finish(Scalars *sc, double cfl, double dtvis) {
+  double cfla = fabs(cfl);
+  double lu = __longlong_as_double((long long)sc->lmax[0]);
+  double lv = __longlong_as_double((long long)sc->lmax[1]);
+  double lw = __longlong_as_double((long long)sc->lmax[2]);
+  double dt_conv = fmin(fmin(cfla * lu, cfla * lv), cfla * lw);
+  sc->dt = fmin(dt_conv, dtvis);
+  sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
+}
+
+__global__ void k_set_time(Scalars *sc, int phase, double coef) {
+  // phase 0: to = t (save at step start); phase 1: t = to + coef*dt
+  if (phase == 0) sc->to = sc->t;
+  else sc->t = sc->to + coef * sc->dt;
+}
+
+// check_divergence (projection.f90:399-408): max |div| over i=2..nxg-2
+template <typename T>
+__global__ void __launch_bounds__(256) k_maxdiv(Geo g, const T *__restrict__ U, const T *__restrict__ V,
+                                                const T *__restrict__ W, unsigned long long *__restrict__ out,
+                                                int kchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  double mx = 0.0;
+  if (i <= g.nxg - 2 && j <= g.nyg - 1) {
+    const int k0 = blockIdx.z * kchunk + 2;
+    const int k1 = min(k0 + kchunk - 1, g.nzg - 1);
+    for (int k = k0; k <= k1; ++k) {
+      long long c = bidx(g, i, j, k);
+      double d = ((double)U[c] - (double)U[c - 1]) / g.ax.F[i] + ((double)V[c] - (double)V[c - g.px]) / g.ay.F[j] +
+                 ((double)W[c] - (double)W[c - g.plane]) / g.az.F[k];
+      mx = fmax(mx, fabs(d));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline dim3 vol_grid(int ni, int nj, int nk, int kchunk) {
+  return dim3((ni + 31) / 32, (nj + 7) / 8, (nk + kchunk - 1) / kchunk);
+}
+
+template <typename T>
+void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *U, const T *V, const T *W,
+                   const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
+                   const Scalars *sc, double c1, double c2, cudaStream_t st) {
+  const int kchunk = 8;
+  dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk), block(32, 8);
+#define BLGPU_RHS_CASE(M, L)                                                                             \
+  k_rhs_rk<T, M, L><<<grid, block, 0, st>>>(g, m, U, V, W, nut, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, \
+                                            c2, kchunk)
+  if (!les) {
+    switch (mode) {
+      case 0: BLGPU_RHS_CASE(0, false); break;
+      case 1: BLGPU_RHS_CASE(1, false); break;
+      case 2: BLGPU_RHS_CASE(2, false); break;
+      default: BLGPU_RHS_CASE(3, false); break;
+    }
+  } else {
+    switch (mode) {
+      case 0: BLGPU_RHS_CASE(0, true); break;
+      case 1: BLGPU_RHS_CASE(1, true); break;
+      case 2: BLGPU_RHS_CASE(2, true); break;
+      default: BLGPU_RHS_CASE(3, true); break;
+    }
+  }
+#undef BLGPU_RHS_CASE
+}
+
+template <typename T>
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
+                    const Scalars *sc, int save_p, cudaStream_t st) {
+  const int kchunk = 8;
+  dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk), block(32, 8);
+  k_project<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p, kchunk);
+  if (save_p) {
+    dim3 b2(32, 8);
+    k_p_ghost<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 0);
+    k_p_ghost<T><<<dim3((g.nxg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 1);
+    k_p_ghost<T><<<dim3((g.nxg + 31) / 32, (g.nyg + 7) / 8), b2, 0, st>>>(g, P, 2);
+  }
+}
+
+int bc_x_parts(const Geo &g) { return ((g.nyg + 31) / 32) * ((g.nzg + 7) / 8); }
+
+template <typename T>
+void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
+               Scalars *sc, double rkt, double *qx_part, double qy, double length_y, cudaStream_t st) {
+  dim3 b(32, 8);
+  dim3 gx((g.nyg + 31) / 32, (g.nzg + 7) / 8);
+  k_bc_x<T><<<gx, b, 0, st>>>(g, bc, U, V, W, Uo, Vo, Wo, sc, rkt, qx_part);
+  k_bc_z<T><<<dim3((g.nxg + 31) / 32, (g.nyg + 7) / 8), b, 0, st>>>(g, U, V, W);
+  k_bc_y<T><<<dim3((g.nxg + 31) / 32, (g.nzg + 7) / 8), b, 0, st>>>(g, bc, U, V, W);
+  k_bc_mass<T><<<gx, b, 0, st>>>(g, U, qx_part, (int)(gx.x * gx.y), qy, length_y, sc);
+}
+
+template <typename T>
+void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
+               cudaStream_t st) {
+  const int kchunk = 16;
+  dim3 grid = vol_grid(g.nxg - 2, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
+  k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk);
+  k_dt_finish<<<1, 1, 0, st>>>(sc, cfl, dtvis);
+}
+
+void launch_set_time(Scalars *sc, int phase, double coef, cudaStream_t st) {
+  k_set_time<<<1, 1, 0, st>>>(sc, phase, coef);
+}
+
+template <typename T>
+void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st) {
+  const int kchunk = 16;
+  dim3 grid = vol_grid(g.nxg - 3, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
+  k_maxdiv<T><<<grid, block, 0, st>>>(g, U, V, W, out, kchunk);
+}
+
+#define BLGPU_INST(T)                                                                                                \
+  template void launch_rhs_rk<T>(const Geo &, const MetT<T> &, int, bool, const T *, const T *, const T *,          \
+                                 const T *, const T *, const T *, const T *, T *, T *, T *, T *, T *, T *,          \
+                                 const Scalars *, double, double, cudaStream_t);                                    \
+  template void launch_project<T>(const Geo &, const MetT<T> &, const T *, const double *, T *, T *, T *, T *,     \
+                                  const Scalars *, int, cudaStream_t);                                              \
+  template void launch_bc<T>(const Geo &, const BcData &, T *, T *, T *, const T *, const T *, const T *,         \
+                             Scalars *, double, double *, double, double, cudaStream_t);                            \
+  template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, cudaStream_t); \
+  template void launch_maxdiv<T>(const Geo &, const T *, const T *, const T *, unsigned long long *, cudaStream_t);
+BLGPU_INST(double)
+BLGPU_INST(float)
+
+}  // namespace blgpu

@@ -1,0 +1,134 @@
+/*
+ * blgpu.h -- C ABI of the B200 step path of the boundary-layer DNS solver.
+ *
+ * Drop-in for the per-step hot path of ms-alvaro/boundary-layer-gpu: the
+ * staggered second-order RHS (equations.f90), the Euler/RK2/RK3 substeps
+ * (time_integration.f90), the boundary-condition pass of the GPU build
+ * (boundary_conditions.f90:127-262) and the fractional-step projection
+ * (projection.f90).  Plain C types only, so a Fortran host binds it with
+ * ISO_C_BINDING and Python with ctypes.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success and a negative BLGPU_E* code on
+ *    failure; blgpu_last_error() then returns a message.  Nothing aborts.
+ *  - Host arrays use the reference's Fortran layout and bounds (column-major,
+ *    i fastest):  U(nx,nyg,nzg)  V(nxg,ny,nzg)  W(nxg,nyg,nz)  P(nxg,nyg,nzg)
+ *    with nxg = nx+1, nyg = ny+1, nzg = nz+1 (global.f90:86-88 at nprocs=1).
+ *  - The context owns all device memory, allocated in blgpu_create; state
+ *    crosses the host boundary only in blgpu_upload_state/download_state,
+ *    i.e. where the reference has its !$acc data copy / update self
+ *    (main.f90:61-81,99-101).
+ *  - One context = one box on one GPU, work in issue order on one stream.
+ */
+#ifndef BLGPU_H
+#define BLGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLGPU_OK 0
+#define BLGPU_EINVAL (-1)   /* bad argument or size */
+#define BLGPU_ECUDA (-2)    /* CUDA runtime error */
+#define BLGPU_ESTATE (-3)   /* call out of order (e.g. no grid yet) */
+#define BLGPU_EDEVICE (-4)  /* device-side check failed (NaN, wait limit) */
+
+#define BLGPU_FP64 0   /* bit-faithful FP64 form */
+#define BLGPU_MIXED 1  /* FP32 fields/RHS/transforms, FP64 Thomas and mean mode */
+
+#define BLGPU_POISSON_NATIVE 0  /* hand-written DCT/DFT/Thomas kernels */
+#define BLGPU_POISSON_CUFFT 1   /* cuFFT comparison path (FP64 only) */
+
+typedef struct blgpu_ctx blgpu_ctx;
+
+/* Run parameters: the .turbb keys of the path (params.f90:119-207). */
+typedef struct blgpu_config {
+  int nx, ny, nz;     /* nxyz: face points (params.f90:131) */
+  double nu;          /* nu (params.f90:119) */
+  double cfl;         /* CFL; < 0 means fixed dt = -CFL (time_integration.f90:539) */
+  double dpdx, dpdz;  /* dPdx, dPdz (params.f90:152-153) */
+  int rk_scheme;      /* RKscheme: 1 Euler, 2 RK2, 3 RK3 (params.f90:195) */
+  int les_model;      /* LES: 0 DNS, 1 eddy viscosity from blgpu_set_nu_t */
+  int precision;      /* BLGPU_FP64 | BLGPU_MIXED */
+  int poisson;        /* BLGPU_POISSON_NATIVE | BLGPU_POISSON_CUFFT */
+  int device;         /* CUDA device ordinal */
+} blgpu_config;
+
+/* initialize/allocation part of initialization.f90:25-759 and
+ * cufft_init_plans (cufft_solver.f90:26) */
+int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out);
+/* finalize (finalization.f90:6-38) */
+int blgpu_destroy(blgpu_ctx *ctx);
+/* message of the last failure (global one when ctx is NULL) */
+const char *blgpu_last_error(const blgpu_ctx *ctx);
+
+/* face grids x(nx), y(ny), z(nz); centres, ghosts, modified wavenumbers,
+ * Dyy and interpolation weights are derived as in initialization.f90:174-222,
+ * 329-344, 395-425, 482-484 */
+int blgpu_set_grid(blgpu_ctx *ctx, const double *x, const double *y, const double *z);
+
+/* inflow/top vectors of compute_blasius_solution_for_bc /
+ * compute_turbulent_solution_for_bc (boundary_conditions.f90:1371-1797):
+ * U_inlet(nyg) V_inlet(ny) W_inlet(nyg) U_top(nx) V_top(nxg) W_top(nxg) */
+int blgpu_set_boundary(blgpu_ctx *ctx, const double *U_inlet, const double *V_inlet, const double *W_inlet,
+                       const double *U_top, const double *V_top, const double *W_top);
+
+/* temporal inflow modes (boundary_conditions.f90:1720-1797): zmode(n) and
+ * tmode(m) already scaled by beta/omega; qu(nyg,n,m), qv(ny,n,m),
+ * qw(nyg,n,m) as interleaved (re,im) doubles */
+int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const double *zmode, const double *tmode,
+                           const double *qu, const double *qv, const double *qw);
+
+/* eddy viscosity nu_t(nxg,nyg,nzg) for LES=1 (subgrid.f90:23, host model) */
+int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t);
+
+/* state in/out (main.f90:61-81 copy-in; main.f90:99-101 update self).
+ * Upload also sets Uo = U as read_input_data does (input_output.f90:476-478). */
+int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
+int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double *P, double *t);
+
+/* compute_dt (time_integration.f90:528-591): device reduction, no host copy
+ * of the fields; the resulting dt is returned and kept on the device */
+int blgpu_compute_dt(blgpu_ctx *ctx, double *dt);
+int blgpu_set_dt(blgpu_ctx *ctx, double dt);
+int blgpu_get_time(blgpu_ctx *ctx, double *t, double *dt);
+
+/* one step of the main loop body (main.f90:87-96): compute_dt, then
+ * compute_time_step_{Euler,RK2,RK3}; repeated nsteps times, replayed from a
+ * captured CUDA graph */
+int blgpu_advance(blgpu_ctx *ctx, int nsteps);
+
+/* compute_time_step_RK3 / _RK2 / _Euler (time_integration.f90:305,145,24):
+ * one step with the current dt, no compute_dt */
+int blgpu_time_step(blgpu_ctx *ctx);
+
+/* compute_rhs_u/v/w (equations.f90:24,163,301) on host arrays; outputs are
+ * the reference's compact interior arrays rhs_u(2:nx-1,2:nyg-1,2:nzg-1),
+ * rhs_v(2:nxg-1,2:ny-1,2:nzg-1), rhs_w(2:nxg-1,2:nyg-1,2:nz-1) */
+int blgpu_compute_rhs(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double *rhs_u,
+                      double *rhs_v, double *rhs_w);
+
+/* apply_boundary_conditions_gpu (boundary_conditions.f90:127) on the
+ * resident state, with the outflow factor rk_t(rk_step) */
+int blgpu_apply_bc(blgpu_ctx *ctx, int rk_step);
+
+/* compute_projection_step (projection.f90:21) on the resident state;
+ * rk_step == 1 also stores P (projection.f90:75-85) */
+int blgpu_projection(blgpu_ctx *ctx, int rk_step);
+
+/* rhs_p(2:nxg-1,2:nyg-1,2:nzg) of the last projection (projection.f90 array) */
+int blgpu_get_rhs_p(blgpu_ctx *ctx, double *rhs_p);
+
+/* check_divergence (projection.f90:391-413) */
+int blgpu_max_divergence(blgpu_ctx *ctx, double *max_div);
+
+/* wait for all queued work */
+int blgpu_sync(blgpu_ctx *ctx);
+
+/* device bytes held by the context */
+long long blgpu_device_bytes(const blgpu_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1208 @@
+/*
+ * bl_oracle.c -- CPU restatement of the boundary-layer DNS step path.
+ *
+ * TEST INFRASTRUCTURE ONLY (parity oracle, CPU baseline).  Never linked into
+ * or called by the product library.  Each routine cites the reference
+ * Fortran it restates (paths relative to the ms-alvaro/boundary-layer-gpu
+ * source tree).  Compile with -O2 -ffp-contract=off so that every FP64
+ * expression is evaluated in the order the Fortran source writes it, without
+ * fused multiply-adds (the reference CPU build, gfortran -O2 on x86-64, has
+ * none either).
+ *
+ * Third-party arithmetic that the reference takes from libraries is restated
+ * here from the published algorithms:
+ *   - FFTW 3 complex DFT (projection.f90:233,277): a recursive mixed-radix
+ *     Cooley-Tukey transform, with Bluestein's chirp-z algorithm for lengths
+ *     with a prime factor above 64;
+ *   - LAPACK ZGTSV (projection.f90:253): Gaussian elimination with partial
+ *     pivoting for a tridiagonal system, as in the LAPACK reference routine.
+ */
+#include "bl_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef double complex cplx;
+
+/* ------------------------------------------------------------------------ */
+/* FFT: recursive decimation in time, arbitrary length                      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct fft_plan {
+  int n;
+  int nfac;
+  int fac[64]; /* pairs (p, m) like the recursion consumes them */
+  cplx *tw;    /* tw[j] = exp(-2 pi i j / n) */
+  /* Bluestein */
+  int blue;
+  int m;
+  cplx *chirp;  /* exp(-i pi j^2 / n), j = 0..n-1 */
+  cplx *bfft;   /* FFT_m of the conjugate chirp, wrapped */
+  struct fft_plan *sub;
+} fft_plan;
+
+static int largest_prime_factor(int n) {
+  int lp = 1;
+  for (int p = 2; p * p <= n; ++p)
+    while (n % p == 0) { lp = p; n /= p; }
+  if (n > 1) lp = n > lp ? n : lp;
+  return lp;
+}
+
+static fft_plan *fft_plan_create(int n);
+static void fft_exec(const fft_plan *pl, cplx *data, cplx *work);
+static size_t fft_work_size(const fft_plan *pl);
+
+static void fft_plan_free(fft_plan *p) {
+  if (!p) return;
+  free(p->tw);
+  free(p->chirp);
+  free(p->bfft);
+  fft_plan_free(p->sub);
+  free(p);
+}
+
+static fft_plan *fft_plan_create(int n) {
+  fft_plan *p = (fft_plan *)calloc(1, sizeof(fft_plan));
+  p->n = n;
+  p->tw = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+  for (int j = 0; j < n; ++j) {
+    double a = -2.0 * M_PI * (double)j / (double)n;
+    p->tw[j] = cos(a) + I * sin(a);
+  }
+  if (n > 64 && largest_prime_factor(n) > 64) {
+    /* Bluestein: X_k = c_k * sum_j (x_j c_j) conj(c_{k-j}), c_j = e^{-i pi j^2/n} */
+    p->blue = 1;
+    int m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    p->m = m;
+    p->chirp = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+    for (int j = 0; j < n; ++j) {
+      long long jj = ((long long)j * j) % (2LL * n);
+      double a = -M_PI * (double)jj / (double)n;
+      p->chirp[j] = cos(a) + I * sin(a);
+    }
+    p->sub = fft_plan_create(m);
+    p->bfft = (cplx *)calloc((size_t)m, sizeof(cplx));
+    p->bfft[0] = conj(p->chirp[0]);
+    for (int j = 1; j < n; ++j) {
+      p->bfft[j] = conj(p->chirp[j]);
+      p->bfft[m - j] = conj(p->chirp[j]);
+    }
+    {
+      cplx *w = (cplx *)malloc(sizeof(cplx) * fft_work_size(p->sub));
+      fft_exec(p->sub, p->bfft, w);
+      free(w);
+    }
+    return p;
+  }
+  /* factorisation: 4s first, then 2, 3, 5, ... */
+  int rem = n, k = 0;
+  while (rem > 1) {
+    int f;
+    if (rem % 4 == 0) f = 4;
+    else if (rem % 2 == 0) f = 2;
+    else {
+      f = 3;
+      while (rem % f) f += 2;
+    }
+    rem /= f;
+    p->fac[k++] = f;
+    p->fac[k++] = rem;
+  }
+  p->nfac = k / 2;
+  return p;
+}
+
+/* one level of the recursion: out[0..p*m) from in with stride */
+static void fft_work(const fft_plan *pl, cplx *out, const cplx *in,
+                     size_t fstride, size_t istride, const int *fac,
+                     cplx *scratch) {
+  const int p = fac[0], m = fac[1];
+  if (m == 1) {
+    for (int q = 0; q < p; ++q) out[q] = in[(size_t)q * fstride * istride];
+  } else {
+    for (int q = 0; q < p; ++q)
+      fft_work(pl, out + (size_t)q * m, in + (size_t)q * fstride * istride,
+               fstride * (size_t)p, istride, fac + 2, scratch);
+  }
+  const int n = pl->n;
+  const cplx *tw = pl->tw;
+  if (p == 2) {
+    for (int u = 0; u < m; ++u) {
+      cplx t = out[u + m] * tw[(size_t)u * fstride];
+      out[u + m] = out[u] - t;
+      out[u] = out[u] + t;
+    }
+    return;
+  }
+  if (p == 4) {
+    for (int u = 0; u < m; ++u) {
+      cplx a0 = out[u];
+      cplx a1 = out[u + m] * tw[(size_t)u * fstride];
+      cplx a2 = out[u + 2 * m] * tw[(size_t)2 * u * fstride];
+      cplx a3 = out[u + 3 * m] * tw[(size_t)3 * u * fstride];
+      cplx s0 = a0 + a2, s1 = a0 - a2, s2 = a1 + a3, s3 = a1 - a3;
+      cplx s3j = cimag(s3) - I * creal(s3); /* -i * s3 */
+      out[u] = s0 + s2;
+      out[u + 2 * m] = s0 - s2;
+      out[u + m] = s1 + s3j;
+      out[u + 3 * m] = s1 - s3j;
+    }
+    return;
+  }
+  /* generic odd radix */
+  for (int u = 0; u < m; ++u) {
+    for (int q = 0; q < p; ++q) scratch[q] = out[u + q * m];
+    for (int q1 = 0; q1 < p; ++q1) {
+      size_t k = (size_t)u + (size_t)q1 * m;
+      cplx acc = scratch[0];
+      size_t idx = 0, step = fstride * k % (size_t)n;
+      for (int q = 1; q < p; ++q) {
+        idx += step;
+        if (idx >= (size_t)n) idx -= (size_t)n;
+        acc += scratch[q] * tw[idx];
+      }
+      out[k] = acc;
+    }
+  }
+}
+
+/* forward (e^{-i}) unnormalised DFT, in place on data[0..n) */
+static void fft_exec(const fft_plan *pl, cplx *data, cplx *work) {
+  const int n = pl->n;
+  if (n == 1) return;
+  if (pl->blue) {
+    const int m = pl->m;
+    cplx *a = work;           /* m */
+    cplx *w2 = work + m;      /* m + sub work */
+    for (int j = 0; j < n; ++j) a[j] = data[j] * pl->chirp[j];
+    for (int j = n; j < m; ++j) a[j] = 0;
+    fft_exec(pl->sub, a, w2);
+    for (int j = 0; j < m; ++j) a[j] *= pl->bfft[j];
+    /* inverse via conjugation */
+    for (int j = 0; j < m; ++j) a[j] = conj(a[j]);
+    fft_exec(pl->sub, a, w2);
+    const double inv = 1.0 / (double)m;
+    for (int j = 0; j < n; ++j) data[j] = conj(a[j]) * inv * pl->chirp[j];
+    return;
+  }
+  cplx *out = work;
+  cplx *scratch = work + n;
+  fft_work(pl, out, data, 1, 1, pl->fac, scratch);
+  memcpy(data, out, sizeof(cplx) * (size_t)n);
+}
+
+static size_t fft_work_size(const fft_plan *pl) {
+  if (pl->blue) return (size_t)pl->m + fft_work_size(pl->sub);
+  return (size_t)pl->n + (size_t)pl->n + 8;
+}
+
+static void fft_exec_dir(const fft_plan *pl, cplx *data, cplx *work,
+                         int inverse) {
+  if (!inverse) {
+    fft_exec(pl, data, work);
+    return;
+  }
+  for (int j = 0; j < pl->n; ++j) data[j] = conj(data[j]);
+  fft_exec(pl, data, work);
+  for (int j = 0; j < pl->n; ++j) data[j] = conj(data[j]);
+}
+
+void blo_fft(int n, double *data, int inverse) {
+  fft_plan *pl = fft_plan_create(n);
+  cplx *work = (cplx *)malloc(sizeof(cplx) * fft_work_size(pl));
+  fft_exec_dir(pl, (cplx *)data, work, inverse);
+  free(work);
+  fft_plan_free(pl);
+}
+
+/* unnormalised DCT-II, c_k = sum_m f_m cos(pi k (2m+1) / 2n), via the 4n
+ * odd-slot embedding of projection.f90:221-233 (returns half of that DFT) */
+void blo_dct2(int n, const double *f, double *c) {
+  fft_plan *pl = fft_plan_create(4 * n);
+  cplx *g = (cplx *)calloc((size_t)4 * n, sizeof(cplx));
+  cplx *work = (cplx *)malloc(sizeof(cplx) * fft_work_size(pl));
+  for (int m = 0; m < n; ++m) {
+    g[2 * m + 1] = f[m];
+    g[4 * n - 1 - 2 * m] = f[m];
+  }
+  fft_exec(pl, g, work);
+  for (int k = 0; k < n; ++k) c[k] = 0.5 * creal(g[k]);
+  free(g);
+  free(work);
+  fft_plan_free(pl);
+}
+
+/* ------------------------------------------------------------------------ */
+/* ZGTSV restated: LAPACK's tridiagonal solve with partial pivoting.         */
+/* dl(n-1), d(n), du(n-1), b(n) complex; returns info like LAPACK.           */
+/* ------------------------------------------------------------------------ */
+static double cabs1(cplx z) { return fabs(creal(z)) + fabs(cimag(z)); }
+
+static int zgtsv_c(int n, cplx *dl, cplx *d, cplx *du, cplx *b) {
+  if (n <= 0) return 0;
+  for (int k = 0; k < n - 1; ++k) {
+    if (dl[k] == 0) {
+      if (d[k] == 0) return k + 1;
+    } else if (cabs1(d[k]) >= cabs1(dl[k])) {
+      cplx mult = dl[k] / d[k];
+      d[k + 1] = d[k + 1] - mult * du[k];
+      b[k + 1] = b[k + 1] - mult * b[k];
+      if (k < n - 2) dl[k] = 0;
+    } else {
+      cplx mult = d[k] / dl[k];
+      d[k] = dl[k];
+      cplx temp = d[k + 1];
+      d[k + 1] = du[k] - mult * temp;
+      if (k < n - 2) {
+        dl[k] = du[k + 1];
+        du[k + 1] = -mult * dl[k];
+      }
+      du[k] = temp;
+      temp = b[k];
+      b[k] = b[k + 1];
+      b[k + 1] = temp - mult * b[k + 1];
+    }
+  }
+  if (d[n - 1] == 0) return n;
+  b[n - 1] = b[n - 1] / d[n - 1];
+  if (n > 1) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) / d[n - 2];
+  for (int k = n - 3; k >= 0; --k)
+    b[k] = (b[k] - du[k] * b[k + 1] - dl[k] * b[k + 2]) / d[k];
+  return 0;
+}
+
+int blo_zgtsv(int n, double *dl, double *d, double *du, double *b) {
+  return zgtsv_c(n, (cplx *)dl, (cplx *)d, (cplx *)du, (cplx *)b);
+}
+
+/* ------------------------------------------------------------------------ */
+/* solver state                                                              */
+/* ------------------------------------------------------------------------ */
+
+struct blo {
+  int nx, ny, nz, nxg, nyg, nzg;
+  int nxp, nzp, nm;
+  double nu, cfl, dpdx, dpdz;
+  int rk_scheme, variant, les;
+  /* grids, 1-based (index 0 unused) */
+  double *x, *y, *z, *xm, *ym, *zm, *xg, *yg, *zg, *wy0, *wy1;
+  double dxmin, dymin, dzmin, dx, dz;
+  double *kxx, *kzz;               /* 0-based */
+  double *Dd, *Dl, *Du;            /* Dyy(j,j), Dyy(j+1,j), Dyy(j,j+1), j=2..nyg-1 stored at [j] */
+  /* fields, Fortran layout */
+  double *U, *V, *W, *P, *Uo, *Vo, *Wo;
+  double *Fu[3], *Fv[3], *Fw[3];
+  double *rhs_p;                   /* (2:nxg-1, 2:nyg-1, 2:nzg) */
+  double *nu_t;                    /* (nxg, nyg, nzg) */
+  /* boundary data */
+  double *U_inlet, *V_inlet, *W_inlet, *U_top, *V_top, *W_top;
+  double *Ut, *Vt, *Wt;            /* (nyg,nzg) (ny,nzg) (nyg,nz) */
+  int n_modes, m_modes;
+  double *zmode, *tmode;
+  cplx *qu, *qv, *qw;
+  double t, dt;
+  int rk_step;
+  /* RK tables (initialization.f90:504-530) */
+  double rk_t[4], rk_coef[3][3], rk2_t[3], rk2_coef[2][2];
+  /* projection work */
+  fft_plan *pl_x, *pl_z;           /* 4N (variant 0) or 2N (variant 1); nzp */
+  cplx *rhs_hat;                   /* (0:nxp-1, nm, 0:nzp-1) */
+  cplx *th_dl, *th_dp, *th_du;     /* variant 1 factors (nxp, nzp, nm) */
+  cplx *twid;                      /* DCT twiddle, 0..nxp-1 */
+};
+
+static int nthreads_req = 1;
+void blo_set_threads(int n) {
+  nthreads_req = n > 0 ? n : 1;
+#ifdef _OPENMP
+  omp_set_num_threads(nthreads_req);
+#endif
+}
+
+/* Fortran-layout index helpers, 1-based indices as in the source */
+#define IX3(i, j, k, n1, n2) \
+  (((size_t)((k)-1) * (size_t)(n2) + (size_t)((j)-1)) * (size_t)(n1) + (size_t)((i)-1))
+#define AU(a, i, j, k) (a)[IX3(i, j, k, o->nx, o->nyg)]
+#define AV(a, i, j, k) (a)[IX3(i, j, k, o->nxg, o->ny)]
+#define AW(a, i, j, k) (a)[IX3(i, j, k, o->nxg, o->nyg)]
+#define AP(a, i, j, k) (a)[IX3(i, j, k, o->nxg, o->nyg)]
+/* rhs arrays with lower bound 2 in every dimension */
+#define RU(a, i, j, k) (a)[IX3((i)-1, (j)-1, (k)-1, o->nx - 2, o->nyg - 2)]
+#define RV(a, i, j, k) (a)[IX3((i)-1, (j)-1, (k)-1, o->nxg - 2, o->ny - 2)]
+#define RW(a, i, j, k) (a)[IX3((i)-1, (j)-1, (k)-1, o->nxg - 2, o->nyg - 2)]
+#define RP(a, i, j, k) (a)[IX3((i)-1, (j)-1, (k)-1, o->nxg - 2, o->nyg - 2)]
+
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+blo_t *blo_create(int nx, int ny, int nz, double nu, double cfl, double dpdx,
+                  double dpdz, int rk_scheme, int poisson_variant) {
+  if (nx < 4 || ny < 4 || nz < 4) return NULL;
+  blo_t *o = (blo_t *)calloc(1, sizeof(blo_t));
+  o->nx = nx; o->ny = ny; o->nz = nz;
+  o->nxg = nx + 1; o->nyg = ny + 1; o->nzg = nz + 1;
+  o->nxp = nx - 2; o->nzp = nz - 2; o->nm = ny - 1;
+  o->nu = nu; o->cfl = cfl; o->dpdx = dpdx; o->dpdz = dpdz;
+  o->rk_scheme = rk_scheme; o->variant = poisson_variant;
+  o->x = dalloc(nx + 1); o->y = dalloc(ny + 1); o->z = dalloc(nz + 1);
+  o->xm = dalloc(nx); o->ym = dalloc(ny); o->zm = dalloc(nz);
+  o->xg = dalloc(nx + 2); o->yg = dalloc(ny + 2); o->zg = dalloc(nz + 2);
+  o->wy0 = dalloc(ny + 1); o->wy1 = dalloc(ny + 1);
+  o->kxx = dalloc(o->nxp); o->kzz = dalloc(o->nzp);
+  o->Dd = dalloc(o->nyg + 1); o->Dl = dalloc(o->nyg + 1); o->Du = dalloc(o->nyg + 1);
+  size_t su = (size_t)nx * o->nyg * o->nzg, sv = (size_t)o->nxg * ny * o->nzg,
+         sw = (size_t)o->nxg * o->nyg * nz, sp = (size_t)o->nxg * o->nyg * o->nzg;
+  o->U = dalloc(su); o->V = dalloc(sv); o->W = dalloc(sw); o->P = dalloc(sp);
+  o->Uo = dalloc(su); o->Vo = dalloc(sv); o->Wo = dalloc(sw);
+  o->nu_t = dalloc(sp);
+  size_t fu = (size_t)(nx - 2) * (o->nyg - 2) * (o->nzg - 2),
+         fv = (size_t)(o->nxg - 2) * (ny - 2) * (o->nzg - 2),
+         fw = (size_t)(o->nxg - 2) * (o->nyg - 2) * (nz - 2);
+  for (int s = 0; s < 3; ++s) {
+    o->Fu[s] = dalloc(fu); o->Fv[s] = dalloc(fv); o->Fw[s] = dalloc(fw);
+  }
+  o->rhs_p = dalloc((size_t)(o->nxg - 2) * (o->nyg - 2) * (o->nzg - 1));
+  o->U_inlet = dalloc(o->nyg + 1); o->V_inlet = dalloc(ny + 1); o->W_inlet = dalloc(o->nyg + 1);
+  o->U_top = dalloc(nx + 1); o->V_top = dalloc(o->nxg + 1); o->W_top = dalloc(o->nxg + 1);
+  o->Ut = dalloc((size_t)o->nyg * o->nzg); o->Vt = dalloc((size_t)ny * o->nzg);
+  o->Wt = dalloc((size_t)o->nyg * nz);
+  o->rk_t[0] = 0.0; o->rk_t[1] = 8.0 / 15.0; o->rk_t[2] = 2.0 / 3.0; o->rk_t[3] = 1.0;
+  memset(o->rk_coef, 0, sizeof(o->rk_coef));
+  o->rk_coef[0][0] = 8.0 / 15.0;
+  o->rk_coef[1][0] = 1.0 / 4.0; o->rk_coef[1][1] = 5.0 / 12.0;
+  o->rk_coef[2][0] = 1.0 / 4.0; o->rk_coef[2][1] = 0.0; o->rk_coef[2][2] = 3.0 / 4.0;
+  o->rk2_t[0] = 0.0; o->rk2_t[1] = 1.0 / 2.0; o->rk2_t[2] = 1.0;
+  o->rk2_coef[0][0] = 1.0 / 2.0; o->rk2_coef[0][1] = 0.0;
+  o->rk2_coef[1][0] = 0.0; o->rk2_coef[1][1] = 1.0;
+  o->rhs_hat = (cplx *)calloc((size_t)o->nxp * o->nm * o->nzp, sizeof(cplx));
+  o->pl_z = fft_plan_create(o->nzp);
+  o->pl_x = fft_plan_create(poisson_variant ? 2 * o->nxp : 4 * o->nxp);
+  return o;
+}
+
+void blo_destroy(blo_t *o) {
+  if (!o) return;
+  double *arrs[] = {o->x, o->y, o->z, o->xm, o->ym, o->zm, o->xg, o->yg, o->zg,
+                    o->wy0, o->wy1, o->kxx, o->kzz, o->Dd, o->Dl, o->Du, o->U,
+                    o->V, o->W, o->P, o->Uo, o->Vo, o->Wo, o->nu_t, o->rhs_p,
+                    o->U_inlet, o->V_inlet, o->W_inlet, o->U_top, o->V_top,
+                    o->W_top, o->Ut, o->Vt, o->Wt, o->zmode, o->tmode};
+  for (size_t q = 0; q < sizeof(arrs) / sizeof(arrs[0]); ++q) free(arrs[q]);
+  for (int s = 0; s < 3; ++s) { free(o->Fu[s]); free(o->Fv[s]); free(o->Fw[s]); }
+  free(o->qu); free(o->qv); free(o->qw);
+  free(o->rhs_hat); free(o->th_dl); free(o->th_dp); free(o->th_du); free(o->twid);
+  fft_plan_free(o->pl_x); fft_plan_free(o->pl_z);
+  free(o);
+}
+
+/* initialization.f90:174-222 (centres, ghosts, minimum spacing),
+ * 254-259 (dx, dz), 329-344 (modified wavenumbers), 395-425 (Dyy),
+ * 428-469 (Thomas factors, variant 1), 482-484 (weights), 316-320 (twiddle) */
+int blo_set_grid(blo_t *o, const double *x, const double *y, const double *z) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const int nxm = nx - 1, nym = ny - 1, nzm = nz - 1;
+  for (int i = 1; i <= nx; ++i) o->x[i] = x[i - 1];
+  for (int j = 1; j <= ny; ++j) o->y[j] = y[j - 1];
+  for (int k = 1; k <= nz; ++k) o->z[k] = z[k - 1];
+  for (int i = 1; i <= nxm; ++i) o->xm[i] = 0.5 * (o->x[i] + o->x[i + 1]);
+  for (int j = 1; j <= nym; ++j) o->ym[j] = 0.5 * (o->y[j] + o->y[j + 1]);
+  for (int k = 1; k <= nzm; ++k) o->zm[k] = 0.5 * (o->z[k] + o->z[k + 1]);
+  for (int i = 1; i <= nxm; ++i) o->xg[i + 1] = o->xm[i];
+  o->xg[1] = o->xm[1] - 2.0 * (o->xm[1] - o->x[1]);
+  o->xg[nxm + 2] = o->xm[nxm] + 2.0 * (o->x[nx] - o->xm[nxm]);
+  for (int j = 1; j <= nym; ++j) o->yg[j + 1] = o->ym[j];
+  o->yg[1] = o->ym[1] - 2.0 * (o->ym[1] - o->y[1]);
+  o->yg[nym + 2] = o->ym[nym] + 2.0 * (o->y[ny] - o->ym[nym]);
+  for (int k = 1; k <= nzm; ++k) o->zg[k + 1] = o->zm[k];
+  o->zg[1] = o->zm[1] - 2.0 * (o->zm[1] - o->z[1]);
+  o->zg[nzm + 2] = o->zm[nzm] + 2.0 * (o->z[nz] - o->zm[nzm]);
+  double mn;
+  mn = INFINITY;
+  for (int i = 2; i <= o->nxg; ++i) { double d = o->xg[i] - o->xg[i - 1]; if (d < mn) mn = d; }
+  o->dxmin = mn;
+  mn = INFINITY;
+  for (int j = 2; j <= o->nyg; ++j) { double d = o->yg[j] - o->yg[j - 1]; if (d < mn) mn = d; }
+  o->dymin = mn;
+  mn = INFINITY;
+  for (int k = 2; k <= o->nzg; ++k) { double d = o->zg[k] - o->zg[k - 1]; if (d < mn) mn = d; }
+  o->dzmin = mn;
+  o->dx = o->dxmin;
+  o->dz = o->dzmin;
+  const double pi = 4.0 * atan(1.0);
+  const int nxp = o->nxp, nzp = o->nzp;
+  for (int i = 0; i < nxp; ++i)
+    o->kxx[i] = 2.0 * (cos(pi * (double)i / (double)nxp) - 1.0) / (o->dx * o->dx);
+  int half = (int)ceil((double)nzp / 2.0);
+  for (int k = 0; k <= half && k < nzp; ++k)
+    o->kzz[k] = 2.0 * (cos(2.0 * pi * (double)k / (double)nzp) - 1.0) / (o->dz * o->dz);
+  for (int k = half + 1; k < nzp; ++k)
+    o->kzz[k] = 2.0 * (cos(2.0 * pi * (double)(-nzp + k) / (double)nzp) - 1.0) / (o->dz * o->dz);
+  /* Dyy: rows j = 2..nyg-1 */
+  const double *yy = o->y, *yg = o->yg;
+  const int nyg = o->nyg;
+  for (int j = 2; j <= nyg - 1; ++j) {
+    double a = 1.0 / (yy[j] - yy[j - 1]) / (yg[j + 1] - yg[j]);
+    double b = 1.0 / (yy[j] - yy[j - 1]) * (-1.0 / (yg[j + 1] - yg[j]) - 1.0 / (yg[j] - yg[j - 1]));
+    double c = 1.0 / (yy[j] - yy[j - 1]) / (yg[j] - yg[j - 1]);
+    o->Du[j] = a;  /* Dyy(j,j+1) */
+    o->Dl[j] = c;  /* Dyy(j,j-1) (sub-diagonal entry of row j) */
+    o->Dd[j] = b;
+    if (j == 2) o->Dd[j] = b + c;
+    if (j == nyg - 1) o->Dd[j] = a + b;
+  }
+  /* weights: weight_y_0(j) = (yg(j+1)-y(j))/(yg(j+1)-yg(j)), j = 1..ny */
+  for (int j = 1; j <= ny; ++j) {
+    o->wy0[j] = (yg[j + 1] - yy[j]) / (yg[j + 1] - yg[j]);
+    o->wy1[j] = 1.0 - o->wy0[j];
+  }
+  if (o->variant == 1) {
+    const int nm = o->nm;
+    free(o->th_dl); free(o->th_dp); free(o->th_du); free(o->twid);
+    o->th_dl = (cplx *)calloc((size_t)nxp * nzp * nm, sizeof(cplx));
+    o->th_dp = (cplx *)calloc((size_t)nxp * nzp * nm, sizeof(cplx));
+    o->th_du = (cplx *)calloc((size_t)nm, sizeof(cplx));
+    o->twid = (cplx *)calloc((size_t)nxp, sizeof(cplx));
+    /* thomas_du(jj) = Dyy(jj+1, jj+2), jj = 1..nm-1 */
+    for (int jj = 1; jj <= nm - 1; ++jj) o->th_du[jj - 1] = o->Du[jj + 1];
+    o->th_du[nm - 1] = 0;
+#define TH(a, ii, kk, jj) (a)[((size_t)((jj)-1) * nzp + (size_t)((kk)-1)) * nxp + (size_t)((ii)-1)]
+    for (int kk = 1; kk <= nzp; ++kk)
+      for (int ii = 1; ii <= nxp; ++ii) {
+        int ig = ii - 1, kg = kk - 1;
+        for (int jj = 1; jj <= nm; ++jj)
+          TH(o->th_dp, ii, kk, jj) = o->Dd[jj + 1] + o->kxx[ig] + o->kzz[kg];
+        /* thomas_dl_fact(jj) = Dyy(jj+2, jj+1): sub-diagonal of row jj+2 */
+        for (int jj = 1; jj <= nm - 1; ++jj) TH(o->th_dl, ii, kk, jj) = o->Dl[jj + 2];
+        TH(o->th_dl, ii, kk, nm) = 0;
+        if (ig == 0 && kg == 0) TH(o->th_dp, ii, kk, 1) = 3.0 / 2.0 * TH(o->th_dp, ii, kk, 1);
+        for (int jj = 2; jj <= nm; ++jj) {
+          cplx dd = TH(o->th_dl, ii, kk, jj - 1) / TH(o->th_dp, ii, kk, jj - 1);
+          TH(o->th_dl, ii, kk, jj - 1) = dd;
+          TH(o->th_dp, ii, kk, jj) = TH(o->th_dp, ii, kk, jj) - dd * o->th_du[jj - 2];
+        }
+        for (int jj = 1; jj <= nm; ++jj) TH(o->th_dp, ii, kk, jj) = 1.0 / TH(o->th_dp, ii, kk, jj);
+      }
+#undef TH
+    for (int i = 0; i < nxp; ++i) {
+      double a = -pi * (double)i / (2.0 * (double)nxp);
+      o->twid[i] = cos(a) + I * sin(a);
+    }
+  }
+  return 0;
+}
+
+void blo_set_bc(blo_t *o, const double *U_inlet, const double *V_inlet,
+                const double *W_inlet, const double *U_top, const double *V_top,
+                const double *W_top) {
+  for (int j = 1; j <= o->nyg; ++j) o->U_inlet[j] = U_inlet[j - 1];
+  for (int j = 1; j <= o->ny; ++j) o->V_inlet[j] = V_inlet[j - 1];
+  for (int j = 1; j <= o->nyg; ++j) o->W_inlet[j] = W_inlet[j - 1];
+  for (int i = 1; i <= o->nx; ++i) o->U_top[i] = U_top[i - 1];
+  for (int i = 1; i <= o->nxg; ++i) o->V_top[i] = V_top[i - 1];
+  for (int i = 1; i <= o->nxg; ++i) o->W_top[i] = W_top[i - 1];
+}
+
+void blo_set_modes(blo_t *o, int n_modes, int m_modes, const double *zmode,
+                   const double *tmode, const double *qu, const double *qv,
+                   const double *qw) {
+  free(o->zmode); free(o->tmode); free(o->qu); free(o->qv); free(o->qw);
+  o->n_modes = n_modes; o->m_modes = m_modes;
+  o->zmode = dalloc(n_modes); o->tmode = dalloc(m_modes);
+  memcpy(o->zmode, zmode, sizeof(double) * (size_t)n_modes);
+  memcpy(o->tmode, tmode, sizeof(double) * (size_t)m_modes);
+  size_t nu_ = (size_t)o->nyg * n_modes * m_modes, nv_ = (size_t)o->ny * n_modes * m_modes;
+  o->qu = (cplx *)malloc(sizeof(cplx) * nu_);
+  o->qv = (cplx *)malloc(sizeof(cplx) * nv_);
+  o->qw = (cplx *)malloc(sizeof(cplx) * nu_);
+  memcpy(o->qu, qu, sizeof(cplx) * nu_);
+  memcpy(o->qv, qv, sizeof(cplx) * nv_);
+  memcpy(o->qw, qw, sizeof(cplx) * nu_);
+}
+
+void blo_set_state(blo_t *o, const double *U, const double *V, const double *W,
+                   double t) {
+  size_t su = (size_t)o->nx * o->nyg * o->nzg, sv = (size_t)o->nxg * o->ny * o->nzg,
+         sw = (size_t)o->nxg * o->nyg * o->nz;
+  memcpy(o->U, U, su * sizeof(double));
+  memcpy(o->V, V, sv * sizeof(double));
+  memcpy(o->W, W, sw * sizeof(double));
+  /* read_input_data sets Uo = U (input_output.f90:476-478) */
+  memcpy(o->Uo, U, su * sizeof(double));
+  memcpy(o->Vo, V, sv * sizeof(double));
+  memcpy(o->Wo, W, sw * sizeof(double));
+  o->t = t;
+}
+
+void blo_get_state(const blo_t *o, double *U, double *V, double *W, double *P,
+                   double *t) {
+  size_t su = (size_t)o->nx * o->nyg * o->nzg, sv = (size_t)o->nxg * o->ny * o->nzg,
+         sw = (size_t)o->nxg * o->nyg * o->nz, sp = (size_t)o->nxg * o->nyg * o->nzg;
+  if (U) memcpy(U, o->U, su * sizeof(double));
+  if (V) memcpy(V, o->V, sv * sizeof(double));
+  if (W) memcpy(W, o->W, sw * sizeof(double));
+  if (P) memcpy(P, o->P, sp * sizeof(double));
+  if (t) *t = o->t;
+}
+
+void blo_set_nu_t(blo_t *o, const double *nu_t, int les_model) {
+  memcpy(o->nu_t, nu_t, sizeof(double) * (size_t)o->nxg * o->nyg * o->nzg);
+  o->les = les_model;
+}
+
+void blo_set_dt(blo_t *o, double dt) { o->dt = dt; }
+double blo_get_dt(const blo_t *o) { return o->dt; }
+
+/* ------------------------------------------------------------------------ */
+/* RHS: equations.f90:24-415 (DNS branch and LES branch)                     */
+/* ------------------------------------------------------------------------ */
+
+#define NUT(i, j, k) o->nu_t[IX3(i, j, k, o->nxg, o->nyg)]
+
+static void rhs_u_impl(blo_t *o, const double *U_, const double *V_,
+                       const double *W_, double *rhs) {
+  const double *x = o->x, *xg = o->xg, *y = o->y, *yg = o->yg, *z = o->z,
+               *zg = o->zg, *w0 = o->wy0, *w1 = o->wy1;
+  const double nu = o->nu, dPdx = o->dpdx;
+  const int nx = o->nx, nyg = o->nyg, nzg = o->nzg;
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        /* equations.f90:53-64 */
+        double a = 0.5 * (AU(U_, i, j, k) + AU(U_, i + 1, j, k));
+        double b = 0.5 * (AU(U_, i - 1, j, k) + AU(U_, i, j, k));
+        double r = -(a * a - b * b) / (xg[i + 1] - xg[i]);
+        double t1 = (w0[j] * AU(U_, i, j, k) + w1[j] * AU(U_, i, j + 1, k)) * 0.5 *
+                    (AV(V_, i, j, k) + AV(V_, i + 1, j, k));
+        double t2 = (w0[j - 1] * AU(U_, i, j - 1, k) + w1[j - 1] * AU(U_, i, j, k)) * 0.5 *
+                    (AV(V_, i, j - 1, k) + AV(V_, i + 1, j - 1, k));
+        r = r - (t1 - t2) / (y[j] - y[j - 1]);
+        double t3 = 0.5 * (AU(U_, i, j, k) + AU(U_, i, j, k + 1)) * 0.5 *
+                    (AW(W_, i, j, k) + AW(W_, i + 1, j, k));
+        double t4 = 0.5 * (AU(U_, i, j, k - 1) + AU(U_, i, j, k)) * 0.5 *
+                    (AW(W_, i, j, k - 1) + AW(W_, i + 1, j, k - 1));
+        r = r - (t3 - t4) / (z[k] - z[k - 1]);
+        double dx_1 = x[i] - x[i - 1], dx_2 = x[i + 1] - x[i], dx_3 = xg[i + 1] - xg[i];
+        double dy_3 = y[j] - y[j - 1];
+        double dz_1 = zg[k] - zg[k - 1], dz_2 = zg[k + 1] - zg[k], dz_3 = z[k] - z[k - 1];
+        double uc = AU(U_, i, j, k);
+        if (o->les == 0) {
+          /* equations.f90:88-91 */
+          double vx = (1.0 / dx_2 * (AU(U_, i + 1, j, k) - uc) - 1.0 / dx_1 * (uc - AU(U_, i - 1, j, k))) / dx_3;
+          double vy = ((AU(U_, i, j + 1, k) - uc) / (yg[j + 1] - yg[j]) -
+                       (uc - AU(U_, i, j - 1, k)) / (yg[j] - yg[j - 1])) / dy_3;
+          double vz = (1.0 / dz_2 * (AU(U_, i, j, k + 1) - uc) - 1.0 / dz_1 * (uc - AU(U_, i, j, k - 1))) / dz_3;
+          r = r + dPdx + nu * (vx + vy + vz);
+        } else {
+          /* equations.f90:98-129 */
+          double nu_x1 = nu + NUT(i, j, k);
+          double nu_x2 = nu + NUT(i + 1, j, k);
+          double nu_y1 = nu + 0.5 * (w0[j - 1] * NUT(i, j - 1, k) + w1[j - 1] * NUT(i, j, k) +
+                                     w0[j - 1] * NUT(i + 1, j - 1, k) + w1[j - 1] * NUT(i + 1, j, k));
+          double nu_y2 = nu + 0.5 * (w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k) +
+                                     w0[j] * NUT(i + 1, j, k) + w1[j] * NUT(i + 1, j + 1, k));
+          double nu_z1 = nu + 0.25 * (NUT(i, j, k) + NUT(i, j, k - 1) + NUT(i + 1, j, k) + NUT(i + 1, j, k - 1));
+          double nu_z2 = nu + 0.25 * (NUT(i, j, k) + NUT(i, j, k + 1) + NUT(i + 1, j, k) + NUT(i + 1, j, k + 1));
+          double t2p = (AU(U_, i, j + 1, k) - uc) / (yg[j + 1] - yg[j]);
+          double t2m = (uc - AU(U_, i, j - 1, k)) / (yg[j] - yg[j - 1]);
+          r = r + dPdx +
+              (nu_x2 / dx_2 * (AU(U_, i + 1, j, k) - uc) - nu_x1 / dx_1 * (uc - AU(U_, i - 1, j, k))) / dx_3 +
+              (nu_y2 * t2p - nu_y1 * t2m) / dy_3 +
+              (nu_z2 / dz_2 * (AU(U_, i, j, k + 1) - uc) - nu_z1 / dz_1 * (uc - AU(U_, i, j, k - 1))) / dz_3;
+        }
+        RU(rhs, i, j, k) = r;
+      }
+  /* equations.f90:149-154 */
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j) RU(rhs, nx - 1, j, k) = 0.0;
+}
+
+static void rhs_v_impl(blo_t *o, const double *U_, const double *V_,
+                       const double *W_, double *rhs) {
+  const double *x = o->x, *xg = o->xg, *y = o->y, *yg = o->yg, *z = o->z,
+               *zg = o->zg, *w0 = o->wy0, *w1 = o->wy1;
+  const double nu = o->nu;
+  const int nxg = o->nxg, ny = o->ny, nzg = o->nzg;
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        /* equations.f90:188-201 */
+        double a = 0.5 * (AV(V_, i, j, k) + AV(V_, i, j + 1, k));
+        double b = 0.5 * (AV(V_, i, j - 1, k) + AV(V_, i, j, k));
+        double r = -(a * a - b * b) / (yg[j + 1] - yg[j]);
+        double t1 = (w0[j] * AU(U_, i, j, k) + w1[j] * AU(U_, i, j + 1, k)) * 0.5 *
+                    (AV(V_, i, j, k) + AV(V_, i + 1, j, k));
+        double t2 = (w0[j] * AU(U_, i - 1, j, k) + w1[j] * AU(U_, i - 1, j + 1, k)) * 0.5 *
+                    (AV(V_, i - 1, j, k) + AV(V_, i, j, k));
+        r = r - (t1 - t2) / (x[i] - x[i - 1]);
+        double t3 = 0.5 * (AV(V_, i, j, k) + AV(V_, i, j, k + 1)) *
+                    (w0[j] * AW(W_, i, j, k) + w1[j] * AW(W_, i, j + 1, k));
+        double t4 = 0.5 * (AV(V_, i, j, k - 1) + AV(V_, i, j, k)) *
+                    (w0[j] * AW(W_, i, j, k - 1) + w1[j] * AW(W_, i, j + 1, k - 1));
+        r = r - (t3 - t4) / (z[k] - z[k - 1]);
+        double dx_1 = xg[i] - xg[i - 1], dx_2 = xg[i + 1] - xg[i], dx_3 = x[i] - x[i - 1];
+        double dy_1 = y[j] - y[j - 1], dy_2 = y[j + 1] - y[j], dy_3 = yg[j + 1] - yg[j];
+        double dz_1 = zg[k] - zg[k - 1], dz_2 = zg[k + 1] - zg[k], dz_3 = z[k] - z[k - 1];
+        double vc = AV(V_, i, j, k);
+        if (o->les == 0) {
+          /* equations.f90:224-227 */
+          double vx = (1.0 / dx_2 * (AV(V_, i + 1, j, k) - vc) - 1.0 / dx_1 * (vc - AV(V_, i - 1, j, k))) / dx_3;
+          double vy = (1.0 / dy_2 * (AV(V_, i, j + 1, k) - vc) - 1.0 / dy_1 * (vc - AV(V_, i, j - 1, k))) / dy_3;
+          double vz = (1.0 / dz_2 * (AV(V_, i, j, k + 1) - vc) - 1.0 / dz_1 * (vc - AV(V_, i, j, k - 1))) / dz_3;
+          r = r + nu * (vx + vy + vz);
+        } else {
+          /* equations.f90:238-266 */
+          double nu_x1 = nu + 0.5 * (w0[j] * NUT(i - 1, j, k) + w1[j] * NUT(i - 1, j + 1, k) +
+                                     w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k));
+          double nu_x2 = nu + 0.5 * (w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k) +
+                                     w0[j] * NUT(i + 1, j, k) + w1[j] * NUT(i + 1, j + 1, k));
+          double nu_y1 = nu + NUT(i, j, k);
+          double nu_y2 = nu + NUT(i, j + 1, k);
+          double nu_z1 = nu + 0.5 * (w0[j] * NUT(i, j, k - 1) + w1[j] * NUT(i, j + 1, k - 1) +
+                                     w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k));
+          double nu_z2 = nu + 0.5 * (w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k) +
+                                     w0[j] * NUT(i, j, k + 1) + w1[j] * NUT(i, j + 1, k + 1));
+          r = r +
+              1.0 / dx_3 * (nu_x2 * 1.0 / dx_2 * (AV(V_, i + 1, j, k) - vc) - nu_x1 * 1.0 / dx_1 * (vc - AV(V_, i - 1, j, k))) +
+              1.0 / dy_3 * (nu_y2 * 1.0 / dy_2 * (AV(V_, i, j + 1, k) - vc) - nu_y1 * 1.0 / dy_1 * (vc - AV(V_, i, j - 1, k))) +
+              1.0 / dz_3 * (nu_z2 * 1.0 / dz_2 * (AV(V_, i, j, k + 1) - vc) - nu_z1 * 1.0 / dz_1 * (vc - AV(V_, i, j, k - 1)));
+        }
+        RV(rhs, i, j, k) = r;
+      }
+  /* equations.f90:287-292 */
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j) RV(rhs, nxg - 1, j, k) = 0.0;
+}
+
+static void rhs_w_impl(blo_t *o, const double *U_, const double *V_,
+                       const double *W_, double *rhs) {
+  const double *x = o->x, *xg = o->xg, *y = o->y, *yg = o->yg, *z = o->z,
+               *zg = o->zg, *w0 = o->wy0, *w1 = o->wy1;
+  const double nu = o->nu, dPdz = o->dpdz;
+  const int nxg = o->nxg, nyg = o->nyg, nz = o->nz;
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        /* equations.f90:328-339 */
+        double a = 0.5 * (AW(W_, i, j, k) + AW(W_, i, j, k + 1));
+        double b = 0.5 * (AW(W_, i, j, k - 1) + AW(W_, i, j, k));
+        double r = -(a * a - b * b) / (zg[k + 1] - zg[k]);
+        double t1 = 0.5 * (AU(U_, i, j, k) + AU(U_, i, j, k + 1)) * 0.5 *
+                    (AW(W_, i, j, k) + AW(W_, i + 1, j, k));
+        double t2 = 0.5 * (AU(U_, i - 1, j, k) + AU(U_, i - 1, j, k + 1)) * 0.5 *
+                    (AW(W_, i - 1, j, k) + AW(W_, i, j, k));
+        r = r - (t1 - t2) / (x[i] - x[i - 1]);
+        double t3 = 0.5 * (AV(V_, i, j, k) + AV(V_, i, j, k + 1)) *
+                    (w0[j] * AW(W_, i, j, k) + w1[j] * AW(W_, i, j + 1, k));
+        double t4 = 0.5 * (AV(V_, i, j - 1, k) + AV(V_, i, j - 1, k + 1)) *
+                    (w0[j - 1] * AW(W_, i, j - 1, k) + w1[j - 1] * AW(W_, i, j, k));
+        r = r - (t3 - t4) / (y[j] - y[j - 1]);
+        double dx_1 = xg[i] - xg[i - 1], dx_2 = xg[i + 1] - xg[i], dx_3 = x[i] - x[i - 1];
+        double dy_3 = y[j] - y[j - 1];
+        double dz_1 = z[k] - z[k - 1], dz_2 = z[k + 1] - z[k], dz_3 = zg[k + 1] - zg[k];
+        double wc = AW(W_, i, j, k);
+        if (o->les == 0) {
+          /* equations.f90:360-363 */
+          double vx = (1.0 / dx_2 * (AW(W_, i + 1, j, k) - wc) - 1.0 / dx_1 * (wc - AW(W_, i - 1, j, k))) / dx_3;
+          double vy = ((AW(W_, i, j + 1, k) - wc) / (yg[j + 1] - yg[j]) -
+                       (wc - AW(W_, i, j - 1, k)) / (yg[j] - yg[j - 1])) / dy_3;
+          double vz = (1.0 / dz_2 * (AW(W_, i, j, k + 1) - wc) - 1.0 / dz_1 * (wc - AW(W_, i, j, k - 1))) / dz_3;
+          r = r + dPdz + nu * (vx + vy + vz);
+        } else {
+          /* equations.f90:370-401 */
+          double nu_x1 = nu + 0.25 * (NUT(i, j, k) + NUT(i, j, k + 1) + NUT(i - 1, j, k) + NUT(i - 1, j, k + 1));
+          double nu_x2 = nu + 0.25 * (NUT(i, j, k) + NUT(i, j, k + 1) + NUT(i + 1, j, k) + NUT(i + 1, j, k + 1));
+          double nu_y1 = nu + 0.5 * (w0[j - 1] * NUT(i, j - 1, k) + w1[j - 1] * NUT(i, j, k) +
+                                     w0[j - 1] * NUT(i, j - 1, k + 1) + w1[j - 1] * NUT(i, j, k + 1));
+          double nu_y2 = nu + 0.5 * (w0[j] * NUT(i, j, k) + w1[j] * NUT(i, j + 1, k) +
+                                     w0[j] * NUT(i, j, k + 1) + w1[j] * NUT(i, j + 1, k + 1));
+          double nu_z1 = nu + NUT(i, j, k);
+          double nu_z2 = nu + NUT(i, j, k + 1);
+          double t2p = (AW(W_, i, j + 1, k) - wc) / (yg[j + 1] - yg[j]);
+          double t2m = (wc - AW(W_, i, j - 1, k)) / (yg[j] - yg[j - 1]);
+          r = r + dPdz +
+              (nu_x2 / dx_2 * (AW(W_, i + 1, j, k) - wc) - nu_x1 / dx_1 * (wc - AW(W_, i - 1, j, k))) / dx_3 +
+              (nu_y2 * t2p - nu_y1 * t2m) / dy_3 +
+              (nu_z2 / dz_2 * (AW(W_, i, j, k + 1) - wc) - nu_z1 / dz_1 * (wc - AW(W_, i, j, k - 1))) / dz_3;
+        }
+        RW(rhs, i, j, k) = r;
+      }
+  /* equations.f90:408-413 */
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j) RW(rhs, nxg - 1, j, k) = 0.0;
+}
+
+void blo_rhs_u(blo_t *o, const double *U, const double *V, const double *W, double *r) { rhs_u_impl(o, U, V, W, r); }
+void blo_rhs_v(blo_t *o, const double *U, const double *V, const double *W, double *r) { rhs_v_impl(o, U, V, W, r); }
+void blo_rhs_w(blo_t *o, const double *U, const double *V, const double *W, double *r) { rhs_w_impl(o, U, V, W, r); }
+
+/* ------------------------------------------------------------------------ */
+/* boundary conditions: boundary_conditions.f90:127-262                     */
+/* (the CPU routine apply_boundary_conditions, :22-121, takes the same steps */
+/*  in the same order for inflow_flag 1/2, top_flag 0 and WM 0)             */
+/* ------------------------------------------------------------------------ */
+void blo_apply_bc(blo_t *o, int rk_step) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+  double *U = o->U, *V = o->V, *W = o->W;
+  const double *Uo = o->Uo, *Vo = o->Vo, *Wo = o->Wo;
+  const double t = o->t, dt = o->dt;
+  /* temporal inflow modes (:137-180) */
+  if (o->n_modes > 0) {
+    const int nm_ = o->n_modes, mm_ = o->m_modes;
+    for (int j = 1; j <= nyg; ++j)
+      for (int k = 1; k <= nzg; ++k) {
+        double acc = 0.0;
+        for (int n = 0; n < nm_; ++n)
+          for (int m = 0; m < mm_; ++m) {
+            cplx q = o->qu[((size_t)m * nm_ + n) * nyg + (j - 1)];
+            double th = o->zmode[n] * o->zg[k] - o->tmode[m] * t;
+            acc = acc + (creal(q) * cos(th) - cimag(q) * sin(th));
+          }
+        o->Ut[(size_t)(k - 1) * nyg + (j - 1)] = acc;
+      }
+    for (int j = 1; j <= ny; ++j)
+      for (int k = 1; k <= nzg; ++k) {
+        double acc = 0.0;
+        for (int n = 0; n < nm_; ++n)
+          for (int m = 0; m < mm_; ++m) {
+            cplx q = o->qv[((size_t)m * nm_ + n) * ny + (j - 1)];
+            double th = o->zmode[n] * o->zg[k] - o->tmode[m] * t;
+            acc = acc + (creal(q) * cos(th) - cimag(q) * sin(th));
+          }
+        o->Vt[(size_t)(k - 1) * ny + (j - 1)] = acc;
+      }
+    for (int j = 1; j <= nyg; ++j)
+      for (int k = 1; k <= nz; ++k) {
+        double acc = 0.0;
+        for (int n = 0; n < nm_; ++n)
+          for (int m = 0; m < mm_; ++m) {
+            cplx q = o->qw[((size_t)m * nm_ + n) * nyg + (j - 1)];
+            double th = o->zmode[n] * o->z[k] - o->tmode[m] * t;
+            acc = acc + (creal(q) * cos(th) - cimag(q) * sin(th));
+          }
+        o->Wt[(size_t)(k - 1) * nyg + (j - 1)] = acc;
+      }
+  }
+  /* inflow plane (:182-190) */
+  for (int j = 1; j <= nyg; ++j) {
+    for (int k = 1; k <= nzg; ++k) AU(U, 1, j, k) = o->U_inlet[j] + o->Ut[(size_t)(k - 1) * nyg + (j - 1)];
+    for (int k = 1; k <= nz; ++k) AW(W, 1, j, k) = o->W_inlet[j] + o->Wt[(size_t)(k - 1) * nyg + (j - 1)];
+  }
+  for (int j = 1; j <= ny; ++j)
+    for (int k = 1; k <= nzg; ++k) AV(V, 1, j, k) = o->V_inlet[j] + o->Vt[(size_t)(k - 1) * ny + (j - 1)];
+  /* convective outflow (:193-201) */
+  const double Uc = o->U_top[nx];
+  const double c = o->rk_t[rk_step] * dt * Uc;
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j)
+      AU(U, nx - 1, j, k) = AU(Uo, nx - 1, j, k) - c * (AU(Uo, nx - 1, j, k) - AU(Uo, nx - 2, j, k)) / (o->x[nx - 1] - o->x[nx - 2]);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= ny; ++j)
+      AV(V, nxg - 1, j, k) = AV(Vo, nxg - 1, j, k) - c * (AV(Vo, nxg - 1, j, k) - AV(Vo, nxg - 2, j, k)) / (o->xg[nxg - 1] - o->xg[nxg - 2]);
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= nyg; ++j)
+      AW(W, nxg - 1, j, k) = AW(Wo, nxg - 1, j, k) - c * (AW(Wo, nxg - 1, j, k) - AW(Wo, nxg - 2, j, k)) / (o->xg[nxg - 1] - o->xg[nxg - 2]);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j) AU(U, nx, j, k) = AU(U, nx - 1, j, k);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= ny; ++j) AV(V, nxg, j, k) = AV(V, nxg - 1, j, k);
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= nyg; ++j) AW(W, nxg, j, k) = AW(W, nxg - 1, j, k);
+  /* periodic z (:204-216) */
+  {
+    size_t pu = (size_t)nx * nyg, pv = (size_t)nxg * ny, pw = (size_t)nxg * nyg;
+    memcpy(U, U + (size_t)(nzg - 3) * pu, pu * sizeof(double));
+    memcpy(U + (size_t)(nzg - 2) * pu, U + 1 * pu, pu * sizeof(double));
+    memcpy(U + (size_t)(nzg - 1) * pu, U + 2 * pu, pu * sizeof(double));
+    memcpy(V, V + (size_t)(nzg - 3) * pv, pv * sizeof(double));
+    memcpy(V + (size_t)(nzg - 2) * pv, V + 1 * pv, pv * sizeof(double));
+    memcpy(V + (size_t)(nzg - 1) * pv, V + 2 * pv, pv * sizeof(double));
+    memcpy(W, W + (size_t)(nz - 2) * pw, pw * sizeof(double));
+    memcpy(W + (size_t)(nz - 1) * pw, W + 1 * pw, pw * sizeof(double));
+  }
+  /* top (:219-227) */
+  for (int k = 1; k <= nzg; ++k)
+    for (int i = 1; i <= nx; ++i) AU(U, i, nyg, k) = o->U_top[i];
+  for (int k = 1; k <= nzg; ++k)
+    for (int i = 1; i <= nxg; ++i) AV(V, i, ny, k) = o->V_top[i];
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nxg; ++i) AW(W, i, nyg, k) = o->W_top[i];
+  /* wall (:230-237) */
+  for (int k = 1; k <= nzg; ++k)
+    for (int i = 1; i <= nx; ++i) AU(U, i, 1, k) = -AU(U, i, 2, k);
+  for (int k = 1; k <= nzg; ++k)
+    for (int i = 1; i <= nxg; ++i) AV(V, i, 1, k) = 0.0;
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nxg; ++i) AW(W, i, 1, k) = -AW(W, i, 2, k);
+  /* global mass conservation (:240-260), kk = 2 at nprocs = 1 */
+  double Qx = 0.0, length_y = 0.0, Qy = 0.0;
+  for (int j = 2; j <= nyg - 1; ++j) {
+    double s = 0.0;
+    for (int k = 2; k <= nzg - 2; ++k) s += (AU(U, 1, j, k) - AU(U, nx - 1, j, k)) * (o->y[j] - o->y[j - 1]);
+    Qx = Qx + s;
+    length_y = length_y + o->y[j] - o->y[j - 1];
+  }
+  for (int i = 2; i <= nxg - 2; ++i) {
+    double s = 0.0;
+    for (int k = 2; k <= nzg - 2; ++k) s += (AV(V, i, 1, k) - AV(V, i, ny, k)) * (o->x[i] - o->x[i - 1]);
+    Qy = Qy + s;
+  }
+  double Q = Qx + Qy;
+  double dU = Q / length_y / (double)(nzg - 3);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j) {
+      AU(U, nx - 1, j, k) = AU(U, nx - 1, j, k) + dU;
+      AU(U, nx, j, k) = AU(U, nx - 1, j, k);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* projection: projection.f90:21-386                                        */
+/* ------------------------------------------------------------------------ */
+
+static void poisson_cpu(blo_t *o) {
+  /* projection.f90:210-288 */
+  const int nxp = o->nxp, nzp = o->nzp, nm = o->nm, nyg = o->nyg;
+  const int L = 4 * nxp;
+  cplx *hat = o->rhs_hat; /* (0:nxp-1, j=2..nyg-1 -> 0..nm-1, 0:nzp-1) */
+#define HAT(i, b, k) hat[((size_t)(k) * nm + (size_t)(b)) * nxp + (size_t)(i)]
+#pragma omp parallel
+  {
+    cplx *plane = (cplx *)malloc(sizeof(cplx) * (size_t)L * nzp);
+    size_t wsz = fft_work_size(o->pl_x);
+    size_t wz = fft_work_size(o->pl_z);
+    cplx *work = (cplx *)malloc(sizeof(cplx) * (wsz > wz ? wsz : wz));
+    cplx *col = (cplx *)malloc(sizeof(cplx) * (size_t)nzp);
+#pragma omp for schedule(static)
+    for (int j = 2; j <= nyg - 1; ++j) {
+      memset(plane, 0, sizeof(cplx) * (size_t)L * nzp);
+      for (int k = 0; k < nzp; ++k)
+        for (int ii = 1; ii <= nxp; ++ii) {
+          double f = RP(o->rhs_p, ii + 1, j, k + 2);
+          plane[(size_t)k * L + (size_t)(2 * ii - 1)] = f;         /* slot i = 2,4,..,2nxp */
+          plane[(size_t)k * L + (size_t)(L - 1 - 2 * (ii - 1))] = f; /* slot i = 4nxp..2nxp+2 */
+        }
+      /* 2D forward DFT: rows (x) then columns (z) */
+      for (int k = 0; k < nzp; ++k) fft_exec(o->pl_x, plane + (size_t)k * L, work);
+      for (int i = 0; i < nxp; ++i) {
+        for (int k = 0; k < nzp; ++k) col[k] = plane[(size_t)k * L + i];
+        fft_exec(o->pl_z, col, work);
+        for (int k = 0; k < nzp; ++k) HAT(i, j - 2, k) = col[k];
+      }
+    }
+    /* tridiagonal per mode (:238-256) */
+    cplx *D = (cplx *)malloc(sizeof(cplx) * (size_t)nm);
+    cplx *DL = (cplx *)malloc(sizeof(cplx) * (size_t)nm);
+    cplx *DU = (cplx *)malloc(sizeof(cplx) * (size_t)nm);
+    cplx *r = (cplx *)malloc(sizeof(cplx) * (size_t)nm);
+#pragma omp for schedule(static)
+    for (int k = 0; k < nzp; ++k)
+      for (int i = 0; i < nxp; ++i) {
+        for (int j = 2; j <= nyg - 1; ++j) D[j - 2] = o->Dd[j] + o->kxx[i] + o->kzz[k];
+        for (int j = 2; j <= nyg - 2; ++j) DL[j - 2] = o->Dl[j + 1];
+        for (int j = 2; j <= nyg - 2; ++j) DU[j - 2] = o->Du[j];
+        if (i == 0 && k == 0) D[0] = 3.0 / 2.0 * D[0];
+        for (int b = 0; b < nm; ++b) r[b] = HAT(i, b, k);
+        zgtsv_c(nm, DL, D, DU, r);
+        for (int b = 0; b < nm; ++b) HAT(i, b, k) = r[b];
+      }
+    /* inverse (:259-283) */
+    const double norm = (double)L * (double)nzp;
+#pragma omp for schedule(static)
+    for (int j = 2; j <= nyg - 1; ++j) {
+      memset(plane, 0, sizeof(cplx) * (size_t)L * nzp);
+      const int b = j - 2;
+      for (int k = 0; k < nzp; ++k) {
+        cplx *row = plane + (size_t)k * L;
+        for (int i = 0; i < nxp; ++i) row[i] = HAT(i, b, k);
+        for (int s = nxp + 1; s <= 2 * nxp; ++s) row[s] = -HAT(2 * nxp - s, b, k);
+        for (int s = 2 * nxp + 1; s <= 3 * nxp - 1; ++s) row[s] = -HAT(s - 2 * nxp, b, k);
+        for (int s = 3 * nxp + 1; s <= 4 * nxp - 1; ++s) row[s] = HAT(4 * nxp - s, b, k);
+      }
+      for (int k = 0; k < nzp; ++k) fft_exec_dir(o->pl_x, plane + (size_t)k * L, work, 1);
+      for (int i = 0; i < L; ++i) {
+        if ((i & 1) == 0) continue; /* only odd slots are read back */
+        for (int k = 0; k < nzp; ++k) col[k] = plane[(size_t)k * L + i];
+        fft_exec_dir(o->pl_z, col, work, 1);
+        for (int k = 0; k < nzp; ++k) plane[(size_t)k * L + i] = col[k];
+      }
+      for (int k = 0; k < nzp; ++k)
+        for (int ii = 2; ii <= nxp + 1; ++ii)
+          RP(o->rhs_p, ii, j, k + 2) = creal(plane[(size_t)k * L + (size_t)(2 * (ii - 1) - 1)]) / norm;
+    }
+    free(D); free(DL); free(DU); free(r);
+    free(plane); free(work); free(col);
+  }
+#undef HAT
+}
+
+static void poisson_gpu_semantics(blo_t *o) {
+  /* projection.f90:93-204 (FP64 restatement of the cuFFT path) */
+  const int nxp = o->nxp, nzp = o->nzp, nm = o->nm;
+  const int L = 2 * nxp;
+  cplx *hat = o->rhs_hat; /* rhs_hat_gpu(mx+1, nm, mz+1) */
+#define HAT(i, b, k) hat[((size_t)(k) * nm + (size_t)(b)) * nxp + (size_t)(i)]
+#define TH(a, i, k, jj) (a)[((size_t)(jj) * nzp + (size_t)(k)) * nxp + (size_t)(i)]
+  const double fft_norm = 1.0 / (double)(2 * nxp * nzp);
+#pragma omp parallel
+  {
+    cplx *plane = (cplx *)malloc(sizeof(cplx) * (size_t)L * nzp);
+    size_t wsz = fft_work_size(o->pl_x), wz = fft_work_size(o->pl_z);
+    cplx *work = (cplx *)malloc(sizeof(cplx) * (wsz > wz ? wsz : wz));
+    cplx *col = (cplx *)malloc(sizeof(cplx) * (size_t)nzp);
+#pragma omp for schedule(static)
+    for (int b = 0; b < nm; ++b) {
+      for (int k = 0; k < nzp; ++k)
+        for (int ii = 1; ii <= nxp; ++ii) {
+          double f = RP(o->rhs_p, ii + 1, b + 2, k + 2);
+          plane[(size_t)k * L + (size_t)(ii - 1)] = f;
+          plane[(size_t)k * L + (size_t)(L - ii)] = f;
+        }
+      for (int k = 0; k < nzp; ++k) fft_exec(o->pl_x, plane + (size_t)k * L, work);
+      for (int i = 0; i < nxp; ++i) {
+        for (int k = 0; k < nzp; ++k) col[k] = plane[(size_t)k * L + i];
+        fft_exec(o->pl_z, col, work);
+        for (int k = 0; k < nzp; ++k) HAT(i, b, k) = col[k] * o->twid[i];
+      }
+    }
+#pragma omp for schedule(static)
+    for (int k = 0; k < nzp; ++k)
+      for (int i = 0; i < nxp; ++i) {
+        for (int jj = 1; jj < nm; ++jj)
+          HAT(i, jj, k) = HAT(i, jj, k) - TH(o->th_dl, i, k, jj - 1) * HAT(i, jj - 1, k);
+        HAT(i, nm - 1, k) = HAT(i, nm - 1, k) * TH(o->th_dp, i, k, nm - 1);
+        for (int jj = nm - 2; jj >= 0; --jj)
+          HAT(i, jj, k) = (HAT(i, jj, k) - o->th_du[jj] * HAT(i, jj + 1, k)) * TH(o->th_dp, i, k, jj);
+      }
+#pragma omp for schedule(static)
+    for (int b = 0; b < nm; ++b) {
+      for (int i = 0; i < nxp; ++i) {
+        for (int k = 0; k < nzp; ++k) col[k] = HAT(i, b, k);
+        fft_exec_dir(o->pl_z, col, work, 1);
+        for (int k = 0; k < nzp; ++k) plane[(size_t)k * L + i] = col[k] * conj(o->twid[i]);
+      }
+      for (int k = 0; k < nzp; ++k) {
+        cplx *row = plane + (size_t)k * L;
+        row[nxp] = 0;
+        for (int ii = 2; ii <= nxp; ++ii) row[L + 1 - ii] = conj(row[ii - 1]);
+        fft_exec_dir(o->pl_x, row, work, 1);
+        for (int ii = 1; ii <= nxp; ++ii) RP(o->rhs_p, ii + 1, b + 2, k + 2) = creal(row[ii - 1]) * fft_norm;
+      }
+    }
+    free(plane); free(work); free(col);
+  }
+#undef HAT
+#undef TH
+}
+
+void blo_projection(blo_t *o, int rk_step) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+  const double *x = o->x, *y = o->y, *z = o->z, *xg = o->xg, *yg = o->yg, *zg = o->zg;
+  double *U = o->U, *V = o->V, *W = o->W;
+  /* compute_pseudo_pressure_rhs, projection.f90:38-47 */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i)
+        RP(o->rhs_p, i, j, k) = (AU(U, i, j, k) - AU(U, i - 1, j, k)) / (x[i] - x[i - 1]) +
+                                (AV(V, i, j, k) - AV(V, i, j - 1, k)) / (y[j] - y[j - 1]) +
+                                (AW(W, i, j, k) - AW(W, i, j, k - 1)) / (z[k] - z[k - 1]);
+  if (o->variant == 0) poisson_cpu(o); else poisson_gpu_semantics(o);
+  /* apply_periodic_z_pressure, :295-303 */
+  for (int k = 2; k <= nzg; ++k)
+    for (int j = 2; j <= nyg - 1; ++j) RP(o->rhs_p, nxg - 1, j, k) = RP(o->rhs_p, nxg - 2, j, k);
+  for (int j = 2; j <= nyg - 1; ++j)
+    for (int i = 2; i <= nxg - 1; ++i) RP(o->rhs_p, i, j, o->nzp + 2) = RP(o->rhs_p, i, j, 2);
+  /* pressure for statistics, :75-85 (P(...,2:nzg-1) = rhs_p(...,2:nzg-1)/(dt/2)) */
+  if (rk_step == 1) {
+    double *P = o->P;
+    const double den = o->dt * o->rk2_coef[0][0];
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AP(P, i, j, k) = RP(o->rhs_p, i, j, k) / den;
+    for (int k = 1; k <= nzg; ++k)
+      for (int j = 1; j <= nyg; ++j) { AP(P, 1, j, k) = AP(P, 2, j, k); }
+    for (int k = 1; k <= nzg; ++k)
+      for (int j = 1; j <= nyg; ++j) { AP(P, nxg, j, k) = AP(P, nxg - 1, j, k); }
+    for (int k = 1; k <= nzg; ++k)
+      for (int i = 1; i <= nxg; ++i) { AP(P, i, 1, k) = AP(P, i, 2, k); }
+    for (int k = 1; k <= nzg; ++k)
+      for (int i = 1; i <= nxg; ++i) { AP(P, i, nyg, k) = AP(P, i, nyg - 1, k); }
+    size_t pp = (size_t)nxg * nyg;
+    memcpy(P, P + pp, pp * sizeof(double));
+    memcpy(P + (size_t)(nzg - 1) * pp, P + (size_t)(nzg - 2) * pp, pp * sizeof(double));
+  }
+  /* project_velocity, :359-384 */
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i)
+        AU(U, i, j, k) = AU(U, i, j, k) - (RP(o->rhs_p, i + 1, j, k) - RP(o->rhs_p, i, j, k)) / (xg[i + 1] - xg[i]);
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i)
+        AV(V, i, j, k) = AV(V, i, j, k) - (RP(o->rhs_p, i, j + 1, k) - RP(o->rhs_p, i, j, k)) / (yg[j + 1] - yg[j]);
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i)
+        AW(W, i, j, k) = AW(W, i, j, k) - (RP(o->rhs_p, i, j, k + 1) - RP(o->rhs_p, i, j, k)) / (zg[k + 1] - zg[k]);
+}
+
+void blo_get_rhs_p(const blo_t *o, double *rhs_p) {
+  memcpy(rhs_p, o->rhs_p, sizeof(double) * (size_t)(o->nxg - 2) * (o->nyg - 2) * (o->nzg - 1));
+}
+
+/* check_divergence, projection.f90:391-413 */
+double blo_max_divergence(const blo_t *o) {
+  const double *U = o->U, *V = o->V, *W = o->W;
+  double div = 0.0;
+  for (int k = 2; k <= o->nzg - 1; ++k)
+    for (int j = 2; j <= o->nyg - 1; ++j)
+      for (int i = 2; i <= o->nxg - 2; ++i) {
+        double d = fabs((AU(U, i, j, k) - AU(U, i - 1, j, k)) / (o->x[i] - o->x[i - 1]) +
+                        (AV(V, i, j, k) - AV(V, i, j - 1, k)) / (o->y[j] - o->y[j - 1]) +
+                        (AW(W, i, j, k) - AW(W, i, j, k - 1)) / (o->z[k] - o->z[k - 1]));
+        if (d > div) div = d;
+      }
+  return div;
+}
+
+/* compute_dt, time_integration.f90:528-591 (note the max, as written) */
+double blo_compute_dt(blo_t *o) {
+  const double CFLa = fabs(o->cfl);
+  if (o->cfl < 0) {
+    o->dt = -o->cfl;
+    return o->dt;
+  }
+  double lU = 0.0, lV = 0.0, lW = 0.0;
+  for (int i = 2; i <= o->nxg - 1; ++i)
+    for (int j = 2; j <= o->nyg - 1; ++j)
+      for (int k = 2; k <= o->nzg - 1; ++k) {
+        double a = (o->xg[i + 1] - o->xg[i]) / fabs(AU(o->U, i, j, k));
+        double b = (o->yg[j + 1] - o->yg[j]) / fabs(AV(o->V, i, j, k));
+        double c = (o->zg[k + 1] - o->zg[k]) / fabs(AW(o->W, i, j, k));
+        lU = fmax(lU, a);
+        lV = fmax(lV, b);
+        lW = fmax(lW, c);
+      }
+  double cu = CFLa * lU, cv = CFLa * lV, cw = CFLa * lW;
+  double dt_conv = fmin(fmin(cu, cv), cw);
+  double vu = CFLa * (o->dxmin * o->dxmin) / o->nu;
+  double vv = CFLa * (o->dymin * o->dymin) / o->nu;
+  double vw = CFLa * (o->dzmin * o->dzmin) / o->nu;
+  double dt_vis = fmin(fmin(vu, vv), vw);
+  o->dt = fmin(dt_conv, dt_vis);
+  return o->dt;
+}
+
+/* ------------------------------------------------------------------------ */
+/* time stepping: time_integration.f90:24-114 (Euler), 145-300 (RK2),       */
+/* 305-465 (RK3)                                                            */
+/* ------------------------------------------------------------------------ */
+
+static void save_state(blo_t *o) {
+  size_t su = (size_t)o->nx * o->nyg * o->nzg, sv = (size_t)o->nxg * o->ny * o->nzg,
+         sw = (size_t)o->nxg * o->nyg * o->nz;
+  memcpy(o->Uo, o->U, su * sizeof(double));
+  memcpy(o->Vo, o->V, sv * sizeof(double));
+  memcpy(o->Wo, o->W, sw * sizeof(double));
+}
+
+/* U = Uo + dt*(sum_j a_j F_j), with the reference's association order */
+static void rk_update(blo_t *o, int nterms, const double *a) {
+  const double dt = o->dt;
+  const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        double s;
+        if (nterms == 1) s = dt * a[0] * RU(o->Fu[0], i, j, k);
+        else if (nterms == 2) s = dt * (a[0] * RU(o->Fu[0], i, j, k) + a[1] * RU(o->Fu[1], i, j, k));
+        else s = dt * (a[0] * RU(o->Fu[0], i, j, k) + a[1] * RU(o->Fu[1], i, j, k) + a[2] * RU(o->Fu[2], i, j, k));
+        AU(o->U, i, j, k) = AU(o->Uo, i, j, k) + s;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= ny - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double s;
+        if (nterms == 1) s = dt * a[0] * RV(o->Fv[0], i, j, k);
+        else if (nterms == 2) s = dt * (a[0] * RV(o->Fv[0], i, j, k) + a[1] * RV(o->Fv[1], i, j, k));
+        else s = dt * (a[0] * RV(o->Fv[0], i, j, k) + a[1] * RV(o->Fv[1], i, j, k) + a[2] * RV(o->Fv[2], i, j, k));
+        AV(o->V, i, j, k) = AV(o->Vo, i, j, k) + s;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double s;
+        if (nterms == 1) s = dt * a[0] * RW(o->Fw[0], i, j, k);
+        else if (nterms == 2) s = dt * (a[0] * RW(o->Fw[0], i, j, k) + a[1] * RW(o->Fw[1], i, j, k));
+        else s = dt * (a[0] * RW(o->Fw[0], i, j, k) + a[1] * RW(o->Fw[1], i, j, k) + a[2] * RW(o->Fw[2], i, j, k));
+        AW(o->W, i, j, k) = AW(o->Wo, i, j, k) + s;
+      }
+}
+
+static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms,
+                    double tnew) {
+  o->rk_step = rk_step;
+  rhs_u_impl(o, o->U, o->V, o->W, o->Fu[s]);
+  rhs_v_impl(o, o->U, o->V, o->W, o->Fv[s]);
+  rhs_w_impl(o, o->U, o->V, o->W, o->Fw[s]);
+  rk_update(o, nterms, coef);
+  o->t = tnew;
+  blo_apply_bc(o, rk_step);
+  blo_projection(o, rk_step);
+  blo_apply_bc(o, rk_step);
+}
+
+void blo_step(blo_t *o) {
+  const double to = o->t, dt = o->dt;
+  save_state(o);
+  if (o->rk_scheme == 3) {
+    double a1[1] = {o->rk_coef[0][0]};
+    substep(o, 0, 1, a1, 1, to + o->rk_t[1] * dt);
+    double a2[2] = {o->rk_coef[1][0], o->rk_coef[1][1]};
+    substep(o, 1, 2, a2, 2, to + o->rk_t[2] * dt);
+    double a3[3] = {o->rk_coef[2][0], o->rk_coef[2][1], o->rk_coef[2][2]};
+    substep(o, 2, 3, a3, 3, to + o->rk_t[3] * dt);
+  } else if (o->rk_scheme == 2) {
+    double a1[1] = {o->rk2_coef[0][0]};
+    substep(o, 0, 1, a1, 1, to + o->rk2_t[1] * dt);
+    double a2[2] = {o->rk2_coef[1][0], o->rk2_coef[1][1]};
+    substep(o, 1, 2, a2, 2, to + o->rk2_t[2] * dt);
+  } else {
+    /* Euler: U = Uo + dt*rhs(Uo); rk_step = 3 (time_integration.f90:24-114) */
+    o->rk_step = 3;
+    rhs_u_impl(o, o->Uo, o->Vo, o->Wo, o->Fu[0]);
+    rhs_v_impl(o, o->Uo, o->Vo, o->Wo, o->Fv[0]);
+    rhs_w_impl(o, o->Uo, o->Vo, o->Wo, o->Fw[0]);
+    /* U = Uo + dt*rhs, evaluated as Uo + (dt*rhs) */
+    const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nx - 1; ++i) AU(o->U, i, j, k) = AU(o->Uo, i, j, k) + dt * RU(o->Fu[0], i, j, k);
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= ny - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AV(o->V, i, j, k) = AV(o->Vo, i, j, k) + dt * RV(o->Fv[0], i, j, k);
+    for (int k = 2; k <= nz - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AW(o->W, i, j, k) = AW(o->Wo, i, j, k) + dt * RW(o->Fw[0], i, j, k);
+    o->t = to + dt;
+    blo_apply_bc(o, 3);
+    blo_projection(o, 3);
+    blo_apply_bc(o, 3);
+  }
+}

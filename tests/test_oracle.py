@@ -1,0 +1,93 @@
+"""CPU tests of the parity oracle (no GPU): its transforms, its ZGTSV
+restatement and its Poisson variants are pinned against numpy/scipy and
+against each other; the step is checked for discrete divergence."""
+import numpy as np
+import pytest
+from scipy.fft import dct
+from scipy.linalg.lapack import zgtsv
+
+import oracle
+from blgpu import cases
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 12, 30, 62, 94, 97, 126, 190, 191, 254, 510, 812, 1022, 3248])
+def test_fft_matches_numpy(n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ref = np.fft.fft(x)
+    scale = np.abs(ref).max()
+    assert np.abs(oracle.fft(x) - ref).max() <= 1e-14 * scale
+    assert np.abs(oracle.fft(x, inverse=True) - np.fft.ifft(x) * n).max() <= 1e-14 * scale
+
+
+@pytest.mark.parametrize("n", [4, 7, 126, 191, 812])
+def test_dct_matches_scipy(n):
+    f = np.random.default_rng(n).standard_normal(n)
+    c = oracle.dct2(f)
+    assert np.abs(c - dct(f, 2) / 2).max() <= 1e-13 * np.abs(f).sum()
+
+
+@pytest.mark.parametrize("pivot", [False, True])
+def test_zgtsv_matches_lapack(pivot):
+    rng = np.random.default_rng(7)
+    n = 64
+    dl = rng.random(n - 1) * (5.0 if pivot else 1.0) + 0j
+    d = -3.0 - rng.random(n) + 0j
+    du = rng.random(n - 1) + 0j
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    x, info = oracle.zgtsv(dl, d, du, b)
+    ref = zgtsv(dl, d, du, b)
+    assert info == 0 and ref[4] == 0
+    assert np.abs(x - ref[3]).max() <= 1e-14 * np.abs(ref[3]).max()
+
+
+def test_zgtsv_singular_reports_info():
+    x, info = oracle.zgtsv(np.zeros(3), np.array([1.0, 0.0, 1.0, 1.0]), np.zeros(3), np.ones(4))
+    assert info == 2
+
+
+def _small_case(nx=24, ny=12, nz=10):
+    return cases.laminar_case(nx=nx, ny=ny, nz=nz, lx=12.0, ly=4.0, lz=3.0)
+
+
+def test_poisson_variants_agree():
+    """4N embedding + ZGTSV (projection.f90:210-288) and 2N twiddle +
+    precomputed Thomas (projection.f90:93-204) give the same projection."""
+    c = _small_case(nx=26, ny=14, nz=11)  # odd nz: prime nzp = 9? (9 = 3^2) and N = 24
+    rng = np.random.default_rng(3)
+    c.V = c.V + 1e-3 * rng.standard_normal(c.V.shape)
+    c.W = c.W + 1e-3 * rng.standard_normal(c.W.shape)
+    o0 = oracle.oracle_for(c, variant=0)
+    o1 = oracle.oracle_for(c, variant=1)
+    for o in (o0, o1):
+        o.set_dt(0.05)
+        o.apply_bc(1)
+        o.projection(1)
+        o.apply_bc(1)
+    U0, V0, W0, P0, _ = o0.state()
+    U1, V1, W1, P1, _ = o1.state()
+    for a, b in ((U0, U1), (V0, V1), (W0, W1)):
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b)
+    assert o0.max_divergence() < 1e-12 and o1.max_divergence() < 1e-12
+
+
+@pytest.mark.parametrize("rk", [1, 2, 3])
+def test_step_is_divergence_free(rk):
+    c = _small_case()
+    c.rk_scheme = rk
+    o = oracle.oracle_for(c)
+    o.advance(3)
+    assert o.max_divergence() < 1e-12
+    U, V, W, P, t = o.state()
+    assert np.isfinite(U).all() and t > 0
+
+
+def test_compute_dt_uses_max_as_written():
+    """compute_dt takes the MAX of spacing/|u| (time_integration.f90:550-558);
+    with W == 0 somewhere the convective bound is +Inf and dt = dt_vis."""
+    c = _small_case()
+    o = oracle.oracle_for(c)
+    dt = o.compute_dt()
+    xg, yg, zg = cases.centres_ghost(c.x), cases.centres_ghost(c.y), cases.centres_ghost(c.z)
+    dt_vis = min(c.cfl * np.diff(xg).min() ** 2, c.cfl * np.diff(yg).min() ** 2, c.cfl * np.diff(zg).min() ** 2) / c.nu
+    assert dt == pytest.approx(dt_vis, rel=1e-15)

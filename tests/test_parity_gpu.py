@@ -1,0 +1,183 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bars: the FP64 RHS is bit-identical to the oracle's restatement of
+equations.f90; boundary conditions and projection agree to rounding; full
+steps agree to relative L2 <= 1e-10 after 10 steps with max divergence
+<= 1e-12 (the FP64 target); the mixed form stays within 1e-5.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from blgpu import cases, Solver, FP64, MIXED
+
+pytestmark = pytest.mark.gpu
+
+REL10 = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def noisy_laminar(nx, ny, nz, seed=0, amp=1e-2, **kw):
+    c = cases.laminar_case(nx=nx, ny=ny, nz=nz, lx=kw.pop("lx", 20.0), ly=kw.pop("ly", 5.0),
+                           lz=kw.pop("lz", 3.0), **kw)
+    rng = np.random.default_rng(seed)
+    c.U = np.asfortranarray(c.U + amp * rng.standard_normal(c.U.shape))
+    c.V = np.asfortranarray(c.V + amp * rng.standard_normal(c.V.shape))
+    c.W = np.asfortranarray(c.W + amp * rng.standard_normal(c.W.shape))
+    return c
+
+
+GRIDS = [(26, 14, 11), (60, 17, 15), (128, 64, 32), (37, 9, 24)]
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_rhs_bit_identical(gpu, grid):
+    c = noisy_laminar(*grid, seed=1)
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    got = s.compute_rhs(c.U, c.V, c.W)
+    ref = o.rhs(c.U, c.V, c.W)
+    for g, r in zip(got, ref):
+        assert g.shape == r.shape
+        assert np.array_equal(g, r), np.abs(g - r).max()
+    s.close()
+
+
+@pytest.mark.parametrize("grid", GRIDS[:3])
+@pytest.mark.parametrize("rk_step", [1, 2, 3])
+def test_boundary_conditions(gpu, grid, rk_step):
+    c = noisy_laminar(*grid, seed=2)
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    for x in (s, o):
+        x.set_dt(0.01)
+    s.apply_boundary_conditions(rk_step)
+    o.apply_bc(rk_step)
+    U, V, W, _, _ = s.download_state()
+    Ur, Vr, Wr, _, _ = o.state()
+    assert np.array_equal(V, Vr) and np.array_equal(W, Wr)
+    # U differs only by the summation order of the mass-flux reduction
+    assert np.abs(U - Ur).max() <= 1e-14 * np.abs(Ur).max()
+    s.close()
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_projection(gpu, grid):
+    c = noisy_laminar(*grid, seed=3)
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    for x in (s, o):
+        x.set_dt(0.02)
+    s.apply_boundary_conditions(1)
+    o.apply_bc(1)
+    s.compute_projection_step(1)
+    o.projection(1)
+    U, V, W, P, _ = s.download_state()
+    Ur, Vr, Wr, Pr, _ = o.state()
+    assert rel(U, Ur) < 1e-13 and rel(V, Vr) < 1e-12 and rel(W, Wr) < 1e-12
+    assert rel(P, Pr) < 1e-11
+    rp, rpr = s.rhs_p()[:, :, :-1], o.rhs_p()[:, :, :-1]
+    assert rel(rp, rpr) < 1e-11
+    s.apply_boundary_conditions(1)
+    o.apply_bc(1)
+    assert s.check_divergence() < 1e-12
+    assert abs(s.check_divergence() - o.max_divergence()) < 1e-12
+    s.close()
+
+
+@pytest.mark.parametrize("rk", [3, 2, 1])
+def test_steps_small(gpu, rk):
+    c = noisy_laminar(60, 17, 15, seed=4, amp=1e-3, rk_scheme=rk)
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    for _ in range(5):
+        dt = s.compute_dt()
+        assert dt == o.compute_dt()
+        s.time_step()
+        o.step()
+    U, V, W, P, t = s.download_state()
+    Ur, Vr, Wr, Pr, tr = o.state()
+    assert t == pytest.approx(tr, rel=1e-15)
+    assert rel(U, Ur) < REL10 and rel(V, Vr) < REL10 and rel(W, Wr) < REL10
+    assert s.check_divergence() <= 1e-12
+    s.close()
+
+
+def test_laminar_cfg1_10_steps(gpu):
+    """Config 1 (128x64x32 laminar Blasius, RK3, CFL 0.5): 10 steps."""
+    c = cases.laminar_case()
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c, threads=4)
+    s.advance(10)
+    o.advance(10)
+    U, V, W, P, t = s.download_state()
+    Ur, Vr, Wr, Pr, tr = o.state()
+    assert rel(U, Ur) < REL10 and rel(V, Vr) < REL10
+    assert np.abs(W - Wr).max() < 1e-12
+    assert rel(P, Pr) < 1e-8
+    assert s.check_divergence() <= 1e-12
+    assert t == pytest.approx(tr, rel=1e-14)
+    s.close()
+
+
+def test_advance_graph_equals_eager(gpu):
+    c = noisy_laminar(37, 9, 24, seed=5, amp=1e-3)
+    a = cases.solver_for(c)
+    b = cases.solver_for(c)
+    a.advance(4)
+    for _ in range(4):
+        b.compute_dt()
+        b.time_step()
+    for x, y in zip(a.download_state()[:4], b.download_state()[:4]):
+        assert np.array_equal(x, y)
+
+
+def test_inflow_modes(gpu):
+    """temporal inflow modes (boundary_conditions.f90:137-180)"""
+    c = noisy_laminar(40, 13, 18, seed=6, amp=1e-4)
+    rng = np.random.default_rng(9)
+    n, m = 3, 2
+    zmode = np.array([0.0, 1.0, 2.0]) * 2 * np.pi / 3.0
+    tmode = np.array([1.0, 2.0]) * 0.1
+    qu = 1e-3 * (rng.standard_normal((c.ny + 1, n, m)) + 1j * rng.standard_normal((c.ny + 1, n, m)))
+    qv = 1e-3 * (rng.standard_normal((c.ny, n, m)) + 1j * rng.standard_normal((c.ny, n, m)))
+    qw = 1e-3 * (rng.standard_normal((c.ny + 1, n, m)) + 1j * rng.standard_normal((c.ny + 1, n, m)))
+    s = cases.solver_for(c)
+    s.set_inflow_modes(zmode, tmode, qu, qv, qw)
+    o = oracle.oracle_for(c)
+    o.set_modes(zmode, tmode, qu, qv, qw)
+    for _ in range(3):
+        s.compute_dt()
+        o.compute_dt()
+        s.time_step()
+        o.step()
+    U, V, W, _, _ = s.download_state()
+    Ur, Vr, Wr, _, _ = o.state()
+    assert rel(U, Ur) < REL10 and rel(V, Vr) < REL10 and rel(W, Wr) < REL10
+    s.close()
+
+
+def test_mixed_precision_error(gpu):
+    """FP32 fields/RHS/transforms with FP64 Thomas, zero mode and mass flux."""
+    c = cases.laminar_case()
+    s = cases.solver_for(c, precision=MIXED)
+    o = oracle.oracle_for(c, threads=4)
+    s.advance(10)
+    o.advance(10)
+    U, V, W, P, t = s.download_state()
+    Ur, Vr, Wr, Pr, tr = o.state()
+    eu, ev = rel(U, Ur), rel(V, Vr)
+    assert eu < 1e-5 and ev < 1e-4, (eu, ev)
+    assert s.check_divergence() < 1e-4
+    s.close()
+
+
+def test_errors_are_reported(gpu):
+    s = Solver(32, 16, 16, 1e-3, -1e-3)
+    with pytest.raises(Exception, match="grid"):
+        s.time_step()
+    s.close()
