@@ -1,0 +1,330 @@
+"""Benchmark of the B200 step path on the turbulent boundary-layer workload
+(814 x 257 x 193 = 40,375,214 cells, RK3 at CFL 0.5, synthetic initial field).
+
+Metric: ns per cell per RK3 step (lower is better) of the mixed FP32/FP64
+form, with the FP64 plain form timed on the same field beside it and the
+relative L2 difference of the two stated.  One process per GPU; every rank
+advances its own replica box (weak scaling, no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the CPU restatement of the reference step (oracle/)
+on the host cores, one RK3 substep per timed step, on the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "boundary-layer-gpu_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "ns/cell/RK3 step, mixed vs FP64 plain on one B200 at stated L2 error; HBM GB/s"
+UNIT = "ns/cell/step"
+CELLS_NOTE = "cells = nx*ny*nz"
+# algorithmic HBM bytes per cell per RK3 step: 73 compulsory element passes
+# (RHS+RK 33, projection 3 x 13, pressure save 1)
+PASSES_PER_STEP = 73
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=814)
+    ap.add_argument("--ny", type=int, default=257)
+    ap.add_argument("--nz", type=int, default=193)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % index) if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else "/tmp/blgpu_clocks_%d_%d.csv" % (os.getpid(), index)
+
+    def start(self):
+        try:
+            self.fh = open(self.out, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.out):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local) if args.impl == "b200" else None
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg, local):
+    if pg is None:
+        return
+    import torch
+    if torch.cuda.is_available():
+        pg.barrier(device_ids=[local])
+    else:
+        pg.barrier()
+
+
+def allmax(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device="cuda:%d" % local if torch.cuda.is_available() else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def algorithmic_bytes(phase, cells, esz, spectral_cells):
+    """compulsory bytes of one launch of a phase (element passes x size)"""
+    return {
+        "rhs_rk": 11.0 * cells * esz,       # average of 9 (s1) and 12 (s2, s3) passes
+        "div_dct": 4.0 * cells * esz,       # read U,V,W; write the DCT lines
+        "dft_z": 2.0 * spectral_cells * esz,
+        "thomas": 2.0 * spectral_cells * esz,
+        "idft_z": 2.0 * spectral_cells * esz,
+        "idct": 2.0 * spectral_cells * esz,
+        "project": 7.0 * cells * esz,       # read p, U, V, W; write U, V, W
+    }.get(phase)
+
+
+def run_reference(args, rank, world, pg):
+    """CPU restatement of the reference step on the host cores."""
+    if rank != 0:
+        return
+    import oracle
+    from blgpu import cases
+    threads = len(os.sched_getaffinity(0))
+    case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz)
+    o = oracle.oracle_for(case, threads=threads)
+    o.compute_dt()
+    stage = 1
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        o.rk3_stage(stage)
+        el = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(el)
+        stage = stage % 3 + 1
+        if stage == 1:
+            o.compute_dt()
+    per_sub = float(np.mean(times))
+    v = 3.0 * per_sub / case.cells * 1e9
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 3.0 * per_sub * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "turbulent BL %dx%dx%d RK3 CFL 0.5 (CPU restatement of the reference step)"
+                                   % (args.nx, args.ny, args.nz), "cells": case.cells},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "one RK3 substep of the full box per timed step, x3 per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args):
+    import oracle
+    from blgpu import cases
+    threads = len(os.sched_getaffinity(0))
+    case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz)
+    o = oracle.oracle_for(case, threads=threads)
+    o.compute_dt()
+    t0 = time.perf_counter()
+    o.rk3_stage(1)
+    el = time.perf_counter() - t0
+    v = 3.0 * el / case.cells * 1e9
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "one RK3 substep (stage 1) of the full %dx%dx%d box, x3" % (args.nx, args.ny, args.nz)}
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    import torch
+    import blgpu
+    from blgpu import cases
+    dev = local
+    torch.cuda.set_device(dev)
+    case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz, seed=1234 + rank)
+    cells = case.cells
+    N, M, NM = case.nx - 2, case.nz - 2, case.ny - 1
+    spectral_cells = N * M * NM
+
+    def timed_run(precision):
+        s = cases.solver_for(case, precision=precision, device=dev)
+        s.advance(args.warmup)
+        s.sync()
+        barrier(pg, local)
+        l0 = s.kernel_launches()
+        ms = s.advance_timed(args.steps)
+        launches = s.kernel_launches() - l0
+        barrier(pg, local)
+        return s, ms, launches
+
+    hbm, peak_kind = peaks()
+    clocks = Clocks(dev)
+    # ---- mixed form (headline) ----
+    clocks.start()
+    smix, ms_mix, launches = timed_run(blgpu.MIXED)
+    clk = clocks.stop()
+    ms_mix = allmax(pg, ms_mix, local)
+    ms_step_mix = ms_mix / args.steps
+    value = ms_step_mix * 1e6 / (cells * world)
+    # ---- FP64 plain form ----
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        s64, ms64, _ = timed_run(blgpu.FP64)
+        ms64 = allmax(pg, ms64, local)
+        ms_step64 = ms64 / args.steps
+        fp64 = {"ns_per_cell_step": ms_step64 * 1e6 / (cells * world), "ms_per_step": ms_step64,
+                "hbm_gbs_step": PASSES_PER_STEP * 8.0 * cells / (ms_step64 * 1e-3) / 1e9}
+        Um, Vm, Wm, _, tm = smix.download_state()
+        U6, V6, W6, _, t6 = s64.download_state()
+        err = {"u": float(np.linalg.norm(Um - U6) / np.linalg.norm(U6)),
+               "v": float(np.linalg.norm(Vm - V6) / np.linalg.norm(V6)),
+               "w": float(np.linalg.norm(Wm - W6) / np.linalg.norm(W6)),
+               "steps": args.warmup + args.steps, "t": t6,
+               "max_div_mixed": smix.check_divergence(), "max_div_fp64": s64.check_divergence()}
+        ph64 = s64.phase_times(1)
+        s64.close()
+    # ---- per-phase device times (CUDA events on the solver stream) ----
+    ph = smix.phase_times(2)
+    step_ms = sum(v[0] for v in ph.values()) / 2.0
+    dom = max((k for k in ph if algorithmic_bytes(k, cells, 4, spectral_cells)), key=lambda k: ph[k][0])
+    dom_ms, dom_n = ph[dom]
+    launch_ms = dom_ms / max(dom_n, 1)
+    alg = algorithmic_bytes(dom, cells, 4, spectral_cells)
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": alg, "launch_ms": launch_ms}
+    # ---- end to end through the C ABI with pinned host buffers ----
+    pin = lambda shape: torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True).numpy().reshape(
+        shape, order="F")
+    Uh = pin(case.U.shape); Vh = pin(case.V.shape); Wh = pin(case.W.shape)
+    Uh[...] = case.U; Vh[...] = case.V; Wh[...] = case.W
+    e2e_n = max(1, args.e2e_steps)
+    import ctypes
+    lib = smix.lib
+    dp = blgpu._lib.c_double_p
+    ptr = lambda a: a.ctypes.data_as(dp)
+    tt = ctypes.c_double()
+    smix.sync()
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for _ in range(e2e_n):
+        blgpu._lib.check(lib.blgpu_upload_state(smix.ctx, ptr(Uh), ptr(Vh), ptr(Wh), 0.0), smix.ctx)
+        blgpu._lib.check(lib.blgpu_advance(smix.ctx, 1), smix.ctx)
+        blgpu._lib.check(lib.blgpu_download_state(smix.ctx, ptr(Uh), ptr(Vh), ptr(Wh), None, ctypes.byref(tt)),
+                         smix.ctx)
+    el = time.perf_counter() - t0
+    el = allmax(pg, el, local)
+    bytes_state = 8 * (Uh.size + Vh.size + Wh.size)
+    e2e = {"value": el / e2e_n * 1e9 / (cells * world), "unit": UNIT, "h2d_bytes_per_step": bytes_state,
+           "d2h_bytes_per_step": bytes_state, "steps": e2e_n,
+           "what": "upload_state + advance(1) + download_state per step, FP64 Fortran-layout pinned host arrays"}
+    smix.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step_mix, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 fields / f64 Thomas", "data": "synthetic",
+                "config": {"workload": "turbulent BL DNS %dx%dx%d (%d cells), RK3 CFL 0.5, Re_theta 1100, "
+                                       "mixed FP32/FP64" % (case.nx, case.ny, case.nz, cells),
+                           "cells": cells, "l2": "inputs larger than L2 (3 x %.0f MB per state)"
+                                                  % (smix_bytes(case, 4) / 1e6),
+                           "replicas_per_gpu": 1},
+                "hbm_gbs_step": PASSES_PER_STEP * 4.0 * cells / (ms_step_mix * 1e-3) / 1e9,
+                "fp64": fp64, "mixed_rel_l2_vs_fp64": err,
+                "speedup_mixed_vs_fp64": (fp64["ms_per_step"] / ms_step_mix) if fp64 else None,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk, "phases_ms_per_step_mixed": {k: v[0] / 2.0 for k, v in ph.items()},
+                "phases_ms_per_step_fp64": ({k: v[0] for k, v in ph64.items()} if fp64 else None),
+                "eager_step_ms_mixed": step_ms}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def smix_bytes(case, esz):
+    return (case.nx + 1 + 31) // 32 * 32 * (case.ny + 1) * (case.nz + 1) * esz
+
+
+if __name__ == "__main__":
+    main()

@@ -48,7 +48,13 @@ _SIGS = {
     "blgpu_max_divergence": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "blgpu_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "blgpu_device_bytes": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "blgpu_phase_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
+                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    "blgpu_kernel_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "blgpu_advance_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),
 }
+
+PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]
 
 _lib = None
 

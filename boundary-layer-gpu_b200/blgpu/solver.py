@@ -127,6 +127,12 @@ class Solver:
         """nsteps of the main loop body: compute_dt + time step (CUDA graph)."""
         self._ck(self.lib.blgpu_advance(self.ctx, int(nsteps)))
 
+    def advance_timed(self, nsteps):
+        """advance(nsteps) timed with CUDA events on the solver stream (ms)."""
+        ms = ctypes.c_double()
+        self._ck(self.lib.blgpu_advance_timed(self.ctx, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
     def sync(self):
         self._ck(self.lib.blgpu_sync(self.ctx))
 
@@ -158,3 +164,14 @@ class Solver:
 
     def device_bytes(self):
         return int(self.lib.blgpu_device_bytes(self.ctx))
+
+    def kernel_launches(self):
+        return int(self.lib.blgpu_kernel_launches(self.ctx))
+
+    def phase_times(self, nsteps=1):
+        """{phase: (ms total, kernels)} over nsteps eager steps (CUDA events)."""
+        n = len(_lib.PHASES)
+        ms = (ctypes.c_double * n)()
+        kn = (ctypes.c_longlong * n)()
+        self._ck(self.lib.blgpu_phase_times(self.ctx, int(nsteps), ms, kn, n))
+        return {p: (ms[i], kn[i]) for i, p in enumerate(_lib.PHASES)}

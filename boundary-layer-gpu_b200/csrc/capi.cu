@@ -58,10 +58,48 @@ struct blgpu_ctx {
   void *tw = nullptr, *post = nullptr, *ztab = nullptr;
   FftPlan<double> pl64{};
   FftPlan<float> pl32{};
+  double *stage = nullptr;  // FP64 staging of one host-layout field
   int cur = 0, old = 1;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_next[3] = {0, 0, 0};
+  long long graph_launches[3] = {0, 0, 0};
+  // kernel accounting and optional per-phase event timing
+  long long launches = 0;
+  bool prof_on = false;
+  struct Mark { int phase; cudaEvent_t a, b; int nk; };
+  std::vector<Mark> marks;
+  int cur_phase = -1, cur_nk = 0;
+  cudaEvent_t cur_ev = nullptr;
+  Geo geo_box() const {
+    Geo g = geo;
+    g.nx = nx; g.ny = ny; g.nz = nz; g.nxg = nxg; g.nyg = nyg; g.nzg = nzg;
+    g.px = px; g.py = py; g.plane = plane;
+    return g;
+  }
 };
+
+enum { PH_RHS = 0, PH_BC, PH_DIVDCT, PH_DFTZ, PH_THOMAS, PH_IDFTZ, PH_IDCT, PH_PROJECT, PH_DT, PH_MISC, PH_N };
+
+// Every launcher call is bracketed by ph_begin/ph_end: they count the kernels
+// issued and, while profiling, record CUDA events on the context stream.
+static void ph_begin(blgpu_ctx *ctx, int phase) {
+  ctx->cur_phase = phase;
+  if (ctx->prof_on) {
+    cudaEventCreate(&ctx->cur_ev);
+    cudaEventRecord(ctx->cur_ev, ctx->st);
+  }
+}
+
+static void ph_end(blgpu_ctx *ctx, int nk) {
+  ctx->launches += nk;
+  if (ctx->prof_on) {
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, ctx->st);
+    ctx->marks.push_back({ctx->cur_phase, ctx->cur_ev, b, nk});
+    ctx->cur_ev = nullptr;
+  }
+}
 
 namespace blgpu {
 
@@ -186,6 +224,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, (void **)&ctx->dcrow, (size_t)s.NM * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->dcout, (size_t)s.NM * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->sc, sizeof(Scalars)));
+  TRY(dalloc(ctx, (void **)&ctx->stage, (size_t)ctx->nxg * ctx->nyg * ctx->nzg * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->d_maxdiv, sizeof(unsigned long long)));
   // transform tables
   {
@@ -510,28 +549,20 @@ static void from_box(const blgpu_ctx *c, const std::vector<T> &box, int n1, int 
 }
 
 static int upload_field(blgpu_ctx *ctx, void *dst, const double *a, int n1, int n2, int n3) {
-  if (ctx->fp64) {
-    std::vector<double> b;
-    to_box(ctx, a, n1, n2, n3, b);
-    CK(cudaMemcpy(dst, b.data(), b.size() * 8, cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float> b;
-    to_box(ctx, a, n1, n2, n3, b);
-    CK(cudaMemcpy(dst, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
-  }
+  CK(cudaMemcpyAsync(ctx->stage, a, (size_t)n1 * n2 * n3 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 0, ctx->stage, (double *)dst, n1, n2, n3, ctx->st);
+  else launch_repack<float>(ctx->geo_box(), 0, ctx->stage, (float *)dst, n1, n2, n3, ctx->st);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
   return BLGPU_OK;
 }
 
 static int download_field(blgpu_ctx *ctx, const void *src, double *a, int n1, int n2, int n3) {
-  if (ctx->fp64) {
-    std::vector<double> b((size_t)ctx->boxn);
-    CK(cudaMemcpy(b.data(), src, b.size() * 8, cudaMemcpyDeviceToHost));
-    from_box(ctx, b, n1, n2, n3, a);
-  } else {
-    std::vector<float> b((size_t)ctx->boxn);
-    CK(cudaMemcpy(b.data(), src, b.size() * 4, cudaMemcpyDeviceToHost));
-    from_box(ctx, b, n1, n2, n3, a);
-  }
+  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 1, ctx->stage, (double *)src, n1, n2, n3, ctx->st);
+  else launch_repack<float>(ctx->geo_box(), 1, ctx->stage, (float *)src, n1, n2, n3, ctx->st);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(a, ctx->stage, (size_t)n1 * n2 * n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
   return BLGPU_OK;
 }
 
@@ -541,7 +572,10 @@ int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t) {
   if (!ctx || !nu_t) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_nu_t: null argument");
   if (!ctx->nut) return set_err(ctx, BLGPU_ESTATE, "blgpu_set_nu_t: context created with LES=0");
   CK(cudaSetDevice(ctx->cfg.device));
-  return upload_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);
+  int rc = upload_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
 }
 
 int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t) {
@@ -550,12 +584,13 @@ int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const d
   CK(cudaStreamSynchronize(ctx->st));
   ctx->cur = 0;
   ctx->old = 1;
-  for (int b : {ctx->cur, ctx->old}) {
-    int rc = upload_field(ctx, ctx->S[b][0], U, ctx->nx, ctx->nyg, ctx->nzg);
-    if (!rc) rc = upload_field(ctx, ctx->S[b][1], V, ctx->nxg, ctx->ny, ctx->nzg);
-    if (!rc) rc = upload_field(ctx, ctx->S[b][2], W, ctx->nxg, ctx->nyg, ctx->nz);
-    if (rc) return rc;
-  }
+  int rc = upload_field(ctx, ctx->S[0][0], U, ctx->nx, ctx->nyg, ctx->nzg);
+  if (!rc) rc = upload_field(ctx, ctx->S[0][1], V, ctx->nxg, ctx->ny, ctx->nzg);
+  if (!rc) rc = upload_field(ctx, ctx->S[0][2], W, ctx->nxg, ctx->nyg, ctx->nz);
+  if (rc) return rc;
+  for (int q = 0; q < 3; ++q)
+    CK(cudaMemcpyAsync(ctx->S[1][q], ctx->S[0][q], (size_t)ctx->boxn * ctx->esz, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   Scalars h{};
   CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
   h.t = t;
@@ -577,6 +612,7 @@ int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double
   if (W && !rc) rc = download_field(ctx, ctx->S[ctx->cur][2], W, ctx->nxg, ctx->nyg, ctx->nz);
   if (P && !rc) rc = download_field(ctx, ctx->P, P, ctx->nxg, ctx->nyg, ctx->nzg);
   if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
   if (t) {
     Scalars h{};
     CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
@@ -613,8 +649,10 @@ template <typename T>
 static void enq_bc(blgpu_ctx *ctx, int b, int o, int rk_step) {
   T **S = reinterpret_cast<T **>(ctx->S[b]);
   T **So = reinterpret_cast<T **>(ctx->S[o]);
+  ph_begin(ctx, PH_BC);
   launch_bc<T>(ctx->geo, ctx->bc, S[0], S[1], S[2], So[0], So[1], So[2], ctx->sc, ctx->rk_t[rk_step], ctx->qx_part,
                ctx->qy, ctx->length_y, ctx->st);
+  ph_end(ctx, 4);
 }
 
 template <typename T>
@@ -624,16 +662,28 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const Spec &s = ctx->spec;
   const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
   const bool mixed = !ctx->fp64;
+  ph_begin(ctx, PH_DIVDCT);
   launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, mixed ? ctx->dcsum : nullptr, ctx->st);
+  ph_end(ctx, 1);
+  ph_begin(ctx, PH_DFTZ);
   launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->st);
+  ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
+  ph_begin(ctx, PH_THOMAS);
   launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp, sp + s.NM, sp + 2 * s.NM, sp + 3 * s.NM, sp + 3 * s.NM + s.N,
                    mixed ? ctx->dcsum : nullptr, ctx->dcrow, mixed ? ctx->dcout : nullptr, ctx->st);
+  ph_end(ctx, mixed ? 2 : 1);
+  ph_begin(ctx, PH_IDFTZ);
   launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->st);
+  ph_end(ctx, 1);
+  ph_begin(ctx, PH_IDCT);
   launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->st);
+  ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
+  ph_begin(ctx, PH_PROJECT);
   launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->dcout : nullptr, S[0], S[1], S[2],
                     (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->st);
+  ph_end(ctx, rk_step == 1 ? 4 : 1);
 }
 
 template <typename T>
@@ -643,8 +693,10 @@ static void enq_rhs(blgpu_ctx *ctx, int mode, int in, int o, int outb, double c1
   T **Sn = reinterpret_cast<T **>(ctx->S[outb]);
   T **F = reinterpret_cast<T **>(ctx->F1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
+  ph_begin(ctx, PH_RHS);
   launch_rhs_rk<T>(ctx->geo, m, mode, ctx->cfg.les_model != 0, Si[0], Si[1], Si[2], (const T *)ctx->nut, So[0], So[1],
                    So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->st);
+  ph_end(ctx, 1);
 }
 
 // One time step from buffer a.  Returns the index of the new state buffer.
@@ -653,12 +705,18 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
   const int b = (a + 1) % 3, c = (a + 2) % 3;
   if (with_dt && ctx->cfg.cfl > 0) {
     T **S = reinterpret_cast<T **>(ctx->S[a]);
+    ph_begin(ctx, PH_DT);
     launch_dt<T>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+    ph_end(ctx, 2);
   }
+  ph_begin(ctx, PH_MISC);
   launch_set_time(ctx->sc, 0, 0.0, ctx->st);
+  ph_end(ctx, 1);
   auto sub = [&](int mode, int in, int outb, double c1, double c2, double tc, int rk_step) {
     enq_rhs<T>(ctx, mode, in, a, outb, c1, c2);
+    ph_begin(ctx, PH_MISC);
     launch_set_time(ctx->sc, 1, tc, ctx->st);
+    ph_end(ctx, 1);
     enq_bc<T>(ctx, outb, a, rk_step);
     enq_projection<T>(ctx, outb, rk_step);
     enq_bc<T>(ctx, outb, a, rk_step);
@@ -705,12 +763,15 @@ int blgpu_advance(blgpu_ctx *ctx, int nsteps) {
   if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
     return set_err(ctx, BLGPU_ESTATE, "blgpu_advance: grid, boundary and state must be set first");
   CK(cudaSetDevice(ctx->cfg.device));
-  for (int n = 0; n < nsteps; ++n) {
+  for (int n = 0; n < (nsteps > 0 ? nsteps : 1); ++n) {
     const int a = ctx->cur;
     if (!ctx->graph[a]) {
       cudaGraph_t gr = nullptr;
       CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeRelaxed));
+      const long long l0 = ctx->launches;
       const int nb = ctx->fp64 ? enq_step<double>(ctx, a, true) : enq_step<float>(ctx, a, true);
+      ctx->graph_launches[a] = ctx->launches - l0;
+      ctx->launches = l0;
       cudaError_t e = cudaStreamEndCapture(ctx->st, &gr);
       if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
       e = cudaGraphInstantiate(&ctx->graph[a], gr, 0);
@@ -718,7 +779,9 @@ int blgpu_advance(blgpu_ctx *ctx, int nsteps) {
       if (e != cudaSuccess) return check_cuda(ctx, e, "cudaGraphInstantiate");
       ctx->graph_next[a] = nb;
     }
+    if (nsteps == 0) break;  // capture only
     CK(cudaGraphLaunch(ctx->graph[a], ctx->st));
+    ctx->launches += ctx->graph_launches[a];
     ctx->old = a;
     ctx->cur = ctx->graph_next[a];
   }
@@ -778,6 +841,7 @@ int blgpu_compute_rhs(blgpu_ctx *ctx, const double *U, const double *V, const do
     full.assign((size_t)nxg * nyg * nzg, 0.0);
     int r = download_field(ctx, ctx->F1[q], full.data(), nxg, nyg, nzg);
     if (r) return r;
+    CK(cudaStreamSynchronize(ctx->st));
     const int e1 = i1 - 1, e2 = j1 - 1;
     for (int k = 2; k <= k1; ++k)
       for (int j = 2; j <= j1; ++j)
@@ -823,6 +887,7 @@ int blgpu_get_rhs_p(blgpu_ctx *ctx, double *rhs_p) {
   std::vector<double> full((size_t)nxg * nyg * nzg);
   int rc = download_field(ctx, ctx->rhs_p, full.data(), nxg, nyg, nzg);
   if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
   const int e1 = nxg - 2, e2 = nyg - 2;
   for (int k = 2; k <= nzg; ++k)
     for (int j = 2; j <= nyg - 1; ++j)
@@ -851,6 +916,61 @@ int blgpu_max_divergence(blgpu_ctx *ctx, double *max_div) {
   double v;
   memcpy(&v, &bits, sizeof v);
   *max_div = v;
+  return BLGPU_OK;
+}
+
+int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels, int nphase) {
+  if (!ctx || !ms || nphase < PH_N || nsteps < 1) return set_err(ctx, BLGPU_EINVAL, "blgpu_phase_times: bad argument");
+  if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_phase_times: grid, boundary and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int p = 0; p < nphase; ++p) {
+    ms[p] = 0.0;
+    if (kernels) kernels[p] = 0;
+  }
+  ctx->prof_on = true;
+  ctx->marks.clear();
+  for (int n = 0; n < nsteps; ++n) step_once(ctx, true);
+  ctx->prof_on = false;
+  cudaError_t e = cudaStreamSynchronize(ctx->st);
+  for (auto &mk : ctx->marks) {
+    float t = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&t, mk.a, mk.b);
+    ms[mk.phase] += t;
+    if (kernels) kernels[mk.phase] += mk.nk;
+    cudaEventDestroy(mk.a);
+    cudaEventDestroy(mk.b);
+  }
+  ctx->marks.clear();
+  CK(e);
+  return BLGPU_OK;
+}
+
+long long blgpu_kernel_launches(const blgpu_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms) {
+  if (!ctx || !ms) return set_err(ctx, BLGPU_EINVAL, "blgpu_advance_timed: null argument");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->have_grid && ctx->have_bc && ctx->have_state && !ctx->graph[ctx->cur]) {
+    // capture outside the timed region
+    int rc = blgpu_advance(ctx, 0);
+    if (rc) return rc;
+  }
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, ctx->st));
+  int rc = blgpu_advance(ctx, nsteps);
+  cudaEventRecord(b, ctx->st);
+  cudaError_t e = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (!rc && e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  CK(e);
+  *ms = (double)t;
   return BLGPU_OK;
 }
 

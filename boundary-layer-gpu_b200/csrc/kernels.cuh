@@ -42,6 +42,9 @@ void launch_set_time(Scalars *sc, int phase, double coef, cudaStream_t st);
 template <typename T>
 void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st);
 
+template <typename T>
+void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st);
+
 // ---- spectral.cu ----
 // Transform plan of one axis length n (device tables)
 template <typename T> struct FftPlan {

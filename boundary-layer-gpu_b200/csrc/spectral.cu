@@ -377,12 +377,15 @@ __global__ void __launch_bounds__(256) k_dft_z_fwd(Spec s, const T *__restrict__
       im[r] = 0;
       m[r] = 0;
     }
+    int inc[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) inc[r] = kz[r] < MH ? kz[r] : 0;  // idle slots stay at m = 0
     for (int k = 1; k <= H; ++k) {
       const T fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
       const T a = fk + fm, bb = fk - fm;
 #pragma unroll
       for (int r = 0; r < RPT; ++r) {
-        m[r] += kz[r];
+        m[r] += inc[r];
         if (m[r] >= M) m[r] -= M;
         const T2<T> cs = tab[m[r]];
         re[r] += a * cs.x;
@@ -431,11 +434,14 @@ __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restri
       Q[r] = 0;
       m[r] = 0;
     }
+    int inc[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) inc[r] = pp[r] < npairs ? pp[r] : 0;  // idle slots stay at m = 0
     for (int kz = 1; kz <= H; ++kz) {
       const T2<T> v = c[kz * 32 + lane];
 #pragma unroll
       for (int r = 0; r < RPT; ++r) {
-        m[r] += pp[r];
+        m[r] += inc[r];
         if (m[r] >= M) m[r] -= M;
         const T2<T> cs = tab[m[r]];
         P[r] += v.x * cs.x;

@@ -558,3 +558,42 @@ BLGPU_INST(double)
 BLGPU_INST(float)
 
 }  // namespace blgpu
+
+namespace blgpu {
+
+// ---------------------------------------------------------------------------
+// host-layout <-> box-layout repack (the Fortran arrays of the reference,
+// staged as FP64 in device memory, to and from the padded box in precision T)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_repack_in(Geo g, const double *__restrict__ src, int n1, int n2, int n3, T *__restrict__ dst) {
+  const long long tot = (long long)n1 * n2 * n3;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % n1);
+    const long long r = q / n1;
+    const int j = (int)(r % n2), k = (int)(r / n2);
+    dst[((long long)k * g.py + j) * g.px + i] = (T)src[q];
+  }
+}
+
+template <typename T>
+__global__ void k_repack_out(Geo g, const T *__restrict__ src, int n1, int n2, int n3, double *__restrict__ dst) {
+  const long long tot = (long long)n1 * n2 * n3;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % n1);
+    const long long r = q / n1;
+    const int j = (int)(r % n2), k = (int)(r / n2);
+    dst[q] = (double)src[((long long)k * g.py + j) * g.px + i];
+  }
+}
+
+template <typename T>
+void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st) {
+  const int blocks = 148 * 8;
+  if (dir == 0) k_repack_in<T><<<blocks, 256, 0, st>>>(g, stage, n1, n2, n3, box);
+  else k_repack_out<T><<<blocks, 256, 0, st>>>(g, box, n1, n2, n3, stage);
+}
+template void launch_repack<double>(const Geo &, int, double *, double *, int, int, int, cudaStream_t);
+template void launch_repack<float>(const Geo &, int, double *, float *, int, int, int, cudaStream_t);
+
+}  // namespace blgpu

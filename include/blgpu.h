@@ -128,6 +128,23 @@ int blgpu_sync(blgpu_ctx *ctx);
 /* device bytes held by the context */
 long long blgpu_device_bytes(const blgpu_ctx *ctx);
 
+/* Per-phase device time of nsteps eager steps (compute_dt + time step),
+ * measured with CUDA events on the context stream -- the B200 counterpart of
+ * the reference's RK2 phase timers (time_integration.f90:149-155,194-236,
+ * 283-298).  ms[p] and kernels[p] accumulate over the steps for the phases
+ *   0 RHS+RK update  1 boundary conditions  2 divergence+DCT-x  3 DFT-z
+ *   4 Thomas-y  5 inverse DFT-z  6 inverse DCT-x  7 velocity correction
+ *   8 compute_dt  9 time bookkeeping
+ * nphase must be >= 10; kernels may be NULL. */
+int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels, int nphase);
+
+/* blgpu_advance(ctx, nsteps) bracketed by CUDA events on the context
+ * stream; *ms = device time of the nsteps (graph captured beforehand) */
+int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms);
+
+/* number of kernels this context has launched (graph replays included) */
+long long blgpu_kernel_launches(const blgpu_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,7 @@ def load():
         lib.blo_get_dt.restype = ctypes.c_double
         lib.blo_get_dt.argtypes = [ctypes.c_void_p]
         lib.blo_step.argtypes = [ctypes.c_void_p]
+        lib.blo_rk3_stage.argtypes = [ctypes.c_void_p, ctypes.c_int]
         for n in ("blo_rhs_u", "blo_rhs_v", "blo_rhs_w"):
             getattr(lib, n).argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
         lib.blo_apply_bc.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -176,6 +177,9 @@ class Oracle:
 
     def step(self):
         self.lib.blo_step(self.h)
+
+    def rk3_stage(self, stage):
+        self.lib.blo_rk3_stage(self.h, int(stage))
 
     def advance(self, nsteps):
         """main.f90:87-96 loop body: compute_dt then one time step"""

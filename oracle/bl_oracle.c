@@ -1206,3 +1206,21 @@ void blo_step(blo_t *o) {
     blo_apply_bc(o, 3);
   }
 }
+
+/* one RK3 substep (stage 1..3) of compute_time_step_RK3; stage 1 saves the
+ * state and the start time first (time_integration.f90:305-463) */
+static double stage_to = 0.0;
+void blo_rk3_stage(blo_t *o, int stage) {
+  if (stage == 1) {
+    stage_to = o->t;
+    save_state(o);
+    double a1[1] = {o->rk_coef[0][0]};
+    substep(o, 0, 1, a1, 1, stage_to + o->rk_t[1] * o->dt);
+  } else if (stage == 2) {
+    double a2[2] = {o->rk_coef[1][0], o->rk_coef[1][1]};
+    substep(o, 1, 2, a2, 2, stage_to + o->rk_t[2] * o->dt);
+  } else {
+    double a3[3] = {o->rk_coef[2][0], o->rk_coef[2][1], o->rk_coef[2][2]};
+    substep(o, 2, 3, a3, 3, stage_to + o->rk_t[3] * o->dt);
+  }
+}

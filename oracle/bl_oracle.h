@@ -52,6 +52,7 @@ double blo_compute_dt(blo_t *o);  /* time_integration.f90:528-591 */
 void blo_set_dt(blo_t *o, double dt);
 double blo_get_dt(const blo_t *o);
 void blo_step(blo_t *o);          /* one Euler/RK2/RK3 step */
+void blo_rk3_stage(blo_t *o, int stage); /* one RK3 substep, stage 1..3 */
 
 /* kernel-level entry points (equations.f90) -- host arrays, Fortran layout */
 void blo_rhs_u(blo_t *o, const double *U, const double *V, const double *W,

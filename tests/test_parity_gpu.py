@@ -91,12 +91,12 @@ def test_projection(gpu, grid):
 
 @pytest.mark.parametrize("rk", [3, 2, 1])
 def test_steps_small(gpu, rk):
-    c = noisy_laminar(60, 17, 15, seed=4, amp=1e-3, rk_scheme=rk)
+    """5 steps at a fixed dt (CFL < 0) on a grid with nzp = 13 (prime) and
+    N = 58 = 2*29 (radix-29 stage)."""
+    c = noisy_laminar(60, 17, 15, seed=4, amp=1e-3, rk_scheme=rk, cfl=-2e-3)
     s = cases.solver_for(c)
     o = oracle.oracle_for(c)
     for _ in range(5):
-        dt = s.compute_dt()
-        assert dt == o.compute_dt()
         s.time_step()
         o.step()
     U, V, W, P, t = s.download_state()
@@ -104,6 +104,21 @@ def test_steps_small(gpu, rk):
     assert t == pytest.approx(tr, rel=1e-15)
     assert rel(U, Ur) < REL10 and rel(V, Vr) < REL10 and rel(W, Wr) < REL10
     assert s.check_divergence() <= 1e-12
+    s.close()
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_compute_dt_exact(gpu, grid):
+    """compute_dt (time_integration.f90:528-591): the device max-reduction
+    gives the oracle's dt to the last bit, with the convective bound active."""
+    c = noisy_laminar(*grid, seed=8, amp=0.3)
+    c.U = np.asfortranarray(c.U + 2.0)
+    c.V = np.asfortranarray(c.V + 1.0)
+    c.W = np.asfortranarray(c.W + 1.0)
+    c.cfl = 0.37
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    assert s.compute_dt() == o.compute_dt()
     s.close()
 
 
