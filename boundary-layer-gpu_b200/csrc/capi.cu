@@ -229,7 +229,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   // transform tables
   {
     const int N = s.N, M = s.M;
-    std::vector<double> tw(2 * N), post(2 * N), zt(2 * M);
+    const int MH = s.MH;
+    std::vector<double> tw(2 * N), post(2 * N), zt(2 * (size_t)MH * MH);
     for (int t = 0; t < N; ++t) {
       double a = -2.0 * M_PI * (double)t / (double)N;
       tw[2 * t] = cos(a);
@@ -238,24 +239,26 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
       post[2 * t] = cos(b);
       post[2 * t + 1] = sin(b);
     }
-    for (int m = 0; m < M; ++m) {
-      double a = 2.0 * M_PI * (double)m / (double)M;
-      zt[2 * m] = cos(a);
-      zt[2 * m + 1] = sin(a);
-    }
+    // tz[m][n] = (cos, sin)(2 pi m n / M), m, n = 0..MH-1
+    for (int m = 0; m < MH; ++m)
+      for (int n = 0; n < MH; ++n) {
+        double a = 2.0 * M_PI * (double)(((long long)m * n) % M) / (double)M;
+        zt[2 * ((size_t)m * MH + n)] = cos(a);
+        zt[2 * ((size_t)m * MH + n) + 1] = sin(a);
+      }
     const size_t es2 = 2 * ctx->esz;
     TRY(dalloc(ctx, &ctx->tw, N * es2));
     TRY(dalloc(ctx, &ctx->post, N * es2));
-    TRY(dalloc(ctx, &ctx->ztab, M * es2));
+    TRY(dalloc(ctx, &ctx->ztab, (size_t)MH * MH * es2));
     if (ctx->fp64) {
       TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, tw.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
       TRY(check_cuda(ctx, cudaMemcpy(ctx->post, post.data(), N * es2, cudaMemcpyHostToDevice), "post"));
-      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, zt.data(), M * es2, cudaMemcpyHostToDevice), "ztab"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, zt.data(), (size_t)MH * MH * es2, cudaMemcpyHostToDevice), "ztab"));
     } else {
       std::vector<float> a(tw.begin(), tw.end()), b(post.begin(), post.end()), c(zt.begin(), zt.end());
       TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, a.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
       TRY(check_cuda(ctx, cudaMemcpy(ctx->post, b.data(), N * es2, cudaMemcpyHostToDevice), "post"));
-      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, c.data(), M * es2, cudaMemcpyHostToDevice), "ztab"));
+      TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, c.data(), (size_t)MH * MH * es2, cudaMemcpyHostToDevice), "ztab"));
     }
     std::vector<int> f = factorize(N);
     if (f.size() > 24) TRY(set_err(ctx, BLGPU_EINVAL, "DCT length %d has too many factors", N));

@@ -157,41 +157,35 @@ __device__ __forceinline__ void bf_loop(const T2<T> *in, T2<T> *out, int R, int 
   }
 }
 
-// L lines of length n in shared memory; returns the buffer holding the result
-template <typename T, bool INV>
-__device__ T2<T> *fft_lines(T2<T> *a, T2<T> *b, const FftPlan<T> &pl, int L, const T2<T> *tw) {
+// warp-level Stockham FFT of one complex line in shared memory (no block
+// barriers: each warp owns its line, stages are separated by __syncwarp)
+template <typename T, bool INV, int MAXR>
+__device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> &pl, const T2<T> *tw, int lane) {
   const int n = pl.n;
   int Ns = 1;
-  const int tid = threadIdx.x, nthr = blockDim.x;
   for (int s = 0; s < pl.nst; ++s) {
     const int R = pl.rad[s];
     const int nb = n / R;
-    const int total = nb * L;
     const int tsc = n / (Ns * R);
-    for (int w = tid; w < total; w += nthr) {
-      const int line = w / nb, jj = w - line * nb;
-      const T2<T> *in = a + line * n;
-      T2<T> *out = b + line * n;
+    for (int jj = lane; jj < nb; jj += 32) {
       const int jm = jj % Ns;
       const int tstep = jm * tsc;
       const int idxD = (jj - jm) * R + jm;
-      switch (R) {
-        case 2: bf2<T, INV>(in, out, jj, nb, tstep, idxD, Ns, tw); break;
-        case 3: bf3<T, INV>(in, out, jj, nb, tstep, idxD, Ns, tw); break;
-        case 4: bf4<T, INV>(in, out, jj, nb, tstep, idxD, Ns, tw); break;
-        case 5: bf_odd<5, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 7: bf_odd<7, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 11: bf_odd<11, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 13: bf_odd<13, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 17: bf_odd<17, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 19: bf_odd<19, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 23: bf_odd<23, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 29: bf_odd<29, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        case 31: bf_odd<31, T, INV>(in, out, jj, nb, tstep, idxD, Ns, n, tw); break;
-        default: bf_loop<T, INV>(in, out, R, jj, nb, tstep, idxD, Ns, n, tw); break;
-      }
+      if (R == 4) bf4<T, INV>(a, b, jj, nb, tstep, idxD, Ns, tw);
+      else if (R == 2) bf2<T, INV>(a, b, jj, nb, tstep, idxD, Ns, tw);
+      else if (R == 3) bf3<T, INV>(a, b, jj, nb, tstep, idxD, Ns, tw);
+      else if (MAXR >= 5 && R == 5) bf_odd<5, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 7 && R == 7) bf_odd<7, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 11 && R == 11) bf_odd<11, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 13 && R == 13) bf_odd<13, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 17 && R == 17) bf_odd<17, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 19 && R == 19) bf_odd<19, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 23 && R == 23) bf_odd<23, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 29 && R == 29) bf_odd<29, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else if (MAXR >= 31 && R == 31) bf_odd<31, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
+      else bf_loop<T, INV>(a, b, R, jj, nb, tstep, idxD, Ns, n, tw);
     }
-    __syncthreads();
+    __syncwarp();
     T2<T> *t = a;
     a = b;
     b = t;
@@ -201,267 +195,260 @@ __device__ T2<T> *fft_lines(T2<T> *a, T2<T> *b, const FftPlan<T> &pl, int L, con
 }
 
 // ---------------------------------------------------------------------------
-// divergence + DCT-II in x.  One CTA transforms 2L real lines (b, k').
-// R[q][kx], q = b*M + k', holds c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
+// divergence + DCT-II in x.  Each warp transforms one complex line holding
+// the real lines q and q+1 (q = b*M + k').  R[q][kx] receives
+// c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
 // ---------------------------------------------------------------------------
 template <typename T>
+__device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const T *__restrict__ V,
+                                    const T *__restrict__ W, long long c, int i, int j, int k) {
+  // projection.f90:42-44
+  return (__ldg(U + c) - __ldg(U + c - 1)) / (T)g.ax.F[i] + (__ldg(V + c) - __ldg(V + c - g.px)) / (T)g.ay.F[j] +
+         (__ldg(W + c) - __ldg(W + c - g.plane)) / (T)g.az.F[k];
+}
+
+template <typename T, int MAXR>
 __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
                                                  const T *__restrict__ V, const T *__restrict__ W,
-                                                 T *__restrict__ R, double *__restrict__ dc_sum, int L) {
+                                                 T *__restrict__ R, double *__restrict__ dc_sum) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = s.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
   T2<T> *post = tw + N;
-  T2<T> *bufA = post + N;
-  T2<T> *bufB = bufA + (size_t)L * N;
-  const int nlines = s.NM * s.M;
-  const int q0 = blockIdx.x * 2 * L;
+  T2<T> *bufA = post + N + (size_t)warp * 2 * N;
+  T2<T> *bufB = bufA + N;
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     tw[t] = pl.tw[t];
     post[t] = pl.post[t];
   }
-  // divergence (projection.f90:42-44) for i = 2..nx-1, Makhoul order
-  const int tot = L * N;
-  for (int w = threadIdx.x; w < tot; w += blockDim.x) {
-    const int l = w / N, ip = w - l * N;
-    T fv[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int q = q0 + 2 * l + h;
-      T f = 0;
-      if (q < nlines) {
-        const int b = q / s.M, kp = q - b * s.M;
-        const int i = ip + 2, j = b + 2, k = kp + 2;
-        const long long c = bidx(g, i, j, k);
-        f = (__ldg(U + c) - __ldg(U + c - 1)) / (T)g.ax.F[i] + (__ldg(V + c) - __ldg(V + c - g.px)) / (T)g.ay.F[j] +
-            (__ldg(W + c) - __ldg(W + c - g.plane)) / (T)g.az.F[k];
-      }
-      fv[h] = f;
+  __syncthreads();
+  const int nlines = s.NM * s.M;
+  const int q = (blockIdx.x * nw + warp) * 2;
+  if (q >= nlines) return;
+  const bool hb = q + 1 < nlines;
+  const int ba = q / s.M, ka = q - ba * s.M;
+  const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
+  const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
+  double sa = 0.0, sb = 0.0;
+#pragma unroll 2
+  for (int ip = lane; ip < N; ip += 32) {
+    const T fa = div_at<T>(g, U, V, W, ca + ip, ip + 2, ba + 2, ka + 2);
+    const T fb = hb ? div_at<T>(g, U, V, W, cb + ip, ip + 2, bb + 2, kb + 2) : (T)0;
+    if (dc_sum) {
+      sa += (double)fa;
+      sb += (double)fb;
     }
     const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
-    bufA[l * N + pos] = mk<T>(fv[0], fv[1]);
+    bufA[pos] = mk<T>(fa, fb);
   }
-  __syncthreads();
   if (dc_sum) {  // FP64 line sums for the zero wavenumber (mixed form)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int l = warp; l < L; l += nw) {
-      double sa = 0.0, sb = 0.0;
-      for (int t = lane; t < N; t += 32) {
-        T2<T> v = bufA[l * N + t];
-        sa += (double)v.x;
-        sb += (double)v.y;
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        sa += __shfl_xor_sync(0xffffffffu, sa, o);
-        sb += __shfl_xor_sync(0xffffffffu, sb, o);
-      }
-      if (lane == 0) {
-        const int q = q0 + 2 * l;
-        if (q < nlines) dc_sum[q] = sa;
-        if (q + 1 < nlines) dc_sum[q + 1] = sb;
-      }
+    for (int o = 16; o > 0; o >>= 1) {
+      sa += __shfl_xor_sync(0xffffffffu, sa, o);
+      sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    if (lane == 0) {
+      dc_sum[q] = sa;
+      if (hb) dc_sum[q + 1] = sb;
     }
   }
-  T2<T> *res = fft_lines<T, false>(bufA, bufB, pl, L, tw);
-  // untangle the two real lines and apply the DCT twiddle
-  for (int w = threadIdx.x; w < tot; w += blockDim.x) {
-    const int l = w / N, k = w - l * N;
-    const T2<T> z = res[l * N + k];
-    const T2<T> zr = res[l * N + (k == 0 ? 0 : N - k)];
-    // V_A = (Z_k + conj Z_{N-k})/2, V_B = (Z_k - conj Z_{N-k})/(2i)
-    const T2<T> va = mk<T>((T)0.5 * (z.x + zr.x), (T)0.5 * (z.y - zr.y));
-    const T2<T> vb = mk<T>((T)0.5 * (z.y + zr.y), (T)0.5 * (zr.x - z.x));
+  __syncwarp();
+  const T2<T> *res = fft_warp<T, false, MAXR>(bufA, bufB, pl, tw, lane);
+  T *ra = R + (long long)q * s.rx;
+  T *rb = ra + s.rx;
+  for (int k = lane; k < N; k += 32) {
+    const T2<T> z = res[k];
+    const T2<T> zr = res[k == 0 ? 0 : N - k];
+    // V_A = (Z_k + conj Z_{N-k})/2, V_B = (Z_k - conj Z_{N-k})/(2i), c = Re(e^{-i pi k/2N} V)
     const T2<T> p = post[k];
-    const int q = q0 + 2 * l;
-    if (q < nlines) R[(long long)q * s.rx + k] = p.x * va.x - p.y * va.y;
-    if (q + 1 < nlines) R[(long long)(q + 1) * s.rx + k] = p.x * vb.x - p.y * vb.y;
+    const T vax = (T)0.5 * (z.x + zr.x), vay = (T)0.5 * (z.y - zr.y);
+    const T vbx = (T)0.5 * (z.y + zr.y), vby = (T)0.5 * (zr.x - z.x);
+    ra[k] = p.x * vax - p.y * vay;
+    if (hb) rb[k] = p.x * vbx - p.y * vby;
   }
 }
 
 // ---------------------------------------------------------------------------
 // inverse DCT in x + box write of rhs_p (with the copies of
 // apply_periodic_z_pressure: rhs_p(nxg-1,:,:) = rhs_p(nxg-2,:,:) and
-// rhs_p(2:nxg-1,:,nzp+2) = rhs_p(2:nxg-1,:,2)).
+// rhs_p(2:nxg-1,:,nzp+2) = rhs_p(2:nxg-1,:,2)); one complex line per warp.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int MAXR>
 __global__ void __launch_bounds__(256) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
-                                              T *__restrict__ p, int L) {
+                                              T *__restrict__ p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = s.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
   T2<T> *post = tw + N;
-  T2<T> *bufA = post + N;
-  T2<T> *bufB = bufA + (size_t)L * N;
-  const int nlines = s.NM * s.M;
-  const int q0 = blockIdx.x * 2 * L;
+  T2<T> *bufA = post + N + (size_t)warp * 2 * N;
+  T2<T> *bufB = bufA + N;
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     tw[t] = pl.tw[t];
     post[t] = pl.post[t];
   }
   __syncthreads();
-  const int tot = L * N;
-  for (int w = threadIdx.x; w < tot; w += blockDim.x) {
-    const int l = w / N, k = w - l * N;
-    const int q = q0 + 2 * l;
-    T xa = 0, xan = 0, xb = 0, xbn = 0;
-    if (q < nlines) {
-      xa = R[(long long)q * s.rx + k];
-      xan = k ? R[(long long)q * s.rx + (N - k)] : (T)0;
-    }
-    if (q + 1 < nlines) {
-      xb = R[(long long)(q + 1) * s.rx + k];
-      xbn = k ? R[(long long)(q + 1) * s.rx + (N - k)] : (T)0;
-    }
+  const int nlines = s.NM * s.M;
+  const int q = (blockIdx.x * nw + warp) * 2;
+  if (q >= nlines) return;
+  const bool hb = q + 1 < nlines;
+  const T *ra = R + (long long)q * s.rx;
+  const T *rb = ra + s.rx;
+  for (int k = lane; k < N; k += 32) {
+    const T xa = ra[k], xan = k ? ra[N - k] : (T)0;
+    const T xb = hb ? rb[k] : (T)0, xbn = (hb && k) ? rb[N - k] : (T)0;
     // V_k = exp(+i pi k/2N) (X_k - i X_{N-k});  Z = V_A + i V_B
     const T2<T> e = mk<T>(post[k].x, -post[k].y);
     const T2<T> va = cmul<T>(e, mk<T>(xa, -xan));
     const T2<T> vb = cmul<T>(e, mk<T>(xb, -xbn));
-    bufA[l * N + k] = mk<T>(va.x - vb.y, va.y + vb.x);
+    bufA[k] = mk<T>(va.x - vb.y, va.y + vb.x);
   }
-  __syncthreads();
-  T2<T> *res = fft_lines<T, true>(bufA, bufB, pl, L, tw);
+  __syncwarp();
+  const T2<T> *res = fft_warp<T, true, MAXR>(bufA, bufB, pl, tw, lane);
   const T inv = (T)1 / (T)N;
-  for (int w = threadIdx.x; w < tot; w += blockDim.x) {
-    const int l = w / N, ip = w - l * N;
+  const int ba = q / s.M, ka = q - ba * s.M;
+  const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
+  const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
+  const long long zsh = (long long)s.M * g.plane;  // k = 2 -> k = nzp+2
+  for (int ip = lane; ip < N; ip += 32) {
     const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
-    const T2<T> z = res[l * N + pos];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int q = q0 + 2 * l + h;
-      if (q >= nlines) continue;
-      const int b = q / s.M, kp = q - b * s.M;
-      const T val = (h ? z.y : z.x) * inv;
-      const long long c = bidx(g, ip + 2, b + 2, kp + 2);
-      p[c] = val;
-      if (ip == N - 1) p[c + 1] = val;  // i = nxg-1 copy
-      if (kp == 0) {
-        const long long cz = c + (long long)s.M * g.plane;  // k = nzp+2
-        p[cz] = val;
-        if (ip == N - 1) p[cz + 1] = val;
+    const T2<T> z = res[pos];
+    const T va = z.x * inv, vb = z.y * inv;
+    p[ca + ip] = va;
+    if (ka == 0) p[ca + ip + zsh] = va;
+    if (hb) {
+      p[cb + ip] = vb;
+      if (kb == 0) p[cb + ip + zsh] = vb;
+    }
+    if (ip == N - 1) {  // i = nxg-1 copy
+      p[ca + N] = va;
+      if (ka == 0) p[ca + N + zsh] = va;
+      if (hb) {
+        p[cb + N] = vb;
+        if (kb == 0) p[cb + N + zsh] = vb;
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// real DFT in z over the half spectrum, direct summation.
-// forward:  C[b][kz][kx], kz = 0..MH-1, from R[b][k'][kx]
-// inverse:  R[b][k'][kx] = (1/M) sum over the Hermitian spectrum
-// ztab[m] = (cos(2 pi m/M), sin(2 pi m/M)), m = 0..M-1
-// One CTA: 32 kx lanes x 8 warps; a thread accumulates RPT outputs.
+// real DFT in z over the half spectrum, as a register-tiled product with the
+// table tz[m][n] = (cos, sin)(2 pi m n / M), m, n = 0..MH-1 (row pitch MH).
+// CTA: one row b, 64 kx (2 per lane), 8 warps x RK wavenumbers.
+// forward: Re C_kz = f_0 + sum_{k=1..H} (f_k + f_{M-k}) cos + [M even] f_{M/2} (-1)^kz
+//          Im C_kz = -sum_{k=1..H} (f_k - f_{M-k}) sin
+// inverse: f_p, f_{M-p} = (C_0 + 2 (P_p -+ Q_p) + [M even] C_{M/2} (-1)^p) / M,
+//          P_p = sum_{kz=1..H} Re C_kz cos, Q_p = sum Im C_kz sin
 // ---------------------------------------------------------------------------
-template <typename T, int RPT>
+template <typename T, int RK>
 __global__ void __launch_bounds__(256) k_dft_z_fwd(Spec s, const T *__restrict__ R, T2<T> *__restrict__ C,
-                                                   const T2<T> *__restrict__ ztab) {
+                                                   const T2<T> *__restrict__ tz) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = s.M, MH = s.MH;
-  T2<T> *tab = reinterpret_cast<T2<T> *>(smem_raw);
-  T *f = reinterpret_cast<T *>(tab + M);  // [M][32]
+  T2<T> *f = reinterpret_cast<T2<T> *>(smem_raw);  // [M][32] pairs of kx
+  const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.y;
-  const int kx = blockIdx.x * 32 + lane;
-  const bool ok = kx < s.N;
-  for (int t = threadIdx.x; t < M; t += blockDim.x) tab[t] = ztab[t];
-  for (int kp = warp; kp < M; kp += 8)
-    f[kp * 32 + lane] = ok ? R[((long long)b * M + kp) * s.rx + kx] : (T)0;
+  const int kx0 = blockIdx.x * 64 + 2 * lane;
+  const int nvalid = min(2, s.N - kx0);
+  for (int k = warp; k < M; k += 8) {
+    const T *row = R + ((long long)b * M + k) * s.rx + kx0;
+    T2<T> v = mk<T>(0, 0);
+    if (nvalid >= 1) v.x = row[0];
+    if (nvalid >= 2) v.y = row[1];
+    f[k * 32 + lane] = v;
+  }
   __syncthreads();
-  const int H = (M - 1) / 2;
+  const int kzb = blockIdx.z * 8 * RK + warp * RK;
+  if (kzb >= MH) return;
+  T re0[RK], re1[RK], im0[RK], im1[RK];
+  const T2<T> f0 = f[lane];
+#pragma unroll
+  for (int r = 0; r < RK; ++r) {
+    re0[r] = f0.x; re1[r] = f0.y; im0[r] = 0; im1[r] = 0;
+  }
+  int rows[RK];
+#pragma unroll
+  for (int r = 0; r < RK; ++r) rows[r] = min(kzb + r, MH - 1) * MH;
+  for (int k = 1; k <= H; ++k) {
+    const T2<T> fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
+    const T a0 = fk.x + fm.x, a1 = fk.y + fm.y, b0 = fk.x - fm.x, b1 = fk.y - fm.y;
+#pragma unroll
+    for (int r = 0; r < RK; ++r) {
+      const T2<T> t = __ldg(tz + rows[r] + k);
+      re0[r] += a0 * t.x; re1[r] += a1 * t.x;
+      im0[r] -= b0 * t.y; im1[r] -= b1 * t.y;
+    }
+  }
   const bool even = (M & 1) == 0;
-  for (int base = warp; base < MH; base += 8 * RPT) {
-    T re[RPT], im[RPT];
-    int kz[RPT], m[RPT];
+  const T2<T> fh = even ? f[(M / 2) * 32 + lane] : mk<T>(0, 0);
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      kz[r] = base + 8 * r;
-      re[r] = f[lane];
-      im[r] = 0;
-      m[r] = 0;
+  for (int r = 0; r < RK; ++r) {
+    const int kz = kzb + r;
+    if (kz >= MH) break;
+    T a = re0[r], c = re1[r];
+    if (even) {
+      a += (kz & 1) ? -fh.x : fh.x;
+      c += (kz & 1) ? -fh.y : fh.y;
     }
-    int inc[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) inc[r] = kz[r] < MH ? kz[r] : 0;  // idle slots stay at m = 0
-    for (int k = 1; k <= H; ++k) {
-      const T fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
-      const T a = fk + fm, bb = fk - fm;
-#pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        m[r] += inc[r];
-        if (m[r] >= M) m[r] -= M;
-        const T2<T> cs = tab[m[r]];
-        re[r] += a * cs.x;
-        im[r] -= bb * cs.y;
-      }
-    }
-    if (ok) {
-#pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        if (kz[r] >= MH) continue;
-        T rr = re[r];
-        if (even) rr += (kz[r] & 1) ? -f[(M / 2) * 32 + lane] : f[(M / 2) * 32 + lane];
-        C[((long long)b * MH + kz[r]) * s.rx + kx] = mk<T>(rr, im[r]);
-      }
-    }
+    T2<T> *out = C + ((long long)b * MH + kz) * s.rx + kx0;
+    if (nvalid >= 1) out[0] = mk<T>(a, im0[r]);
+    if (nvalid >= 2) out[1] = mk<T>(c, im1[r]);
   }
 }
 
-template <typename T, int RPT>
+template <typename T, int RK>
 __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restrict__ C, T *__restrict__ R,
-                                                   const T2<T> *__restrict__ ztab) {
+                                                   const T2<T> *__restrict__ tz) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int M = s.M, MH = s.MH;
-  T2<T> *tab = reinterpret_cast<T2<T> *>(smem_raw);
-  T2<T> *c = tab + M;  // [MH][32]
+  T2<T> *c = reinterpret_cast<T2<T> *>(smem_raw);  // [MH][64]: kx pairs interleaved
+  const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.y;
-  const int kx = blockIdx.x * 32 + lane;
-  const bool ok = kx < s.N;
-  for (int t = threadIdx.x; t < M; t += blockDim.x) tab[t] = ztab[t];
-  for (int kz = warp; kz < MH; kz += 8) c[kz * 32 + lane] = ok ? C[((long long)b * MH + kz) * s.rx + kx] : mk<T>(0, 0);
+  const int kx0 = blockIdx.x * 64 + 2 * lane;
+  const int nvalid = min(2, s.N - kx0);
+  for (int kz = warp; kz < MH; kz += 8) {
+    const T2<T> *row = C + ((long long)b * MH + kz) * s.rx + kx0;
+    c[kz * 64 + 2 * lane] = nvalid >= 1 ? row[0] : mk<T>(0, 0);
+    c[kz * 64 + 2 * lane + 1] = nvalid >= 2 ? row[1] : mk<T>(0, 0);
+  }
   __syncthreads();
-  const int H = (M - 1) / 2;  // conjugate pairs kz = 1..H
+  const int npairs = M / 2 + 1;
+  const int pb = blockIdx.z * 8 * RK + warp * RK;
+  if (pb >= npairs) return;
+  T P0[RK], P1[RK], Q0[RK], Q1[RK];
+  int rows[RK];
+#pragma unroll
+  for (int r = 0; r < RK; ++r) {
+    P0[r] = 0; P1[r] = 0; Q0[r] = 0; Q1[r] = 0;
+    rows[r] = min(pb + r, MH - 1) * MH;
+  }
+  for (int kz = 1; kz <= H; ++kz) {
+    const T2<T> v0 = c[kz * 64 + 2 * lane], v1 = c[kz * 64 + 2 * lane + 1];
+#pragma unroll
+    for (int r = 0; r < RK; ++r) {
+      const T2<T> t = __ldg(tz + rows[r] + kz);
+      P0[r] += v0.x * t.x; Q0[r] += v0.y * t.y;
+      P1[r] += v1.x * t.x; Q1[r] += v1.y * t.y;
+    }
+  }
   const bool even = (M & 1) == 0;
-  const T c0 = c[lane].x;
-  const T nyq = even ? c[(M / 2) * 32 + lane].x : (T)0;
+  const T2<T> c00 = c[2 * lane], c01 = c[2 * lane + 1];
+  const T2<T> n0 = even ? c[(M / 2) * 64 + 2 * lane] : mk<T>(0, 0);
+  const T2<T> n1 = even ? c[(M / 2) * 64 + 2 * lane + 1] : mk<T>(0, 0);
   const T invM = (T)1 / (T)M;
-  const int npairs = M / 2 + 1;  // p = 0..M/2 covers every output once with its partner M-p
-  for (int base = warp; base < npairs; base += 8 * RPT) {
-    T P[RPT], Q[RPT];
-    int pp[RPT], m[RPT];
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      pp[r] = base + 8 * r;
-      P[r] = 0;
-      Q[r] = 0;
-      m[r] = 0;
-    }
-    int inc[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) inc[r] = pp[r] < npairs ? pp[r] : 0;  // idle slots stay at m = 0
-    for (int kz = 1; kz <= H; ++kz) {
-      const T2<T> v = c[kz * 32 + lane];
-#pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        m[r] += inc[r];
-        if (m[r] >= M) m[r] -= M;
-        const T2<T> cs = tab[m[r]];
-        P[r] += v.x * cs.x;
-        Q[r] += v.y * cs.y;
-      }
-    }
-    if (ok) {
-#pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        const int p = pp[r];
-        if (p >= npairs) continue;
-        const T ny = (p & 1) ? -nyq : nyq;
-        const T lo = (c0 + (T)2 * (P[r] - Q[r]) + ny) * invM;
-        R[((long long)b * M + p) * s.rx + kx] = lo;
-        const int pm = M - p;
-        if (pm != p && pm < M) {
-          const T hi = (c0 + (T)2 * (P[r] + Q[r]) + ny) * invM;
-          R[((long long)b * M + pm) * s.rx + kx] = hi;
-        }
-      }
+  for (int r = 0; r < RK; ++r) {
+    const int pp = pb + r;
+    if (pp >= npairs) break;
+    const T y0 = (pp & 1) ? -n0.x : n0.x, y1 = (pp & 1) ? -n1.x : n1.x;
+    T *lo = R + ((long long)b * M + pp) * s.rx + kx0;
+    if (nvalid >= 1) lo[0] = (c00.x + (T)2 * (P0[r] - Q0[r]) + y0) * invM;
+    if (nvalid >= 2) lo[1] = (c01.x + (T)2 * (P1[r] - Q1[r]) + y1) * invM;
+    const int pm = M - pp;
+    if (pm != pp && pm < M) {
+      T *hi = R + ((long long)b * M + pm) * s.rx + kx0;
+      if (nvalid >= 1) hi[0] = (c00.x + (T)2 * (P0[r] + Q0[r]) + y0) * invM;
+      if (nvalid >= 2) hi[1] = (c01.x + (T)2 * (P1[r] + Q1[r]) + y1) * invM;
     }
   }
 }
@@ -562,52 +549,94 @@ __global__ void k_dc_rows(Spec s, const double *__restrict__ lines, double *__re
 // launchers
 // ---------------------------------------------------------------------------
 int dct_lines_per_cta(int n, int elem_bytes) {
-  const size_t line = (size_t)n * 2 * elem_bytes;   // one complex line
-  const size_t budget = 100 * 1024;                 // two CTAs per SM
-  size_t fixed = 2 * line;                          // twiddle + DCT tables
-  int L = (int)((budget > fixed ? budget - fixed : 0) / (2 * line));
-  if (L < 1) L = 1;
-  if (L > 8) L = 8;
-  return L;
+  // warps (complex lines) per CTA: two CTAs per SM within 113 KB each
+  const size_t line = (size_t)n * 2 * elem_bytes * 2;  // ping-pong buffers of one complex line
+  const size_t fixed = (size_t)n * 2 * elem_bytes * 2; // twiddle + DCT tables
+  const size_t budget = 113 * 1024;
+  int w = (int)((budget > fixed ? budget - fixed : 0) / line);
+  if (w < 1) w = 1;
+  if (w > 6) w = 6;
+  return w;
 }
 
-size_t dct_smem_bytes(int n, int elem_bytes, int lines) {
-  return (size_t)n * 2 * elem_bytes * (2 + 2 * (size_t)lines);
+size_t dct_smem_bytes(int n, int elem_bytes, int warps) {
+  return (size_t)n * 2 * elem_bytes * (2 + 2 * (size_t)warps);
+}
+
+// Register-resident odd butterflies raise the register count of the whole
+// kernel to that of the largest radix compiled in, so the transform kernels
+// are instantiated per largest radix class; radices above the class (and
+// primes above 31) take the shared-memory summation path.
+static int radix_class(const int *rad, int nst) {
+  int mx = 2;
+  for (int i = 0; i < nst; ++i)
+    if (rad[i] <= 31) mx = rad[i] > mx ? rad[i] : mx;
+  if (mx <= 7) return 7;
+  if (mx <= 13) return 13;
+  if (mx <= 19) return 19;
+  if (mx <= 29) return 29;
+  return 31;
+}
+
+template <typename T, int MAXR>
+static void launch_div_dct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W,
+                               T *R, double *dc_sum, int nw, size_t sm, int grid, cudaStream_t st) {
+  cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_div_dct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R, dc_sum);
+}
+
+template <typename T, int MAXR>
+static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, size_t sm,
+                            int grid, cudaStream_t st) {
+  cudaFuncSetAttribute(k_idct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_idct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p);
 }
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
                     double *dc_sum, cudaStream_t st) {
-  const int L = dct_lines_per_cta(s.N, sizeof(T));
-  const size_t sm = dct_smem_bytes(s.N, sizeof(T), L);
-  const int nlines = s.NM * s.M;
-  const int grid = (nlines + 2 * L - 1) / (2 * L);
-  cudaFuncSetAttribute(k_div_dct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_div_dct<T><<<grid, 256, sm, st>>>(g, s, pl, U, V, W, R, dc_sum, L);
+  const int nw = dct_lines_per_cta(s.N, sizeof(T));
+  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
+  const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
+  const int grid = (ncl + nw - 1) / nw;
+  switch (radix_class(pl.rad, pl.nst)) {
+    case 7: launch_div_dct_cls<T, 7>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+    case 13: launch_div_dct_cls<T, 13>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+    case 19: launch_div_dct_cls<T, 19>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+    case 29: launch_div_dct_cls<T, 29>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+    default: launch_div_dct_cls<T, 31>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+  }
 }
 
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, cudaStream_t st) {
-  const int L = dct_lines_per_cta(s.N, sizeof(T));
-  const size_t sm = dct_smem_bytes(s.N, sizeof(T), L);
-  const int nlines = s.NM * s.M;
-  const int grid = (nlines + 2 * L - 1) / (2 * L);
-  cudaFuncSetAttribute(k_idct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_idct<T><<<grid, 256, sm, st>>>(g, s, pl, R, p, L);
+  const int nw = dct_lines_per_cta(s.N, sizeof(T));
+  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
+  const int ncl = (s.NM * s.M + 1) / 2;
+  const int grid = (ncl + nw - 1) / nw;
+  switch (radix_class(pl.rad, pl.nst)) {
+    case 7: launch_idct_cls<T, 7>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 13: launch_idct_cls<T, 13>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 19: launch_idct_cls<T, 19>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 29: launch_idct_cls<T, 29>(g, s, pl, R, p, nw, sm, grid, st); break;
+    default: launch_idct_cls<T, 31>(g, s, pl, R, p, nw, sm, grid, st); break;
+  }
 }
 
 template <typename T>
-void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *ztab, int inverse, cudaStream_t st) {
-  constexpr int RPT = 8;
-  dim3 grid((s.N + 31) / 32, s.NM);
+void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inverse, cudaStream_t st) {
+  constexpr int RK = 12;
   if (!inverse) {
-    const size_t sm = (size_t)s.M * sizeof(T2<T>) + (size_t)s.M * 32 * sizeof(T);
-    cudaFuncSetAttribute(k_dft_z_fwd<T, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_dft_z_fwd<T, RPT><<<grid, 256, sm, st>>>(s, R, C, ztab);
+    dim3 grid((s.N + 63) / 64, s.NM, (s.MH + 8 * RK - 1) / (8 * RK));
+    const size_t sm = (size_t)s.M * 32 * sizeof(T2<T>);
+    cudaFuncSetAttribute(k_dft_z_fwd<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_dft_z_fwd<T, RK><<<grid, 256, sm, st>>>(s, R, C, tz);
   } else {
-    const size_t sm = (size_t)s.M * sizeof(T2<T>) + (size_t)s.MH * 32 * sizeof(T2<T>);
-    cudaFuncSetAttribute(k_dft_z_inv<T, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_dft_z_inv<T, RPT><<<grid, 256, sm, st>>>(s, C, const_cast<T *>(R), ztab);
+    const int npairs = s.M / 2 + 1;
+    dim3 grid((s.N + 63) / 64, s.NM, (npairs + 8 * RK - 1) / (8 * RK));
+    const size_t sm = (size_t)s.MH * 64 * sizeof(T2<T>);
+    cudaFuncSetAttribute(k_dft_z_inv<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_dft_z_inv<T, RK><<<grid, 256, sm, st>>>(s, C, const_cast<T *>(R), tz);
   }
 }
 
