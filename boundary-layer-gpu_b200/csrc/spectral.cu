@@ -230,17 +230,30 @@ __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, c
   const int ba = q / s.M, ka = q - ba * s.M;
   const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
   const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
+  // line B aliases line A when it does not exist, so every load is valid
+  const long long cbb = hb ? cb : ca;
+  const int jb = hb ? bb + 2 : ba + 2, kbb = hb ? kb + 2 : ka + 2;
   double sa = 0.0, sb = 0.0;
-#pragma unroll 2
-  for (int ip = lane; ip < N; ip += 32) {
-    const T fa = div_at<T>(g, U, V, W, ca + ip, ip + 2, ba + 2, ka + 2);
-    const T fb = hb ? div_at<T>(g, U, V, W, cb + ip, ip + 2, bb + 2, kb + 2) : (T)0;
-    if (dc_sum) {
-      sa += (double)fa;
-      sb += (double)fb;
+  // batches of 4 points per lane: all 48 loads issued before any use
+  for (int base = 0; base < N; base += 128) {
+    T fa[4], fb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ip = min(base + lane + 32 * u, N - 1);
+      fa[u] = div_at<T>(g, U, V, W, ca + ip, ip + 2, ba + 2, ka + 2);
+      fb[u] = div_at<T>(g, U, V, W, cbb + ip, ip + 2, jb, kbb);
     }
-    const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
-    bufA[pos] = mk<T>(fa, fb);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ip = base + lane + 32 * u;
+      if (ip < N) {
+        const T vb = hb ? fb[u] : (T)0;
+        sa += (double)fa[u];
+        sb += (double)vb;
+        const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
+        bufA[pos] = mk<T>(fa[u], vb);
+      }
+    }
   }
   if (dc_sum) {  // FP64 line sums for the zero wavenumber (mixed form)
     for (int o = 16; o > 0; o >>= 1) {
@@ -340,115 +353,148 @@ __global__ void __launch_bounds__(256) k_idct(Geo g, Spec s, FftPlan<T> pl, cons
 // inverse: f_p, f_{M-p} = (C_0 + 2 (P_p -+ Q_p) + [M even] C_{M/2} (-1)^p) / M,
 //          P_p = sum_{kz=1..H} Re C_kz cos, Q_p = sum Im C_kz sin
 // ---------------------------------------------------------------------------
+template <typename T> struct Vec16;  // 16-byte vector of T
+template <> struct Vec16<float> { typedef float4 type; static constexpr int n = 4; };
+template <> struct Vec16<double> { typedef double2 type; static constexpr int n = 2; };
+
+template <typename T> __device__ __forceinline__ T vget(const typename Vec16<T>::type &v, int e);
+template <> __device__ __forceinline__ float vget<float>(const float4 &v, int e) {
+  return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w;
+}
+template <> __device__ __forceinline__ double vget<double>(const double2 &v, int e) { return e == 0 ? v.x : v.y; }
+
 template <typename T, int RK>
 __global__ void __launch_bounds__(256) k_dft_z_fwd(Spec s, const T *__restrict__ R, T2<T> *__restrict__ C,
                                                    const T2<T> *__restrict__ tz) {
+  typedef typename Vec16<T>::type VT;
+  constexpr int KX = Vec16<T>::n;   // kx values per lane
+  constexpr int TW = 32 * KX;       // kx per CTA
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T2<T> *f = reinterpret_cast<T2<T> *>(smem_raw);  // [M][32] pairs of kx
+  VT *f = reinterpret_cast<VT *>(smem_raw);  // [M][32] vectors of KX kx
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.y;
-  const int kx0 = blockIdx.x * 64 + 2 * lane;
-  const int nvalid = min(2, s.N - kx0);
+  const int kx0 = blockIdx.x * TW + KX * lane;
+  const int nvalid = min(KX, s.N - kx0);
   for (int k = warp; k < M; k += 8) {
     const T *row = R + ((long long)b * M + k) * s.rx + kx0;
-    T2<T> v = mk<T>(0, 0);
-    if (nvalid >= 1) v.x = row[0];
-    if (nvalid >= 2) v.y = row[1];
-    f[k * 32 + lane] = v;
+    T v[KX];
+#pragma unroll
+    for (int e = 0; e < KX; ++e) v[e] = e < nvalid ? row[e] : (T)0;
+    f[k * 32 + lane] = *reinterpret_cast<VT *>(v);
   }
   __syncthreads();
   const int kzb = blockIdx.z * 8 * RK + warp * RK;
   if (kzb >= MH) return;
-  T re0[RK], re1[RK], im0[RK], im1[RK];
-  const T2<T> f0 = f[lane];
-#pragma unroll
-  for (int r = 0; r < RK; ++r) {
-    re0[r] = f0.x; re1[r] = f0.y; im0[r] = 0; im1[r] = 0;
-  }
+  T re[RK][KX], im[RK][KX];
+  const VT f0 = f[lane];
   int rows[RK];
 #pragma unroll
-  for (int r = 0; r < RK; ++r) rows[r] = min(kzb + r, MH - 1) * MH;
+  for (int r = 0; r < RK; ++r) {
+    rows[r] = min(kzb + r, MH - 1) * MH;
+#pragma unroll
+    for (int e = 0; e < KX; ++e) {
+      re[r][e] = vget<T>(f0, e);
+      im[r][e] = 0;
+    }
+  }
   for (int k = 1; k <= H; ++k) {
-    const T2<T> fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
-    const T a0 = fk.x + fm.x, a1 = fk.y + fm.y, b0 = fk.x - fm.x, b1 = fk.y - fm.y;
+    const VT fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
+    T a[KX], bb[KX];
+#pragma unroll
+    for (int e = 0; e < KX; ++e) {
+      a[e] = vget<T>(fk, e) + vget<T>(fm, e);
+      bb[e] = vget<T>(fk, e) - vget<T>(fm, e);
+    }
 #pragma unroll
     for (int r = 0; r < RK; ++r) {
       const T2<T> t = __ldg(tz + rows[r] + k);
-      re0[r] += a0 * t.x; re1[r] += a1 * t.x;
-      im0[r] -= b0 * t.y; im1[r] -= b1 * t.y;
+#pragma unroll
+      for (int e = 0; e < KX; ++e) {
+        re[r][e] += a[e] * t.x;
+        im[r][e] -= bb[e] * t.y;
+      }
     }
   }
   const bool even = (M & 1) == 0;
-  const T2<T> fh = even ? f[(M / 2) * 32 + lane] : mk<T>(0, 0);
+  const VT fh = f[(even ? M / 2 : 0) * 32 + lane];
 #pragma unroll
   for (int r = 0; r < RK; ++r) {
     const int kz = kzb + r;
     if (kz >= MH) break;
-    T a = re0[r], c = re1[r];
-    if (even) {
-      a += (kz & 1) ? -fh.x : fh.x;
-      c += (kz & 1) ? -fh.y : fh.y;
-    }
     T2<T> *out = C + ((long long)b * MH + kz) * s.rx + kx0;
-    if (nvalid >= 1) out[0] = mk<T>(a, im0[r]);
-    if (nvalid >= 2) out[1] = mk<T>(c, im1[r]);
+#pragma unroll
+    for (int e = 0; e < KX; ++e) {
+      T a = re[r][e];
+      if (even) a += (kz & 1) ? -vget<T>(fh, e) : vget<T>(fh, e);
+      if (e < nvalid) out[e] = mk<T>(a, im[r][e]);
+    }
   }
 }
 
 template <typename T, int RK>
 __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restrict__ C, T *__restrict__ R,
                                                    const T2<T> *__restrict__ tz) {
+  constexpr int KX = Vec16<T>::n;
+  constexpr int TW = 32 * KX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T2<T> *c = reinterpret_cast<T2<T> *>(smem_raw);  // [MH][64]: kx pairs interleaved
+  T2<T> *c = reinterpret_cast<T2<T> *>(smem_raw);  // [MH][TW]
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.y;
-  const int kx0 = blockIdx.x * 64 + 2 * lane;
-  const int nvalid = min(2, s.N - kx0);
+  const int kx0 = blockIdx.x * TW + KX * lane;
+  const int nvalid = min(KX, s.N - kx0);
   for (int kz = warp; kz < MH; kz += 8) {
     const T2<T> *row = C + ((long long)b * MH + kz) * s.rx + kx0;
-    c[kz * 64 + 2 * lane] = nvalid >= 1 ? row[0] : mk<T>(0, 0);
-    c[kz * 64 + 2 * lane + 1] = nvalid >= 2 ? row[1] : mk<T>(0, 0);
+#pragma unroll
+    for (int e = 0; e < KX; ++e) c[kz * TW + KX * lane + e] = e < nvalid ? row[e] : mk<T>(0, 0);
   }
   __syncthreads();
   const int npairs = M / 2 + 1;
   const int pb = blockIdx.z * 8 * RK + warp * RK;
   if (pb >= npairs) return;
-  T P0[RK], P1[RK], Q0[RK], Q1[RK];
+  T P[RK][KX], Q[RK][KX];
   int rows[RK];
 #pragma unroll
   for (int r = 0; r < RK; ++r) {
-    P0[r] = 0; P1[r] = 0; Q0[r] = 0; Q1[r] = 0;
     rows[r] = min(pb + r, MH - 1) * MH;
+#pragma unroll
+    for (int e = 0; e < KX; ++e) {
+      P[r][e] = 0;
+      Q[r][e] = 0;
+    }
   }
   for (int kz = 1; kz <= H; ++kz) {
-    const T2<T> v0 = c[kz * 64 + 2 * lane], v1 = c[kz * 64 + 2 * lane + 1];
+    T2<T> v[KX];
+#pragma unroll
+    for (int e = 0; e < KX; ++e) v[e] = c[kz * TW + KX * lane + e];
 #pragma unroll
     for (int r = 0; r < RK; ++r) {
       const T2<T> t = __ldg(tz + rows[r] + kz);
-      P0[r] += v0.x * t.x; Q0[r] += v0.y * t.y;
-      P1[r] += v1.x * t.x; Q1[r] += v1.y * t.y;
+#pragma unroll
+      for (int e = 0; e < KX; ++e) {
+        P[r][e] += v[e].x * t.x;
+        Q[r][e] += v[e].y * t.y;
+      }
     }
   }
   const bool even = (M & 1) == 0;
-  const T2<T> c00 = c[2 * lane], c01 = c[2 * lane + 1];
-  const T2<T> n0 = even ? c[(M / 2) * 64 + 2 * lane] : mk<T>(0, 0);
-  const T2<T> n1 = even ? c[(M / 2) * 64 + 2 * lane + 1] : mk<T>(0, 0);
   const T invM = (T)1 / (T)M;
 #pragma unroll
   for (int r = 0; r < RK; ++r) {
     const int pp = pb + r;
     if (pp >= npairs) break;
-    const T y0 = (pp & 1) ? -n0.x : n0.x, y1 = (pp & 1) ? -n1.x : n1.x;
     T *lo = R + ((long long)b * M + pp) * s.rx + kx0;
-    if (nvalid >= 1) lo[0] = (c00.x + (T)2 * (P0[r] - Q0[r]) + y0) * invM;
-    if (nvalid >= 2) lo[1] = (c01.x + (T)2 * (P1[r] - Q1[r]) + y1) * invM;
     const int pm = M - pp;
-    if (pm != pp && pm < M) {
-      T *hi = R + ((long long)b * M + pm) * s.rx + kx0;
-      if (nvalid >= 1) hi[0] = (c00.x + (T)2 * (P0[r] + Q0[r]) + y0) * invM;
-      if (nvalid >= 2) hi[1] = (c01.x + (T)2 * (P1[r] + Q1[r]) + y1) * invM;
+    T *hi = R + ((long long)b * M + pm) * s.rx + kx0;
+#pragma unroll
+    for (int e = 0; e < KX; ++e) {
+      if (e >= nvalid) continue;
+      const T c0 = c[KX * lane + e].x;
+      const T ny = even ? c[(M / 2) * TW + KX * lane + e].x : (T)0;
+      const T y = (pp & 1) ? -ny : ny;
+      lo[e] = (c0 + (T)2 * (P[r][e] - Q[r][e]) + y) * invM;
+      if (pm != pp && pm < M) hi[e] = (c0 + (T)2 * (P[r][e] + Q[r][e]) + y) * invM;
     }
   }
 }
@@ -505,34 +551,79 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
     for (int b = 0; b < NM; ++b) C[base + b * rs] = mk<T>(0, 0);
     return;
   }
+  // forward sweep in batches of PF rows: the next batch is loaded while the
+  // current one is eliminated, so PF loads per thread are always in flight
+  constexpr int PF = 8;
   double dprev = 1.0, gx = 0.0, gy = 0.0;
-  for (int b = 0; b < NM; ++b) {
-    const long long a = base + b * rs;
-    const T2<T> r = C[a];
-    double rx = (double)r.x, ry = (double)r.y;
-    double d = (dd[b] + kk) + kzv;
-    if (zero && b == 0) d = 3.0 / 2.0 * d;
-    if (b > 0) {
-      const double w = dl[b] / dprev;
-      d = d - w * du[b - 1];
-      rx = rx - w * gx;
-      ry = ry - w * gy;
+  T2<T> cur[PF], nxt[PF];
+#pragma unroll
+  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? C[base + u * rs] : mk<T>(0, 0);
+  for (int b0 = 0; b0 < NM; b0 += PF) {
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int bn = b0 + PF + u;
+      nxt[u] = bn < NM ? C[base + bn * rs] : mk<T>(0, 0);
     }
-    dprev = d;
-    gx = rx;
-    gy = ry;
-    C[a] = mk<T>((T)rx, (T)ry);
-    piv[a] = 1.0 / d;
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int b = b0 + u;
+      if (b < NM) {
+        const long long a = base + b * rs;
+        double rx = (double)cur[u].x, ry = (double)cur[u].y;
+        double d = (dd[b] + kk) + kzv;
+        if (zero && b == 0) d = 3.0 / 2.0 * d;
+        if (b > 0) {
+          const double w = dl[b] / dprev;
+          d = d - w * du[b - 1];
+          rx = rx - w * gx;
+          ry = ry - w * gy;
+        }
+        dprev = d;
+        gx = rx;
+        gy = ry;
+        C[a] = mk<T>((T)rx, (T)ry);
+        piv[a] = 1.0 / d;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) cur[u] = nxt[u];
   }
-  double xx = gx * piv[base + (NM - 1) * rs], xy = gy * piv[base + (NM - 1) * rs];
-  C[base + (NM - 1) * rs] = mk<T>((T)xx, (T)xy);
-  for (int b = NM - 2; b >= 0; --b) {
-    const long long a = base + b * rs;
-    const T2<T> gv = C[a];
-    const double pv = piv[a];
-    xx = ((double)gv.x - du[b] * xx) * pv;
-    xy = ((double)gv.y - du[b] * xy) * pv;
-    C[a] = mk<T>((T)xx, (T)xy);
+  // backward sweep, batches of PF rows from the top down
+  double xx = 0.0, xy = 0.0;
+  double pv[PF], pn[PF];
+  const int top = NM - 1;
+#pragma unroll
+  for (int u = 0; u < PF; ++u) {
+    const int b = top - u;
+    cur[u] = b >= 0 ? C[base + b * rs] : mk<T>(0, 0);
+    pv[u] = b >= 0 ? piv[base + b * rs] : 0.0;
+  }
+  for (int b0 = top; b0 >= 0; b0 -= PF) {
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int bn = b0 - PF - u;
+      nxt[u] = bn >= 0 ? C[base + bn * rs] : mk<T>(0, 0);
+      pn[u] = bn >= 0 ? piv[base + bn * rs] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int b = b0 - u;
+      if (b >= 0) {
+        if (b == top) {
+          xx = (double)cur[u].x * pv[u];
+          xy = (double)cur[u].y * pv[u];
+        } else {
+          xx = ((double)cur[u].x - du[b] * xx) * pv[u];
+          xy = ((double)cur[u].y - du[b] * xy) * pv[u];
+        }
+        C[base + b * rs] = mk<T>((T)xx, (T)xy);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      cur[u] = nxt[u];
+      pv[u] = pn[u];
+    }
   }
 }
 
@@ -625,16 +716,17 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
 
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inverse, cudaStream_t st) {
-  constexpr int RK = 12;
+  constexpr int RK = 8;
+  constexpr int TW = 32 * Vec16<T>::n;
   if (!inverse) {
-    dim3 grid((s.N + 63) / 64, s.NM, (s.MH + 8 * RK - 1) / (8 * RK));
-    const size_t sm = (size_t)s.M * 32 * sizeof(T2<T>);
+    dim3 grid((s.N + TW - 1) / TW, s.NM, (s.MH + 8 * RK - 1) / (8 * RK));
+    const size_t sm = (size_t)s.M * TW * sizeof(T);
     cudaFuncSetAttribute(k_dft_z_fwd<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_dft_z_fwd<T, RK><<<grid, 256, sm, st>>>(s, R, C, tz);
   } else {
     const int npairs = s.M / 2 + 1;
-    dim3 grid((s.N + 63) / 64, s.NM, (npairs + 8 * RK - 1) / (8 * RK));
-    const size_t sm = (size_t)s.MH * 64 * sizeof(T2<T>);
+    dim3 grid((s.N + TW - 1) / TW, s.NM, (npairs + 8 * RK - 1) / (8 * RK));
+    const size_t sm = (size_t)s.MH * TW * sizeof(T2<T>);
     cudaFuncSetAttribute(k_dft_z_inv<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_dft_z_inv<T, RK><<<grid, 256, sm, st>>>(s, C, const_cast<T *>(R), tz);
   }

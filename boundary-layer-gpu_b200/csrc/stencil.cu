@@ -191,6 +191,126 @@ __global__ void __launch_bounds__(256) k_rhs_rk(Geo g, MetT<T> m, const T *__res
 }
 
 // ---------------------------------------------------------------------------
+// DNS form of the same kernel: each thread owns one (i,j) column and marches
+// up a chunk of k-planes with a register window over k-1, k, k+1, so a plane
+// step loads 17 field values instead of 27; the x and y metric values are
+// loaded once per thread and the z ones once per plane.  Expressions are
+// those of rhs_*_at above, term for term.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_rhs_rk_dns(Geo g, MetT<T> m, const T *__restrict__ U,
+                                                    const T *__restrict__ V, const T *__restrict__ W,
+                                                    const T *__restrict__ Uo, const T *__restrict__ Vo,
+                                                    const T *__restrict__ Wo, T *__restrict__ F1u,
+                                                    T *__restrict__ F1v, T *__restrict__ F1w, T *__restrict__ Un,
+                                                    T *__restrict__ Vn, T *__restrict__ Wn,
+                                                    const Scalars *__restrict__ sc, double c1, double c2,
+                                                    int kchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (i > g.nx || j > g.ny) return;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  if (k0 > k1) return;
+  const long long px = g.px, pl = g.plane;
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  const T cdt1 = (T)(dt * c1);
+  const T tdt = (T)dt, tc1 = (T)c1, tc2 = (T)c2;
+  const bool du = (i <= g.nx - 1), dv = (j <= g.ny - 1);
+  const bool zu = (i == g.nx - 1), zvw = (i == g.nx);
+  const T h = (T)0.5;
+  // per-thread metrics (x: i, y: j)
+  const T xC = m.xC[i], xrC = m.xrC[i], xF = m.xF[i], xrF = m.xrF[i], xrFp = m.xrF[i + 1], xrCm = m.xrC[i - 1];
+  const T yF = m.yF[j], yrF = m.yrF[j], yC = m.yC[j], yrC = m.yrC[j], yCm = m.yC[j - 1], yrCm = m.yrC[j - 1];
+  const T yrFp = m.yrF[j + 1], w0 = m.w0[j], w1 = m.w1[j], w0m = m.w0[j - 1], w1m = m.w1[j - 1];
+  const T nu = m.nu, dpdx = m.dpdx, dpdz = m.dpdz;
+  long long c = bidx(g, i, j, k0);
+  // window at k0
+  T uc = __ldg(U + c), ue = __ldg(U + c + 1), uw = __ldg(U + c - 1), un = __ldg(U + c + px), us = __ldg(U + c - px);
+  T ut = __ldg(U + c + pl), ub = __ldg(U + c - pl), unw = __ldg(U + c - 1 + px), utw = __ldg(U + c - 1 + pl);
+  T vc = __ldg(V + c), ve = __ldg(V + c + 1), vw = __ldg(V + c - 1), vn = __ldg(V + c + px), vs = __ldg(V + c - px);
+  T vt = __ldg(V + c + pl), vb = __ldg(V + c - pl), vse = __ldg(V + c + 1 - px), vst = __ldg(V + c - px + pl);
+  T wc = __ldg(W + c), we = __ldg(W + c + 1), ww = __ldg(W + c - 1), wn = __ldg(W + c + px), ws = __ldg(W + c - px);
+  T wt = __ldg(W + c + pl), wb = __ldg(W + c - pl), web = __ldg(W + c + 1 - pl), wnb = __ldg(W + c + px - pl);
+  for (int k = k0;; ++k) {
+    const T zF = m.zF[k], zrF = m.zrF[k], zC = m.zC[k], zrC = m.zrC[k], zrCm = m.zrC[k - 1], zrFp = m.zrF[k + 1];
+    if (du) {
+      T f = 0;
+      if (!zu) {
+        const T a = h * (uc + ue), b = h * (uw + uc);
+        T r = -qdiv(a * a - b * b, xC, xrC);
+        const T t1 = (w0 * uc + w1 * un) * h * (vc + ve);
+        const T t2 = (w0m * us + w1m * uc) * h * (vs + vse);
+        r = r - qdiv(t1 - t2, yF, yrF);
+        const T t3 = h * (uc + ut) * h * (wc + we);
+        const T t4 = h * (ub + uc) * h * (wb + web);
+        r = r - qdiv(t3 - t4, zF, zrF);
+        const T vx = qdiv(xrFp * (ue - uc) - xrF * (uc - uw), xC, xrC);
+        const T vy = qdiv(qdiv(un - uc, yC, yrC) - qdiv(uc - us, yCm, yrCm), yF, yrF);
+        const T vz = qdiv(zrC * (ut - uc) - zrCm * (uc - ub), zF, zrF);
+        f = r + dpdx + nu * (vx + vy + vz);
+      }
+      if (MODE == 0) F1u[c] = f;
+      else if (MODE == 1) { F1u[c] = f; Un[c] = Uo[c] + cdt1 * f; }
+      else Un[c] = Uo[c] + tdt * (tc1 * F1u[c] + tc2 * f);
+    }
+    if (dv) {
+      T f = 0;
+      if (!zvw) {
+        const T a = h * (vc + vn), b = h * (vs + vc);
+        T r = -qdiv(a * a - b * b, yC, yrC);
+        const T t1 = (w0 * uc + w1 * un) * h * (vc + ve);
+        const T t2 = (w0 * uw + w1 * unw) * h * (vw + vc);
+        r = r - qdiv(t1 - t2, xF, xrF);
+        const T t3 = h * (vc + vt) * (w0 * wc + w1 * wn);
+        const T t4 = h * (vb + vc) * (w0 * wb + w1 * wnb);
+        r = r - qdiv(t3 - t4, zF, zrF);
+        const T vx = qdiv(xrC * (ve - vc) - xrCm * (vc - vw), xF, xrF);
+        const T vy = qdiv(yrFp * (vn - vc) - yrF * (vc - vs), yC, yrC);
+        const T vz = qdiv(zrC * (vt - vc) - zrCm * (vc - vb), zF, zrF);
+        f = r + nu * (vx + vy + vz);
+      }
+      if (MODE == 0) F1v[c] = f;
+      else if (MODE == 1) { F1v[c] = f; Vn[c] = Vo[c] + cdt1 * f; }
+      else Vn[c] = Vo[c] + tdt * (tc1 * F1v[c] + tc2 * f);
+    }
+    if (k <= g.nz - 1) {
+      T f = 0;
+      if (!zvw) {
+        const T a = h * (wc + wt), b = h * (wb + wc);
+        T r = -qdiv(a * a - b * b, zC, zrC);
+        const T t1 = h * (uc + ut) * h * (wc + we);
+        const T t2 = h * (uw + utw) * h * (ww + wc);
+        r = r - qdiv(t1 - t2, xF, xrF);
+        const T t3 = h * (vc + vt) * (w0 * wc + w1 * wn);
+        const T t4 = h * (vs + vst) * (w0m * ws + w1m * wc);
+        r = r - qdiv(t3 - t4, yF, yrF);
+        const T vx = qdiv(xrC * (we - wc) - xrCm * (wc - ww), xF, xrF);
+        const T vy = qdiv(qdiv(wn - wc, yC, yrC) - qdiv(wc - ws, yCm, yrCm), yF, yrF);
+        const T vz = qdiv(zrFp * (wt - wc) - zrF * (wc - wb), zC, zrC);
+        f = r + dpdz + nu * (vx + vy + vz);
+      }
+      if (MODE == 0) F1w[c] = f;
+      else if (MODE == 1) { F1w[c] = f; Wn[c] = Wo[c] + cdt1 * f; }
+      else Wn[c] = Wo[c] + tdt * (tc1 * F1w[c] + tc2 * f);
+    }
+    if (k == k1) break;
+    // slide the window to k+1
+    c += pl;
+    ub = uc; uc = ut; uw = utw;
+    vb = vc; vc = vt; vs = vst;
+    wb = wc; wc = wt; web = we; wnb = wn;
+    ut = __ldg(U + c + pl); utw = __ldg(U + c - 1 + pl);
+    ue = __ldg(U + c + 1); un = __ldg(U + c + px); us = __ldg(U + c - px); unw = __ldg(U + c - 1 + px);
+    vt = __ldg(V + c + pl); vst = __ldg(V + c - px + pl);
+    ve = __ldg(V + c + 1); vw = __ldg(V + c - 1); vn = __ldg(V + c + px); vse = __ldg(V + c + 1 - px);
+    wt = __ldg(W + c + pl);
+    we = __ldg(W + c + 1); ww = __ldg(W + c - 1); wn = __ldg(W + c + px); ws = __ldg(W + c - px);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // project_velocity (projection.f90:359-384) + pressure save at rk_step 1
 // (projection.f90:75-78, P(2:nxg-1,2:nyg-1,2:nzg-1) = rhs_p/(dt*rk2_coef(1,1))).
 // p holds rhs_p in the box layout (i=2..nx, j=2..ny, k=2..nz valid).
@@ -480,12 +600,17 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
   k_rhs_rk<T, M, L><<<grid, block, 0, st>>>(g, m, U, V, W, nut, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, \
                                             c2, kchunk)
   if (!les) {
+    const int kc = 32;
+    dim3 gd = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc);
+#define BLGPU_DNS_CASE(M)                                                                                     \
+  k_rhs_rk_dns<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc)
     switch (mode) {
-      case 0: BLGPU_RHS_CASE(0, false); break;
-      case 1: BLGPU_RHS_CASE(1, false); break;
-      case 2: BLGPU_RHS_CASE(2, false); break;
-      default: BLGPU_RHS_CASE(3, false); break;
+      case 0: BLGPU_DNS_CASE(0); break;
+      case 1: BLGPU_DNS_CASE(1); break;
+      case 2: BLGPU_DNS_CASE(2); break;
+      default: BLGPU_DNS_CASE(3); break;
     }
+#undef BLGPU_DNS_CASE
   } else {
     switch (mode) {
       case 0: BLGPU_RHS_CASE(0, true); break;
@@ -500,7 +625,7 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 template <typename T>
 void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
                     const Scalars *sc, int save_p, cudaStream_t st) {
-  const int kchunk = 8;
+  const int kchunk = 1;  // one point per thread: loads of different points overlap across warps
   dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk), block(32, 8);
   k_project<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p, kchunk);
   if (save_p) {
