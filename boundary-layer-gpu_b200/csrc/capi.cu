@@ -194,7 +194,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   ctx->cfg = *cfg;
   ctx->nx = cfg->nx; ctx->ny = cfg->ny; ctx->nz = cfg->nz;
   ctx->nxg = cfg->nx + 1; ctx->nyg = cfg->ny + 1; ctx->nzg = cfg->nz + 1;
-  ctx->px = (ctx->nxg + 31) / 32 * 32;
+  ctx->px = (ctx->nxg + 8 + 31) / 32 * 32;  // room for 16-byte vectors past i = nxg
   ctx->py = ctx->nyg;
   ctx->plane = (long long)ctx->px * ctx->py;
   ctx->boxn = ctx->plane * ctx->nzg;
@@ -529,28 +529,7 @@ int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const doubl
 
 }  // extern "C"
 
-// ---- host <-> box layout ----
-template <typename T>
-static void to_box(const blgpu_ctx *c, const double *a, int n1, int n2, int n3, std::vector<T> &box) {
-  box.assign((size_t)c->boxn, (T)0);
-  for (int k = 0; k < n3; ++k)
-    for (int j = 0; j < n2; ++j) {
-      const double *src = a + ((size_t)k * n2 + j) * n1;
-      T *dst = box.data() + ((size_t)k * c->py + j) * c->px;
-      for (int i = 0; i < n1; ++i) dst[i] = (T)src[i];
-    }
-}
-
-template <typename T>
-static void from_box(const blgpu_ctx *c, const std::vector<T> &box, int n1, int n2, int n3, double *a) {
-  for (int k = 0; k < n3; ++k)
-    for (int j = 0; j < n2; ++j) {
-      double *dst = a + ((size_t)k * n2 + j) * n1;
-      const T *src = box.data() + ((size_t)k * c->py + j) * c->px;
-      for (int i = 0; i < n1; ++i) dst[i] = (double)src[i];
-    }
-}
-
+// ---- host <-> box layout (staged through device memory, repacked on the GPU) ----
 static int upload_field(blgpu_ctx *ctx, void *dst, const double *a, int n1, int n2, int n3) {
   CK(cudaMemcpyAsync(ctx->stage, a, (size_t)n1 * n2 * n3 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
   if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 0, ctx->stage, (double *)dst, n1, n2, n3, ctx->st);

@@ -3,9 +3,11 @@
 // Every 3D field (U, V, W, P, rhs_p and the RK stage F1) lives in one padded
 // "box" layout in HBM: k-planes of py rows of px elements, i fastest, with
 // the reference's 1-based Fortran indices (i,j,k) mapped to
-//     ((k-1)*py + (j-1))*px + (i-1).
-// px is nxg rounded up to 32 elements, so every row starts on a 256-byte
-// (FP64) or 128-byte (FP32) boundary and the TMA/vector rules hold; py = nyg.
+//     ((k-1)*py + (j-1))*px + (i+2).
+// px is nxg+8 rounded up to 32 elements, so every row starts on a 256-byte
+// (FP64) or 128-byte (FP32) boundary; the shift by 2 puts the first interior
+// point i = 2 on a 16-byte boundary, so 16-byte vector loads of a row
+// segment i = 2+4q .. 5+4q (FP32) or 2+2q .. 3+2q (FP64) are aligned; py = nyg.
 // The reference's arrays U(nx,nyg,nzg), V(nxg,ny,nzg), W(nxg,nyg,nz) and
 // P(nxg,nyg,nzg) (global.f90:86-88) are all sub-boxes of this one shape.
 #pragma once
@@ -38,7 +40,7 @@ struct Geo {
 };
 
 __host__ __device__ inline long long bidx(const Geo &g, int i, int j, int k) {
-  return ((long long)(k - 1) * g.py + (j - 1)) * (long long)g.px + (i - 1);
+  return ((long long)(k - 1) * g.py + (j - 1)) * (long long)g.px + (i + 2);
 }
 
 // Device-resident scalars of the running time step.  Kernels read dt and t

@@ -199,12 +199,17 @@ __device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> 
 // the real lines q and q+1 (q = b*M + k').  R[q][kx] receives
 // c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
 // ---------------------------------------------------------------------------
+// FP64: the source's divisions; FP32: products with the reciprocal spacing
+__device__ __forceinline__ double dq(double a, double F, double) { return a / F; }
+__device__ __forceinline__ float dq(float a, double, double rF) { return a * (float)rF; }
+
 template <typename T>
 __device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const T *__restrict__ V,
                                     const T *__restrict__ W, long long c, int i, int j, int k) {
   // projection.f90:42-44
-  return (__ldg(U + c) - __ldg(U + c - 1)) / (T)g.ax.F[i] + (__ldg(V + c) - __ldg(V + c - g.px)) / (T)g.ay.F[j] +
-         (__ldg(W + c) - __ldg(W + c - g.plane)) / (T)g.az.F[k];
+  return dq(__ldg(U + c) - __ldg(U + c - 1), g.ax.F[i], g.ax.rF[i]) +
+         dq(__ldg(V + c) - __ldg(V + c - g.px), g.ay.F[j], g.ay.rF[j]) +
+         dq(__ldg(W + c) - __ldg(W + c - g.plane), g.az.F[k], g.az.rF[k]);
 }
 
 template <typename T, int MAXR>
@@ -398,7 +403,16 @@ __global__ void __launch_bounds__(256) k_dft_z_fwd(Spec s, const T *__restrict__
       im[r][e] = 0;
     }
   }
+  T2<T> tn[RK];  // table values of the next k, loaded one iteration ahead
+#pragma unroll
+  for (int r = 0; r < RK; ++r) tn[r] = __ldg(tz + rows[r] + 1);
   for (int k = 1; k <= H; ++k) {
+    T2<T> t[RK];
+#pragma unroll
+    for (int r = 0; r < RK; ++r) {
+      t[r] = tn[r];
+      tn[r] = __ldg(tz + rows[r] + min(k + 1, H));
+    }
     const VT fk = f[k * 32 + lane], fm = f[(M - k) * 32 + lane];
     T a[KX], bb[KX];
 #pragma unroll
@@ -408,11 +422,10 @@ __global__ void __launch_bounds__(256) k_dft_z_fwd(Spec s, const T *__restrict__
     }
 #pragma unroll
     for (int r = 0; r < RK; ++r) {
-      const T2<T> t = __ldg(tz + rows[r] + k);
 #pragma unroll
       for (int e = 0; e < KX; ++e) {
-        re[r][e] += a[e] * t.x;
-        im[r][e] -= bb[e] * t.y;
+        re[r][e] += a[e] * t[r].x;
+        im[r][e] -= bb[e] * t[r].y;
       }
     }
   }
@@ -464,17 +477,25 @@ __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restri
       Q[r][e] = 0;
     }
   }
+  T2<T> tn[RK];
+#pragma unroll
+  for (int r = 0; r < RK; ++r) tn[r] = __ldg(tz + rows[r] + 1);
   for (int kz = 1; kz <= H; ++kz) {
+    T2<T> t[RK];
+#pragma unroll
+    for (int r = 0; r < RK; ++r) {
+      t[r] = tn[r];
+      tn[r] = __ldg(tz + rows[r] + min(kz + 1, H));
+    }
     T2<T> v[KX];
 #pragma unroll
     for (int e = 0; e < KX; ++e) v[e] = c[kz * TW + KX * lane + e];
 #pragma unroll
     for (int r = 0; r < RK; ++r) {
-      const T2<T> t = __ldg(tz + rows[r] + kz);
 #pragma unroll
       for (int e = 0; e < KX; ++e) {
-        P[r][e] += v[e].x * t.x;
-        Q[r][e] += v[e].y * t.y;
+        P[r][e] += v[e].x * t[r].x;
+        Q[r][e] += v[e].y * t[r].y;
       }
     }
   }
@@ -514,7 +535,9 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
                                                 const double *__restrict__ du, const double *__restrict__ kxx,
                                                 const double *__restrict__ kzz, const double *__restrict__ dc_in,
                                                 double *__restrict__ dc_out) {
-  const int kx = blockIdx.x * 32 + (threadIdx.x & 31);
+  // lane pairs share a mode: even lane = real part, odd lane = imaginary part
+  const int lane = threadIdx.x & 31, part = lane & 1;
+  const int kx = blockIdx.x * 16 + (lane >> 1);
   const int kz = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (kx >= s.N || kz >= s.MH) return;
   const int NM = s.NM;
@@ -525,6 +548,7 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
   const bool zero = (kx == 0 && kz == 0);
   if (zero && dc_in) {
     // mixed form: zero wavenumber from FP64 line sums, solution kept in FP64
+    if (part) return;
     double dprev = 0.0, gr = 0.0;
     for (int b = 0; b < NM; ++b) {
       double r = dc_in[b];
@@ -551,72 +575,64 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
     for (int b = 0; b < NM; ++b) C[base + b * rs] = mk<T>(0, 0);
     return;
   }
-  // forward sweep in batches of PF rows: the next batch is loaded while the
-  // current one is eliminated, so PF loads per thread are always in flight
-  constexpr int PF = 8;
-  double dprev = 1.0, gx = 0.0, gy = 0.0;
-  T2<T> cur[PF], nxt[PF];
+  T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
+  // forward sweep in batches of PF rows, next batch in flight meanwhile
+  constexpr int PF = 16;
+  double rinv = 0.0, g = 0.0;
+  T cur[PF], nxt[PF];
 #pragma unroll
-  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? C[base + u * rs] : mk<T>(0, 0);
+  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? Cs[2 * (base + u * rs)] : (T)0;
   for (int b0 = 0; b0 < NM; b0 += PF) {
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int bn = b0 + PF + u;
-      nxt[u] = bn < NM ? C[base + bn * rs] : mk<T>(0, 0);
+      nxt[u] = bn < NM ? Cs[2 * (base + bn * rs)] : (T)0;
     }
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int b = b0 + u;
       if (b < NM) {
-        const long long a = base + b * rs;
-        double rx = (double)cur[u].x, ry = (double)cur[u].y;
+        double r = (double)cur[u];
         double d = (dd[b] + kk) + kzv;
         if (zero && b == 0) d = 3.0 / 2.0 * d;
         if (b > 0) {
-          const double w = dl[b] / dprev;
+          const double w = dl[b] * rinv;  // l_b / d'_{b-1}
           d = d - w * du[b - 1];
-          rx = rx - w * gx;
-          ry = ry - w * gy;
+          r = r - w * g;
         }
-        dprev = d;
-        gx = rx;
-        gy = ry;
-        C[a] = mk<T>((T)rx, (T)ry);
-        piv[a] = 1.0 / d;
+        rinv = 1.0 / d;
+        g = r;
+        Cs[2 * (base + b * rs)] = (T)r;
+        if (!part) piv[base + b * rs] = rinv;
       }
     }
 #pragma unroll
     for (int u = 0; u < PF; ++u) cur[u] = nxt[u];
   }
+  __syncwarp();
   // backward sweep, batches of PF rows from the top down
-  double xx = 0.0, xy = 0.0;
+  double x = 0.0;
   double pv[PF], pn[PF];
   const int top = NM - 1;
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
     const int b = top - u;
-    cur[u] = b >= 0 ? C[base + b * rs] : mk<T>(0, 0);
+    cur[u] = b >= 0 ? Cs[2 * (base + b * rs)] : (T)0;
     pv[u] = b >= 0 ? piv[base + b * rs] : 0.0;
   }
   for (int b0 = top; b0 >= 0; b0 -= PF) {
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int bn = b0 - PF - u;
-      nxt[u] = bn >= 0 ? C[base + bn * rs] : mk<T>(0, 0);
+      nxt[u] = bn >= 0 ? Cs[2 * (base + bn * rs)] : (T)0;
       pn[u] = bn >= 0 ? piv[base + bn * rs] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int b = b0 - u;
       if (b >= 0) {
-        if (b == top) {
-          xx = (double)cur[u].x * pv[u];
-          xy = (double)cur[u].y * pv[u];
-        } else {
-          xx = ((double)cur[u].x - du[b] * xx) * pv[u];
-          xy = ((double)cur[u].y - du[b] * xy) * pv[u];
-        }
-        C[base + b * rs] = mk<T>((T)xx, (T)xy);
+        x = (b == top) ? (double)cur[u] * pv[u] : ((double)cur[u] - du[b] * x) * pv[u];
+        Cs[2 * (base + b * rs)] = (T)x;
       }
     }
 #pragma unroll
@@ -673,6 +689,7 @@ template <typename T, int MAXR>
 static void launch_div_dct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W,
                                T *R, double *dc_sum, int nw, size_t sm, int grid, cudaStream_t st) {
   cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   k_div_dct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R, dc_sum);
 }
 
@@ -680,6 +697,7 @@ template <typename T, int MAXR>
 static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, size_t sm,
                             int grid, cudaStream_t st) {
   cudaFuncSetAttribute(k_idct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_idct<T, MAXR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   k_idct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p);
 }
 
@@ -722,12 +740,14 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
     dim3 grid((s.N + TW - 1) / TW, s.NM, (s.MH + 8 * RK - 1) / (8 * RK));
     const size_t sm = (size_t)s.M * TW * sizeof(T);
     cudaFuncSetAttribute(k_dft_z_fwd<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_dft_z_fwd<T, RK>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     k_dft_z_fwd<T, RK><<<grid, 256, sm, st>>>(s, R, C, tz);
   } else {
     const int npairs = s.M / 2 + 1;
     dim3 grid((s.N + TW - 1) / TW, s.NM, (npairs + 8 * RK - 1) / (8 * RK));
     const size_t sm = (size_t)s.MH * TW * sizeof(T2<T>);
     cudaFuncSetAttribute(k_dft_z_inv<T, RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_dft_z_inv<T, RK>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     k_dft_z_inv<T, RK><<<grid, 256, sm, st>>>(s, C, const_cast<T *>(R), tz);
   }
 }
@@ -737,7 +757,7 @@ void launch_thomas(const Spec &s, T2<T> *C, double *piv, const double *dd, const
                    const double *kxx, const double *kzz, const double *dc_lines, double *dc_rows, double *dc_out,
                    cudaStream_t st) {
   if (dc_lines) k_dc_rows<<<s.NM, 32, 0, st>>>(s, dc_lines, dc_rows);
-  dim3 grid((s.N + 31) / 32, (s.MH + 7) / 8);
+  dim3 grid((s.N + 15) / 16, (s.MH + 7) / 8);
   k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dd, dl, du, kxx, kzz, dc_lines ? dc_rows : nullptr, dc_out);
 }
 

@@ -1,6 +1,8 @@
-// stencil.cu -- finite-difference kernels of the step path (compiled with
-// -fmad=false so the FP64 instantiation evaluates every expression in the
-// order and rounding of the Fortran source, with no fused multiply-adds).
+#pragma once
+// stencil_impl.cuh -- finite-difference kernels of the step path.  Included
+// by stencil64.cu (FP64, compiled with -fmad=false so every expression keeps
+// the order and rounding of the Fortran source, with no fused multiply-adds)
+// and by stencil32.cu (FP32 mixed form, contraction allowed).
 //
 //   k_rhs_rk      RHS of u, v, w (equations.f90:24-415) fused with the RK
 //                 substep update (time_integration.f90:351-458)
@@ -345,6 +347,72 @@ __global__ void __launch_bounds__(256) k_project(Geo g, MetT<T> m, const T *__re
   }
 }
 
+// Vector form of k_project: a thread updates VN = 16/sizeof(T) consecutive
+// points i0..i0+VN-1 (i0 = 2 + VN*q, a 16-byte aligned box position) with
+// 16-byte loads and stores; points outside the update ranges keep their
+// loaded value.
+template <typename T> struct V16;
+template <> struct V16<float> { typedef float4 t; };
+template <> struct V16<double> { typedef double2 t; };
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__restrict__ p,
+                                                   const double *__restrict__ dc, T *__restrict__ U,
+                                                   T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
+                                                   const Scalars *__restrict__ sc, int save_p) {
+  typedef typename V16<T>::t VT;
+  constexpr int VN = 16 / sizeof(T);
+  const int i0 = 2 + VN * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z + 2;
+  if (i0 > g.nx || j > g.ny) return;
+  const long long c = bidx(g, i0, j, k);
+  union Vec {
+    VT v;
+    T e[VN];
+  };
+  Vec pc, pn, pt, u, v, w;
+  pc.v = __ldg(reinterpret_cast<const VT *>(p + c));
+  const T pe = __ldg(p + c + VN);
+  pn.v = __ldg(reinterpret_cast<const VT *>(p + c + g.px));
+  pt.v = __ldg(reinterpret_cast<const VT *>(p + c + g.plane));
+  u.v = *reinterpret_cast<const VT *>(U + c);
+  v.v = *reinterpret_cast<const VT *>(V + c);
+  w.v = *reinterpret_cast<const VT *>(W + c);
+  const bool vj = (j <= g.ny - 1), wk = (k <= g.nz - 1);
+  const T yC = m.yC[j], yrC = m.yrC[j], zC = m.zC[k], zrC = m.zrC[k];
+  const double ddc = dc ? (dc[j + 1 - 2] - dc[j - 2]) : 0.0;
+#pragma unroll
+  for (int e = 0; e < VN; ++e) {
+    const int i = i0 + e;
+    const T pe1 = (e + 1 < VN) ? pc.e[e + 1] : pe;
+    if (i <= g.nx - 1) u.e[e] = u.e[e] - qdiv(pe1 - pc.e[e], m.xC[i], m.xrC[i]);
+    if (i <= g.nx) {
+      if (vj) {
+        T dd = pn.e[e] - pc.e[e];
+        if (dc) dd = (T)((double)dd + ddc);
+        v.e[e] = v.e[e] - qdiv(dd, yC, yrC);
+      }
+      if (wk) w.e[e] = w.e[e] - qdiv(pt.e[e] - pc.e[e], zC, zrC);
+    }
+  }
+  *reinterpret_cast<VT *>(U + c) = u.v;
+  *reinterpret_cast<VT *>(V + c) = v.v;
+  *reinterpret_cast<VT *>(W + c) = w.v;
+  if (save_p) {
+    const double den = sc->dt * 0.5;  // dt*rk2_coef(1,1)
+    const double dj = dc ? dc[j - 2] : 0.0;
+    Vec q;
+#pragma unroll
+    for (int e = 0; e < VN; ++e) {
+      double pv = (double)pc.e[e];
+      if (dc) pv += dj;
+      q.e[e] = (i0 + e <= g.nx) ? (T)(pv / den) : (T)0;
+    }
+    *reinterpret_cast<VT *>(P + c) = q.v;
+  }
+}
+
 // P ghost planes, projection.f90:78-83 (three ordered phases)
 template <typename T>
 __global__ void k_p_ghost(Geo g, T *__restrict__ P, int phase) {
@@ -545,7 +613,7 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
 
 // time_integration.f90:560-575 (dt = min(dt_conv, dt_vis)); also arms the
 // accumulators for the next call and records to = t for the RK substeps.
-__global__ void k_dt_finish(Scalars *sc, double cfl, double dtvis) {
+static __global__ void k_dt_finish(Scalars *sc, double cfl, double dtvis) {
   double cfla = fabs(cfl);
   double lu = __longlong_as_double((long long)sc->lmax[0]);
   double lv = __longlong_as_double((long long)sc->lmax[1]);
@@ -555,11 +623,13 @@ __global__ void k_dt_finish(Scalars *sc, double cfl, double dtvis) {
   sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
 }
 
+#ifdef BLGPU_STENCIL_PRIMARY
 __global__ void k_set_time(Scalars *sc, int phase, double coef) {
   // phase 0: to = t (save at step start); phase 1: t = to + coef*dt
   if (phase == 0) sc->to = sc->t;
   else sc->t = sc->to + coef * sc->dt;
 }
+#endif
 
 // check_divergence (projection.f90:399-408): max |div| over i=2..nxg-2
 template <typename T>
@@ -599,7 +669,7 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 #define BLGPU_RHS_CASE(M, L)                                                                             \
   k_rhs_rk<T, M, L><<<grid, block, 0, st>>>(g, m, U, V, W, nut, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, \
                                             c2, kchunk)
-  if (!les) {
+  if (!les && sizeof(T) == 4) {  // FP32: register-window kernel (FP64 keeps the lower-register form)
     const int kc = 32;
     dim3 gd = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc);
 #define BLGPU_DNS_CASE(M)                                                                                     \
@@ -611,6 +681,13 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
       default: BLGPU_DNS_CASE(3); break;
     }
 #undef BLGPU_DNS_CASE
+  } else if (!les) {
+    switch (mode) {
+      case 0: BLGPU_RHS_CASE(0, false); break;
+      case 1: BLGPU_RHS_CASE(1, false); break;
+      case 2: BLGPU_RHS_CASE(2, false); break;
+      default: BLGPU_RHS_CASE(3, false); break;
+    }
   } else {
     switch (mode) {
       case 0: BLGPU_RHS_CASE(0, true); break;
@@ -625,9 +702,10 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 template <typename T>
 void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
                     const Scalars *sc, int save_p, cudaStream_t st) {
-  const int kchunk = 1;  // one point per thread: loads of different points overlap across warps
-  dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk), block(32, 8);
-  k_project<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p, kchunk);
+  constexpr int VN = 16 / sizeof(T);
+  const int ngrp = (g.nx - 1 + VN - 1) / VN;  // i = 2..nx in groups of VN
+  dim3 block(32, 8), grid((ngrp + 31) / 32, (g.ny - 1 + 7) / 8, g.nz - 1);
+  k_project_v<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p);
   if (save_p) {
     dim3 b2(32, 8);
     k_p_ghost<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 0);
@@ -636,7 +714,9 @@ void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc
   }
 }
 
+#ifdef BLGPU_STENCIL_PRIMARY
 int bc_x_parts(const Geo &g) { return ((g.nyg + 31) / 32) * ((g.nzg + 7) / 8); }
+#endif
 
 template <typename T>
 void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
@@ -658,9 +738,11 @@ void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, do
   k_dt_finish<<<1, 1, 0, st>>>(sc, cfl, dtvis);
 }
 
+#ifdef BLGPU_STENCIL_PRIMARY
 void launch_set_time(Scalars *sc, int phase, double coef, cudaStream_t st) {
   k_set_time<<<1, 1, 0, st>>>(sc, phase, coef);
 }
+#endif
 
 template <typename T>
 void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st) {
@@ -679,8 +761,7 @@ void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned lo
                              Scalars *, double, double *, double, double, cudaStream_t);                            \
   template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, cudaStream_t); \
   template void launch_maxdiv<T>(const Geo &, const T *, const T *, const T *, unsigned long long *, cudaStream_t);
-BLGPU_INST(double)
-BLGPU_INST(float)
+BLGPU_INST(BLGPU_STENCIL_T)
 
 }  // namespace blgpu
 
@@ -697,7 +778,7 @@ __global__ void k_repack_in(Geo g, const double *__restrict__ src, int n1, int n
     const int i = (int)(q % n1);
     const long long r = q / n1;
     const int j = (int)(r % n2), k = (int)(r / n2);
-    dst[((long long)k * g.py + j) * g.px + i] = (T)src[q];
+    dst[bidx(g, i + 1, j + 1, k + 1)] = (T)src[q];
   }
 }
 
@@ -708,7 +789,7 @@ __global__ void k_repack_out(Geo g, const T *__restrict__ src, int n1, int n2, i
     const int i = (int)(q % n1);
     const long long r = q / n1;
     const int j = (int)(r % n2), k = (int)(r / n2);
-    dst[q] = (double)src[((long long)k * g.py + j) * g.px + i];
+    dst[q] = (double)src[bidx(g, i + 1, j + 1, k + 1)];
   }
 }
 
@@ -718,7 +799,6 @@ void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2,
   if (dir == 0) k_repack_in<T><<<blocks, 256, 0, st>>>(g, stage, n1, n2, n3, box);
   else k_repack_out<T><<<blocks, 256, 0, st>>>(g, box, n1, n2, n3, stage);
 }
-template void launch_repack<double>(const Geo &, int, double *, double *, int, int, int, cudaStream_t);
-template void launch_repack<float>(const Geo &, int, double *, float *, int, int, int, cudaStream_t);
+template void launch_repack<BLGPU_STENCIL_T>(const Geo &, int, double *, BLGPU_STENCIL_T *, int, int, int, cudaStream_t);
 
 }  // namespace blgpu
