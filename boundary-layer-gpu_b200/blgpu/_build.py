@@ -23,6 +23,7 @@ SOURCES = {
     "stencil32.cu": [],
     "spectral.cu": [],
     "capi.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -52,6 +52,8 @@ _SIGS = {
                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     "blgpu_kernel_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "blgpu_advance_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),
+    "blgpu_check_divergence_noalloc": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
+                                       + [ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]

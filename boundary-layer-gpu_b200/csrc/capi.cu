@@ -111,6 +111,8 @@ int fail_cuda(cudaError_t e, const char *what, const char *file, int line) {
   return BLGPU_ECUDA;
 }
 
+void set_global_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 }  // namespace blgpu
 
 static int set_err(blgpu_ctx *c, int code, const char *fmt, ...) {

@@ -145,6 +145,20 @@ int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms);
 /* number of kernels this context has launched (graph replays included) */
 long long blgpu_kernel_launches(const blgpu_ctx *ctx);
 
+/* check_divergence on device arrays the caller owns, with no device
+ * allocation: no counterpart in the reference.  For hosts that cannot call
+ * cudaMalloc (an OpenACC program passing its data-region arrays by device
+ * address, or code under a pool allocator / in a no-allocation region).
+ * U(nx,nyg,nzg), V(nxg,ny,nzg), W(nxg,nyg,nz), x(nx), y(ny), z(nz) and the
+ * result *max_div are device addresses in the reference layout; stream may be
+ * NULL.  Scratch is a fixed 512 KiB __device__ array: (ny-1)*(nz-1) must be
+ * <= 65536 (else BLGPU_EINVAL); the first call on a device sets it up and
+ * should come before any stream capture; calls that overlap on the GPU race.
+ * The result is ready when the stream reaches the call. */
+int blgpu_check_divergence_noalloc(const double *U, const double *V, const double *W, const double *x,
+                                   const double *y, const double *z, int nx, int ny, int nz, double *max_div,
+                                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif
