@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--err-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -219,6 +220,7 @@ def main():
     dev = local
     torch.cuda.set_device(dev)
     case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz, seed=1234 + rank)
+    cases.project_initial(case, device=dev)
     cells = case.cells
     N, M, NM = case.nx - 2, case.nz - 2, case.ny - 1
     spectral_cells = N * M * NM
@@ -261,6 +263,16 @@ def main():
                "max_div_mixed": smix.check_divergence(), "max_div_fp64": s64.check_divergence()}
         ph64 = s64.phase_times(1)
         s64.close()
+        # error of the mixed form after ERR_STEPS RK3 steps from the same field
+        a = cases.solver_for(case, precision=blgpu.FP64, device=dev)
+        b = cases.solver_for(case, precision=blgpu.MIXED, device=dev)
+        a.advance(args.err_steps)
+        b.advance(args.err_steps)
+        A, B = a.download_state()[:3], b.download_state()[:3]
+        err["after_%d_steps" % args.err_steps] = {
+            n: float(np.linalg.norm(x - y) / np.linalg.norm(y)) for n, x, y in zip("uvw", B, A)}
+        a.close()
+        b.close()
     # ---- per-phase device times (CUDA events on the solver stream) ----
     ph = smix.phase_times(2)
     step_ms = sum(v[0] for v in ph.values()) / 2.0

@@ -52,6 +52,10 @@ _SIGS = {
                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     "blgpu_kernel_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "blgpu_advance_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),
+    "blgpu_eddy_viscosity": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_get_nu_t": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "blgpu_statistics": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 5),
+    "blgpu_law_of_wall": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int)]),
     "blgpu_check_divergence_noalloc": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
                                        + [ctypes.c_void_p, ctypes.c_void_p]),
 }

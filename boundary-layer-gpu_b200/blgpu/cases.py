@@ -350,3 +350,18 @@ def solver_for(case, precision=0, device=0, les_model=0):
         s.set_dt(-case.cfl)
     return s
 
+
+
+def project_initial(case, device=0):
+    """Make the initial field discretely divergence free: one boundary pass,
+    projection and boundary pass of the FP64 path (the config-2 recipe's
+    "one projection" of the noisy initial field).  Updates case.U/V/W."""
+    from ._lib import FP64
+    s = solver_for(case, precision=FP64, device=device)
+    s.set_dt(abs(case.cfl) if case.cfl < 0 else 1.0)
+    s.apply_boundary_conditions(3)
+    s.compute_projection_step(3)
+    s.apply_boundary_conditions(3)
+    case.U, case.V, case.W = s.download_state()[:3]
+    s.close()
+    return case

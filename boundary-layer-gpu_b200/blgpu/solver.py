@@ -162,6 +162,39 @@ class Solver:
         self._ck(self.lib.blgpu_max_divergence(self.ctx, ctypes.byref(d)))
         return d.value
 
+    # -- models and diagnostics -------------------------------------------
+    def compute_eddy_viscosity(self):
+        """sgs_Smagorinsky on the resident state; returns nu_t(nxg,nyg,nzg)."""
+        self._ck(self.lib.blgpu_eddy_viscosity(self.ctx))
+        return self.nu_t()
+
+    def nu_t(self):
+        a = np.zeros((self.nxg, self.nyg, self.nzg), order="F")
+        self._ck(self.lib.blgpu_get_nu_t(self.ctx, _p(a)))
+        return a
+
+    def compute_statistics(self):
+        """compute_statistics: dict of z-means, Cf, dUdy_wall and inlet scalars."""
+        nx, ny = self.nx, self.ny
+        means = np.zeros((9, ny, nx))
+        ntm = np.zeros((self.nyg, self.nxg))
+        cf = np.zeros(nx)
+        du = np.zeros(nx)
+        sc = np.zeros(5)
+        self._ck(self.lib.blgpu_statistics(self.ctx, _p(means), _p(ntm), _p(cf), _p(du), _p(sc)))
+        names = ["Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "UVmean", "Pmean", "P2mean"]
+        out = {n: means[q].T.copy(order="F") for q, n in enumerate(names)}
+        out.update(nu_t_mean=ntm.T.copy(order="F"), Cf=cf, dUdy_wall=du, theta_inlet=sc[0], delta99_inlet=sc[1],
+                   Rex_inlet=sc[2], Retheta_inlet=sc[3], Redelta_inlet=sc[4])
+        return out
+
+    def law_of_the_wall(self, utau_guess):
+        """compute_law_of_the_wall_model: (utau_model, iters_max)."""
+        u = np.ascontiguousarray(utau_guess, dtype=np.float64).copy()
+        it = ctypes.c_int()
+        self._ck(self.lib.blgpu_law_of_wall(self.ctx, _p(u), ctypes.byref(it)))
+        return u, it.value
+
     def device_bytes(self):
         return int(self.lib.blgpu_device_bytes(self.ctx))
 

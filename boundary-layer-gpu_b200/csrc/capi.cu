@@ -59,6 +59,10 @@ struct blgpu_ctx {
   FftPlan<double> pl64{};
   FftPlan<float> pl32{};
   double *stage = nullptr;  // FP64 staging of one host-layout field
+  double *d_cs2 = nullptr;  // (Cs Delta_j f)^2 of the Smagorinsky model, j = 0..nyg
+  double *d_stats = nullptr;
+  double *d_utau = nullptr;
+  int *d_iters = nullptr;
   int cur = 0, old = 1;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_next[3] = {0, 0, 0};
@@ -227,6 +231,11 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, (void **)&ctx->dcout, (size_t)s.NM * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->sc, sizeof(Scalars)));
   TRY(dalloc(ctx, (void **)&ctx->stage, (size_t)ctx->nxg * ctx->nyg * ctx->nzg * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->d_cs2, (size_t)(ctx->nyg + 2) * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->d_stats,
+             ((size_t)9 * ctx->nx * ctx->ny + (size_t)ctx->nxg * ctx->nyg + 2 * (size_t)ctx->nx) * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->d_utau, (size_t)ctx->nx * sizeof(double)));
+  TRY(dalloc(ctx, (void **)&ctx->d_iters, (size_t)ctx->nx * sizeof(int)));
   TRY(dalloc(ctx, (void **)&ctx->d_maxdiv, sizeof(unsigned long long)));
   // transform tables
   {
@@ -371,6 +380,15 @@ int blgpu_set_grid(blgpu_ctx *ctx, const double *x, const double *y, const doubl
       ctx->kzz[k] = 2.0 * (cos(2.0 * pi * (double)k / (double)s.M) - 1.0) / (ctx->dzmin * ctx->dzmin);
     else
       ctx->kzz[k] = 2.0 * (cos(2.0 * pi * (double)(-s.M + k) / (double)s.M) - 1.0) / (ctx->dzmin * ctx->dzmin);
+  }
+  // Smagorinsky (Cs Delta_j f)^2, subgrid.f90:629-639 (f = 1, Cs = 0.11)
+  {
+    std::vector<double> cs2(ctx->nyg + 2, 0.0);
+    for (int j = 2; j <= ctx->nyg - 1; ++j) {
+      const double Delta = pow(ctx->dxmin * ctx->dzmin * (ctx->y[j] - ctx->y[j - 1]), 1.0 / 3.0);
+      cs2[j] = (0.11 * Delta * 1.0) * (0.11 * Delta * 1.0);
+    }
+    CK(cudaMemcpy(ctx->d_cs2, cs2.data(), cs2.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   // length_y of the mass balance (boundary_conditions.f90:242-246)
   ctx->length_y = 0.0;
@@ -697,6 +715,12 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
   launch_set_time(ctx->sc, 0, 0.0, ctx->st);
   ph_end(ctx, 1);
   auto sub = [&](int mode, int in, int outb, double c1, double c2, double tc, int rk_step) {
+    if (ctx->cfg.les_model == 1) {  // Smagorinsky from the substep's state (time_integration.f90:341-346)
+      T **Si = reinterpret_cast<T **>(ctx->S[in]);
+      ph_begin(ctx, PH_MISC);
+      launch_smagorinsky<T>(ctx->geo, Si[0], Si[1], Si[2], ctx->d_cs2, (T *)ctx->nut, ctx->st);
+      ph_end(ctx, 1);
+    }
     enq_rhs<T>(ctx, mode, in, a, outb, c1, c2);
     ph_begin(ctx, PH_MISC);
     launch_set_time(ctx->sc, 1, tc, ctx->st);
@@ -955,6 +979,119 @@ int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms) {
   if (rc) return rc;
   CK(e);
   *ms = (double)t;
+  return BLGPU_OK;
+}
+
+int blgpu_eddy_viscosity(blgpu_ctx *ctx) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->nut) return set_err(ctx, BLGPU_ESTATE, "blgpu_eddy_viscosity: context created with LES=0");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_eddy_viscosity: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_smagorinsky<double>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (double *)ctx->nut, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_smagorinsky<float>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (float *)ctx->nut, ctx->st);
+  }
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_get_nu_t(blgpu_ctx *ctx, double *nu_t) {
+  if (!ctx || !nu_t) return set_err(ctx, BLGPU_EINVAL, "blgpu_get_nu_t: null argument");
+  if (!ctx->nut) return set_err(ctx, BLGPU_ESTATE, "blgpu_get_nu_t: context created with LES=0");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  int rc = download_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_statistics(blgpu_ctx *ctx, double *means, double *nu_t_mean, double *Cf, double *dUdy_wall,
+                     double *scalars) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_statistics: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_stats<double>(ctx->geo, S[0], S[1], S[2], (const double *)ctx->P, (const double *)ctx->nut, ctx->d_stats,
+                         ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_stats<float>(ctx->geo, S[0], S[1], S[2], (const float *)ctx->P, (const float *)ctx->nut, ctx->d_stats,
+                        ctx->st);
+  }
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  const int nx = ctx->nx, ny = ctx->ny, nxg = ctx->nxg, nyg = ctx->nyg;
+  const size_t pl = (size_t)nx * ny, ntot = 9 * pl + (size_t)nxg * nyg + 2 * (size_t)nx;
+  std::vector<double> h(ntot);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_stats, ntot * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (means) memcpy(means, h.data(), 9 * pl * sizeof(double));
+  const double *ntm = h.data() + 9 * pl;
+  if (nu_t_mean) memcpy(nu_t_mean, ntm, (size_t)nxg * nyg * sizeof(double));
+  const double *a1 = ntm + (size_t)nxg * nyg, *a2 = a1 + nx;
+  const double *Um = h.data(), *UV = h.data() + 6 * pl;
+  // statistics.f90:138-201 (wall gradient, Cf, inlet theta, delta99, Reynolds numbers)
+  std::vector<double> dU(nx), cf(nx);
+  for (int ii = 1; ii <= nx; ++ii) dU[ii - 1] = (a2[ii - 1] - a1[ii - 1]) / (ctx->yg[2] - ctx->yg[1]);
+  for (int ii = 1; ii <= nx; ++ii) {
+    const double tau = 0.25 * (ntm[ii - 1] + ntm[(size_t)nxg + ii - 1] + ntm[ii] + ntm[(size_t)nxg + ii]) * dU[ii - 1];
+    cf[ii - 1] = 2.0 * (-UV[ii - 1] + ctx->cfg.nu * dU[ii - 1] + tau) / 1.0;
+  }
+  if (Cf) memcpy(Cf, cf.data(), nx * sizeof(double));
+  if (dUdy_wall) memcpy(dUdy_wall, dU.data(), nx * sizeof(double));
+  if (scalars) {
+    const double Uinf = 1.0;
+    double theta = 0.0;
+    for (int j = 2; j <= ny; ++j) {
+      const double tj = Um[(size_t)(j - 1) * nx] / Uinf * (1.0 - Um[(size_t)(j - 1) * nx] / Uinf);
+      const double tm = Um[(size_t)(j - 2) * nx] / Uinf * (1.0 - Um[(size_t)(j - 2) * nx] / Uinf);
+      theta = theta + 0.5 * (tj + tm) * (ctx->y[j] - ctx->y[j - 1]);
+    }
+    int jref = 0;
+    for (int j = 1; j <= ny; ++j)
+      if (Um[(size_t)(j - 1) * nx] >= 0.99 * Uinf) { jref = j; break; }
+    if (jref < 2) jref = 2;
+    const double u1 = Um[(size_t)(jref - 2) * nx], u2 = Um[(size_t)(jref - 1) * nx];
+    const double w1 = (0.99 * Uinf - u1) / (u2 - u1), w0 = 1.0 - w1;
+    const double d99 = w1 * ctx->y[jref] + w0 * ctx->y[jref - 1];
+    scalars[0] = theta;
+    scalars[1] = d99;
+    scalars[2] = ctx->x[1] * Uinf / ctx->cfg.nu;
+    scalars[3] = theta * Uinf / ctx->cfg.nu;
+    scalars[4] = d99 * Uinf / ctx->cfg.nu;
+  }
+  return BLGPU_OK;
+}
+
+int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max) {
+  if (!ctx || !utau) return set_err(ctx, BLGPU_EINVAL, "blgpu_law_of_wall: null argument");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_law_of_wall: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const int nx = ctx->nx;
+  CK(cudaMemcpyAsync(ctx->d_utau, utau, nx * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  if (ctx->fp64)
+    launch_law_of_wall<double>(ctx->geo, ((double **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, ctx->st);
+  else
+    launch_law_of_wall<float>(ctx->geo, ((float **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, ctx->st);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  std::vector<int> it(nx, 0);
+  CK(cudaMemcpyAsync(utau, ctx->d_utau, nx * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(it.data(), ctx->d_iters, nx * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  // utau_model(1) = utau_model(2); utau_model(nx) = utau_model(nx-1) (wallmodel.f90:1979-1980)
+  utau[0] = utau[1];
+  utau[nx - 1] = utau[nx - 2];
+  int mx = 0;
+  for (int i = 2; i <= nx - 1; ++i) mx = it[i - 1] > mx ? it[i - 1] : mx;
+  if (iters_max) *iters_max = mx;
   return BLGPU_OK;
 }
 

@@ -43,6 +43,13 @@ template <typename T>
 void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st);
 
 template <typename T>
+void launch_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, const double *cs2, T *nut, cudaStream_t st);
+template <typename T>
+void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, const T *nut, double *out,
+                  cudaStream_t st);
+template <typename T>
+void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cudaStream_t st);
+template <typename T>
 void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st);
 
 // ---- spectral.cu ----

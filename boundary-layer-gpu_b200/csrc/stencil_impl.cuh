@@ -654,6 +654,148 @@ __global__ void __launch_bounds__(256) k_maxdiv(Geo g, const T *__restrict__ U, 
 }
 
 // ---------------------------------------------------------------------------
+// Constant-coefficient Smagorinsky eddy viscosity (subgrid.f90:609-662) with
+// the rate of strain of compute_Sij (subgrid.f90:672-730): diagonal terms at
+// the cell centre, off-diagonal terms on the cell edges averaged to the
+// centre, |S| = sqrt(2 Sij Sij).  cs2[j] = (Cs Delta_j f)^2 with
+// Delta_j = (dx dz (y(j)-y(j-1)))^(1/3) and f = 1 (Dirichlet_nu_t is forced 0,
+// initialization.f90:586).  Interior points i=2..nxg-1, j=2..nyg-1,
+// k=2..nzg-1 only.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T sij4(const Geo &g, const T *U, const T *V, int i, int j, int k) {
+  const long long c = bidx(g, i, j, k);
+  return (T)0.5 * ((U[c - 1] - U[c - 1 - g.px]) / (T)(g.yg[j] - g.yg[j - 1]) +
+                   (V[c - g.px] - V[c - 1 - g.px]) / (T)(g.xg[i] - g.xg[i - 1]));
+}
+template <typename T>
+__device__ __forceinline__ T sij5(const Geo &g, const T *U, const T *W, int i, int j, int k) {
+  const long long c = bidx(g, i, j, k);
+  return (T)0.5 * ((U[c - 1] - U[c - 1 - g.plane]) / (T)(g.zg[k] - g.zg[k - 1]) +
+                   (W[c - g.plane] - W[c - 1 - g.plane]) / (T)(g.xg[i] - g.xg[i - 1]));
+}
+template <typename T>
+__device__ __forceinline__ T sij6(const Geo &g, const T *V, const T *W, int i, int j, int k) {
+  const long long c = bidx(g, i, j, k);
+  return (T)0.5 * ((V[c - g.px] - V[c - g.px - g.plane]) / (T)(g.zg[k] - g.zg[k - 1]) +
+                   (W[c - g.plane] - W[c - g.px - g.plane]) / (T)(g.yg[j] - g.yg[j - 1]));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_smagorinsky(Geo g, const T *__restrict__ U, const T *__restrict__ V,
+                                                     const T *__restrict__ W, const double *__restrict__ cs2,
+                                                     T *__restrict__ nut) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z + 2;
+  if (i > g.nxg - 1 || j > g.nyg - 1 || k > g.nzg - 1) return;
+  const long long c = bidx(g, i, j, k);
+  const T s1 = (U[c] - U[c - 1]) / (T)(g.x[i] - g.x[i - 1]);
+  const T s2 = (V[c] - V[c - g.px]) / (T)(g.y[j] - g.y[j - 1]);
+  const T s3 = (W[c] - W[c - g.plane]) / (T)(g.z[k] - g.z[k - 1]);
+  const T q = (T)0.25;
+  const T s4 = q * (sij4<T>(g, U, V, i, j, k) + sij4<T>(g, U, V, i + 1, j, k) + sij4<T>(g, U, V, i, j + 1, k) +
+                    sij4<T>(g, U, V, i + 1, j + 1, k));
+  const T s5 = q * (sij5<T>(g, U, W, i, j, k) + sij5<T>(g, U, W, i + 1, j, k) + sij5<T>(g, U, W, i, j, k + 1) +
+                    sij5<T>(g, U, W, i + 1, j, k + 1));
+  const T s6 = q * (sij6<T>(g, V, W, i, j, k) + sij6<T>(g, V, W, i, j + 1, k) + sij6<T>(g, V, W, i, j, k + 1) +
+                    sij6<T>(g, V, W, i, j + 1, k + 1));
+  T S = 0;
+  S = S + (T)2 * s1 * s1;
+  S = S + (T)2 * s2 * s2;
+  S = S + (T)2 * s3 * s3;
+  S = S + (T)4 * s4 * s4;
+  S = S + (T)4 * s5 * s5;
+  S = S + (T)4 * s6 * s6;
+  nut[c] = (T)cs2[j] * sqrt(S);
+}
+
+// ---------------------------------------------------------------------------
+// z-averaged statistics of statistics.f90:37-80, FP64 accumulators in the
+// source's summation order: for ii=1..nx, jj=1..ny the sums over k of the
+// y-interpolated U, the x-interpolated V, the xy-interpolated W, their
+// squares, U*V, P, P^2 and nu_t.  out: 9 (nx,ny) arrays + nu_t_mean(nxg,nyg)
+// + the wall sums of U at j = 1, 2 (2 x nx).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_stats(Geo g, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
+                        const T *__restrict__ P, const T *__restrict__ nut, double *__restrict__ out) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (ii > g.nx || jj > g.ny) return;
+  const int nx = g.nx, ny = g.ny;
+  const double w0 = g.w0[jj], w1 = g.w1[jj];
+  double su = 0, sv = 0, sw = 0, su2 = 0, sv2 = 0, sw2 = 0, suv = 0, sp = 0, sp2 = 0, sn = 0;
+  for (int k = 2; k <= g.nzg - 1; ++k) {
+    const long long c = bidx(g, ii, jj, k);
+    const double t1 = w0 * (double)U[c] + w1 * (double)U[c + g.px];
+    const double t2 = 0.5 * ((double)V[c] + (double)V[c + 1]);
+    su += t1;
+    sv += t2;
+    su2 += t1 * t1;
+    sv2 += t2 * t2;
+    suv += t1 * t2;
+    const double pv = (double)P[c];
+    sp += pv;
+    sp2 += pv * pv;
+    if (nut) sn += (double)nut[c];
+  }
+  for (int k = 1; k <= g.nz - 2; ++k) {
+    const long long c = bidx(g, ii, jj, k);
+    const double a = 0.5 * ((double)W[c] + (double)W[c + 1]);
+    const double b = 0.5 * ((double)W[c + g.px] + (double)W[c + g.px + 1]);
+    const double t = w0 * a + w1 * b;
+    sw += t;
+    sw2 += t * t;
+  }
+  const long long pl = (long long)nx * ny, q = (long long)(jj - 1) * nx + (ii - 1);
+  const double dn = (double)(g.nzg - 2), dw = (double)(g.nz - 2);
+  out[q] = su / dn;
+  out[q + pl] = sv / dn;
+  out[q + 2 * pl] = sw / dw;
+  out[q + 3 * pl] = su2 / dn;
+  out[q + 4 * pl] = sv2 / dn;
+  out[q + 5 * pl] = sw2 / dw;
+  out[q + 6 * pl] = suv / dn;
+  out[q + 7 * pl] = sp / dn;
+  out[q + 8 * pl] = sp2 / dn;
+  out[9 * pl + (long long)(jj - 1) * g.nxg + (ii - 1)] = sn / dn;
+  if (jj <= 2) {  // wall sums of statistics.f90:138-146
+    double a = 0.0;
+    for (int k = 2; k <= g.nzg - 1; ++k) a += (double)U[bidx(g, ii, jj, k)];
+    out[9 * pl + (long long)g.nxg * g.nyg + (long long)(jj - 1) * nx + (ii - 1)] = a / dn;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// equilibrium law of the wall at each x (wallmodel.f90:1951-1985) solved with
+// Newton_iter_solver (Newton_solver.f90:13-79): kappa = 0.38, B = 5.2,
+// y = yg(3), at most 30 iterations, stop when |f| < 1e-10.  utau holds the
+// initial guess on entry (the previous model) and the model on exit; iters
+// receives the iteration count of each x.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_law_of_wall(Geo g, const T *__restrict__ U, double *__restrict__ utau, int *__restrict__ iters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (i > g.nx - 1) return;
+  const int jref = 3;
+  const double kap = 0.38, B = 5.20, yref = g.yg[jref], nu = g.nu;
+  double x = utau[i - 1];
+  double um = 0.0;
+  for (int k = 2; k <= g.nzg - 1; ++k) um += (double)U[bidx(g, i, jref, k)];
+  um = um / (double)(g.nzg - 2);
+  int k;
+  for (k = 1; k <= 30; ++k) {
+    const double fx = x / kap * log(yref * x / nu) + B * x - um;
+    const double fp = 1.0 / kap * log(yref * x / nu) + 1.0 / kap + B;
+    if (fabs(fx) < 1e-10) break;
+    x = x - fx / fp;
+  }
+  utau[i - 1] = (x != x) ? 0.0 : x;
+  iters[i - 1] = k - 1;
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static inline dim3 vol_grid(int ni, int nj, int nk, int kchunk) {
@@ -751,6 +893,24 @@ void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned lo
   k_maxdiv<T><<<grid, block, 0, st>>>(g, U, V, W, out, kchunk);
 }
 
+template <typename T>
+void launch_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, const double *cs2, T *nut, cudaStream_t st) {
+  dim3 block(32, 8), grid((g.nxg - 2 + 31) / 32, (g.nyg - 2 + 7) / 8, g.nzg - 2);
+  k_smagorinsky<T><<<grid, block, 0, st>>>(g, U, V, W, cs2, nut);
+}
+
+template <typename T>
+void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, const T *nut, double *out,
+                  cudaStream_t st) {
+  dim3 block(32, 8), grid((g.nx + 31) / 32, (g.ny + 7) / 8);
+  k_stats<T><<<grid, block, 0, st>>>(g, U, V, W, P, nut, out);
+}
+
+template <typename T>
+void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cudaStream_t st) {
+  k_law_of_wall<T><<<(g.nx + 127) / 128, 128, 0, st>>>(g, U, utau, iters);
+}
+
 #define BLGPU_INST(T)                                                                                                \
   template void launch_rhs_rk<T>(const Geo &, const MetT<T> &, int, bool, const T *, const T *, const T *,          \
                                  const T *, const T *, const T *, const T *, T *, T *, T *, T *, T *, T *,          \
@@ -760,7 +920,12 @@ void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned lo
   template void launch_bc<T>(const Geo &, const BcData &, T *, T *, T *, const T *, const T *, const T *,         \
                              Scalars *, double, double *, double, double, cudaStream_t);                            \
   template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, cudaStream_t); \
-  template void launch_maxdiv<T>(const Geo &, const T *, const T *, const T *, unsigned long long *, cudaStream_t);
+  template void launch_maxdiv<T>(const Geo &, const T *, const T *, const T *, unsigned long long *, cudaStream_t); \
+  template void launch_smagorinsky<T>(const Geo &, const T *, const T *, const T *, const double *, T *,            \
+                                      cudaStream_t);                                                                \
+  template void launch_stats<T>(const Geo &, const T *, const T *, const T *, const T *, const T *, double *,       \
+                                cudaStream_t);                                                                      \
+  template void launch_law_of_wall<T>(const Geo &, const T *, double *, int *, cudaStream_t);
 BLGPU_INST(BLGPU_STENCIL_T)
 
 }  // namespace blgpu

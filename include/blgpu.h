@@ -48,7 +48,9 @@ typedef struct blgpu_config {
   double cfl;         /* CFL; < 0 means fixed dt = -CFL (time_integration.f90:539) */
   double dpdx, dpdz;  /* dPdx, dPdz (params.f90:152-153) */
   int rk_scheme;      /* RKscheme: 1 Euler, 2 RK2, 3 RK3 (params.f90:195) */
-  int les_model;      /* LES: 0 DNS, 1 eddy viscosity from blgpu_set_nu_t */
+  int les_model;      /* LES: 0 DNS; 1 constant-coefficient Smagorinsky computed on the device
+                         before every substep (subgrid.f90:609-730); 2 eddy viscosity given
+                         by blgpu_set_nu_t and held fixed */
   int precision;      /* BLGPU_FP64 | BLGPU_MIXED */
   int poisson;        /* BLGPU_POISSON_NATIVE | BLGPU_POISSON_CUFFT */
   int device;         /* CUDA device ordinal */
@@ -79,7 +81,7 @@ int blgpu_set_boundary(blgpu_ctx *ctx, const double *U_inlet, const double *V_in
 int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const double *zmode, const double *tmode,
                            const double *qu, const double *qv, const double *qw);
 
-/* eddy viscosity nu_t(nxg,nyg,nzg) for LES=1 (subgrid.f90:23, host model) */
+/* eddy viscosity nu_t(nxg,nyg,nzg) supplied by the host (LES = 2) */
 int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t);
 
 /* state in/out (main.f90:61-81 copy-in; main.f90:99-101 update self).
@@ -137,6 +139,25 @@ long long blgpu_device_bytes(const blgpu_ctx *ctx);
  *   8 compute_dt  9 time bookkeeping
  * nphase must be >= 10; kernels may be NULL. */
 int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels, int nphase);
+
+/* sgs_Smagorinsky (subgrid.f90:609-730) on the resident state: nu_t on the
+ * interior i=2..nxg-1, j=2..nyg-1, k=2..nzg-1 (Cs = 0.11, f = 1) */
+int blgpu_eddy_viscosity(blgpu_ctx *ctx);
+int blgpu_get_nu_t(blgpu_ctx *ctx, double *nu_t);
+
+/* compute_statistics (statistics.f90:26-201) on the device, FP64
+ * accumulators: means = Umean,Vmean,Wmean,U2mean,V2mean,W2mean,UVmean,
+ * Pmean,P2mean as 9 consecutive (nx,ny) arrays; nu_t_mean(nxg,nyg); Cf(nx);
+ * dUdy_wall(nx); scalars = theta_inlet, delta99_inlet, Re_x, Re_theta,
+ * Re_delta.  Any output may be NULL. */
+int blgpu_statistics(blgpu_ctx *ctx, double *means, double *nu_t_mean, double *Cf, double *dUdy_wall,
+                     double *scalars);
+
+/* compute_law_of_the_wall_model (wallmodel.f90:1951-1985) with
+ * Newton_iter_solver (Newton_solver.f90:13-79): utau(nx) is the initial
+ * guess on entry and utau_model on exit; *iters_max = largest iteration
+ * count (30 = not converged) */
+int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max);
 
 /* blgpu_advance(ctx, nsteps) bracketed by CUDA events on the context
  * stream; *ms = device time of the nsteps (graph captured beforehand) */

@@ -79,6 +79,12 @@ def load():
         lib.blo_zgtsv.restype = ctypes.c_int
         lib.blo_zgtsv.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         lib.blo_dct2.argtypes = [ctypes.c_int, _dp, _dp]
+        lib.blo_smagorinsky.argtypes = [ctypes.c_void_p]
+        lib.blo_set_les.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.blo_get_nu_t.argtypes = [ctypes.c_void_p, _dp]
+        lib.blo_statistics.argtypes = [ctypes.c_void_p] + [_dp] * 5
+        lib.blo_law_of_wall.restype = ctypes.c_int
+        lib.blo_law_of_wall.argtypes = [ctypes.c_void_p, _dp]
         _lib = lib
     return _lib
 
@@ -153,6 +159,9 @@ class Oracle:
         U, V, W = _f(U), _f(V), _f(W)
         self.lib.blo_set_state(self.h, _p(U), _p(V), _p(W), float(t))
 
+    def set_les(self, les_model):
+        self.lib.blo_set_les(self.h, int(les_model))
+
     def set_nu_t(self, nu_t, les_model=1):
         a = _f(nu_t)
         self.lib.blo_set_nu_t(self.h, _p(a), int(les_model))
@@ -211,6 +220,29 @@ class Oracle:
 
     def max_divergence(self):
         return self.lib.blo_max_divergence(self.h)
+
+    def smagorinsky(self):
+        self.lib.blo_smagorinsky(self.h)
+        a = np.zeros((self.nxg, self.nyg, self.nzg), order="F")
+        self.lib.blo_get_nu_t(self.h, _p(a))
+        return a
+
+    def statistics(self):
+        nx, ny = self.nx, self.ny
+        means = np.zeros((9, ny, nx))
+        ntm = np.zeros((self.nyg, self.nxg))
+        cf, du, sc = np.zeros(nx), np.zeros(nx), np.zeros(5)
+        self.lib.blo_statistics(self.h, _p(means), _p(ntm), _p(cf), _p(du), _p(sc))
+        names = ["Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "UVmean", "Pmean", "P2mean"]
+        out = {n: means[q].T.copy(order="F") for q, n in enumerate(names)}
+        out.update(nu_t_mean=ntm.T.copy(order="F"), Cf=cf, dUdy_wall=du, theta_inlet=sc[0], delta99_inlet=sc[1],
+                   Rex_inlet=sc[2], Retheta_inlet=sc[3], Redelta_inlet=sc[4])
+        return out
+
+    def law_of_the_wall(self, utau_guess):
+        u = np.ascontiguousarray(utau_guess, dtype=np.float64).copy()
+        it = self.lib.blo_law_of_wall(self.h, _p(u))
+        return u, it
 
 
 def oracle_for(case, variant=0, threads=1):

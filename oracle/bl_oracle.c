@@ -1155,9 +1155,11 @@ static void rk_update(blo_t *o, int nterms, const double *a) {
       }
 }
 
+void blo_smagorinsky(blo_t *o);
 static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms,
                     double tnew) {
   o->rk_step = rk_step;
+  if (o->les == 1) blo_smagorinsky(o); /* time_integration.f90:341-346 */
   rhs_u_impl(o, o->U, o->V, o->W, o->Fu[s]);
   rhs_v_impl(o, o->U, o->V, o->W, o->Fv[s]);
   rhs_w_impl(o, o->U, o->V, o->W, o->Fw[s]);
@@ -1224,3 +1226,173 @@ void blo_rk3_stage(blo_t *o, int stage) {
     substep(o, 2, 3, a3, 3, stage_to + o->rk_t[3] * o->dt);
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* constant-coefficient Smagorinsky: subgrid.f90:609-662 (sgs_Smagorinsky)  */
+/* with compute_Sij, :672-730.  Dirichlet_nu_t is forced to 0               */
+/* (initialization.f90:586), so the damping f = 1.  nu_t is written on the  */
+/* interior i=2..nxg-1, j=2..nyg-1, k=2..nzg-1; ghosts keep their values.   */
+/* ------------------------------------------------------------------------ */
+static double sij_edge4(const blo_t *o, const double *U_, const double *V_, int i, int j, int k) {
+  return 0.5 * ((AU(U_, i - 1, j, k) - AU(U_, i - 1, j - 1, k)) / (o->yg[j] - o->yg[j - 1]) +
+                (AV(V_, i, j - 1, k) - AV(V_, i - 1, j - 1, k)) / (o->xg[i] - o->xg[i - 1]));
+}
+static double sij_edge5(const blo_t *o, const double *U_, const double *W_, int i, int j, int k) {
+  return 0.5 * ((AU(U_, i - 1, j, k) - AU(U_, i - 1, j, k - 1)) / (o->zg[k] - o->zg[k - 1]) +
+                (AW(W_, i, j, k - 1) - AW(W_, i - 1, j, k - 1)) / (o->xg[i] - o->xg[i - 1]));
+}
+static double sij_edge6(const blo_t *o, const double *V_, const double *W_, int i, int j, int k) {
+  return 0.5 * ((AV(V_, i, j - 1, k) - AV(V_, i, j - 1, k - 1)) / (o->zg[k] - o->zg[k - 1]) +
+                (AW(W_, i, j, k - 1) - AW(W_, i, j - 1, k - 1)) / (o->yg[j] - o->yg[j - 1]));
+}
+
+void blo_smagorinsky(blo_t *o) {
+  const double Cs = 0.11, f = 1.0;
+  const double *U = o->U, *V = o->V, *W = o->W;
+  for (int j = 2; j <= o->nyg - 1; ++j) {
+    const double Delta = pow(o->dx * o->dz * (o->y[j] - o->y[j - 1]), 1.0 / 3.0);
+    const double c2 = (Cs * Delta * f) * (Cs * Delta * f);
+    for (int k = 2; k <= o->nzg - 1; ++k)
+      for (int i = 2; i <= o->nxg - 1; ++i) {
+        double s1 = (AU(U, i, j, k) - AU(U, i - 1, j, k)) / (o->x[i] - o->x[i - 1]);
+        double s2 = (AV(V, i, j, k) - AV(V, i, j - 1, k)) / (o->y[j] - o->y[j - 1]);
+        double s3 = (AW(W, i, j, k) - AW(W, i, j, k - 1)) / (o->z[k] - o->z[k - 1]);
+        double s4 = 0.25 * (sij_edge4(o, U, V, i, j, k) + sij_edge4(o, U, V, i + 1, j, k) +
+                            sij_edge4(o, U, V, i, j + 1, k) + sij_edge4(o, U, V, i + 1, j + 1, k));
+        double s5 = 0.25 * (sij_edge5(o, U, W, i, j, k) + sij_edge5(o, U, W, i + 1, j, k) +
+                            sij_edge5(o, U, W, i, j, k + 1) + sij_edge5(o, U, W, i + 1, j, k + 1));
+        double s6 = 0.25 * (sij_edge6(o, V, W, i, j, k) + sij_edge6(o, V, W, i, j + 1, k) +
+                            sij_edge6(o, V, W, i, j, k + 1) + sij_edge6(o, V, W, i, j + 1, k + 1));
+        double S = 0.0;
+        S = S + 2.0 * s1 * s1;
+        S = S + 2.0 * s2 * s2;
+        S = S + 2.0 * s3 * s3;
+        S = S + 4.0 * s4 * s4;
+        S = S + 4.0 * s5 * s5;
+        S = S + 4.0 * s6 * s6;
+        S = sqrt(S);
+        NUT(i, j, k) = c2 * S;
+      }
+  }
+}
+
+void blo_get_nu_t(const blo_t *o, double *nu_t) {
+  memcpy(nu_t, o->nu_t, sizeof(double) * (size_t)o->nxg * o->nyg * o->nzg);
+}
+
+/* ------------------------------------------------------------------------ */
+/* statistics: statistics.f90:26-201.  means = 9 arrays (nx,ny):            */
+/* Umean Vmean Wmean U2mean V2mean W2mean UVmean Pmean P2mean; nu_t_mean    */
+/* (nxg,nyg); Cf, dUdy_wall (nx); sc = theta_inlet, delta99, Re_x, Re_theta,*/
+/* Re_delta                                                                 */
+/* ------------------------------------------------------------------------ */
+void blo_statistics(const blo_t *o, double *means, double *nu_t_mean, double *Cf, double *dUdy_wall, double *sc) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+  const double *U = o->U, *V = o->V, *W = o->W, *P = o->P;
+  const size_t pl = (size_t)nx * ny;
+  double *Um = means, *Vm = means + pl, *Wm = means + 2 * pl, *U2 = means + 3 * pl, *V2 = means + 4 * pl,
+         *W2 = means + 5 * pl, *UV = means + 6 * pl, *Pm = means + 7 * pl, *P2 = means + 8 * pl;
+  memset(nu_t_mean, 0, sizeof(double) * (size_t)nxg * nyg);
+  for (int jj = 1; jj <= ny; ++jj)
+    for (int ii = 1; ii <= nx; ++ii) {
+      double su = 0, sv = 0, sw = 0, su2 = 0, sv2 = 0, sw2 = 0, suv = 0, sp = 0, sp2 = 0, sn = 0;
+      for (int k = 2; k <= nzg - 1; ++k) {
+        /* term_1 = interp_y(U) (weighted), term_2 = interp_x(V) */
+        double t1 = o->wy0[jj] * AU(U, ii, jj, k) + o->wy1[jj] * AU(U, ii, jj + 1, k);
+        double t2 = 0.5 * (AV(V, ii, jj, k) + AV(V, ii + 1, jj, k));
+        su += t1;
+        sv += t2;
+        su2 += t1 * t1;
+        sv2 += t2 * t2;
+        suv += t1 * t2;
+        sp += AP(P, ii, jj, k);
+        sp2 += AP(P, ii, jj, k) * AP(P, ii, jj, k);
+        sn += NUT(ii, jj, k);
+      }
+      for (int k = 1; k <= nz - 2; ++k) {
+        /* term = interp_y(interp_x(W)) */
+        double a = 0.5 * (AW(W, ii, jj, k) + AW(W, ii + 1, jj, k));
+        double b = 0.5 * (AW(W, ii, jj + 1, k) + AW(W, ii + 1, jj + 1, k));
+        double t = o->wy0[jj] * a + o->wy1[jj] * b;
+        sw += t;
+        sw2 += t * t;
+      }
+      size_t q = (size_t)(jj - 1) * nx + (ii - 1);
+      const double dn = (double)(nzg - 2), dw = (double)(nz - 2);
+      Um[q] = su / dn; Vm[q] = sv / dn; Wm[q] = sw / dw;
+      U2[q] = su2 / dn; V2[q] = sv2 / dn; W2[q] = sw2 / dw;
+      UV[q] = suv / dn; Pm[q] = sp / dn; P2[q] = sp2 / dn;
+      nu_t_mean[(size_t)(jj - 1) * nxg + (ii - 1)] = sn / dn;
+    }
+  for (int ii = 1; ii <= nx; ++ii) {
+    double a1 = 0, a2 = 0;
+    for (int k = 2; k <= nzg - 1; ++k) {
+      a1 += AU(U, ii, 1, k);
+      a2 += AU(U, ii, 2, k);
+    }
+    a1 /= (double)(nzg - 2);
+    a2 /= (double)(nzg - 2);
+    dUdy_wall[ii - 1] = (a2 - a1) / (o->yg[2] - o->yg[1]);
+  }
+  for (int ii = 1; ii <= nx; ++ii) {
+    double n11 = nu_t_mean[ii - 1], n12 = nu_t_mean[(size_t)nxg + ii - 1];
+    double n21 = nu_t_mean[ii], n22 = nu_t_mean[(size_t)nxg + ii];
+    double tau = 0.25 * (n11 + n12 + n21 + n22) * dUdy_wall[ii - 1];
+    double uvw = UV[ii - 1];
+    Cf[ii - 1] = 2.0 * (-uvw + o->nu * dUdy_wall[ii - 1] + tau) / 1.0;
+  }
+  /* inlet theta, delta99 and Reynolds numbers (statistics.f90:178-201) */
+  const double Uinf = 1.0;
+  double theta = 0.0;
+  for (int j = 2; j <= ny; ++j) {
+    double tj = Um[(size_t)(j - 1) * nx] / Uinf * (1.0 - Um[(size_t)(j - 1) * nx] / Uinf);
+    double tm = Um[(size_t)(j - 2) * nx] / Uinf * (1.0 - Um[(size_t)(j - 2) * nx] / Uinf);
+    theta = theta + 0.5 * (tj + tm) * (o->y[j] - o->y[j - 1]);
+  }
+  int jref = 0;
+  for (int j = 1; j <= ny; ++j)
+    if (Um[(size_t)(j - 1) * nx] >= 0.99 * Uinf) { jref = j; break; }
+  if (jref < 2) jref = 2;
+  double u1 = Um[(size_t)(jref - 2) * nx], u2 = Um[(size_t)(jref - 1) * nx];
+  double w1 = (0.99 * Uinf - u1) / (u2 - u1), w0 = 1.0 - w1;
+  double d99 = w1 * o->y[jref] + w0 * o->y[jref - 1];
+  sc[0] = theta;
+  sc[1] = d99;
+  sc[2] = o->x[1] * Uinf / o->nu;
+  sc[3] = theta * Uinf / o->nu;
+  sc[4] = d99 * Uinf / o->nu;
+}
+
+/* ------------------------------------------------------------------------ */
+/* equilibrium law of the wall: wallmodel.f90:1951-1985 with                */
+/* Newton_iter_solver (Newton_solver.f90:13-79): kappa 0.38, B 5.2,          */
+/* y = yg(3), 30 iterations, |f| < 1e-10.  utau (nx) is the initial guess on */
+/* entry and the model on exit; returns the largest iteration count.         */
+/* ------------------------------------------------------------------------ */
+int blo_law_of_wall(const blo_t *o, double *utau) {
+  const int jref = 3;
+  const double kap = 0.38, B = 5.20, yref = o->yg[jref], nu = o->nu;
+  int iters_max = 0;
+  for (int i = 2; i <= o->nx - 1; ++i) {
+    double x = utau[i - 1];
+    if (utau[i - 1] != utau[i - 1]) utau[i - 1] = 0.0;
+    double um = 0.0;
+    for (int k = 2; k <= o->nzg - 1; ++k) um += AU(o->U, i, jref, k);
+    um = um / (double)(o->nzg - 2);
+    int k;
+    for (k = 1; k <= 30; ++k) {
+      double fx = x / kap * log(yref * x / nu) + B * x - um;
+      double fp = 1.0 / kap * log(yref * x / nu) + 1.0 / kap + B;
+      if (fabs(fx) < 1e-10) break;
+      x = x - fx / fp;
+    }
+    int iters = k - 1;
+    utau[i - 1] = (x != x) ? 0.0 : x;
+    if (iters > iters_max) iters_max = iters;
+  }
+  utau[0] = utau[1];
+  utau[o->nx - 1] = utau[o->nx - 2];
+  return iters_max;
+}
+
+void blo_set_les(blo_t *o, int les_model) { o->les = les_model; }

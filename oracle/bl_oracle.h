@@ -47,6 +47,7 @@ void blo_set_state(blo_t *o, const double *U, const double *V,
 void blo_get_state(const blo_t *o, double *U, double *V, double *W,
                    double *P, double *t);
 void blo_set_nu_t(blo_t *o, const double *nu_t, int les_model);
+void blo_set_les(blo_t *o, int les_model); /* 1: Smagorinsky before every substep */
 
 double blo_compute_dt(blo_t *o);  /* time_integration.f90:528-591 */
 void blo_set_dt(blo_t *o, double dt);
@@ -66,6 +67,13 @@ void blo_projection(blo_t *o, int rk_step); /* projection.f90:21 */
 double blo_max_divergence(const blo_t *o);  /* projection.f90:391 */
 /* rhs_p(2:nxg-1,2:nyg-1,2:nzg) after the last projection */
 void blo_get_rhs_p(const blo_t *o, double *rhs_p);
+
+/* models and diagnostics */
+void blo_smagorinsky(blo_t *o);          /* subgrid.f90:609-730 */
+void blo_get_nu_t(const blo_t *o, double *nu_t);
+void blo_statistics(const blo_t *o, double *means, double *nu_t_mean, double *Cf,
+                    double *dUdy_wall, double *sc); /* statistics.f90:26-201 */
+int blo_law_of_wall(const blo_t *o, double *utau); /* wallmodel.f90:1951-1985 */
 
 /* test hooks for the transform and the tridiagonal solver */
 void blo_fft(int n, double *data, int inverse);
