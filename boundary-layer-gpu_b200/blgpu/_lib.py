@@ -33,6 +33,10 @@ _SIGS = {
     "blgpu_set_grid": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p]),
     "blgpu_set_boundary": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 6),
     "blgpu_set_inflow_modes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [c_double_p] * 5),
+    "blgpu_set_rescaling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, c_double_p, c_double_p]),
+    "blgpu_rescaled_inflow": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_get_rescaling": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 8 + [ctypes.POINTER(ctypes.c_int)]),
     "blgpu_set_nu_t": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "blgpu_upload_state": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, ctypes.c_double]),
     "blgpu_download_state": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 5),

@@ -81,6 +81,34 @@ class Solver:
             qs.append(np.ascontiguousarray(q.ravel(order="F")).view(np.float64))
         self._ck(self.lib.blgpu_set_inflow_modes(self.ctx, n, m, _p(zmode), _p(tmode), *[_p(q) for q in qs]))
 
+    def set_rescaling(self, mode, i_rescale, delta_inlet, T_resc, Umean0=None, Vmean0=None):
+        """Lund recycling inflow (inflow_flag 3 or 5; 0 switches it off).
+        i_rescale is the reference's 1-based Lund_ix."""
+        u = None if Umean0 is None else np.ascontiguousarray(Umean0, dtype=np.float64)
+        v = None if Vmean0 is None else np.ascontiguousarray(Vmean0, dtype=np.float64)
+        self._ck(self.lib.blgpu_set_rescaling(self.ctx, int(mode), int(i_rescale), float(delta_inlet),
+                                              float(T_resc), _p(u) if u is not None else None,
+                                              _p(v) if v is not None else None))
+
+    def rescaled_inflow(self):
+        """One compute_rescaled_inflow from the current state and dt."""
+        self._ck(self.lib.blgpu_rescaled_inflow(self.ctx))
+
+    def rescaling(self):
+        """Running means, last inflow planes and diagnostics of the Lund inflow."""
+        nyg, ny, nzg, nz = self.nyg, self.ny, self.nzg, self.nz
+        um, vm, ui, vi = np.zeros(nyg), np.zeros(ny), np.zeros(nyg), np.zeros(ny)
+        lu, lv, lw = (np.zeros((nyg, nzg), order="F"), np.zeros((ny, nzg), order="F"),
+                      np.zeros((nyg, nz), order="F"))
+        dg = np.zeros(8)
+        err = ctypes.c_int(0)
+        self._ck(self.lib.blgpu_get_rescaling(self.ctx, _p(um), _p(vm), _p(ui), _p(vi), _p(lu), _p(lv), _p(lw),
+                                              _p(dg), ctypes.byref(err)))
+        names = ["Uinf", "delta_resc", "delta_inlet", "theta_resc", "theta_inlet", "utau_resc", "utau_inlet",
+                 "gamma"]
+        return dict(Umean_resc=um, Vmean_resc=vm, Umean_inlet=ui, Vmean_inlet=vi, U=lu, V=lv, W=lw,
+                    diag=dict(zip(names, dg)), err=err.value)
+
     def set_nu_t(self, nu_t):
         a = _f64(nu_t)
         assert a.shape == (self.nxg, self.nyg, self.nzg)

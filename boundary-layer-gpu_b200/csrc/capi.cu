@@ -63,6 +63,7 @@ struct blgpu_ctx {
   double *d_stats = nullptr;
   double *d_utau = nullptr;
   int *d_iters = nullptr;
+  LundData lund{};
   int cur = 0, old = 1;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_next[3] = {0, 0, 0};
@@ -237,6 +238,30 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, (void **)&ctx->d_utau, (size_t)ctx->nx * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->d_iters, (size_t)ctx->nx * sizeof(int)));
   TRY(dalloc(ctx, (void **)&ctx->d_maxdiv, sizeof(unsigned long long)));
+  {  // Lund inflow state, FP64, laid out as described at LundData
+    const size_t nyg = ctx->nyg, ny = ctx->ny, nzg = ctx->nzg, nz = ctx->nz;
+    const size_t nd = (2 * nyg + 2 * ny + 1) + (2 * nyg + 2 * ny) + 4 * nyg + (nyg + ny) + 4 * nyg +
+                      nyg * nzg + ny * nzg + nyg * nz + 8;
+    double *d = nullptr;
+    int *ip = nullptr;
+    TRY(dalloc(ctx, (void **)&d, nd * sizeof(double)));
+    TRY(dalloc(ctx, (void **)&ip, (4 * nyg + 1) * sizeof(int)));
+    LundData &L = ctx->lund;
+    L.inst = d; d += 2 * nyg + 2 * ny + 1;
+    L.mean = d; d += 2 * nyg + 2 * ny;
+    L.rowc = d; d += 4 * nyg;
+    L.wgt = d; d += nyg + ny;
+    L.mprof = d; d += 4 * nyg;
+    L.lu = d; d += nyg * nzg;
+    L.lv = d; d += ny * nzg;
+    L.lw = d; d += nyg * nz;
+    L.diag = d;
+    L.rowi = ip;
+    L.err = ip + 4 * nyg;
+    ctx->bc.lu = L.lu;
+    ctx->bc.lv = L.lv;
+    ctx->bc.lw = L.lw;
+  }
   // transform tables
   {
     const int N = s.N, M = s.M;
@@ -547,6 +572,90 @@ int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const doubl
   return BLGPU_OK;
 }
 
+int blgpu_set_rescaling(blgpu_ctx *ctx, int mode, int i_rescale, double delta_inlet, double T_resc,
+                        const double *Umean0, const double *Vmean0) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (mode != 0 && mode != 3 && mode != 5)
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_rescaling: mode %d is not 0, 3 or 5", mode);
+  if (mode != 0 && (i_rescale < 2 || i_rescale > ctx->nx))
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_rescaling: i_rescale %d outside 2..nx", i_rescale);
+  if (mode != 0 && !(delta_inlet > 0.0 && T_resc > 0.0))
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_rescaling: delta_inlet and T_resc must be > 0");
+  if (mode != 0 && (!ctx->have_grid || !ctx->have_state))
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_set_rescaling: grid and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  drop_graphs(ctx);
+  LundData &L = ctx->lund;
+  L.mode = mode;
+  L.ir = i_rescale;
+  L.delta_inlet = delta_inlet;
+  L.T_resc = T_resc;
+  ctx->bc.lund = mode;
+  if (!mode) return BLGPU_OK;
+  // running means at start-up (initialization.f90:636-664)
+  const int nyg = ctx->nyg, ny = ctx->ny;
+  CK(cudaMemsetAsync(L.err, 0, sizeof(int), ctx->st));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_lund<double>(ctx->geo, L, S[0], S[1], S[2], ctx->sc, 0, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_lund<float>(ctx->geo, L, S[0], S[1], S[2], ctx->sc, 0, ctx->st);
+  }
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(L.mean, L.inst, (size_t)(2 * nyg + 2 * ny) * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+  double s0 = 0.0;
+  if (Umean0)
+    for (int j = 0; j < nyg; ++j) s0 += Umean0[j];
+  if (Umean0 && s0 > 1e-4) {  // restart means (input_output.f90:439-460)
+    std::vector<double> v(ny, 0.0);
+    if (Vmean0) v.assign(Vmean0, Vmean0 + ny);
+    CK(cudaMemcpyAsync(L.mean, Umean0, (size_t)nyg * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(L.mean + 2 * nyg, v.data(), (size_t)ny * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_rescaled_inflow(blgpu_ctx *ctx) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->lund.mode) return set_err(ctx, BLGPU_ESTATE, "blgpu_rescaled_inflow: rescaling is off");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_lund<double>(ctx->geo, ctx->lund, S[0], S[1], S[2], ctx->sc, 1, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_lund<float>(ctx->geo, ctx->lund, S[0], S[1], S[2], ctx->sc, 1, ctx->st);
+  }
+  ctx->launches += 3;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+int blgpu_get_rescaling(blgpu_ctx *ctx, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
+                        double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const LundData &L = ctx->lund;
+  const size_t nyg = ctx->nyg, ny = ctx->ny, nzg = ctx->nzg, nz = ctx->nz;
+  auto get = [&](double *h, const double *d, size_t n) -> int {
+    if (h) CK(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    return BLGPU_OK;
+  };
+  int rc;
+  if ((rc = get(Umean_resc, L.mean, nyg)) || (rc = get(Umean_inlet, L.mean + nyg, nyg)) ||
+      (rc = get(Vmean_resc, L.mean + 2 * nyg, ny)) || (rc = get(Vmean_inlet, L.mean + 2 * nyg + ny, ny)) ||
+      (rc = get(Lu, L.lu, nyg * nzg)) || (rc = get(Lv, L.lv, ny * nzg)) || (rc = get(Lw, L.lw, nyg * nz)) ||
+      (rc = get(diag, L.diag, 8)))
+    return rc;
+  if (err) CK(cudaMemcpyAsync(err, L.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
 }  // extern "C"
 
 // ---- host <-> box layout (staged through device memory, repacked on the GPU) ----
@@ -714,6 +823,12 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
   ph_begin(ctx, PH_MISC);
   launch_set_time(ctx->sc, 0, 0.0, ctx->st);
   ph_end(ctx, 1);
+  if (ctx->lund.mode) {  // Lund inflow once per step from the step's start fields
+    T **S = reinterpret_cast<T **>(ctx->S[a]);
+    ph_begin(ctx, PH_BC);
+    launch_lund<T>(ctx->geo, ctx->lund, S[0], S[1], S[2], ctx->sc, 1, ctx->st);
+    ph_end(ctx, 3);
+  }
   auto sub = [&](int mode, int in, int outb, double c1, double c2, double tc, int rk_step) {
     if (ctx->cfg.les_model == 1) {  // Smagorinsky from the substep's state (time_integration.f90:341-346)
       T **Si = reinterpret_cast<T **>(ctx->S[in]);

@@ -21,6 +21,25 @@ struct BcData {
   const double *zmode, *tmode;                // (n) (m)
   const double2 *qu, *qv, *qw;                // (nyg|ny, n, m) complex
   const double *ut, *vt, *wt;                 // optional precomputed inflow perturbation planes
+  int lund;                                   // 0 modes, 3 Lund plane, 5 Lund fluctuations
+  const double *lu, *lv, *lw;                 // Lund planes (nyg,nzg) (ny,nzg) (nyg,nz), j fastest
+};
+
+// Lund recycling/rescaling inflow state (rescaled_inlet_bc.f90:60-345), FP64.
+// inst and mean hold four profiles back to back: U at the recycling station
+// (nyg), U at the inlet (nyg), V at the station (ny), V at the inlet (ny);
+// inst has one more entry, the z-mean of 0.5(U(1)+U(2))V(1) at the station.
+// The four interpolation maps are m = 0 (U/W rows, wall units), 1 (U/W rows,
+// delta units), 2 (V rows, wall units), 3 (V rows, delta units), each with
+// nyg slots: rowi = -1 row 1 (left 0), 0 top value, j > 1 the pair (j-1, j).
+struct LundData {
+  int mode, ir;
+  double delta_inlet, T_resc;
+  double *inst, *mean;
+  double *rowc, *wgt, *mprof;  // rowc 4 x nyg; wgt: Weig (nyg) + Wei (ny); mprof: U inner/outer, V inner/outer
+  int *rowi, *err;
+  double *lu, *lv, *lw, *diag;  // diag: Uinf, delta_resc, delta_inlet, theta_resc, theta_inlet,
+                                //       utau_resc, utau_inlet, gamma
 };
 
 // ---- stencil.cu ----
@@ -49,6 +68,9 @@ void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, 
                   cudaStream_t st);
 template <typename T>
 void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cudaStream_t st);
+template <typename T>
+void launch_lund(const Geo &g, const LundData &L, const T *U, const T *V, const T *W, const Scalars *sc, int phase,
+                 cudaStream_t st);
 template <typename T>
 void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st);
 

@@ -465,20 +465,40 @@ __global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T
     const double t = sc->t, dt = sc->dt;
     const int nx = g.nx, nxg = g.nxg;
     // inflow (:182-190), with the temporal modes of :137-180
-    double ut = 0.0, vt = 0.0, wt = 0.0;
-    if (bc.n_modes > 0) {
-      ut = mode_sum(bc.qu, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
-      if (j <= g.ny) vt = mode_sum(bc.qv, g.ny, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
-      if (k <= g.nz) wt = mode_sum(bc.qw, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.z[k], t);
-    } else if (bc.ut) {
-      ut = bc.ut[(long long)(k - 1) * g.nyg + (j - 1)];
-      if (j <= g.ny) vt = bc.vt[(long long)(k - 1) * g.ny + (j - 1)];
-      if (k <= g.nz) wt = bc.wt[(long long)(k - 1) * g.nyg + (j - 1)];
+    // or the Lund planes of the step: flag 3 replaces the whole plane
+    // (boundary_conditions.f90:586-594), flag 5 adds the fluctuations to the
+    // inlet profile with W taken at ks = mod(k+16,nz)+1 (:527-553)
+    double u1d, v1d = 0.0, w1d = 0.0;
+    if (bc.lund == 3) {
+      u1d = bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
+      if (k <= g.nz) w1d = bc.lw[(long long)(k - 1) * g.nyg + (j - 1)];
+      if (j <= g.ny) v1d = bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
+    } else if (bc.lund == 5) {
+      u1d = bc.U_inlet[j] + bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
+      if (k <= g.nz) {
+        const int ks = (k + 16) % g.nz + 1;
+        w1d = bc.W_inlet[j] + bc.lw[(long long)(ks - 1) * g.nyg + (j - 1)];
+      }
+      if (j <= g.ny) v1d = bc.V_inlet[j] + bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
+    } else {
+      double ut = 0.0, vt = 0.0, wt = 0.0;
+      if (bc.n_modes > 0) {
+        ut = mode_sum(bc.qu, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+        if (j <= g.ny) vt = mode_sum(bc.qv, g.ny, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+        if (k <= g.nz) wt = mode_sum(bc.qw, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.z[k], t);
+      } else if (bc.ut) {
+        ut = bc.ut[(long long)(k - 1) * g.nyg + (j - 1)];
+        if (j <= g.ny) vt = bc.vt[(long long)(k - 1) * g.ny + (j - 1)];
+        if (k <= g.nz) wt = bc.wt[(long long)(k - 1) * g.nyg + (j - 1)];
+      }
+      u1d = bc.U_inlet[j] + ut;
+      if (k <= g.nz) w1d = bc.W_inlet[j] + wt;
+      if (j <= g.ny) v1d = bc.V_inlet[j] + vt;
     }
-    const T u1 = (T)(bc.U_inlet[j] + ut);
+    const T u1 = (T)u1d;
     U[bidx(g, 1, j, k)] = u1;
-    if (k <= g.nz) W[bidx(g, 1, j, k)] = (T)(bc.W_inlet[j] + wt);
-    if (j <= g.ny) V[bidx(g, 1, j, k)] = (T)(bc.V_inlet[j] + vt);
+    if (k <= g.nz) W[bidx(g, 1, j, k)] = (T)w1d;
+    if (j <= g.ny) V[bidx(g, 1, j, k)] = (T)v1d;
     // outflow (:193-201): rk_t(rk_step)*dt*Uc*(Uo(nx-1)-Uo(nx-2))/(x(nx-1)-x(nx-2))
     const double cc = rkt * dt * bc.U_top[nx];
     {
@@ -967,3 +987,194 @@ void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2,
 template void launch_repack<BLGPU_STENCIL_T>(const Geo &, int, double *, BLGPU_STENCIL_T *, int, int, int, cudaStream_t);
 
 }  // namespace blgpu
+
+#ifdef BLGPU_STENCIL_PRIMARY
+namespace blgpu {
+
+// ---------------------------------------------------------------------------
+// Lund recycling/rescaling inflow (rescaled_inlet_bc.f90:60-345), evaluated
+// once per step from the step's starting fields (the Uo, Vo, Wo of
+// boundary_conditions.f90:569-597).  All arithmetic is FP64 in this
+// translation unit (no FMA contraction), whatever the storage type T.
+//
+// k_lund_sums: one block per z-mean row (:109-125, :218-222); the 128
+// partial sums are combined in a fixed tree order.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) k_lund_sums(Geo g, LundData L, const T *__restrict__ U,
+                                                   const T *__restrict__ V) {
+  const int r = blockIdx.x, nyg = g.nyg, ny = g.ny;
+  double s = 0.0;
+  for (int k = 2 + threadIdx.x; k <= g.nzg - 1; k += blockDim.x) {
+    double v;
+    if (r < nyg) v = (double)U[bidx(g, L.ir, r + 1, k)];
+    else if (r < 2 * nyg) v = (double)U[bidx(g, 1, r - nyg + 1, k)];
+    else if (r < 2 * nyg + ny) v = (double)V[bidx(g, L.ir, r - 2 * nyg + 1, k)];
+    else if (r < 2 * nyg + 2 * ny) v = (double)V[bidx(g, 1, r - 2 * nyg - ny + 1, k)];
+    else v = 0.5 * ((double)U[bidx(g, L.ir, 1, k)] + (double)U[bidx(g, L.ir, 2, k)]) * (double)V[bidx(g, L.ir, 1, k)];
+    s += v;
+  }
+  __shared__ double red[128];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 64; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) L.inst[r] = red[0] / (double)(g.nzg - 2);
+}
+
+__device__ double lund_delta99(const double *Um, const double *yg, int nyg, double Umean99) {
+  int jref = 0;
+  for (int j = 1; j <= nyg; ++j)
+    if (Um[j - 1] >= Umean99) { jref = j; break; }
+  if (jref < 2) jref = nyg / 2;
+  const double w1 = (Umean99 - Um[jref - 2]) / (Um[jref - 1] - Um[jref - 2]);
+  const double w0 = 1.0 - w1;
+  const double d = w1 * yg[jref] + w0 * yg[jref - 1];
+  return d < 0 ? fabs(d) : d;
+}
+
+__device__ double lund_theta(const double *Um, const double *yg, int nyg, double Uinf) {
+  double th = 0.0;
+  for (int j = 2; j <= nyg; ++j) {
+    const double a = Um[j - 1] / Uinf * (1.0 - Um[j - 1] / Uinf), b = Um[j - 2] / Uinf * (1.0 - Um[j - 2] / Uinf);
+    th = th + 0.5 * (a + b) * (yg[j] - yg[j - 1]);
+  }
+  return th < 0 ? fabs(th) : th;
+}
+
+// source / target coordinate of row k of map m (:235-246)
+__device__ __forceinline__ double lund_coord(const Geo &g, int m, int k, double scale_w, double scale_d) {
+  const double *y = (m < 2) ? g.yg : g.y;
+  return (m & 1) ? y[k] / scale_d : scale_w * y[k] / g.nu;
+}
+
+// k_lund_rows: one block.  Running means (:133-137), thicknesses, friction
+// velocities and gamma (:153-231) on thread 0, then per row the
+// interpolation pair of interp_vel (:305-345), the blending weights
+// (:248-251) and the inner/outer mean profiles (:255-263, :285-289).
+__global__ void __launch_bounds__(256) k_lund_rows(Geo g, LundData L, const Scalars *__restrict__ sc) {
+  const int nyg = g.nyg, ny = g.ny, tid = threadIdx.x, nt = blockDim.x;
+  const double ra = sc->dt / L.T_resc, rb = 1.0 - sc->dt / L.T_resc;
+  for (int q = tid; q < 2 * nyg + 2 * ny; q += nt) L.mean[q] = ra * L.inst[q] + rb * L.mean[q];
+  __syncthreads();
+  __shared__ double sh[8];
+  const double *Umr = L.mean, *Umi = L.mean + nyg, *Vmr = L.mean + 2 * nyg;
+  if (tid == 0) {
+    const double Uinf = L.inst[nyg - 1];
+    const double Umean99 = 0.99 * Uinf;
+    const double d_resc = lund_delta99(Umr, g.yg, nyg, Umean99);
+    const double d_in2 = lund_delta99(Umi, g.yg, nyg, Umean99);
+    const double th_r = lund_theta(Umr, g.yg, nyg, Uinf), th_i = lund_theta(Umi, g.yg, nyg, Uinf);
+    const double uv = L.inst[2 * nyg + 2 * ny];
+    const double dUw = (Umr[1] - Umr[0]) / (g.yg[2] - g.yg[1]);
+    const double ut_r = sqrt(fabs(g.nu * dUw - uv));
+    const double ut_i = ut_r * pow(th_r / th_i, 1.0 / 8.0);
+    const double gam = ut_i / ut_r;
+    const double dg[8] = {Uinf, d_resc, d_in2, th_r, th_i, ut_r, ut_i, gam};
+    for (int q = 0; q < 8; ++q) { sh[q] = dg[q]; L.diag[q] = dg[q]; }
+  }
+  __syncthreads();
+  const double Uinf = sh[0], d_resc = sh[1], ut_r = sh[5], ut_i = sh[6], gam = sh[7];
+  const double alpha = 4.0, bb = 0.2;
+  for (int q = tid; q < 4 * nyg; q += nt) {
+    const int m = q / nyg, i = q % nyg + 1;  // target row i of map m
+    const int n1 = (m < 2) ? nyg : ny;
+    if (i > n1) continue;
+    int j = -1;
+    double coef = 0.0;
+    if (i > 1) {
+      const double yi = lund_coord(g, m, i, ut_i, L.delta_inlet);
+      j = 0;
+      for (int k = 1; k <= n1; ++k)
+        if (lund_coord(g, m, k, ut_r, d_resc) > yi) { j = k; break; }
+      if (j == 1) { atomicOr(L.err, 1); j = 0; }
+      if (j > 0) {
+        const double ysj = lund_coord(g, m, j, ut_r, d_resc), ysm = lund_coord(g, m, j - 1, ut_r, d_resc);
+        coef = (ysj - yi) / (ysj - ysm);
+      }
+    }
+    L.rowi[q] = j;
+    L.rowc[q] = coef;
+    // mean profile through the same pair
+    const double *src = (m < 2) ? Umr : Vmr;
+    double v = 0.0;
+    if (j == 0) v = src[n1 - 1];
+    else if (j > 0) v = coef * src[j - 2] + (1.0 - coef) * src[j - 1];
+    if (m == 0) v = gam * v;
+    else if (m == 1) v = gam * v + (1.0 - gam) * Uinf;
+    if (L.mode == 5) v = 0.0;  // iflag_fluc = 1 (:285-290)
+    L.mprof[q] = v;
+    if (m == 0 || m == 2) {  // inner/outer weight of row i (:248-251)
+      const double e = ((m == 0) ? g.yg[i] : g.y[i]) / L.delta_inlet;
+      L.wgt[(m == 0 ? 0 : nyg) + i - 1] = 0.5 * (1.0 + tanh(alpha * (e - bb) / ((1.0 - 2.0 * bb) * e + bb)) / tanh(alpha));
+    }
+  }
+}
+
+// fluctuation at source row r of the station plane (the mean removed for U, V)
+template <typename T>
+__device__ __forceinline__ double lund_src(const Geo &g, const LundData &L, const T *F, const double *mean, int r,
+                                           int k) {
+  const double v = (double)F[bidx(g, L.ir, r, k)];
+  return mean ? v - mean[r - 1] : v;
+}
+
+template <typename T>
+__device__ __forceinline__ double lund_interp(const Geo &g, const LundData &L, int q, int n1, const T *F,
+                                              const double *mean, int k) {
+  const int j = L.rowi[q];
+  if (j < 0) return 0.0;
+  if (j == 0) return lund_src<T>(g, L, F, mean, n1, k);
+  const double c = L.rowc[q];
+  return c * lund_src<T>(g, L, F, mean, j - 1, k) + (1.0 - c) * lund_src<T>(g, L, F, mean, j, k);
+}
+
+// k_lund_plane: the blended inflow planes (:287-298)
+template <typename T>
+__global__ void k_lund_plane(Geo g, LundData L, const T *__restrict__ U, const T *__restrict__ V,
+                             const T *__restrict__ W) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int nyg = g.nyg, ny = g.ny;
+  if (j > nyg || k > g.nzg) return;
+  const double gam = L.diag[7];
+  const double *Umr = L.mean, *Vmr = L.mean + 2 * nyg;
+  const double wg = L.wgt[j - 1];
+  {
+    const double fi = lund_interp<T>(g, L, j - 1, nyg, U, Umr, k);
+    const double fo = lund_interp<T>(g, L, nyg + j - 1, nyg, U, Umr, k);
+    L.lu[(long long)(k - 1) * nyg + (j - 1)] =
+        (L.mprof[j - 1] + gam * fi) * (1.0 - wg) + (L.mprof[nyg + j - 1] + gam * fo) * wg;
+  }
+  if (k <= g.nz) {
+    const double fi = lund_interp<T>(g, L, j - 1, nyg, W, nullptr, k);
+    const double fo = lund_interp<T>(g, L, nyg + j - 1, nyg, W, nullptr, k);
+    L.lw[(long long)(k - 1) * nyg + (j - 1)] = (gam * fi) * (1.0 - wg) + (gam * fo) * wg;
+  }
+  if (j <= ny) {
+    const double wv = L.wgt[nyg + j - 1];
+    const double fi = lund_interp<T>(g, L, 2 * nyg + j - 1, ny, V, Vmr, k);
+    const double fo = lund_interp<T>(g, L, 3 * nyg + j - 1, ny, V, Vmr, k);
+    L.lv[(long long)(k - 1) * ny + (j - 1)] =
+        (L.mprof[2 * nyg + j - 1] + gam * fi) * (1.0 - wv) + (L.mprof[3 * nyg + j - 1] + gam * fo) * wv;
+  }
+}
+
+// phase 0: z-means only (start-up of the running means); 1: full evaluation
+template <typename T>
+void launch_lund(const Geo &g, const LundData &L, const T *U, const T *V, const T *W, const Scalars *sc, int phase,
+                 cudaStream_t st) {
+  k_lund_sums<T><<<2 * g.nyg + 2 * g.ny + 1, 128, 0, st>>>(g, L, U, V);
+  if (phase == 0) return;
+  k_lund_rows<<<1, 256, 0, st>>>(g, L, sc);
+  k_lund_plane<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), dim3(32, 8), 0, st>>>(g, L, U, V, W);
+}
+template void launch_lund<double>(const Geo &, const LundData &, const double *, const double *, const double *,
+                                  const Scalars *, int, cudaStream_t);
+template void launch_lund<float>(const Geo &, const LundData &, const float *, const float *, const float *,
+                                 const Scalars *, int, cudaStream_t);
+
+}  // namespace blgpu
+#endif

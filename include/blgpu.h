@@ -81,6 +81,33 @@ int blgpu_set_boundary(blgpu_ctx *ctx, const double *U_inlet, const double *V_in
 int blgpu_set_inflow_modes(blgpu_ctx *ctx, int n_modes, int m_modes, const double *zmode, const double *tmode,
                            const double *qu, const double *qv, const double *qw);
 
+/* Lund recycling/rescaling inflow (rescaled_inlet_bc.f90:60-345), the
+ * inflow_flag 3 / 5 branches of apply_boundary_conditions
+ * (boundary_conditions.f90:35-43, 512-597).  mode 0 = off (inflow modes as
+ * above), 3 = the rescaled plane replaces the inlet plane, 5 = the rescaled
+ * fluctuations are added to U_inlet/V_inlet/W_inlet.  The plane is computed
+ * once per step on the device from the step's starting fields at
+ * x-index i_rescale (Lund_ix, 2..nx); delta_inlet = Lund_deltai, T_resc =
+ * Lund_T.  The running means start from the current device state
+ * (initialization.f90:636-664), or from Umean0(nyg)/Vmean0(ny) -- the
+ * .mean.rescaling restart means -- when Umean0 is non-null and sums above
+ * 1e-4.  Requires grid and state; replaces the GPU routine's inflow plane
+ * (boundary_conditions.f90:182-190), which the reference leaves undefined
+ * for these flags. */
+int blgpu_set_rescaling(blgpu_ctx *ctx, int mode, int i_rescale, double delta_inlet, double T_resc,
+                        const double *Umean0, const double *Vmean0);
+/* one evaluation of compute_rescaled_inflow from the current state, with the
+ * current dt (what a step does before its first boundary pass) */
+int blgpu_rescaled_inflow(blgpu_ctx *ctx);
+/* running means Umean_resc_T(nyg), Vmean_resc_T(ny), Umean_inlet_T(nyg),
+ * Vmean_inlet_T(ny); the last planes Ut_inlet(nyg,nzg), Vt_inlet(ny,nzg),
+ * Wt_inlet(nyg,nz); diag[8] = Uinf, delta_resc, delta99 at the inlet,
+ * theta_resc, theta_inlet, utau_resc, utau_inlet, gamma; err != 0 when
+ * interp_vel met its 'j==1' stop (rescaled_inlet_bc.f90:334).  Any pointer
+ * may be NULL. */
+int blgpu_get_rescaling(blgpu_ctx *ctx, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
+                        double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err);
+
 /* eddy viscosity nu_t(nxg,nyg,nzg) supplied by the host (LES = 2) */
 int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t);
 

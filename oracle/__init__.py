@@ -85,6 +85,11 @@ def load():
         lib.blo_statistics.argtypes = [ctypes.c_void_p] + [_dp] * 5
         lib.blo_law_of_wall.restype = ctypes.c_int
         lib.blo_law_of_wall.argtypes = [ctypes.c_void_p, _dp]
+        lib.blo_set_rescaling.restype = ctypes.c_int
+        lib.blo_set_rescaling.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double, _dp, _dp]
+        lib.blo_rescaled_inflow.argtypes = [ctypes.c_void_p]
+        lib.blo_get_rescaling.argtypes = [ctypes.c_void_p] + [_dp] * 8 + [ctypes.POINTER(ctypes.c_int)]
         _lib = lib
     return _lib
 
@@ -243,6 +248,33 @@ class Oracle:
         u = np.ascontiguousarray(utau_guess, dtype=np.float64).copy()
         it = self.lib.blo_law_of_wall(self.h, _p(u))
         return u, it
+
+    def set_rescaling(self, mode, i_rescale, delta_inlet, T_resc, Umean0=None, Vmean0=None):
+        u = None if Umean0 is None else np.ascontiguousarray(Umean0, dtype=np.float64)
+        v = None if Vmean0 is None else np.ascontiguousarray(Vmean0, dtype=np.float64)
+        rc = self.lib.blo_set_rescaling(self.h, mode, i_rescale, delta_inlet, T_resc,
+                                        _p(u) if u is not None else None, _p(v) if v is not None else None)
+        if rc:
+            raise ValueError("blo_set_rescaling: %d" % rc)
+
+    def rescaled_inflow(self):
+        self.lib.blo_rescaled_inflow(self.h)
+
+    def rescaling(self):
+        """Running means, inflow planes (Fortran-ordered (nyg,nzg), (ny,nzg),
+        (nyg,nz)) and diagnostics of the last Lund evaluation."""
+        nyg, ny, nzg, nz = self.nyg, self.ny, self.nzg, self.nz
+        um, vm, ui, vi = np.zeros(nyg), np.zeros(ny), np.zeros(nyg), np.zeros(ny)
+        lu, lv, lw = (np.zeros((nyg, nzg), order="F"), np.zeros((ny, nzg), order="F"),
+                      np.zeros((nyg, nz), order="F"))
+        dg = np.zeros(8)
+        err = ctypes.c_int(0)
+        self.lib.blo_get_rescaling(self.h, _p(um), _p(vm), _p(ui), _p(vi), _p(lu), _p(lv), _p(lw), _p(dg),
+                                   ctypes.byref(err))
+        names = ["Uinf", "delta_resc", "delta_inlet", "theta_resc", "theta_inlet", "utau_resc", "utau_inlet",
+                 "gamma"]
+        return dict(Umean_resc=um, Vmean_resc=vm, Umean_inlet=ui, Vmean_inlet=vi, U=lu, V=lv, W=lw,
+                    diag=dict(zip(names, dg)), err=err.value)
 
 
 def oracle_for(case, variant=0, threads=1):

@@ -317,6 +317,12 @@ struct blo {
   cplx *rhs_hat;                   /* (0:nxp-1, nm, 0:nzp-1) */
   cplx *th_dl, *th_dp, *th_du;     /* variant 1 factors (nxp, nzp, nm) */
   cplx *twid;                      /* DCT twiddle, 0..nxp-1 */
+  /* Lund recycling/rescaling inflow (rescaled_inlet_bc.f90) */
+  int resc_mode, i_rescale, lund_err;  /* mode 0 off, 3 full plane, 5 fluctuations */
+  double delta_inlet, T_resc;
+  double *Umr, *Vmr, *Umi, *Vmi;   /* Umean_resc_T(nyg) Vmean_resc_T(ny) Umean_inlet_T Vmean_inlet_T, 1-based */
+  double *Lu, *Lv, *Lw;            /* Ut_inlet(nyg,nzg) Vt_inlet(ny,nzg) Wt_inlet(nyg,nz) */
+  double lund_diag[8];
 };
 
 static int nthreads_req = 1;
@@ -373,6 +379,10 @@ blo_t *blo_create(int nx, int ny, int nz, double nu, double cfl, double dpdx,
   o->U_top = dalloc(nx + 1); o->V_top = dalloc(o->nxg + 1); o->W_top = dalloc(o->nxg + 1);
   o->Ut = dalloc((size_t)o->nyg * o->nzg); o->Vt = dalloc((size_t)ny * o->nzg);
   o->Wt = dalloc((size_t)o->nyg * nz);
+  o->Umr = dalloc(o->nyg + 1); o->Vmr = dalloc(ny + 1);
+  o->Umi = dalloc(o->nyg + 1); o->Vmi = dalloc(ny + 1);
+  o->Lu = dalloc((size_t)o->nyg * o->nzg); o->Lv = dalloc((size_t)ny * o->nzg);
+  o->Lw = dalloc((size_t)o->nyg * nz);
   o->rk_t[0] = 0.0; o->rk_t[1] = 8.0 / 15.0; o->rk_t[2] = 2.0 / 3.0; o->rk_t[3] = 1.0;
   memset(o->rk_coef, 0, sizeof(o->rk_coef));
   o->rk_coef[0][0] = 8.0 / 15.0;
@@ -393,7 +403,8 @@ void blo_destroy(blo_t *o) {
                     o->wy0, o->wy1, o->kxx, o->kzz, o->Dd, o->Dl, o->Du, o->U,
                     o->V, o->W, o->P, o->Uo, o->Vo, o->Wo, o->nu_t, o->rhs_p,
                     o->U_inlet, o->V_inlet, o->W_inlet, o->U_top, o->V_top,
-                    o->W_top, o->Ut, o->Vt, o->Wt, o->zmode, o->tmode};
+                    o->W_top, o->Ut, o->Vt, o->Wt, o->zmode, o->tmode,
+                    o->Umr, o->Vmr, o->Umi, o->Vmi, o->Lu, o->Lv, o->Lw};
   for (size_t q = 0; q < sizeof(arrs) / sizeof(arrs[0]); ++q) free(arrs[q]);
   for (int s = 0; s < 3; ++s) { free(o->Fu[s]); free(o->Fv[s]); free(o->Fw[s]); }
   free(o->qu); free(o->qv); free(o->qw);
@@ -755,8 +766,8 @@ void blo_apply_bc(blo_t *o, int rk_step) {
   double *U = o->U, *V = o->V, *W = o->W;
   const double *Uo = o->Uo, *Vo = o->Vo, *Wo = o->Wo;
   const double t = o->t, dt = o->dt;
-  /* temporal inflow modes (:137-180) */
-  if (o->n_modes > 0) {
+  /* temporal inflow modes (:137-180); a Lund inflow replaces them */
+  if (o->n_modes > 0 && o->resc_mode == 0) {
     const int nm_ = o->n_modes, mm_ = o->m_modes;
     for (int j = 1; j <= nyg; ++j)
       for (int k = 1; k <= nzg; ++k) {
@@ -792,13 +803,35 @@ void blo_apply_bc(blo_t *o, int rk_step) {
         o->Wt[(size_t)(k - 1) * nyg + (j - 1)] = acc;
       }
   }
-  /* inflow plane (:182-190) */
-  for (int j = 1; j <= nyg; ++j) {
-    for (int k = 1; k <= nzg; ++k) AU(U, 1, j, k) = o->U_inlet[j] + o->Ut[(size_t)(k - 1) * nyg + (j - 1)];
-    for (int k = 1; k <= nz; ++k) AW(W, 1, j, k) = o->W_inlet[j] + o->Wt[(size_t)(k - 1) * nyg + (j - 1)];
+  /* inflow plane (:182-190), or the plane of the Lund inflow computed at the
+   * start of the step: flag 3 sets the whole plane (:586-594), flag 5 adds
+   * the rescaled fluctuations to the inlet profile with W shifted by
+   * ks = mod(k+16,nz)+1 (:527-553) */
+  if (o->resc_mode == 3) {
+    for (int j = 1; j <= nyg; ++j) {
+      for (int k = 1; k <= nzg; ++k) AU(U, 1, j, k) = o->Lu[(size_t)(k - 1) * nyg + (j - 1)];
+      for (int k = 1; k <= nz; ++k) AW(W, 1, j, k) = o->Lw[(size_t)(k - 1) * nyg + (j - 1)];
+    }
+    for (int j = 1; j <= ny; ++j)
+      for (int k = 1; k <= nzg; ++k) AV(V, 1, j, k) = o->Lv[(size_t)(k - 1) * ny + (j - 1)];
+  } else if (o->resc_mode == 5) {
+    for (int j = 1; j <= nyg; ++j) {
+      for (int k = 1; k <= nzg; ++k) AU(U, 1, j, k) = o->U_inlet[j] + o->Lu[(size_t)(k - 1) * nyg + (j - 1)];
+      for (int k = 1; k <= nz; ++k) {
+        const int ks = (k + 16) % nz + 1;
+        AW(W, 1, j, k) = o->W_inlet[j] + o->Lw[(size_t)(ks - 1) * nyg + (j - 1)];
+      }
+    }
+    for (int j = 1; j <= ny; ++j)
+      for (int k = 1; k <= nzg; ++k) AV(V, 1, j, k) = o->V_inlet[j] + o->Lv[(size_t)(k - 1) * ny + (j - 1)];
+  } else {
+    for (int j = 1; j <= nyg; ++j) {
+      for (int k = 1; k <= nzg; ++k) AU(U, 1, j, k) = o->U_inlet[j] + o->Ut[(size_t)(k - 1) * nyg + (j - 1)];
+      for (int k = 1; k <= nz; ++k) AW(W, 1, j, k) = o->W_inlet[j] + o->Wt[(size_t)(k - 1) * nyg + (j - 1)];
+    }
+    for (int j = 1; j <= ny; ++j)
+      for (int k = 1; k <= nzg; ++k) AV(V, 1, j, k) = o->V_inlet[j] + o->Vt[(size_t)(k - 1) * ny + (j - 1)];
   }
-  for (int j = 1; j <= ny; ++j)
-    for (int k = 1; k <= nzg; ++k) AV(V, 1, j, k) = o->V_inlet[j] + o->Vt[(size_t)(k - 1) * ny + (j - 1)];
   /* convective outflow (:193-201) */
   const double Uc = o->U_top[nx];
   const double c = o->rk_t[rk_step] * dt * Uc;
@@ -1155,6 +1188,231 @@ static void rk_update(blo_t *o, int nterms, const double *a) {
       }
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* Lund recycling/rescaling inflow: rescaled_inlet_bc.f90:60-345           */
+/* ------------------------------------------------------------------------ */
+
+/* interp_vel (rescaled_inlet_bc.f90:305-345): for each target row i = 2..n1,
+ * the first source row j with ys(j) > yi(i) selects the pair (j-1, j); none
+ * selects the top row n1; j == 1 is the reference's stop (flagged here).
+ * src(n1, ncol) and dst(n1, ncol) are column-major; ys, yi are 1-based.
+ * Row 1 is never written by the reference (its value is undefined there and
+ * the wall condition overwrites the inflow cells it feeds); it is 0 here. */
+static void lund_interp(const double *src, int n1, int ncol, const double *ys, const double *yi,
+                        double *dst, int *err) {
+  for (int c = 0; c < ncol; ++c) dst[(size_t)c * n1] = 0.0;
+  for (int i = 2; i <= n1; ++i) {
+    int j = 0;
+    for (int k = 1; k <= n1; ++k)
+      if (ys[k] > yi[i]) { j = k; break; }
+    if (j == 1) { *err = 1; j = 0; }
+    if (j > 0) {
+      const double coef = (ys[j] - yi[i]) / (ys[j] - ys[j - 1]);
+      for (int c = 0; c < ncol; ++c)
+        dst[(size_t)c * n1 + (i - 1)] = coef * src[(size_t)c * n1 + (j - 2)] + (1.0 - coef) * src[(size_t)c * n1 + (j - 1)];
+    } else {
+      for (int c = 0; c < ncol; ++c) dst[(size_t)c * n1 + (i - 1)] = src[(size_t)c * n1 + (n1 - 1)];
+    }
+  }
+}
+
+/* delta_99 by linear interpolation of a mean profile (:148-182) */
+static double lund_delta99(const blo_t *o, const double *Um, double Umean99) {
+  int jref = 0;
+  for (int j = 1; j <= o->nyg; ++j)
+    if (Um[j] >= Umean99) { jref = j; break; }
+  if (jref < 2) jref = o->nyg / 2;
+  const double w1 = (Umean99 - Um[jref - 1]) / (Um[jref] - Um[jref - 1]);
+  const double w0 = 1.0 - w1;
+  double d = w1 * o->yg[jref] + w0 * o->yg[jref - 1];
+  return d < 0 ? fabs(d) : d;
+}
+
+/* momentum thickness by the trapezoidal rule over the centres (:188-210) */
+static double lund_theta(const blo_t *o, const double *Um, double Uinf) {
+  double th = 0.0;
+  for (int j = 2; j <= o->nyg; ++j) {
+    const double a = Um[j] / Uinf * (1.0 - Um[j] / Uinf), b = Um[j - 1] / Uinf * (1.0 - Um[j - 1] / Uinf);
+    th = th + 0.5 * (a + b) * (o->yg[j] - o->yg[j - 1]);
+  }
+  return th < 0 ? fabs(th) : th;
+}
+
+/* compute_rescaled_inflow (:60-300) from the fields U_,V_,W_ (the step's
+ * Uo, Vo, Wo); fluc = iflag_fluc.  Updates the running means and writes the
+ * planes Lu(nyg,nzg), Lv(ny,nzg), Lw(nyg,nz). */
+static void lund_inflow(blo_t *o, const double *U_, const double *V_, const double *W_, int fluc) {
+  const int ny = o->ny, nyg = o->nyg, nz = o->nz, nzg = o->nzg, ir = o->i_rescale;
+  const double nu = o->nu;
+  double *Ur = dalloc((size_t)nyg * nzg), *Vr = dalloc((size_t)ny * nzg), *Wr = dalloc((size_t)nyg * nz);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j) Ur[(size_t)(k - 1) * nyg + (j - 1)] = AU(U_, ir, j, k);
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= ny; ++j) Vr[(size_t)(k - 1) * ny + (j - 1)] = AV(V_, ir, j, k);
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= nyg; ++j) Wr[(size_t)(k - 1) * nyg + (j - 1)] = AW(W_, ir, j, k);
+  /* instantaneous z-means (:109-125) and their running averages (:133-137) */
+  double *Umr_i = dalloc(nyg + 1), *Vmr_i = dalloc(ny + 1), *Umi_i = dalloc(nyg + 1), *Vmi_i = dalloc(ny + 1);
+  const double dn = (double)(nzg - 2);
+  for (int j = 1; j <= nyg; ++j) {
+    double a = 0.0, b = 0.0;
+    for (int k = 2; k <= nzg - 1; ++k) { a += AU(U_, ir, j, k); b += AU(U_, 1, j, k); }
+    Umr_i[j] = a / dn;
+    Umi_i[j] = b / dn;
+  }
+  for (int j = 1; j <= ny; ++j) {
+    double a = 0.0, b = 0.0;
+    for (int k = 2; k <= nzg - 1; ++k) { a += AV(V_, ir, j, k); b += AV(V_, 1, j, k); }
+    Vmr_i[j] = a / dn;
+    Vmi_i[j] = b / dn;
+  }
+  const double Uinf = Umr_i[nyg];
+  const double ra = o->dt / o->T_resc, rb = 1.0 - o->dt / o->T_resc;
+  for (int j = 1; j <= nyg; ++j) {
+    o->Umr[j] = ra * Umr_i[j] + rb * o->Umr[j];
+    o->Umi[j] = ra * Umi_i[j] + rb * o->Umi[j];
+  }
+  for (int j = 1; j <= ny; ++j) {
+    o->Vmr[j] = ra * Vmr_i[j] + rb * o->Vmr[j];
+    o->Vmi[j] = ra * Vmi_i[j] + rb * o->Vmi[j];
+  }
+  /* fluctuations at the recycling station (:141-150; the inlet ones are unused) */
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j) Ur[(size_t)(k - 1) * nyg + (j - 1)] -= o->Umr[j];
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= ny; ++j) Vr[(size_t)(k - 1) * ny + (j - 1)] -= o->Vmr[j];
+  /* thicknesses (:153-210) */
+  const double Umean99 = 0.99 * Uinf;
+  const double delta_resc = lund_delta99(o, o->Umr, Umean99);
+  const double delta_inlet2 = lund_delta99(o, o->Umi, Umean99);
+  const double theta_resc = lund_theta(o, o->Umr, Uinf), theta_inlet = lund_theta(o, o->Umi, Uinf);
+  /* friction velocities (:214-231); the wall product uses the plane before
+   * the mean is removed */
+  double uv = 0.0;
+  for (int k = 2; k <= nzg - 1; ++k)
+    uv += 0.5 * (AU(U_, ir, 1, k) + AU(U_, ir, 2, k)) * AV(V_, ir, 1, k);
+  uv = uv / dn;
+  const double dUw = (o->Umr[2] - o->Umr[1]) / (o->yg[2] - o->yg[1]);
+  const double utau_resc = sqrt(fabs(nu * dUw - uv));
+  const double utau_inlet = utau_resc * pow(theta_resc / theta_inlet, 1.0 / 8.0);
+  const double gamma = utau_inlet / utau_resc;
+  /* inner (wall units) and outer (delta_99 units) coordinates (:235-246) */
+  double *ygp_i = dalloc(nyg + 1), *ygp_r = dalloc(nyg + 1), *etg_i = dalloc(nyg + 1), *etg_r = dalloc(nyg + 1);
+  double *yp_i = dalloc(ny + 1), *yp_r = dalloc(ny + 1), *et_i = dalloc(ny + 1), *et_r = dalloc(ny + 1);
+  double *Weig = dalloc(nyg + 1), *Wei = dalloc(ny + 1);
+  const double alpha = 4.0, bb = 0.2;
+  for (int j = 1; j <= nyg; ++j) {
+    ygp_i[j] = utau_inlet * o->yg[j] / nu;
+    ygp_r[j] = utau_resc * o->yg[j] / nu;
+    etg_i[j] = o->yg[j] / o->delta_inlet;
+    etg_r[j] = o->yg[j] / delta_resc;
+    Weig[j] = 0.5 * (1.0 + tanh(alpha * (etg_i[j] - bb) / ((1.0 - 2.0 * bb) * etg_i[j] + bb)) / tanh(alpha));
+  }
+  for (int j = 1; j <= ny; ++j) {
+    yp_i[j] = utau_inlet * o->y[j] / nu;
+    yp_r[j] = utau_resc * o->y[j] / nu;
+    et_i[j] = o->y[j] / o->delta_inlet;
+    et_r[j] = o->y[j] / delta_resc;
+    Wei[j] = 0.5 * (1.0 + tanh(alpha * (et_i[j] - bb) / ((1.0 - 2.0 * bb) * et_i[j] + bb)) / tanh(alpha));
+  }
+  /* inner and outer components (:255-283) */
+  int err = 0;
+  double *Umi_n = dalloc(nyg), *Umo_n = dalloc(nyg), *Vmi_n = dalloc(ny), *Vmo_n = dalloc(ny);
+  lund_interp(o->Umr + 1, nyg, 1, ygp_r, ygp_i, Umi_n, &err);
+  lund_interp(o->Umr + 1, nyg, 1, etg_r, etg_i, Umo_n, &err);
+  lund_interp(o->Vmr + 1, ny, 1, yp_r, yp_i, Vmi_n, &err);
+  lund_interp(o->Vmr + 1, ny, 1, et_r, et_i, Vmo_n, &err);
+  for (int j = 0; j < nyg; ++j) {
+    Umi_n[j] = gamma * Umi_n[j];
+    Umo_n[j] = gamma * Umo_n[j] + (1.0 - gamma) * Uinf;
+  }
+  double *Ufi = dalloc((size_t)nyg * nzg), *Ufo = dalloc((size_t)nyg * nzg);
+  double *Vfi = dalloc((size_t)ny * nzg), *Vfo = dalloc((size_t)ny * nzg);
+  double *Wfi = dalloc((size_t)nyg * nz), *Wfo = dalloc((size_t)nyg * nz);
+  lund_interp(Ur, nyg, nzg, ygp_r, ygp_i, Ufi, &err);
+  lund_interp(Ur, nyg, nzg, etg_r, etg_i, Ufo, &err);
+  lund_interp(Vr, ny, nzg, yp_r, yp_i, Vfi, &err);
+  lund_interp(Vr, ny, nzg, et_r, et_i, Vfo, &err);
+  lund_interp(Wr, nyg, nz, ygp_r, ygp_i, Wfi, &err);
+  lund_interp(Wr, nyg, nz, etg_r, etg_i, Wfo, &err);
+  if (fluc) {
+    for (int j = 0; j < nyg; ++j) Umi_n[j] = Umo_n[j] = 0.0;
+    for (int j = 0; j < ny; ++j) Vmi_n[j] = Vmo_n[j] = 0.0;
+  }
+  /* blend (:287-298) */
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j) {
+      const size_t q = (size_t)(k - 1) * nyg + (j - 1);
+      o->Lu[q] = (Umi_n[j - 1] + gamma * Ufi[q]) * (1.0 - Weig[j]) + (Umo_n[j - 1] + gamma * Ufo[q]) * Weig[j];
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= nyg; ++j) {
+      const size_t q = (size_t)(k - 1) * nyg + (j - 1);
+      o->Lw[q] = (gamma * Wfi[q]) * (1.0 - Weig[j]) + (gamma * Wfo[q]) * Weig[j];
+    }
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const size_t q = (size_t)(k - 1) * ny + (j - 1);
+      o->Lv[q] = (Vmi_n[j - 1] + gamma * Vfi[q]) * (1.0 - Wei[j]) + (Vmo_n[j - 1] + gamma * Vfo[q]) * Wei[j];
+    }
+  o->lund_err |= err;
+  double dg[8] = {Uinf, delta_resc, delta_inlet2, theta_resc, theta_inlet, utau_resc, utau_inlet, gamma};
+  memcpy(o->lund_diag, dg, sizeof(dg));
+  double *fr[] = {Ur, Vr, Wr, Umr_i, Vmr_i, Umi_i, Vmi_i, ygp_i, ygp_r, etg_i, etg_r, yp_i, yp_r, et_i, et_r,
+                  Weig, Wei, Umi_n, Umo_n, Vmi_n, Vmo_n, Ufi, Ufo, Vfi, Vfo, Wfi, Wfo};
+  for (size_t q = 0; q < sizeof(fr) / sizeof(fr[0]); ++q) free(fr[q]);
+}
+
+/* running means at start-up (initialization.f90:636-664): taken from the
+ * restart file's means when their sum exceeds 1e-4, else from the field */
+int blo_set_rescaling(blo_t *o, int mode, int i_rescale, double delta_inlet, double T_resc,
+                      const double *Umean0, const double *Vmean0) {
+  if (mode != 0 && mode != 3 && mode != 5) return -1;
+  if (mode != 0 && (i_rescale < 2 || i_rescale > o->nx)) return -2;
+  o->resc_mode = mode;
+  o->i_rescale = i_rescale;
+  o->delta_inlet = delta_inlet;
+  o->T_resc = T_resc;
+  o->lund_err = 0;
+  if (!mode) return 0;
+  const double dn = (double)(o->nzg - 2);
+  double s0 = 0.0;
+  if (Umean0)
+    for (int j = 0; j < o->nyg; ++j) s0 += Umean0[j];
+  for (int j = 1; j <= o->nyg; ++j) {
+    double a = 0.0, b = 0.0;
+    for (int k = 2; k <= o->nzg - 1; ++k) { a += AU(o->U, i_rescale, j, k); b += AU(o->U, 1, j, k); }
+    o->Umr[j] = (Umean0 && s0 > 1e-4) ? Umean0[j - 1] : a / dn;
+    o->Umi[j] = b / dn;
+  }
+  for (int j = 1; j <= o->ny; ++j) {
+    double a = 0.0, b = 0.0;
+    for (int k = 2; k <= o->nzg - 1; ++k) { a += AV(o->V, i_rescale, j, k); b += AV(o->V, 1, j, k); }
+    o->Vmr[j] = (Umean0 && s0 > 1e-4) ? (Vmean0 ? Vmean0[j - 1] : 0.0) : a / dn;
+    o->Vmi[j] = b / dn;
+  }
+  return 0;
+}
+
+/* one evaluation from the current state (the test hook of the step-start call) */
+void blo_rescaled_inflow(blo_t *o) {
+  if (o->resc_mode) lund_inflow(o, o->U, o->V, o->W, o->resc_mode == 5);
+}
+
+void blo_get_rescaling(const blo_t *o, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
+                       double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err) {
+  if (Umean_resc) memcpy(Umean_resc, o->Umr + 1, sizeof(double) * o->nyg);
+  if (Vmean_resc) memcpy(Vmean_resc, o->Vmr + 1, sizeof(double) * o->ny);
+  if (Umean_inlet) memcpy(Umean_inlet, o->Umi + 1, sizeof(double) * o->nyg);
+  if (Vmean_inlet) memcpy(Vmean_inlet, o->Vmi + 1, sizeof(double) * o->ny);
+  if (Lu) memcpy(Lu, o->Lu, sizeof(double) * (size_t)o->nyg * o->nzg);
+  if (Lv) memcpy(Lv, o->Lv, sizeof(double) * (size_t)o->ny * o->nzg);
+  if (Lw) memcpy(Lw, o->Lw, sizeof(double) * (size_t)o->nyg * o->nz);
+  if (diag) memcpy(diag, o->lund_diag, sizeof(o->lund_diag));
+  if (err) *err = o->lund_err;
+}
+
 void blo_smagorinsky(blo_t *o);
 static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms,
                     double tnew) {
@@ -1173,6 +1431,8 @@ static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms
 void blo_step(blo_t *o) {
   const double to = o->t, dt = o->dt;
   save_state(o);
+  /* Lund inflow once per step from Uo (boundary_conditions.f90:569-597) */
+  if (o->resc_mode) lund_inflow(o, o->Uo, o->Vo, o->Wo, o->resc_mode == 5);
   if (o->rk_scheme == 3) {
     double a1[1] = {o->rk_coef[0][0]};
     substep(o, 0, 1, a1, 1, to + o->rk_t[1] * dt);
@@ -1216,6 +1476,7 @@ void blo_rk3_stage(blo_t *o, int stage) {
   if (stage == 1) {
     stage_to = o->t;
     save_state(o);
+    if (o->resc_mode) lund_inflow(o, o->Uo, o->Vo, o->Wo, o->resc_mode == 5);
     double a1[1] = {o->rk_coef[0][0]};
     substep(o, 0, 1, a1, 1, stage_to + o->rk_t[1] * o->dt);
   } else if (stage == 2) {

@@ -75,6 +75,17 @@ void blo_statistics(const blo_t *o, double *means, double *nu_t_mean, double *Cf
                     double *dUdy_wall, double *sc); /* statistics.f90:26-201 */
 int blo_law_of_wall(const blo_t *o, double *utau); /* wallmodel.f90:1951-1985 */
 
+/* Lund recycling/rescaling inflow (rescaled_inlet_bc.f90:60-345); mode 0 off,
+ * 3 = whole inlet plane (inflow flag 3), 5 = fluctuations added to the inlet
+ * profile (flag 5).  Umean0(nyg)/Vmean0(ny): restart means or NULL. */
+int blo_set_rescaling(blo_t *o, int mode, int i_rescale, double delta_inlet, double T_resc,
+                      const double *Umean0, const double *Vmean0);
+void blo_rescaled_inflow(blo_t *o);
+/* diag: Uinf, delta_resc, delta_inlet, theta_resc, theta_inlet, utau_resc,
+ * utau_inlet, gamma */
+void blo_get_rescaling(const blo_t *o, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
+                       double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err);
+
 /* test hooks for the transform and the tridiagonal solver */
 void blo_fft(int n, double *data, int inverse);
 int blo_zgtsv(int n, double *dl, double *d, double *du, double *b);

@@ -1,0 +1,143 @@
+"""Device Lund recycling/rescaling inflow (rescaled_inlet_bc.f90:60-345) against
+the oracle: one evaluation (running means, thicknesses, friction velocities,
+gamma and the three inflow planes), whole steps with inflow flags 3 and 5 in
+FP64 and in the mixed form, the rescaling identity (station plane reproduced
+when the inlet is the station and delta_inlet = delta_resc), and argument
+errors."""
+import numpy as np
+import pytest
+
+import oracle
+from blgpu import cases, FP64, MIXED, BlgpuError
+
+pytestmark = pytest.mark.gpu
+
+IR = 16
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def turb(nx=64, ny=40, nz=24, seed=3, dt=0.05):
+    c = cases.turbulent_case(nx=nx, ny=ny, nz=nz, seed=seed, cfl=-dt)
+    return c
+
+
+def pair(c, mode, precision=FP64, delta_inlet=1.0, T_resc=10.0):
+    s = cases.solver_for(c, precision=precision)
+    s.set_dt(-c.cfl)
+    s.set_rescaling(mode, IR, delta_inlet, T_resc)
+    o = oracle.oracle_for(c)
+    o.set_rescaling(mode, IR, delta_inlet, T_resc)
+    return s, o
+
+
+@pytest.mark.parametrize("mode", [3, 5])
+def test_one_evaluation_matches_oracle(gpu, mode):
+    c = turb()
+    s, o = pair(c, mode)
+    s.rescaled_inflow()
+    o.rescaled_inflow()
+    a, b = s.rescaling(), o.rescaling()
+    assert a["err"] == 0 and b["err"] == 0
+    for n in ("Umean_resc", "Vmean_resc", "Umean_inlet", "Vmean_inlet"):
+        assert np.abs(a[n] - b[n]).max() <= 1e-14 * max(1.0, np.abs(b[n]).max()), n
+    for n, v in b["diag"].items():
+        assert abs(a["diag"][n] - v) <= 1e-12 * max(abs(v), 1e-300), (n, a["diag"][n], v)
+    for n in ("U", "V", "W"):
+        scale = max(np.abs(b[n]).max(), 1e-300)
+        assert np.abs(a[n] - b[n]).max() <= 1e-12 * scale, n
+    s.close()
+
+
+def test_identity_when_inlet_is_station(gpu):
+    c = turb(seed=4)
+    for F in (c.U, c.V, c.W):
+        F[0] = F[IR - 1]
+    s, o = pair(c, 3)
+    s.rescaled_inflow()
+    d = s.rescaling()["diag"]["delta_resc"]
+    s.set_rescaling(3, IR, d, 10.0)
+    s.rescaled_inflow()
+    r = s.rescaling()
+    assert r["diag"]["gamma"] == 1.0
+    for F, L in ((c.U, r["U"]), (c.V, r["V"]), (c.W, r["W"])):
+        assert np.abs(F[IR - 1][1:] - L[1:]).max() <= 1e-14 * np.abs(F).max()
+    s.close()
+
+
+@pytest.mark.parametrize("mode", [3, 5])
+def test_fp64_steps_match_oracle(gpu, mode):
+    c = turb(seed=5)
+    s, o = pair(c, mode)
+    for _ in range(4):
+        s.time_step()
+        o.step()
+    U, V, W, _, _ = s.download_state()
+    Ur, Vr, Wr, _, _ = o.state()
+    assert rel(U, Ur) < 1e-10 and rel(V, Vr) < 1e-10 and rel(W, Wr) < 1e-10
+    a, b = s.rescaling(), o.rescaling()
+    assert np.abs(a["Umean_resc"] - b["Umean_resc"]).max() < 1e-12
+    assert np.abs(a["U"] - b["U"]).max() < 1e-10
+    assert s.check_divergence() < 1e-10
+    s.close()
+
+
+def test_graph_advance_matches_time_step(gpu):
+    c = turb(seed=6)
+    s1, _ = pair(c, 3)
+    s2, _ = pair(c, 3)
+    for _ in range(3):
+        s1.time_step()
+    s2.advance(3)
+    A, B = s1.download_state(), s2.download_state()
+    for x, y in zip(A[:3], B[:3]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(s1.rescaling()["U"], s2.rescaling()["U"])
+    s1.close()
+    s2.close()
+
+
+def test_mixed_steps_close_to_oracle(gpu):
+    c = turb(seed=7)
+    s, o = pair(c, 3, precision=MIXED)
+    for _ in range(4):
+        s.time_step()
+        o.step()
+    U, V, W, _, _ = s.download_state()
+    Ur, Vr, Wr, _, _ = o.state()
+    assert rel(U, Ur) < 1e-5 and rel(V, Vr) < 1e-4 and rel(W, Wr) < 1e-4
+    s.close()
+
+
+def test_restart_means_are_used(gpu):
+    c = turb(seed=8)
+    s = cases.solver_for(c)
+    s.set_dt(-c.cfl)
+    um = np.linspace(0.0, 1.0, c.ny + 1)
+    vm = np.full(c.ny, 1e-3)
+    s.set_rescaling(3, IR, 1.0, 10.0, Umean0=um, Vmean0=vm)
+    r = s.rescaling()
+    assert np.array_equal(r["Umean_resc"], um) and np.array_equal(r["Vmean_resc"], vm)
+    o = oracle.oracle_for(c)
+    o.set_rescaling(3, IR, 1.0, 10.0, Umean0=um, Vmean0=vm)
+    s.rescaled_inflow()
+    o.rescaled_inflow()
+    assert np.abs(s.rescaling()["U"] - o.rescaling()["U"]).max() < 1e-12
+    s.close()
+
+
+def test_rescaling_errors(gpu):
+    c = turb()
+    s = cases.solver_for(c)
+    with pytest.raises(BlgpuError):
+        s.set_rescaling(4, IR, 1.0, 1.0)
+    with pytest.raises(BlgpuError):
+        s.set_rescaling(3, c.nx + 1, 1.0, 1.0)
+    with pytest.raises(BlgpuError):
+        s.set_rescaling(3, IR, 0.0, 1.0)
+    with pytest.raises(BlgpuError):
+        s.rescaled_inflow()
+    s.close()

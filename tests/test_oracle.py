@@ -91,3 +91,42 @@ def test_compute_dt_uses_max_as_written():
     xg, yg, zg = cases.centres_ghost(c.x), cases.centres_ghost(c.y), cases.centres_ghost(c.z)
     dt_vis = min(c.cfl * np.diff(xg).min() ** 2, c.cfl * np.diff(yg).min() ** 2, c.cfl * np.diff(zg).min() ** 2) / c.nu
     assert dt == pytest.approx(dt_vis, rel=1e-15)
+
+
+def test_lund_identity_when_inlet_is_station():
+    """With the inlet plane equal to the recycling plane and delta_inlet set
+    to the station's delta_99, gamma = 1 and every interpolation pair
+    collapses to its own row: the rescaled plane is the station plane."""
+    from blgpu import cases
+    c = cases.turbulent_case(nx=40, ny=32, nz=16, seed=3)
+    ir = 12
+    for F in (c.U, c.V, c.W):
+        F[0] = F[ir - 1]
+    o = oracle.oracle_for(c)
+    o.set_dt(0.01)
+    o.set_rescaling(3, ir, 1.0, 10.0)
+    o.rescaled_inflow()
+    d = o.rescaling()["diag"]["delta_resc"]
+    o.set_rescaling(3, ir, d, 10.0)
+    o.rescaled_inflow()
+    r = o.rescaling()
+    assert r["diag"]["gamma"] == 1.0 and r["err"] == 0
+    for F, L in ((c.U, r["U"]), (c.V, r["V"]), (c.W, r["W"])):
+        assert np.abs(F[ir - 1][1:] - L[1:]).max() <= 1e-14 * np.abs(F).max()
+
+
+def test_lund_gamma_follows_momentum_thickness():
+    """gamma = (theta_resc/theta_inlet)^(1/8) (rescaled_inlet_bc.f90:230) and
+    the running means move by dt/T_resc toward the instantaneous means."""
+    from blgpu import cases
+    c = cases.turbulent_case(nx=40, ny=32, nz=16, seed=4)
+    o = oracle.oracle_for(c)
+    o.set_dt(0.5)
+    o.set_rescaling(3, 20, 1.0, 5.0)
+    m0 = o.rescaling()["Umean_resc"].copy()
+    o.rescaled_inflow()
+    r = o.rescaling()
+    d = r["diag"]
+    assert abs(d["gamma"] - (d["theta_resc"] / d["theta_inlet"]) ** 0.125) < 1e-14
+    inst = c.U[19, :, 1:-1].mean(axis=1)
+    assert np.allclose(r["Umean_resc"], 0.1 * inst + 0.9 * m0, rtol=0, atol=1e-14)
