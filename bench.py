@@ -47,6 +47,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-boxes", type=int, default=64)
+    ap.add_argument("--ens-steps", type=int, default=20)
+    ap.add_argument("--profile", default=None, choices=["mixed", "fp64", "ensemble"],
+                    help="profiling driver: set up, warm up, then run --steps steps between "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); prints one line")
     return ap.parse_args()
 
 
@@ -183,8 +189,8 @@ def run_reference(args, rank, world, pg):
             "warmup": args.warmup, "ms_per_step": 3.0 * per_sub * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "turbulent BL %dx%dx%d RK3 CFL 0.5 (CPU restatement of the reference step)"
-                                   % (args.nx, args.ny, args.nz), "cells": case.cells},
+            "config": {"workload": "turbulent BL %dx%dx%d RK3 CFL 0.5, Lund inflow (flag 3), CPU restatement of "
+                                   "the reference step" % (args.nx, args.ny, args.nz), "cells": case.cells},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": "one RK3 substep of the full box per timed step, x3 per step"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -206,8 +212,87 @@ def cpu_baseline(args):
             "sample": "one RK3 substep (stage 1) of the full %dx%dx%d box, x3" % (args.nx, args.ny, args.nz)}
 
 
+def ensemble_boxes(args, dev, seed_offset=0):
+    """The batched ensemble: uneven turbulent boxes with Lund inflow, mixed form."""
+    import blgpu
+    from blgpu import cases
+    cs = cases.ensemble_cases(nbox=args.ens_boxes, seed=2024 + seed_offset)
+    return cs, [cases.solver_for(c, precision=blgpu.MIXED, device=dev) for c in cs]
+
+
+def run_ensemble(args, dev, pg, local, world):
+    """Aggregate cells*steps/s of the ensemble in one graph launch per step,
+    against the same boxes advanced one after another."""
+    import blgpu
+    cs, box = ensemble_boxes(args, dev, seed_offset=int(os.environ.get("RANK", "0")))
+    ens = blgpu.Ensemble(box)
+    cells = ens.cells
+    t0 = time.perf_counter()
+    ens.advance(args.warmup)
+    ens.sync()
+    ms_default = ens.time(args.ens_steps) / args.ens_steps
+    ms_seq_default = ens.time(args.ens_steps, sequential=True) / args.ens_steps
+    ntuned = ens.autotune(steps=3)
+    tune_s = time.perf_counter() - t0
+    ens.advance(1)
+    ens.sync()
+    barrier(pg, local)
+    ms = allmax(pg, ens.time(args.ens_steps), local) / args.ens_steps
+    ms_seq = allmax(pg, ens.time(args.ens_steps, sequential=True), local) / args.ens_steps
+    shapes = sorted({(s.nx, s.ny, s.nz) for s in box})
+    tiles = {"%dx%dx%d" % sh: next(s.tiles() for s in box if (s.nx, s.ny, s.nz) == sh) for sh in shapes}
+    out = {"boxes": len(box), "cells": cells, "steps_timed": args.ens_steps, "precision": "mixed",
+           "recipe": "nx in {128,192,256}, ny 65, nz in {64,96}, Re_theta in [800,1500], Lund inflow, RK3 CFL 0.5",
+           "ms_per_step": ms, "cells_steps_per_s": cells * world / (ms * 1e-3),
+           "ns_per_cell_step": ms * 1e6 / (cells * world),
+           "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms,
+           "before_autotune": {"ms_per_step": ms_default, "sequential_ms_per_step": ms_seq_default},
+           "autotuned_shapes": ntuned, "tiles": tiles, "setup_and_tune_s": tune_s,
+           "graph_launches_per_step": 1, "kernels_per_step": None}
+    l0 = ens.launches()
+    ens.advance(1)
+    out["kernels_per_step"] = ens.launches() - l0
+    ens.close()
+    for s in box:
+        s.close()
+    return out
+
+
+def run_profile(args):
+    """Small driver for ncu: set-up and warm-up outside the profiled range."""
+    import torch
+    import blgpu
+    from blgpu import cases
+    torch.cuda.set_device(0)
+    if args.profile == "ensemble":
+        _, box = ensemble_boxes(args, 0)
+        ens = blgpu.Ensemble(box)
+        ens.advance(args.warmup)
+        ens.sync()
+        torch.cuda.profiler.start()
+        ens.advance(args.steps)
+        ens.sync()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile": "ensemble", "boxes": len(box), "steps": args.steps}))
+        return
+    case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz)
+    prec = blgpu.MIXED if args.profile == "mixed" else blgpu.FP64
+    s = cases.solver_for(case, precision=prec)
+    s.advance(args.warmup)
+    s.sync()
+    torch.cuda.profiler.start()
+    s.advance(args.steps)
+    s.sync()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile": args.profile, "grid": [args.nx, args.ny, args.nz], "steps": args.steps,
+                      "max_div": s.check_divergence()}))
+
+
 def main():
     args = parse()
+    if args.profile:
+        run_profile(args)
+        return
     rank, world, local, pg = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, rank, world, pg)
@@ -310,6 +395,9 @@ def main():
            "d2h_bytes_per_step": bytes_state, "steps": e2e_n,
            "what": "upload_state + advance(1) + download_state per step, FP64 Fortran-layout pinned host arrays"}
     smix.close()
+    ens = None
+    if not args.no_ensemble:
+        ens = run_ensemble(args, dev, pg, local, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -318,7 +406,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_step_mix, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 fields / f64 Thomas", "data": "synthetic",
                 "config": {"workload": "turbulent BL DNS %dx%dx%d (%d cells), RK3 CFL 0.5, Re_theta 1100, "
-                                       "mixed FP32/FP64" % (case.nx, case.ny, case.nz, cells),
+                                       "Lund inflow (flag 3, station i=%d), mixed FP32/FP64"
+                                       % (case.nx, case.ny, case.nz, cells, case.lund[1]),
                            "cells": cells, "l2": "inputs larger than L2 (3 x %.0f MB per state)"
                                                   % (smix_bytes(case, 4) / 1e6),
                            "replicas_per_gpu": 1},
@@ -328,7 +417,7 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk, "phases_ms_per_step_mixed": {k: v[0] / 2.0 for k, v in ph.items()},
                 "phases_ms_per_step_fp64": ({k: v[0] for k, v in ph64.items()} if fp64 else None),
-                "eager_step_ms_mixed": step_ms}
+                "eager_step_ms_mixed": step_ms, "ensemble": ens}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

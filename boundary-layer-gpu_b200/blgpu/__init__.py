@@ -1,8 +1,10 @@
 """blgpu -- B200 step path of the boundary-layer DNS solver (host side).
 
 Solver      the reference's step-path subroutines over the C ABI
+Ensemble    independent boxes advanced by one graph launch per step
 cases       grids, Blasius/turbulent inflow and synthetic initial fields
 """
 from ._lib import FP64, MIXED, POISSON_NATIVE, POISSON_CUFFT, BlgpuError, load  # noqa: F401
 from .solver import Solver  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401
 from . import cases  # noqa: F401

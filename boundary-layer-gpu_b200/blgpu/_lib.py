@@ -62,6 +62,19 @@ _SIGS = {
     "blgpu_law_of_wall": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int)]),
     "blgpu_check_divergence_noalloc": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
                                        + [ctypes.c_void_p, ctypes.c_void_p]),
+    "blgpu_set_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "blgpu_get_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "blgpu_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p, c_double_p]),
+    "blgpu_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_void_p)]),
+    "blgpu_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "blgpu_ensemble_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_ensemble_advance_sequential": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_ensemble_time": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_double_p]),
+    "blgpu_ensemble_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_ensemble_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "blgpu_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
 }
 
 PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]
@@ -97,4 +110,10 @@ class BlgpuError(RuntimeError):
 def check(rc, ctx=None):
     if rc != 0:
         msg = load().blgpu_last_error(ctx)
+        raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))
+
+
+def check_ensemble(rc, ens=None):
+    if rc != 0:
+        msg = load().blgpu_ensemble_last_error(ens)
         raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))

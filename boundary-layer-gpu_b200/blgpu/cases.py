@@ -281,17 +281,20 @@ def _smooth_noise(shape, seed, sigma_pts):
         sh = [1] * len(shape)
         sh[d] = k.size
         g = g * np.exp(-0.5 * (2 * np.pi * k * sigma_pts[d]) ** 2).reshape(sh)
-    a = np.fft.irfftn(A * g, s=shape)
+    a = np.fft.irfftn(A * g, s=shape, axes=tuple(range(len(shape))))
     return a / a.std()
 
 
 def turbulent_case(nx=814, ny=257, nz=193, lx=100.0, ly=4.0, lz=8.0, alpha=2.0, retheta=1100.0, cfl=0.5,
-                   rk_scheme=3, seed=1234, noise=0.10, coarse=4):
+                   rk_scheme=3, seed=1234, noise=0.10, coarse=4, lund=3, T_resc=10.0):
     """Turbulent boundary layer in inflow delta99 units: composite mean profile
     plus divergence-free noise (curl of a Gaussian-filtered random vector
     potential, `noise` U_inf rms) confined below y = 1.5 delta.  The noise is
     built on a grid `coarse` times coarser and interpolated; the first
-    projection of the solver makes the field discretely divergence free."""
+    projection of the solver makes the field discretely divergence free.
+    Inflow: Lund recycling (inflow_flag `lund`, 0 for the fixed profile) from
+    the station i = nx/10 (about 10 inflow delta99 downstream at the default
+    length), delta_inlet = 1, averaging time T_resc."""
     nu, utau, theta = turbulent_inflow_profile(retheta)
     rex_theta = (retheta / 0.036) ** 1.25  # theta/x = 0.036 Re_x^-1/5
     x0 = rex_theta * nu
@@ -335,11 +338,31 @@ def turbulent_case(nx=814, ny=257, nz=193, lx=100.0, ly=4.0, lz=8.0, alpha=2.0, 
     W = np.asfortranarray(resample(w_c, (nx + 1, ny + 1, nz)) * amp * (mask_c * wall_c)[None, :, None])
     return Case(name="turbulent", nx=nx, ny=ny, nz=nz, x=x, y=y, z=z, nu=nu, cfl=cfl, rk_scheme=rk_scheme,
                 dpdx=0.0, dpdz=0.0, bc=(U_in, V_in, W_in, U_top, V_top, W_top), U=U, V=V, W=W, t=0.0,
-                utau=utau, theta=theta, retheta=retheta)
+                utau=utau, theta=theta, retheta=retheta,
+                lund=(lund, max(2, nx // 10), 1.0, T_resc) if lund else None)
 
 
-def solver_for(case, precision=0, device=0, les_model=0):
-    """Create a Solver loaded with a case (grid, boundary vectors, state)."""
+def ensemble_cases(nbox=64, seed=2024, nx_set=(128, 192, 256), ny=65, nz_set=(64, 96),
+                   retheta=(800.0, 1500.0), cfl=0.5):
+    """Boxes of the batched training-data ensemble: nx drawn uniformly from
+    nx_set, nz from nz_set, Re_theta uniform in `retheta`, each built with
+    the turbulent recipe (seeded noise, Lund inflow) at the streamwise and
+    spanwise resolution of the 814x257x193 box (dx = 100/814, dz = 8/193 in
+    inflow delta99 units) and ly = 4."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(nbox):
+        nx = int(rng.choice(nx_set))
+        nz = int(rng.choice(nz_set))
+        rt = float(rng.uniform(*retheta))
+        out.append(turbulent_case(nx=nx, ny=ny, nz=nz, lx=nx * 100.0 / 814.0, ly=4.0, lz=nz * 8.0 / 193.0,
+                                  retheta=rt, cfl=cfl, seed=seed + 7919 * (b + 1)))
+    return out
+
+
+def solver_for(case, precision=0, device=0, les_model=0, inflow=True):
+    """Create a Solver loaded with a case (grid, boundary vectors, state and,
+    unless inflow=False, the case's Lund recycling inflow)."""
     from .solver import Solver
     s = Solver(case.nx, case.ny, case.nz, case.nu, case.cfl, case.dpdx, case.dpdz, case.rk_scheme,
                les_model=les_model, precision=precision, device=device)
@@ -348,6 +371,8 @@ def solver_for(case, precision=0, device=0, les_model=0):
     s.upload_state(case.U, case.V, case.W, case.t)
     if case.cfl < 0:
         s.set_dt(-case.cfl)
+    if inflow and getattr(case, "lund", None):
+        s.set_rescaling(*case.lund)
     return s
 
 
@@ -357,7 +382,7 @@ def project_initial(case, device=0):
     projection and boundary pass of the FP64 path (the config-2 recipe's
     "one projection" of the noisy initial field).  Updates case.U/V/W."""
     from ._lib import FP64
-    s = solver_for(case, precision=FP64, device=device)
+    s = solver_for(case, precision=FP64, device=device, inflow=False)
     s.set_dt(abs(case.cfl) if case.cfl < 0 else 1.0)
     s.apply_boundary_conditions(3)
     s.compute_projection_step(3)

@@ -229,6 +229,29 @@ class Solver:
     def kernel_launches(self):
         return int(self.lib.blgpu_kernel_launches(self.ctx))
 
+    # -- launch shapes -----------------------------------------------------
+    TILE_NAMES = ("rhs_kc", "rhs_by", "dct_nw", "dftz_rk", "proj_by")
+
+    def tiles(self):
+        t = (ctypes.c_int * 5)()
+        self._ck(self.lib.blgpu_get_tiles(self.ctx, t, 5))
+        return dict(zip(self.TILE_NAMES, list(t)))
+
+    def set_tiles(self, **kw):
+        cur = self.tiles()
+        for k, v in kw.items():
+            if k not in cur:
+                raise KeyError(k)
+            cur[k] = int(v)
+        t = (ctypes.c_int * 5)(*[cur[k] for k in self.TILE_NAMES])
+        self._ck(self.lib.blgpu_set_tiles(self.ctx, t, 5))
+
+    def autotune(self, steps=3):
+        """Choose the launch shapes by timing; returns (ms/step before, after)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.lib.blgpu_autotune(self.ctx, int(steps), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def phase_times(self, nsteps=1):
         """{phase: (ms total, kernels)} over nsteps eager steps (CUDA events)."""
         n = len(_lib.PHASES)

@@ -64,6 +64,8 @@ struct blgpu_ctx {
   double *d_utau = nullptr;
   int *d_iters = nullptr;
   LundData lund{};
+  Tiles tiles{};
+  long long gen = 0;  // bumped whenever the captured step graphs are dropped
   int cur = 0, old = 1;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_next[3] = {0, 0, 0};
@@ -154,6 +156,7 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 }
 
 static void drop_graphs(blgpu_ctx *ctx) {
+  ctx->gen += 1;
   for (int r = 0; r < 3; ++r)
     if (ctx->graph[r]) {
       cudaGraphExecDestroy(ctx->graph[r]);
@@ -774,10 +777,11 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
   const bool mixed = !ctx->fp64;
   ph_begin(ctx, PH_DIVDCT);
-  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, mixed ? ctx->dcsum : nullptr, ctx->st);
+  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, mixed ? ctx->dcsum : nullptr, ctx->tiles.dct_nw,
+                    ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_DFTZ);
-  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->st);
+  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
@@ -785,15 +789,15 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
                    mixed ? ctx->dcsum : nullptr, ctx->dcrow, mixed ? ctx->dcout : nullptr, ctx->st);
   ph_end(ctx, mixed ? 2 : 1);
   ph_begin(ctx, PH_IDFTZ);
-  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->st);
+  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
-  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->st);
+  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.dct_nw, ctx->st);
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
   launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->dcout : nullptr, S[0], S[1], S[2],
-                    (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->st);
+                    (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
   ph_end(ctx, rk_step == 1 ? 4 : 1);
 }
 
@@ -806,7 +810,7 @@ static void enq_rhs(blgpu_ctx *ctx, int mode, int in, int o, int outb, double c1
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_RHS);
   launch_rhs_rk<T>(ctx->geo, m, mode, ctx->cfg.les_model != 0, Si[0], Si[1], Si[2], (const T *)ctx->nut, So[0], So[1],
-                   So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->st);
+                   So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->tiles, ctx->st);
   ph_end(ctx, 1);
 }
 
@@ -1207,6 +1211,418 @@ int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max) {
   int mx = 0;
   for (int i = 2; i <= nx - 1; ++i) mx = it[i - 1] > mx ? it[i - 1] : mx;
   if (iters_max) *iters_max = mx;
+  return BLGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// launch shapes and their autotuner
+// ---------------------------------------------------------------------------
+static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
+  auto pow2 = [](int v) { return v == 1 || v == 2 || v == 4 || v == 8; };
+  if (t.rhs_kc < 0 || t.rhs_kc > 256) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_kc %d outside 0..256", t.rhs_kc);
+  if (t.rhs_by != 0 && !pow2(t.rhs_by)) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_by %d not in {1,2,4,8}", t.rhs_by);
+  if (t.proj_by != 0 && !pow2(t.proj_by))
+    return set_err(ctx, BLGPU_EINVAL, "tiles: proj_by %d not in {1,2,4,8}", t.proj_by);
+  if (t.dftz_rk != 0 && t.dftz_rk != 4 && t.dftz_rk != 8)
+    return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
+  if (t.dct_nw < 0 || t.dct_nw > 8) return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d outside 0..8", t.dct_nw);
+  if (t.dct_nw > 0) {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
+    const size_t sm = dct_smem_bytes(ctx->spec.N, (int)ctx->esz, t.dct_nw);
+    if (sm > (size_t)optin)
+      return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d needs %zu B of shared memory (> %d)", t.dct_nw, sm, optin);
+  }
+  return BLGPU_OK;
+}
+
+// state of a context that stepping changes: the current fields, the device
+// scalars and the Lund running means
+struct Snapshot {
+  void *f[3] = {nullptr, nullptr, nullptr};
+  Scalars sc{};
+  std::vector<double> lund;
+  int cur = 0, old = 1;
+};
+
+static int snap_take(blgpu_ctx *ctx, Snapshot &sn) {
+  const size_t box = (size_t)ctx->boxn * ctx->esz;
+  for (int q = 0; q < 3; ++q) {
+    cudaError_t e = cudaMalloc(&sn.f[q], box);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "autotune snapshot");
+    CK(cudaMemcpyAsync(sn.f[q], ctx->S[ctx->cur][q], box, cudaMemcpyDeviceToDevice, ctx->st));
+  }
+  CK(cudaMemcpyAsync(&sn.sc, ctx->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, ctx->st));
+  sn.lund.resize(2 * (size_t)ctx->nyg + 2 * (size_t)ctx->ny);
+  CK(cudaMemcpyAsync(sn.lund.data(), ctx->lund.mean, sn.lund.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  sn.cur = ctx->cur;
+  sn.old = ctx->old;
+  return BLGPU_OK;
+}
+
+static int snap_restore(blgpu_ctx *ctx, Snapshot &sn) {
+  const size_t box = (size_t)ctx->boxn * ctx->esz;
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->cur = sn.cur;
+  ctx->old = sn.old;
+  for (int q = 0; q < 3; ++q)
+    if (sn.f[q]) CK(cudaMemcpyAsync(ctx->S[ctx->cur][q], sn.f[q], box, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->sc, &sn.sc, sizeof(Scalars), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->lund.mean, sn.lund.data(), sn.lund.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+static void snap_free(Snapshot &sn) {
+  for (int q = 0; q < 3; ++q)
+    if (sn.f[q]) cudaFree(sn.f[q]);
+  sn.f[0] = sn.f[1] = sn.f[2] = nullptr;
+}
+
+// device time of `steps` graph-replayed steps after one untimed step
+static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
+  int rc = blgpu_advance(ctx, 1);
+  if (rc) return rc;
+  rc = blgpu_advance_timed(ctx, steps, ms);
+  if (rc) return rc;
+  *ms /= (double)steps;
+  return BLGPU_OK;
+}
+
+extern "C" {
+
+int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 values");
+  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4]};
+  int rc = tiles_check(ctx, t);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->tiles = t;
+  drop_graphs(ctx);
+  return BLGPU_OK;
+}
+
+int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
+  if (!ctx || !tiles || n < 5) return BLGPU_EINVAL;
+  const Tiles &t = ctx->tiles;
+  tiles[0] = t.rhs_kc;
+  tiles[1] = t.rhs_by;
+  tiles[2] = t.dct_nw;
+  tiles[3] = t.dftz_rk;
+  tiles[4] = t.proj_by;
+  return BLGPU_OK;
+}
+
+int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_best) {
+  if (!ctx || steps < 1) return set_err(ctx, BLGPU_EINVAL, "blgpu_autotune: bad argument");
+  if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
+    return set_err(ctx, BLGPU_ESTATE, "blgpu_autotune: grid, boundary and state must be set first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  Snapshot sn;
+  int rc = snap_take(ctx, sn);
+  if (rc) { snap_free(sn); return rc; }
+  const bool window = !ctx->fp64 && ctx->cfg.les_model == 0;  // FP32 register-window RHS kernel
+  std::vector<std::vector<int>> cand = {
+      window ? std::vector<int>{8, 16, 32, 64} : std::vector<int>{4, 8, 16},  // rhs_kc
+      {4, 8},                                                                  // rhs_by
+      {0, 1, 2, 3, 4, 6},                                                      // dct_nw
+      {4, 8},                                                                  // dftz_rk
+      {4, 8}};                                                                 // proj_by
+  auto measure = [&](const Tiles &t, double *ms) -> int {
+    int r = snap_restore(ctx, sn);
+    if (r) return r;
+    ctx->tiles = t;
+    drop_graphs(ctx);
+    double a = 0, b = 0;
+    if ((r = time_steps(ctx, steps, &a))) return r;
+    if ((r = time_steps(ctx, steps, &b))) return r;
+    *ms = a < b ? a : b;
+    return BLGPU_OK;
+  };
+  const Tiles t0 = ctx->tiles;
+  Tiles best = t0;
+  double best_ms = 0;
+  rc = measure(best, &best_ms);
+  const double def_ms = best_ms;
+  for (int knob = 0; knob < 5 && !rc; ++knob) {  // one pass of coordinate descent
+    for (int v : cand[knob]) {
+      Tiles t = best;
+      int *f[5] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by};
+      if (*f[knob] == v) continue;
+      *f[knob] = v;
+      if (tiles_check(ctx, t)) continue;
+      double ms = 0;
+      rc = measure(t, &ms);
+      if (rc) break;
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+  }
+  int rc2 = snap_restore(ctx, sn);
+  snap_free(sn);
+  ctx->tiles = rc ? t0 : best;
+  drop_graphs(ctx);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  if (ms_default) *ms_default = def_ms;
+  if (ms_best) *ms_best = best_ms;
+  return BLGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// ensemble: independent boxes advanced by one CUDA-graph launch per step.
+// The graph forks one branch per box from the ensemble stream (each branch is
+// that box's whole step on its own stream, so branches run concurrently) and
+// joins them back.  Graphs are kept per rotation of the three state buffers
+// and re-captured when a box's own graphs were dropped.
+// ---------------------------------------------------------------------------
+struct blgpu_ensemble {
+  std::vector<blgpu_ctx *> box;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  std::vector<long long> gens[3];
+  std::vector<int> next[3];
+  long long graph_launches[3] = {0, 0, 0};
+  long long launches = 0;
+  std::string err;
+};
+
+static int ens_err(blgpu_ensemble *e, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (e) e->err = buf;
+  g_last_error = buf;
+  return code;
+}
+
+#define ECK(expr)                                                                                             \
+  do {                                                                                                        \
+    cudaError_t _e = (expr);                                                                                  \
+    if (_e != cudaSuccess)                                                                                    \
+      return ens_err(e, BLGPU_ECUDA, "CUDA error %s (%s) in %s", cudaGetErrorName(_e), cudaGetErrorString(_e), \
+                     #expr);                                                                                  \
+  } while (0)
+
+static void ens_drop(blgpu_ensemble *e) {
+  for (int r = 0; r < 3; ++r)
+    if (e->graph[r]) {
+      cudaGraphExecDestroy(e->graph[r]);
+      e->graph[r] = nullptr;
+    }
+}
+
+static int ens_capture(blgpu_ensemble *e, int a) {
+  cudaGraph_t gr = nullptr;
+  ECK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed));
+  cudaEventRecord(e->fork, e->st);
+  long long nl = 0;
+  e->next[a].assign(e->box.size(), 0);
+  e->gens[a].assign(e->box.size(), 0);
+  for (size_t b = 0; b < e->box.size(); ++b) {
+    blgpu_ctx *ctx = e->box[b];
+    cudaStreamWaitEvent(ctx->st, e->fork, 0);
+    const long long l0 = ctx->launches;
+    e->next[a][b] = ctx->fp64 ? enq_step<double>(ctx, a, true) : enq_step<float>(ctx, a, true);
+    nl += ctx->launches - l0;
+    ctx->launches = l0;
+    cudaEventRecord(e->join[b], ctx->st);
+    cudaStreamWaitEvent(e->st, e->join[b], 0);
+    e->gens[a][b] = ctx->gen;
+  }
+  cudaError_t ce = cudaStreamEndCapture(e->st, &gr);
+  if (ce != cudaSuccess) return ens_err(e, BLGPU_ECUDA, "ensemble capture failed: %s", cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&e->graph[a], gr, 0);
+  cudaGraphDestroy(gr);
+  if (ce != cudaSuccess) return ens_err(e, BLGPU_ECUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ce));
+  e->graph_launches[a] = nl;
+  return BLGPU_OK;
+}
+
+extern "C" {
+
+int blgpu_ensemble_create(blgpu_ctx *const *boxes, int nbox, blgpu_ensemble **out) {
+  if (!boxes || nbox < 1 || !out) return set_err(nullptr, BLGPU_EINVAL, "blgpu_ensemble_create: bad argument");
+  *out = nullptr;
+  for (int b = 0; b < nbox; ++b) {
+    if (!boxes[b]) return set_err(nullptr, BLGPU_EINVAL, "blgpu_ensemble_create: box %d is null", b);
+    if (boxes[b]->cfg.device != boxes[0]->cfg.device)
+      return set_err(nullptr, BLGPU_EINVAL, "blgpu_ensemble_create: boxes on different devices");
+    for (int c = 0; c < b; ++c)
+      if (boxes[c] == boxes[b]) return set_err(nullptr, BLGPU_EINVAL, "blgpu_ensemble_create: box %d repeated", b);
+  }
+  blgpu_ensemble *e = new blgpu_ensemble();
+  e->box.assign(boxes, boxes + nbox);
+  e->device = boxes[0]->cfg.device;
+  e->join.assign(nbox, nullptr);
+  cudaError_t ce = cudaSetDevice(e->device);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  for (int b = 0; b < nbox && ce == cudaSuccess; ++b) ce = cudaEventCreateWithFlags(&e->join[b], cudaEventDisableTiming);
+  if (ce != cudaSuccess) {
+    int rc = set_err(nullptr, BLGPU_ECUDA, "blgpu_ensemble_create: %s", cudaGetErrorString(ce));
+    blgpu_ensemble_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return BLGPU_OK;
+}
+
+int blgpu_ensemble_destroy(blgpu_ensemble *e) {
+  if (!e) return BLGPU_OK;
+  cudaSetDevice(e->device);
+  if (e->st) cudaStreamSynchronize(e->st);
+  ens_drop(e);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+  return BLGPU_OK;
+}
+
+const char *blgpu_ensemble_last_error(const blgpu_ensemble *e) {
+  if (e && !e->err.empty()) return e->err.c_str();
+  return g_last_error.c_str();
+}
+
+int blgpu_ensemble_advance(blgpu_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return ens_err(e, BLGPU_EINVAL, "blgpu_ensemble_advance: bad argument");
+  ECK(cudaSetDevice(e->device));
+  for (blgpu_ctx *c : e->box) {
+    if (!c->have_grid || !c->have_bc || !c->have_state)
+      return ens_err(e, BLGPU_ESTATE, "blgpu_ensemble_advance: every box needs grid, boundary and state");
+    ECK(cudaStreamSynchronize(c->st));  // earlier work of a box on its own stream comes first
+  }
+  for (int n = 0; n < (nsteps > 0 ? nsteps : 1); ++n) {
+    const int a = e->box[0]->cur;
+    for (blgpu_ctx *c : e->box)
+      if (c->cur != a)
+        return ens_err(e, BLGPU_ESTATE, "blgpu_ensemble_advance: boxes are at different buffer rotations");
+    bool stale = !e->graph[a];
+    for (size_t b = 0; b < e->box.size() && !stale; ++b) stale = e->gens[a][b] != e->box[b]->gen;
+    if (stale) {
+      if (e->graph[a]) {
+        cudaGraphExecDestroy(e->graph[a]);
+        e->graph[a] = nullptr;
+      }
+      int rc = ens_capture(e, a);
+      if (rc) return rc;
+    }
+    if (nsteps == 0) break;
+    ECK(cudaGraphLaunch(e->graph[a], e->st));
+    e->launches += e->graph_launches[a];
+    for (size_t b = 0; b < e->box.size(); ++b) {
+      e->box[b]->old = a;
+      e->box[b]->cur = e->next[a][b];
+    }
+  }
+  ECK(cudaGetLastError());
+  return BLGPU_OK;
+}
+
+// Baseline: the same steps with the boxes one after another (each box's own
+// step graph launched on the ensemble stream, so no two boxes overlap).
+int blgpu_ensemble_advance_sequential(blgpu_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return ens_err(e, BLGPU_EINVAL, "blgpu_ensemble_advance_sequential: bad argument");
+  ECK(cudaSetDevice(e->device));
+  for (blgpu_ctx *c : e->box) {
+    if (!c->have_grid || !c->have_bc || !c->have_state)
+      return ens_err(e, BLGPU_ESTATE, "blgpu_ensemble_advance_sequential: every box needs grid, boundary and state");
+    ECK(cudaStreamSynchronize(c->st));
+    for (int r = 0; r < 3; ++r)  // capture each rotation's graph up front, outside any timed region
+      if (!c->graph[r]) {
+        const int keep_cur = c->cur, keep_old = c->old;
+        c->cur = r;
+        int rc = blgpu_advance(c, 0);
+        c->cur = keep_cur;
+        c->old = keep_old;
+        if (rc) return ens_err(e, rc, "%s", c->err.c_str());
+      }
+  }
+  for (int n = 0; n < nsteps; ++n)
+    for (blgpu_ctx *c : e->box) {
+      const int a = c->cur;
+      ECK(cudaGraphLaunch(c->graph[a], e->st));
+      c->launches += c->graph_launches[a];
+      e->launches += c->graph_launches[a];
+      c->old = a;
+      c->cur = c->graph_next[a];
+    }
+  ECK(cudaGetLastError());
+  return BLGPU_OK;
+}
+
+int blgpu_ensemble_time(blgpu_ensemble *e, int nsteps, int sequential, double *ms) {
+  if (!e || !ms || nsteps < 1) return ens_err(e, BLGPU_EINVAL, "blgpu_ensemble_time: bad argument");
+  ECK(cudaSetDevice(e->device));
+  int rc = sequential ? blgpu_ensemble_advance_sequential(e, 0) : blgpu_ensemble_advance(e, 0);
+  if (rc) return rc;
+  cudaEvent_t a, b;
+  ECK(cudaEventCreate(&a));
+  ECK(cudaEventCreate(&b));
+  cudaEventRecord(a, e->st);
+  rc = sequential ? blgpu_ensemble_advance_sequential(e, nsteps) : blgpu_ensemble_advance(e, nsteps);
+  cudaEventRecord(b, e->st);
+  cudaError_t ce = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (!rc && ce == cudaSuccess) ce = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  ECK(ce);
+  *ms = (double)t;
+  return BLGPU_OK;
+}
+
+int blgpu_ensemble_sync(blgpu_ensemble *e) {
+  if (!e) return BLGPU_EINVAL;
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
+  return BLGPU_OK;
+}
+
+long long blgpu_ensemble_launches(const blgpu_ensemble *e) { return e ? e->launches : 0; }
+
+// Autotune each distinct box shape once (the first box of that shape) and
+// give its launch shapes to every box of the same shape and precision.
+int blgpu_ensemble_autotune(blgpu_ensemble *e, int steps, int *ntuned) {
+  if (!e || steps < 1) return ens_err(e, BLGPU_EINVAL, "blgpu_ensemble_autotune: bad argument");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
+  int n = 0;
+  for (size_t b = 0; b < e->box.size(); ++b) {
+    blgpu_ctx *c = e->box[b];
+    blgpu_ctx *twin = nullptr;
+    for (size_t q = 0; q < b && !twin; ++q) {
+      blgpu_ctx *d = e->box[q];
+      if (d->nx == c->nx && d->ny == c->ny && d->nz == c->nz && d->fp64 == c->fp64 &&
+          d->cfg.les_model == c->cfg.les_model)
+        twin = d;
+    }
+    if (twin) {
+      c->tiles = twin->tiles;
+      drop_graphs(c);
+      continue;
+    }
+    int rc = blgpu_autotune(c, steps, nullptr, nullptr);
+    if (rc) return ens_err(e, rc, "%s", c->err.c_str());
+    ++n;
+  }
+  ens_drop(e);
+  if (ntuned) *ntuned = n;
   return BLGPU_OK;
 }
 

@@ -13,6 +13,16 @@ template <typename T> struct MetT {
   T nu, dpdx, dpdz;
 };
 
+// Launch shapes of the main kernels.  0 selects the built-in choice; the
+// autotuner (blgpu_autotune) searches these per box.
+struct Tiles {
+  int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8, FP32 register window 32)
+  int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
+  int dct_nw;   // complex lines (warps) per CTA of the DCT kernels (0: sized from shared memory)
+  int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
+  int proj_by;  // projection block is 32 x proj_by threads (0: 8)
+};
+
 // boundary data (FP64, 1-based like the Fortran vectors)
 struct BcData {
   const double *U_inlet, *V_inlet, *W_inlet;  // (nyg) (ny) (nyg)
@@ -46,10 +56,10 @@ struct LundData {
 template <typename T>
 void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *U, const T *V, const T *W,
                    const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
-                   const Scalars *sc, double c1, double c2, cudaStream_t st);
+                   const Scalars *sc, double c1, double c2, const Tiles &tl, cudaStream_t st);
 template <typename T>
 void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
-                    const Scalars *sc, int save_p, cudaStream_t st);
+                    const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st);
 int bc_x_parts(const Geo &g);
 template <typename T>
 void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
@@ -94,16 +104,16 @@ struct Spec {  // spectral layout of the Poisson solve
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    double *dc_sum, cudaStream_t st);
+                    double *dc_sum, int nw, cudaStream_t st);
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
-                  cudaStream_t st);
+                  int rk, cudaStream_t st);
 template <typename T>
 void launch_thomas(const Spec &s, typename vec2<T>::type *C, double *piv, const double *dd, const double *dl,
                    const double *du, const double *kxx, const double *kzz, const double *dc_lines,
                    double *dc_rows, double *dc_out, cudaStream_t st);
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, cudaStream_t st);
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, cudaStream_t st);
 size_t dct_smem_bytes(int n, int elem_bytes, int lines);
 int dct_lines_per_cta(int n, int elem_bytes);
 

@@ -703,8 +703,8 @@ static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, c
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    double *dc_sum, cudaStream_t st) {
-  const int nw = dct_lines_per_cta(s.N, sizeof(T));
+                    double *dc_sum, int nw_req, cudaStream_t st) {
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T));
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
   const int grid = (ncl + nw - 1) / nw;
@@ -718,8 +718,8 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
 }
 
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, cudaStream_t st) {
-  const int nw = dct_lines_per_cta(s.N, sizeof(T));
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, cudaStream_t st) {
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T));
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;
@@ -732,9 +732,8 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
   }
 }
 
-template <typename T>
-void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inverse, cudaStream_t st) {
-  constexpr int RK = 8;
+template <typename T, int RK>
+static void launch_dft_z_rk(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inverse, cudaStream_t st) {
   constexpr int TW = 32 * Vec16<T>::n;
   if (!inverse) {
     dim3 grid((s.N + TW - 1) / TW, s.NM, (s.MH + 8 * RK - 1) / (8 * RK));
@@ -753,6 +752,12 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 }
 
 template <typename T>
+void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inverse, int rk, cudaStream_t st) {
+  if (rk == 4) launch_dft_z_rk<T, 4>(s, R, C, tz, inverse, st);
+  else launch_dft_z_rk<T, 8>(s, R, C, tz, inverse, st);
+}
+
+template <typename T>
 void launch_thomas(const Spec &s, T2<T> *C, double *piv, const double *dd, const double *dl, const double *du,
                    const double *kxx, const double *kzz, const double *dc_lines, double *dc_rows, double *dc_out,
                    cudaStream_t st) {
@@ -763,9 +768,9 @@ void launch_thomas(const Spec &s, T2<T> *C, double *piv, const double *dd, const
 
 #define BLGPU_SPEC_INST(T)                                                                                        \
   template void launch_div_dct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, const T *, const T *, \
-                                  T *, double *, cudaStream_t);                                                   \
-  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, cudaStream_t);     \
-  template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, cudaStream_t);             \
+                                  T *, double *, int, cudaStream_t);                                              \
+  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, cudaStream_t); \
+  template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
   template void launch_thomas<T>(const Spec &, T2<T> *, double *, const double *, const double *,                \
                                  const double *, const double *, const double *, const double *, double *,       \
                                  double *, cudaStream_t);

@@ -818,22 +818,23 @@ __global__ void k_law_of_wall(Geo g, const T *__restrict__ U, double *__restrict
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-static inline dim3 vol_grid(int ni, int nj, int nk, int kchunk) {
-  return dim3((ni + 31) / 32, (nj + 7) / 8, (nk + kchunk - 1) / kchunk);
+static inline dim3 vol_grid(int ni, int nj, int nk, int kchunk, int by = 8) {
+  return dim3((ni + 31) / 32, (nj + by - 1) / by, (nk + kchunk - 1) / kchunk);
 }
 
 template <typename T>
 void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *U, const T *V, const T *W,
                    const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
-                   const Scalars *sc, double c1, double c2, cudaStream_t st) {
-  const int kchunk = 8;
-  dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk), block(32, 8);
+                   const Scalars *sc, double c1, double c2, const Tiles &tl, cudaStream_t st) {
+  const int kchunk = tl.rhs_kc > 0 ? tl.rhs_kc : 8;
+  const int by = tl.rhs_by > 0 ? tl.rhs_by : 8;
+  dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk, by), block(32, by);
 #define BLGPU_RHS_CASE(M, L)                                                                             \
   k_rhs_rk<T, M, L><<<grid, block, 0, st>>>(g, m, U, V, W, nut, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, \
                                             c2, kchunk)
   if (!les && sizeof(T) == 4) {  // FP32: register-window kernel (FP64 keeps the lower-register form)
-    const int kc = 32;
-    dim3 gd = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc);
+    const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 32;
+    dim3 gd = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc, by);
 #define BLGPU_DNS_CASE(M)                                                                                     \
   k_rhs_rk_dns<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc)
     switch (mode) {
@@ -863,10 +864,11 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 
 template <typename T>
 void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
-                    const Scalars *sc, int save_p, cudaStream_t st) {
+                    const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st) {
   constexpr int VN = 16 / sizeof(T);
   const int ngrp = (g.nx - 1 + VN - 1) / VN;  // i = 2..nx in groups of VN
-  dim3 block(32, 8), grid((ngrp + 31) / 32, (g.ny - 1 + 7) / 8, g.nz - 1);
+  const int by = tl.proj_by > 0 ? tl.proj_by : 8;
+  dim3 block(32, by), grid((ngrp + 31) / 32, (g.ny - 1 + by - 1) / by, g.nz - 1);
   k_project_v<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p);
   if (save_p) {
     dim3 b2(32, 8);
@@ -934,9 +936,9 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cuda
 #define BLGPU_INST(T)                                                                                                \
   template void launch_rhs_rk<T>(const Geo &, const MetT<T> &, int, bool, const T *, const T *, const T *,          \
                                  const T *, const T *, const T *, const T *, T *, T *, T *, T *, T *, T *,          \
-                                 const Scalars *, double, double, cudaStream_t);                                    \
+                                 const Scalars *, double, double, const Tiles &, cudaStream_t);                     \
   template void launch_project<T>(const Geo &, const MetT<T> &, const T *, const double *, T *, T *, T *, T *,     \
-                                  const Scalars *, int, cudaStream_t);                                              \
+                                  const Scalars *, int, const Tiles &, cudaStream_t);                               \
   template void launch_bc<T>(const Geo &, const BcData &, T *, T *, T *, const T *, const T *, const T *,         \
                              Scalars *, double, double *, double, double, cudaStream_t);                            \
   template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, cudaStream_t); \

@@ -207,6 +207,44 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
                                    const double *y, const double *z, int nx, int ny, int nz, double *max_div,
                                    void *stream);
 
+/* ---- launch shapes and the autotuner ----
+ * tiles[5] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS block
+ * 32 x rhs_by), dct_nw (complex lines per CTA of the DCT kernels), dftz_rk
+ * (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection block
+ * 32 x proj_by); 0 = the built-in choice.  Results do not depend on them.
+ * No counterpart in the reference (its OpenACC loops take compiler-chosen
+ * gangs). */
+int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n);
+int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n);
+/* Coordinate search over the tile candidates, timing `steps` graph-replayed
+ * steps per candidate on the device; keeps the fastest.  The fields, time,
+ * dt and Lund means are restored afterwards.  ms_default / ms_best (may be
+ * NULL) receive the per-step times of the starting and the chosen tiles. */
+int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_best);
+
+/* ---- ensembles of independent boxes (no counterpart in the reference) ----
+ * Boxes are ordinary contexts on one device, created and loaded by the
+ * caller (grid, boundary, state, Lund); the ensemble does not own them.
+ * blgpu_ensemble_advance runs each step of every box as ONE CUDA-graph launch
+ * whose branches (one per box) run concurrently; results equal those of
+ * blgpu_advance on each box.  Boxes must be at the same buffer rotation
+ * (advanced the same number of RK3 steps since their last upload). */
+typedef struct blgpu_ensemble blgpu_ensemble;
+int blgpu_ensemble_create(blgpu_ctx *const *boxes, int nbox, blgpu_ensemble **ens);
+int blgpu_ensemble_destroy(blgpu_ensemble *ens);
+const char *blgpu_ensemble_last_error(const blgpu_ensemble *ens);
+int blgpu_ensemble_advance(blgpu_ensemble *ens, int nsteps);
+/* the same steps with one box at a time (the sequential baseline) */
+int blgpu_ensemble_advance_sequential(blgpu_ensemble *ens, int nsteps);
+/* device time (CUDA events on the ensemble stream) of nsteps steps, graph
+ * capture excluded; sequential != 0 times the sequential baseline */
+int blgpu_ensemble_time(blgpu_ensemble *ens, int nsteps, int sequential, double *ms);
+int blgpu_ensemble_sync(blgpu_ensemble *ens);
+long long blgpu_ensemble_launches(const blgpu_ensemble *ens);
+/* blgpu_autotune on the first box of each distinct shape; the others of
+ * that shape take its tiles.  ntuned (may be NULL) = shapes tuned. */
+int blgpu_ensemble_autotune(blgpu_ensemble *ens, int steps, int *ntuned);
+
 #ifdef __cplusplus
 }
 #endif

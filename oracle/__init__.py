@@ -286,4 +286,6 @@ def oracle_for(case, variant=0, threads=1):
     o.set_state(case.U, case.V, case.W, case.t)
     if case.cfl < 0:
         o.set_dt(-case.cfl)
+    if getattr(case, "lund", None):
+        o.set_rescaling(*case.lund)
     return o

@@ -46,3 +46,14 @@ def test_grid_builders():
 def test_temporal_mode_file_fixture():
     g = json.load(open(os.path.join(GOLD, "temporal_modes_ref.json")))
     assert g["bytes"] == 28 + 8 * (g["ny_inlet"] + g["n_modes"] + g["m_modes"]) + 48 * g["ny_inlet"] * g["n_modes"] * g["m_modes"]
+
+
+def test_ensemble_cases_follow_the_recipe():
+    bs = cases.ensemble_cases(nbox=12, seed=5)
+    assert len(bs) == 12
+    for c in bs:
+        assert c.nx in (128, 192, 256) and c.ny == 65 and c.nz in (64, 96)
+        assert 800.0 <= c.retheta <= 1500.0
+        assert c.lund[0] == 3 and 2 <= c.lund[1] <= c.nx
+        assert abs((c.x[1] - c.x[0]) - 100.0 / 814.0) < 1e-3
+    assert len({(c.nx, c.nz) for c in bs}) > 1
