@@ -24,6 +24,8 @@ SOURCES = {
     "spectral.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
+    "mlp.cu": [],
+    "capi_mlp.cu": [],
 }
 
 

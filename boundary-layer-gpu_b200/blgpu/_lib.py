@@ -9,6 +9,7 @@ import os
 from ._build import LIB_PATH
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
+c_float_p = ctypes.POINTER(ctypes.c_float)
 
 
 class Config(ctypes.Structure):
@@ -75,6 +76,25 @@ _SIGS = {
     "blgpu_ensemble_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "blgpu_ensemble_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "blgpu_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "blgpu_mlp_nparams": (ctypes.c_int, []),
+    "blgpu_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
+    "blgpu_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_mlp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "blgpu_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "blgpu_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "blgpu_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int, c_float_p]),
+    "blgpu_mlp_gradient": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_int, c_float_p, c_float_p]),
+    "blgpu_mlp_add_data": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_int]),
+    "blgpu_mlp_sample": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "blgpu_mlp_clear_data": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_mlp_num_samples": (ctypes.c_int, [ctypes.c_void_p]),
+    "blgpu_mlp_get_data": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, ctypes.c_int]),
+    "blgpu_mlp_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, c_float_p]),
+    "blgpu_mlp_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "blgpu_mlp_loss_history": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "blgpu_mlp_eval": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "blgpu_set_wall_model": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "blgpu_wall_stress": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),
 }
 
 PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]
@@ -110,6 +130,12 @@ class BlgpuError(RuntimeError):
 def check(rc, ctx=None):
     if rc != 0:
         msg = load().blgpu_last_error(ctx)
+        raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))
+
+
+def check_mlp(rc, net=None):
+    if rc != 0:
+        msg = load().blgpu_mlp_last_error(net) if net is not None else load().blgpu_last_error(None)
         raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))
 
 

@@ -207,12 +207,14 @@ def turbulent_top(x, nu, u_inf=1.0):
 # ---------------------------------------------------------------------------
 # turbulent mean profile (composite law of the wall + Coles wake)
 # ---------------------------------------------------------------------------
-def composite_profile(y, delta, utau, nu, kappa=0.41, B=5.0, Pi=0.45, u_inf=1.0):
-    """Musker-style smooth inner profile blended with Coles' wake, clipped at
-    U_inf above delta."""
+def composite_profile(y, delta, utau, nu, kappa=0.38, B=5.2, Pi=0.45, u_inf=1.0):
+    """Reichardt's inner law blended with Coles' wake, clipped at U_inf above
+    delta.  kappa and B default to the constants of the reference's
+    equilibrium wall model (wallmodel.f90:1960-1961); Reichardt's constant is
+    chosen so that the profile tends to u+ = ln(y+)/kappa + B in the log layer."""
     yp = np.maximum(y, 0.0) * utau / nu
-    # Reichardt inner law
-    up = (1.0 / kappa) * np.log1p(kappa * yp) + 7.8 * (1.0 - np.exp(-yp / 11.0) - (yp / 11.0) * np.exp(-yp / 3.0))
+    C = B - math.log(kappa) / kappa
+    up = (1.0 / kappa) * np.log1p(kappa * yp) + C * (1.0 - np.exp(-yp / 11.0) - (yp / 11.0) * np.exp(-yp / 3.0))
     eta = np.clip(y / delta, 0.0, 1.0)
     wake = 2.0 * Pi / kappa * np.sin(0.5 * np.pi * eta) ** 2
     u = utau * (up + wake)

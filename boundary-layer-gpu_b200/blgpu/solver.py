@@ -62,6 +62,7 @@ class Solver:
         x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
         assert x.size == self.nx and y.size == self.ny and z.size == self.nz
         self._ck(self.lib.blgpu_set_grid(self.ctx, _p(x), _p(y), _p(z)))
+        self.x, self.y, self.z = x.copy(), y.copy(), z.copy()
 
     def set_boundary(self, U_inlet, V_inlet, W_inlet, U_top, V_top, W_top):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (U_inlet, V_inlet, W_inlet, U_top, V_top, W_top)]
@@ -228,6 +229,19 @@ class Solver:
 
     def kernel_launches(self):
         return int(self.lib.blgpu_kernel_launches(self.ctx))
+
+    # -- wall model ----------------------------------------------------------
+    def set_wall_model(self, mode, jh=3, net=None):
+        """0 no-slip, 1 law of the wall at row jh, 2 the WallNet `net` at row jh."""
+        self._wall_net = net  # the solver reads the network's device weights every substep
+        self._ck(self.lib.blgpu_set_wall_model(self.ctx, int(mode), int(jh), net.h if net is not None else None))
+
+    def wall_stress(self):
+        """(tau_x, tau_z) of the wall model on the current state, shape (nzg-3, nx-2)."""
+        n = (self.nx - 2) * (self.nzg - 3)
+        tx, tz = np.zeros(n), np.zeros(n)
+        self._ck(self.lib.blgpu_wall_stress(self.ctx, _p(tx), _p(tz)))
+        return tx.reshape(self.nzg - 3, self.nx - 2), tz.reshape(self.nzg - 3, self.nx - 2)
 
     # -- launch shapes -----------------------------------------------------
     TILE_NAMES = ("rhs_kc", "rhs_by", "dct_nw", "dftz_rk", "proj_by")

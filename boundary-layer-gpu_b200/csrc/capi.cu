@@ -12,6 +12,7 @@
 
 #include "../../include/blgpu.h"
 #include "kernels.cuh"
+#include "mlp.cuh"
 
 namespace blgpu {
 
@@ -52,7 +53,9 @@ struct blgpu_ctx {
   void *S[3][3] = {};  // state buffers [buffer][u,v,w]
   void *F1[3] = {};
   void *P = nullptr, *nut = nullptr, *rhs_p = nullptr, *R = nullptr, *C = nullptr;
-  double *piv = nullptr, *dcsum = nullptr, *dcrow = nullptr, *dcout = nullptr, *qx_part = nullptr;
+  double *piv = nullptr, *qx_part = nullptr;
+  // mixed form: FP64 kz = 0 pressure plane p0 [NM][N] and its scratch H, cosine matrix cm [N][N]
+  double *kz0 = nullptr, *kz0h = nullptr, *cmat = nullptr;
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   void *tw = nullptr, *post = nullptr, *ztab = nullptr;
@@ -65,6 +68,10 @@ struct blgpu_ctx {
   int *d_iters = nullptr;
   LundData lund{};
   Tiles tiles{};
+  // wall model: 0 no-slip, 1 law of the wall, 2 network; d_wm = alpha_x, alpha_z, tau_x, tau_z
+  int wm_mode = 0, wm_jh = 3;
+  MlpDev wm_net{};
+  double *d_wm = nullptr;
   long long gen = 0;  // bumped whenever the captured step graphs are dropped
   int cur = 0, old = 1;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
@@ -230,9 +237,20 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, &ctx->R, (size_t)s.NM * s.M * s.rx * ctx->esz));
   TRY(dalloc(ctx, &ctx->C, (size_t)s.NM * s.MH * s.rx * ctx->esz * 2));
   TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
-  TRY(dalloc(ctx, (void **)&ctx->dcsum, (size_t)s.NM * s.M * sizeof(double)));
-  TRY(dalloc(ctx, (void **)&ctx->dcrow, (size_t)s.NM * sizeof(double)));
-  TRY(dalloc(ctx, (void **)&ctx->dcout, (size_t)s.NM * sizeof(double)));
+  if (!ctx->fp64) {
+    TRY(dalloc(ctx, (void **)&ctx->kz0, (size_t)s.NM * s.N * sizeof(double)));
+    TRY(dalloc(ctx, (void **)&ctx->kz0h, (size_t)s.NM * s.N * sizeof(double)));
+    TRY(dalloc(ctx, (void **)&ctx->cmat, (size_t)s.N * s.N * sizeof(double)));
+    // inverse DCT-II of length N with the 1/(N M) of the inverse transforms
+    std::vector<double> ct(4 * (size_t)s.N), cm((size_t)s.N * s.N);
+    for (int q = 0; q < 4 * s.N; ++q) ct[q] = cos(M_PI * (double)q / (2.0 * (double)s.N));
+    const double nrm = 1.0 / ((double)s.N * (double)s.M);
+    for (int kx = 0; kx < s.N; ++kx)
+      for (int i = 0; i < s.N; ++i)
+        cm[(size_t)kx * s.N + i] = (kx ? 2.0 : 1.0) * nrm * ct[((long long)kx * (2 * i + 1)) % (4 * s.N)];
+    TRY(check_cuda(ctx, cudaMemcpy(ctx->cmat, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice),
+                   "cosine matrix"));
+  }
   TRY(dalloc(ctx, (void **)&ctx->sc, sizeof(Scalars)));
   TRY(dalloc(ctx, (void **)&ctx->stage, (size_t)ctx->nxg * ctx->nyg * ctx->nzg * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->d_cs2, (size_t)(ctx->nyg + 2) * sizeof(double)));
@@ -241,6 +259,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, (void **)&ctx->d_utau, (size_t)ctx->nx * sizeof(double)));
   TRY(dalloc(ctx, (void **)&ctx->d_iters, (size_t)ctx->nx * sizeof(int)));
   TRY(dalloc(ctx, (void **)&ctx->d_maxdiv, sizeof(unsigned long long)));
+  TRY(dalloc(ctx, (void **)&ctx->d_wm, 4 * (size_t)(ctx->nx - 2) * (ctx->nzg - 3) * sizeof(double)));
   {  // Lund inflow state, FP64, laid out as described at LundData
     const size_t nyg = ctx->nyg, ny = ctx->ny, nzg = ctx->nzg, nz = ctx->nz;
     const size_t nd = (2 * nyg + 2 * ny + 1) + (2 * nyg + 2 * ny) + 4 * nyg + (nyg + ny) + 4 * nyg +
@@ -777,17 +796,19 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
   const bool mixed = !ctx->fp64;
   ph_begin(ctx, PH_DIVDCT);
-  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, mixed ? ctx->dcsum : nullptr, ctx->tiles.dct_nw,
-                    ctx->st);
+  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_DFTZ);
   launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
+  if (mixed)  // the z-mean pressure in FP64 (see k_kz0_thomas), before the FP32 Thomas drops kz = 0
+    launch_kz0_plane<T>(s, (const T2 *)ctx->C, ctx->kz0h, ctx->kz0, ctx->piv, ctx->cmat, sp, sp + s.NM,
+                        sp + 2 * s.NM, sp + 3 * s.NM, ctx->kzz[0], ctx->st);
   launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp, sp + s.NM, sp + 2 * s.NM, sp + 3 * s.NM, sp + 3 * s.NM + s.N,
-                   mixed ? ctx->dcsum : nullptr, ctx->dcrow, mixed ? ctx->dcout : nullptr, ctx->st);
-  ph_end(ctx, mixed ? 2 : 1);
+                   mixed ? 1 : 0, ctx->st);
+  ph_end(ctx, mixed ? 3 : 1);
   ph_begin(ctx, PH_IDFTZ);
   launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
@@ -796,7 +817,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
-  launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->dcout : nullptr, S[0], S[1], S[2],
+  launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, S[0], S[1], S[2],
                     (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
   ph_end(ctx, rk_step == 1 ? 4 : 1);
 }
@@ -812,6 +833,20 @@ static void enq_rhs(blgpu_ctx *ctx, int mode, int in, int o, int outb, double c1
   launch_rhs_rk<T>(ctx->geo, m, mode, ctx->cfg.les_model != 0, Si[0], Si[1], Si[2], (const T *)ctx->nut, So[0], So[1],
                    So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->tiles, ctx->st);
   ph_end(ctx, 1);
+}
+
+// wall stress of the current model from fields U, W (the saved P and, with
+// LES, the eddy viscosity); returns the number of kernels launched
+template <typename T>
+static int enq_wall_model(blgpu_ctx *ctx, const T *U, const T *W) {
+  const T *nut = ctx->cfg.les_model ? (const T *)ctx->nut : nullptr;
+  if (ctx->wm_mode == 1) {
+    launch_law_of_wall<T>(ctx->geo, U, ctx->d_utau, ctx->d_iters, ctx->wm_jh, ctx->st);
+    launch_wall_eq<T>(ctx->geo, ctx->d_utau, nut, ctx->d_wm, ctx->st);
+    return 2;
+  }
+  launch_wall_mlp<T>(ctx->geo, ctx->wm_net, U, W, (const T *)ctx->P, nut, ctx->wm_jh, ctx->d_wm, ctx->st);
+  return 1;
 }
 
 // One time step from buffer a.  Returns the index of the new state buffer.
@@ -839,6 +874,11 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
       ph_begin(ctx, PH_MISC);
       launch_smagorinsky<T>(ctx->geo, Si[0], Si[1], Si[2], ctx->d_cs2, (T *)ctx->nut, ctx->st);
       ph_end(ctx, 1);
+    }
+    if (ctx->wm_mode) {  // wall model from the substep's state (time_integration.f90:341-346)
+      T **Si = reinterpret_cast<T **>(ctx->S[in]);
+      ph_begin(ctx, PH_BC);
+      ph_end(ctx, enq_wall_model<T>(ctx, Si[0], Si[2]));
     }
     enq_rhs<T>(ctx, mode, in, a, outb, c1, c2);
     ph_begin(ctx, PH_MISC);
@@ -1016,11 +1056,19 @@ int blgpu_get_rhs_p(blgpu_ctx *ctx, double *rhs_p) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->st));
   const int e1 = nxg - 2, e2 = nyg - 2;
+  std::vector<double> p0;  // mixed form: the FP64 z-mean part, [j-2][i-2] of pitch N
+  const int N = ctx->spec.N;
+  if (ctx->kz0) {
+    p0.resize((size_t)ctx->spec.NM * N);
+    CK(cudaMemcpy(p0.data(), ctx->kz0, p0.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   for (int k = 2; k <= nzg; ++k)
     for (int j = 2; j <= nyg - 1; ++j)
-      for (int i = 2; i <= nxg - 1; ++i)
-        rhs_p[((size_t)(k - 2) * e2 + (j - 2)) * e1 + (i - 2)] =
-            (k == nzg) ? 0.0 : full[((size_t)(k - 1) * nyg + (j - 1)) * nxg + (i - 1)];
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double v = (k == nzg) ? 0.0 : full[((size_t)(k - 1) * nyg + (j - 1)) * nxg + (i - 1)];
+        if (!p0.empty() && k < nzg) v += p0[(size_t)(j - 2) * N + std::min(i - 2, N - 1)];
+        rhs_p[((size_t)(k - 2) * e2 + (j - 2)) * e1 + (i - 2)] = v;
+      }
   return BLGPU_OK;
 }
 
@@ -1196,9 +1244,9 @@ int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max) {
   const int nx = ctx->nx;
   CK(cudaMemcpyAsync(ctx->d_utau, utau, nx * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
   if (ctx->fp64)
-    launch_law_of_wall<double>(ctx->geo, ((double **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, ctx->st);
+    launch_law_of_wall<double>(ctx->geo, ((double **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, 3, ctx->st);
   else
-    launch_law_of_wall<float>(ctx->geo, ((float **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, ctx->st);
+    launch_law_of_wall<float>(ctx->geo, ((float **)ctx->S[ctx->cur])[0], ctx->d_utau, ctx->d_iters, 3, ctx->st);
   ctx->launches += 1;
   CK(cudaGetLastError());
   std::vector<int> it(nx, 0);
@@ -1211,6 +1259,89 @@ int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max) {
   int mx = 0;
   for (int i = 2; i <= nx - 1; ++i) mx = it[i - 1] > mx ? it[i - 1] : mx;
   if (iters_max) *iters_max = mx;
+  return BLGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// wall models and the training-sample extractor
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int blgpu_set_wall_model(blgpu_ctx *ctx, int mode, int jh, const blgpu_mlp *net) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (mode < 0 || mode > 2) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_wall_model: mode %d not in 0..2", mode);
+  if (mode && (jh < 2 || jh > ctx->nyg - 1))
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_wall_model: row %d outside 2..nyg-1", jh);
+  if (mode == 2 && !net) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_wall_model: mode 2 needs a network");
+  if (mode == 2 && blgpu_mlp_device(net) != ctx->cfg.device)
+    return set_err(ctx, BLGPU_EINVAL, "blgpu_set_wall_model: network on another device");
+  if (mode && !ctx->have_grid) return set_err(ctx, BLGPU_ESTATE, "blgpu_set_wall_model: grid first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  drop_graphs(ctx);
+  ctx->wm_mode = mode;
+  ctx->wm_jh = jh;
+  ctx->wm_net = mode == 2 ? blgpu_mlp_view(net) : MlpDev{};
+  const size_t nw = (size_t)(ctx->nx - 2) * (ctx->nzg - 3);
+  ctx->bc.wm_ax = mode ? ctx->d_wm : nullptr;
+  ctx->bc.wm_az = mode == 2 ? ctx->d_wm + nw : nullptr;
+  if (mode == 1) {  // Newton's first guess: utau_ref (initialization.f90:744-745)
+    std::vector<double> u(ctx->nx);
+    for (int i = 1; i <= ctx->nx; ++i) u[i - 1] = std::sqrt(0.5 * 0.027 * std::pow(ctx->x[i] / ctx->cfg.nu, -1.0 / 7.0));
+    CK(cudaMemcpy(ctx->d_utau, u.data(), ctx->nx * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return BLGPU_OK;
+}
+
+// the current model's wall stress on the current state at the wall points
+// (i = 2..nx-1 fastest, k = 2..nzg-2)
+int blgpu_wall_stress(blgpu_ctx *ctx, double *tau_x, double *tau_z) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->wm_mode) return set_err(ctx, BLGPU_ESTATE, "blgpu_wall_stress: no wall model set");
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_wall_stress: no grid/state");
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    ctx->launches += enq_wall_model<double>(ctx, S[0], S[2]);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    ctx->launches += enq_wall_model<float>(ctx, S[0], S[2]);
+  }
+  CK(cudaGetLastError());
+  const size_t nw = (size_t)(ctx->nx - 2) * (ctx->nzg - 3);
+  if (tau_x) CK(cudaMemcpyAsync(tau_x, ctx->d_wm + 2 * nw, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  if (tau_z) CK(cudaMemcpyAsync(tau_z, ctx->d_wm + 3 * nw, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return BLGPU_OK;
+}
+
+// append the wall samples of the solver's current state (features at row
+// jh, stress of the resolved wall gradient) to the network's training set
+int blgpu_mlp_sample(blgpu_mlp *m, blgpu_ctx *ctx, int jh) {
+  if (!ctx || !m) return set_err(ctx, BLGPU_EINVAL, "blgpu_mlp_sample: null argument");
+  if (jh < 2 || jh > ctx->nyg - 1) return set_err(ctx, BLGPU_EINVAL, "blgpu_mlp_sample: row %d outside 2..nyg-1", jh);
+  if (!ctx->have_grid || !ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_mlp_sample: no grid/state");
+  if (blgpu_mlp_device(m) != ctx->cfg.device) return set_err(ctx, BLGPU_EINVAL, "blgpu_mlp_sample: other device");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaStreamSynchronize(blgpu_mlp_stream(m)));
+  const int rows = (ctx->nx - 2) * (ctx->nzg - 3);
+  float *X = nullptr, *Tg = nullptr;
+  int rc = blgpu_mlp_reserve(m, rows, &X, &Tg);
+  if (rc) return set_err(ctx, rc, "blgpu_mlp_sample: %s", blgpu_mlp_last_error(m));
+  if (ctx->fp64) {
+    double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
+    launch_wall_samples<double>(ctx->geo, S[0], S[2], (const double *)ctx->P, jh, X, Tg, ctx->st);
+  } else {
+    float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
+    launch_wall_samples<float>(ctx->geo, S[0], S[2], (const float *)ctx->P, jh, X, Tg, ctx->st);
+  }
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  blgpu_mlp_commit(m, rows);
   return BLGPU_OK;
 }
 

@@ -33,6 +33,7 @@ struct BcData {
   const double *ut, *vt, *wt;                 // optional precomputed inflow perturbation planes
   int lund;                                   // 0 modes, 3 Lund plane, 5 Lund fluctuations
   const double *lu, *lv, *lw;                 // Lund planes (nyg,nzg) (ny,nzg) (nyg,nz), j fastest
+  const double *wm_ax, *wm_az;                // wall model: tau/nu_wall at (i,k), i=2..nx-1, k=2..nzg-2 (or null)
 };
 
 // Lund recycling/rescaling inflow state (rescaled_inlet_bc.f90:60-345), FP64.
@@ -58,7 +59,7 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
                    const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
                    const Scalars *sc, double c1, double c2, const Tiles &tl, cudaStream_t st);
 template <typename T>
-void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, T *U, T *V, T *W, T *P,
                     const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st);
 int bc_x_parts(const Geo &g);
 template <typename T>
@@ -77,7 +78,7 @@ template <typename T>
 void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, const T *nut, double *out,
                   cudaStream_t st);
 template <typename T>
-void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cudaStream_t st);
+void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int jref, cudaStream_t st);
 template <typename T>
 void launch_lund(const Geo &g, const LundData &L, const T *U, const T *V, const T *W, const Scalars *sc, int phase,
                  cudaStream_t st);
@@ -104,14 +105,20 @@ struct Spec {  // spectral layout of the Poisson solve
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    double *dc_sum, int nw, cudaStream_t st);
+                    int nw, cudaStream_t st);
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
                   int rk, cudaStream_t st);
 template <typename T>
 void launch_thomas(const Spec &s, typename vec2<T>::type *C, double *piv, const double *dd, const double *dl,
-                   const double *du, const double *kxx, const double *kzz, const double *dc_lines,
-                   double *dc_rows, double *dc_out, cudaStream_t st);
+                   const double *du, const double *kxx, const double *kzz, int skip_kz0, cudaStream_t st);
+// mixed form: the kz = 0 plane of the pressure solve in FP64, from the kz = 0
+// row of C (before the FP32 Thomas zeroes it) -> p0[NM][N]; H scratch
+// [NM][N]; cm[kx][i] = w_kx cos(pi kx (2i+1) / 2N) / (N M)
+template <typename T>
+void launch_kz0_plane(const Spec &s, const typename vec2<T>::type *C, double *H, double *p0, double *piv,
+                      const double *cm, const double *dd, const double *dl, const double *du, const double *kxx,
+                      double kz0, cudaStream_t st);
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, cudaStream_t st);
 size_t dct_smem_bytes(int n, int elem_bytes, int lines);

@@ -215,7 +215,7 @@ __device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const
 template <typename T, int MAXR>
 __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
                                                  const T *__restrict__ V, const T *__restrict__ W,
-                                                 T *__restrict__ R, double *__restrict__ dc_sum) {
+                                                 T *__restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = s.N;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -238,7 +238,6 @@ __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, c
   // line B aliases line A when it does not exist, so every load is valid
   const long long cbb = hb ? cb : ca;
   const int jb = hb ? bb + 2 : ba + 2, kbb = hb ? kb + 2 : ka + 2;
-  double sa = 0.0, sb = 0.0;
   // batches of 4 points per lane: all 48 loads issued before any use
   for (int base = 0; base < N; base += 128) {
     T fa[4], fb[4];
@@ -253,21 +252,9 @@ __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, c
       const int ip = base + lane + 32 * u;
       if (ip < N) {
         const T vb = hb ? fb[u] : (T)0;
-        sa += (double)fa[u];
-        sb += (double)vb;
         const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
         bufA[pos] = mk<T>(fa[u], vb);
       }
-    }
-  }
-  if (dc_sum) {  // FP64 line sums for the zero wavenumber (mixed form)
-    for (int o = 16; o > 0; o >>= 1) {
-      sa += __shfl_xor_sync(0xffffffffu, sa, o);
-      sb += __shfl_xor_sync(0xffffffffu, sb, o);
-    }
-    if (lane == 0) {
-      dc_sum[q] = sa;
-      if (hb) dc_sum[q + 1] = sb;
     }
   }
   __syncwarp();
@@ -526,15 +513,14 @@ __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restri
 // mode (0,0) scaled by 3/2, initialization.f90:454), sub dl[b] = Dyy(j,j-1),
 // super du[b] = Dyy(j,j+1).  Forward sweep writes g in place and the inverse
 // pivots to piv; the backward sweep reads them back.
-// dc_in/dc_out (mixed form): the (0,0) mode is solved from FP64 line sums
-// and its solution kept in FP64 (per-row constant), not in C.
+// skip_kz0 (mixed form): the kz = 0 plane is solved in FP64 by the kz0
+// kernels below, so its coefficients here are zeroed.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, double *__restrict__ piv,
                                                 const double *__restrict__ dd, const double *__restrict__ dl,
                                                 const double *__restrict__ du, const double *__restrict__ kxx,
-                                                const double *__restrict__ kzz, const double *__restrict__ dc_in,
-                                                double *__restrict__ dc_out) {
+                                                const double *__restrict__ kzz, int skip_kz0) {
   // lane pairs share a mode: even lane = real part, odd lane = imaginary part
   const int lane = threadIdx.x & 31, part = lane & 1;
   const int kx = blockIdx.x * 16 + (lane >> 1);
@@ -546,33 +532,8 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
   const double kk = kxx[kx];
   const double kzv = kzz[kz];
   const bool zero = (kx == 0 && kz == 0);
-  if (zero && dc_in) {
-    // mixed form: zero wavenumber from FP64 line sums, solution kept in FP64
-    if (part) return;
-    double dprev = 0.0, gr = 0.0;
-    for (int b = 0; b < NM; ++b) {
-      double r = dc_in[b];
-      double d = (dd[b] + kk) + kzv;
-      if (b == 0) d = 3.0 / 2.0 * d;
-      if (b > 0) {
-        const double w = dl[b] / dprev;
-        d = d - w * du[b - 1];
-        r = r - w * gr;
-      }
-      dprev = d;
-      gr = r;
-      dc_out[b] = r;
-      piv[base + b * rs] = 1.0 / d;
-    }
-    double x = dc_out[NM - 1] * piv[base + (NM - 1) * rs];
-    dc_out[NM - 1] = x;
-    for (int b = NM - 2; b >= 0; --b) {
-      x = (dc_out[b] - du[b] * x) * piv[base + b * rs];
-      dc_out[b] = x;
-    }
-    const double nrm = 1.0 / ((double)s.N * (double)s.M);
-    for (int b = 0; b < NM; ++b) dc_out[b] *= nrm;
-    for (int b = 0; b < NM; ++b) C[base + b * rs] = mk<T>(0, 0);
+  if (skip_kz0 && kz == 0) {
+    for (int b = 0; b < NM; ++b) reinterpret_cast<T *>(C)[2 * (base + b * rs) + part] = (T)0;
     return;
   }
   T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
@@ -643,13 +604,110 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
   }
 }
 
-// per-row sums of the FP64 line sums (mixed form zero wavenumber), fixed order
-__global__ void k_dc_rows(Spec s, const double *__restrict__ lines, double *__restrict__ rows) {
-  const int b = blockIdx.x, lane = threadIdx.x;
-  double acc = 0.0;
-  for (int kp = lane; kp < s.M; kp += 32) acc += lines[(long long)b * s.M + kp];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) rows[b] = acc;
+// ---------------------------------------------------------------------------
+// Mixed form: the kz = 0 plane of the pressure solve in FP64.  A step whose
+// inflow flux differs from the interior's drives a pressure that varies
+// along the whole box; FP32 keeps only ~7 digits of it, and near the wall
+// (small y spacings) the rounding noise of p alone leaves a divergence of
+// order eps32 |p| / dy^2.  The z-mean part of p carries that large-scale
+// field, so it is solved and kept in FP64:
+//   forcing  G(kx,j) = Re C(j, kz=0, kx)   (the FP32 transforms of the
+//            divergence: small numbers, accurate to FP32 relative to |div|)
+//   k_kz0_thomas: tridiagonal solve in y per kx in FP64 -> H(kx,j)
+//   k_kz0_idct:   p0(i,j) = sum_kx H(kx,j) w_kx cos(pi kx (2i+1)/2N)/(N M)
+//                 (w_0 = 1, w_kx = 2), a dense product with a cosine table
+// The FP32 Thomas then zeroes its kz = 0 coefficients, and the projection
+// adds the FP64 p0 to the FP32 part.  H and p0: [NM][N] doubles.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(64) k_kz0_thomas(Spec s, const T2<T> *__restrict__ C, double *__restrict__ H,
+                                                   double *__restrict__ piv, const double *__restrict__ dd,
+                                                   const double *__restrict__ dl, const double *__restrict__ du,
+                                                   const double *__restrict__ kxx, double kz0) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kx >= s.N) return;
+  const int N = s.N, NM = s.NM;
+  const long long rs = (long long)s.MH * s.rx;  // row stride of C (kz = 0 row of each b)
+  const double kk = kxx[kx];
+  constexpr int PF = 16;
+  double cur[PF], nxt[PF];
+#pragma unroll
+  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? (double)C[u * rs + kx].x : 0.0;
+  double rinv = 0.0, gr = 0.0;
+  for (int b0 = 0; b0 < NM; b0 += PF) {
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int bn = b0 + PF + u;
+      nxt[u] = bn < NM ? (double)C[bn * rs + kx].x : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int b = b0 + u;
+      if (b < NM) {
+        double r = cur[u];
+        double d = (dd[b] + kk) + kz0;
+        if (kx == 0 && b == 0) d = 3.0 / 2.0 * d;  // initialization.f90:454
+        if (b > 0) {
+          const double w = dl[b] * rinv;
+          d = d - w * du[b - 1];
+          r = r - w * gr;
+        }
+        rinv = 1.0 / d;
+        gr = r;
+        H[(long long)b * N + kx] = r;
+        piv[(long long)b * N + kx] = rinv;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) cur[u] = nxt[u];
+  }
+  double x = 0.0;
+  for (int b = NM - 1; b >= 0; --b) {
+    const double r = H[(long long)b * N + kx], pv = piv[(long long)b * N + kx];
+    x = (b == NM - 1) ? r * pv : (r - du[b] * x) * pv;
+    H[(long long)b * N + kx] = x;
+  }
+}
+
+// p0[b][i] = sum_kx H[b][kx] cm[kx][i]: 32 x 64 output tiles, k-tiles of 32
+__global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restrict__ H, const double *__restrict__ cm,
+                                                  double *__restrict__ p0) {
+  constexpr int BM = 32, BN = 64, BK = 32;
+  __shared__ double As[BK][BM + 1];
+  __shared__ double Bs[BK][BN];
+  const int N = s.N, NM = s.NM;
+  const int b0 = blockIdx.y * BM, i0 = blockIdx.x * BN;
+  const int t = threadIdx.x, tr = t >> 4, tc = t & 15;
+  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  for (int k0 = 0; k0 < N; k0 += BK) {
+    for (int q = t; q < BM * BK; q += 256) {
+      const int r = q / BK, c = q % BK;
+      As[c][r] = (b0 + r < NM && k0 + c < N) ? H[(long long)(b0 + r) * N + k0 + c] : 0.0;
+    }
+    for (int q = t; q < BK * BN; q += 256) {
+      const int r = q / BN, c = q % BN;
+      Bs[r][c] = (k0 + r < N && i0 + c < N) ? cm[(long long)(k0 + r) * N + i0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < BK; ++kk) {
+      const double a0 = As[kk][2 * tr], a1 = As[kk][2 * tr + 1];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double bv = Bs[kk][tc + 16 * q];
+        acc[0][q] += a0 * bv;
+        acc[1][q] += a1 * bv;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int b = b0 + 2 * tr + r, i = i0 + tc + 16 * q;
+      if (b < NM && i < N) p0[(long long)b * N + i] = acc[r][q];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -687,10 +745,10 @@ static int radix_class(const int *rad, int nst) {
 
 template <typename T, int MAXR>
 static void launch_div_dct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W,
-                               T *R, double *dc_sum, int nw, size_t sm, int grid, cudaStream_t st) {
+                               T *R, int nw, size_t sm, int grid, cudaStream_t st) {
   cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  k_div_dct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R, dc_sum);
+  k_div_dct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R);
 }
 
 template <typename T, int MAXR>
@@ -703,17 +761,17 @@ static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, c
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    double *dc_sum, int nw_req, cudaStream_t st) {
+                    int nw_req, cudaStream_t st) {
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T));
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
   const int grid = (ncl + nw - 1) / nw;
   switch (radix_class(pl.rad, pl.nst)) {
-    case 7: launch_div_dct_cls<T, 7>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
-    case 13: launch_div_dct_cls<T, 13>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
-    case 19: launch_div_dct_cls<T, 19>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
-    case 29: launch_div_dct_cls<T, 29>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
-    default: launch_div_dct_cls<T, 31>(g, s, pl, U, V, W, R, dc_sum, nw, sm, grid, st); break;
+    case 7: launch_div_dct_cls<T, 7>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 13: launch_div_dct_cls<T, 13>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 19: launch_div_dct_cls<T, 19>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 29: launch_div_dct_cls<T, 29>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    default: launch_div_dct_cls<T, 31>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
   }
 }
 
@@ -759,21 +817,29 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 
 template <typename T>
 void launch_thomas(const Spec &s, T2<T> *C, double *piv, const double *dd, const double *dl, const double *du,
-                   const double *kxx, const double *kzz, const double *dc_lines, double *dc_rows, double *dc_out,
-                   cudaStream_t st) {
-  if (dc_lines) k_dc_rows<<<s.NM, 32, 0, st>>>(s, dc_lines, dc_rows);
+                   const double *kxx, const double *kzz, int skip_kz0, cudaStream_t st) {
   dim3 grid((s.N + 15) / 16, (s.MH + 7) / 8);
-  k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dd, dl, du, kxx, kzz, dc_lines ? dc_rows : nullptr, dc_out);
+  k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dd, dl, du, kxx, kzz, skip_kz0);
+}
+
+template <typename T>
+void launch_kz0_plane(const Spec &s, const T2<T> *C, double *H, double *p0, double *piv, const double *cm,
+                      const double *dd, const double *dl, const double *du, const double *kxx, double kz0,
+                      cudaStream_t st) {
+  k_kz0_thomas<T><<<(s.N + 63) / 64, 64, 0, st>>>(s, C, H, piv, dd, dl, du, kxx, kz0);
+  k_kz0_idct<<<dim3((s.N + 63) / 64, (s.NM + 31) / 32), 256, 0, st>>>(s, H, cm, p0);
 }
 
 #define BLGPU_SPEC_INST(T)                                                                                        \
   template void launch_div_dct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, const T *, const T *, \
-                                  T *, double *, int, cudaStream_t);                                              \
+                                  T *, int, cudaStream_t);                                                        \
   template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, cudaStream_t); \
   template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
   template void launch_thomas<T>(const Spec &, T2<T> *, double *, const double *, const double *,                \
-                                 const double *, const double *, const double *, const double *, double *,       \
-                                 double *, cudaStream_t);
+                                 const double *, const double *, const double *, int, cudaStream_t);            \
+  template void launch_kz0_plane<T>(const Spec &, const T2<T> *, double *, double *, double *, const double *,   \
+                                    const double *, const double *, const double *, const double *, double,       \
+                                    cudaStream_t);
 BLGPU_SPEC_INST(double)
 BLGPU_SPEC_INST(float)
 

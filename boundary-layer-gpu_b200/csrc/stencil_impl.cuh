@@ -316,38 +316,10 @@ __global__ void __launch_bounds__(256) k_rhs_rk_dns(Geo g, MetT<T> m, const T *_
 // project_velocity (projection.f90:359-384) + pressure save at rk_step 1
 // (projection.f90:75-78, P(2:nxg-1,2:nyg-1,2:nzg-1) = rhs_p/(dt*rk2_coef(1,1))).
 // p holds rhs_p in the box layout (i=2..nx, j=2..ny, k=2..nz valid).
-// dc (mixed form only): per-row constant of the zero wavenumber, kept in FP64.
+// p0 (mixed form only): the z-mean part of rhs_p, kept in FP64 as a
+// [j-2][i-2] plane of pitch nx-2 (x-Neumann copy at i = nx).
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_project(Geo g, MetT<T> m, const T *__restrict__ p, const double *__restrict__ dc,
-                                                 T *__restrict__ U, T *__restrict__ V, T *__restrict__ W,
-                                                 T *__restrict__ P, const Scalars *__restrict__ sc, int save_p,
-                                                 int kchunk) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  if (i > g.nx || j > g.ny) return;
-  const int k0 = blockIdx.z * kchunk + 2;
-  const int k1 = min(k0 + kchunk - 1, g.nz);
-  const double den = save_p ? sc->dt * 0.5 : 1.0;  // dt*rk2_coef(1,1)
-  for (int k = k0; k <= k1; ++k) {
-    const long long c = bidx(g, i, j, k);
-    const T pc = __ldg(p + c);
-    if (i <= g.nx - 1) U[c] = U[c] - qdiv(__ldg(p + c + 1) - pc, m.xC[i], m.xrC[i]);
-    if (j <= g.ny - 1) {
-      T d = __ldg(p + c + g.px) - pc;
-      if (dc) d = (T)((double)d + (dc[j + 1 - 2] - dc[j - 2]));
-      V[c] = V[c] - qdiv(d, m.yC[j], m.yrC[j]);
-    }
-    if (k <= g.nz - 1) W[c] = W[c] - qdiv(__ldg(p + c + g.plane) - pc, m.zC[k], m.zrC[k]);
-    if (save_p) {
-      double pv = (double)pc;
-      if (dc) pv += dc[j - 2];
-      P[c] = (T)(pv / den);
-    }
-  }
-}
-
-// Vector form of k_project: a thread updates VN = 16/sizeof(T) consecutive
+// A thread updates VN = 16/sizeof(T) consecutive
 // points i0..i0+VN-1 (i0 = 2 + VN*q, a 16-byte aligned box position) with
 // 16-byte loads and stores; points outside the update ranges keep their
 // loaded value.
@@ -357,7 +329,7 @@ template <> struct V16<double> { typedef double2 t; };
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__restrict__ p,
-                                                   const double *__restrict__ dc, T *__restrict__ U,
+                                                   const double *__restrict__ p0, T *__restrict__ U,
                                                    T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
                                                    const Scalars *__restrict__ sc, int save_p) {
   typedef typename V16<T>::t VT;
@@ -381,16 +353,25 @@ __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__
   w.v = *reinterpret_cast<const VT *>(W + c);
   const bool vj = (j <= g.ny - 1), wk = (k <= g.nz - 1);
   const T yC = m.yC[j], yrC = m.yrC[j], zC = m.zC[k], zrC = m.zrC[k];
-  const double ddc = dc ? (dc[j + 1 - 2] - dc[j - 2]) : 0.0;
+  const int N = g.nx - 2;
+  const double *p0r = p0 ? p0 + (long long)(j - 2) * N : nullptr;  // row j of the FP64 part
+  const double *p0n = (p0 && vj) ? p0r + N : nullptr;               // row j+1
 #pragma unroll
   for (int e = 0; e < VN; ++e) {
     const int i = i0 + e;
     const T pe1 = (e + 1 < VN) ? pc.e[e + 1] : pe;
-    if (i <= g.nx - 1) u.e[e] = u.e[e] - qdiv(pe1 - pc.e[e], m.xC[i], m.xrC[i]);
+    if (i <= g.nx - 1) {
+      T dd = pe1 - pc.e[e];
+      if (p0) dd = (T)((double)dd + (p0r[min(i - 1, N - 1)] - p0r[i - 2]));
+      u.e[e] = u.e[e] - qdiv(dd, m.xC[i], m.xrC[i]);
+    }
     if (i <= g.nx) {
       if (vj) {
         T dd = pn.e[e] - pc.e[e];
-        if (dc) dd = (T)((double)dd + ddc);
+        if (p0) {
+          const int ic = min(i - 2, N - 1);
+          dd = (T)((double)dd + (p0n[ic] - p0r[ic]));
+        }
         v.e[e] = v.e[e] - qdiv(dd, yC, yrC);
       }
       if (wk) w.e[e] = w.e[e] - qdiv(pt.e[e] - pc.e[e], zC, zrC);
@@ -401,12 +382,11 @@ __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__
   *reinterpret_cast<VT *>(W + c) = w.v;
   if (save_p) {
     const double den = sc->dt * 0.5;  // dt*rk2_coef(1,1)
-    const double dj = dc ? dc[j - 2] : 0.0;
     Vec q;
 #pragma unroll
     for (int e = 0; e < VN; ++e) {
       double pv = (double)pc.e[e];
-      if (dc) pv += dj;
+      if (p0 && i0 + e <= g.nx) pv += p0r[min(i0 + e - 2, N - 1)];
       q.e[e] = (i0 + e <= g.nx) ? (T)(pv / den) : (T)0;
     }
     *reinterpret_cast<VT *>(P + c) = q.v;
@@ -569,9 +549,25 @@ __global__ void k_bc_y(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T
   if (i <= g.nx) U[bidx(g, i, g.nyg, k)] = (T)bc.U_top[i];
   V[bidx(g, i, g.ny, k)] = (T)bc.V_top[i];
   if (k <= g.nz) W[bidx(g, i, g.nyg, k)] = (T)bc.W_top[i];
-  if (i <= g.nx) U[bidx(g, i, 1, k)] = -U[bidx(g, i, 2, k)];
+  // a wall model replaces the no-slip U (and W) rows by the non-zero Neumann
+  // condition F(:,1,:) = F(:,2,:) - alpha (yg(2) - yg(1)) of
+  // boundary_conditions.f90:359-372, alpha = tau_wall / nu_wall per wall
+  // point (i = 2..nx-1, k = 2..nzg-2; ghost rows take their periodic / end value)
+  if (bc.wm_ax) {
+    const int ic = min(max(i, 2), g.nx - 1);
+    const int kc = k == 1 ? g.nzg - 2 : (k == g.nzg - 1 ? 2 : (k == g.nzg ? 3 : k));
+    const long long q = (long long)(kc - 2) * (g.nx - 2) + (ic - 2);
+    const double dy = g.yg[2] - g.yg[1];
+    if (i <= g.nx) U[bidx(g, i, 1, k)] = (T)((double)U[bidx(g, i, 2, k)] - bc.wm_ax[q] * dy);
+    if (k <= g.nz) {
+      if (bc.wm_az) W[bidx(g, i, 1, k)] = (T)((double)W[bidx(g, i, 2, k)] - bc.wm_az[q] * dy);
+      else W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
+    }
+  } else {
+    if (i <= g.nx) U[bidx(g, i, 1, k)] = -U[bidx(g, i, 2, k)];
+    if (k <= g.nz) W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
+  }
   V[bidx(g, i, 1, k)] = (T)0;
-  if (k <= g.nz) W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
 }
 
 template <typename T>
@@ -790,15 +786,16 @@ __global__ void k_stats(Geo g, const T *__restrict__ U, const T *__restrict__ V,
 // ---------------------------------------------------------------------------
 // equilibrium law of the wall at each x (wallmodel.f90:1951-1985) solved with
 // Newton_iter_solver (Newton_solver.f90:13-79): kappa = 0.38, B = 5.2,
-// y = yg(3), at most 30 iterations, stop when |f| < 1e-10.  utau holds the
+// y = yg(jref) (jref = 3 in the reference), at most 30 iterations, stop when
+// |f| < 1e-10.  utau holds the
 // initial guess on entry (the previous model) and the model on exit; iters
 // receives the iteration count of each x.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_law_of_wall(Geo g, const T *__restrict__ U, double *__restrict__ utau, int *__restrict__ iters) {
+__global__ void k_law_of_wall(Geo g, const T *__restrict__ U, double *__restrict__ utau, int *__restrict__ iters,
+                              int jref) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (i > g.nx - 1) return;
-  const int jref = 3;
   const double kap = 0.38, B = 5.20, yref = g.yg[jref], nu = g.nu;
   double x = utau[i - 1];
   double um = 0.0;
@@ -863,13 +860,13 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 }
 
 template <typename T>
-void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *dc, T *U, T *V, T *W, T *P,
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, T *U, T *V, T *W, T *P,
                     const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st) {
   constexpr int VN = 16 / sizeof(T);
   const int ngrp = (g.nx - 1 + VN - 1) / VN;  // i = 2..nx in groups of VN
   const int by = tl.proj_by > 0 ? tl.proj_by : 8;
   dim3 block(32, by), grid((ngrp + 31) / 32, (g.ny - 1 + by - 1) / by, g.nz - 1);
-  k_project_v<T><<<grid, block, 0, st>>>(g, m, p, dc, U, V, W, P, sc, save_p);
+  k_project_v<T><<<grid, block, 0, st>>>(g, m, p, p0, U, V, W, P, sc, save_p);
   if (save_p) {
     dim3 b2(32, 8);
     k_p_ghost<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 0);
@@ -929,8 +926,8 @@ void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, 
 }
 
 template <typename T>
-void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cudaStream_t st) {
-  k_law_of_wall<T><<<(g.nx + 127) / 128, 128, 0, st>>>(g, U, utau, iters);
+void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int jref, cudaStream_t st) {
+  k_law_of_wall<T><<<(g.nx + 127) / 128, 128, 0, st>>>(g, U, utau, iters, jref);
 }
 
 #define BLGPU_INST(T)                                                                                                \
@@ -947,7 +944,7 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, cuda
                                       cudaStream_t);                                                                \
   template void launch_stats<T>(const Geo &, const T *, const T *, const T *, const T *, const T *, double *,       \
                                 cudaStream_t);                                                                      \
-  template void launch_law_of_wall<T>(const Geo &, const T *, double *, int *, cudaStream_t);
+  template void launch_law_of_wall<T>(const Geo &, const T *, double *, int *, int, cudaStream_t);
 BLGPU_INST(BLGPU_STENCIL_T)
 
 }  // namespace blgpu
@@ -1063,22 +1060,28 @@ __global__ void __launch_bounds__(256) k_lund_rows(Geo g, LundData L, const Scal
   __syncthreads();
   __shared__ double sh[8];
   const double *Umr = L.mean, *Umi = L.mean + nyg, *Vmr = L.mean + 2 * nyg;
+  // the four serial scans run on four warps at once
+  const double Uinf = L.inst[nyg - 1];
+  if (tid == 0) sh[1] = lund_delta99(Umr, g.yg, nyg, 0.99 * Uinf);
+  if (tid == 32) sh[2] = lund_delta99(Umi, g.yg, nyg, 0.99 * Uinf);
+  if (tid == 64) sh[3] = lund_theta(Umr, g.yg, nyg, Uinf);
+  if (tid == 96) sh[4] = lund_theta(Umi, g.yg, nyg, Uinf);
+  __syncthreads();
   if (tid == 0) {
-    const double Uinf = L.inst[nyg - 1];
-    const double Umean99 = 0.99 * Uinf;
-    const double d_resc = lund_delta99(Umr, g.yg, nyg, Umean99);
-    const double d_in2 = lund_delta99(Umi, g.yg, nyg, Umean99);
-    const double th_r = lund_theta(Umr, g.yg, nyg, Uinf), th_i = lund_theta(Umi, g.yg, nyg, Uinf);
+    const double th_r = sh[3], th_i = sh[4];
     const double uv = L.inst[2 * nyg + 2 * ny];
     const double dUw = (Umr[1] - Umr[0]) / (g.yg[2] - g.yg[1]);
     const double ut_r = sqrt(fabs(g.nu * dUw - uv));
     const double ut_i = ut_r * pow(th_r / th_i, 1.0 / 8.0);
     const double gam = ut_i / ut_r;
-    const double dg[8] = {Uinf, d_resc, d_in2, th_r, th_i, ut_r, ut_i, gam};
-    for (int q = 0; q < 8; ++q) { sh[q] = dg[q]; L.diag[q] = dg[q]; }
+    sh[0] = Uinf;
+    sh[5] = ut_r;
+    sh[6] = ut_i;
+    sh[7] = gam;
+    for (int q = 0; q < 8; ++q) L.diag[q] = sh[q];
   }
   __syncthreads();
-  const double Uinf = sh[0], d_resc = sh[1], ut_r = sh[5], ut_i = sh[6], gam = sh[7];
+  const double d_resc = sh[1], ut_r = sh[5], ut_i = sh[6], gam = sh[7];
   const double alpha = 4.0, bb = 0.2;
   for (int q = tid; q < 4 * nyg; q += nt) {
     const int m = q / nyg, i = q % nyg + 1;  // target row i of map m
@@ -1088,9 +1091,15 @@ __global__ void __launch_bounds__(256) k_lund_rows(Geo g, LundData L, const Scal
     double coef = 0.0;
     if (i > 1) {
       const double yi = lund_coord(g, m, i, ut_i, L.delta_inlet);
-      j = 0;
-      for (int k = 1; k <= n1; ++k)
-        if (lund_coord(g, m, k, ut_r, d_resc) > yi) { j = k; break; }
+      // first k in 1..n1 with ys(k) > yi; ys is non-decreasing in k, so a
+      // bisection finds the same k as the reference's forward scan
+      int lo = 1, hi = n1 + 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (lund_coord(g, m, mid, ut_r, d_resc) > yi) hi = mid;
+        else lo = mid + 1;
+      }
+      j = lo <= n1 ? lo : 0;
       if (j == 1) { atomicOr(L.err, 1); j = 0; }
       if (j > 0) {
         const double ysj = lund_coord(g, m, j, ut_r, d_resc), ysm = lund_coord(g, m, j - 1, ut_r, d_resc);

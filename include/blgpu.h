@@ -245,6 +245,51 @@ long long blgpu_ensemble_launches(const blgpu_ensemble *ens);
  * that shape take its tiles.  ntuned (may be NULL) = shapes tuned. */
 int blgpu_ensemble_autotune(blgpu_ensemble *ens, int steps, int *ntuned);
 
+/* ---- learned wall model (no counterpart in the reference) ----
+ * A 4 -> 64 -> 64 -> 64 -> 2 GELU network evaluated and trained on the
+ * tensor cores (BF16 operands, FP32 accumulation).  Parameters are FP32 in
+ * the order W0[64][4] b0[64] W1[64][64] b1[64] W2[64][64] b2[64] W3[2][64]
+ * b3[2] (blgpu_mlp_nparams() = 8770).  Inputs per wall point: u and w at the
+ * sampling row jh, ln(h |u| / nu) / 10 and 100 h dP/dx (h = yg(jh));
+ * outputs: 1000 tau_x, 1000 tau_z.  Loss: mean over samples of the summed
+ * squared output error. */
+typedef struct blgpu_mlp blgpu_mlp;
+int blgpu_mlp_nparams(void);
+int blgpu_mlp_create(int device, unsigned long long seed, blgpu_mlp **net); /* Glorot init */
+int blgpu_mlp_destroy(blgpu_mlp *net);
+const char *blgpu_mlp_last_error(const blgpu_mlp *net);
+int blgpu_mlp_set_params(blgpu_mlp *net, const float *params, int n); /* resets the Adam state */
+int blgpu_mlp_get_params(blgpu_mlp *net, float *params, int n);
+/* host arrays X[rows][4] -> Y[rows][2] */
+int blgpu_mlp_forward(blgpu_mlp *net, const float *X, int rows, float *Y);
+/* loss and its gradient (8770 values) over host samples X[rows][4], T[rows][2] */
+int blgpu_mlp_gradient(blgpu_mlp *net, const float *X, const float *T, int rows, float *grad, float *loss);
+/* the device training set */
+int blgpu_mlp_add_data(blgpu_mlp *net, const float *X, const float *T, int rows);
+int blgpu_mlp_sample(blgpu_mlp *net, blgpu_ctx *ctx, int jh); /* wall samples of the solver state */
+int blgpu_mlp_clear_data(blgpu_mlp *net);
+int blgpu_mlp_num_samples(const blgpu_mlp *net);
+int blgpu_mlp_get_data(blgpu_mlp *net, float *X, float *T, int rows);
+/* `steps` Adam steps (lr, betas 0.9 / 0.999) on minibatches of `batch`
+ * samples in a shuffled order; loss_last = loss of the last batch */
+int blgpu_mlp_train(blgpu_mlp *net, int steps, int batch, float lr, float *loss_last);
+int blgpu_mlp_steps(blgpu_mlp *net, long long *steps);
+int blgpu_mlp_loss_history(blgpu_mlp *net, float *hist, int n);
+int blgpu_mlp_eval(blgpu_mlp *net, float *loss); /* loss over the whole training set */
+
+/* Wall model of the step, evaluated at the start of every substep
+ * (time_integration.f90:341-346) from the substep's fields and applied as
+ * the non-zero Neumann condition U(:,1,:) = U(:,2,:) - tau/nu_w (yg(2)-yg(1))
+ * (boundary_conditions.f90:359-372), nu_w the viscosity of the wall flux (nu
+ * plus the interpolated eddy viscosity with LES).  mode 0: no-slip (the
+ * reference GPU routine); 1: law of the wall (wallmodel.f90:1951-1985) at
+ * row jh, tau = u_tau(x)^2, V and W no-slip; 2: the network at row jh,
+ * tau_x on U and tau_z on W. */
+int blgpu_set_wall_model(blgpu_ctx *ctx, int mode, int jh, const blgpu_mlp *net);
+/* the model's stress on the current state at i = 2..nx-1 (fastest),
+ * k = 2..nzg-2: (nx-2)(nzg-3) values each */
+int blgpu_wall_stress(blgpu_ctx *ctx, double *tau_x, double *tau_z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "bl_oracle.c")
+SRCS = [SRC, os.path.join(HERE, "mlp_oracle.c")]
 LIB = os.path.join(HERE, "liboracle.so")
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -32,10 +33,10 @@ _dp = ctypes.POINTER(ctypes.c_double)
 def build(force=False):
     """gcc -O2 -ffp-contract=off -fopenmp; output oracle/liboracle.so."""
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(
-            os.path.getmtime(SRC), os.path.getmtime(os.path.join(HERE, "bl_oracle.h"))):
+            [os.path.getmtime(p) for p in SRCS] + [os.path.getmtime(os.path.join(HERE, "bl_oracle.h"))]):
         return LIB
     cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=gnu99",
-           "-o", LIB + ".tmp", SRC, "-lm"]
+           "-o", LIB + ".tmp"] + SRCS + ["-lm"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
@@ -90,6 +91,14 @@ def load():
                                           ctypes.c_double, _dp, _dp]
         lib.blo_rescaled_inflow.argtypes = [ctypes.c_void_p]
         lib.blo_get_rescaling.argtypes = [ctypes.c_void_p] + [_dp] * 8 + [ctypes.POINTER(ctypes.c_int)]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        lib.blo_mlp_nparams.restype = ctypes.c_int
+        lib.blo_mlp_forward.argtypes = [_dp, _fp, ctypes.c_int, _fp, ctypes.c_int]
+        lib.blo_mlp_gradient.restype = ctypes.c_double
+        lib.blo_mlp_gradient.argtypes = [_dp, _fp, _fp, ctypes.c_int, _dp, ctypes.c_int]
+        lib.blo_set_wall_model.restype = ctypes.c_int
+        lib.blo_set_wall_model.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        lib.blo_wall_stress.argtypes = [ctypes.c_void_p, _dp, _dp]
         _lib = lib
     return _lib
 
@@ -275,6 +284,45 @@ class Oracle:
                  "gamma"]
         return dict(Umean_resc=um, Vmean_resc=vm, Umean_inlet=ui, Vmean_inlet=vi, U=lu, V=lv, W=lw,
                     diag=dict(zip(names, dg)), err=err.value)
+
+    def set_wall_model(self, mode, jh=3, params=None):
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        rc = self.lib.blo_set_wall_model(self.h, mode, jh, _p(p) if p is not None else None)
+        if rc:
+            raise ValueError("blo_set_wall_model: %d" % rc)
+
+    def wall_stress(self):
+        """(tau_x, tau_z) of the wall model on the current state, shape (nzg-3, nx-2)."""
+        n = (self.nx - 2) * (self.nzg - 3)
+        tx, tz = np.zeros(n), np.zeros(n)
+        self.lib.blo_wall_stress(self.h, _p(tx), _p(tz))
+        return tx.reshape(self.nzg - 3, self.nx - 2), tz.reshape(self.nzg - 3, self.nx - 2)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_forward(params, X, exact=False):
+    """Network outputs Y[rows][2] for inputs X[rows][4] (the BF16 roundings of
+    the tensor-core kernels unless exact)."""
+    lib = load()
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros((X.shape[0], 2), dtype=np.float32)
+    lib.blo_mlp_forward(_p(p), _fptr(X), X.shape[0], _fptr(Y), 1 if exact else 0)
+    return Y
+
+
+def mlp_gradient(params, X, T, exact=False):
+    """(loss, gradient[8770]) of the network over samples X, T."""
+    lib = load()
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    g = np.zeros(lib.blo_mlp_nparams())
+    loss = lib.blo_mlp_gradient(_p(p), _fptr(X), _fptr(T), X.shape[0], _p(g), 1 if exact else 0)
+    return loss, g
 
 
 def oracle_for(case, variant=0, threads=1):

@@ -323,6 +323,9 @@ struct blo {
   double *Umr, *Vmr, *Umi, *Vmi;   /* Umean_resc_T(nyg) Vmean_resc_T(ny) Umean_inlet_T Vmean_inlet_T, 1-based */
   double *Lu, *Lv, *Lw;            /* Ut_inlet(nyg,nzg) Vt_inlet(ny,nzg) Wt_inlet(nyg,nz) */
   double lund_diag[8];
+  /* wall model */
+  int wm, wm_jh;
+  double *wm_ax, *wm_az, *utau_wm, *mlp_params;
 };
 
 static int nthreads_req = 1;
@@ -383,6 +386,10 @@ blo_t *blo_create(int nx, int ny, int nz, double nu, double cfl, double dpdx,
   o->Umi = dalloc(o->nyg + 1); o->Vmi = dalloc(ny + 1);
   o->Lu = dalloc((size_t)o->nyg * o->nzg); o->Lv = dalloc((size_t)ny * o->nzg);
   o->Lw = dalloc((size_t)o->nyg * nz);
+  o->wm_ax = dalloc((size_t)(nx - 2) * (o->nzg - 3));
+  o->wm_az = dalloc((size_t)(nx - 2) * (o->nzg - 3));
+  o->utau_wm = dalloc(nx);
+  o->mlp_params = dalloc(blo_mlp_nparams());
   o->rk_t[0] = 0.0; o->rk_t[1] = 8.0 / 15.0; o->rk_t[2] = 2.0 / 3.0; o->rk_t[3] = 1.0;
   memset(o->rk_coef, 0, sizeof(o->rk_coef));
   o->rk_coef[0][0] = 8.0 / 15.0;
@@ -404,7 +411,8 @@ void blo_destroy(blo_t *o) {
                     o->V, o->W, o->P, o->Uo, o->Vo, o->Wo, o->nu_t, o->rhs_p,
                     o->U_inlet, o->V_inlet, o->W_inlet, o->U_top, o->V_top,
                     o->W_top, o->Ut, o->Vt, o->Wt, o->zmode, o->tmode,
-                    o->Umr, o->Vmr, o->Umi, o->Vmi, o->Lu, o->Lv, o->Lw};
+                    o->Umr, o->Vmr, o->Umi, o->Vmi, o->Lu, o->Lv, o->Lw, o->wm_ax, o->wm_az,
+                    o->utau_wm, o->mlp_params};
   for (size_t q = 0; q < sizeof(arrs) / sizeof(arrs[0]); ++q) free(arrs[q]);
   for (int s = 0; s < 3; ++s) { free(o->Fu[s]); free(o->Fv[s]); free(o->Fw[s]); }
   free(o->qu); free(o->qv); free(o->qw);
@@ -869,13 +877,27 @@ void blo_apply_bc(blo_t *o, int rk_step) {
     for (int i = 1; i <= nxg; ++i) AV(V, i, ny, k) = o->V_top[i];
   for (int k = 1; k <= nz; ++k)
     for (int i = 1; i <= nxg; ++i) AW(W, i, nyg, k) = o->W_top[i];
-  /* wall (:230-237) */
-  for (int k = 1; k <= nzg; ++k)
-    for (int i = 1; i <= nx; ++i) AU(U, i, 1, k) = -AU(U, i, 2, k);
+  /* wall (:230-237); with a wall model the non-zero Neumann condition of
+   * :359-372 on U (and on W for the network), alpha = tau/nu_w at the wall
+   * point (i clamped to 2..nx-1, ghost k planes to their periodic image) */
+  if (o->wm) {
+    const double dy = o->yg[2] - o->yg[1];
+    for (int k = 1; k <= nzg; ++k)
+      for (int i = 1; i <= nxg; ++i) {
+        const int ic = i < 2 ? 2 : (i > nx - 1 ? nx - 1 : i);
+        const int kc = k == 1 ? nzg - 2 : (k == nzg - 1 ? 2 : (k == nzg ? 3 : k));
+        const size_t q = (size_t)(kc - 2) * (nx - 2) + (ic - 2);
+        if (i <= nx) AU(U, i, 1, k) = AU(U, i, 2, k) - o->wm_ax[q] * dy;
+        if (k <= nz) AW(W, i, 1, k) = o->wm == 2 ? AW(W, i, 2, k) - o->wm_az[q] * dy : -AW(W, i, 2, k);
+      }
+  } else {
+    for (int k = 1; k <= nzg; ++k)
+      for (int i = 1; i <= nx; ++i) AU(U, i, 1, k) = -AU(U, i, 2, k);
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nxg; ++i) AW(W, i, 1, k) = -AW(W, i, 2, k);
+  }
   for (int k = 1; k <= nzg; ++k)
     for (int i = 1; i <= nxg; ++i) AV(V, i, 1, k) = 0.0;
-  for (int k = 1; k <= nz; ++k)
-    for (int i = 1; i <= nxg; ++i) AW(W, i, 1, k) = -AW(W, i, 2, k);
   /* global mass conservation (:240-260), kk = 2 at nprocs = 1 */
   double Qx = 0.0, length_y = 0.0, Qy = 0.0;
   for (int j = 2; j <= nyg - 1; ++j) {
@@ -1414,10 +1436,12 @@ void blo_get_rescaling(const blo_t *o, double *Umean_resc, double *Vmean_resc, d
 }
 
 void blo_smagorinsky(blo_t *o);
+static void wall_model_eval(blo_t *o);
 static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms,
                     double tnew) {
   o->rk_step = rk_step;
   if (o->les == 1) blo_smagorinsky(o); /* time_integration.f90:341-346 */
+  if (o->wm) wall_model_eval(o);
   rhs_u_impl(o, o->U, o->V, o->W, o->Fu[s]);
   rhs_v_impl(o, o->U, o->V, o->W, o->Fv[s]);
   rhs_w_impl(o, o->U, o->V, o->W, o->Fw[s]);
@@ -1448,6 +1472,8 @@ void blo_step(blo_t *o) {
   } else {
     /* Euler: U = Uo + dt*rhs(Uo); rk_step = 3 (time_integration.f90:24-114) */
     o->rk_step = 3;
+    if (o->les == 1) blo_smagorinsky(o);
+    if (o->wm) wall_model_eval(o);
     rhs_u_impl(o, o->Uo, o->Vo, o->Wo, o->Fu[0]);
     rhs_v_impl(o, o->Uo, o->Vo, o->Wo, o->Fv[0]);
     rhs_w_impl(o, o->Uo, o->Vo, o->Wo, o->Fw[0]);
@@ -1630,8 +1656,10 @@ void blo_statistics(const blo_t *o, double *means, double *nu_t_mean, double *Cf
 /* y = yg(3), 30 iterations, |f| < 1e-10.  utau (nx) is the initial guess on */
 /* entry and the model on exit; returns the largest iteration count.         */
 /* ------------------------------------------------------------------------ */
-int blo_law_of_wall(const blo_t *o, double *utau) {
-  const int jref = 3;
+static int law_of_wall_at(const blo_t *o, int jref, double *utau);
+int blo_law_of_wall(const blo_t *o, double *utau) { return law_of_wall_at(o, 3, utau); }
+
+static int law_of_wall_at(const blo_t *o, int jref, double *utau) {
   const double kap = 0.38, B = 5.20, yref = o->yg[jref], nu = o->nu;
   int iters_max = 0;
   for (int i = 2; i <= o->nx - 1; ++i) {
@@ -1657,3 +1685,76 @@ int blo_law_of_wall(const blo_t *o, double *utau) {
 }
 
 void blo_set_les(blo_t *o, int les_model) { o->les = les_model; }
+
+/* ------------------------------------------------------------------------ */
+/* wall models of the step                                                  */
+/* ------------------------------------------------------------------------ */
+int blo_set_wall_model(blo_t *o, int mode, int jh, const double *params) {
+  if (mode < 0 || mode > 2) return -1;
+  if (mode && (jh < 2 || jh > o->nyg - 1)) return -2;
+  if (mode == 2 && !params) return -3;
+  o->wm = mode;
+  o->wm_jh = jh;
+  if (mode == 2) memcpy(o->mlp_params, params, sizeof(double) * blo_mlp_nparams());
+  /* Newton's first guess utau_ref (initialization.f90:744-745) */
+  for (int i = 1; i <= o->nx; ++i) o->utau_wm[i - 1] = sqrt(0.5 * 0.027 * pow(o->x[i] / o->nu, -1.0 / 7.0));
+  return 0;
+}
+
+/* the network's inputs at wall point (i,k) from row jh */
+static void wall_features(const blo_t *o, int i, int jh, int k, float *x) {
+  const double h = o->yg[jh];
+  const double u = AU(o->U, i, jh, k);
+  const double w = 0.25 * (AW(o->W, i, jh, k) + AW(o->W, i + 1, jh, k) + AW(o->W, i, jh, k - 1) +
+                           AW(o->W, i + 1, jh, k - 1));
+  const double dp = (AP(o->P, i + 1, jh, k) - AP(o->P, i, jh, k)) / (o->xg[i + 1] - o->xg[i]);
+  x[0] = (float)u;
+  x[1] = (float)w;
+  x[2] = (float)(log(fmax(h * fabs(u) / o->nu, 1.0)) / 10.0);
+  x[3] = (float)(100.0 * h * dp);
+}
+
+/* viscosity of the U-equation's wall flux at (i,k): nu_y1 of the LES branch
+ * (equations.f90:97-98) at j = 2, nu alone without LES */
+static double wall_flux_nu(const blo_t *o, int i, int k) {
+  if (!o->les) return o->nu;
+  return o->nu + 0.5 * (o->wy0[1] * AP(o->nu_t, i, 1, k) + o->wy1[1] * AP(o->nu_t, i, 2, k) +
+                        o->wy0[1] * AP(o->nu_t, i + 1, 1, k) + o->wy1[1] * AP(o->nu_t, i + 1, 2, k));
+}
+
+static void wall_model_eval(blo_t *o) {
+  const int ni = o->nx - 2, nk = o->nzg - 3;
+  if (o->wm == 1) {
+    law_of_wall_at(o, o->wm_jh, o->utau_wm);
+    for (int k = 0; k < nk; ++k)
+      for (int q = 0; q < ni; ++q) {
+        const double u = o->utau_wm[q + 1];
+        o->wm_ax[(size_t)k * ni + q] = u * u / wall_flux_nu(o, q + 2, k + 2);
+        o->wm_az[(size_t)k * ni + q] = 0.0;
+      }
+  } else if (o->wm == 2) {
+    const int rows = ni * nk;
+    float *X = (float *)malloc(sizeof(float) * 4 * (size_t)rows), *Y = (float *)malloc(sizeof(float) * 2 * (size_t)rows);
+    for (int r = 0; r < rows; ++r) wall_features(o, r % ni + 2, o->wm_jh, r / ni + 2, X + (size_t)r * 4);
+    blo_mlp_forward(o->mlp_params, X, rows, Y, 0);
+    for (int r = 0; r < rows; ++r) {
+      const double nuw = wall_flux_nu(o, r % ni + 2, r / ni + 2);
+      o->wm_ax[r] = 1e-3 * (double)Y[(size_t)r * 2] / nuw;
+      o->wm_az[r] = 1e-3 * (double)Y[(size_t)r * 2 + 1] / nuw;
+    }
+    free(X);
+    free(Y);
+  }
+}
+
+void blo_wall_stress(blo_t *o, double *tau_x, double *tau_z) {
+  wall_model_eval(o);
+  const int ni = o->nx - 2;
+  const size_t n = (size_t)ni * (o->nzg - 3);
+  for (size_t q = 0; q < n; ++q) {
+    const double nuw = wall_flux_nu(o, (int)(q % ni) + 2, (int)(q / ni) + 2);
+    if (tau_x) tau_x[q] = o->wm_ax[q] * nuw;
+    if (tau_z) tau_z[q] = o->wm_az[q] * nuw;
+  }
+}
+

@@ -86,6 +86,19 @@ void blo_rescaled_inflow(blo_t *o);
 void blo_get_rescaling(const blo_t *o, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
                        double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err);
 
+/* wall-stress network (mlp_oracle.c): params[8770] in the device order;
+ * exact = 0 rounds like the BF16 tensor-core kernels, 1 is plain FP64 */
+int blo_mlp_nparams(void);
+void blo_mlp_forward(const double *params, const float *X, int rows, float *Y, int exact);
+double blo_mlp_gradient(const double *params, const float *X, const float *T, int rows, double *grad, int exact);
+
+/* wall model of the step (mode 0 no-slip, 1 law of the wall at row jh,
+ * 2 the network at row jh with params[8770]), evaluated at the start of
+ * every substep and applied as U(:,1,:) = U(:,2,:) - tau/nu_w (yg(2)-yg(1)) */
+int blo_set_wall_model(blo_t *o, int mode, int jh, const double *params);
+/* the model's stress on the current state: (nx-2)(nzg-3) values each */
+void blo_wall_stress(blo_t *o, double *tau_x, double *tau_z);
+
 /* test hooks for the transform and the tridiagonal solver */
 void blo_fft(int n, double *data, int inverse);
 int blo_zgtsv(int n, double *dl, double *d, double *du, double *b);

@@ -130,3 +130,38 @@ def test_lund_gamma_follows_momentum_thickness():
     assert abs(d["gamma"] - (d["theta_resc"] / d["theta_inlet"]) ** 0.125) < 1e-14
     inst = c.U[19, :, 1:-1].mean(axis=1)
     assert np.allclose(r["Umean_resc"], 0.1 * inst + 0.9 * m0, rtol=0, atol=1e-14)
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The oracle's back-propagation (plain FP64 mode) against central
+    differences of its loss, and its BF16 mode within the BF16 rounding."""
+    rng = np.random.default_rng(0)
+    n = oracle.load().blo_mlp_nparams()
+    assert n == 8770
+    p = rng.standard_normal(n) * 0.2
+    X = rng.standard_normal((40, 4)).astype(np.float32)
+    T = rng.standard_normal((40, 2)).astype(np.float32)
+    loss, g = oracle.mlp_gradient(p, X, T, exact=True)
+    idx = rng.choice(n, 25, replace=False)
+    h = 1e-6
+    for q in idx:
+        pp, pm = p.copy(), p.copy()
+        pp[q] += h
+        pm[q] -= h
+        fd = (oracle.mlp_gradient(pp, X, T, exact=True)[0] - oracle.mlp_gradient(pm, X, T, exact=True)[0]) / (2 * h)
+        assert abs(fd - g[q]) <= 1e-6 * max(1.0, abs(g[q]))
+    lb, gb = oracle.mlp_gradient(p, X, T)
+    assert abs(lb - loss) < 1e-2 * loss
+    assert np.linalg.norm(gb - g) < 2e-2 * np.linalg.norm(g)
+
+
+def test_wall_model_law_of_the_wall_on_log_profile():
+    """On a mean profile that follows u+ = ln(y+)/kappa + B at the sampling
+    row, the equilibrium wall model returns that profile's u_tau^2."""
+    from blgpu import wallmodel
+    c = wallmodel.wmles_case(nx=24, nz=8)
+    o = oracle.oracle_for(c)
+    o.set_wall_model(1, 3)
+    tx, tz = o.wall_stress()
+    assert abs(tx.mean() / c.utau ** 2 - 1) < 0.02
+    assert np.all(tz == 0.0)
