@@ -207,13 +207,19 @@ def turbulent_top(x, nu, u_inf=1.0):
 # ---------------------------------------------------------------------------
 # turbulent mean profile (composite law of the wall + Coles wake)
 # ---------------------------------------------------------------------------
-def composite_profile(y, delta, utau, nu, kappa=0.38, B=5.2, Pi=0.45, u_inf=1.0):
-    """Reichardt's inner law blended with Coles' wake, clipped at U_inf above
-    delta.  kappa and B default to the constants of the reference's
-    equilibrium wall model (wallmodel.f90:1960-1961); Reichardt's constant is
-    chosen so that the profile tends to u+ = ln(y+)/kappa + B in the log layer."""
+# the reference's equilibrium wall-model constants (wallmodel.f90:1960-1961)
+KAPPA_WM, B_WM = 0.38, 5.2
+
+
+def reichardt_c(kappa, B):
+    """Reichardt's constant for which his law tends to ln(y+)/kappa + B."""
+    return B - math.log(kappa) / kappa
+
+
+def composite_profile(y, delta, utau, nu, kappa=0.41, C=7.8, Pi=0.45, u_inf=1.0):
+    """Reichardt's inner law (constant C) blended with Coles' wake, clipped at
+    U_inf above delta."""
     yp = np.maximum(y, 0.0) * utau / nu
-    C = B - math.log(kappa) / kappa
     up = (1.0 / kappa) * np.log1p(kappa * yp) + C * (1.0 - np.exp(-yp / 11.0) - (yp / 11.0) * np.exp(-yp / 3.0))
     eta = np.clip(y / delta, 0.0, 1.0)
     wake = 2.0 * Pi / kappa * np.sin(0.5 * np.pi * eta) ** 2
@@ -222,7 +228,7 @@ def composite_profile(y, delta, utau, nu, kappa=0.38, B=5.2, Pi=0.45, u_inf=1.0)
     return np.where(y < 0, -u, u)
 
 
-def turbulent_inflow_profile(retheta, delta=1.0, u_inf=1.0, n_fit=4000):
+def turbulent_inflow_profile(retheta, delta=1.0, u_inf=1.0, n_fit=4000, kappa=0.41, C=7.8):
     """nu and utau for which the composite profile of thickness delta has
     momentum thickness Re_theta (Coles-Fernholz skin friction)."""
     # Coles-Fernholz: cf = 2 (1/0.384 ln Re_theta + 4.127)^-2
@@ -231,7 +237,7 @@ def turbulent_inflow_profile(retheta, delta=1.0, u_inf=1.0, n_fit=4000):
     yy = np.linspace(0.0, delta, n_fit)
     nu = 1e-4
     for _ in range(60):
-        u = composite_profile(yy, delta, utau, nu, u_inf=u_inf) / u_inf
+        u = composite_profile(yy, delta, utau, nu, kappa=kappa, C=C, u_inf=u_inf) / u_inf
         theta = np.trapezoid(u * (1.0 - u), yy)
         nu_new = theta * u_inf / retheta
         if abs(nu_new - nu) < 1e-14:
@@ -288,7 +294,7 @@ def _smooth_noise(shape, seed, sigma_pts):
 
 
 def turbulent_case(nx=814, ny=257, nz=193, lx=100.0, ly=4.0, lz=8.0, alpha=2.0, retheta=1100.0, cfl=0.5,
-                   rk_scheme=3, seed=1234, noise=0.10, coarse=4, lund=3, T_resc=10.0):
+                   rk_scheme=3, seed=1234, noise=0.10, coarse=4, lund=3, T_resc=10.0, kappa=0.41, C=7.8):
     """Turbulent boundary layer in inflow delta99 units: composite mean profile
     plus divergence-free noise (curl of a Gaussian-filtered random vector
     potential, `noise` U_inf rms) confined below y = 1.5 delta.  The noise is
@@ -297,14 +303,14 @@ def turbulent_case(nx=814, ny=257, nz=193, lx=100.0, ly=4.0, lz=8.0, alpha=2.0, 
     Inflow: Lund recycling (inflow_flag `lund`, 0 for the fixed profile) from
     the station i = nx/10 (about 10 inflow delta99 downstream at the default
     length), delta_inlet = 1, averaging time T_resc."""
-    nu, utau, theta = turbulent_inflow_profile(retheta)
+    nu, utau, theta = turbulent_inflow_profile(retheta, kappa=kappa, C=C)
     rex_theta = (retheta / 0.036) ** 1.25  # theta/x = 0.036 Re_x^-1/5
     x0 = rex_theta * nu
     x = uniform_faces(nx, lx, x0)
     y = tanh_faces(ny, ly, alpha)
     z = periodic_faces(nz, lz)
     xg, yg, zg = centres_ghost(x), centres_ghost(y), centres_ghost(z)
-    prof_c = composite_profile(yg, 1.0, utau, nu)  # U at y centres (nyg)
+    prof_c = composite_profile(yg, 1.0, utau, nu, kappa=kappa, C=C)  # U at y centres (nyg)
     U_in = prof_c.copy()
     V_in = np.zeros(ny)
     W_in = np.zeros(ny + 1)

@@ -17,6 +17,10 @@ import numpy as np
 from . import cases
 from ._lib import MIXED
 
+# mean profiles whose log layer follows the equilibrium model's law
+# u+ = ln(y+)/0.38 + 5.2, so the judge compares like with like
+LOG_LAW = dict(kappa=cases.KAPPA_WM, C=cases.reichardt_c(cases.KAPPA_WM, cases.B_WM))
+
 
 def closed_top(case):
     """The case with V_top = 0 (no transpiration through the top)."""
@@ -28,7 +32,7 @@ def closed_top(case):
 def dns_boxes(retheta=(700.0, 900.0, 1100.0, 1400.0, 1700.0, 2000.0, 2400.0), nx=64, ny=97, nz=16, seed=77):
     """Wall-resolved boxes (first cell centre below y+ = 1), 2 delta99 high."""
     return [closed_top(cases.turbulent_case(nx=nx, ny=ny, nz=nz, lx=nx * 0.125, ly=2.0, lz=nz * 0.0625,
-                                            alpha=2.5, retheta=rt, seed=seed + q, lund=0, noise=0.0))
+                                            alpha=2.5, retheta=rt, seed=seed + q, lund=0, noise=0.0, **LOG_LAW))
             for q, rt in enumerate(retheta)]
 
 
@@ -71,7 +75,7 @@ def wmles_case(retheta=1100.0, nx=128, ny=33, nz=32, seed=5):
     Re_theta 1100) sits in the log layer and the first cell centre is at
     y+ ~ 30, far from resolving the wall."""
     return closed_top(cases.turbulent_case(nx=nx, ny=ny, nz=nz, lx=nx * 0.125, ly=2.0, lz=nz * 0.0625, alpha=0.05,
-                                           retheta=retheta, seed=seed, lund=0, noise=0.05))
+                                           retheta=retheta, seed=seed, lund=0, noise=0.05, **LOG_LAW))
 
 
 def mean_cf(tau_x):

@@ -54,8 +54,11 @@ struct blgpu_ctx {
   void *F1[3] = {};
   void *P = nullptr, *nut = nullptr, *rhs_p = nullptr, *R = nullptr, *C = nullptr;
   double *piv = nullptr, *qx_part = nullptr;
-  // mixed form: FP64 kz = 0 pressure plane p0 [NM][N] and its scratch H, cosine matrix cm [N][N]
+  // mixed form: the low-kx kz = 0 part of the pressure in FP64: p0 [NM][N], its modes
+  // H0 [NM][klow], FP32 differences [2][NM][N], inverse-cosine matrix cm [klow][N]
   double *kz0 = nullptr, *kz0h = nullptr, *cmat = nullptr;
+  float *kz0g = nullptr;
+  int klow = 0;
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   void *tw = nullptr, *post = nullptr, *ztab = nullptr;
@@ -238,14 +241,18 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, &ctx->C, (size_t)s.NM * s.MH * s.rx * ctx->esz * 2));
   TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
   if (!ctx->fp64) {
+    // the modes kx < klow of kz = 0 carry the box-scale pressure of a step's
+    // flux change; above them the modes are small enough for FP32
+    ctx->klow = std::min(128, s.N);
     TRY(dalloc(ctx, (void **)&ctx->kz0, (size_t)s.NM * s.N * sizeof(double)));
-    TRY(dalloc(ctx, (void **)&ctx->kz0h, (size_t)s.NM * s.N * sizeof(double)));
-    TRY(dalloc(ctx, (void **)&ctx->cmat, (size_t)s.N * s.N * sizeof(double)));
+    TRY(dalloc(ctx, (void **)&ctx->kz0h, (size_t)s.NM * ctx->klow * sizeof(double)));
+    TRY(dalloc(ctx, (void **)&ctx->kz0g, 2 * (size_t)s.NM * s.N * sizeof(float)));
+    TRY(dalloc(ctx, (void **)&ctx->cmat, (size_t)ctx->klow * s.N * sizeof(double)));
     // inverse DCT-II of length N with the 1/(N M) of the inverse transforms
-    std::vector<double> ct(4 * (size_t)s.N), cm((size_t)s.N * s.N);
+    std::vector<double> ct(4 * (size_t)s.N), cm((size_t)ctx->klow * s.N);
     for (int q = 0; q < 4 * s.N; ++q) ct[q] = cos(M_PI * (double)q / (2.0 * (double)s.N));
     const double nrm = 1.0 / ((double)s.N * (double)s.M);
-    for (int kx = 0; kx < s.N; ++kx)
+    for (int kx = 0; kx < ctx->klow; ++kx)
       for (int i = 0; i < s.N; ++i)
         cm[(size_t)kx * s.N + i] = (kx ? 2.0 : 1.0) * nrm * ct[((long long)kx * (2 * i + 1)) % (4 * s.N)];
     TRY(check_cuda(ctx, cudaMemcpy(ctx->cmat, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice),
@@ -484,6 +491,12 @@ int blgpu_set_grid(blgpu_ctx *ctx, const double *x, const double *y, const doubl
   sp.insert(sp.end(), ctx->kxx.begin(), ctx->kxx.end());
   sp.insert(sp.end(), ctx->kzz.begin(), ctx->kzz.end());
   CK(cudaMemcpy(ctx->d_spec, sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  {  // inverse pivots of the y-solve, fixed by the grid
+    const double *d = ctx->d_spec;
+    launch_thomas_factors(s, ctx->piv, d, d + s.NM, d + 2 * s.NM, d + 3 * s.NM, d + 3 * s.NM + s.N, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+  }
   // views
   Geo &g = ctx->geo;
   g.nx = nx; g.ny = ny; g.nz = nz; g.nxg = ctx->nxg; g.nyg = ctx->nyg; g.nzg = ctx->nzg;
@@ -803,11 +816,10 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
-  if (mixed)  // the z-mean pressure in FP64 (see k_kz0_thomas), before the FP32 Thomas drops kz = 0
-    launch_kz0_plane<T>(s, (const T2 *)ctx->C, ctx->kz0h, ctx->kz0, ctx->piv, ctx->cmat, sp, sp + s.NM,
-                        sp + 2 * s.NM, sp + 3 * s.NM, ctx->kzz[0], ctx->st);
-  launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp, sp + s.NM, sp + 2 * s.NM, sp + 3 * s.NM, sp + 3 * s.NM + s.N,
-                   mixed ? 1 : 0, ctx->st);
+  launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
+                   ctx->st);
+  if (mixed)  // the box-scale pressure (kz = 0, kx < klow) in FP64
+    launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
   ph_end(ctx, mixed ? 3 : 1);
   ph_begin(ctx, PH_IDFTZ);
   launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
@@ -817,7 +829,8 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
-  launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, S[0], S[1], S[2],
+  launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, mixed ? ctx->kz0g : nullptr,
+                    S[0], S[1], S[2],
                     (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
   ph_end(ctx, rk_step == 1 ? 4 : 1);
 }

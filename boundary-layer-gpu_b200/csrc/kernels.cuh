@@ -59,7 +59,8 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
                    const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
                    const Scalars *sc, double c1, double c2, const Tiles &tl, cudaStream_t st);
 template <typename T>
-void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, T *U, T *V, T *W, T *P,
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, const float *p0g, T *U, T *V,
+                    T *W, T *P,
                     const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st);
 int bc_x_parts(const Geo &g);
 template <typename T>
@@ -109,16 +110,18 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
                   int rk, cudaStream_t st);
+// H0 (mixed form): the kz = 0 modes kx < klow are solved in FP64 into
+// H0[NM][klow] and zeroed in C; null for the FP64 form
 template <typename T>
-void launch_thomas(const Spec &s, typename vec2<T>::type *C, double *piv, const double *dd, const double *dl,
-                   const double *du, const double *kxx, const double *kzz, int skip_kz0, cudaStream_t st);
-// mixed form: the kz = 0 plane of the pressure solve in FP64, from the kz = 0
-// row of C (before the FP32 Thomas zeroes it) -> p0[NM][N]; H scratch
-// [NM][N]; cm[kx][i] = w_kx cos(pi kx (2i+1) / 2N) / (N M)
-template <typename T>
-void launch_kz0_plane(const Spec &s, const typename vec2<T>::type *C, double *H, double *p0, double *piv,
-                      const double *cm, const double *dd, const double *dl, const double *du, const double *kxx,
-                      double kz0, cudaStream_t st);
+void launch_thomas(const Spec &s, typename vec2<T>::type *C, const double *piv, const double *dl, const double *du,
+                   double *H0, int klow, cudaStream_t st);
+// p0[NM][N] = inverse cosine sum of H0 (cm[kx][i] = w_kx cos(pi kx (2i+1)/2N)/(N M))
+// and grad = FP32 x and y differences of p0 ([2][NM][N])
+void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm, double *p0, float *grad,
+                     cudaStream_t st);
+// inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
+void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
+                           const double *kxx, const double *kzz, cudaStream_t st);
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, cudaStream_t st);
 size_t dct_smem_bytes(int n, int elem_bytes, int lines);

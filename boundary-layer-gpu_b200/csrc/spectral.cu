@@ -511,16 +511,41 @@ __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restri
 // Tridiagonal solve in y for every (kx, kz) mode, FP64 arithmetic.
 // Row b (= j-2) of the operator: diag dd[b] + kxx[kx] + kzz[kz] (row 0 of
 // mode (0,0) scaled by 3/2, initialization.f90:454), sub dl[b] = Dyy(j,j-1),
-// super du[b] = Dyy(j,j+1).  Forward sweep writes g in place and the inverse
-// pivots to piv; the backward sweep reads them back.
+// super du[b] = Dyy(j,j+1).  The pivots of the elimination depend on the
+// grid only, so k_thomas_factors computes their inverses once (piv[b][kz][kx]
+// = 1/d'_b); the solve is then the two linear recurrences
+//   g_b = r_b - (dl_b piv_{b-1}) g_{b-1},  x_b = (g_b - du_b x_{b+1}) piv_b
+// with the arithmetic of the on-the-fly elimination, without a division on
+// the serial chain.
 // skip_kz0 (mixed form): the kz = 0 plane is solved in FP64 by the kz0
 // kernels below, so its coefficients here are zeroed.
 // ---------------------------------------------------------------------------
+__global__ void k_thomas_factors(Spec s, double *__restrict__ piv, const double *__restrict__ dd,
+                                 const double *__restrict__ dl, const double *__restrict__ du,
+                                 const double *__restrict__ kxx, const double *__restrict__ kzz) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kz = blockIdx.y;
+  if (kx >= s.N || kz >= s.MH) return;
+  const long long rs = (long long)s.MH * s.rx;
+  const long long base = (long long)kz * s.rx + kx;
+  const double kk = kxx[kx], kzv = kzz[kz];
+  double rinv = 0.0;
+  for (int b = 0; b < s.NM; ++b) {
+    double d = (dd[b] + kk) + kzv;
+    if (kx == 0 && kz == 0 && b == 0) d = 3.0 / 2.0 * d;
+    if (b > 0) {
+      const double w = dl[b] * rinv;
+      d = d - w * du[b - 1];
+    }
+    rinv = 1.0 / d;
+    piv[base + b * rs] = rinv;
+  }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, double *__restrict__ piv,
-                                                const double *__restrict__ dd, const double *__restrict__ dl,
-                                                const double *__restrict__ du, const double *__restrict__ kxx,
-                                                const double *__restrict__ kzz, int skip_kz0) {
+__global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, const double *__restrict__ piv,
+                                                const double *__restrict__ dl, const double *__restrict__ du,
+                                                double *__restrict__ H0, int klow) {
   // lane pairs share a mode: even lane = real part, odd lane = imaginary part
   const int lane = threadIdx.x & 31, part = lane & 1;
   const int kx = blockIdx.x * 16 + (lane >> 1);
@@ -529,46 +554,65 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
   const int NM = s.NM;
   const long long rs = (long long)s.MH * s.rx;  // stride between rows b
   const long long base = (long long)kz * s.rx + kx;
-  const double kk = kxx[kx];
-  const double kzv = kzz[kz];
-  const bool zero = (kx == 0 && kz == 0);
-  if (skip_kz0 && kz == 0) {
-    for (int b = 0; b < NM; ++b) reinterpret_cast<T *>(C)[2 * (base + b * rs) + part] = (T)0;
+  T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
+  if (H0 && kz == 0 && kx < klow) {
+    // mixed form: the low-kx modes of kz = 0 carry the box-scale pressure;
+    // solve them in FP64 into H0[b][kx] and drop them from the FP32 data
+    if (!part) {
+      double g = 0.0, rprev = 0.0;
+      for (int b = 0; b < NM; ++b) {
+        double r = (double)Cs[2 * (base + b * rs)];
+        if (b > 0) r = r - (dl[b] * rprev) * g;
+        rprev = piv[base + b * rs];
+        g = r;
+        H0[(long long)b * klow + kx] = r;
+      }
+      double x = 0.0;
+      for (int b = NM - 1; b >= 0; --b) {
+        const double r = H0[(long long)b * klow + kx];
+        x = (b == NM - 1) ? r * piv[base + b * rs] : (r - du[b] * x) * piv[base + b * rs];
+        H0[(long long)b * klow + kx] = x;
+      }
+    }
+    for (int b = 0; b < NM; ++b) Cs[2 * (base + b * rs)] = (T)0;
     return;
   }
-  T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
   // forward sweep in batches of PF rows, next batch in flight meanwhile
   constexpr int PF = 16;
-  double rinv = 0.0, g = 0.0;
+  double rprev = 0.0, g = 0.0;
   T cur[PF], nxt[PF];
+  double pc[PF], pnx[PF];
 #pragma unroll
-  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? Cs[2 * (base + u * rs)] : (T)0;
+  for (int u = 0; u < PF; ++u) {
+    cur[u] = u < NM ? Cs[2 * (base + u * rs)] : (T)0;
+    pc[u] = u < NM ? piv[base + u * rs] : 0.0;
+  }
   for (int b0 = 0; b0 < NM; b0 += PF) {
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int bn = b0 + PF + u;
       nxt[u] = bn < NM ? Cs[2 * (base + bn * rs)] : (T)0;
+      pnx[u] = bn < NM ? piv[base + bn * rs] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int b = b0 + u;
       if (b < NM) {
         double r = (double)cur[u];
-        double d = (dd[b] + kk) + kzv;
-        if (zero && b == 0) d = 3.0 / 2.0 * d;
         if (b > 0) {
-          const double w = dl[b] * rinv;  // l_b / d'_{b-1}
-          d = d - w * du[b - 1];
+          const double w = dl[b] * rprev;  // l_b / d'_{b-1}
           r = r - w * g;
         }
-        rinv = 1.0 / d;
+        rprev = pc[u];
         g = r;
         Cs[2 * (base + b * rs)] = (T)r;
-        if (!part) piv[base + b * rs] = rinv;
       }
     }
 #pragma unroll
-    for (int u = 0; u < PF; ++u) cur[u] = nxt[u];
+    for (int u = 0; u < PF; ++u) {
+      cur[u] = nxt[u];
+      pc[u] = pnx[u];
+    }
   }
   __syncwarp();
   // backward sweep, batches of PF rows from the top down
@@ -605,73 +649,22 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, d
 }
 
 // ---------------------------------------------------------------------------
-// Mixed form: the kz = 0 plane of the pressure solve in FP64.  A step whose
+// Mixed form: the box-scale part of the pressure in FP64.  A step whose
 // inflow flux differs from the interior's drives a pressure that varies
 // along the whole box; FP32 keeps only ~7 digits of it, and near the wall
 // (small y spacings) the rounding noise of p alone leaves a divergence of
-// order eps32 |p| / dy^2.  The z-mean part of p carries that large-scale
-// field, so it is solved and kept in FP64:
-//   forcing  G(kx,j) = Re C(j, kz=0, kx)   (the FP32 transforms of the
-//            divergence: small numbers, accurate to FP32 relative to |div|)
-//   k_kz0_thomas: tridiagonal solve in y per kx in FP64 -> H(kx,j)
-//   k_kz0_idct:   p0(i,j) = sum_kx H(kx,j) w_kx cos(pi kx (2i+1)/2N)/(N M)
-//                 (w_0 = 1, w_kx = 2), a dense product with a cosine table
-// The FP32 Thomas then zeroes its kz = 0 coefficients, and the projection
-// adds the FP64 p0 to the FP32 part.  H and p0: [NM][N] doubles.
+// order eps32 |p| / dy^2.  That field lives in the z-mean (kz = 0) modes of
+// low kx, so k_thomas solves the modes kz = 0, kx < klow in FP64 into H0
+// (their forcing, the FP32 transform of the divergence, is accurate to FP32
+// relative to |div|), and
+//   k_kz0_idct: p0(i,j) = sum_{kx<klow} H0(kx,j) w_kx cos(pi kx (2i+1)/2N)/(N M)
+//               (w_0 = 1, w_kx = 2), a dense product with a cosine table;
+//   k_kz0_grad: the x and y differences of p0 taken in FP64, stored as FP32
+// and the projection adds them to the differences of the FP32 part.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(64) k_kz0_thomas(Spec s, const T2<T> *__restrict__ C, double *__restrict__ H,
-                                                   double *__restrict__ piv, const double *__restrict__ dd,
-                                                   const double *__restrict__ dl, const double *__restrict__ du,
-                                                   const double *__restrict__ kxx, double kz0) {
-  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kx >= s.N) return;
-  const int N = s.N, NM = s.NM;
-  const long long rs = (long long)s.MH * s.rx;  // row stride of C (kz = 0 row of each b)
-  const double kk = kxx[kx];
-  constexpr int PF = 16;
-  double cur[PF], nxt[PF];
-#pragma unroll
-  for (int u = 0; u < PF; ++u) cur[u] = u < NM ? (double)C[u * rs + kx].x : 0.0;
-  double rinv = 0.0, gr = 0.0;
-  for (int b0 = 0; b0 < NM; b0 += PF) {
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int bn = b0 + PF + u;
-      nxt[u] = bn < NM ? (double)C[bn * rs + kx].x : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int b = b0 + u;
-      if (b < NM) {
-        double r = cur[u];
-        double d = (dd[b] + kk) + kz0;
-        if (kx == 0 && b == 0) d = 3.0 / 2.0 * d;  // initialization.f90:454
-        if (b > 0) {
-          const double w = dl[b] * rinv;
-          d = d - w * du[b - 1];
-          r = r - w * gr;
-        }
-        rinv = 1.0 / d;
-        gr = r;
-        H[(long long)b * N + kx] = r;
-        piv[(long long)b * N + kx] = rinv;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < PF; ++u) cur[u] = nxt[u];
-  }
-  double x = 0.0;
-  for (int b = NM - 1; b >= 0; --b) {
-    const double r = H[(long long)b * N + kx], pv = piv[(long long)b * N + kx];
-    x = (b == NM - 1) ? r * pv : (r - du[b] * x) * pv;
-    H[(long long)b * N + kx] = x;
-  }
-}
-
-// p0[b][i] = sum_kx H[b][kx] cm[kx][i]: 32 x 64 output tiles, k-tiles of 32
-__global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restrict__ H, const double *__restrict__ cm,
-                                                  double *__restrict__ p0) {
+// p0[b][i] = sum_{kx < K} H[b][kx] cm[kx][i]: 32 x 64 output tiles, k-tiles of 32
+__global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restrict__ H, int K,
+                                                  const double *__restrict__ cm, double *__restrict__ p0) {
   constexpr int BM = 32, BN = 64, BK = 32;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN];
@@ -679,14 +672,14 @@ __global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restri
   const int b0 = blockIdx.y * BM, i0 = blockIdx.x * BN;
   const int t = threadIdx.x, tr = t >> 4, tc = t & 15;
   double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-  for (int k0 = 0; k0 < N; k0 += BK) {
+  for (int k0 = 0; k0 < K; k0 += BK) {
     for (int q = t; q < BM * BK; q += 256) {
       const int r = q / BK, c = q % BK;
-      As[c][r] = (b0 + r < NM && k0 + c < N) ? H[(long long)(b0 + r) * N + k0 + c] : 0.0;
+      As[c][r] = (b0 + r < NM && k0 + c < K) ? H[(long long)(b0 + r) * K + k0 + c] : 0.0;
     }
     for (int q = t; q < BK * BN; q += 256) {
       const int r = q / BN, c = q % BN;
-      Bs[r][c] = (k0 + r < N && i0 + c < N) ? cm[(long long)(k0 + r) * N + i0 + c] : 0.0;
+      Bs[r][c] = (k0 + r < K && i0 + c < N) ? cm[(long long)(k0 + r) * N + i0 + c] : 0.0;
     }
     __syncthreads();
 #pragma unroll 8
@@ -708,6 +701,18 @@ __global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restri
       const int b = b0 + 2 * tr + r, i = i0 + tc + 16 * q;
       if (b < NM && i < N) p0[(long long)b * N + i] = acc[r][q];
     }
+}
+
+// FP32 copies of the p0 differences the projection uses (taken in FP64):
+// gx[b][i] = p0[b][min(i+1,N-1)] - p0[b][i], gy[b][i] = p0[b+1][i] - p0[b][i]
+__global__ void k_kz0_grad(Spec s, const double *__restrict__ p0, float *__restrict__ gx, float *__restrict__ gy) {
+  const int N = s.N, NM = s.NM;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N * NM) return;
+  const int b = q / N, i = q % N;
+  const double v = p0[q];
+  gx[q] = (float)(p0[(long long)b * N + min(i + 1, N - 1)] - v);
+  gy[q] = b < NM - 1 ? (float)(p0[q + N] - v) : 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -816,18 +821,21 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 }
 
 template <typename T>
-void launch_thomas(const Spec &s, T2<T> *C, double *piv, const double *dd, const double *dl, const double *du,
-                   const double *kxx, const double *kzz, int skip_kz0, cudaStream_t st) {
+void launch_thomas(const Spec &s, T2<T> *C, const double *piv, const double *dl, const double *du, double *H0,
+                   int klow, cudaStream_t st) {
   dim3 grid((s.N + 15) / 16, (s.MH + 7) / 8);
-  k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dd, dl, du, kxx, kzz, skip_kz0);
+  k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dl, du, H0, klow);
 }
 
-template <typename T>
-void launch_kz0_plane(const Spec &s, const T2<T> *C, double *H, double *p0, double *piv, const double *cm,
-                      const double *dd, const double *dl, const double *du, const double *kxx, double kz0,
-                      cudaStream_t st) {
-  k_kz0_thomas<T><<<(s.N + 63) / 64, 64, 0, st>>>(s, C, H, piv, dd, dl, du, kxx, kz0);
-  k_kz0_idct<<<dim3((s.N + 63) / 64, (s.NM + 31) / 32), 256, 0, st>>>(s, H, cm, p0);
+void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
+                           const double *kxx, const double *kzz, cudaStream_t st) {
+  k_thomas_factors<<<dim3((s.N + 127) / 128, s.MH), 128, 0, st>>>(s, piv, dd, dl, du, kxx, kzz);
+}
+
+void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm, double *p0, float *grad,
+                     cudaStream_t st) {
+  k_kz0_idct<<<dim3((s.N + 63) / 64, (s.NM + 31) / 32), 256, 0, st>>>(s, H0, klow, cm, p0);
+  k_kz0_grad<<<(s.N * s.NM + 255) / 256, 256, 0, st>>>(s, p0, grad, grad + (long long)s.N * s.NM);
 }
 
 #define BLGPU_SPEC_INST(T)                                                                                        \
@@ -835,11 +843,8 @@ void launch_kz0_plane(const Spec &s, const T2<T> *C, double *H, double *p0, doub
                                   T *, int, cudaStream_t);                                                        \
   template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, cudaStream_t); \
   template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
-  template void launch_thomas<T>(const Spec &, T2<T> *, double *, const double *, const double *,                \
-                                 const double *, const double *, const double *, int, cudaStream_t);            \
-  template void launch_kz0_plane<T>(const Spec &, const T2<T> *, double *, double *, double *, const double *,   \
-                                    const double *, const double *, const double *, const double *, double,       \
-                                    cudaStream_t);
+  template void launch_thomas<T>(const Spec &, T2<T> *, const double *, const double *, const double *,          \
+                                 double *, int, cudaStream_t);
 BLGPU_SPEC_INST(double)
 BLGPU_SPEC_INST(float)
 

@@ -329,7 +329,8 @@ template <> struct V16<double> { typedef double2 t; };
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__restrict__ p,
-                                                   const double *__restrict__ p0, T *__restrict__ U,
+                                                   const double *__restrict__ p0, const float *__restrict__ p0g,
+                                                   T *__restrict__ U,
                                                    T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
                                                    const Scalars *__restrict__ sc, int save_p) {
   typedef typename V16<T>::t VT;
@@ -355,23 +356,21 @@ __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__
   const T yC = m.yC[j], yrC = m.yrC[j], zC = m.zC[k], zrC = m.zrC[k];
   const int N = g.nx - 2;
   const double *p0r = p0 ? p0 + (long long)(j - 2) * N : nullptr;  // row j of the FP64 part
-  const double *p0n = (p0 && vj) ? p0r + N : nullptr;               // row j+1
+  const float *gxr = p0g ? p0g + (long long)(j - 2) * N : nullptr;  // its x and y differences
+  const float *gyr = p0g ? gxr + (long long)N * (g.ny - 1) : nullptr;
 #pragma unroll
   for (int e = 0; e < VN; ++e) {
     const int i = i0 + e;
     const T pe1 = (e + 1 < VN) ? pc.e[e + 1] : pe;
     if (i <= g.nx - 1) {
       T dd = pe1 - pc.e[e];
-      if (p0) dd = (T)((double)dd + (p0r[min(i - 1, N - 1)] - p0r[i - 2]));
+      if (p0g) dd = dd + (T)gxr[i - 2];
       u.e[e] = u.e[e] - qdiv(dd, m.xC[i], m.xrC[i]);
     }
     if (i <= g.nx) {
       if (vj) {
         T dd = pn.e[e] - pc.e[e];
-        if (p0) {
-          const int ic = min(i - 2, N - 1);
-          dd = (T)((double)dd + (p0n[ic] - p0r[ic]));
-        }
+        if (p0g) dd = dd + (T)gyr[min(i - 2, N - 1)];
         v.e[e] = v.e[e] - qdiv(dd, yC, yrC);
       }
       if (wk) w.e[e] = w.e[e] - qdiv(pt.e[e] - pc.e[e], zC, zrC);
@@ -608,11 +607,20 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
     const int k0 = blockIdx.z * kchunk + 2;
     const int k1 = min(k0 + kchunk - 1, g.nzg - 1);
     const double cu = g.ax.C[i], cv = g.ay.C[j];
+    // a thread keeps i and j, so max_k C/|u_k| = C / min_k |u_k| (division
+    // is monotone: the same double as the per-point maximum)
+    double au = INFINITY, av = INFINITY, aw = INFINITY;
     for (int k = k0; k <= k1; ++k) {
       long long c = bidx(g, i, j, k);
-      mu = fmax(mu, cu / fabs((double)__ldg(U + c)));
-      mv = fmax(mv, cv / fabs((double)__ldg(V + c)));
-      mw = fmax(mw, g.az.C[k] / fabs((double)__ldg(W + c)));
+      au = fmin(au, fabs((double)__ldg(U + c)));
+      av = fmin(av, fabs((double)__ldg(V + c)));
+      if (sizeof(T) == 8) mw = fmax(mw, g.az.C[k] / fabs((double)__ldg(W + c)));
+      else aw = fmin(aw, fabs((double)__ldg(W + c)) * g.az.rC[k]);  // mixed form: 1/max(C/|w|)
+    }
+    if (k1 >= k0) {
+      mu = cu / au;
+      mv = cv / av;
+      if (sizeof(T) != 8) mw = 1.0 / aw;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -860,13 +868,14 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
 }
 
 template <typename T>
-void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, T *U, T *V, T *W, T *P,
+void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0, const float *p0g, T *U, T *V,
+                    T *W, T *P,
                     const Scalars *sc, int save_p, const Tiles &tl, cudaStream_t st) {
   constexpr int VN = 16 / sizeof(T);
   const int ngrp = (g.nx - 1 + VN - 1) / VN;  // i = 2..nx in groups of VN
   const int by = tl.proj_by > 0 ? tl.proj_by : 8;
   dim3 block(32, by), grid((ngrp + 31) / 32, (g.ny - 1 + by - 1) / by, g.nz - 1);
-  k_project_v<T><<<grid, block, 0, st>>>(g, m, p, p0, U, V, W, P, sc, save_p);
+  k_project_v<T><<<grid, block, 0, st>>>(g, m, p, p0, p0g, U, V, W, P, sc, save_p);
   if (save_p) {
     dim3 b2(32, 8);
     k_p_ghost<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 0);
@@ -934,7 +943,8 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int 
   template void launch_rhs_rk<T>(const Geo &, const MetT<T> &, int, bool, const T *, const T *, const T *,          \
                                  const T *, const T *, const T *, const T *, T *, T *, T *, T *, T *, T *,          \
                                  const Scalars *, double, double, const Tiles &, cudaStream_t);                     \
-  template void launch_project<T>(const Geo &, const MetT<T> &, const T *, const double *, T *, T *, T *, T *,     \
+  template void launch_project<T>(const Geo &, const MetT<T> &, const T *, const double *, const float *, T *,    \
+                                  T *, T *, T *,                                                                    \
                                   const Scalars *, int, const Tiles &, cudaStream_t);                               \
   template void launch_bc<T>(const Geo &, const BcData &, T *, T *, T *, const T *, const T *, const T *,         \
                              Scalars *, double, double *, double, double, cudaStream_t);                            \

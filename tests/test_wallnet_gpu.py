@@ -108,7 +108,10 @@ def test_wall_model_step_matches_oracle(gpu, mode):
     assert rel(U, Ur) < tol and rel(V, Vr) < tol and rel(W, Wr) < tol, (rel(U, Ur), rel(V, Vr), rel(W, Wr))
     tx, _ = s.wall_stress()
     txo, _ = o.wall_stress()
-    assert np.abs(tx - txo).max() <= (1e-10 if mode == 1 else 1e-4) * np.abs(txo).max()
+    if mode == 1:
+        assert np.abs(tx - txo).max() <= 1e-10 * np.abs(txo).max()
+    else:  # FP32 sums in a different order may flip a BF16 rounding of an activation
+        assert np.abs(tx - txo).max() <= 5e-3 * np.abs(txo).max() and rel(tx, txo) < 2e-4
 
 
 def test_wall_model_errors(gpu):
