@@ -555,28 +555,15 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, c
   const long long rs = (long long)s.MH * s.rx;  // stride between rows b
   const long long base = (long long)kz * s.rx + kx;
   T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
-  if (H0 && kz == 0 && kx < klow) {
-    // mixed form: the low-kx modes of kz = 0 carry the box-scale pressure;
-    // solve them in FP64 into H0[b][kx] and drop them from the FP32 data
-    if (!part) {
-      double g = 0.0, rprev = 0.0;
-      for (int b = 0; b < NM; ++b) {
-        double r = (double)Cs[2 * (base + b * rs)];
-        if (b > 0) r = r - (dl[b] * rprev) * g;
-        rprev = piv[base + b * rs];
-        g = r;
-        H0[(long long)b * klow + kx] = r;
-      }
-      double x = 0.0;
-      for (int b = NM - 1; b >= 0; --b) {
-        const double r = H0[(long long)b * klow + kx];
-        x = (b == NM - 1) ? r * piv[base + b * rs] : (r - du[b] * x) * piv[base + b * rs];
-        H0[(long long)b * klow + kx] = x;
-      }
-    }
+  // mixed form: the low-kx modes of kz = 0 carry the box-scale pressure;
+  // they are solved with FP64 intermediates into H0[b][kx] (real part; the
+  // imaginary part of kz = 0 is zero) and dropped from the FP32 data
+  const bool hp = H0 && kz == 0 && kx < klow;
+  if (hp && part) {
     for (int b = 0; b < NM; ++b) Cs[2 * (base + b * rs)] = (T)0;
     return;
   }
+  double *Hd = hp ? H0 + kx : nullptr;  // H0[b * klow + kx]
   // forward sweep in batches of PF rows, next batch in flight meanwhile
   constexpr int PF = 16;
   double rprev = 0.0, g = 0.0;
@@ -605,7 +592,8 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, c
         }
         rprev = pc[u];
         g = r;
-        Cs[2 * (base + b * rs)] = (T)r;
+        if (hp) Hd[(long long)b * klow] = r;
+        else Cs[2 * (base + b * rs)] = (T)r;
       }
     }
 #pragma unroll
@@ -614,7 +602,29 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, c
       pc[u] = pnx[u];
     }
   }
-  __syncwarp();
+  if (hp) {  // FP64 backward sweep of the kz = 0, low-kx modes
+    double x = 0.0;
+    constexpr int PB = 8;
+    for (int b0 = NM - 1; b0 >= 0; b0 -= PB) {
+      double hv[PB], pvv[PB];
+#pragma unroll
+      for (int u = 0; u < PB; ++u) {
+        const int b = b0 - u;
+        hv[u] = b >= 0 ? Hd[(long long)b * klow] : 0.0;
+        pvv[u] = b >= 0 ? piv[base + b * rs] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < PB; ++u) {
+        const int b = b0 - u;
+        if (b >= 0) {
+          x = (b == NM - 1) ? hv[u] * pvv[u] : (hv[u] - du[b] * x) * pvv[u];
+          Hd[(long long)b * klow] = x;
+        }
+      }
+    }
+    for (int b = 0; b < NM; ++b) Cs[2 * (base + b * rs)] = (T)0;
+    return;
+  }
   // backward sweep, batches of PF rows from the top down
   double x = 0.0;
   double pv[PF], pn[PF];

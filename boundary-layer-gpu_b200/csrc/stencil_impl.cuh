@@ -628,7 +628,22 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
     mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
     mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
   }
+  // one atomic per block and field (the maxima are order-free, so the
+  // result is deterministic); per-warp atomics on three words serialise
+  __shared__ double red[3][8];
+  const int wid = (threadIdx.y * blockDim.x + threadIdx.x) >> 5, nwarp = (blockDim.x * blockDim.y) >> 5;
   if ((threadIdx.x & 31) == 0) {
+    red[0][wid] = mu;
+    red[1][wid] = mv;
+    red[2][wid] = mw;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int w = 1; w < nwarp; ++w) {
+      mu = fmax(mu, red[0][w]);
+      mv = fmax(mv, red[1][w]);
+      mw = fmax(mw, red[2][w]);
+    }
     atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
     atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
     atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
@@ -902,7 +917,7 @@ void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, co
 template <typename T>
 void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
                cudaStream_t st) {
-  const int kchunk = 16;
+  const int kchunk = 32;
   dim3 grid = vol_grid(g.nxg - 2, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
   k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk);
   k_dt_finish<<<1, 1, 0, st>>>(sc, cfl, dtvis);
