@@ -26,6 +26,7 @@ SOURCES = {
     "noalloc.cu": [],
     "mlp.cu": [],
     "capi_mlp.cu": [],
+    "zdft_tc.cu": [],
 }
 
 

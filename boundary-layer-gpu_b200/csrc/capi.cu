@@ -59,6 +59,8 @@ struct blgpu_ctx {
   double *kz0 = nullptr, *kz0h = nullptr, *cmat = nullptr;
   float *kz0g = nullptr;
   int klow = 0;
+  uint32_t *zfrag = nullptr;  // mixed form: table fragments of the tensor-core z transforms (or null)
+  int nsm = 148;
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   void *tw = nullptr, *post = nullptr, *ztab = nullptr;
@@ -240,6 +242,14 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, &ctx->R, (size_t)s.NM * s.M * s.rx * ctx->esz));
   TRY(dalloc(ctx, &ctx->C, (size_t)s.NM * s.MH * s.rx * ctx->esz * 2));
   TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
+  if (!ctx->fp64 && zdft_tc_qp(s)) {
+    std::vector<uint32_t> fr;
+    zdft_tc_fragments(s, fr);
+    TRY(dalloc(ctx, (void **)&ctx->zfrag, fr.size() * sizeof(uint32_t)));
+    TRY(check_cuda(ctx, cudaMemcpy(ctx->zfrag, fr.data(), fr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                   "z-transform tables"));
+  }
   if (!ctx->fp64) {
     // the modes kx < klow of kz = 0 carry the box-scale pressure of a step's
     // flux change; above them the modes are small enough for FP32
@@ -811,8 +821,10 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_begin(ctx, PH_DIVDCT);
   launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->st);
   ph_end(ctx, 1);
+  const bool tc = mixed && ctx->zfrag && ctx->tiles.zdft == 0;
   ph_begin(ctx, PH_DFTZ);
-  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
+  if (tc) launch_zdft_tc(s, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, ctx->st);
+  else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
@@ -822,7 +834,8 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
     launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
   ph_end(ctx, mixed ? 3 : 1);
   ph_begin(ctx, PH_IDFTZ);
-  launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
+  if (tc) launch_zdft_tc(s, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, ctx->st);
+  else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
   launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.dct_nw, ctx->st);
@@ -1372,6 +1385,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   if (t.dftz_rk != 0 && t.dftz_rk != 4 && t.dftz_rk != 8)
     return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
   if (t.dct_nw < 0 || t.dct_nw > 8) return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d outside 0..8", t.dct_nw);
+  if (t.zdft != 0 && t.zdft != 1) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1}", t.zdft);
   if (t.dct_nw > 0) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
@@ -1441,8 +1455,8 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 values");
-  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4]};
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 or 6 values");
+  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1460,6 +1474,7 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   tiles[2] = t.dct_nw;
   tiles[3] = t.dftz_rk;
   tiles[4] = t.proj_by;
+  if (n >= 6) tiles[5] = t.zdft;
   return BLGPU_OK;
 }
 
@@ -1477,7 +1492,8 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {4, 8},                                                                  // rhs_by
       {0, 1, 2, 3, 4, 6},                                                      // dct_nw
       {4, 8},                                                                  // dftz_rk
-      {4, 8}};                                                                 // proj_by
+      {4, 8},                                                                  // proj_by
+      {0, 1}};                                                                 // zdft
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1494,10 +1510,11 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 5 && !rc; ++knob) {  // one pass of coordinate descent
+  for (int knob = 0; knob < 6 && !rc; ++knob) {  // one pass of coordinate descent
+    if (knob == 5 && !ctx->zfrag) break;           // no tensor-core z transform for this box
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[5] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by};
+      int *f[6] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

@@ -1,5 +1,7 @@
 // kernels.cuh -- launcher declarations shared by the kernel and host files.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace blgpu {
@@ -21,6 +23,7 @@ struct Tiles {
   int dct_nw;   // complex lines (warps) per CTA of the DCT kernels (0: sized from shared memory)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
+  int zdft;     // mixed form z transforms: 0 tensor cores where the order is served, 1 FP32 direct sums
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)
@@ -119,6 +122,14 @@ void launch_thomas(const Spec &s, typename vec2<T>::type *C, const double *piv, 
 // and grad = FP32 x and y differences of p0 ([2][NM][N])
 void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm, double *p0, float *grad,
                      cudaStream_t st);
+// ---- zdft_tc.cu: mixed-form z transforms on the tensor cores ----
+// order of the square products (M/2+1 rounded up to 16) when served, else 0
+int zdft_tc_qp(const Spec &s);
+size_t zdft_tc_frag_words(const Spec &s);
+void zdft_tc_fragments(const Spec &s, std::vector<uint32_t> &out);
+// inverse = 0: R -> C (forward); 1: C -> R; nsm: persistent CTAs
+void launch_zdft_tc(const Spec &s, float *R, float2 *C, const uint32_t *frag, int inverse, int nsm,
+                    cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);
