@@ -1386,6 +1386,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
     return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
   if (t.dct_nw < 0 || t.dct_nw > 8) return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d outside 0..8", t.dct_nw);
   if (t.zdft != 0 && t.zdft != 1) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1}", t.zdft);
+  if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
   if (t.dct_nw > 0) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
@@ -1455,8 +1456,9 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 or 6 values");
-  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft};
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 7 values");
+  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft,
+          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1475,6 +1477,7 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   tiles[3] = t.dftz_rk;
   tiles[4] = t.proj_by;
   if (n >= 6) tiles[5] = t.zdft;
+  if (n >= 7) tiles[6] = t.rhs_pts;
   return BLGPU_OK;
 }
 
@@ -1493,7 +1496,8 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {0, 1, 2, 3, 4, 6},                                                      // dct_nw
       {4, 8},                                                                  // dftz_rk
       {4, 8},                                                                  // proj_by
-      {0, 1}};                                                                 // zdft
+      {0, 1},                                                                  // zdft
+      {1, 2}};                                                                 // rhs_pts
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1510,11 +1514,12 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 6 && !rc; ++knob) {  // one pass of coordinate descent
-    if (knob == 5 && !ctx->zfrag) break;           // no tensor-core z transform for this box
+  for (int knob = 0; knob < 7 && !rc; ++knob) {  // one pass of coordinate descent
+    if (knob == 5 && !ctx->zfrag) continue;        // no tensor-core z transform for this box
+    if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[6] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft};
+      int *f[7] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

@@ -18,12 +18,13 @@ template <typename T> struct MetT {
 // Launch shapes of the main kernels.  0 selects the built-in choice; the
 // autotuner (blgpu_autotune) searches these per box.
 struct Tiles {
-  int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8, FP32 register window 32)
+  int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8; FP32 DNS 8 for two points, 32 for one)
   int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
   int dct_nw;   // complex lines (warps) per CTA of the DCT kernels (0: sized from shared memory)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed form z transforms: 0 tensor cores where the order is served, 1 FP32 direct sums
+  int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)

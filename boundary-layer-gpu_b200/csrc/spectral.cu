@@ -137,24 +137,31 @@ __device__ __forceinline__ void bf_odd(const T2<T> *in, T2<T> *out, int jj, int 
   }
 }
 
-// any radix, outputs by direct summation from shared memory (large primes)
+// any radix: output k of butterfly jj by direct summation from shared
+// memory (large primes).  e = tstep + k n/R < n, so one subtraction keeps
+// the table index q*e mod n in range.
 template <typename T, bool INV>
-__device__ __forceinline__ void bf_loop(const T2<T> *in, T2<T> *out, int R, int jj, int nb, int tstep, int idxD,
-                                        int Ns, int n, const T2<T> *tw) {
-  const int stride = n / R;
-  for (int k = 0; k < R; ++k) {
-    const int e = tstep + k * stride;
-    T ax = 0, ay = 0;
-    int idx = 0;
-    for (int q = 0; q < R; ++q) {
-      T2<T> v = twm<T, INV>(in[jj + q * nb], tw[idx]);
-      ax += v.x;
-      ay += v.y;
-      idx += e;
-      if (idx >= n) idx -= n;
-    }
-    out[idxD + k * Ns] = mk<T>(ax, ay);
+__device__ __forceinline__ void bf_loop_out(const T2<T> *in, T2<T> *out, int R, int k, int jj, int nb, int tstep,
+                                            int idxD, int Ns, int n, const T2<T> *tw) {
+  const int e = tstep + k * (n / R);
+  T ax = 0, ay = 0;
+  int idx = 0;
+  for (int q = 0; q < R; ++q) {
+    T2<T> v = twm<T, INV>(in[jj + q * nb], tw[idx]);
+    ax += v.x;
+    ay += v.y;
+    idx += e;
+    if (idx >= n) idx -= n;
   }
+  out[idxD + k * Ns] = mk<T>(ax, ay);
+}
+
+// radices with a dedicated butterfly in the kernel instantiated for MAXR
+template <int MAXR>
+__device__ __forceinline__ bool reg_radix(int R) {
+  if (R == 2 || R == 3 || R == 4) return true;
+  if (R > MAXR) return false;
+  return R == 5 || R == 7 || R == 11 || R == 13 || R == 17 || R == 19 || R == 23 || R == 29 || R == 31;
 }
 
 // warp-level Stockham FFT of one complex line in shared memory (no block
@@ -167,6 +174,21 @@ __device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> 
     const int R = pl.rad[s];
     const int nb = n / R;
     const int tsc = n / (Ns * R);
+    if (!reg_radix<MAXR>(R)) {
+      // a large prime has few butterflies (nb = n/R), so the lanes take
+      // (butterfly, output) pairs: n items of R terms each
+      for (int t = lane; t < n; t += 32) {
+        const int k = t / nb, jj = t - k * nb;
+        const int jm = jj % Ns;
+        bf_loop_out<T, INV>(a, b, R, k, jj, nb, jm * tsc, (jj - jm) * R + jm, Ns, n, tw);
+      }
+      __syncwarp();
+      T2<T> *t = a;
+      a = b;
+      b = t;
+      Ns *= R;
+      continue;
+    }
     for (int jj = lane; jj < nb; jj += 32) {
       const int jm = jj % Ns;
       const int tstep = jm * tsc;
@@ -183,7 +205,6 @@ __device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> 
       else if (MAXR >= 23 && R == 23) bf_odd<23, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
       else if (MAXR >= 29 && R == 29) bf_odd<29, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
       else if (MAXR >= 31 && R == 31) bf_odd<31, T, INV>(a, b, jj, nb, tstep, idxD, Ns, n, tw);
-      else bf_loop<T, INV>(a, b, R, jj, nb, tstep, idxD, Ns, n, tw);
     }
     __syncwarp();
     T2<T> *t = a;

@@ -313,6 +313,249 @@ __global__ void __launch_bounds__(256) k_rhs_rk_dns(Geo g, MetT<T> m, const T *_
 }
 
 // ---------------------------------------------------------------------------
+// DNS form with two x-points per thread (i0 = 2+2q and i0+1, one aligned
+// 2-vector in the box).  The face fluxes are evaluated once and shared:
+//   X(i)   = h*(U(i)+U(i+1))                    u x-advection (a and b terms)
+//   Fxy(i) = (w0*U(i,j)+w1*U(i,j+1))*h*(V(i)+V(i+1))   u's t1, v's t1; v's t2 = Fxy(i-1)
+//   Fxz(i) = h*(U(k)+U(k+1))*h*(W(i)+W(i+1))   u's t3, w's t1; w's t2 = Fxz(i-1)
+//   Fyz    = h*(V(k)+V(k+1))*(w0*W(j)+w1*W(j+1))      v's t3, w's t3
+// and the k-1 face values (u's t4, v's t4, w's advection b term and the three
+// lower z differences) are carried from the previous plane, where they were
+// the upper face values.  Every shared or carried value is the same
+// expression, in the same order, as the term it replaces in rhs_*_at.  The
+// rows of plane k+2 and the Uo/F1 values of plane k+1 are fetched one plane
+// ahead so their DRAM latency overlaps a plane of arithmetic.
+// ---------------------------------------------------------------------------
+// w0*a + w1*b with both products rounded (no contraction), so that a carried
+// Fyz and one formed afresh at the first plane of a chunk round alike and the
+// chunk length does not change results
+__device__ __forceinline__ float wsum(float w0, float a, float w1, float b) {
+  return __fadd_rn(__fmul_rn(w0, a), __fmul_rn(w1, b));
+}
+__device__ __forceinline__ double wsum(double w0, double a, double w1, double b) {
+  return __dadd_rn(__dmul_rn(w0, a), __dmul_rn(w1, b));
+}
+
+template <typename T> struct Row4 { T m, a, b, p; };  // i0-1 .. i0+2
+template <typename T> struct Row3 { T m, a, b; };     // i0-1 .. i0+1
+template <typename T> struct Row2 { T a, b; };        // i0 .. i0+1
+
+template <typename T>
+__device__ __forceinline__ Row2<T> ld2(const T *__restrict__ p, long long c) {
+  typedef typename vec2<T>::type T2;
+  const T2 v = __ldg(reinterpret_cast<const T2 *>(p + c));
+  return Row2<T>{v.x, v.y};
+}
+template <typename T>
+__device__ __forceinline__ Row3<T> ld3(const T *__restrict__ p, long long c) {
+  const Row2<T> v = ld2(p, c);
+  return Row3<T>{__ldg(p + c - 1), v.a, v.b};
+}
+// stores the points of the pair that lie in the update range (sa implies
+// nothing about sb, but sb implies sa since b = a+1 and ranges are prefixes)
+template <typename T>
+__device__ __forceinline__ void st2(T *__restrict__ p, long long c, T fa, T fb, bool sa, bool sb) {
+  typedef typename vec2<T>::type T2;
+  if (sb) {
+    T2 v;
+    v.x = fa;
+    v.y = fb;
+    *reinterpret_cast<T2 *>(p + c) = v;
+  } else if (sa) {
+    p[c] = fa;
+  }
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ void rk_store2(T *__restrict__ F1, T *__restrict__ Un, long long c, Row2<T> f,
+                                          Row2<T> o, Row2<T> f1, T cdt1, T tdt, T tc1, T tc2, bool sa, bool sb) {
+  if (MODE == 0) {
+    st2(F1, c, f.a, f.b, sa, sb);
+  } else if (MODE == 1) {
+    st2(F1, c, f.a, f.b, sa, sb);
+    st2(Un, c, o.a + cdt1 * f.a, o.b + cdt1 * f.b, sa, sb);
+  } else {
+    st2(Un, c, o.a + tdt * (tc1 * f1.a + tc2 * f.a), o.b + tdt * (tc1 * f1.b + tc2 * f.b), sa, sb);
+  }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_rhs_rk_pair(Geo g, MetT<T> m, const T *__restrict__ U,
+                                                     const T *__restrict__ V, const T *__restrict__ W,
+                                                     const T *__restrict__ Uo, const T *__restrict__ Vo,
+                                                     const T *__restrict__ Wo, T *__restrict__ F1u,
+                                                     T *__restrict__ F1v, T *__restrict__ F1w, T *__restrict__ Un,
+                                                     T *__restrict__ Vn, T *__restrict__ Wn,
+                                                     const Scalars *__restrict__ sc, double c1, double c2,
+                                                     int kchunk) {
+  const int i0 = 2 + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (i0 > g.nx || j > g.ny) return;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  if (k0 > k1) return;
+  const long long px = g.px, pl = g.plane;
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  const T cdt1 = (T)(dt * c1);
+  const T tdt = (T)dt, tc1 = (T)c1, tc2 = (T)c2;
+  const int ib = i0 + 1;
+  // store ranges: u at i <= nx-1 (zero at nx-1), v and w at i <= nx (zero at nx)
+  const bool su_a = i0 <= g.nx - 1, su_b = ib <= g.nx - 1;
+  const bool sv_a = true, sv_b = ib <= g.nx;
+  const bool dv = (j <= g.ny - 1);
+  const bool zu_a = (i0 == g.nx - 1), zu_b = (ib == g.nx - 1);
+  const bool zx_a = (i0 == g.nx), zx_b = (ib == g.nx);
+  const T h = (T)0.5;
+  // x metrics of both points (tables run to nx+2, so i0+2 is in range)
+  const T xC_a = m.xC[i0], xrC_a = m.xrC[i0], xC_b = m.xC[ib], xrC_b = m.xrC[ib];
+  const T xF_a = m.xF[i0], xrF_a = m.xrF[i0], xF_b = m.xF[ib], xrF_b = m.xrF[ib];
+  const T xrF_p = m.xrF[i0 + 2], xrC_m = m.xrC[i0 - 1];
+  const T yF = m.yF[j], yrF = m.yrF[j], yC = m.yC[j], yrC = m.yrC[j], yCm = m.yC[j - 1], yrCm = m.yrC[j - 1];
+  const T yrFp = m.yrF[j + 1], w0 = m.w0[j], w1 = m.w1[j], w0m = m.w0[j - 1], w1m = m.w1[j - 1];
+  const T nu = m.nu, dpdx = m.dpdx, dpdz = m.dpdz;
+  long long c = bidx(g, i0, j, k0);
+  // window at k0: rows of planes k0 (c), k0+1 (t), and the k0-1 values the
+  // carried terms start from
+  Row4<T> uc, vc, wc;
+  {
+    const Row3<T> u3 = ld3(U, c), v3 = ld3(V, c), w3 = ld3(W, c);
+    uc = Row4<T>{u3.m, u3.a, u3.b, __ldg(U + c + 2)};
+    vc = Row4<T>{v3.m, v3.a, v3.b, __ldg(V + c + 2)};
+    wc = Row4<T>{w3.m, w3.a, w3.b, __ldg(W + c + 2)};
+  }
+  Row3<T> un = ld3(U, c + px), ut = ld3(U, c + pl);
+  Row2<T> us = ld2(U, c - px);
+  Row2<T> vn = ld2(V, c + px), vt = ld2(V, c + pl), vst = ld2(V, c - px + pl);
+  Row2<T> vs = ld2(V, c - px);
+  T vs_p = __ldg(V + c - px + 2);
+  Row2<T> wn = ld2(W, c + px), ws = ld2(W, c - px), wt = ld2(W, c + pl);
+  // carried k-1 face terms
+  Row2<T> FxzB, FyzB, dUz, dVz, dWz, WbA;
+  {
+    const Row2<T> ub = ld2(U, c - pl), vb = ld2(V, c - pl), wb = ld2(W, c - pl), wnb = ld2(W, c + px - pl);
+    const T wb_p = __ldg(W + c + 2 - pl);
+    FxzB.a = h * (ub.a + uc.a) * h * (wb.a + wb.b);
+    FxzB.b = h * (ub.b + uc.b) * h * (wb.b + wb_p);
+    FyzB.a = h * (vb.a + vc.a) * wsum(w0, wb.a, w1, wnb.a);
+    FyzB.b = h * (vb.b + vc.b) * wsum(w0, wb.b, w1, wnb.b);
+    dUz = Row2<T>{uc.a - ub.a, uc.b - ub.b};
+    dVz = Row2<T>{vc.a - vb.a, vc.b - vb.b};
+    dWz = Row2<T>{wc.a - wb.a, wc.b - wb.b};
+    WbA = Row2<T>{h * (wb.a + wc.a), h * (wb.b + wc.b)};
+  }
+  Row2<T> oU{}, oV{}, oW{}, fU{}, fV{}, fW{};
+  if (MODE != 0 && MODE != 1) { fU = ld2(F1u, c); fV = ld2(F1v, c); fW = ld2(F1w, c); }
+  if (MODE != 0) { oU = ld2(Uo, c); oV = ld2(Vo, c); oW = ld2(Wo, c); }
+  for (int k = k0;; ++k) {
+    // fetch ahead: rows of plane k+2 and Uo/F1 of plane k+1
+    const bool more = k < k1;
+    Row3<T> ut2{};
+    Row2<T> vt2{}, vst2{}, wt2{}, oU2{}, oV2{}, oW2{}, fU2{}, fV2{}, fW2{};
+    if (more) {
+      const long long c2p = c + 2 * pl, c1p = c + pl;
+      ut2 = ld3(U, c2p);
+      vt2 = ld2(V, c2p);
+      vst2 = ld2(V, c2p - px);
+      wt2 = ld2(W, c2p);
+      if (MODE != 0) { oU2 = ld2(Uo, c1p); oV2 = ld2(Vo, c1p); oW2 = ld2(Wo, c1p); }
+      if (MODE != 0 && MODE != 1) { fU2 = ld2(F1u, c1p); fV2 = ld2(F1v, c1p); fW2 = ld2(F1w, c1p); }
+    }
+    const T zF = m.zF[k], zrF = m.zrF[k], zC = m.zC[k], zrC = m.zrC[k], zrCm = m.zrC[k - 1], zrFp = m.zrF[k + 1];
+    // shared face fluxes of this plane
+    const T Xm = h * (uc.m + uc.a), Xa = h * (uc.a + uc.b), Xb = h * (uc.b + uc.p);
+    const T Fxy_m = (w0 * uc.m + w1 * un.m) * h * (vc.m + vc.a);
+    const T Fxy_a = (w0 * uc.a + w1 * un.a) * h * (vc.a + vc.b);
+    const T Fxy_b = (w0 * uc.b + w1 * un.b) * h * (vc.b + vc.p);
+    const T Fxz_m = h * (uc.m + ut.m) * h * (wc.m + wc.a);
+    const T Fxz_a = h * (uc.a + ut.a) * h * (wc.a + wc.b);
+    const T Fxz_b = h * (uc.b + ut.b) * h * (wc.b + wc.p);
+    const T Fyz_a = h * (vc.a + vt.a) * wsum(w0, wc.a, w1, wn.a);
+    const T Fyz_b = h * (vc.b + vt.b) * wsum(w0, wc.b, w1, wn.b);
+    const Row2<T> dUt{ut.a - uc.a, ut.b - uc.b}, dVt{vt.a - vc.a, vt.b - vc.b}, dWt{wt.a - wc.a, wt.b - wc.b};
+    // u
+    {
+      Row2<T> f{(T)0, (T)0};
+      T r = -qdiv(Xa * Xa - Xm * Xm, xC_a, xrC_a);
+      r = r - qdiv(Fxy_a - (w0m * us.a + w1m * uc.a) * h * (vs.a + vs.b), yF, yrF);
+      r = r - qdiv(Fxz_a - FxzB.a, zF, zrF);
+      T vx = qdiv(xrF_b * (uc.b - uc.a) - xrF_a * (uc.a - uc.m), xC_a, xrC_a);
+      T vy = qdiv(qdiv(un.a - uc.a, yC, yrC) - qdiv(uc.a - us.a, yCm, yrCm), yF, yrF);
+      T vz = qdiv(zrC * dUt.a - zrCm * dUz.a, zF, zrF);
+      if (!zu_a) f.a = r + dpdx + nu * (vx + vy + vz);
+      r = -qdiv(Xb * Xb - Xa * Xa, xC_b, xrC_b);
+      r = r - qdiv(Fxy_b - (w0m * us.b + w1m * uc.b) * h * (vs.b + vs_p), yF, yrF);
+      r = r - qdiv(Fxz_b - FxzB.b, zF, zrF);
+      vx = qdiv(xrF_p * (uc.p - uc.b) - xrF_b * (uc.b - uc.a), xC_b, xrC_b);
+      vy = qdiv(qdiv(un.b - uc.b, yC, yrC) - qdiv(uc.b - us.b, yCm, yrCm), yF, yrF);
+      vz = qdiv(zrC * dUt.b - zrCm * dUz.b, zF, zrF);
+      if (!zu_b) f.b = r + dpdx + nu * (vx + vy + vz);
+      rk_store2<T, MODE>(F1u, Un, c, f, oU, fU, cdt1, tdt, tc1, tc2, su_a, su_b);
+    }
+    // v
+    if (dv) {
+      Row2<T> f{(T)0, (T)0};
+      T aa = h * (vc.a + vn.a), bb = h * (vs.a + vc.a);
+      T r = -qdiv(aa * aa - bb * bb, yC, yrC);
+      r = r - qdiv(Fxy_a - Fxy_m, xF_a, xrF_a);
+      r = r - qdiv(Fyz_a - FyzB.a, zF, zrF);
+      T vx = qdiv(xrC_a * (vc.b - vc.a) - xrC_m * (vc.a - vc.m), xF_a, xrF_a);
+      T vy = qdiv(yrFp * (vn.a - vc.a) - yrF * (vc.a - vs.a), yC, yrC);
+      T vz = qdiv(zrC * dVt.a - zrCm * dVz.a, zF, zrF);
+      if (!zx_a) f.a = r + nu * (vx + vy + vz);
+      aa = h * (vc.b + vn.b);
+      bb = h * (vs.b + vc.b);
+      r = -qdiv(aa * aa - bb * bb, yC, yrC);
+      r = r - qdiv(Fxy_b - Fxy_a, xF_b, xrF_b);
+      r = r - qdiv(Fyz_b - FyzB.b, zF, zrF);
+      vx = qdiv(xrC_b * (vc.p - vc.b) - xrC_a * (vc.b - vc.a), xF_b, xrF_b);
+      vy = qdiv(yrFp * (vn.b - vc.b) - yrF * (vc.b - vs.b), yC, yrC);
+      vz = qdiv(zrC * dVt.b - zrCm * dVz.b, zF, zrF);
+      if (!zx_b) f.b = r + nu * (vx + vy + vz);
+      rk_store2<T, MODE>(F1v, Vn, c, f, oV, fV, cdt1, tdt, tc1, tc2, sv_a, sv_b);
+    }
+    // w
+    Row2<T> WtA{h * (wc.a + wt.a), h * (wc.b + wt.b)};
+    if (k <= g.nz - 1) {
+      Row2<T> f{(T)0, (T)0};
+      T r = -qdiv(WtA.a * WtA.a - WbA.a * WbA.a, zC, zrC);
+      r = r - qdiv(Fxz_a - Fxz_m, xF_a, xrF_a);
+      r = r - qdiv(Fyz_a - h * (vs.a + vst.a) * (w0m * ws.a + w1m * wc.a), yF, yrF);
+      T vx = qdiv(xrC_a * (wc.b - wc.a) - xrC_m * (wc.a - wc.m), xF_a, xrF_a);
+      T vy = qdiv(qdiv(wn.a - wc.a, yC, yrC) - qdiv(wc.a - ws.a, yCm, yrCm), yF, yrF);
+      T vz = qdiv(zrFp * dWt.a - zrF * dWz.a, zC, zrC);
+      if (!zx_a) f.a = r + dpdz + nu * (vx + vy + vz);
+      r = -qdiv(WtA.b * WtA.b - WbA.b * WbA.b, zC, zrC);
+      r = r - qdiv(Fxz_b - Fxz_a, xF_b, xrF_b);
+      r = r - qdiv(Fyz_b - h * (vs.b + vst.b) * (w0m * ws.b + w1m * wc.b), yF, yrF);
+      vx = qdiv(xrC_b * (wc.p - wc.b) - xrC_a * (wc.b - wc.a), xF_b, xrF_b);
+      vy = qdiv(qdiv(wn.b - wc.b, yC, yrC) - qdiv(wc.b - ws.b, yCm, yrCm), yF, yrF);
+      vz = qdiv(zrFp * dWt.b - zrF * dWz.b, zC, zrC);
+      if (!zx_b) f.b = r + dpdz + nu * (vx + vy + vz);
+      rk_store2<T, MODE>(F1w, Wn, c, f, oW, fW, cdt1, tdt, tc1, tc2, sv_a, sv_b);
+    }
+    if (!more) break;
+    // carry the upper face terms down and slide the window to k+1
+    FxzB = Row2<T>{Fxz_a, Fxz_b};
+    FyzB = Row2<T>{Fyz_a, Fyz_b};
+    dUz = dUt; dVz = dVt; dWz = dWt; WbA = WtA;
+    c += pl;
+    uc = Row4<T>{ut.m, ut.a, ut.b, __ldg(U + c + 2)};
+    vc = Row4<T>{__ldg(V + c - 1), vt.a, vt.b, __ldg(V + c + 2)};
+    wc = Row4<T>{__ldg(W + c - 1), wt.a, wt.b, __ldg(W + c + 2)};
+    vs = vst;
+    vs_p = __ldg(V + c - px + 2);
+    un = ld3(U, c + px);
+    us = ld2(U, c - px);
+    vn = ld2(V, c + px);
+    wn = ld2(W, c + px);
+    ws = ld2(W, c - px);
+    ut = ut2; vt = vt2; vst = vst2; wt = wt2;
+    oU = oU2; oV = oV2; oW = oW2; fU = fU2; fV = fV2; fW = fW2;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // project_velocity (projection.f90:359-384) + pressure save at rk_step 1
 // (projection.f90:75-78, P(2:nxg-1,2:nyg-1,2:nzg-1) = rhs_p/(dt*rk2_coef(1,1))).
 // p holds rhs_p in the box layout (i=2..nx, j=2..ny, k=2..nz valid).
@@ -853,10 +1096,17 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
   k_rhs_rk<T, M, L><<<grid, block, 0, st>>>(g, m, U, V, W, nut, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, \
                                             c2, kchunk)
   if (!les && sizeof(T) == 4) {  // FP32: register-window kernel (FP64 keeps the lower-register form)
-    const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 32;
-    dim3 gd = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc, by);
-#define BLGPU_DNS_CASE(M)                                                                                     \
-  k_rhs_rk_dns<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc)
+    const bool pair = tl.rhs_pts != 1;
+    const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : (pair ? 8 : 32);
+    // pairs cover i = 2..nx two points at a time
+    dim3 gd = vol_grid(pair ? g.nx / 2 : g.nx - 1, g.ny - 1, g.nz - 1, kc, by);
+#define BLGPU_DNS_CASE(M)                                                                                           \
+  do {                                                                                                              \
+    if (pair)                                                                                                       \
+      k_rhs_rk_pair<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); \
+    else                                                                                                            \
+      k_rhs_rk_dns<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc);  \
+  } while (0)
     switch (mode) {
       case 0: BLGPU_DNS_CASE(0); break;
       case 1: BLGPU_DNS_CASE(1); break;

@@ -65,7 +65,9 @@ def test_boundary_conditions(gpu, grid, rk_step):
     s.close()
 
 
-@pytest.mark.parametrize("grid", GRIDS)
+# N = nx-2 = 129 = 3*43 and 254 = 2*127: x transforms with a prime stage
+# above the register butterflies (direct summation over (butterfly, output))
+@pytest.mark.parametrize("grid", GRIDS + [(131, 9, 12), (256, 9, 12)])
 def test_projection(gpu, grid):
     c = noisy_laminar(*grid, seed=3)
     s = cases.solver_for(c)
