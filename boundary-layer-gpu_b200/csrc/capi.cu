@@ -60,6 +60,7 @@ struct blgpu_ctx {
   float *kz0g = nullptr;
   int klow = 0;
   uint32_t *zfrag = nullptr;  // mixed form: table fragments of the tensor-core z transforms (or null)
+  ZdftMaps zmaps{};           // and the TMA maps of R and C they read and write
   int nsm = 148;
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
@@ -167,6 +168,16 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
   return BLGPU_OK;
 }
 
+// the sticky device flag of the step kernels (stream already synchronized);
+// bit 2: a TMA copy of the tensor-core z transform missed its wait limit
+static int device_flag(blgpu_ctx *ctx) {
+  int f = 0;
+  CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
+  if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
+  if (f) return set_err(ctx, BLGPU_EDEVICE, "device flag %d set by a step kernel", f);
+  return BLGPU_OK;
+}
+
 static void drop_graphs(blgpu_ctx *ctx) {
   ctx->gen += 1;
   for (int r = 0; r < 3; ++r)
@@ -249,6 +260,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
     TRY(dalloc(ctx, (void **)&ctx->zfrag, fr.size() * sizeof(uint32_t)));
     TRY(check_cuda(ctx, cudaMemcpy(ctx->zfrag, fr.data(), fr.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
                    "z-transform tables"));
+    // without tensor maps the direct sums serve this box
+    if (!zdft_tc_maps(s, (float *)ctx->R, (float2 *)ctx->C, &ctx->zmaps)) ctx->zfrag = nullptr;
   }
   if (!ctx->fp64) {
     // the modes kx < klow of kz = 0 carry the box-scale pressure of a step's
@@ -823,7 +836,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const bool tc = mixed && ctx->zfrag && ctx->tiles.zdft == 0;
   ph_begin(ctx, PH_DFTZ);
-  if (tc) launch_zdft_tc(s, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, ctx->st);
+  if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, &ctx->sc->err, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
@@ -834,7 +847,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
     launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
   ph_end(ctx, mixed ? 3 : 1);
   ph_begin(ctx, PH_IDFTZ);
-  if (tc) launch_zdft_tc(s, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, ctx->st);
+  if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, &ctx->sc->err, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
@@ -986,7 +999,7 @@ int blgpu_sync(blgpu_ctx *ctx) {
   if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
   CK(cudaSetDevice(ctx->cfg.device));
   CK(cudaStreamSynchronize(ctx->st));
-  return BLGPU_OK;
+  return device_flag(ctx);
 }
 
 int blgpu_compute_dt(blgpu_ctx *ctx, double *dt) {
@@ -1172,7 +1185,7 @@ int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms) {
   if (rc) return rc;
   CK(e);
   *ms = (double)t;
-  return BLGPU_OK;
+  return device_flag(ctx);
 }
 
 int blgpu_eddy_viscosity(blgpu_ctx *ctx) {

@@ -128,9 +128,16 @@ void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm
 int zdft_tc_qp(const Spec &s);
 size_t zdft_tc_frag_words(const Spec &s);
 void zdft_tc_fragments(const Spec &s, std::vector<uint32_t> &out);
-// inverse = 0: R -> C (forward); 1: C -> R; nsm: persistent CTAs
-void launch_zdft_tc(const Spec &s, float *R, float2 *C, const uint32_t *frag, int inverse, int nsm,
-                    cudaStream_t st);
+// TMA tensor maps of R and C (CUtensorMap bytes); false when unavailable
+struct ZdftMaps {
+  alignas(64) unsigned char r[128];
+  alignas(64) unsigned char c[128];
+};
+bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
+// inverse = 0: R -> C (forward); 1: C -> R; nsm: persistent CTAs; err: device
+// flag, bit 2 set when a TMA copy did not complete within the wait limit
+void launch_zdft_tc(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *frag, int inverse,
+                    int nsm, int *err, cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);

@@ -14,11 +14,16 @@
 // which keeps the FP32 accuracy of the direct sums (error ~ 2^-22 relative).
 //
 // A persistent CTA per SM keeps the table fragments of its warp in registers
-// (loaded once) and walks the (b, kx-tile) work items: it stages the split
-// line data of NT = 64 kx columns in shared memory, each warp multiplies one
-// 16-row tile of the cos or the sin table by all of it, and the results leave
-// through shared memory as coalesced rows.
+// (loaded once) and walks the (b, kx-tile) work items.  The raw line data of
+// a work item (M rows x NT = 64 kx of R, or MH rows x 64 complex kx of C)
+// arrives by one TMA tensor copy into a double buffer, issued one item ahead
+// and completed on an mbarrier, so the DRAM latency of item i+1 overlaps the
+// products of item i.  The CTA then splits the operands into shared memory,
+// each warp multiplies one 16-row tile of the cos or the sin table by all of
+// them, and the results leave through shared memory as coalesced rows.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -28,9 +33,12 @@
 
 namespace blgpu {
 
+static_assert(sizeof(CUtensorMap) == sizeof(ZdftMaps::r), "tensor map size");
+
 namespace {
-constexpr int ZNT = 64;         // kx columns per work item
-constexpr int ZLD = ZNT + 8;    // row pitch of the staged operands (conflict-free fragment loads)
+constexpr int ZNT = 64;              // kx columns per work item
+constexpr int ZLD = ZNT + 8;         // row pitch of the staged operands (conflict-free fragment loads)
+constexpr int WAIT_LIMIT = 1 << 24;  // mbarrier polls (with back-off) before a copy counts as lost
 
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
   uint32_t r;
@@ -51,29 +59,85 @@ __device__ __forceinline__ void split(float x, uint32_t &hi, uint32_t &lo) {
   hi = tf32_rna(x);
   lo = tf32_rna(x - __uint_as_float(hi));
 }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for phase `parity` of an mbarrier; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if (it >= 32) __nanosleep(64);
+  }
+  return false;
+}
+// 2D tiled TMA load of one box into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
 }  // namespace
 
 // Table fragments, in the order the kernel reads them: for table t (0 cos,
 // 1 -sin), row tile mt, k step ks, lane l: 4 hi then 4 lo words of the
 // m16n8k8 A fragment (rows g, g+8; columns tig, tig+4 of the 16x8 block).
 // QP = Q rounded up to 16; entries beyond Q are zero.
+// Shared memory (floats): raw[2][rawf] | B0h B0l B1h B1l [QP][ZLD] | aux[2][ZNT] | 2 mbarriers.
 template <int QP>
-__global__ void __launch_bounds__(QP / 8 * 32, 1) k_zdft_tc(Spec s, float *__restrict__ R,
-                                                           float2 *__restrict__ C, const uint4 *__restrict__ frag,
-                                                           int inverse) {
+__global__ void __launch_bounds__(QP / 8 * 32, 1)
+    k_zdft_tc(const __grid_constant__ CUtensorMap mapR, const __grid_constant__ CUtensorMap mapC, Spec s,
+              float *__restrict__ R, float2 *__restrict__ C, const uint4 *__restrict__ frag, int inverse, int rawf,
+              int *__restrict__ err) {
   constexpr int MT = QP / 16;  // row tiles per table
   constexpr int KS = QP / 8;   // k steps
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float *B0h = reinterpret_cast<float *>(smem_raw);  // [QP][ZLD]: S (fwd) or Re (inv), hi part
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float *raw0 = reinterpret_cast<float *>(smem_raw);
+  float *B0h = raw0 + 2 * (size_t)rawf;  // [QP][ZLD]: S (fwd) or Re (inv), hi part
   float *B0l = B0h + QP * ZLD;
-  float *B1h = B0l + QP * ZLD;                       // D (fwd) or Im (inv)
+  float *B1h = B0l + QP * ZLD;           // D (fwd) or Im (inv)
   float *B1l = B1h + QP * ZLD;
-  float *aux = B1l + QP * ZLD;                       // [2][ZNT]: f_{M/2} row / c0 and Nyquist rows
-  float *stage = reinterpret_cast<float *>(smem_raw);  // epilogue staging, aliases the operands
+  float *aux = B1l + QP * ZLD;           // [2][ZNT]: f_{M/2} row / c0 and Nyquist rows
+  uint64_t *bar = reinterpret_cast<uint64_t *>(aux + 2 * ZNT);
+  float *stage = B0h;                    // epilogue staging, aliases the operands
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const bool even = (M & 1) == 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
   const int tbl = warp / MT, mt = warp % MT;  // table (0 cos, 1 -sin) and its row tile
+  const int ntile = (s.N + ZNT - 1) / ZNT;
+  const int nitems = s.NM * ntile;
+  const int nthr = blockDim.x;
+  // one box per work item: M rows x 64 floats of R, or MH rows x 128 floats (64 complex) of C
+  const uint32_t box_bytes = inverse ? (uint32_t)MH * 2 * ZNT * 4 : (uint32_t)M * ZNT * 4;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if ((int)blockIdx.x < nitems) {
+      const int b = blockIdx.x / ntile, kx0 = (blockIdx.x % ntile) * ZNT;
+      mbar_expect_tx(&bar[0], box_bytes);
+      if (inverse) tma_load_2d(raw0, &mapC, 2 * kx0, b * MH, &bar[0]);
+      else tma_load_2d(raw0, &mapR, kx0, b * M, &bar[0]);
+    }
+  }
   // the warp's table fragments, resident for the whole kernel
   uint32_t ahi[KS][4], alo[KS][4];
 #pragma unroll
@@ -84,24 +148,44 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1) k_zdft_tc(Spec s, float *__res
     alo[ks][0] = l.x; alo[ks][1] = l.y; alo[ks][2] = l.z; alo[ks][3] = l.w;
   }
   const float *Bh = tbl ? B1h : B0h, *Bl = tbl ? B1l : B0l;
-  const int ntile = (s.N + ZNT - 1) / ZNT;
-  const int nitems = s.NM * ntile;
-  const int nthr = blockDim.x;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+  int i = 0;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++i) {
     const int b = item / ntile, kx0 = (item % ntile) * ZNT;
-    __syncthreads();  // the previous item's staging is no longer read
-    // ---- stage the split operands ----
+    const int buf = i & 1;
+    const float *rw = raw0 + (size_t)buf * rawf;
+    // the previous item's staging and results are no longer read, and the
+    // other raw buffer was consumed before the previous item's products
+    __syncthreads();
+    const int next = item + gridDim.x;
+    if (threadIdx.x == 0 && next < nitems) {
+      const int nb = next / ntile, nk0 = (next % ntile) * ZNT;
+      float *dst = raw0 + (size_t)(buf ^ 1) * rawf;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic reads before the async write
+      mbar_expect_tx(&bar[buf ^ 1], box_bytes);
+      if (inverse) tma_load_2d(dst, &mapC, 2 * nk0, nb * MH, &bar[buf ^ 1]);
+      else tma_load_2d(dst, &mapR, nk0, nb * M, &bar[buf ^ 1]);
+    }
+    const bool ok = mbar_wait(&bar[buf], (uint32_t)(i >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(err, 2);
+        // let the copies this CTA issued finish (bounded) before leaving
+        mbar_wait(&bar[buf], (uint32_t)(i >> 1) & 1u);
+        if (next < nitems) mbar_wait(&bar[buf ^ 1], (uint32_t)((i + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    // ---- split the operands ----
     if (!inverse) {
-      const float *Rb = R + (size_t)b * M * s.rx + kx0;
       for (int q = threadIdx.x; q < QP * ZNT; q += nthr) {
         const int k = q / ZNT, c = q % ZNT;
         float sv = 0.f, dv = 0.f;
         if (kx0 + c < s.N && k <= H) {
-          const float fk = Rb[(size_t)k * s.rx + c];
+          const float fk = rw[k * ZNT + c];
           if (k == 0) {
             sv = fk;
           } else {
-            const float fm = Rb[(size_t)(M - k) * s.rx + c];
+            const float fm = rw[(M - k) * ZNT + c];
             sv = fk + fm;
             dv = fk - fm;
           }
@@ -115,14 +199,13 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1) k_zdft_tc(Spec s, float *__res
         B1l[k * ZLD + c] = __uint_as_float(l);
       }
       if (even)
-        for (int c = threadIdx.x; c < ZNT; c += nthr)
-          aux[c] = kx0 + c < s.N ? Rb[(size_t)(M / 2) * s.rx + c] : 0.f;
+        for (int c = threadIdx.x; c < ZNT; c += nthr) aux[c] = kx0 + c < s.N ? rw[(M / 2) * ZNT + c] : 0.f;
     } else {
-      const float2 *Cb = C + (size_t)b * MH * s.rx + kx0;
+      const float2 *cw = reinterpret_cast<const float2 *>(rw);  // [MH][ZNT]
       for (int q = threadIdx.x; q < QP * ZNT; q += nthr) {
         const int kz = q / ZNT, c = q % ZNT;
         float2 v = make_float2(0.f, 0.f);
-        if (kx0 + c < s.N && kz >= 1 && kz <= H) v = Cb[(size_t)kz * s.rx + c];
+        if (kx0 + c < s.N && kz >= 1 && kz <= H) v = cw[kz * ZNT + c];
         uint32_t h, l;
         split(v.x, h, l);
         B0h[kz * ZLD + c] = __uint_as_float(h);
@@ -132,9 +215,9 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1) k_zdft_tc(Spec s, float *__res
         B1l[kz * ZLD + c] = __uint_as_float(l);
       }
       for (int c = threadIdx.x; c < ZNT; c += nthr) {
-        const bool ok = kx0 + c < s.N;
-        aux[c] = ok ? Cb[c].x : 0.f;                                          // c0
-        aux[ZNT + c] = (ok && even) ? Cb[(size_t)(M / 2) * s.rx + c].x : 0.f;  // Nyquist
+        const bool okc = kx0 + c < s.N;
+        aux[c] = okc ? cw[c].x : 0.f;                                  // c0
+        aux[ZNT + c] = (okc && even) ? cw[(M / 2) * ZNT + c].x : 0.f;  // Nyquist
       }
     }
     __syncthreads();
@@ -197,10 +280,58 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1) k_zdft_tc(Spec s, float *__res
   }
 }
 
-// Q rounded up to 16 when the tensor-core path serves it, else 0
+// floats of one raw buffer: the larger of the two boxes, in 128-byte units
+static int raw_floats(const Spec &s) {
+  const int f = s.M * ZNT > s.MH * 2 * ZNT ? s.M * ZNT : s.MH * 2 * ZNT;
+  return (f + 31) / 32 * 32;
+}
+
+static size_t smem_bytes(const Spec &s, int qp) {
+  return ((size_t)2 * raw_floats(s) + (size_t)4 * qp * ZLD + 2 * ZNT) * sizeof(float) + 2 * sizeof(uint64_t);
+}
+
+// Q rounded up to 16 when the tensor-core path serves it, else 0 (the TMA
+// boxes are at most 256 rows and the buffers fit one CTA's shared memory)
 int zdft_tc_qp(const Spec &s) {
   const int qp = (s.MH + 15) / 16 * 16;
-  return (qp == 32 || qp == 48 || qp == 64 || qp == 80 || qp == 96) ? qp : 0;
+  if (!(qp == 32 || qp == 48 || qp == 64 || qp == 80 || qp == 96)) return 0;
+  if (s.M > 256 || smem_bytes(s, qp) > 227 * 1024) return 0;
+  return qp;
+}
+
+// Tensor maps of R (rx x NM*M floats, box 64 x M) and of C viewed as floats
+// (2 rx x NM*MH, box 128 x MH); false when the driver entry point or the
+// encoding is unavailable (the caller then keeps the direct sums).
+bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+  if (!enc) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  if ((reinterpret_cast<uintptr_t>(R) & 15) || (reinterpret_cast<uintptr_t>(C) & 15)) return false;
+  CUtensorMap mr, mc;
+  const cuuint32_t es[2] = {1, 1};
+  const cuuint64_t dr[2] = {(cuuint64_t)s.rx, (cuuint64_t)s.NM * s.M};
+  const cuuint64_t sr[1] = {(cuuint64_t)s.rx * sizeof(float)};
+  const cuuint32_t br[2] = {(cuuint32_t)ZNT, (cuuint32_t)s.M};
+  if (enc(&mr, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, R, dr, sr, br, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  const cuuint64_t dc[2] = {(cuuint64_t)2 * s.rx, (cuuint64_t)s.NM * s.MH};
+  const cuuint64_t sc[1] = {(cuuint64_t)2 * s.rx * sizeof(float)};
+  const cuuint32_t bc[2] = {(cuuint32_t)(2 * ZNT), (cuuint32_t)s.MH};
+  if (enc(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dc, sc, bc, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  memcpy(out->r, &mr, sizeof mr);
+  memcpy(out->c, &mc, sizeof mc);
+  return true;
 }
 
 size_t zdft_tc_frag_words(const Spec &s) {
@@ -246,24 +377,27 @@ void zdft_tc_fragments(const Spec &s, std::vector<uint32_t> &out) {
 }
 
 template <int QP>
-static void launch_qp(const Spec &s, float *R, float2 *C, const uint4 *frag, int inverse, int nsm,
-                      cudaStream_t st) {
-  const size_t sm = ((size_t)4 * QP * ZLD + 2 * ZNT) * sizeof(float);
+static void launch_qp(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, const uint4 *frag, int inverse,
+                      int nsm, int *err, cudaStream_t st) {
+  const size_t sm = smem_bytes(s, QP);
   cudaFuncSetAttribute(k_zdft_tc<QP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int nitems = s.NM * ((s.N + ZNT - 1) / ZNT);
   const int grid = nitems < nsm ? nitems : nsm;
-  k_zdft_tc<QP><<<grid, QP / 8 * 32, sm, st>>>(s, R, C, frag, inverse);
+  CUtensorMap mr, mc;
+  memcpy(&mr, mp.r, sizeof mr);
+  memcpy(&mc, mp.c, sizeof mc);
+  k_zdft_tc<QP><<<grid, QP / 8 * 32, sm, st>>>(mr, mc, s, R, C, frag, inverse, raw_floats(s), err);
 }
 
-void launch_zdft_tc(const Spec &s, float *R, float2 *C, const uint32_t *frag, int inverse, int nsm,
-                    cudaStream_t st) {
+void launch_zdft_tc(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *frag, int inverse,
+                    int nsm, int *err, cudaStream_t st) {
   const uint4 *f = reinterpret_cast<const uint4 *>(frag);
   switch (zdft_tc_qp(s)) {
-    case 32: launch_qp<32>(s, R, C, f, inverse, nsm, st); break;
-    case 48: launch_qp<48>(s, R, C, f, inverse, nsm, st); break;
-    case 64: launch_qp<64>(s, R, C, f, inverse, nsm, st); break;
-    case 80: launch_qp<80>(s, R, C, f, inverse, nsm, st); break;
-    case 96: launch_qp<96>(s, R, C, f, inverse, nsm, st); break;
+    case 32: launch_qp<32>(s, maps, R, C, f, inverse, nsm, err, st); break;
+    case 48: launch_qp<48>(s, maps, R, C, f, inverse, nsm, err, st); break;
+    case 64: launch_qp<64>(s, maps, R, C, f, inverse, nsm, err, st); break;
+    case 80: launch_qp<80>(s, maps, R, C, f, inverse, nsm, err, st); break;
+    case 96: launch_qp<96>(s, maps, R, C, f, inverse, nsm, err, st); break;
     default: break;
   }
 }
