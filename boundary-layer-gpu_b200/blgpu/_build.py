@@ -27,6 +27,7 @@ SOURCES = {
     "mlp.cu": [],
     "capi_mlp.cu": [],
     "zdft_tc.cu": [],
+    "snapshot.cpp": [],
 }
 
 
@@ -50,7 +51,7 @@ def build(force=False, verbose=False):
 
     def compile_one(name):
         src = os.path.join(CSRC, name)
-        obj = os.path.join(OBJ_DIR, name.replace(".cu", ".o"))
+        obj = os.path.join(OBJ_DIR, os.path.splitext(name)[0] + ".o")
         cmd = [NVCC] + COMMON + SOURCES[name] + ["-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

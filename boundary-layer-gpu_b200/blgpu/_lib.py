@@ -22,6 +22,37 @@ class Config(ctypes.Structure):
     ]
 
 
+class Params(ctypes.Structure):
+    """blgpu_params: the .turbb keys of initparams (params.f90:119-197)."""
+    _fields_ = [
+        ("nu", ctypes.c_double), ("cfl", ctypes.c_double), ("vmax", ctypes.c_double),
+        ("x0", ctypes.c_double), ("sigma", ctypes.c_double), ("phi", ctypes.c_double),
+        ("nsteps", ctypes.c_int), ("nsave", ctypes.c_int), ("nstats", ctypes.c_int), ("nmonitor", ctypes.c_int),
+        ("nxyz", ctypes.c_int * 3), ("boxsize", ctypes.c_double * 4),
+        ("inflow_flag", ctypes.c_int), ("top_flag", ctypes.c_int), ("inflow_file", ctypes.c_char * 201),
+        ("lund_ix", ctypes.c_int), ("lund_deltai", ctypes.c_double), ("lund_T", ctypes.c_double),
+        ("dpdx", ctypes.c_double), ("dpdz", ctypes.c_double),
+        ("les", ctypes.c_int), ("wm", ctypes.c_int), ("tauw_model", ctypes.c_int), ("nut_bc", ctypes.c_int),
+        ("wm_nut_flag", ctypes.c_int), ("wm_nut", ctypes.c_double), ("amplitude", ctypes.c_double),
+        ("init_step", ctypes.c_int), ("init_rand", ctypes.c_int),
+        ("filein", ctypes.c_char * 201), ("fileout", ctypes.c_char * 201), ("timeinflow_file", ctypes.c_char * 201),
+        ("rk_scheme", ctypes.c_int), ("alphas", ctypes.c_double * 5), ("found", ctypes.c_ulonglong),
+    ]
+
+
+# .turbb keys in the order of the bits of Params.found
+PARAM_KEYS = ["nu", "CFL", "Vmax", "x0", "sigma", "phi", "nsteps", "nsave", "nstats", "nmonitor", "nxyz",
+              "boxsize", "inflow_flag", "top_flag", "inflow_file", "Lund_ix", "Lund_deltai", "Lund_T", "dPdx",
+              "dPdz", "LES", "WM", "TauwModel", "nutBC", "WMnutflag", "WMnut", "Amplitude", "init_step",
+              "init_rand", "filein", "fileout", "timeinflow_file", "RKscheme", "alphas"]
+
+
+class SnapshotInfo(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("nu", ctypes.c_double), ("step", ctypes.c_int),
+                ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("full_planes", ctypes.c_int), ("has_nu_t_p", ctypes.c_int)]
+
+
 FP64 = 0
 MIXED = 1
 POISSON_NATIVE = 0
@@ -95,6 +126,20 @@ _SIGS = {
     "blgpu_mlp_eval": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
     "blgpu_set_wall_model": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "blgpu_wall_stress": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),
+    "blgpu_box": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 3 + [c_double_p]),
+    "blgpu_get_grid": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p]),
+    "blgpu_io_last_error": (ctypes.c_char_p, []),
+    "blgpu_read_params": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Params)]),
+    "blgpu_params_config": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(Config)]),
+    "blgpu_snapshot_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(SnapshotInfo)]),
+    "blgpu_read_snapshot": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(SnapshotInfo)] + [c_double_p] * 8),
+    "blgpu_write_snapshot": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 + [ctypes.c_double] * 2
+                             + [ctypes.c_int] + [c_double_p] * 8),
+    "blgpu_read_rescaling": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p]),
+    "blgpu_write_rescaling": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p]),
+    "blgpu_snapshot_name": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "blgpu_output_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "blgpu_read_input_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
 }
 
 PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]
@@ -130,6 +175,12 @@ class BlgpuError(RuntimeError):
 def check(rc, ctx=None):
     if rc != 0:
         msg = load().blgpu_last_error(ctx)
+        raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))
+
+
+def check_io(rc):
+    if rc != 0:
+        msg = load().blgpu_io_last_error()
         raise BlgpuError("blgpu error %d: %s" % (rc, msg.decode() if msg else "?"))
 
 

@@ -1,0 +1,104 @@
+"""The reference's files through the C ABI (host code, no device needed).
+
+read_params       .turbb run parameters (params.f90:119-207, miscel.f90:13-262)
+read_snapshot     flow snapshot (read_input_data, input_output.f90:288-487)
+write_snapshot    flow snapshot in the one-process layout (output_data, input_output.f90:496-680)
+read_rescaling,
+write_rescaling   <snapshot>.mean.rescaling Lund means (input_output.f90:440-458, 668-676)
+snapshot_name     fileout.%08d
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import Config, Params, PARAM_KEYS, SnapshotInfo, check_io, load
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def _f64(a):
+    return np.asfortranarray(a, dtype=np.float64)
+
+
+def read_params(path):
+    """dict of the .turbb keys that were given (reference key names), plus
+    'found' (list of those names) and 'config' (the blgpu_config fields)."""
+    p = Params()
+    check_io(load().blgpu_read_params(str(path).encode(), ctypes.byref(p)))
+    out = {}
+    vals = {
+        "nu": p.nu, "CFL": p.cfl, "Vmax": p.vmax, "x0": p.x0, "sigma": p.sigma, "phi": p.phi,
+        "nsteps": p.nsteps, "nsave": p.nsave, "nstats": p.nstats, "nmonitor": p.nmonitor,
+        "nxyz": list(p.nxyz), "boxsize": list(p.boxsize), "inflow_flag": p.inflow_flag, "top_flag": p.top_flag,
+        "inflow_file": p.inflow_file.decode(), "Lund_ix": p.lund_ix, "Lund_deltai": p.lund_deltai,
+        "Lund_T": p.lund_T, "dPdx": p.dpdx, "dPdz": p.dpdz, "LES": p.les, "WM": p.wm,
+        "TauwModel": p.tauw_model, "nutBC": p.nut_bc, "WMnutflag": p.wm_nut_flag, "WMnut": p.wm_nut,
+        "Amplitude": p.amplitude, "init_step": p.init_step, "init_rand": p.init_rand,
+        "filein": p.filein.decode(), "fileout": p.fileout.decode(), "timeinflow_file": p.timeinflow_file.decode(),
+        "RKscheme": p.rk_scheme, "alphas": list(p.alphas),
+    }
+    found = [k for q, k in enumerate(PARAM_KEYS) if p.found >> q & 1]
+    for k in found:
+        out[k] = vals[k]
+    out["found"] = found
+    out["init_step"] = p.init_step  # -45 when not given
+    cfg = Config()
+    check_io(load().blgpu_params_config(ctypes.byref(p), ctypes.byref(cfg)))
+    out["config"] = {f: getattr(cfg, f) for f, _ in Config._fields_ if f in
+                     ("nx", "ny", "nz", "nu", "cfl", "dpdx", "dpdz", "rk_scheme", "les_model")}
+    return out
+
+
+def snapshot_info(path):
+    h = SnapshotInfo()
+    check_io(load().blgpu_snapshot_info_read(str(path).encode(), ctypes.byref(h)))
+    return {f: getattr(h, f) for f, _ in SnapshotInfo._fields_}
+
+
+def read_snapshot(path):
+    """dict with t, nu, step, x, y, z, U, V, W, nu_t, P (Fortran-layout arrays)."""
+    info = snapshot_info(path)
+    nx, ny, nz = info["nx"], info["ny"], info["nz"]
+    nxg, nyg, nzg = nx + 1, ny + 1, nz + 1
+    x, y, z = np.zeros(nx), np.zeros(ny), np.zeros(nz)
+    U = np.zeros((nx, nyg, nzg), order="F")
+    V = np.zeros((nxg, ny, nzg), order="F")
+    W = np.zeros((nxg, nyg, nz), order="F")
+    nt = np.zeros((nxg, nyg, nzg), order="F")
+    P = np.zeros((nxg, nyg, nzg), order="F")
+    h = SnapshotInfo()
+    check_io(load().blgpu_read_snapshot(str(path).encode(), ctypes.byref(h), _p(x), _p(y), _p(z), _p(U), _p(V),
+                                        _p(W), _p(nt), _p(P)))
+    out = {f: getattr(h, f) for f, _ in SnapshotInfo._fields_}
+    out.update(x=x, y=y, z=z, U=U, V=V, W=W, nu_t=nt, P=P)
+    return out
+
+
+def write_snapshot(path, t, nu, step, x, y, z, U, V, W, nu_t=None, P=None):
+    nx, ny, nz = len(x), len(y), len(z)
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    U, V, W = _f64(U), _f64(V), _f64(W)
+    nu_t = _f64(nu_t) if nu_t is not None else None
+    P = _f64(P) if P is not None else None
+    assert U.shape == (nx, ny + 1, nz + 1) and V.shape == (nx + 1, ny, nz + 1) and W.shape == (nx + 1, ny + 1, nz)
+    check_io(load().blgpu_write_snapshot(str(path).encode(), nx, ny, nz, float(t), float(nu), int(step), _p(x),
+                                         _p(y), _p(z), _p(U), _p(V), _p(W), _p(nu_t), _p(P)))
+
+
+def read_rescaling(path, ny):
+    um, vm = np.zeros(ny + 1), np.zeros(ny)
+    check_io(load().blgpu_read_rescaling(str(path).encode(), ny + 1, ny, _p(um), _p(vm)))
+    return um, vm
+
+
+def write_rescaling(path, Umean, Vmean):
+    um, vm = np.ascontiguousarray(Umean, dtype=np.float64), np.ascontiguousarray(Vmean, dtype=np.float64)
+    check_io(load().blgpu_write_rescaling(str(path).encode(), len(um), len(vm), _p(um), _p(vm)))
+
+
+def snapshot_name(fileout, step):
+    buf = ctypes.create_string_buffer(4096)
+    check_io(load().blgpu_snapshot_name(str(fileout).encode(), int(step), buf, 4096))
+    return buf.value.decode()

@@ -132,6 +132,22 @@ class Solver:
         self._ck(self.lib.blgpu_download_state(self.ctx, _p(U), _p(V), _p(W), _p(P), ctypes.byref(t)))
         return U, V, W, P, t.value
 
+    # -- the reference's files -------------------------------------------------
+    def output_data(self, fileout, step, rescaling=False):
+        """output_data: writes fileout.<step> (one-process layout), links
+        fileout.restart to it and, with rescaling, the Lund means file."""
+        _lib.check_io(self.lib.blgpu_output_data(self.ctx, str(fileout).encode(), int(step), int(bool(rescaling))))
+
+    def read_input_data(self, filein):
+        """read_input_data: grid (replaces the current one), U, V, W and t
+        from a snapshot; returns the file's step (-1 when absent)."""
+        st = ctypes.c_int(0)
+        _lib.check_io(self.lib.blgpu_read_input_data(self.ctx, str(filein).encode(), ctypes.byref(st)))
+        x, y, z = np.zeros(self.nx), np.zeros(self.ny), np.zeros(self.nz)
+        self._ck(self.lib.blgpu_get_grid(self.ctx, _p(x), _p(y), _p(z)))
+        self.x, self.y, self.z = x, y, z
+        return st.value
+
     # -- the step path ------------------------------------------------------
     def compute_dt(self):
         dt = ctypes.c_double()

@@ -809,6 +809,24 @@ int blgpu_get_time(blgpu_ctx *ctx, double *t, double *dt) {
   return BLGPU_OK;
 }
 
+int blgpu_box(const blgpu_ctx *ctx, int *nx, int *ny, int *nz, double *nu) {
+  if (!ctx) return BLGPU_EINVAL;
+  if (nx) *nx = ctx->nx;
+  if (ny) *ny = ctx->ny;
+  if (nz) *nz = ctx->nz;
+  if (nu) *nu = ctx->cfg.nu;
+  return BLGPU_OK;
+}
+
+int blgpu_get_grid(blgpu_ctx *ctx, double *x, double *y, double *z) {
+  if (!ctx || !x || !y || !z) return set_err(ctx, BLGPU_EINVAL, "blgpu_get_grid: null argument");
+  if (!ctx->have_grid) return set_err(ctx, BLGPU_ESTATE, "blgpu_get_grid: no grid yet");
+  for (int i = 0; i < ctx->nx; ++i) x[i] = ctx->x[i + 1];
+  for (int j = 0; j < ctx->ny; ++j) y[j] = ctx->y[j + 1];
+  for (int k = 0; k < ctx->nz; ++k) z[k] = ctx->z[k + 1];
+  return BLGPU_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -111,6 +111,10 @@ int blgpu_get_rescaling(blgpu_ctx *ctx, double *Umean_resc, double *Vmean_resc, 
 /* eddy viscosity nu_t(nxg,nyg,nzg) supplied by the host (LES = 2) */
 int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t);
 
+/* box sizes and viscosity of a context; the face grids given to set_grid */
+int blgpu_box(const blgpu_ctx *ctx, int *nx, int *ny, int *nz, double *nu);
+int blgpu_get_grid(blgpu_ctx *ctx, double *x, double *y, double *z);
+
 /* state in/out (main.f90:61-81 copy-in; main.f90:99-101 update self).
  * Upload also sets Uo = U as read_input_data does (input_output.f90:476-478). */
 int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
@@ -292,6 +296,92 @@ int blgpu_set_wall_model(blgpu_ctx *ctx, int mode, int jh, const blgpu_mlp *net)
 /* the model's stress on the current state at i = 2..nx-1 (fastest),
  * k = 2..nzg-2: (nx-2)(nzg-3) values each */
 int blgpu_wall_stress(blgpu_ctx *ctx, double *tau_x, double *tau_z);
+
+/* ---- the reference's files: .turbb parameters, snapshots, Lund means ----
+ * Host code only (no device needed); messages of these calls come from
+ * blgpu_io_last_error(). */
+
+/* Every key initparams reads (params.f90:119-197), in its order; bit q of
+ * `found` is set when the q-th key was present (BLGPU_PARAM_*).  Keys not
+ * given keep 0 (init_step: -45, "not given", input_output.f90:33). */
+typedef struct blgpu_params {
+  double nu, cfl, vmax, x0, sigma, phi;       /* nu CFL Vmax x0 sigma phi */
+  int nsteps, nsave, nstats, nmonitor;
+  int nxyz[3];
+  double boxsize[4];                         /* Lx Ly Lz alpha */
+  int inflow_flag, top_flag;
+  char inflow_file[201];
+  int lund_ix;
+  double lund_deltai, lund_T;
+  double dpdx, dpdz;
+  int les, wm, tauw_model, nut_bc, wm_nut_flag;  /* LES WM TauwModel nutBC WMnutflag */
+  double wm_nut, amplitude;                  /* WMnut Amplitude */
+  int init_step, init_rand;
+  char filein[201], fileout[201], timeinflow_file[201];
+  int rk_scheme;                             /* RKscheme */
+  double alphas[5];
+  unsigned long long found;
+} blgpu_params;
+enum {
+  BLGPU_PARAM_NU, BLGPU_PARAM_CFL, BLGPU_PARAM_VMAX, BLGPU_PARAM_X0, BLGPU_PARAM_SIGMA, BLGPU_PARAM_PHI,
+  BLGPU_PARAM_NSTEPS, BLGPU_PARAM_NSAVE, BLGPU_PARAM_NSTATS, BLGPU_PARAM_NMONITOR, BLGPU_PARAM_NXYZ,
+  BLGPU_PARAM_BOXSIZE, BLGPU_PARAM_INFLOW_FLAG, BLGPU_PARAM_TOP_FLAG, BLGPU_PARAM_INFLOW_FILE, BLGPU_PARAM_LUND_IX,
+  BLGPU_PARAM_LUND_DELTAI, BLGPU_PARAM_LUND_T, BLGPU_PARAM_DPDX, BLGPU_PARAM_DPDZ, BLGPU_PARAM_LES, BLGPU_PARAM_WM,
+  BLGPU_PARAM_TAUWMODEL, BLGPU_PARAM_NUTBC, BLGPU_PARAM_WMNUTFLAG, BLGPU_PARAM_WMNUT, BLGPU_PARAM_AMPLITUDE,
+  BLGPU_PARAM_INIT_STEP, BLGPU_PARAM_INIT_RAND, BLGPU_PARAM_FILEIN, BLGPU_PARAM_FILEOUT,
+  BLGPU_PARAM_TIMEINFLOW_FILE, BLGPU_PARAM_RKSCHEME, BLGPU_PARAM_ALPHAS
+};
+const char *blgpu_io_last_error(void);
+/* initparams through getvar (miscel.f90:13-262): a line matches a key when
+ * the text before its first '=' is the key; the value runs to a '!'; the
+ * first match wins.  BLGPU_EINVAL for a missing file, an unreadable value,
+ * no inflow_file, or init_rand = 1 with a filein (params.f90:136-139,166-169). */
+int blgpu_read_params(const char *path, blgpu_params *p);
+/* the blgpu_config fields a .turbb sets (sizes, nu, CFL, dPdx, dPdz,
+ * RKscheme, LES); the others are left as they are */
+int blgpu_params_config(const blgpu_params *p, blgpu_config *cfg);
+
+/* Snapshot: t, nu; -73 and the step; x, y, z, xm, ym, zm with their sizes;
+ * then U, V, W, nu_t, P, each after its 3 dims (input_output.f90:521-636).
+ * One process writes n3-1 planes of U, V, W and nu_t and all planes of P
+ * (the layout of the reference's GPU runs and of its plotting scripts); a
+ * file assembled from several processes holds every plane.  The reader
+ * accepts both, and files that end after W (then nu_t and P read as 0); a
+ * plane left out is filled as the z-periodic boundary pass fills it. */
+typedef struct blgpu_snapshot_info {
+  double t, nu;
+  int step;          /* -1 when the file has no magic number */
+  int nx, ny, nz;
+  int full_planes;   /* 1: every plane stored; 0: the one-process layout */
+  int has_nu_t_p;
+} blgpu_snapshot_info;
+int blgpu_snapshot_info_read(const char *path, blgpu_snapshot_info *h);
+/* any output pointer may be NULL; U(nx,nyg,nzg) V(nxg,ny,nzg) W(nxg,nyg,nz)
+ * nu_t, P (nxg,nyg,nzg) as everywhere in this header */
+int blgpu_read_snapshot(const char *path, blgpu_snapshot_info *h, double *x, double *y, double *z, double *U,
+                        double *V, double *W, double *nu_t, double *P);
+/* writes the one-process layout; nu_t and P may be NULL (zeros) */
+int blgpu_write_snapshot(const char *path, int nx, int ny, int nz, double t, double nu, int step, const double *x,
+                         const double *y, const double *z, const double *U, const double *V, const double *W,
+                         const double *nu_t, const double *P);
+/* <snapshot>.mean.rescaling: nyg, Umean_resc(nyg), Vmean_resc(ny); written
+ * in native byte order, read in either (the reference writes native and
+ * reads big-endian, input_output.f90:445,671) */
+int blgpu_read_rescaling(const char *path, int nyg, int ny, double *Umean, double *Vmean);
+int blgpu_write_rescaling(const char *path, int nyg, int ny, const double *Umean, const double *Vmean);
+/* fileout.%08d (input_output.f90:516-518) */
+int blgpu_snapshot_name(const char *fileout, int step, char *name, int cap);
+/* output_data (input_output.f90:496-680) for a context: downloads the state,
+ * writes fileout.<step>, points fileout.restart at it and, when rescaling
+ * != 0, writes the Lund means to fileout.<step>.mean.rescaling.  Creates the
+ * directory of fileout if missing (params.f90:177-191). */
+int blgpu_output_data(blgpu_ctx *ctx, const char *fileout, int step, int rescaling);
+/* read_input_data (input_output.f90:288-487) for a context: size checks,
+ * the file's grid replaces the context's (blgpu_set_grid), U, V, W and t are
+ * uploaded; *step (may be NULL) = the file's step or -1.  The Lund means of
+ * filein.mean.rescaling go to blgpu_set_rescaling through
+ * blgpu_read_rescaling. */
+int blgpu_read_input_data(blgpu_ctx *ctx, const char *filein, int *step);
 
 #ifdef __cplusplus
 }

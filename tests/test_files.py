@@ -1,0 +1,198 @@
+"""The reference's files through the C ABI (host code; no device needed):
+.turbb parameters as initparams reads them (params.f90:119-207 through
+miscel.f90:13-262), snapshots in the layout of output_data / read_input_data
+(input_output.f90:288-680) and the Lund means file."""
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from blgpu import files, BlgpuError
+
+REF = "/root/reference"
+
+
+def write_turbb(path, text):
+    path.write_text(text)
+    return str(path)
+
+
+def test_turbb_syntax(tmp_path):
+    f = write_turbb(tmp_path / "a.turbb", "\n".join([
+        "! comment line, nu = 7 is not read",
+        "nxyz = 34 17 12 ! (*) trailing comment",
+        "!WM = 3",
+        "  nu   =  1.5d-5",
+        "CFL = -2E-3",
+        "nu = 9.0             ! a second nu: the first line wins",
+        "RKscheme = 3",
+        "boxsize = 10.0, 0.5 ,0.2 3.",
+        "alphas = 5*0.25",
+        "inflow_file =./profiles/blasius.dat",
+        "fileout = out/BL ! where to write",
+        "init_rand = 1",
+        "LES =",                      # blank value: absent
+        "WMnut = 0.05",
+        "line without an equals sign",
+    ]))
+    p = files.read_params(f)
+    assert p["nxyz"] == [34, 17, 12]
+    assert p["nu"] == 1.5e-5 and p["CFL"] == -2e-3 and p["RKscheme"] == 3
+    assert p["boxsize"] == [10.0, 0.5, 0.2, 3.0]
+    assert p["alphas"] == [0.25] * 5
+    assert p["inflow_file"] == "./profiles/blasius.dat" and p["fileout"] == "out/BL"
+    assert "WM" not in p and "LES" not in p and "filein" not in p
+    assert p["WMnut"] == 0.05
+    assert p["init_step"] == -45  # not given
+    assert p["config"] == dict(nx=34, ny=17, nz=12, nu=1.5e-5, cfl=-2e-3, dpdx=0.0, dpdz=0.0, rk_scheme=3,
+                               les_model=0)
+
+
+def test_turbb_errors(tmp_path):
+    with pytest.raises(BlgpuError, match="does not exist"):
+        files.read_params(tmp_path / "missing.turbb")
+    with pytest.raises(BlgpuError, match="inflow_file"):
+        files.read_params(write_turbb(tmp_path / "b.turbb", "nxyz = 4 4 4\n"))
+    with pytest.raises(BlgpuError, match="init_rand = 1, but filein exists"):
+        files.read_params(write_turbb(tmp_path / "c.turbb", "inflow_file = a\ninit_rand = 1\nfilein = x\n"))
+    with pytest.raises(BlgpuError, match="not an integer"):
+        files.read_params(write_turbb(tmp_path / "d.turbb", "inflow_file = a\nnsteps = 1e3\n"))
+    with pytest.raises(BlgpuError, match="expected 3"):
+        files.read_params(write_turbb(tmp_path / "e.turbb", "inflow_file = a\nnxyz = 4 4\n"))
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+def test_reference_turbb_files():
+    p = files.read_params(os.path.join(REF, "laminar_test", "laminar.turbb"))
+    assert p["nxyz"] == [302, 64, 8] and p["CFL"] == -5e-5 and p["nu"] == 1e-5
+    assert p["RKscheme"] == 2 and p["init_rand"] == 1 and p["inflow_flag"] == 1 and p["top_flag"] == 0
+    assert p["boxsize"] == [10.0, 0.10, 0.2, 3.0]
+    assert p["inflow_file"] == "blasius_solution.dat" and p["fileout"] == "./data/BL_laminar"
+    q = files.read_params(os.path.join(REF, "tests", "test.turbb"))
+    assert q["nxyz"] == [1156, 192, 34] and q["inflow_flag"] == 5 and q["LES"] == 1
+    assert q["Lund_ix"] == 200 and q["Lund_deltai"] == 0.024998 and q["Lund_T"] == 0.5
+    assert q["filein"] == "./data/test_swap.00500000" and q["init_step"] == 500000
+    r = files.read_params(os.path.join(REF, "transition_test", "transition.turbb"))
+    assert r["nxyz"] == [814, 125, 66] and r["Amplitude"] == 0.20
+    assert r["timeinflow_file"] == "temporal_modes_inlet.dat"
+
+
+def box(nx, ny, nz, seed):
+    rng = np.random.default_rng(seed)
+    nxg, nyg, nzg = nx + 1, ny + 1, nz + 1
+    x = 1.0 + np.cumsum(rng.uniform(0.5, 1.5, nx)) - 0.75
+    y = np.concatenate([[0.0], np.cumsum(rng.uniform(0.1, 1.0, ny - 1))])
+    z = np.linspace(0.0, 3.0, nz)
+    U = np.asfortranarray(rng.standard_normal((nx, nyg, nzg)))
+    V = np.asfortranarray(rng.standard_normal((nxg, ny, nzg)))
+    W = np.asfortranarray(rng.standard_normal((nxg, nyg, nz)))
+    nt = np.asfortranarray(rng.standard_normal((nxg, nyg, nzg)))
+    P = np.asfortranarray(rng.standard_normal((nxg, nyg, nzg)))
+    return x, y, z, U, V, W, nt, P
+
+
+def reader_one_process(path):
+    """The snapshot layout restated in numpy: the reference's GPU runs write
+    n3-1 z-planes of U, V, W (and nu_t) after their 3 dims, P in full."""
+    with open(path, "rb") as f:
+        t, nu = struct.unpack("dd", f.read(16))
+        magic, step = struct.unpack("ii", f.read(8))
+        mesh = []
+        for _ in range(6):
+            n = struct.unpack("i", f.read(4))[0]
+            mesh.append(np.frombuffer(f.read(8 * n), dtype="<f8"))
+        fields = []
+        for q in range(5):
+            n1, n2, n3 = struct.unpack("iii", f.read(12))
+            n3a = n3 if q == 4 else n3 - 1
+            a = np.frombuffer(f.read(8 * n1 * n2 * n3a), dtype="<f8").reshape((n3a, n2, n1)).transpose(2, 1, 0)
+            fields.append(a)
+        assert f.read() == b""
+    return t, nu, magic, step, mesh, fields
+
+
+def test_snapshot_layout_and_round_trip(tmp_path):
+    nx, ny, nz = 9, 7, 6
+    x, y, z, U, V, W, nt, P = box(nx, ny, nz, 1)
+    path = tmp_path / "BL.00000042"
+    files.write_snapshot(path, 1.25, 1e-5, 42, x, y, z, U, V, W, nt, P)
+    t, nu, magic, step, mesh, fl = reader_one_process(path)
+    assert (t, nu, magic, step) == (1.25, 1e-5, -73, 42)
+    assert np.array_equal(mesh[0], x) and np.array_equal(mesh[1], y) and np.array_equal(mesh[2], z)
+    for m, f in zip(mesh[3:], (x, y, z)):
+        assert np.array_equal(m, 0.5 * (f[:-1] + f[1:]))  # initialization.f90:181-189
+    assert np.array_equal(fl[0], U[:, :, :-1]) and np.array_equal(fl[1], V[:, :, :-1])
+    assert np.array_equal(fl[2], W[:, :, :-1]) and np.array_equal(fl[3], nt[:, :, :-1])
+    assert np.array_equal(fl[4], P)
+    s = files.read_snapshot(path)
+    assert s["step"] == 42 and s["t"] == 1.25 and s["full_planes"] == 0 and s["has_nu_t_p"] == 1
+    assert np.array_equal(s["x"], x) and np.array_equal(s["y"], y) and np.array_equal(s["z"], z)
+    # the plane left out comes back as the z-periodic boundary pass sets it
+    for got, ref, face in ((s["U"], U, False), (s["V"], V, False), (s["W"], W, True), (s["nu_t"], nt, False)):
+        assert np.array_equal(got[:, :, :-1], ref[:, :, :-1])
+        assert np.array_equal(got[:, :, -1], ref[:, :, 1 if face else 2])
+    assert np.array_equal(s["P"], P)
+
+
+def write_full(path, t, nu, step, x, y, z, fields, magic=True, tail=True):
+    with open(path, "wb") as f:
+        f.write(struct.pack("dd", t, nu))
+        if magic:
+            f.write(struct.pack("ii", -73, step))
+        for a in (x, y, z, 0.5 * (x[:-1] + x[1:]), 0.5 * (y[:-1] + y[1:]), 0.5 * (z[:-1] + z[1:])):
+            f.write(struct.pack("i", len(a)) + np.asarray(a, "<f8").tobytes())
+        for a in (fields if tail else fields[:3]):
+            f.write(struct.pack("iii", *a.shape) + np.asarray(a, "<f8").tobytes(order="F"))
+
+
+def test_snapshot_full_layout_and_older_files(tmp_path):
+    nx, ny, nz = 8, 6, 7
+    x, y, z, U, V, W, nt, P = box(nx, ny, nz, 2)
+    path = tmp_path / "full"
+    write_full(path, 0.5, 2e-5, 7, x, y, z, [U, V, W, nt, P])
+    s = files.read_snapshot(path)
+    assert s["full_planes"] == 1 and s["step"] == 7
+    for k, a in zip(("U", "V", "W", "nu_t", "P"), (U, V, W, nt, P)):
+        assert np.array_equal(s[k], a)
+    # no magic number (older files) and no nu_t / P records
+    path2 = tmp_path / "old"
+    write_full(path2, 0.5, 2e-5, 0, x, y, z, [U, V, W, nt, P], magic=False, tail=False)
+    s2 = files.read_snapshot(path2)
+    assert s2["step"] == -1 and s2["has_nu_t_p"] == 0
+    assert np.array_equal(s2["U"], U) and not s2["P"].any() and not s2["nu_t"].any()
+
+
+def test_snapshot_errors(tmp_path):
+    nx, ny, nz = 8, 6, 7
+    x, y, z, U, V, W, nt, P = box(nx, ny, nz, 3)
+    path = tmp_path / "s"
+    files.write_snapshot(path, 0.0, 1e-5, 0, x, y, z, U, V, W, nt, P)
+    data = path.read_bytes()
+    (tmp_path / "cut").write_bytes(data[:-8])
+    with pytest.raises(BlgpuError, match="fit neither"):
+        files.read_snapshot(tmp_path / "cut")
+    with pytest.raises(BlgpuError, match="cannot open"):
+        files.read_snapshot(tmp_path / "none")
+
+
+def test_rescaling_means_either_byte_order(tmp_path):
+    rng = np.random.default_rng(4)
+    ny = 9
+    um, vm = rng.standard_normal(ny + 1), rng.standard_normal(ny)
+    files.write_rescaling(tmp_path / "m", um, vm)
+    raw = (tmp_path / "m").read_bytes()
+    assert raw == struct.pack("<i", ny + 1) + um.astype("<f8").tobytes() + vm.astype("<f8").tobytes()
+    a, b = files.read_rescaling(tmp_path / "m", ny)
+    assert np.array_equal(a, um) and np.array_equal(b, vm)
+    # big-endian, as read_input_data opens it (input_output.f90:445)
+    (tmp_path / "be").write_bytes(struct.pack(">i", ny + 1) + um.astype(">f8").tobytes() + vm.astype(">f8").tobytes())
+    a, b = files.read_rescaling(tmp_path / "be", ny)
+    assert np.array_equal(a, um) and np.array_equal(b, vm)
+    with pytest.raises(BlgpuError, match="nyg_resc"):
+        files.read_rescaling(tmp_path / "m", ny + 1)
+
+
+def test_snapshot_name():
+    assert files.snapshot_name("./data/BL", 500) == "./data/BL.00000500"
+    assert files.snapshot_name("  out/x ", 123456789) == "out/x.123456789"

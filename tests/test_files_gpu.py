@@ -1,0 +1,47 @@
+"""output_data / read_input_data for a context: a run restarted from its
+own snapshot continues as the uninterrupted run does, and the Lund means
+file carries the running means."""
+import os
+
+import numpy as np
+import pytest
+
+from blgpu import cases, files, FP64, MIXED
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_restart_continues_bit_identically(gpu, tmp_path, precision):
+    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=5, cfl=0.5)
+    a = cases.solver_for(c, precision=precision, inflow=False)
+    a.advance(3)
+    out = str(tmp_path / "data" / "BL")
+    a.output_data(out, 3)
+    name = files.snapshot_name(out, 3)
+    assert os.path.realpath(out + ".restart") == os.path.realpath(name)
+    b = cases.solver_for(c, precision=precision, inflow=False)
+    assert b.read_input_data(name) == 3
+    assert np.array_equal(b.x, c.x) and np.array_equal(b.y, c.y) and np.array_equal(b.z, c.z)
+    assert b.time()[0] == a.time()[0]
+    a.advance(2)
+    b.advance(2)
+    for p, q in zip(a.download_state()[:3], b.download_state()[:3]):
+        assert np.array_equal(p, q)
+    a.close()
+    b.close()
+
+
+def test_rescaling_means_file(gpu, tmp_path):
+    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=6, cfl=0.5)
+    a = cases.solver_for(c, precision=FP64)
+    a.advance(2)
+    out = str(tmp_path / "BL")
+    a.output_data(out, 2, rescaling=True)
+    um, vm = files.read_rescaling(files.snapshot_name(out, 2) + ".mean.rescaling", c.ny)
+    r = a.rescaling()
+    assert np.array_equal(um, r["Umean_resc"]) and np.array_equal(vm, r["Vmean_resc"])
+    s = files.read_snapshot(files.snapshot_name(out, 2))
+    U, V, W, P, t = a.download_state()
+    assert s["t"] == t and np.array_equal(s["U"][:, :, :-1], U[:, :, :-1]) and np.array_equal(s["P"], P)
+    a.close()
