@@ -1226,7 +1226,10 @@ int blgpu_eddy_viscosity(blgpu_ctx *ctx) {
 
 int blgpu_get_nu_t(blgpu_ctx *ctx, double *nu_t) {
   if (!ctx || !nu_t) return set_err(ctx, BLGPU_EINVAL, "blgpu_get_nu_t: null argument");
-  if (!ctx->nut) return set_err(ctx, BLGPU_ESTATE, "blgpu_get_nu_t: context created with LES=0");
+  if (!ctx->nut) {  // LES = 0: the reference's nu_t stays zero
+    memset(nu_t, 0, sizeof(double) * (size_t)ctx->nxg * ctx->nyg * ctx->nzg);
+    return BLGPU_OK;
+  }
   CK(cudaSetDevice(ctx->cfg.device));
   CK(cudaStreamSynchronize(ctx->st));
   int rc = download_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);

@@ -174,6 +174,7 @@ int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels
 /* sgs_Smagorinsky (subgrid.f90:609-730) on the resident state: nu_t on the
  * interior i=2..nxg-1, j=2..nyg-1, k=2..nzg-1 (Cs = 0.11, f = 1) */
 int blgpu_eddy_viscosity(blgpu_ctx *ctx);
+/* nu_t(nxg,nyg,nzg); zeros for a context created with LES = 0 */
 int blgpu_get_nu_t(blgpu_ctx *ctx, double *nu_t);
 
 /* compute_statistics (statistics.f90:26-201) on the device, FP64
