@@ -563,67 +563,119 @@ __global__ void k_thomas_factors(Spec s, double *__restrict__ piv, const double 
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, const double *__restrict__ piv,
-                                                const double *__restrict__ dl, const double *__restrict__ du,
-                                                double *__restrict__ H0, int klow) {
-  // lane pairs share a mode: even lane = real part, odd lane = imaginary part
-  const int lane = threadIdx.x & 31, part = lane & 1;
-  const int kx = blockIdx.x * 16 + (lane >> 1);
-  const int kz = blockIdx.y * 8 + (threadIdx.x >> 5);
-  if (kx >= s.N || kz >= s.MH) return;
-  const int NM = s.NM;
-  const long long rs = (long long)s.MH * s.rx;  // stride between rows b
-  const long long base = (long long)kz * s.rx + kx;
-  T *Cs = reinterpret_cast<T *>(C) + part;  // element a of this part at Cs[2a]
-  // mixed form: the low-kx modes of kz = 0 carry the box-scale pressure;
-  // they are solved with FP64 intermediates into H0[b][kx] (real part; the
-  // imaginary part of kz = 0 is zero) and dropped from the FP32 data
-  const bool hp = H0 && kz == 0 && kx < klow;
-  if (hp && part) {
-    for (int b = 0; b < NM; ++b) Cs[2 * (base + b * rs)] = (T)0;
-    return;
-  }
-  double *Hd = hp ? H0 + kx : nullptr;  // H0[b * klow + kx]
-  // forward sweep in batches of PF rows, next batch in flight meanwhile
-  constexpr int PF = 16;
-  double rprev = 0.0, g = 0.0;
-  T cur[PF], nxt[PF];
-  double pc[PF], pnx[PF];
+// One thread per complex mode (a CTA takes 128 consecutive kx of one kz, so
+// each row step reads 1 KB runs of C and of piv), both sweeps down the NM rows b with a ring of PF rows in flight:
+// row b+PF is requested when row b is consumed.  Rows are reached by
+// stepping one pointer into C and one into piv by the row stride.
+template <typename T, int PF>
+__device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const double *__restrict__ pm, long long rs,
+                                              int NM, const double *__restrict__ dl, const double *__restrict__ du) {
+  // forward: g_b = r_b - (l_b / d'_{b-1}) g_{b-1}, stored over r_b
+  T2<T> cr[PF];
+  double pr[PF];
+  const T2<T> *cn = Cm;
+  const double *pn = pm;
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
-    cur[u] = u < NM ? Cs[2 * (base + u * rs)] : (T)0;
-    pc[u] = u < NM ? piv[base + u * rs] : 0.0;
+    cr[u] = u < NM ? cn[0] : mk<T>((T)0, (T)0);
+    pr[u] = u < NM ? pn[0] : 0.0;
+    if (u < NM) { cn += rs; pn += rs; }
   }
+  double gx = 0.0, gy = 0.0, rprev = 0.0;
+  T2<T> *cw = Cm;
   for (int b0 = 0; b0 < NM; b0 += PF) {
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int bn = b0 + PF + u;
-      nxt[u] = bn < NM ? Cs[2 * (base + bn * rs)] : (T)0;
-      pnx[u] = bn < NM ? piv[base + bn * rs] : 0.0;
-    }
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int b = b0 + u;
       if (b < NM) {
-        double r = (double)cur[u];
+        const T2<T> cv = cr[u];
+        const double pv = pr[u];
+        if (b + PF < NM) {
+          cr[u] = cn[0];
+          pr[u] = pn[0];
+          cn += rs;
+          pn += rs;
+        }
+        double rx = (double)cv.x, ry = (double)cv.y;
         if (b > 0) {
           const double w = dl[b] * rprev;  // l_b / d'_{b-1}
-          r = r - w * g;
+          rx = rx - w * gx;
+          ry = ry - w * gy;
         }
-        rprev = pc[u];
-        g = r;
-        if (hp) Hd[(long long)b * klow] = r;
-        else Cs[2 * (base + b * rs)] = (T)r;
+        rprev = pv;
+        gx = rx;
+        gy = ry;
+        *cw = mk<T>((T)rx, (T)ry);
+        cw += rs;
       }
     }
+  }
+  // backward: x_b = (g_b - u_b x_{b+1}) / d'_b from the top row down
+  const int top = NM - 1;
+  const T2<T> *cb = Cm + (long long)top * rs;
+  const double *pb = pm + (long long)top * rs;
+#pragma unroll
+  for (int u = 0; u < PF; ++u) {
+    cr[u] = u < NM ? cb[0] : mk<T>((T)0, (T)0);
+    pr[u] = u < NM ? pb[0] : 0.0;
+    if (u < NM) { cb -= rs; pb -= rs; }
+  }
+  double xx = 0.0, xy = 0.0;
+  cw = Cm + (long long)top * rs;
+  for (int b0 = top; b0 >= 0; b0 -= PF) {
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
-      cur[u] = nxt[u];
-      pc[u] = pnx[u];
+      const int b = b0 - u;
+      if (b >= 0) {
+        const T2<T> cv = cr[u];
+        const double pv = pr[u];
+        if (b - PF >= 0) {
+          cr[u] = cb[0];
+          pr[u] = pb[0];
+          cb -= rs;
+          pb -= rs;
+        }
+        if (b == top) {
+          xx = (double)cv.x * pv;
+          xy = (double)cv.y * pv;
+        } else {
+          xx = ((double)cv.x - du[b] * xx) * pv;
+          xy = ((double)cv.y - du[b] * xy) * pv;
+        }
+        *cw = mk<T>((T)xx, (T)xy);
+        cw -= rs;
+      }
     }
   }
-  if (hp) {  // FP64 backward sweep of the kz = 0, low-kx modes
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, const double *__restrict__ piv,
+                                                const double *__restrict__ dl, const double *__restrict__ du,
+                                                double *__restrict__ H0, int klow) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kz = blockIdx.y;
+  if (kx >= s.N || kz >= s.MH) return;
+  const int NM = s.NM;
+  const long long rs = (long long)s.MH * s.rx;  // stride between rows b
+  const long long base = (long long)kz * s.rx + kx;
+  // mixed form: the low-kx modes of kz = 0 carry the box-scale pressure;
+  // they are solved with FP64 intermediates into H0[b][kx] (real part; the
+  // imaginary part of kz = 0 is zero) and dropped from the FP32 data
+  if (H0 && kz == 0 && kx < klow) {
+    const T *Cr = reinterpret_cast<const T *>(C + base);  // real part of row b at Cr[2 b rs]
+    double *Hd = H0 + kx;                                   // H0[b * klow + kx]
+    double g = 0.0, rprev = 0.0;
+    for (int b = 0; b < NM; ++b) {
+      double r = (double)Cr[2 * (long long)b * rs];
+      if (b > 0) {
+        const double w = dl[b] * rprev;
+        r = r - w * g;
+      }
+      rprev = piv[base + b * rs];
+      g = r;
+      Hd[(long long)b * klow] = r;
+    }
     double x = 0.0;
     constexpr int PB = 8;
     for (int b0 = NM - 1; b0 >= 0; b0 -= PB) {
@@ -643,40 +695,10 @@ __global__ void __launch_bounds__(256) k_thomas(Spec s, T2<T> *__restrict__ C, c
         }
       }
     }
-    for (int b = 0; b < NM; ++b) Cs[2 * (base + b * rs)] = (T)0;
+    for (int b = 0; b < NM; ++b) C[base + b * rs] = mk<T>((T)0, (T)0);
     return;
   }
-  // backward sweep, batches of PF rows from the top down
-  double x = 0.0;
-  double pv[PF], pn[PF];
-  const int top = NM - 1;
-#pragma unroll
-  for (int u = 0; u < PF; ++u) {
-    const int b = top - u;
-    cur[u] = b >= 0 ? Cs[2 * (base + b * rs)] : (T)0;
-    pv[u] = b >= 0 ? piv[base + b * rs] : 0.0;
-  }
-  for (int b0 = top; b0 >= 0; b0 -= PF) {
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int bn = b0 - PF - u;
-      nxt[u] = bn >= 0 ? Cs[2 * (base + bn * rs)] : (T)0;
-      pn[u] = bn >= 0 ? piv[base + bn * rs] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      const int b = b0 - u;
-      if (b >= 0) {
-        x = (b == top) ? (double)cur[u] * pv[u] : ((double)cur[u] - du[b] * x) * pv[u];
-        Cs[2 * (base + b * rs)] = (T)x;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      cur[u] = nxt[u];
-      pv[u] = pn[u];
-    }
-  }
+  thomas_sweeps<T, (sizeof(T) == 4 ? 12 : 16)>(C + base, piv + base, rs, NM, dl, du);
 }
 
 // ---------------------------------------------------------------------------
@@ -854,8 +876,8 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 template <typename T>
 void launch_thomas(const Spec &s, T2<T> *C, const double *piv, const double *dl, const double *du, double *H0,
                    int klow, cudaStream_t st) {
-  dim3 grid((s.N + 15) / 16, (s.MH + 7) / 8);
-  k_thomas<T><<<grid, 256, 0, st>>>(s, C, piv, dl, du, H0, klow);
+  dim3 grid((s.N + 127) / 128, s.MH);  // 128 kx of one kz per CTA
+  k_thomas<T><<<grid, 128, 0, st>>>(s, C, piv, dl, du, H0, klow);
 }
 
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("precision", [FP64, MIXED])
 def test_restart_continues_bit_identically(gpu, tmp_path, precision):
-    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=5, cfl=0.5)
+    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=5, cfl=-0.01)
     a = cases.solver_for(c, precision=precision, inflow=False)
     a.advance(3)
     out = str(tmp_path / "data" / "BL")
@@ -33,7 +33,7 @@ def test_restart_continues_bit_identically(gpu, tmp_path, precision):
 
 
 def test_rescaling_means_file(gpu, tmp_path):
-    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=6, cfl=0.5)
+    c = cases.turbulent_case(nx=66, ny=33, nz=20, lx=8.0, ly=2.0, lz=3.0, seed=6, cfl=-0.01)
     a = cases.solver_for(c, precision=FP64)
     a.advance(2)
     out = str(tmp_path / "BL")
