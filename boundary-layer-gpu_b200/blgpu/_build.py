@@ -28,6 +28,7 @@ SOURCES = {
     "capi_mlp.cu": [],
     "zdft_tc.cu": [],
     "snapshot.cpp": [],
+    "thomas_tma.cu": [],
 }
 
 

@@ -61,6 +61,8 @@ struct blgpu_ctx {
   int klow = 0;
   uint32_t *zfrag = nullptr;  // mixed form: table fragments of the tensor-core z transforms (or null)
   ZdftMaps zmaps{};           // and the TMA maps of R and C they read and write
+  ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
+  bool have_tmaps = false;
   int nsm = 148;
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
@@ -169,11 +171,13 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 }
 
 // the sticky device flag of the step kernels (stream already synchronized);
-// bit 2: a TMA copy of the tensor-core z transform missed its wait limit
+// bit 2: a TMA copy of the tensor-core z transform missed its wait limit;
+// bit 4: one of the tiled y-solve
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
   if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
+  if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
   if (f) return set_err(ctx, BLGPU_EDEVICE, "device flag %d set by a step kernel", f);
   return BLGPU_OK;
 }
@@ -253,6 +257,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, &ctx->R, (size_t)s.NM * s.M * s.rx * ctx->esz));
   TRY(dalloc(ctx, &ctx->C, (size_t)s.NM * s.MH * s.rx * ctx->esz * 2));
   TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
+  ctx->have_tmaps = ctx->fp64 ? thomas_maps<double>(s, ctx->C, ctx->piv, &ctx->tmaps)
+                              : thomas_maps<float>(s, ctx->C, ctx->piv, &ctx->tmaps);
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
   if (!ctx->fp64 && zdft_tc_qp(s)) {
     std::vector<uint32_t> fr;
@@ -859,8 +865,13 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
-  launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
-                   ctx->st);
+  const bool tiled = ctx->have_tmaps && (ctx->tiles.thomas == 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
+  if (tiled)
+    launch_thomas_tile<T>(s, ctx->tmaps, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
+                          &ctx->sc->err, ctx->st);
+  else
+    launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
+                     ctx->st);
   if (mixed)  // the box-scale pressure (kz = 0, kx < klow) in FP64
     launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
   ph_end(ctx, mixed ? 3 : 1);
@@ -1421,6 +1432,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   if (t.dct_nw < 0 || t.dct_nw > 8) return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d outside 0..8", t.dct_nw);
   if (t.zdft != 0 && t.zdft != 1) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
+  if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
   if (t.dct_nw > 0) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
@@ -1490,9 +1502,9 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 7 values");
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 8 values");
   Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft,
-          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts};
+          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts, n >= 8 ? tiles[7] : ctx->tiles.thomas};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1512,6 +1524,7 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   tiles[4] = t.proj_by;
   if (n >= 6) tiles[5] = t.zdft;
   if (n >= 7) tiles[6] = t.rhs_pts;
+  if (n >= 8) tiles[7] = t.thomas;
   return BLGPU_OK;
 }
 
@@ -1531,7 +1544,8 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {4, 8},                                                                  // dftz_rk
       {4, 8},                                                                  // proj_by
       {0, 1},                                                                  // zdft
-      {1, 2}};                                                                 // rhs_pts
+      {1, 2},                                                                  // rhs_pts
+      {1, 2}};                                                                 // thomas
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1548,12 +1562,13 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 7 && !rc; ++knob) {  // one pass of coordinate descent
+  for (int knob = 0; knob < 8 && !rc; ++knob) {  // one pass of coordinate descent
     if (knob == 5 && !ctx->zfrag) continue;        // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
+    if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[7] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts};
+      int *f[8] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

@@ -25,6 +25,7 @@ struct Tiles {
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed form z transforms: 0 tensor cores where the order is served, 1 FP32 direct sums
   int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
+  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)
@@ -138,6 +139,19 @@ bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
 // flag, bit 2 set when a TMA copy did not complete within the wait limit
 void launch_zdft_tc(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *frag, int inverse,
                     int nsm, int *err, cudaStream_t st);
+// ---- thomas_tma.cu: the y-solve as one TMA-fed pass over tiles ----
+struct ThomasMaps {  // CUtensorMap bytes of C and of the pivots
+  alignas(64) unsigned char c[128];
+  alignas(64) unsigned char p[128];
+};
+// false when the maps cannot be encoded or NM > 256 (the register-ring
+// k_thomas then serves the box)
+template <typename T>
+bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out);
+// err: device flag, bit 4 set when a tile copy missed its wait limit
+template <typename T>
+void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
+                        int klow, int *err, cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);

@@ -21,24 +21,22 @@
 // products of item i.  The CTA then splits the operands into shared memory,
 // each warp multiplies one 16-row tile of the cos or the sin table by all of
 // them, and the results leave through shared memory as coalesced rows.
-#include <cuda.h>
-#include <cuda_runtime.h>
-#include <cudaTypedefs.h>
-
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace blgpu {
+
+using namespace tma;
 
 static_assert(sizeof(CUtensorMap) == sizeof(ZdftMaps::r), "tensor map size");
 
 namespace {
 constexpr int ZNT = 64;              // kx columns per work item
 constexpr int ZLD = ZNT + 8;         // row pitch of the staged operands (conflict-free fragment loads)
-constexpr int WAIT_LIMIT = 1 << 24;  // mbarrier polls (with back-off) before a copy counts as lost
 
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
   uint32_t r;
@@ -60,41 +58,6 @@ __device__ __forceinline__ void split(float x, uint32_t &hi, uint32_t &lo) {
   lo = tf32_rna(x - __uint_as_float(hi));
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait for phase `parity` of an mbarrier; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < WAIT_LIMIT; ++it) {
-    if (mbar_test(bar, parity)) return true;
-    if (it >= 32) __nanosleep(64);
-  }
-  return false;
-}
-// 2D tiled TMA load of one box into shared memory, completing on `bar`
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
 }  // namespace
 
 // Table fragments, in the order the kernel reads them: for table t (0 cos,
@@ -130,12 +93,12 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1)
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_init_fence();
     if ((int)blockIdx.x < nitems) {
       const int b = blockIdx.x / ntile, kx0 = (blockIdx.x % ntile) * ZNT;
       mbar_expect_tx(&bar[0], box_bytes);
-      if (inverse) tma_load_2d(raw0, &mapC, 2 * kx0, b * MH, &bar[0]);
-      else tma_load_2d(raw0, &mapR, kx0, b * M, &bar[0]);
+      if (inverse) load_2d(raw0, &mapC, 2 * kx0, b * MH, &bar[0]);
+      else load_2d(raw0, &mapR, kx0, b * M, &bar[0]);
     }
   }
   // the warp's table fragments, resident for the whole kernel
@@ -160,10 +123,10 @@ __global__ void __launch_bounds__(QP / 8 * 32, 1)
     if (threadIdx.x == 0 && next < nitems) {
       const int nb = next / ntile, nk0 = (next % ntile) * ZNT;
       float *dst = raw0 + (size_t)(buf ^ 1) * rawf;
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic reads before the async write
+      fence_async_shared();  // generic reads before the async write
       mbar_expect_tx(&bar[buf ^ 1], box_bytes);
-      if (inverse) tma_load_2d(dst, &mapC, 2 * nk0, nb * MH, &bar[buf ^ 1]);
-      else tma_load_2d(dst, &mapR, nk0, nb * M, &bar[buf ^ 1]);
+      if (inverse) load_2d(dst, &mapC, 2 * nk0, nb * MH, &bar[buf ^ 1]);
+      else load_2d(dst, &mapR, nk0, nb * M, &bar[buf ^ 1]);
     }
     const bool ok = mbar_wait(&bar[buf], (uint32_t)(i >> 1) & 1u);
     if (__syncthreads_or(!ok)) {
@@ -303,32 +266,15 @@ int zdft_tc_qp(const Spec &s) {
 // (2 rx x NM*MH, box 128 x MH); false when the driver entry point or the
 // encoding is unavailable (the caller then keeps the direct sums).
 bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out) {
-  static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
-  if (!enc) {
-    void *fn = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-      return false;
-    enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  }
-  if ((reinterpret_cast<uintptr_t>(R) & 15) || (reinterpret_cast<uintptr_t>(C) & 15)) return false;
   CUtensorMap mr, mc;
-  const cuuint32_t es[2] = {1, 1};
   const cuuint64_t dr[2] = {(cuuint64_t)s.rx, (cuuint64_t)s.NM * s.M};
   const cuuint64_t sr[1] = {(cuuint64_t)s.rx * sizeof(float)};
   const cuuint32_t br[2] = {(cuuint32_t)ZNT, (cuuint32_t)s.M};
-  if (enc(&mr, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, R, dr, sr, br, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-      CUDA_SUCCESS)
-    return false;
+  if (!encode(&mr, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, R, dr, sr, br)) return false;
   const cuuint64_t dc[2] = {(cuuint64_t)2 * s.rx, (cuuint64_t)s.NM * s.MH};
   const cuuint64_t sc[1] = {(cuuint64_t)2 * s.rx * sizeof(float)};
   const cuuint32_t bc[2] = {(cuuint32_t)(2 * ZNT), (cuuint32_t)s.MH};
-  if (enc(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dc, sc, bc, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-      CUDA_SUCCESS)
-    return false;
+  if (!encode(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dc, sc, bc)) return false;
   memcpy(out->r, &mr, sizeof mr);
   memcpy(out->c, &mc, sizeof mc);
   return true;
