@@ -260,6 +260,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   ctx->have_tmaps = ctx->fp64 ? thomas_maps<double>(s, ctx->C, ctx->piv, &ctx->tmaps)
                               : thomas_maps<float>(s, ctx->C, ctx->piv, &ctx->tmaps);
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
+  TRY(upload_dft_constants() == 0 ? BLGPU_OK : set_err(ctx, BLGPU_ECUDA, "DFT constants upload failed"));
   if (!ctx->fp64 && zdft_tc_qp(s)) {
     std::vector<uint32_t> fr;
     zdft_tc_fragments(s, fr);
@@ -363,7 +364,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
     ctx->pl64.post = (const double2 *)ctx->post;
     ctx->pl32.tw = (const float2 *)ctx->tw;
     ctx->pl32.post = (const float2 *)ctx->post;
-    const size_t sm = dct_smem_bytes(N, (int)ctx->esz, dct_lines_per_cta(N, (int)ctx->esz));
+    const size_t sm = dct_smem_bytes(N, (int)ctx->esz, 1);  // one line per CTA at the least
     int dev_sm = 0;
     cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg->device);
     if ((long long)sm > dev_sm) TRY(set_err(ctx, BLGPU_EINVAL, "nx=%d needs %zu B shared memory per CTA", ctx->nx, sm));
@@ -880,7 +881,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
-  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.dct_nw, ctx->st);
+  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->st);
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
@@ -1429,17 +1430,22 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
     return set_err(ctx, BLGPU_EINVAL, "tiles: proj_by %d not in {1,2,4,8}", t.proj_by);
   if (t.dftz_rk != 0 && t.dftz_rk != 4 && t.dftz_rk != 8)
     return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
-  if (t.dct_nw < 0 || t.dct_nw > 8) return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d outside 0..8", t.dct_nw);
+  const int maxnw = dct_max_lines((int)ctx->esz);
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
+  for (int q = 0; q < 2; ++q) {
+    const int nw = q ? t.idct_nw : t.dct_nw;
+    const char *name = q ? "idct_nw" : "dct_nw";
+    if (nw < 0 || nw > maxnw) return set_err(ctx, BLGPU_EINVAL, "tiles: %s %d outside 0..%d", name, nw, maxnw);
+    if (nw > 0) {
+      const size_t sm = dct_smem_bytes(ctx->spec.N, (int)ctx->esz, nw);
+      if (sm > (size_t)optin)
+        return set_err(ctx, BLGPU_EINVAL, "tiles: %s %d needs %zu B of shared memory (> %d)", name, nw, sm, optin);
+    }
+  }
   if (t.zdft != 0 && t.zdft != 1) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
   if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
-  if (t.dct_nw > 0) {
-    int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
-    const size_t sm = dct_smem_bytes(ctx->spec.N, (int)ctx->esz, t.dct_nw);
-    if (sm > (size_t)optin)
-      return set_err(ctx, BLGPU_EINVAL, "tiles: dct_nw %d needs %zu B of shared memory (> %d)", t.dct_nw, sm, optin);
-  }
   return BLGPU_OK;
 }
 
@@ -1502,9 +1508,10 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 8 values");
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 9 values");
   Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft,
-          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts, n >= 8 ? tiles[7] : ctx->tiles.thomas};
+          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts, n >= 8 ? tiles[7] : ctx->tiles.thomas,
+          n >= 9 ? tiles[8] : ctx->tiles.idct_nw};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1525,6 +1532,7 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   if (n >= 6) tiles[5] = t.zdft;
   if (n >= 7) tiles[6] = t.rhs_pts;
   if (n >= 8) tiles[7] = t.thomas;
+  if (n >= 9) tiles[8] = t.idct_nw;
   return BLGPU_OK;
 }
 
@@ -1540,12 +1548,13 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   std::vector<std::vector<int>> cand = {
       window ? std::vector<int>{8, 16, 32, 64} : std::vector<int>{4, 8, 16},  // rhs_kc
       {4, 8},                                                                  // rhs_by
-      {0, 1, 2, 3, 4, 6},                                                      // dct_nw
+      {0, 2, 4, 6, 8, 12, 16},                                                 // dct_nw
       {4, 8},                                                                  // dftz_rk
       {4, 8},                                                                  // proj_by
       {0, 1},                                                                  // zdft
       {1, 2},                                                                  // rhs_pts
-      {1, 2}};                                                                 // thomas
+      {1, 2},                                                                  // thomas
+      {0, 4, 8, 12, 16}};                                                      // idct_nw
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1562,13 +1571,14 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 8 && !rc; ++knob) {  // one pass of coordinate descent
+  for (int knob = 0; knob < 9 && !rc; ++knob) {  // one pass of coordinate descent
     if (knob == 5 && !ctx->zfrag) continue;        // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[8] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas};
+      int *f[9] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,
+                   &t.idct_nw};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

@@ -20,12 +20,13 @@ template <typename T> struct MetT {
 struct Tiles {
   int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8; FP32 DNS 8 for two points, 32 for one)
   int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
-  int dct_nw;   // complex lines (warps) per CTA of the DCT kernels (0: sized from shared memory)
+  int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 and 8 in FP64 (0: built-in)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed form z transforms: 0 tensor cores where the order is served, 1 FP32 direct sums
   int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
+  int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)
@@ -158,6 +159,9 @@ void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const d
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, cudaStream_t st);
 size_t dct_smem_bytes(int n, int elem_bytes, int lines);
-int dct_lines_per_cta(int n, int elem_bytes);
+// the R-point DFT constants of the odd register butterflies (once per device)
+int upload_dft_constants();
+int dct_lines_per_cta(int n, int elem_bytes, bool inverse);
+int dct_max_lines(int elem_bytes);  // launch bound of the DCT kernels, in warps
 
 }  // namespace blgpu

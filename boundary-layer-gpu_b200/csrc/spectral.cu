@@ -87,6 +87,36 @@ __device__ __forceinline__ void bf3(const T2<T> *in, T2<T> *out, int jj, int nb,
   out[idxD + 2 * Ns] = sub<T>(m, it);
 }
 
+// R-point DFT constants (cos, sin)(2 pi m / R), m = 0..R-1, of the odd
+// register radices, in constant memory so that the butterflies take them as
+// instruction operands instead of holding them in registers
+constexpr int DFT_RSUM = 5 + 7 + 11 + 13 + 17 + 19 + 23 + 29 + 31;
+__constant__ double2 c_dft64[DFT_RSUM];
+__constant__ float2 c_dft32[DFT_RSUM];
+template <int R> __host__ __device__ constexpr int dft_off() {
+  return R == 5 ? 0 : R == 7 ? 5 : R == 11 ? 12 : R == 13 ? 23 : R == 17 ? 36 : R == 19 ? 53 : R == 23 ? 72
+       : R == 29 ? 95 : 124;
+}
+template <typename T> __device__ __forceinline__ const T2<T> *dft_consts();
+template <> __device__ __forceinline__ const double2 *dft_consts<double>() { return c_dft64; }
+template <> __device__ __forceinline__ const float2 *dft_consts<float>() { return c_dft32; }
+
+int upload_dft_constants() {
+  const int rad[9] = {5, 7, 11, 13, 17, 19, 23, 29, 31};
+  double2 h64[DFT_RSUM];
+  float2 h32[DFT_RSUM];
+  int o = 0;
+  for (int r : rad)
+    for (int m = 0; m < r; ++m, ++o) {
+      const double a = 2.0 * M_PI * (double)m / (double)r;
+      h64[o] = make_double2(cos(a), sin(a));
+      h32[o] = make_float2((float)cos(a), (float)sin(a));
+    }
+  if (cudaMemcpyToSymbol(c_dft64, h64, sizeof h64) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_dft32, h32, sizeof h32) != cudaSuccess) return -1;
+  return 0;
+}
+
 // odd radix R (5..31) in registers, pairing inputs q and R-q
 template <int R, typename T, bool INV>
 __device__ __forceinline__ void bf_odd(const T2<T> *in, T2<T> *out, int jj, int nb, int tstep, int idxD, int Ns,
@@ -105,12 +135,17 @@ __device__ __forceinline__ void bf_odd(const T2<T> *in, T2<T> *out, int jj, int 
     s[q - 1] = add<T>(a, b);
     d[q - 1] = sub<T>(a, b);
   }
+  // (cos, sin)(2 pi m / R): FP32 reads them from constant memory as operands;
+  // FP64 keeps the half table in registers (taken from the twiddles)
+  const T2<T> *K = dft_consts<T>() + dft_off<R>();
   T cs[H], sn[H];
+  if constexpr (sizeof(T) == 8) {
 #pragma unroll
-  for (int q = 1; q <= H; ++q) {
-    T2<T> w = tw[q * stride];
-    cs[q - 1] = w.x;
-    sn[q - 1] = -w.y;  // sin(2 pi q / R)
+    for (int q = 1; q <= H; ++q) {
+      const T2<T> w = tw[q * stride];
+      cs[q - 1] = w.x;
+      sn[q - 1] = -w.y;  // sin(2 pi q / R)
+    }
   }
   T2<T> y0 = x0;
 #pragma unroll
@@ -122,8 +157,14 @@ __device__ __forceinline__ void bf_odd(const T2<T> *in, T2<T> *out, int jj, int 
 #pragma unroll
     for (int q = 1; q <= H; ++q) {
       const int m = (q * k) % R;
-      const T c = (m <= H) ? cs[m - 1] : cs[R - m - 1];
-      const T sv = (m <= H) ? sn[m - 1] : -sn[R - m - 1];
+      T c, sv;
+      if constexpr (sizeof(T) == 4) {
+        c = K[m].x;
+        sv = K[m].y;
+      } else {
+        c = (m <= H) ? cs[m - 1] : cs[R - m - 1];
+        sv = (m <= H) ? sn[m - 1] : -sn[R - m - 1];
+      }
       ax += s[q - 1].x * c;
       ay += s[q - 1].y * c;
       bx += d[q - 1].x * sv;
@@ -233,8 +274,12 @@ __device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const
          dq(__ldg(W + c) - __ldg(W + c - g.plane), g.az.F[k], g.az.rF[k]);
 }
 
+// FP32 CTAs take up to 16 lines (one CTA fills an SM's shared memory); the
+// FP64 kernels need more registers per thread and stop at 8
+template <typename T> struct DctCta { static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256; };
+
 template <typename T, int MAXR>
-__global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
+__global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
                                                  const T *__restrict__ V, const T *__restrict__ W,
                                                  T *__restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,7 +345,7 @@ __global__ void __launch_bounds__(256) k_div_dct(Geo g, Spec s, FftPlan<T> pl, c
 // rhs_p(2:nxg-1,:,nzp+2) = rhs_p(2:nxg-1,:,2)); one complex line per warp.
 // ---------------------------------------------------------------------------
 template <typename T, int MAXR>
-__global__ void __launch_bounds__(256) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
+__global__ void __launch_bounds__(DctCta<T>::max_threads) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
                                               T *__restrict__ p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = s.N;
@@ -771,16 +816,22 @@ __global__ void k_kz0_grad(Spec s, const double *__restrict__ p0, float *__restr
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-int dct_lines_per_cta(int n, int elem_bytes) {
-  // warps (complex lines) per CTA: two CTAs per SM within 113 KB each
+int dct_lines_per_cta(int n, int elem_bytes, bool inverse) {
+  // warps (complex lines) per CTA, as measured at 814 x 257 x 193: the FP32
+  // inverse fills one SM's shared memory with up to 16 lines, the FP32
+  // forward (its divergence loads want more CTAs in flight) takes three CTAs
+  // of up to 4 lines per SM, FP64 (register-limited) two CTAs within 113 KB
   const size_t line = (size_t)n * 2 * elem_bytes * 2;  // ping-pong buffers of one complex line
   const size_t fixed = (size_t)n * 2 * elem_bytes * 2; // twiddle + DCT tables
-  const size_t budget = 113 * 1024;
+  const size_t budget = elem_bytes == 8 ? 113 * 1024 : inverse ? 226 * 1024 : 75 * 1024;
+  const int cap = elem_bytes == 8 ? 6 : inverse ? 16 : 4;
   int w = (int)((budget > fixed ? budget - fixed : 0) / line);
   if (w < 1) w = 1;
-  if (w > 6) w = 6;
+  if (w > cap) w = cap;
   return w;
 }
+
+int dct_max_lines(int elem_bytes) { return elem_bytes == 4 ? 16 : 8; }
 
 size_t dct_smem_bytes(int n, int elem_bytes, int warps) {
   return (size_t)n * 2 * elem_bytes * (2 + 2 * (size_t)warps);
@@ -820,7 +871,7 @@ static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, c
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
                     int nw_req, cudaStream_t st) {
-  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T));
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
   const int grid = (ncl + nw - 1) / nw;
@@ -835,7 +886,7 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
 
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, cudaStream_t st) {
-  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T));
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;

@@ -69,8 +69,9 @@ def test_tiles_do_not_change_results(gpu, precision):
     s0.advance(3)
     kc = 16 if precision == MIXED else 4
     s1 = cases.solver_for(c, precision=precision)
-    s1.set_tiles(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4)
-    assert s1.tiles() == dict(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4, zdft=0, rhs_pts=0, thomas=0)
+    s1.set_tiles(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4, idct_nw=3)
+    assert s1.tiles() == dict(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4, zdft=0, rhs_pts=0, thomas=0,
+                              idct_nw=3)
     s1.advance(3)
     assert same(states([s0]), states([s1]))
 
