@@ -57,6 +57,7 @@ FP64 = 0
 MIXED = 1
 POISSON_NATIVE = 0
 POISSON_CUFFT = 1
+LES_HOST = -1  # les_model: eddy viscosity supplied by the host
 
 _SIGS = {
     "blgpu_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),

@@ -216,6 +216,13 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
                    cfg->nx, cfg->ny, cfg->nz);
   if (cfg->rk_scheme < 1 || cfg->rk_scheme > 3)
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: RKscheme %d not in {1,2,3}", cfg->rk_scheme);
+  // LES as in compute_eddy_viscosity (subgrid.f90:23-47): 0 none, 1 constant-coefficient
+  // Smagorinsky; 2 and 3 (dynamic Smagorinsky) are not built; BLGPU_LES_HOST: nu_t from the host
+  if (cfg->les_model == 2 || cfg->les_model == 3)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: LES=%d (dynamic Smagorinsky, subgrid.f90:261-583) is not built",
+                   cfg->les_model);
+  if (cfg->les_model != 0 && cfg->les_model != 1 && cfg->les_model != BLGPU_LES_HOST)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown LES model %d", cfg->les_model);
   if (cfg->precision != BLGPU_FP64 && cfg->precision != BLGPU_MIXED)
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown precision %d", cfg->precision);
   if (cfg->poisson != BLGPU_POISSON_NATIVE)

@@ -36,6 +36,8 @@ extern "C" {
 #define BLGPU_FP64 0   /* bit-faithful FP64 form */
 #define BLGPU_MIXED 1  /* FP32 fields/RHS/transforms, FP64 Thomas and mean mode */
 
+#define BLGPU_LES_HOST (-1)  /* les_model: nu_t supplied by the host (blgpu_set_nu_t) */
+
 #define BLGPU_POISSON_NATIVE 0  /* hand-written DCT/DFT/Thomas kernels */
 #define BLGPU_POISSON_CUFFT 1   /* cuFFT comparison path (FP64 only) */
 
@@ -49,8 +51,9 @@ typedef struct blgpu_config {
   double dpdx, dpdz;  /* dPdx, dPdz (params.f90:152-153) */
   int rk_scheme;      /* RKscheme: 1 Euler, 2 RK2, 3 RK3 (params.f90:195) */
   int les_model;      /* LES: 0 DNS; 1 constant-coefficient Smagorinsky computed on the device
-                         before every substep (subgrid.f90:609-730); 2 eddy viscosity given
-                         by blgpu_set_nu_t and held fixed */
+                         before every substep (subgrid.f90:609-730); BLGPU_LES_HOST: eddy
+                         viscosity given by blgpu_set_nu_t and held fixed.  The reference's
+                         2 and 3 (dynamic Smagorinsky) are refused with BLGPU_EINVAL */
   int precision;      /* BLGPU_FP64 | BLGPU_MIXED */
   int poisson;        /* BLGPU_POISSON_NATIVE | BLGPU_POISSON_CUFFT */
   int device;         /* CUDA device ordinal */
@@ -108,7 +111,7 @@ int blgpu_rescaled_inflow(blgpu_ctx *ctx);
 int blgpu_get_rescaling(blgpu_ctx *ctx, double *Umean_resc, double *Vmean_resc, double *Umean_inlet,
                         double *Vmean_inlet, double *Lu, double *Lv, double *Lw, double *diag, int *err);
 
-/* eddy viscosity nu_t(nxg,nyg,nzg) supplied by the host (LES = 2) */
+/* eddy viscosity nu_t(nxg,nyg,nzg) supplied by the host (les_model = BLGPU_LES_HOST) */
 int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t);
 
 /* box sizes and viscosity of a context; the face grids given to set_grid */

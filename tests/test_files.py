@@ -196,3 +196,10 @@ def test_rescaling_means_either_byte_order(tmp_path):
 def test_snapshot_name():
     assert files.snapshot_name("./data/BL", 500) == "./data/BL.00000500"
     assert files.snapshot_name("  out/x ", 123456789) == "out/x.123456789"
+
+
+def test_params_les_flag_maps_to_config(tmp_path):
+    """The .turbb LES flag goes to blgpu_config.les_model unchanged; the
+    dynamic models (2, 3) are then refused by blgpu_create (not built)."""
+    p = files.read_params(write_turbb(tmp_path / "l.turbb", "inflow_file = a\nLES = 2\n"))
+    assert p["LES"] == 2 and p["config"]["les_model"] == 2

@@ -45,3 +45,12 @@ def test_rescaling_means_file(gpu, tmp_path):
     U, V, W, P, t = a.download_state()
     assert s["t"] == t and np.array_equal(s["U"][:, :, :-1], U[:, :, :-1]) and np.array_equal(s["P"], P)
     a.close()
+
+
+def test_dynamic_les_models_refused(gpu):
+    """LES = 2, 3 (dynamic Smagorinsky) are not built: blgpu_create says so
+    instead of running another model."""
+    from blgpu import Solver, BlgpuError
+    for les in (2, 3):
+        with pytest.raises(BlgpuError, match="dynamic Smagorinsky"):
+            Solver(34, 17, 12, 1e-3, -0.01, les_model=les)
