@@ -27,6 +27,7 @@ SOURCES = {
     "mlp.cu": [],
     "capi_mlp.cu": [],
     "zdft_tc.cu": [],
+    "zdft_umma.cu": [],
     "snapshot.cpp": [],
     "thomas_tma.cu": [],
 }

@@ -61,6 +61,8 @@ struct blgpu_ctx {
   int klow = 0;
   uint32_t *zfrag = nullptr;  // mixed form: table fragments of the tensor-core z transforms (or null)
   ZdftMaps zmaps{};           // and the TMA maps of R and C they read and write
+  uint32_t *utab = nullptr;   // mixed form: tcgen05 z transforms, tables (or null)
+  ZdftMaps umaps{};           // and their TMA maps
   ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
   bool have_tmaps = false;
   int nsm = 148;
@@ -172,12 +174,13 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 
 // the sticky device flag of the step kernels (stream already synchronized);
 // bit 2: a TMA copy of the tensor-core z transform missed its wait limit;
-// bit 4: one of the tiled y-solve
+// bit 4: one of the tiled y-solve; bit 8: one of the tcgen05 z transform
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
   if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
   if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
+  if (f & 8) return set_err(ctx, BLGPU_EDEVICE, "z transform (tcgen05): a copy or a product missed its wait limit");
   if (f) return set_err(ctx, BLGPU_EDEVICE, "device flag %d set by a step kernel", f);
   return BLGPU_OK;
 }
@@ -276,6 +279,14 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
                    "z-transform tables"));
     // without tensor maps the direct sums serve this box
     if (!zdft_tc_maps(s, (float *)ctx->R, (float2 *)ctx->C, &ctx->zmaps)) ctx->zfrag = nullptr;
+  }
+  if (!ctx->fp64 && zdft_umma_qp(s)) {
+    std::vector<uint32_t> ut;
+    zdft_umma_tables(s, ut);
+    TRY(dalloc(ctx, (void **)&ctx->utab, ut.size() * sizeof(uint32_t)));
+    TRY(check_cuda(ctx, cudaMemcpy(ctx->utab, ut.data(), ut.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                   "tcgen05 z-transform tables"));
+    if (!zdft_umma_maps(s, (float *)ctx->R, (float2 *)ctx->C, &ctx->umaps)) ctx->utab = nullptr;
   }
   if (!ctx->fp64) {
     // the modes kx < klow of kz = 0 carry the box-scale pressure of a step's
@@ -866,9 +877,13 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_begin(ctx, PH_DIVDCT);
   launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->st);
   ph_end(ctx, 1);
-  const bool tc = mixed && ctx->zfrag && ctx->tiles.zdft == 0;
+  // z transforms: tcgen05 (zdft 0 or 3), mma.sync TF32 (0 without tcgen05, or 2), FP32/FP64 sums (1)
+  const int zd = ctx->tiles.zdft;
+  const bool um = mixed && ctx->utab && (zd == 0 || zd == 3);
+  const bool tc = mixed && !um && ctx->zfrag && (zd == 0 || zd == 2);
   ph_begin(ctx, PH_DFTZ);
-  if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, &ctx->sc->err, ctx->st);
+  if (um) launch_zdft_umma(s, ctx->umaps, (float *)ctx->R, (float2 *)ctx->C, ctx->utab, 0, ctx->nsm, &ctx->sc->err, ctx->st);
+  else if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, &ctx->sc->err, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
@@ -884,7 +899,8 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
     launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
   ph_end(ctx, mixed ? 3 : 1);
   ph_begin(ctx, PH_IDFTZ);
-  if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, &ctx->sc->err, ctx->st);
+  if (um) launch_zdft_umma(s, ctx->umaps, (float *)ctx->R, (float2 *)ctx->C, ctx->utab, 1, ctx->nsm, &ctx->sc->err, ctx->st);
+  else if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, &ctx->sc->err, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
@@ -1450,7 +1466,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
         return set_err(ctx, BLGPU_EINVAL, "tiles: %s %d needs %zu B of shared memory (> %d)", name, nw, sm, optin);
     }
   }
-  if (t.zdft != 0 && t.zdft != 1) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1}", t.zdft);
+  if (t.zdft < 0 || t.zdft > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1,2,3}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
   if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
   return BLGPU_OK;
@@ -1558,7 +1574,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {0, 2, 4, 6, 8, 12, 16},                                                 // dct_nw
       {4, 8},                                                                  // dftz_rk
       {4, 8},                                                                  // proj_by
-      {0, 1},                                                                  // zdft
+      {1, 2, 3},                                                               // zdft
       {1, 2},                                                                  // rhs_pts
       {1, 2},                                                                  // thomas
       {0, 4, 8, 12, 16}};                                                      // idct_nw
@@ -1579,7 +1595,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
   for (int knob = 0; knob < 9 && !rc; ++knob) {  // one pass of coordinate descent
-    if (knob == 5 && !ctx->zfrag) continue;        // no tensor-core z transform for this box
+    if (knob == 5 && !ctx->zfrag && !ctx->utab) continue;  // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
     for (int v : cand[knob]) {

@@ -23,7 +23,7 @@ struct Tiles {
   int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 and 8 in FP64 (0: built-in)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
-  int zdft;     // mixed form z transforms: 0 tensor cores where the order is served, 1 FP32 direct sums
+  int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
   int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
@@ -130,6 +130,14 @@ void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm
 int zdft_tc_qp(const Spec &s);
 size_t zdft_tc_frag_words(const Spec &s);
 void zdft_tc_fragments(const Spec &s, std::vector<uint32_t> &out);
+// ---- zdft_umma.cu: the same transforms on tcgen05 tensor cores (TMEM) ----
+int zdft_umma_qp(const Spec &s);
+void zdft_umma_tables(const Spec &s, std::vector<uint32_t> &out);
+struct ZdftMaps;
+bool zdft_umma_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
+// err: device flag, bit 8 set when a copy or a product missed its wait limit
+void launch_zdft_umma(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *tab, int inverse,
+                      int nsm, int *err, cudaStream_t st);
 // TMA tensor maps of R and C (CUtensorMap bytes); false when unavailable
 struct ZdftMaps {
   alignas(64) unsigned char r[128];

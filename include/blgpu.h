@@ -220,8 +220,9 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * block 32 x rhs_by), dct_nw (complex lines per CTA of the forward DCT, up
  * to 16 in the mixed form and 8 in FP64),
  * dftz_rk (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection
- * block 32 x proj_by), zdft (mixed form: 0 = z transforms on the tensor
- * cores where M/2+1 <= 96, 1 = FP32 direct sums), rhs_pts (mixed-form DNS
+ * block 32 x proj_by), zdft (mixed form, where M/2+1 <= 96: 1 = FP32 direct
+ * sums, 2 = mma.sync TF32 tensor cores, 3 = tcgen05 tensor cores with the
+ * accumulators in tensor memory), rhs_pts (mixed-form DNS
  * RHS: x-points per thread, 1 or 2), thomas (y-solve: 1 = register ring,
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT); 0 = the built-in choice.  Values not passed keep their

@@ -1,7 +1,7 @@
-"""The mixed form's z transforms on the tensor cores (TF32 MMAs with a
-three-term split): against the FP32 direct sums and against the FP64 path,
-for odd and even z lengths of every served order (M/2+1 rounded up to 16:
-32, 48, 64, 80, 96)."""
+"""The mixed form's z transforms on the tensor cores (TF32 products with a
+three-term split; mma.sync and tcgen05 with tensor-memory accumulators):
+against the FP32 direct sums and against the FP64 path, for odd and even z
+lengths of every served order (M/2+1 rounded up to 16: 32, 48, 64, 80, 96)."""
 import numpy as np
 import pytest
 
@@ -24,11 +24,12 @@ def noisy(nz, seed):
     return c
 
 
+@pytest.mark.parametrize("form", [2, 3])
 @pytest.mark.parametrize("nz", [64, 65, 96, 97, 127, 159, 193, 194])
-def test_tensor_core_z_transform_matches_direct_and_fp64(gpu, nz):
+def test_tensor_core_z_transform_matches_direct_and_fp64(gpu, nz, form):
     c = noisy(nz, nz)
     out = {}
-    for name, prec, zdft in (("tc", MIXED, 0), ("direct", MIXED, 1), ("fp64", FP64, 0)):
+    for name, prec, zdft in (("tc", MIXED, form), ("direct", MIXED, 1), ("fp64", FP64, 0)):
         s = cases.solver_for(c, precision=prec)
         if prec == MIXED:
             s.set_tiles(zdft=zdft)
@@ -51,10 +52,12 @@ def test_tensor_core_z_transform_matches_direct_and_fp64(gpu, nz):
     assert dt < 1e-3 and dt <= 10 * dd + 1e-6
 
 
-def test_tensor_core_path_steps_close_to_fp64(gpu):
+@pytest.mark.parametrize("form", [0, 2, 3])
+def test_tensor_core_path_steps_close_to_fp64(gpu, form):
     c = cases.turbulent_case(nx=66, ny=33, nz=193, lx=8.0, ly=2.0, lz=8.0, seed=9, cfl=-0.01)
     a = cases.solver_for(c, precision=MIXED)
     assert a.tiles()["zdft"] == 0
+    a.set_tiles(zdft=form)
     b = cases.solver_for(c, precision=FP64)
     a.advance(10)
     b.advance(10)
