@@ -42,6 +42,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
   return false;
 }
+// bounded wait with the hardware-suspended try_wait (fewer issue slots
+// than polling); false when the limit ran out
+__device__ __forceinline__ bool mbar_wait_hw(uint64_t *bar, uint32_t parity) {
+  for (int it = 0; it < WAIT_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
 // generic-proxy shared-memory accesses before async-proxy ones (TMA)
 __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   uint64_t *tbar = reinterpret_cast<uint64_t *>(aux + 4 * UN);     // TMA, per raw buffer
   uint64_t *mbar = tbar + 2;                                       // MMA, per accumulator pair
   uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);         // tensor-memory base
+  int *fail_s = reinterpret_cast<int *>(slot + 1);                  // a warp's wait ran out
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const bool even = (M & 1) == 0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -145,6 +146,7 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 32) {
+    *fail_s = 0;
     mbar_init(&tbar[0], 1);
     mbar_init(&tbar[1], 1);
     mbar_init(&mbar[0], 1);
@@ -177,11 +179,14 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   tc_fence_after();
   const int nmine = ((int)blockIdx.x < nitems) ? (nitems - 1 - (int)blockIdx.x) / G + 1 : 0;
   bool failed = false;
-  // epilogue of local item j (accumulator pair j & 1)
+  // epilogue of local item j (accumulator pair j & 1); each warp waits for
+  // the products itself, so the issuing warp does not hold the others back
   auto epilogue = [&](int j) -> bool {
     const int item = blockIdx.x + j * G, bb = j & 1;
-    const bool ok = mbar_wait(&mbar[bb], (uint32_t)(j >> 1) & 1u);
-    if (__syncthreads_or(!ok)) return false;
+    if (!mbar_wait_hw(&mbar[bb], (uint32_t)(j >> 1) & 1u)) {
+      atomicExch(fail_s, 1);
+      return false;
+    }
     tc_fence_after();
     const int b = item / ntile, kx0 = (item % ntile) * UN;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;  // output row, column half
@@ -195,13 +200,18 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     const int cbase = kx0 + 16 * h;
     if (!inverse) {
       if (row < MH) {
-        float2 *dst = C + ((size_t)b * MH + row) * s.rx + cbase;
+        float2 *dst = C + ((size_t)b * MH + row) * s.rx + cbase;  // 128-byte aligned
+        float v[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          if (cbase + q >= s.N) break;
-          float v = re[q];
-          if (even) v += (row & 1) ? -ax[16 * h + q] : ax[16 * h + q];
-          dst[q] = make_float2(v, im[q]);
+        for (int q = 0; q < 16; ++q) v[q] = even ? re[q] + ((row & 1) ? -ax[16 * h + q] : ax[16 * h + q]) : re[q];
+        if (cbase + 16 <= s.N) {
+#pragma unroll
+          for (int q = 0; q < 16; q += 2)
+            *reinterpret_cast<float4 *>(dst + q) = make_float4(v[q], im[q], v[q + 1], im[q + 1]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (cbase + q < s.N) dst[q] = make_float2(v[q], im[q]);
         }
       }
     } else {
@@ -212,13 +222,27 @@ __global__ void __launch_bounds__(UTHREADS, 1)
         const int pm = M - row;
         float *d2 = R + ((size_t)b * M + pm) * s.rx + cbase;
         const bool two = pm != row && pm < M;
+        float f1[16], f2[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          if (cbase + q >= s.N) break;
           const float c0 = ax[16 * h + q];
           const float y = even ? ((row & 1) ? -ax[UN + 16 * h + q] : ax[UN + 16 * h + q]) : 0.f;
-          d1[q] = (c0 + 2.0f * (re[q] + im[q]) + y) * invM;
-          if (two) d2[q] = (c0 + 2.0f * (re[q] - im[q]) + y) * invM;
+          f1[q] = (c0 + 2.0f * (re[q] + im[q]) + y) * invM;
+          f2[q] = (c0 + 2.0f * (re[q] - im[q]) + y) * invM;
+        }
+        if (cbase + 16 <= s.N) {  // rows are 64-byte aligned at cbase
+#pragma unroll
+          for (int q = 0; q < 16; q += 4) {
+            *reinterpret_cast<float4 *>(d1 + q) = make_float4(f1[q], f1[q + 1], f1[q + 2], f1[q + 3]);
+            if (two) *reinterpret_cast<float4 *>(d2 + q) = make_float4(f2[q], f2[q + 1], f2[q + 2], f2[q + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (cbase + q < s.N) {
+              d1[q] = f1[q];
+              if (two) d2[q] = f2[q];
+            }
         }
       }
     }
@@ -229,12 +253,15 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     const int kx0 = (item % ntile) * UN;
     // the other raw buffer and this item's B buffer are free: their last
     // readers (staging of item i-1, MMAs of item i-2) finished before here
-    __syncthreads();
+    if (__syncthreads_or(*fail_s)) {
+      failed = true;
+      break;
+    }
     if (tid == 32 && i + 1 < nmine) {
       fence_async_shared();
       issue_copy(item + G, bb ^ 1);
     }
-    const bool ok = mbar_wait(&tbar[bb], (uint32_t)(i >> 1) & 1u);
+    const bool ok = mbar_wait_hw(&tbar[bb], (uint32_t)(i >> 1) & 1u);
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -294,28 +321,28 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     if (tid == 0) {
       tc_fence_after();
       const uint32_t sB = smem_u32(Bi);
-#pragma unroll 1
+      // descriptors step by 1 KB (64 in the address field) per K step
+#pragma unroll
       for (int part = 0; part < 2; ++part) {  // 0: cos x S (or Re), 1: -sin x D (or Im)
         const uint32_t d = tmem + acc_col + (uint32_t)(bb * 2 * UN + part * UN);
         const uint32_t ahi = tmem + tab_col + (uint32_t)((2 * part) * QP);
         const uint32_t alo = ahi + QP;
-        const uint32_t bhi = sB + (uint32_t)(2 * part) * OPB, blo = bhi + OPB;
-#pragma unroll 1
+        uint64_t dh = b_desc(sB + (uint32_t)(2 * part) * OPB), dl = dh + (OPB >> 4);
+#pragma unroll
         for (int ks = 0; ks < KS; ++ks) {
-          const uint32_t o = (uint32_t)ks << 10;
-          umma_tf32(d, alo + 8 * ks, b_desc(bhi + o), ks > 0 ? 1u : 0u);  // lo x hi
-          umma_tf32(d, ahi + 8 * ks, b_desc(blo + o), 1u);                // hi x lo
-          umma_tf32(d, ahi + 8 * ks, b_desc(bhi + o), 1u);                // hi x hi
+          umma_tf32(d, alo + 8 * ks, dh, ks > 0 ? 1u : 0u);  // lo x hi
+          umma_tf32(d, ahi + 8 * ks, dl, 1u);                // hi x lo
+          umma_tf32(d, ahi + 8 * ks, dh, 1u);                // hi x hi
+          dh += 64;
+          dl += 64;
         }
       }
       umma_commit(&mbar[bb]);
     }
-    if (i >= 1 && !epilogue(i - 1)) {
-      failed = true;
-      break;
-    }
+    if (i >= 1) epilogue(i - 1);
   }
-  if (!failed && nmine > 0 && !epilogue(nmine - 1)) failed = true;
+  if (!failed && nmine > 0) epilogue(nmine - 1);
+  if (__syncthreads_or(*fail_s)) failed = true;
   if (failed) {
     // let the copies and products this CTA issued finish (bounded), then leave
     if (tid == 0) {
@@ -341,7 +368,7 @@ int u_raw_floats(const Spec &s) {
 }
 size_t u_smem_bytes(const Spec &s, int qp) {
   return 1024 + (size_t)8 * (qp / 8) * 1024 + (size_t)2 * u_raw_floats(s) * sizeof(float) + 4 * UN * sizeof(float) +
-         4 * sizeof(uint64_t) + 16;
+         4 * sizeof(uint64_t) + 16;  // the last 16: tensor-memory slot and failure flag
 }
 uint32_t tf32_host_rna(float x) {
   uint32_t u;
