@@ -138,10 +138,13 @@ bool zdft_umma_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
 // err: device flag, bit 8 set when a copy or a product missed its wait limit
 void launch_zdft_umma(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *tab, int inverse,
                       int nsm, int *err, cudaStream_t st);
-// TMA tensor maps of R and C (CUtensorMap bytes); false when unavailable
+// TMA tensor maps of R and C (CUtensorMap bytes) for the loads, and the
+// 128-byte-swizzled ones the tcgen05 form stores through; false when unavailable
 struct ZdftMaps {
   alignas(64) unsigned char r[128];
   alignas(64) unsigned char c[128];
+  alignas(64) unsigned char rs[128];
+  alignas(64) unsigned char cs[128];
 };
 bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
 // inverse = 0: R -> C (forward); 1: C -> R; nsm: persistent CTAs; err: device

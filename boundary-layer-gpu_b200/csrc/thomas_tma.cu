@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
 }
 
 bool tma::encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *base, const cuuint64_t *dims,
-                 const cuuint64_t *strides, const cuuint32_t *box) {
+                 const cuuint64_t *strides, const cuuint32_t *box, CUtensorMapSwizzle swizzle) {
   static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
   if (!enc) {
     void *fn = nullptr;
@@ -160,9 +160,8 @@ bool tma::encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *bas
   }
   if (reinterpret_cast<uintptr_t>(base) & 15) return false;
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  return enc(map, type, (cuuint32_t)rank, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return enc(map, type, (cuuint32_t)rank, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // C viewed as elements of T (dims 2 rx, MH, NM) with boxes of 2 MT x 1 x NM;

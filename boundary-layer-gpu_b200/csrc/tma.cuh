@@ -74,6 +74,20 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
+// 2D tiled store from shared memory (coordinates in range, never negative)
+__device__ __forceinline__ void store_2d(const CUtensorMap *map, const void *src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void store_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// wait until at most N bulk groups of this thread still read shared memory
+template <int N> __device__ __forceinline__ void store_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// wait until all bulk groups of this thread have completed (writes done)
+__device__ __forceinline__ void store_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // 3D tiled store from shared memory (coordinates must be in range, never
 // negative); completion through the bulk-group of the issuing thread
 __device__ __forceinline__ void store_3d(const CUtensorMap *map, const void *src, int x, int y, int z) {
@@ -90,7 +104,8 @@ __device__ __forceinline__ void store_commit_and_wait_read() {
 // host: tiled tensor map, row-major dims[0] fastest; strides in bytes for
 // dims 1..rank-1; false when the driver entry point or the encoding fails
 bool encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *base, const cuuint64_t *dims,
-            const cuuint64_t *strides, const cuuint32_t *box);
+            const cuuint64_t *strides, const cuuint32_t *box,
+            CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE);
 
 }  // namespace tma
 }  // namespace blgpu

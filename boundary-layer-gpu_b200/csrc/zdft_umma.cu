@@ -102,13 +102,24 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 }  // namespace
 
+// bytes of one output tile (forward: two halves of MH rows; inverse: M rows;
+// 128 bytes a row, each part rounded up to 1 KB)
+__host__ __device__ inline uint32_t u_otile_bytes(int M, int MH) {
+  const uint32_t f = 2u * (((uint32_t)MH * 128u + 1023u) & ~1023u);
+  const uint32_t i = ((uint32_t)M * 128u + 1023u) & ~1023u;
+  return f > i ? f : i;
+}
+// byte offset of 16-byte chunk c of row r in a 128-byte-swizzled tile
+__device__ __forceinline__ uint32_t sw128(int r, int c) { return ((uint32_t)r << 7) + ((uint32_t)((c ^ r) & 7) << 4); }
+
 // Shared memory, from a 1 KB aligned base: B[2 buffers][4 operands][Q/8
-// K-steps of 1 KB] | raw[2][rawf floats] | aux[2][2][32] | 4 mbarriers | tmem slot.
+// K-steps of 1 KB] | raw[2][rawf floats] | aux[2][2][32] | output tiles[2]
+// (1 KB aligned) | 4 mbarriers | tmem slot and failure flag.
 template <int QP>
 __global__ void __launch_bounds__(UTHREADS, 1)
-    k_zdft_umma(const __grid_constant__ CUtensorMap mapR, const __grid_constant__ CUtensorMap mapC, Spec s,
-                float *__restrict__ R, float2 *__restrict__ C, const uint32_t *__restrict__ tab, int inverse,
-                int rawf, int *__restrict__ err) {
+    k_zdft_umma(const __grid_constant__ CUtensorMap mapR, const __grid_constant__ CUtensorMap mapC,
+                const __grid_constant__ CUtensorMap mapRs, const __grid_constant__ CUtensorMap mapCs, Spec s,
+                const uint32_t *__restrict__ tab, int inverse, int rawf, int *__restrict__ err) {
   constexpr int KS = QP / 8;                 // K steps (1 KB of B each) per product
   constexpr uint32_t OPB = (uint32_t)KS << 10;  // bytes of one B operand
   // tensor-memory columns: tables and accumulators, rounded up to a power of two
@@ -120,7 +131,13 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   unsigned char *Bb = sm;                                          // 2 x 4 x OPB
   float *raw0 = reinterpret_cast<float *>(sm + 8 * OPB);           // [2][rawf]
   float *aux = raw0 + 2 * (size_t)rawf;                            // [2][2][UN]
-  uint64_t *tbar = reinterpret_cast<uint64_t *>(aux + 4 * UN);     // TMA, per raw buffer
+  // output tiles [2][otb bytes], 1 KB aligned (128-byte swizzle): forward two
+  // halves of MH rows x 16 complex, inverse M rows x 32 values, 128 B a row
+  const uint32_t ohb = ((uint32_t)s.MH * 128u + 1023u) & ~1023u;  // one forward half
+  const uint32_t otb = u_otile_bytes(s.M, s.MH);
+  unsigned char *ot0 = reinterpret_cast<unsigned char *>(aux + 4 * UN);
+  ot0 += (1024u - (smem_u32(ot0) & 1023u)) & 1023u;
+  uint64_t *tbar = reinterpret_cast<uint64_t *>(ot0 + 2 * otb);    // TMA, per raw buffer
   uint64_t *mbar = tbar + 2;                                       // MMA, per accumulator pair
   uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);         // tensor-memory base
   int *fail_s = reinterpret_cast<int *>(slot + 1);                  // a warp's wait ran out
@@ -179,16 +196,17 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   tc_fence_after();
   const int nmine = ((int)blockIdx.x < nitems) ? (nitems - 1 - (int)blockIdx.x) / G + 1 : 0;
   bool failed = false;
-  // epilogue of local item j (accumulator pair j & 1); each warp waits for
-  // the products itself, so the issuing warp does not hold the others back
-  auto epilogue = [&](int j) -> bool {
-    const int item = blockIdx.x + j * G, bb = j & 1;
+  // epilogue of local item j (accumulator pair j & 1, output tile j & 1):
+  // each warp waits for the products itself (the issuing warp does not hold
+  // the others back) and moves its rows from tensor memory into the swizzled
+  // output tile; the tile leaves by TMA store, issued after the next barrier
+  auto epilogue = [&](int j) {
+    const int bb = j & 1;
     if (!mbar_wait_hw(&mbar[bb], (uint32_t)(j >> 1) & 1u)) {
       atomicExch(fail_s, 1);
-      return false;
+      return;
     }
     tc_fence_after();
-    const int b = item / ntile, kx0 = (item % ntile) * UN;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;  // output row, column half
     float re[16], im[16];
     const uint32_t acc = tmem + lane_base + acc_col + (uint32_t)(bb * 2 * UN) + 16 * h;
@@ -197,56 +215,54 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     tmem_wait_ld();
     tc_fence_before();
     const float *ax = aux + bb * 2 * UN;
-    const int cbase = kx0 + 16 * h;
+    unsigned char *ot = ot0 + (size_t)bb * otb;
     if (!inverse) {
       if (row < MH) {
-        float2 *dst = C + ((size_t)b * MH + row) * s.rx + cbase;  // 128-byte aligned
-        float v[16];
+        unsigned char *oh = ot + h * ohb;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = even ? re[q] + ((row & 1) ? -ax[16 * h + q] : ax[16 * h + q]) : re[q];
-        if (cbase + 16 <= s.N) {
-#pragma unroll
-          for (int q = 0; q < 16; q += 2)
-            *reinterpret_cast<float4 *>(dst + q) = make_float4(v[q], im[q], v[q + 1], im[q + 1]);
-        } else {
-#pragma unroll
-          for (int q = 0; q < 16; ++q)
-            if (cbase + q < s.N) dst[q] = make_float2(v[q], im[q]);
+        for (int c = 0; c < 8; ++c) {  // chunk c: complex values 2c, 2c+1 of this half
+          const int q = 2 * c;
+          const float v0 = even ? re[q] + ((row & 1) ? -ax[16 * h + q] : ax[16 * h + q]) : re[q];
+          const float v1 = even ? re[q + 1] + ((row & 1) ? -ax[16 * h + q + 1] : ax[16 * h + q + 1]) : re[q + 1];
+          *reinterpret_cast<float4 *>(oh + sw128(row, c)) = make_float4(v0, im[q], v1, im[q + 1]);
         }
       }
     } else {
       const int npairs = M / 2 + 1;
       if (row < npairs) {
         const float invM = 1.0f / (float)M;
-        float *d1 = R + ((size_t)b * M + row) * s.rx + cbase;
         const int pm = M - row;
-        float *d2 = R + ((size_t)b * M + pm) * s.rx + cbase;
         const bool two = pm != row && pm < M;
-        float f1[16], f2[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const float c0 = ax[16 * h + q];
-          const float y = even ? ((row & 1) ? -ax[UN + 16 * h + q] : ax[UN + 16 * h + q]) : 0.f;
-          f1[q] = (c0 + 2.0f * (re[q] + im[q]) + y) * invM;
-          f2[q] = (c0 + 2.0f * (re[q] - im[q]) + y) * invM;
-        }
-        if (cbase + 16 <= s.N) {  // rows are 64-byte aligned at cbase
+        for (int c = 0; c < 4; ++c) {  // chunk 4h + c: values 16h + 4c .. 16h + 4c + 3
+          float f1[4], f2[4];
 #pragma unroll
-          for (int q = 0; q < 16; q += 4) {
-            *reinterpret_cast<float4 *>(d1 + q) = make_float4(f1[q], f1[q + 1], f1[q + 2], f1[q + 3]);
-            if (two) *reinterpret_cast<float4 *>(d2 + q) = make_float4(f2[q], f2[q + 1], f2[q + 2], f2[q + 3]);
+          for (int e = 0; e < 4; ++e) {
+            const int q = 4 * c + e;
+            const float c0 = ax[16 * h + q];
+            const float y = even ? ((row & 1) ? -ax[UN + 16 * h + q] : ax[UN + 16 * h + q]) : 0.f;
+            f1[e] = (c0 + 2.0f * (re[q] + im[q]) + y) * invM;
+            f2[e] = (c0 + 2.0f * (re[q] - im[q]) + y) * invM;
           }
-        } else {
-#pragma unroll
-          for (int q = 0; q < 16; ++q)
-            if (cbase + q < s.N) {
-              d1[q] = f1[q];
-              if (two) d2[q] = f2[q];
-            }
+          *reinterpret_cast<float4 *>(ot + sw128(row, 4 * h + c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
+          if (two) *reinterpret_cast<float4 *>(ot + sw128(pm, 4 * h + c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
         }
       }
     }
-    return true;
+    fence_async_shared();  // the tile's writes before the TMA store reads them
+  };
+  // TMA store of the output tile of local item j (all its writers have
+  // passed a barrier since)
+  auto store_tile = [&](int j) {
+    const int item = blockIdx.x + j * G, bb = j & 1;
+    const int b = item / ntile, kx0 = (item % ntile) * UN;
+    const unsigned char *ot = ot0 + (size_t)bb * otb;
+    if (!inverse) {
+      store_2d(&mapCs, ot, 2 * kx0, b * MH);
+      store_2d(&mapCs, ot + ohb, 2 * kx0 + UN, b * MH);
+    } else {
+      store_2d(&mapRs, ot, kx0, b * M);
+    }
   };
   for (int i = 0; i < nmine && !failed; ++i) {
     const int item = blockIdx.x + i * G, bb = i & 1;
@@ -256,6 +272,13 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     if (__syncthreads_or(*fail_s)) {
       failed = true;
       break;
+    }
+    if (tid == 0 && i >= 2) {
+      // the tile of item i-2 (written before the barrier above) leaves; the
+      // one of item i-3 must be read out before epilogue(i-1) reuses its buffer
+      store_tile(i - 2);
+      store_commit();
+      store_wait_read<1>();
     }
     if (tid == 32 && i + 1 < nmine) {
       fence_async_shared();
@@ -341,8 +364,20 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     }
     if (i >= 1) epilogue(i - 1);
   }
-  if (!failed && nmine > 0) epilogue(nmine - 1);
+  if (!failed && nmine > 0) {
+    if (tid == 0) store_wait_read<0>();  // the buffer of item nmine-1 is free
+    __syncthreads();
+    epilogue(nmine - 1);
+  }
   if (__syncthreads_or(*fail_s)) failed = true;
+  if (tid == 0) {
+    if (!failed) {
+      if (nmine >= 2) store_tile(nmine - 2);
+      if (nmine >= 1) store_tile(nmine - 1);
+      store_commit();
+    }
+    store_wait_all();  // no store reads shared memory after this CTA leaves
+  }
   if (failed) {
     // let the copies and products this CTA issued finish (bounded), then leave
     if (tid == 0) {
@@ -367,8 +402,10 @@ int u_raw_floats(const Spec &s) {
   return (f + 31) / 32 * 32;
 }
 size_t u_smem_bytes(const Spec &s, int qp) {
+  // the output tiles start at the next 1 KB boundary after aux (at most 1 KB on)
   return 1024 + (size_t)8 * (qp / 8) * 1024 + (size_t)2 * u_raw_floats(s) * sizeof(float) + 4 * UN * sizeof(float) +
-         4 * sizeof(uint64_t) + 16;  // the last 16: tensor-memory slot and failure flag
+         1024 + 2 * (size_t)u_otile_bytes(s.M, s.MH) + 4 * sizeof(uint64_t) +
+         16;  // the last 16: tensor-memory slot and failure flag
 }
 uint32_t tf32_host_rna(float x) {
   uint32_t u;
@@ -407,9 +444,11 @@ void zdft_umma_tables(const Spec &s, std::vector<uint32_t> &out) {
     }
 }
 
-// tensor maps: R with boxes 32 x M, C (as floats) with boxes 64 x MH
+// tensor maps: R with boxes 32 x M, C (as floats) with boxes 64 x MH for the
+// loads; for the stores R with boxes 32 x M and C with boxes 32 x MH (one
+// 128-byte row each), swizzled by 128 bytes
 bool zdft_umma_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out) {
-  CUtensorMap mr, mc;
+  CUtensorMap mr, mc, mrs, mcs;
   const cuuint64_t dr[2] = {(cuuint64_t)s.rx, (cuuint64_t)s.NM * s.M};
   const cuuint64_t sr[1] = {(cuuint64_t)s.rx * sizeof(float)};
   const cuuint32_t br[2] = {(cuuint32_t)UN, (cuuint32_t)s.M};
@@ -418,8 +457,13 @@ bool zdft_umma_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out) {
   const cuuint64_t sc[1] = {(cuuint64_t)2 * s.rx * sizeof(float)};
   const cuuint32_t bc[2] = {(cuuint32_t)(2 * UN), (cuuint32_t)s.MH};
   if (!encode(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dc, sc, bc)) return false;
+  if (!encode(&mrs, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, R, dr, sr, br, CU_TENSOR_MAP_SWIZZLE_128B)) return false;
+  const cuuint32_t bcs[2] = {(cuuint32_t)UN, (cuuint32_t)s.MH};
+  if (!encode(&mcs, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dc, sc, bcs, CU_TENSOR_MAP_SWIZZLE_128B)) return false;
   memcpy(out->r, &mr, sizeof mr);
   memcpy(out->c, &mc, sizeof mc);
+  memcpy(out->rs, &mrs, sizeof mrs);
+  memcpy(out->cs, &mcs, sizeof mcs);
   return true;
 }
 
@@ -430,10 +474,14 @@ static void launch_u(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, con
   cudaFuncSetAttribute(k_zdft_umma<QP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int nitems = s.NM * ((s.N + UN - 1) / UN);
   const int grid = nitems < nsm ? nitems : nsm;
-  CUtensorMap mr, mc;
+  CUtensorMap mr, mc, mrs, mcs;
   memcpy(&mr, mp.r, sizeof mr);
   memcpy(&mc, mp.c, sizeof mc);
-  k_zdft_umma<QP><<<grid, UTHREADS, sm, st>>>(mr, mc, s, R, C, tab, inverse, u_raw_floats(s), err);
+  memcpy(&mrs, mp.rs, sizeof mrs);
+  memcpy(&mcs, mp.cs, sizeof mcs);
+  (void)R;
+  (void)C;
+  k_zdft_umma<QP><<<grid, UTHREADS, sm, st>>>(mr, mc, mrs, mcs, s, tab, inverse, u_raw_floats(s), err);
 }
 
 void launch_zdft_umma(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *tab, int inverse,
