@@ -260,11 +260,12 @@ class Solver:
         return tx.reshape(self.nzg - 3, self.nx - 2), tz.reshape(self.nzg - 3, self.nx - 2)
 
     # -- launch shapes -----------------------------------------------------
-    TILE_NAMES = ("rhs_kc", "rhs_by", "dct_nw", "dftz_rk", "proj_by", "zdft", "rhs_pts", "thomas", "idct_nw")
+    TILE_NAMES = ("rhs_kc", "rhs_by", "dct_nw", "dftz_rk", "proj_by", "zdft", "rhs_pts", "thomas", "idct_nw",
+                  "xfft")
 
     def tiles(self):
-        t = (ctypes.c_int * 9)()
-        self._ck(self.lib.blgpu_get_tiles(self.ctx, t, 9))
+        t = (ctypes.c_int * 10)()
+        self._ck(self.lib.blgpu_get_tiles(self.ctx, t, 10))
         return dict(zip(self.TILE_NAMES, list(t)))
 
     def set_tiles(self, **kw):
@@ -273,8 +274,8 @@ class Solver:
             if k not in cur:
                 raise KeyError(k)
             cur[k] = int(v)
-        t = (ctypes.c_int * 9)(*[cur[k] for k in self.TILE_NAMES])
-        self._ck(self.lib.blgpu_set_tiles(self.ctx, t, 9))
+        t = (ctypes.c_int * 10)(*[cur[k] for k in self.TILE_NAMES])
+        self._ck(self.lib.blgpu_set_tiles(self.ctx, t, 10))
 
     def autotune(self, steps=3):
         """Choose the launch shapes by timing; returns (ms/step before, after)."""

@@ -382,7 +382,7 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
     ctx->pl64.post = (const double2 *)ctx->post;
     ctx->pl32.tw = (const float2 *)ctx->tw;
     ctx->pl32.post = (const float2 *)ctx->post;
-    const size_t sm = dct_smem_bytes(N, (int)ctx->esz, 1);  // one line per CTA at the least
+    const size_t sm = dct_smem_bytes(N, (int)ctx->esz, 1, 0);  // one line per CTA at the least
     int dev_sm = 0;
     cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg->device);
     if ((long long)sm > dev_sm) TRY(set_err(ctx, BLGPU_EINVAL, "nx=%d needs %zu B shared memory per CTA", ctx->nx, sm));
@@ -875,7 +875,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
   const bool mixed = !ctx->fp64;
   ph_begin(ctx, PH_DIVDCT);
-  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->st);
+  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->tiles.xfft, ctx->st);
   ph_end(ctx, 1);
   // z transforms: tcgen05 (zdft 0 or 3), mma.sync TF32 (0 without tcgen05, or 2), FP32/FP64 sums (1)
   const int zd = ctx->tiles.zdft;
@@ -904,7 +904,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
-  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->st);
+  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->tiles.xfft, ctx->st);
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
@@ -1453,6 +1453,11 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
     return set_err(ctx, BLGPU_EINVAL, "tiles: proj_by %d not in {1,2,4,8}", t.proj_by);
   if (t.dftz_rk != 0 && t.dftz_rk != 4 && t.dftz_rk != 8)
     return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
+  if (t.xfft < 0 || t.xfft > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: xfft %d not in {0,1,2}", t.xfft);
+  const int split = (ctx->fp64 || t.xfft == 1) ? 0 : xfft_split(ctx->spec.N);
+  if (t.xfft == 2 && !split)
+    return set_err(ctx, BLGPU_EINVAL, "tiles: xfft 2 (two-pass x transforms) not built for N = %d in %s", ctx->spec.N,
+                   ctx->fp64 ? "FP64" : "FP32");
   const int maxnw = dct_max_lines((int)ctx->esz);
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
@@ -1461,7 +1466,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
     const char *name = q ? "idct_nw" : "dct_nw";
     if (nw < 0 || nw > maxnw) return set_err(ctx, BLGPU_EINVAL, "tiles: %s %d outside 0..%d", name, nw, maxnw);
     if (nw > 0) {
-      const size_t sm = dct_smem_bytes(ctx->spec.N, (int)ctx->esz, nw);
+      const size_t sm = dct_smem_bytes(ctx->spec.N, (int)ctx->esz, nw, split);
       if (sm > (size_t)optin)
         return set_err(ctx, BLGPU_EINVAL, "tiles: %s %d needs %zu B of shared memory (> %d)", name, nw, sm, optin);
     }
@@ -1531,10 +1536,17 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 9 values");
-  Tiles t{tiles[0], tiles[1], tiles[2], tiles[3], tiles[4], n >= 6 ? tiles[5] : ctx->tiles.zdft,
-          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts, n >= 8 ? tiles[7] : ctx->tiles.thomas,
-          n >= 9 ? tiles[8] : ctx->tiles.idct_nw};
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 10 values");
+  Tiles t{tiles[0],
+          tiles[1],
+          tiles[2],
+          tiles[3],
+          tiles[4],
+          n >= 6 ? tiles[5] : ctx->tiles.zdft,
+          n >= 7 ? tiles[6] : ctx->tiles.rhs_pts,
+          n >= 8 ? tiles[7] : ctx->tiles.thomas,
+          n >= 9 ? tiles[8] : ctx->tiles.idct_nw,
+          n >= 10 ? tiles[9] : ctx->tiles.xfft};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1556,6 +1568,7 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   if (n >= 7) tiles[6] = t.rhs_pts;
   if (n >= 8) tiles[7] = t.thomas;
   if (n >= 9) tiles[8] = t.idct_nw;
+  if (n >= 10) tiles[9] = t.xfft;
   return BLGPU_OK;
 }
 
@@ -1577,7 +1590,8 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {1, 2, 3},                                                               // zdft
       {1, 2},                                                                  // rhs_pts
       {1, 2},                                                                  // thomas
-      {0, 4, 8, 12, 16}};                                                      // idct_nw
+      {0, 4, 8, 12, 16},                                                       // idct_nw
+      {1, 2}};                                                                 // xfft
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1594,14 +1608,15 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 9 && !rc; ++knob) {  // one pass of coordinate descent
+  for (int knob = 0; knob < 10 && !rc; ++knob) {  // one pass of coordinate descent
     if (knob == 5 && !ctx->zfrag && !ctx->utab) continue;  // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
+    if (knob == 9 && (ctx->fp64 || !xfft_split(ctx->spec.N))) continue;  // one x-transform kernel
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[9] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,
-                   &t.idct_nw};
+      int *f[10] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,
+                    &t.idct_nw, &t.xfft};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

@@ -27,6 +27,7 @@ struct Tiles {
   int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
+  int xfft;     // FP32 x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)
@@ -112,7 +113,7 @@ struct Spec {  // spectral layout of the Poisson solve
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    int nw, cudaStream_t st);
+                    int nw, int xfft, cudaStream_t st);
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
                   int rk, cudaStream_t st);
@@ -168,11 +169,15 @@ void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl,
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, cudaStream_t st);
-size_t dct_smem_bytes(int n, int elem_bytes, int lines);
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, int xfft,
+                 cudaStream_t st);
+// shared memory of a DCT CTA of `lines` warps; split: that of xfft_split, 0 for the Stockham kernels
+size_t dct_smem_bytes(int n, int elem_bytes, int lines, int split);
+// the split A of N = A B served by the two-pass FP32 x transforms, 0 if none
+int xfft_split(int n);
 // the R-point DFT constants of the odd register butterflies (once per device)
 int upload_dft_constants();
-int dct_lines_per_cta(int n, int elem_bytes, bool inverse);
+int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split);
 int dct_max_lines(int elem_bytes);  // launch bound of the DCT kernels, in warps
 
 }  // namespace blgpu

@@ -101,7 +101,22 @@ template <typename T> __device__ __forceinline__ const T2<T> *dft_consts();
 template <> __device__ __forceinline__ const double2 *dft_consts<double>() { return c_dft64; }
 template <> __device__ __forceinline__ const float2 *dft_consts<float>() { return c_dft32; }
 
+// (cos, sin)(2 pi e / R) for R = 2..32, e = 0..R-1, R's entries from
+// root_off<R>(): the constants of the in-register DFTs of the two-pass FFT
+constexpr int ROOTS_N = 33 * 32 / 2 - 1;
+__constant__ float2 c_roots32[ROOTS_N];
+template <int R> __host__ __device__ constexpr int root_off() { return R * (R - 1) / 2 - 1; }
+
 int upload_dft_constants() {
+  {
+    float2 h[ROOTS_N];
+    for (int R = 2; R <= 32; ++R)
+      for (int e = 0; e < R; ++e) {
+        const double a = 2.0 * M_PI * (double)e / (double)R;
+        h[R * (R - 1) / 2 - 1 + e] = make_float2((float)cos(a), (float)sin(a));
+      }
+    if (cudaMemcpyToSymbol(c_roots32, h, sizeof h) != cudaSuccess) return -1;
+  }
   const int rad[9] = {5, 7, 11, 13, 17, 19, 23, 29, 31};
   double2 h64[DFT_RSUM];
   float2 h32[DFT_RSUM];
@@ -257,6 +272,186 @@ __device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> 
 }
 
 // ---------------------------------------------------------------------------
+// Two-pass register FFT (FP32) of a line of N = A B complex values, one warp
+// per line, every index a compile-time constant.  With n = B n1 + n2 and
+// k = k1 + A k2:
+//   pass 1 (lane n2 < B): A-point DFT over n1 of z[B n1 + n2] in registers,
+//          times W_N^{n2 k1}, into S[k1][n2] (row pitch B | 1, odd, so that
+//          the column reads of pass 2 meet distinct banks);
+//   pass 2 (lane k1 < A): B-point DFT over n2 of S[k1][n2] in registers,
+//          into Z[k1 + A k2].
+// Both passes work in place in one buffer (reads, warp barrier, writes).
+// The in-register DFTs split composite lengths (radix 4, 2, then the odd
+// primes) and take prime lengths >= 5 by the f_q +- f_{R-q} pairing; their
+// constants are constant-memory operands.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int first_factor(int R) {
+  if (R % 4 == 0 && R != 4) return 4;
+  for (int f = 2; f * f <= R; ++f)
+    if (R % f == 0) return f;
+  return R;
+}
+
+// a * W_R^e (W_R = exp(-2 pi i / R)), or a * conj(W_R^e) for the inverse
+template <int R, bool INV>
+__device__ __forceinline__ float2 twr(float2 a, int e) {
+  if (e == 0) return a;
+  if (2 * e == R) return make_float2(-a.x, -a.y);
+  if (4 * e == R) return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+  if (4 * e == 3 * R) return INV ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+  const float2 w = c_roots32[root_off<R>() + e];  // (cos, sin)
+  return INV ? make_float2(a.x * w.x - a.y * w.y, a.y * w.x + a.x * w.y)
+             : make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
+  if constexpr (R == 2) {
+    const float2 a = x[0], b = x[1];
+    x[0] = make_float2(a.x + b.x, a.y + b.y);
+    x[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 3) {
+    const float s60 = 0.86602540378443864676f;
+    const float2 a0 = x[0], t1 = make_float2(x[1].x + x[2].x, x[1].y + x[2].y);
+    const float2 t2 = make_float2(x[1].x - x[2].x, x[1].y - x[2].y);
+    const float2 m = make_float2(a0.x - 0.5f * t1.x, a0.y - 0.5f * t1.y);
+    const float2 it = INV ? make_float2(-s60 * t2.y, s60 * t2.x) : make_float2(s60 * t2.y, -s60 * t2.x);
+    x[0] = make_float2(a0.x + t1.x, a0.y + t1.y);
+    x[1] = make_float2(m.x + it.x, m.y + it.y);
+    x[2] = make_float2(m.x - it.x, m.y - it.y);
+  } else if constexpr (R == 4) {
+    const float2 s0 = make_float2(x[0].x + x[2].x, x[0].y + x[2].y), s1 = make_float2(x[0].x - x[2].x, x[0].y - x[2].y);
+    const float2 s2 = make_float2(x[1].x + x[3].x, x[1].y + x[3].y), s3 = make_float2(x[1].x - x[3].x, x[1].y - x[3].y);
+    const float2 r3 = INV ? make_float2(-s3.y, s3.x) : make_float2(s3.y, -s3.x);  // +-i s3
+    x[0] = make_float2(s0.x + s2.x, s0.y + s2.y);
+    x[1] = make_float2(s1.x + r3.x, s1.y + r3.y);
+    x[2] = make_float2(s0.x - s2.x, s0.y - s2.y);
+    x[3] = make_float2(s1.x - r3.x, s1.y - r3.y);
+  } else if constexpr (first_factor(R) == R) {
+    // prime R >= 5: X_k = x_0 + sum_q s_q cos - (+) i d_q sin, s, d = x_q +- x_{R-q}
+    constexpr int H = (R - 1) / 2;
+    const float2 x0 = x[0];
+    float2 s[H], d[H];
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      s[q - 1] = make_float2(x[q].x + x[R - q].x, x[q].y + x[R - q].y);
+      d[q - 1] = make_float2(x[q].x - x[R - q].x, x[q].y - x[R - q].y);
+    }
+    float2 y0 = x0;
+#pragma unroll
+    for (int q = 0; q < H; ++q) y0 = make_float2(y0.x + s[q].x, y0.y + s[q].y);
+    x[0] = y0;
+    const float2 *K = c_roots32 + root_off<R>();
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+      float ax = x0.x, ay = x0.y, bx = 0.f, by = 0.f;
+#pragma unroll
+      for (int q = 1; q <= H; ++q) {
+        const int m = (q * k) % R;
+        const float c = K[m].x, sv = K[m].y;
+        ax += s[q - 1].x * c;
+        ay += s[q - 1].y * c;
+        bx += d[q - 1].x * sv;
+        by += d[q - 1].y * sv;
+      }
+      if (!INV) {
+        x[k] = make_float2(ax + by, ay - bx);
+        x[R - k] = make_float2(ax - by, ay + bx);
+      } else {
+        x[k] = make_float2(ax - by, ay + bx);
+        x[R - k] = make_float2(ax + by, ay - bx);
+      }
+    }
+  } else {
+    // R = p m: m-point DFTs of the p decimated sequences x[p j + r], twiddles
+    // W_R^{r k}, p-point DFTs across r: X[k + m q]
+    constexpr int p = first_factor(R), m = R / p;
+    float2 y[p][m];
+#pragma unroll
+    for (int r = 0; r < p; ++r)
+#pragma unroll
+      for (int j = 0; j < m; ++j) y[r][j] = x[p * j + r];
+#pragma unroll
+    for (int r = 0; r < p; ++r) dft_reg<m, INV>(y[r]);
+#pragma unroll
+    for (int r = 1; r < p; ++r)
+#pragma unroll
+      for (int k = 1; k < m; ++k) y[r][k] = twr<R, INV>(y[r][k], r * k);
+#pragma unroll
+    for (int k = 0; k < m; ++k) {
+      float2 t[p];
+#pragma unroll
+      for (int r = 0; r < p; ++r) t[r] = y[r][k];
+      dft_reg<p, INV>(t);
+#pragma unroll
+      for (int q = 0; q < p; ++q) x[k + m * q] = t[q];
+    }
+  }
+}
+
+// FFT engines of the x transforms: the shared-memory twiddle table, the
+// per-line buffer and the transform of one line by one warp (result in
+// natural order).  Stockham: any N, ping-pong buffers of N values.
+template <typename T, int MAXR> struct StockhamX {
+  static size_t line(int N) { return 2 * (size_t)N; }
+  __device__ static size_t dline(int N) { return 2 * (size_t)N; }
+  __device__ static void fill(T2<T> *tw, const FftPlan<T> &pl, int tid, int nt) {
+    for (int t = tid; t < pl.n; t += nt) tw[t] = pl.tw[t];
+  }
+  template <bool INV>
+  __device__ static T2<T> *run(T2<T> *buf, const FftPlan<T> &pl, const T2<T> *tw, int lane) {
+    return fft_warp<T, INV, MAXR>(buf, buf + pl.n, pl, tw, lane);
+  }
+};
+
+// Two-pass: N = A B (A, B <= 32), one buffer of max(N, A (B | 1)) values;
+// the table holds W_N^{n2 k1} at [k1][n2] (row pitch B)
+template <int A, int B> struct TwoPassX {
+  static constexpr int N = A * B, SB = B | 1, LINE = N > A * SB ? N : A * SB;
+  static_assert(A <= 32 && B <= 32, "one lane per butterfly");
+  static size_t line(int) { return LINE; }
+  __device__ static size_t dline(int) { return LINE; }
+  __device__ static void fill(float2 *tw, const FftPlan<float> &pl, int tid, int nt) {
+    for (int t = tid; t < N; t += nt) {
+      const int k1 = t / B, n2 = t - k1 * B;
+      tw[t] = pl.tw[n2 * k1];  // n2 k1 < N
+    }
+  }
+  template <bool INV>
+  __device__ static float2 *run(float2 *buf, const FftPlan<float> &, const float2 *tw, int lane) {
+    {
+      float2 x[A];
+      if (lane < B) {
+#pragma unroll
+        for (int n1 = 0; n1 < A; ++n1) x[n1] = buf[B * n1 + lane];
+        dft_reg<A, INV>(x);
+#pragma unroll
+        for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<float, INV>(x[k1], tw[k1 * B + lane]);
+      }
+      __syncwarp();
+      if (lane < B) {
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) buf[k1 * SB + lane] = x[k1];
+      }
+      __syncwarp();
+    }
+    float2 y[B];
+    if (lane < A) {
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) y[n2] = buf[lane * SB + n2];
+      dft_reg<B, INV>(y);
+    }
+    __syncwarp();
+    if (lane < A) {
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) buf[lane + A * k2] = y[k2];
+    }
+    __syncwarp();
+    return buf;
+  }
+};
+
+// ---------------------------------------------------------------------------
 // divergence + DCT-II in x.  Each warp transforms one complex line holding
 // the real lines q and q+1 (q = b*M + k').  R[q][kx] receives
 // c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
@@ -278,7 +473,7 @@ __device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const
 // FP64 kernels need more registers per thread and stop at 8
 template <typename T> struct DctCta { static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256; };
 
-template <typename T, int MAXR>
+template <typename T, class E>
 __global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
                                                  const T *__restrict__ V, const T *__restrict__ W,
                                                  T *__restrict__ R) {
@@ -287,12 +482,9 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
   T2<T> *post = tw + N;
-  T2<T> *bufA = post + N + (size_t)warp * 2 * N;
-  T2<T> *bufB = bufA + N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    tw[t] = pl.tw[t];
-    post[t] = pl.post[t];
-  }
+  T2<T> *bufA = post + N + (size_t)warp * E::dline(N);
+  E::fill(tw, pl, threadIdx.x, blockDim.x);
+  for (int t = threadIdx.x; t < N; t += blockDim.x) post[t] = pl.post[t];
   __syncthreads();
   const int nlines = s.NM * s.M;
   const int q = (blockIdx.x * nw + warp) * 2;
@@ -324,7 +516,7 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec 
     }
   }
   __syncwarp();
-  const T2<T> *res = fft_warp<T, false, MAXR>(bufA, bufB, pl, tw, lane);
+  const T2<T> *res = E::template run<false>(bufA, pl, tw, lane);
   T *ra = R + (long long)q * s.rx;
   T *rb = ra + s.rx;
   for (int k = lane; k < N; k += 32) {
@@ -344,7 +536,7 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec 
 // apply_periodic_z_pressure: rhs_p(nxg-1,:,:) = rhs_p(nxg-2,:,:) and
 // rhs_p(2:nxg-1,:,nzp+2) = rhs_p(2:nxg-1,:,2)); one complex line per warp.
 // ---------------------------------------------------------------------------
-template <typename T, int MAXR>
+template <typename T, class E>
 __global__ void __launch_bounds__(DctCta<T>::max_threads) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
                                               T *__restrict__ p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -352,12 +544,9 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_idct(Geo g, Spec s, 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
   T2<T> *post = tw + N;
-  T2<T> *bufA = post + N + (size_t)warp * 2 * N;
-  T2<T> *bufB = bufA + N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    tw[t] = pl.tw[t];
-    post[t] = pl.post[t];
-  }
+  T2<T> *bufA = post + N + (size_t)warp * E::dline(N);
+  E::fill(tw, pl, threadIdx.x, blockDim.x);
+  for (int t = threadIdx.x; t < N; t += blockDim.x) post[t] = pl.post[t];
   __syncthreads();
   const int nlines = s.NM * s.M;
   const int q = (blockIdx.x * nw + warp) * 2;
@@ -375,7 +564,7 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_idct(Geo g, Spec s, 
     bufA[k] = mk<T>(va.x - vb.y, va.y + vb.x);
   }
   __syncwarp();
-  const T2<T> *res = fft_warp<T, true, MAXR>(bufA, bufB, pl, tw, lane);
+  const T2<T> *res = E::template run<true>(bufA, pl, tw, lane);
   const T inv = (T)1 / (T)N;
   const int ba = q / s.M, ka = q - ba * s.M;
   const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
@@ -816,11 +1005,29 @@ __global__ void k_kz0_grad(Spec s, const double *__restrict__ p0, float *__restr
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-int dct_lines_per_cta(int n, int elem_bytes, bool inverse) {
+// the split A (N = A B) of the two-pass FP32 kernels built for N, else 0
+int xfft_split(int n) {
+  switch (n) {
+    case 812: return 29;  // 29 x 28
+    case 510: return 17;  // 17 x 30
+    default: return 0;
+  }
+}
+
+static size_t xfft_line(int n, int split) {
+  if (!split) return 2 * (size_t)n;
+  const int B = n / split, SB = B | 1;
+  return (size_t)(n > split * SB ? n : split * SB);
+}
+
+int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
   // warps (complex lines) per CTA, as measured at 814 x 257 x 193: the FP32
   // inverse fills one SM's shared memory with up to 16 lines, the FP32
   // forward (its divergence loads want more CTAs in flight) takes three CTAs
-  // of up to 4 lines per SM, FP64 (register-limited) two CTAs within 113 KB
+  // of up to 4 lines per SM, FP64 (register-limited) two CTAs within 113 KB;
+  // the two-pass kernels (122 registers, 16 warps per SM) take 4 forward
+  // and 8 inverse lines per CTA
+  if (split) return inverse ? 8 : 4;
   const size_t line = (size_t)n * 2 * elem_bytes * 2;  // ping-pong buffers of one complex line
   const size_t fixed = (size_t)n * 2 * elem_bytes * 2; // twiddle + DCT tables
   const size_t budget = elem_bytes == 8 ? 113 * 1024 : inverse ? 226 * 1024 : 75 * 1024;
@@ -833,8 +1040,8 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse) {
 
 int dct_max_lines(int elem_bytes) { return elem_bytes == 4 ? 16 : 8; }
 
-size_t dct_smem_bytes(int n, int elem_bytes, int warps) {
-  return (size_t)n * 2 * elem_bytes * (2 + 2 * (size_t)warps);
+size_t dct_smem_bytes(int n, int elem_bytes, int warps, int split) {
+  return (size_t)2 * elem_bytes * (2 * (size_t)n + (size_t)warps * xfft_line(n, split));
 }
 
 // Register-resident odd butterflies raise the register count of the whole
@@ -852,50 +1059,61 @@ static int radix_class(const int *rad, int nst) {
   return 31;
 }
 
-template <typename T, int MAXR>
-static void launch_div_dct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W,
-                               T *R, int nw, size_t sm, int grid, cudaStream_t st) {
-  cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  cudaFuncSetAttribute(k_div_dct<T, MAXR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  k_div_dct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R);
+template <typename T, class E>
+static void launch_div_dct_e(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W,
+                             T *R, int nw, size_t sm, int grid, cudaStream_t st) {
+  cudaFuncSetAttribute(k_div_dct<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_div_dct<T, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  k_div_dct<T, E><<<grid, 32 * nw, sm, st>>>(g, s, pl, U, V, W, R);
 }
 
-template <typename T, int MAXR>
-static void launch_idct_cls(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, size_t sm,
-                            int grid, cudaStream_t st) {
-  cudaFuncSetAttribute(k_idct<T, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  cudaFuncSetAttribute(k_idct<T, MAXR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  k_idct<T, MAXR><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p);
+template <typename T, class E>
+static void launch_idct_e(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, size_t sm,
+                          int grid, cudaStream_t st) {
+  cudaFuncSetAttribute(k_idct<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_idct<T, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  k_idct<T, E><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p);
 }
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    int nw_req, cudaStream_t st) {
-  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false);
-  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
+                    int nw_req, int xfft, cudaStream_t st) {
+  const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false, split);
+  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
   const int grid = (ncl + nw - 1) / nw;
+  if constexpr (sizeof(T) == 4) {
+    if (split == 29) return launch_div_dct_e<T, TwoPassX<29, 28>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
+    if (split == 17) return launch_div_dct_e<T, TwoPassX<17, 30>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
+  }
   switch (radix_class(pl.rad, pl.nst)) {
-    case 7: launch_div_dct_cls<T, 7>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
-    case 13: launch_div_dct_cls<T, 13>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
-    case 19: launch_div_dct_cls<T, 19>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
-    case 29: launch_div_dct_cls<T, 29>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
-    default: launch_div_dct_cls<T, 31>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 7: launch_div_dct_e<T, StockhamX<T, 7>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 13: launch_div_dct_e<T, StockhamX<T, 13>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 19: launch_div_dct_e<T, StockhamX<T, 19>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    case 29: launch_div_dct_e<T, StockhamX<T, 29>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
+    default: launch_div_dct_e<T, StockhamX<T, 31>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
   }
 }
 
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, cudaStream_t st) {
-  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true);
-  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw);
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft,
+                 cudaStream_t st) {
+  const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
+  const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true, split);
+  const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;
+  if constexpr (sizeof(T) == 4) {
+    if (split == 29) return launch_idct_e<T, TwoPassX<29, 28>>(g, s, pl, R, p, nw, sm, grid, st);
+    if (split == 17) return launch_idct_e<T, TwoPassX<17, 30>>(g, s, pl, R, p, nw, sm, grid, st);
+  }
   switch (radix_class(pl.rad, pl.nst)) {
-    case 7: launch_idct_cls<T, 7>(g, s, pl, R, p, nw, sm, grid, st); break;
-    case 13: launch_idct_cls<T, 13>(g, s, pl, R, p, nw, sm, grid, st); break;
-    case 19: launch_idct_cls<T, 19>(g, s, pl, R, p, nw, sm, grid, st); break;
-    case 29: launch_idct_cls<T, 29>(g, s, pl, R, p, nw, sm, grid, st); break;
-    default: launch_idct_cls<T, 31>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 7: launch_idct_e<T, StockhamX<T, 7>>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 13: launch_idct_e<T, StockhamX<T, 13>>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 19: launch_idct_e<T, StockhamX<T, 19>>(g, s, pl, R, p, nw, sm, grid, st); break;
+    case 29: launch_idct_e<T, StockhamX<T, 29>>(g, s, pl, R, p, nw, sm, grid, st); break;
+    default: launch_idct_e<T, StockhamX<T, 31>>(g, s, pl, R, p, nw, sm, grid, st); break;
   }
 }
 
@@ -944,8 +1162,9 @@ void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm
 
 #define BLGPU_SPEC_INST(T)                                                                                        \
   template void launch_div_dct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, const T *, const T *, \
-                                  T *, int, cudaStream_t);                                                        \
-  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, cudaStream_t); \
+                                  T *, int, int, cudaStream_t);                                                   \
+  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, int,          \
+                               cudaStream_t);                                                                    \
   template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
   template void launch_thomas<T>(const Spec &, T2<T> *, const double *, const double *, const double *,          \
                                  double *, int, cudaStream_t);

@@ -216,7 +216,7 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
                                    void *stream);
 
 /* ---- launch shapes and the autotuner ----
- * tiles[5 to 9] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS
+ * tiles[5 to 10] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS
  * block 32 x rhs_by), dct_nw (complex lines per CTA of the forward DCT, up
  * to 16 in the mixed form and 8 in FP64),
  * dftz_rk (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection
@@ -225,9 +225,11 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * accumulators in tensor memory), rhs_pts (mixed-form DNS
  * RHS: x-points per thread, 1 or 2), thomas (y-solve: 1 = register ring,
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
- * inverse DCT); 0 = the built-in choice.  Values not passed keep their
- * current setting.  All but zdft and rhs_pts leave results unchanged;
- * those two change them at FP32 rounding level.  No counterpart in the
+ * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
+ * in shared memory, any N; 2 = two-pass register FFT, built for
+ * N = nx-2 = 812 (29 x 28) and 510 (17 x 30)); 0 = the built-in choice.
+ * Values not passed keep their current setting.  All but zdft, rhs_pts and
+ * xfft leave results unchanged; those change them at FP32 rounding level.  No counterpart in the
  * reference (its OpenACC loops take compiler-chosen gangs). */
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n);
 int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n);

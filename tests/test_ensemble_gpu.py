@@ -71,7 +71,7 @@ def test_tiles_do_not_change_results(gpu, precision):
     s1 = cases.solver_for(c, precision=precision)
     s1.set_tiles(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4, idct_nw=3)
     assert s1.tiles() == dict(rhs_kc=kc, rhs_by=4, dct_nw=2, dftz_rk=4, proj_by=4, zdft=0, rhs_pts=0, thomas=0,
-                              idct_nw=3)
+                              idct_nw=3, xfft=0)
     s1.advance(3)
     assert same(states([s0]), states([s1]))
 
@@ -85,8 +85,8 @@ def test_autotune_restores_state_and_keeps_results(gpu):
     assert t0 > 0 and 0 < t1 <= t0
     assert same(before, states([s]))
     ref = cases.solver_for(c, precision=MIXED)
-    # the z-transform and RHS-form choices are the knobs that move roundings
-    ref.set_tiles(zdft=s.tiles()["zdft"], rhs_pts=s.tiles()["rhs_pts"])
+    # the z-transform, RHS-form and x-transform choices are the knobs that move roundings
+    ref.set_tiles(zdft=s.tiles()["zdft"], rhs_pts=s.tiles()["rhs_pts"], xfft=s.tiles()["xfft"])
     ref.advance(2)
     s.advance(3)
     ref.advance(3)
