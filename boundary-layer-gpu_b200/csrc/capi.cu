@@ -1458,7 +1458,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   if (t.xfft == 2 && !split)
     return set_err(ctx, BLGPU_EINVAL, "tiles: xfft 2 (two-pass x transforms) not built for N = %d in %s", ctx->spec.N,
                    ctx->fp64 ? "FP64" : "FP32");
-  const int maxnw = dct_max_lines((int)ctx->esz);
+  const int maxnw = dct_max_lines((int)ctx->esz, split);
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device);
   for (int q = 0; q < 2; ++q) {

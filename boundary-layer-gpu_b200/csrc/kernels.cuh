@@ -20,7 +20,7 @@ template <typename T> struct MetT {
 struct Tiles {
   int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8; FP32 DNS 8 for two points, 32 for one)
   int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
-  int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 and 8 in FP64 (0: built-in)
+  int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 (8 two-pass) and 8 in FP64 (0: built-in)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
@@ -178,6 +178,6 @@ int xfft_split(int n);
 // the R-point DFT constants of the odd register butterflies (once per device)
 int upload_dft_constants();
 int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split);
-int dct_max_lines(int elem_bytes);  // launch bound of the DCT kernels, in warps
+int dct_max_lines(int elem_bytes, int split);  // launch bound of the DCT kernels, in warps
 
 }  // namespace blgpu

@@ -393,6 +393,7 @@ __device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
 // per-line buffer and the transform of one line by one warp (result in
 // natural order).  Stockham: any N, ping-pong buffers of N values.
 template <typename T, int MAXR> struct StockhamX {
+  static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256, min_blocks = 0;  // 16 or 8 lines, no bound
   static size_t line(int N) { return 2 * (size_t)N; }
   __device__ static size_t dline(int N) { return 2 * (size_t)N; }
   __device__ static void fill(T2<T> *tw, const FftPlan<T> &pl, int tid, int nt) {
@@ -409,6 +410,9 @@ template <typename T, int MAXR> struct StockhamX {
 template <int A, int B> struct TwoPassX {
   static constexpr int N = A * B, SB = B | 1, LINE = N > A * SB ? N : A * SB;
   static_assert(A <= 32 && B <= 32, "one lane per butterfly");
+  // up to 8 lines per CTA and three CTAs of 8 per SM: 80 registers, which
+  // hold the 29-point pass without spills and leave room for 24 warps per SM
+  static constexpr int max_threads = 256, min_blocks = 3;
   static size_t line(int) { return LINE; }
   __device__ static size_t dline(int) { return LINE; }
   __device__ static void fill(float2 *tw, const FftPlan<float> &pl, int tid, int nt) {
@@ -474,7 +478,7 @@ __device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const
 template <typename T> struct DctCta { static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256; };
 
 template <typename T, class E>
-__global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
+__global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_div_dct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ U,
                                                  const T *__restrict__ V, const T *__restrict__ W,
                                                  T *__restrict__ R) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -537,7 +541,7 @@ __global__ void __launch_bounds__(DctCta<T>::max_threads) k_div_dct(Geo g, Spec 
 // rhs_p(2:nxg-1,:,nzp+2) = rhs_p(2:nxg-1,:,2)); one complex line per warp.
 // ---------------------------------------------------------------------------
 template <typename T, class E>
-__global__ void __launch_bounds__(DctCta<T>::max_threads) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
+__global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_idct(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R,
                                               T *__restrict__ p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = s.N;
@@ -1025,9 +1029,9 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
   // inverse fills one SM's shared memory with up to 16 lines, the FP32
   // forward (its divergence loads want more CTAs in flight) takes three CTAs
   // of up to 4 lines per SM, FP64 (register-limited) two CTAs within 113 KB;
-  // the two-pass kernels (122 registers, 16 warps per SM) take 4 forward
-  // and 8 inverse lines per CTA
-  if (split) return inverse ? 8 : 4;
+  // the two-pass kernels (80 registers, 24 warps per SM) take 6 lines per
+  // CTA in both directions
+  if (split) return 6;
   const size_t line = (size_t)n * 2 * elem_bytes * 2;  // ping-pong buffers of one complex line
   const size_t fixed = (size_t)n * 2 * elem_bytes * 2; // twiddle + DCT tables
   const size_t budget = elem_bytes == 8 ? 113 * 1024 : inverse ? 226 * 1024 : 75 * 1024;
@@ -1038,7 +1042,7 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
   return w;
 }
 
-int dct_max_lines(int elem_bytes) { return elem_bytes == 4 ? 16 : 8; }
+int dct_max_lines(int elem_bytes, int split) { return split ? 8 : elem_bytes == 4 ? 16 : 8; }
 
 size_t dct_smem_bytes(int n, int elem_bytes, int warps, int split) {
   return (size_t)2 * elem_bytes * (2 * (size_t)n + (size_t)warps * xfft_line(n, split));

@@ -218,7 +218,7 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
 /* ---- launch shapes and the autotuner ----
  * tiles[5 to 10] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS
  * block 32 x rhs_by), dct_nw (complex lines per CTA of the forward DCT, up
- * to 16 in the mixed form and 8 in FP64),
+ * to 16 in the mixed form (8 with the two-pass x transforms) and 8 in FP64),
  * dftz_rk (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection
  * block 32 x proj_by), zdft (mixed form, where M/2+1 <= 96: 1 = FP32 direct
  * sums, 2 = mma.sync TF32 tensor cores, 3 = tcgen05 tensor cores with the
