@@ -174,13 +174,15 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 
 // the sticky device flag of the step kernels (stream already synchronized);
 // bit 2: a TMA copy of the tensor-core z transform missed its wait limit;
-// bit 4: one of the tiled y-solve; bit 8: one of the tcgen05 z transform
+// bit 4: one of the tiled y-solve; bit 8: one of the tcgen05 z transform;
+// bit 16: a row copy of the two-pass inverse x transform
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
   if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
   if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
   if (f & 8) return set_err(ctx, BLGPU_EDEVICE, "z transform (tcgen05): a copy or a product missed its wait limit");
+  if (f & 16) return set_err(ctx, BLGPU_EDEVICE, "inverse x transform: a row copy did not complete within the wait limit");
   if (f) return set_err(ctx, BLGPU_EDEVICE, "device flag %d set by a step kernel", f);
   return BLGPU_OK;
 }
@@ -904,7 +906,8 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
-  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->tiles.xfft, ctx->st);
+  launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->tiles.xfft,
+                 &ctx->sc->err, ctx->st);
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);

@@ -169,7 +169,8 @@ void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl,
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, int xfft,
+// err: device flag, bit 16 set when a row copy of the two-pass kernel missed its wait limit
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, int xfft, int *err,
                  cudaStream_t st);
 // shared memory of a DCT CTA of `lines` warps; split: that of xfft_split, 0 for the Stockham kernels
 size_t dct_smem_bytes(int n, int elem_bytes, int lines, int split);

@@ -18,6 +18,7 @@
 //               z-periodic copies of apply_periodic_z_pressure
 //               (projection.f90:295-303).
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace blgpu {
 
@@ -408,7 +409,8 @@ template <typename T, int MAXR> struct StockhamX {
 // Two-pass: N = A B (A, B <= 32), one buffer of max(N, A (B | 1)) values;
 // the table holds W_N^{n2 k1} at [k1][n2] (row pitch B)
 template <int A, int B> struct TwoPassX {
-  static constexpr int N = A * B, SB = B | 1, LINE = N > A * SB ? N : A * SB;
+  // LINE even keeps every line buffer 16-byte aligned
+  static constexpr int N = A * B, SB = B | 1, LINE = ((N > A * SB ? N : A * SB) + 1) & ~1;
   static_assert(A <= 32 && B <= 32, "one lane per butterfly");
   // up to 8 lines per CTA and three CTAs of 8 per SM: 80 registers, which
   // hold the 29-point pass without spills and leave room for 24 warps per SM
@@ -487,8 +489,13 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_div_dct(Geo g
   T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
   T2<T> *post = tw + N;
   T2<T> *bufA = post + N + (size_t)warp * E::dline(N);
+  // FP32: the reciprocal x spacings of the points, N rounded up to 4
+  const int N4 = (N + 3) & ~3;
+  float *rfx = reinterpret_cast<float *>(post + N + (size_t)nw * E::dline(N));
   E::fill(tw, pl, threadIdx.x, blockDim.x);
   for (int t = threadIdx.x; t < N; t += blockDim.x) post[t] = pl.post[t];
+  if (sizeof(T) == 4)
+    for (int t = threadIdx.x; t < N4; t += blockDim.x) rfx[t] = t < N ? (float)g.ax.rF[t + 2] : 0.f;
   __syncthreads();
   const int nlines = s.NM * s.M;
   const int q = (blockIdx.x * nw + warp) * 2;
@@ -500,8 +507,65 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_div_dct(Geo g
   // line B aliases line A when it does not exist, so every load is valid
   const long long cbb = hb ? cb : ca;
   const int jb = hb ? bb + 2 : ba + 2, kbb = hb ? kb + 2 : ka + 2;
+  const bool vec = sizeof(T) == 4 &&
+                   ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(W)) &
+                    15) == 0 && (g.px & 3) == 0;
+  if constexpr (sizeof(T) == 4) {
+    if (vec) {
+      // four consecutive points per lane, 16-byte loads (the box rows start
+      // 16-byte aligned at i = 2); U at i-1 of the first point comes from the
+      // previous lane, or from the previous round for lane 0
+      const float ryA = (float)g.ay.rF[ba + 2], rzA = (float)g.az.rF[ka + 2];
+      const float ryB = (float)g.ay.rF[jb], rzB = (float)g.az.rF[kbb];
+      float carA = __ldg(U + ca - 1), carB = __ldg(U + cbb - 1);
+      for (int base = 0; base < N; base += 128) {
+        const int i4 = base + 4 * lane, ic = i4 < N4 ? i4 : N4 - 4;  // in-row address for idle lanes
+        const float4 rx = *reinterpret_cast<const float4 *>(rfx + ic);
+        float fa[4], fb[4];
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+          const long long c = (l ? cbb : ca) + ic;
+          const float4 u = __ldg(reinterpret_cast<const float4 *>(U + c));
+          const float4 v = __ldg(reinterpret_cast<const float4 *>(V + c));
+          const float4 vm = __ldg(reinterpret_cast<const float4 *>(V + c - g.px));
+          const float4 w = __ldg(reinterpret_cast<const float4 *>(W + c));
+          const float4 wm = __ldg(reinterpret_cast<const float4 *>(W + c - g.plane));
+          float um0 = __shfl_up_sync(0xffffffffu, u.w, 1);
+          const float car = l ? carB : carA;
+          if (lane == 0) um0 = car;
+          const float nc = __shfl_sync(0xffffffffu, u.w, 31);
+          if (l) carB = nc;
+          else carA = nc;
+          const float ry = l ? ryB : ryA, rz = l ? rzB : rzA;
+          float *f = l ? fb : fa;
+          // projection.f90:42-44, as div_at
+          f[0] = (u.x - um0) * rx.x + (v.x - vm.x) * ry + (w.x - wm.x) * rz;
+          f[1] = (u.y - u.x) * rx.y + (v.y - vm.y) * ry + (w.y - wm.y) * rz;
+          f[2] = (u.z - u.y) * rx.z + (v.z - vm.z) * ry + (w.z - wm.z) * rz;
+          f[3] = (u.w - u.z) * rx.w + (v.w - vm.w) * ry + (w.w - wm.w) * rz;
+        }
+        if (!hb) fb[0] = fb[1] = fb[2] = fb[3] = 0.f;
+        if (i4 + 3 < N && (N & 1) == 0) {
+          // points i4, i4+2 go to the adjacent slots i4/2, i4/2+1; points
+          // i4+3, i4+1 to N-2-i4/2, N-1-i4/2
+          float *b = reinterpret_cast<float *>(bufA);
+          *reinterpret_cast<float4 *>(b + i4) = make_float4(fa[0], fb[0], fa[2], fb[2]);
+          *reinterpret_cast<float4 *>(b + 2 * (N - 2 - i4 / 2)) = make_float4(fa[3], fb[3], fa[1], fb[1]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int ip = i4 + e;
+            if (ip < N) {
+              const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
+              bufA[pos] = mk<T>(fa[e], fb[e]);
+            }
+          }
+        }
+      }
+    }
+  }
   // batches of 4 points per lane: all 48 loads issued before any use
-  for (int base = 0; base < N; base += 128) {
+  for (int base = 0; base < N && !vec; base += 128) {
     T fa[4], fb[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -590,6 +654,108 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_idct(Geo g, S
       if (hb) {
         p[cb + N] = vb;
         if (kb == 0) p[cb + N + zsh] = vb;
+      }
+    }
+  }
+}
+
+// Inverse DCT with the two-pass FFT (FP32), the steps around the transform
+// folded into its passes: one bulk copy brings the two rows of R into the
+// line buffer; pass 1 forms its inputs Z_n = V_A + i V_B from them in
+// registers; pass 2 writes its outputs from registers straight to the box
+// positions (Z_n holds the points i = 2n, or 2N-1-2n for 2n >= N).  The
+// copy's wait is bounded: when it runs out, bit 16 of the device flag is set
+// and the line is left unwritten.
+template <int A, int B>
+__global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> pl, const float *__restrict__ R,
+                                                  float *__restrict__ p, int *__restrict__ err) {
+  using E = TwoPassX<A, B>;
+  using namespace tma;
+  constexpr int N = E::N, SB = E::SB, LINE = E::LINE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  float2 *tw = reinterpret_cast<float2 *>(smem_raw);
+  float2 *post = tw + N;
+  float2 *buf = post + N + (size_t)warp * LINE;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(
+      reinterpret_cast<unsigned char *>(post + N + (size_t)nw * LINE) + 4 * ((N + 3) / 4 * 4)) + warp;
+  E::fill(tw, pl, threadIdx.x, blockDim.x);
+  for (int t = threadIdx.x; t < N; t += blockDim.x) post[t] = pl.post[t];
+  const int nlines = s.NM * s.M;
+  const int q = (blockIdx.x * nw + warp) * 2;
+  const bool hb = q + 1 < nlines;
+  if (lane == 0 && q < nlines) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+    // rows q and q+1 (rx apart) as one block, the length rounded up to 16 bytes
+    const uint32_t bytes = 4u * (uint32_t)((hb ? s.rx : 0) + ((N + 3) & ~3));
+    mbar_expect_tx(bar, bytes);
+    bulk_load(buf, R + (long long)q * s.rx, bytes, bar);
+  }
+  __syncthreads();
+  if (q >= nlines) return;
+  if (!__all_sync(0xffffffffu, mbar_wait(bar, 0))) {
+    if (lane == 0) {
+      atomicOr(err, 16);
+      mbar_wait(bar, 0);  // let the copy finish (bounded) before leaving
+    }
+    return;
+  }
+  const float *ra = reinterpret_cast<const float *>(buf);
+  const float *rb = ra + s.rx;
+  {
+    // pass 1 (lane n2 < B): Z_n for n = B n1 + n2, V_n = exp(+i pi n/2N) (X_n - i X_{N-n})
+    float2 x[A];
+    if (lane < B) {
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) {
+        const int n = B * n1 + lane;
+        const float xa = ra[n], xan = n ? ra[N - n] : 0.f;
+        const float xb = hb ? rb[n] : 0.f, xbn = (hb && n) ? rb[N - n] : 0.f;
+        const float2 e = make_float2(post[n].x, -post[n].y);
+        const float2 va = cmul<float>(e, make_float2(xa, -xan));
+        const float2 vb = cmul<float>(e, make_float2(xb, -xbn));
+        x[n1] = make_float2(va.x - vb.y, va.y + vb.x);
+      }
+      dft_reg<A, true>(x);
+#pragma unroll
+      for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<float, true>(x[k1], tw[k1 * B + lane]);
+    }
+    __syncwarp();  // every read of the raw rows is done
+    if (lane < B) {
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) buf[k1 * SB + lane] = x[k1];
+    }
+    __syncwarp();
+  }
+  if (lane < A) {
+    float2 y[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) y[n2] = buf[lane * SB + n2];
+    dft_reg<B, true>(y);
+    const float inv = 1.0f / (float)N;
+    const int ba = q / s.M, ka = q - ba * s.M;
+    const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
+    const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
+    const long long zsh = (long long)s.M * g.plane;  // k = 2 -> k = nzp+2
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) {
+      const int n = lane + A * k2;
+      const int ip = 2 * n < N ? 2 * n : 2 * N - 1 - 2 * n;
+      const float va = y[k2].x * inv, vb = y[k2].y * inv;
+      p[ca + ip] = va;
+      if (ka == 0) p[ca + ip + zsh] = va;
+      if (hb) {
+        p[cb + ip] = vb;
+        if (kb == 0) p[cb + ip + zsh] = vb;
+      }
+      if (ip == N - 1) {  // i = nxg-1 copy
+        p[ca + N] = va;
+        if (ka == 0) p[ca + N + zsh] = va;
+        if (hb) {
+          p[cb + N] = vb;
+          if (kb == 0) p[cb + N + zsh] = vb;
+        }
       }
     }
   }
@@ -1021,7 +1187,7 @@ int xfft_split(int n) {
 static size_t xfft_line(int n, int split) {
   if (!split) return 2 * (size_t)n;
   const int B = n / split, SB = B | 1;
-  return (size_t)(n > split * SB ? n : split * SB);
+  return (size_t)(((n > split * SB ? n : split * SB) + 1) & ~1);
 }
 
 int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
@@ -1044,8 +1210,11 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
 
 int dct_max_lines(int elem_bytes, int split) { return split ? 8 : elem_bytes == 4 ? 16 : 8; }
 
+// twiddle and DCT tables, the line buffers, the x reciprocal spacings as
+// FP32 (forward) and one mbarrier per line (inverse, two-pass)
 size_t dct_smem_bytes(int n, int elem_bytes, int warps, int split) {
-  return (size_t)2 * elem_bytes * (2 * (size_t)n + (size_t)warps * xfft_line(n, split));
+  return (size_t)2 * elem_bytes * (2 * (size_t)n + (size_t)warps * xfft_line(n, split)) +
+         4 * (size_t)((n + 3) / 4 * 4) + 8 * (size_t)warps;
 }
 
 // Register-resident odd butterflies raise the register count of the whole
@@ -1100,8 +1269,21 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
   }
 }
 
+template <int A, int B>
+static void launch_idct2(const Geo &g, const Spec &s, const FftPlan<float> &pl, const float *R, float *p, int nw,
+                         size_t sm, int grid, int *err, cudaStream_t st) {
+  cudaFuncSetAttribute(k_idct2<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_idct2<A, B>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  k_idct2<A, B><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p, err);
+}
+
+// the two rows of the bulk copy fit one line buffer of the two-pass kernel
+static bool idct2_fits(const Spec &s, int split) {
+  return (size_t)s.rx + (size_t)((s.N + 3) & ~3) <= 2 * xfft_line(s.N, split) && s.rx % 4 == 0;
+}
+
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft,
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft, int *err,
                  cudaStream_t st) {
   const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true, split);
@@ -1109,6 +1291,9 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;
   if constexpr (sizeof(T) == 4) {
+    const bool fused = idct2_fits(s, split) && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
+    if (split == 29 && fused) return launch_idct2<29, 28>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 17 && fused) return launch_idct2<17, 30>(g, s, pl, R, p, nw, sm, grid, err, st);
     if (split == 29) return launch_idct_e<T, TwoPassX<29, 28>>(g, s, pl, R, p, nw, sm, grid, st);
     if (split == 17) return launch_idct_e<T, TwoPassX<17, 30>>(g, s, pl, R, p, nw, sm, grid, st);
   }
@@ -1167,7 +1352,7 @@ void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm
 #define BLGPU_SPEC_INST(T)                                                                                        \
   template void launch_div_dct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, const T *, const T *, \
                                   T *, int, int, cudaStream_t);                                                   \
-  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, int,          \
+  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, int, int *,   \
                                cudaStream_t);                                                                    \
   template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
   template void launch_thomas<T>(const Spec &, T2<T> *, const double *, const double *, const double *,          \

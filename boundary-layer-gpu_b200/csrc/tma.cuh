@@ -74,6 +74,14 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
+// untiled bulk copy global -> shared (both addresses 16-byte aligned, bytes
+// a multiple of 16), completion counted on the mbarrier
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 // 2D tiled store from shared memory (coordinates in range, never negative)
 __device__ __forceinline__ void store_2d(const CUtensorMap *map, const void *src, int x, int y) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
