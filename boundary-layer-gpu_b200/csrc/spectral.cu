@@ -1053,7 +1053,7 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
   }
 }
 
-template <typename T>
+template <typename T, int PF>
 __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, const double *__restrict__ piv,
                                                 const double *__restrict__ dl, const double *__restrict__ du,
                                                 double *__restrict__ H0, int klow) {
@@ -1069,19 +1069,35 @@ __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, c
   if (H0 && kz == 0 && kx < klow) {
     const T *Cr = reinterpret_cast<const T *>(C + base);  // real part of row b at Cr[2 b rs]
     double *Hd = H0 + kx;                                   // H0[b * klow + kx]
+    // rows in batches of PB, every load of a batch issued before its first
+    // use (one CTA runs this path; unbatched it would be the kernel's tail);
+    // PB = 8 keeps the kernel's register count that of the main path
+    constexpr int PB = 8;
     double g = 0.0, rprev = 0.0;
-    for (int b = 0; b < NM; ++b) {
-      double r = (double)Cr[2 * (long long)b * rs];
-      if (b > 0) {
-        const double w = dl[b] * rprev;
-        r = r - w * g;
+    for (int b0 = 0; b0 < NM; b0 += PB) {
+      double rv[PB], pvv[PB];
+#pragma unroll
+      for (int u = 0; u < PB; ++u) {
+        const int b = b0 + u;
+        rv[u] = b < NM ? (double)Cr[2 * (long long)b * rs] : 0.0;
+        pvv[u] = b < NM ? piv[base + b * rs] : 0.0;
       }
-      rprev = piv[base + b * rs];
-      g = r;
-      Hd[(long long)b * klow] = r;
+#pragma unroll
+      for (int u = 0; u < PB; ++u) {
+        const int b = b0 + u;
+        if (b < NM) {
+          double r = rv[u];
+          if (b > 0) {
+            const double w = dl[b] * rprev;
+            r = r - w * g;
+          }
+          rprev = pvv[u];
+          g = r;
+          Hd[(long long)b * klow] = r;
+        }
+      }
     }
     double x = 0.0;
-    constexpr int PB = 8;
     for (int b0 = NM - 1; b0 >= 0; b0 -= PB) {
       double hv[PB], pvv[PB];
 #pragma unroll
@@ -1102,7 +1118,7 @@ __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, c
     for (int b = 0; b < NM; ++b) C[base + b * rs] = mk<T>((T)0, (T)0);
     return;
   }
-  thomas_sweeps<T, (sizeof(T) == 4 ? 12 : 16)>(C + base, piv + base, rs, NM, dl, du);
+  thomas_sweeps<T, PF>(C + base, piv + base, rs, NM, dl, du);
 }
 
 // ---------------------------------------------------------------------------
@@ -1334,8 +1350,10 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 template <typename T>
 void launch_thomas(const Spec &s, T2<T> *C, const double *piv, const double *dl, const double *du, double *H0,
                    int klow, cudaStream_t st) {
+  // rows in flight per thread: 12 in FP32 (80 registers; 4, 6 and 8 measured
+  // slower at 814 x 257 x 193), 16 in FP64
   dim3 grid((s.N + 127) / 128, s.MH);  // 128 kx of one kz per CTA
-  k_thomas<T><<<grid, 128, 0, st>>>(s, C, piv, dl, du, H0, klow);
+  k_thomas<T, sizeof(T) == 4 ? 12 : 16><<<grid, 128, 0, st>>>(s, C, piv, dl, du, H0, klow);
 }
 
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
