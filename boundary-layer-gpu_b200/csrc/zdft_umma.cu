@@ -7,8 +7,8 @@
 // three-term TF32 split hi*hi + hi*lo + lo*hi); see there for the algebra.
 //
 // One persistent CTA (8 warps) per SM.  Work items are (row b, 32 kx
-// columns).  Per item: one TMA tensor copy brings the raw columns (double
-// buffer, one item ahead); the CTA splits them into the B operands (double
+// columns).  Per item: one TMA tensor copy brings the raw columns (NRAW
+// buffers, NRAW-1 items ahead); the CTA splits them into the B operands (double
 // buffer); one thread issues the 3 x Q/8 x 2 MMAs of M = 128, N = 32, K = 8
 // into one of two accumulator pairs and commits them to an mbarrier; while
 // they run, the CTA reads the previous item's accumulators with tcgen05.ld
@@ -32,6 +32,7 @@ namespace {
 constexpr int UN = 32;        // kx columns per work item = N of the MMA
 constexpr int UWARPS = 8;     // warps per CTA
 constexpr int UTHREADS = UWARPS * 32;
+constexpr int NRAW = 2;       // raw column buffers: copies of the next NRAW-1 items in flight (3 measured slower)
 
 __device__ __forceinline__ uint32_t u_tf32_rna(float x) {
   uint32_t r;
@@ -113,7 +114,7 @@ __host__ __device__ inline uint32_t u_otile_bytes(int M, int MH) {
 __device__ __forceinline__ uint32_t sw128(int r, int c) { return ((uint32_t)r << 7) + ((uint32_t)((c ^ r) & 7) << 4); }
 
 // Shared memory, from a 1 KB aligned base: B[2 buffers][4 operands][Q/8
-// K-steps of 1 KB] | raw[2][rawf floats] | aux[2][2][32] | output tiles[2]
+// K-steps of 1 KB] | raw[NRAW][rawf floats] | aux[2][2][32] | output tiles[2]
 // (1 KB aligned) | 4 mbarriers | tmem slot and failure flag.
 template <int QP>
 __global__ void __launch_bounds__(UTHREADS, 1)
@@ -129,8 +130,8 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   const uint32_t s0 = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
   unsigned char *Bb = sm;                                          // 2 x 4 x OPB
-  float *raw0 = reinterpret_cast<float *>(sm + 8 * OPB);           // [2][rawf]
-  float *aux = raw0 + 2 * (size_t)rawf;                            // [2][2][UN]
+  float *raw0 = reinterpret_cast<float *>(sm + 8 * OPB);           // [NRAW][rawf]
+  float *aux = raw0 + NRAW * (size_t)rawf;                         // [2][2][UN]
   // output tiles [2][otb bytes], 1 KB aligned (128-byte swizzle): forward two
   // halves of MH rows x 16 complex, inverse M rows x 32 values, 128 B a row
   const uint32_t ohb = ((uint32_t)s.MH * 128u + 1023u) & ~1023u;  // one forward half
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   unsigned char *ot0 = reinterpret_cast<unsigned char *>(aux + 4 * UN);
   ot0 += (1024u - (smem_u32(ot0) & 1023u)) & 1023u;
   uint64_t *tbar = reinterpret_cast<uint64_t *>(ot0 + 2 * otb);    // TMA, per raw buffer
-  uint64_t *mbar = tbar + 2;                                       // MMA, per accumulator pair
+  uint64_t *mbar = tbar + NRAW;                                    // MMA, per accumulator pair
   uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);         // tensor-memory base
   int *fail_s = reinterpret_cast<int *>(slot + 1);                  // a warp's wait ran out
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
@@ -164,12 +165,12 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   }
   if (tid == 32) {
     *fail_s = 0;
-    mbar_init(&tbar[0], 1);
-    mbar_init(&tbar[1], 1);
+    for (int q = 0; q < NRAW; ++q) mbar_init(&tbar[q], 1);
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     mbar_init_fence();
-    if ((int)blockIdx.x < nitems) issue_copy(blockIdx.x, 0);
+    for (int q = 0; q < NRAW - 1; ++q)
+      if ((int)blockIdx.x + q * G < nitems) issue_copy(blockIdx.x + q * G, q);
   }
   tc_fence_before();
   __syncthreads();
@@ -267,8 +268,8 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   for (int i = 0; i < nmine && !failed; ++i) {
     const int item = blockIdx.x + i * G, bb = i & 1;
     const int kx0 = (item % ntile) * UN;
-    // the other raw buffer and this item's B buffer are free: their last
-    // readers (staging of item i-1, MMAs of item i-2) finished before here
+    // raw buffer (i-1) mod NRAW and this item's B buffer are free: their
+    // last readers (staging of item i-1, MMAs of item i-2) finished before here
     if (__syncthreads_or(*fail_s)) {
       failed = true;
       break;
@@ -280,11 +281,12 @@ __global__ void __launch_bounds__(UTHREADS, 1)
       store_commit();
       store_wait_read<1>();
     }
-    if (tid == 32 && i + 1 < nmine) {
+    const int rb = i % NRAW;
+    if (tid == 32 && i + NRAW - 1 < nmine) {
       fence_async_shared();
-      issue_copy(item + G, bb ^ 1);
+      issue_copy(item + (NRAW - 1) * G, (i + NRAW - 1) % NRAW);
     }
-    const bool ok = mbar_wait_hw(&tbar[bb], (uint32_t)(i >> 1) & 1u);
+    const bool ok = mbar_wait_hw(&tbar[rb], (uint32_t)(i / NRAW) & 1u);
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     // ---- split the operands of item i into B[bb] ----
     // a thread takes column n and four consecutive rows k = 4 k4 .. 4 k4 + 3
     // and writes one 16-byte chunk per operand
-    const float *rw = raw0 + (size_t)bb * rawf;
+    const float *rw = raw0 + (size_t)rb * rawf;
     unsigned char *Bi = Bb + (size_t)bb * 4 * OPB;
     const int n = lane, col = kx0 + n;
     const bool okc = col < s.N;
@@ -382,10 +384,8 @@ __global__ void __launch_bounds__(UTHREADS, 1)
     // let the copies and products this CTA issued finish (bounded), then leave
     if (tid == 0) {
       atomicOr(err, 8);
-      for (int q = 0; q < 2; ++q) {
-        mbar_wait(&mbar[q], 0);
-        mbar_wait(&tbar[q], 0);
-      }
+      for (int q = 0; q < 2; ++q) mbar_wait(&mbar[q], 0);
+      for (int q = 0; q < NRAW; ++q) mbar_wait(&tbar[q], 0);
     }
   }
   tc_fence_before();
@@ -403,8 +403,8 @@ int u_raw_floats(const Spec &s) {
 }
 size_t u_smem_bytes(const Spec &s, int qp) {
   // the output tiles start at the next 1 KB boundary after aux (at most 1 KB on)
-  return 1024 + (size_t)8 * (qp / 8) * 1024 + (size_t)2 * u_raw_floats(s) * sizeof(float) + 4 * UN * sizeof(float) +
-         1024 + 2 * (size_t)u_otile_bytes(s.M, s.MH) + 4 * sizeof(uint64_t) +
+  return 1024 + (size_t)8 * (qp / 8) * 1024 + (size_t)NRAW * u_raw_floats(s) * sizeof(float) +
+         4 * UN * sizeof(float) + 1024 + 2 * (size_t)u_otile_bytes(s.M, s.MH) + (NRAW + 2) * sizeof(uint64_t) +
          16;  // the last 16: tensor-memory slot and failure flag
 }
 uint32_t tf32_host_rna(float x) {
