@@ -56,6 +56,27 @@ __device__ __forceinline__ bool mbar_wait_hw(uint64_t *bar, uint32_t parity) {
   }
   return false;
 }
+// plain arrival (count one) on an mbarrier
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// hardware-suspended wait that also gives up when *fail is set by another
+// thread of the CTA (checked every 64 tries) or after WAIT_LIMIT tries (then
+// it sets *fail); false when it gave up
+__device__ __forceinline__ bool mbar_wait_or_fail(uint64_t *bar, uint32_t parity, volatile int *fail) {
+  for (int it = 0; it < WAIT_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 63) == 63 && *fail) return false;
+  }
+  *fail = 1;
+  return false;
+}
 // generic-proxy shared-memory accesses before async-proxy ones (TMA)
 __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -6,17 +6,20 @@
 // two square products of order Q = M/2+1 with the f_k +- f_{M-k} pairing,
 // three-term TF32 split hi*hi + hi*lo + lo*hi); see there for the algebra.
 //
-// One persistent CTA (8 warps) per SM.  Work items are (row b, 32 kx
-// columns).  Per item: one TMA tensor copy brings the raw columns (NRAW
-// buffers, NRAW-1 items ahead); the CTA splits them into the B operands (double
-// buffer); one thread issues the 3 x Q/8 x 2 MMAs of M = 128, N = 32, K = 8
-// into one of two accumulator pairs and commits them to an mbarrier; while
-// they run, the CTA reads the previous item's accumulators with tcgen05.ld
-// and writes that item's output rows.  Tensor memory: 4 Q columns of tables
-// (cos hi, cos lo, -sin hi, -sin lo; lane = output row) and 2 x 2 x 32
-// accumulator columns (256 or 512 allocated).  Every wait is bounded; a wait that
-// runs out sets bit 8 of the device flag and the CTA releases its tensor
-// memory and leaves.
+// One persistent CTA (12 warps) per SM, warp-specialised.  Work items are
+// (row b, 32 kx columns).  A producer thread brings the raw columns of the
+// coming items by TMA tensor copies (NRAW buffers); four warps split them
+// into the B operands (NB buffers); one thread issues the 3 x Q/8 x 2 MMAs
+// of M = 128, N = 32, K = 8 into one of NACC accumulator pairs and commits
+// them to mbarriers; four warps read the accumulators with tcgen05.ld and
+// write 128-byte-swizzled output tiles, which one thread stores by TMA.  All
+// stages run concurrently on successive items, handing slots over through
+// full / empty mbarrier rings.  Tensor memory: 4 Q columns of tables (cos
+// hi, cos lo, -sin hi, -sin lo; lane = output row) and NACC x 2 x 32
+// accumulator columns (256 or 512 allocated).  Every wait is bounded and
+// gives up as soon as another thread of the CTA has given up; then bit 8 of
+// the device flag is set and the CTA drains its copies and products
+// (bounded), releases its tensor memory and leaves.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -30,9 +33,7 @@ using namespace tma;
 
 namespace {
 constexpr int UN = 32;        // kx columns per work item = N of the MMA
-constexpr int UWARPS = 8;     // warps per CTA
-constexpr int UTHREADS = UWARPS * 32;
-constexpr int NRAW = 2;       // raw column buffers: copies of the next NRAW-1 items in flight (3 measured slower)
+constexpr int NRAW = 3;       // raw column buffers: copies of the next NRAW-1 items in flight
 
 __device__ __forceinline__ uint32_t u_tf32_rna(float x) {
   uint32_t r;
@@ -113,50 +114,52 @@ __host__ __device__ inline uint32_t u_otile_bytes(int M, int MH) {
 // byte offset of 16-byte chunk c of row r in a 128-byte-swizzled tile
 __device__ __forceinline__ uint32_t sw128(int r, int c) { return ((uint32_t)r << 7) + ((uint32_t)((c ^ r) & 7) << 4); }
 
-// Shared memory, from a 1 KB aligned base: B[2 buffers][4 operands][Q/8
-// K-steps of 1 KB] | raw[NRAW][rawf floats] | aux[2][2][32] | output tiles[2]
-// (1 KB aligned) | 4 mbarriers | tmem slot and failure flag.
+// Warp roles (12 warps): warp 0 lane 0 issues the TMA copies of the raw
+// columns, warp 1 lane 0 the MMAs, warp 2 lane 0 the TMA stores of the
+// output tiles; warps 4-7 split raw columns into B operands, warps 8-11 (one
+// per 32 tensor-memory lanes) read the accumulators and write the output
+// tiles.  Every hand-off is an mbarrier ring: raw (NRAW), B (NB), accumulator
+// pairs (NACC), output tiles (NOUT), each with a "full" and an "empty"
+// barrier; a producer waits for the empty phase before reusing a slot.
+constexpr int NB = 2, NACC = 2, NOUT = 2;
+constexpr int WS_WARPS = 12, WS_THREADS = WS_WARPS * 32;
+
+// Shared memory, from a 1 KB aligned base: B[NB][4 operands][Q/8 K-steps of
+// 1 KB] | raw[NRAW][rawf floats] | output tiles[NOUT] (1 KB aligned) |
+// mbarriers | tmem slot and failure flag.
 template <int QP>
-__global__ void __launch_bounds__(UTHREADS, 1)
+__global__ void __launch_bounds__(WS_THREADS, 1)
     k_zdft_umma(const __grid_constant__ CUtensorMap mapR, const __grid_constant__ CUtensorMap mapC,
                 const __grid_constant__ CUtensorMap mapRs, const __grid_constant__ CUtensorMap mapCs, Spec s,
                 const uint32_t *__restrict__ tab, int inverse, int rawf, int *__restrict__ err) {
-  constexpr int KS = QP / 8;                 // K steps (1 KB of B each) per product
+  constexpr int KS = QP / 8;                    // K steps (1 KB of B each) per product
   constexpr uint32_t OPB = (uint32_t)KS << 10;  // bytes of one B operand
   // tensor-memory columns: tables and accumulators, rounded up to a power of two
-  constexpr uint32_t TCOLS = (4 * QP + 4 * UN) <= 256 ? 256u : 512u;
+  constexpr uint32_t TCOLS = (4 * QP + 2 * NACC * UN) <= 256 ? 256u : 512u;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1 KB alignment of the B operands
   const uint32_t s0 = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
-  unsigned char *Bb = sm;                                          // 2 x 4 x OPB
-  float *raw0 = reinterpret_cast<float *>(sm + 8 * OPB);           // [NRAW][rawf]
-  float *aux = raw0 + NRAW * (size_t)rawf;                         // [2][2][UN]
-  // output tiles [2][otb bytes], 1 KB aligned (128-byte swizzle): forward two
-  // halves of MH rows x 16 complex, inverse M rows x 32 values, 128 B a row
+  unsigned char *Bb = sm;                                          // NB x 4 x OPB
+  float *raw0 = reinterpret_cast<float *>(sm + NB * 4 * OPB);      // [NRAW][rawf]
   const uint32_t ohb = ((uint32_t)s.MH * 128u + 1023u) & ~1023u;  // one forward half
   const uint32_t otb = u_otile_bytes(s.M, s.MH);
-  unsigned char *ot0 = reinterpret_cast<unsigned char *>(aux + 4 * UN);
+  unsigned char *ot0 = reinterpret_cast<unsigned char *>(raw0 + NRAW * (size_t)rawf);
   ot0 += (1024u - (smem_u32(ot0) & 1023u)) & 1023u;
-  uint64_t *tbar = reinterpret_cast<uint64_t *>(ot0 + 2 * otb);    // TMA, per raw buffer
-  uint64_t *mbar = tbar + NRAW;                                    // MMA, per accumulator pair
-  uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);         // tensor-memory base
-  int *fail_s = reinterpret_cast<int *>(slot + 1);                  // a warp's wait ran out
+  uint64_t *raw_full = reinterpret_cast<uint64_t *>(ot0 + NOUT * otb);
+  uint64_t *raw_empty = raw_full + NRAW;
+  uint64_t *b_full = raw_empty + NRAW, *b_empty = b_full + NB;
+  uint64_t *acc_full = b_empty + NB, *acc_empty = acc_full + NACC;
+  uint64_t *out_full = acc_empty + NACC, *out_empty = out_full + NOUT;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(out_empty + NOUT);  // tensor-memory base
+  volatile int *fail_s = reinterpret_cast<volatile int *>(slot + 1);  // a wait ran out
   const int M = s.M, MH = s.MH, H = (M - 1) / 2;
   const bool even = (M & 1) == 0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntile = (s.N + UN - 1) / UN;
   const int nitems = s.NM * ntile;
   const int G = gridDim.x;
-  const uint32_t box_bytes = inverse ? (uint32_t)MH * 2 * UN * 4 : (uint32_t)M * UN * 4;
-  auto issue_copy = [&](int item, int buf) {
-    const int b = item / ntile, kx0 = (item % ntile) * UN;
-    float *dst = raw0 + (size_t)buf * rawf;
-    mbar_expect_tx(&tbar[buf], box_bytes);
-    if (inverse) load_2d(dst, &mapC, 2 * kx0, b * MH, &tbar[buf]);
-    else load_2d(dst, &mapR, kx0, b * M, &tbar[buf]);
-  };
-  // ---- set-up: tensor memory, barriers, first copy, tables ----
+  const int nmine = ((int)blockIdx.x < nitems) ? (nitems - 1 - (int)blockIdx.x) / G + 1 : 0;
+  // ---- set-up: tensor memory, barriers, tables ----
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
                  "r"(TCOLS)
@@ -165,191 +168,73 @@ __global__ void __launch_bounds__(UTHREADS, 1)
   }
   if (tid == 32) {
     *fail_s = 0;
-    for (int q = 0; q < NRAW; ++q) mbar_init(&tbar[q], 1);
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
+    for (int q = 0; q < NRAW; ++q) {
+      mbar_init(&raw_full[q], 1);
+      mbar_init(&raw_empty[q], 4);
+    }
+    for (int q = 0; q < NB; ++q) {
+      mbar_init(&b_full[q], 4);
+      mbar_init(&b_empty[q], 1);
+    }
+    for (int q = 0; q < NACC; ++q) {
+      mbar_init(&acc_full[q], 1);
+      mbar_init(&acc_empty[q], 4);
+    }
+    for (int q = 0; q < NOUT; ++q) {
+      mbar_init(&out_full[q], 4);
+      mbar_init(&out_empty[q], 1);
+    }
     mbar_init_fence();
-    for (int q = 0; q < NRAW - 1; ++q)
-      if ((int)blockIdx.x + q * G < nitems) issue_copy(blockIdx.x + q * G, q);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *slot;
-  const uint32_t tab_col = 0, acc_col = 4 * QP;  // tables, then the accumulators
-  const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
-  {
+  const uint32_t tab_col = 0, acc_col = 4 * QP;  // tables, then the accumulator pairs
+  if (warp >= 8) {
     // table t (0 cos hi, 1 cos lo, 2 -sin hi, 3 -sin lo) in columns t*QP.. of
-    // lane = output row; the two warps of a lane quarter take two tables each
+    // lane = output row, by the warp of that lane quarter
     const int row = 32 * (warp & 3) + lane;
-    for (int t = 2 * (warp >> 2); t < 2 * (warp >> 2) + 2; ++t)
+    const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+    for (int t = 0; t < 4; ++t)
       for (int c0 = 0; c0 < QP; c0 += 16) {
         uint32_t r[16];
         const uint32_t *src = tab + ((size_t)t * 128 + row) * QP + c0;
 #pragma unroll
         for (int j = 0; j < 16; ++j) r[j] = src[j];
-        tmem_st16(tmem + lane_base + tab_col + t * QP + c0, r);
+        tmem_st16(tmem + lb + tab_col + t * QP + c0, r);
       }
     tmem_wait_st();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const int nmine = ((int)blockIdx.x < nitems) ? (nitems - 1 - (int)blockIdx.x) / G + 1 : 0;
-  bool failed = false;
-  // epilogue of local item j (accumulator pair j & 1, output tile j & 1):
-  // each warp waits for the products itself (the issuing warp does not hold
-  // the others back) and moves its rows from tensor memory into the swizzled
-  // output tile; the tile leaves by TMA store, issued after the next barrier
-  auto epilogue = [&](int j) {
-    const int bb = j & 1;
-    if (!mbar_wait_hw(&mbar[bb], (uint32_t)(j >> 1) & 1u)) {
-      atomicExch(fail_s, 1);
-      return;
+  int issued_loads = 0, issued_mma = 0;  // for the bounded drain after a failure
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: raw columns of item i into raw[i % NRAW] ----
+    const uint32_t box_bytes = inverse ? (uint32_t)MH * 2 * UN * 4 : (uint32_t)M * UN * 4;
+    for (int i = 0; i < nmine; ++i) {
+      const int r = i % NRAW;
+      if (!mbar_wait_or_fail(&raw_empty[r], ((uint32_t)(i / NRAW) & 1u) ^ 1u, fail_s)) break;
+      const int item = blockIdx.x + i * G;
+      const int b = item / ntile, kx0 = (item % ntile) * UN;
+      float *dst = raw0 + (size_t)r * rawf;
+      mbar_expect_tx(&raw_full[r], box_bytes);
+      if (inverse) load_2d(dst, &mapC, 2 * kx0, b * MH, &raw_full[r]);
+      else load_2d(dst, &mapR, kx0, b * M, &raw_full[r]);
+      issued_loads = i + 1;
     }
-    tc_fence_after();
-    const int row = 32 * (warp & 3) + lane, h = warp >> 2;  // output row, column half
-    float re[16], im[16];
-    const uint32_t acc = tmem + lane_base + acc_col + (uint32_t)(bb * 2 * UN) + 16 * h;
-    tmem_ld16(acc, re);
-    tmem_ld16(acc + UN, im);
-    tmem_wait_ld();
-    tc_fence_before();
-    const float *ax = aux + bb * 2 * UN;
-    unsigned char *ot = ot0 + (size_t)bb * otb;
-    if (!inverse) {
-      if (row < MH) {
-        unsigned char *oh = ot + h * ohb;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {  // chunk c: complex values 2c, 2c+1 of this half
-          const int q = 2 * c;
-          const float v0 = even ? re[q] + ((row & 1) ? -ax[16 * h + q] : ax[16 * h + q]) : re[q];
-          const float v1 = even ? re[q + 1] + ((row & 1) ? -ax[16 * h + q + 1] : ax[16 * h + q + 1]) : re[q + 1];
-          *reinterpret_cast<float4 *>(oh + sw128(row, c)) = make_float4(v0, im[q], v1, im[q + 1]);
-        }
-      }
-    } else {
-      const int npairs = M / 2 + 1;
-      if (row < npairs) {
-        const float invM = 1.0f / (float)M;
-        const int pm = M - row;
-        const bool two = pm != row && pm < M;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {  // chunk 4h + c: values 16h + 4c .. 16h + 4c + 3
-          float f1[4], f2[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int q = 4 * c + e;
-            const float c0 = ax[16 * h + q];
-            const float y = even ? ((row & 1) ? -ax[UN + 16 * h + q] : ax[UN + 16 * h + q]) : 0.f;
-            f1[e] = (c0 + 2.0f * (re[q] + im[q]) + y) * invM;
-            f2[e] = (c0 + 2.0f * (re[q] - im[q]) + y) * invM;
-          }
-          *reinterpret_cast<float4 *>(ot + sw128(row, 4 * h + c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
-          if (two) *reinterpret_cast<float4 *>(ot + sw128(pm, 4 * h + c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
-        }
-      }
-    }
-    fence_async_shared();  // the tile's writes before the TMA store reads them
-  };
-  // TMA store of the output tile of local item j (all its writers have
-  // passed a barrier since)
-  auto store_tile = [&](int j) {
-    const int item = blockIdx.x + j * G, bb = j & 1;
-    const int b = item / ntile, kx0 = (item % ntile) * UN;
-    const unsigned char *ot = ot0 + (size_t)bb * otb;
-    if (!inverse) {
-      store_2d(&mapCs, ot, 2 * kx0, b * MH);
-      store_2d(&mapCs, ot + ohb, 2 * kx0 + UN, b * MH);
-    } else {
-      store_2d(&mapRs, ot, kx0, b * M);
-    }
-  };
-  for (int i = 0; i < nmine && !failed; ++i) {
-    const int item = blockIdx.x + i * G, bb = i & 1;
-    const int kx0 = (item % ntile) * UN;
-    // raw buffer (i-1) mod NRAW and this item's B buffer are free: their
-    // last readers (staging of item i-1, MMAs of item i-2) finished before here
-    if (__syncthreads_or(*fail_s)) {
-      failed = true;
-      break;
-    }
-    if (tid == 0 && i >= 2) {
-      // the tile of item i-2 (written before the barrier above) leaves; the
-      // one of item i-3 must be read out before epilogue(i-1) reuses its buffer
-      store_tile(i - 2);
-      store_commit();
-      store_wait_read<1>();
-    }
-    const int rb = i % NRAW;
-    if (tid == 32 && i + NRAW - 1 < nmine) {
-      fence_async_shared();
-      issue_copy(item + (NRAW - 1) * G, (i + NRAW - 1) % NRAW);
-    }
-    const bool ok = mbar_wait_hw(&tbar[rb], (uint32_t)(i / NRAW) & 1u);
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
-    }
-    // ---- split the operands of item i into B[bb] ----
-    // a thread takes column n and four consecutive rows k = 4 k4 .. 4 k4 + 3
-    // and writes one 16-byte chunk per operand
-    const float *rw = raw0 + (size_t)rb * rawf;
-    unsigned char *Bi = Bb + (size_t)bb * 4 * OPB;
-    const int n = lane, col = kx0 + n;
-    const bool okc = col < s.N;
-    for (int k4 = warp; k4 < QP / 4; k4 += UWARPS) {
-      uint4 h0, l0, h1, l1;
-      uint32_t *ph0 = &h0.x, *pl0 = &l0.x, *ph1 = &h1.x, *pl1 = &l1.x;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int k = 4 * k4 + r;
-        float x0 = 0.f, x1 = 0.f;
-        if (!inverse) {
-          if (okc && k <= H) {
-            const float fk = rw[k * UN + n];
-            if (k == 0) {
-              x0 = fk;
-            } else {
-              const float fm = rw[(M - k) * UN + n];
-              x0 = fk + fm;
-              x1 = fk - fm;
-            }
-          }
-        } else if (okc && k >= 1 && k <= H) {
-          const float2 v = reinterpret_cast<const float2 *>(rw)[k * UN + n];
-          x0 = v.x;
-          x1 = v.y;
-        }
-        u_split(x0, ph0[r], pl0[r]);
-        u_split(x1, ph1[r], pl1[r]);
-      }
-      const uint32_t off = b_off4(k4, n);
-      *reinterpret_cast<uint4 *>(Bi + 0 * OPB + off) = h0;
-      *reinterpret_cast<uint4 *>(Bi + 1 * OPB + off) = l0;
-      *reinterpret_cast<uint4 *>(Bi + 2 * OPB + off) = h1;
-      *reinterpret_cast<uint4 *>(Bi + 3 * OPB + off) = l1;
-    }
-    if (warp == UWARPS - 1) {
-      float *ax = aux + bb * 2 * UN;
-      if (!inverse) {
-        ax[n] = (okc && even) ? rw[(M / 2) * UN + n] : 0.f;  // f_{M/2}
-      } else {
-        const float2 *cw = reinterpret_cast<const float2 *>(rw);
-        ax[n] = okc ? cw[n].x : 0.f;                                     // c0
-        ax[UN + n] = (okc && even) ? cw[(M / 2) * UN + n].x : 0.f;       // Nyquist
-      }
-    }
-    fence_async_shared();  // the B operands before the tensor cores read them
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: item i from B[i % NB] into accumulator pair i % NACC ----
+    for (int i = 0; i < nmine; ++i) {
+      const int bs = i % NB, a = i % NACC;
+      if (!mbar_wait_or_fail(&b_full[bs], (uint32_t)(i / NB) & 1u, fail_s)) break;
+      if (!mbar_wait_or_fail(&acc_empty[a], ((uint32_t)(i / NACC) & 1u) ^ 1u, fail_s)) break;
       tc_fence_after();
-      const uint32_t sB = smem_u32(Bi);
-      // descriptors step by 1 KB (64 in the address field) per K step
+      const uint32_t sB = smem_u32(Bb + (size_t)bs * 4 * OPB);
 #pragma unroll
       for (int part = 0; part < 2; ++part) {  // 0: cos x S (or Re), 1: -sin x D (or Im)
-        const uint32_t d = tmem + acc_col + (uint32_t)(bb * 2 * UN + part * UN);
+        const uint32_t d = tmem + acc_col + (uint32_t)(a * 2 * UN + part * UN);
         const uint32_t ahi = tmem + tab_col + (uint32_t)((2 * part) * QP);
         const uint32_t alo = ahi + QP;
         uint64_t dh = b_desc(sB + (uint32_t)(2 * part) * OPB), dl = dh + (OPB >> 4);
@@ -362,30 +247,156 @@ __global__ void __launch_bounds__(UTHREADS, 1)
           dl += 64;
         }
       }
-      umma_commit(&mbar[bb]);
+      umma_commit(&b_empty[bs]);   // B[bs] free once these products are done
+      umma_commit(&acc_full[a]);   // and the accumulators ready
+      issued_mma = i + 1;
     }
-    if (i >= 1) epilogue(i - 1);
-  }
-  if (!failed && nmine > 0) {
-    if (tid == 0) store_wait_read<0>();  // the buffer of item nmine-1 is free
-    __syncthreads();
-    epilogue(nmine - 1);
-  }
-  if (__syncthreads_or(*fail_s)) failed = true;
-  if (tid == 0) {
-    if (!failed) {
-      if (nmine >= 2) store_tile(nmine - 2);
-      if (nmine >= 1) store_tile(nmine - 1);
+  } else if (warp == 2 && lane == 0) {
+    // ---- TMA stores of the output tiles ----
+    for (int i = 0; i < nmine; ++i) {
+      const int o = i % NOUT;
+      if (!mbar_wait_or_fail(&out_full[o], (uint32_t)(i / NOUT) & 1u, fail_s)) break;
+      const int item = blockIdx.x + i * G;
+      const int b = item / ntile, kx0 = (item % ntile) * UN;
+      const unsigned char *ot = ot0 + (size_t)o * otb;
+      if (!inverse) {
+        store_2d(&mapCs, ot, 2 * kx0, b * MH);
+        store_2d(&mapCs, ot + ohb, 2 * kx0 + UN, b * MH);
+      } else {
+        store_2d(&mapRs, ot, kx0, b * M);
+      }
       store_commit();
+      store_wait_read<0>();
+      mbar_arrive(&out_empty[o]);
     }
     store_wait_all();  // no store reads shared memory after this CTA leaves
+  } else if (warp >= 4 && warp < 8) {
+    // ---- split raw columns into the B operands ----
+    // thread: column n = lane, rows k = 4 k4 .. 4 k4 + 3 for k4 = sw, sw + 4, ..;
+    // one 16-byte chunk per operand.  The f_{M/2} term (forward, even M) and
+    // the c0 and Nyquist terms (inverse, halved) ride in the products as rows
+    // 0 and M/2 of the tables, so the epilogue needs nothing else.
+    const int sw = warp - 4, n = lane;
+    for (int i = 0; i < nmine; ++i) {
+      const int r = i % NRAW, bs = i % NB;
+      const int item = blockIdx.x + i * G;
+      const int col = (item % ntile) * UN + n;
+      const bool okc = col < s.N;
+      if (!mbar_wait_or_fail(&raw_full[r], (uint32_t)(i / NRAW) & 1u, fail_s)) break;
+      if (!mbar_wait_or_fail(&b_empty[bs], ((uint32_t)(i / NB) & 1u) ^ 1u, fail_s)) break;
+      const float *rw = raw0 + (size_t)r * rawf;
+      unsigned char *Bi = Bb + (size_t)bs * 4 * OPB;
+      for (int k4 = sw; k4 < QP / 4; k4 += 4) {
+        uint4 h0, l0, h1, l1;
+        uint32_t *ph0 = &h0.x, *pl0 = &l0.x, *ph1 = &h1.x, *pl1 = &l1.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = 4 * k4 + e;
+          float x0 = 0.f, x1 = 0.f;
+          if (okc) {
+            if (!inverse) {
+              if (k == 0) {
+                x0 = rw[n];
+              } else if (k <= H) {
+                const float fk = rw[k * UN + n], fm = rw[(M - k) * UN + n];
+                x0 = fk + fm;
+                x1 = fk - fm;
+              } else if (even && k == M / 2) {
+                x0 = rw[k * UN + n];
+              }
+            } else {
+              const float2 *cw = reinterpret_cast<const float2 *>(rw);
+              if (k == 0 || (even && k == M / 2)) {
+                x0 = 0.5f * cw[k * UN + n].x;
+              } else if (k <= H) {
+                const float2 v = cw[k * UN + n];
+                x0 = v.x;
+                x1 = v.y;
+              }
+            }
+          }
+          u_split(x0, ph0[e], pl0[e]);
+          u_split(x1, ph1[e], pl1[e]);
+        }
+        const uint32_t off = b_off4(k4, n);
+        *reinterpret_cast<uint4 *>(Bi + 0 * OPB + off) = h0;
+        *reinterpret_cast<uint4 *>(Bi + 1 * OPB + off) = l0;
+        *reinterpret_cast<uint4 *>(Bi + 2 * OPB + off) = h1;
+        *reinterpret_cast<uint4 *>(Bi + 3 * OPB + off) = l1;
+      }
+      fence_async_shared();  // the B operands before the tensor cores read them
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&raw_empty[r]);
+        mbar_arrive(&b_full[bs]);
+      }
+    }
+  } else if (warp >= 8) {
+    // ---- epilogue: accumulators -> swizzled output tile ----
+    const int row = 32 * (warp & 3) + lane;
+    const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+    const float scale = 2.0f / (float)M;
+    for (int i = 0; i < nmine; ++i) {
+      const int a = i % NACC, o = i % NOUT;
+      if (!mbar_wait_or_fail(&acc_full[a], (uint32_t)(i / NACC) & 1u, fail_s)) break;
+      tc_fence_after();
+      float re[32], im[32];
+      const uint32_t acc = tmem + lb + acc_col + (uint32_t)(a * 2 * UN);
+      tmem_ld16(acc, *reinterpret_cast<float(*)[16]>(re));
+      tmem_ld16(acc + 16, *reinterpret_cast<float(*)[16]>(re + 16));
+      tmem_ld16(acc + UN, *reinterpret_cast<float(*)[16]>(im));
+      tmem_ld16(acc + UN + 16, *reinterpret_cast<float(*)[16]>(im + 16));
+      tmem_wait_ld();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
+      if (!mbar_wait_or_fail(&out_empty[o], ((uint32_t)(i / NOUT) & 1u) ^ 1u, fail_s)) break;
+      unsigned char *ot = ot0 + (size_t)o * otb;
+      if (!inverse) {
+        if (row < MH) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {  // chunk c of half h: complex values 16h + 2c, 16h + 2c + 1
+              const int q = 16 * h + 2 * c;
+              *reinterpret_cast<float4 *>(ot + h * ohb + sw128(row, c)) =
+                  make_float4(re[q], im[q], re[q + 1], im[q + 1]);
+            }
+        }
+      } else if (row <= M / 2) {
+        const int pm = M - row;
+        const bool two = pm != row && pm < M;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {  // chunk c: values 4c .. 4c + 3
+          float f1[4], f2[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int q = 4 * c + e;
+            f1[e] = (re[q] + im[q]) * scale;
+            f2[e] = (re[q] - im[q]) * scale;
+          }
+          *reinterpret_cast<float4 *>(ot + sw128(row, c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
+          if (two) *reinterpret_cast<float4 *>(ot + sw128(pm, c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
+        }
+      }
+      fence_async_shared();  // the tile's writes before the TMA store reads them
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&out_full[o]);
+    }
   }
+  __syncwarp();
+  __syncthreads();
+  const bool failed = *fail_s != 0;
   if (failed) {
     // let the copies and products this CTA issued finish (bounded), then leave
-    if (tid == 0) {
+    if (warp == 0 && lane == 0) {
       atomicOr(err, 8);
-      for (int q = 0; q < 2; ++q) mbar_wait(&mbar[q], 0);
-      for (int q = 0; q < NRAW; ++q) mbar_wait(&tbar[q], 0);
+      for (int i = issued_loads - NRAW > 0 ? issued_loads - NRAW : 0; i < issued_loads; ++i)
+        mbar_wait(&raw_full[i % NRAW], (uint32_t)(i / NRAW) & 1u);
+    }
+    if (warp == 1 && lane == 0 && issued_mma > 0) {
+      const int i = issued_mma - 1;
+      mbar_wait(&acc_full[i % NACC], (uint32_t)(i / NACC) & 1u);
     }
   }
   tc_fence_before();
@@ -402,9 +413,9 @@ int u_raw_floats(const Spec &s) {
   return (f + 31) / 32 * 32;
 }
 size_t u_smem_bytes(const Spec &s, int qp) {
-  // the output tiles start at the next 1 KB boundary after aux (at most 1 KB on)
-  return 1024 + (size_t)8 * (qp / 8) * 1024 + (size_t)NRAW * u_raw_floats(s) * sizeof(float) +
-         4 * UN * sizeof(float) + 1024 + 2 * (size_t)u_otile_bytes(s.M, s.MH) + (NRAW + 2) * sizeof(uint64_t) +
+  // the output tiles start at the next 1 KB boundary after raw (at most 1 KB on)
+  return 1024 + (size_t)NB * 4 * (qp / 8) * 1024 + (size_t)NRAW * u_raw_floats(s) * sizeof(float) + 1024 +
+         NOUT * (size_t)u_otile_bytes(s.M, s.MH) + 2 * (NRAW + NB + NACC + NOUT) * sizeof(uint64_t) +
          16;  // the last 16: tensor-memory slot and failure flag
 }
 uint32_t tf32_host_rna(float x) {
@@ -481,7 +492,7 @@ static void launch_u(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, con
   memcpy(&mcs, mp.cs, sizeof mcs);
   (void)R;
   (void)C;
-  k_zdft_umma<QP><<<grid, UTHREADS, sm, st>>>(mr, mc, mrs, mcs, s, tab, inverse, u_raw_floats(s), err);
+  k_zdft_umma<QP><<<grid, WS_THREADS, sm, st>>>(mr, mc, mrs, mcs, s, tab, inverse, u_raw_floats(s), err);
 }
 
 void launch_zdft_umma(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *tab, int inverse,
