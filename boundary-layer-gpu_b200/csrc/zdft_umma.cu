@@ -6,21 +6,24 @@
 // two square products of order Q = M/2+1 with the f_k +- f_{M-k} pairing,
 // three-term TF32 split hi*hi + hi*lo + lo*hi); see there for the algebra.
 //
-// One persistent CTA (12 warps) per SM, warp-specialised.  Work items are
+// One persistent CTA (16 warps) per SM, warp-specialised.  Work items are
 // (row b, 32 kx columns).  A producer thread brings the raw columns of the
-// coming items by TMA tensor copies (NRAW buffers); four warps split them
-// into the B operands (NB buffers); one thread issues the 3 x Q/8 x 2 MMAs
-// of M = 128, N = 32, K = 8 into one of NACC accumulator pairs and commits
-// them to mbarriers; four warps read the accumulators with tcgen05.ld and
+// coming items by TMA tensor copies (NRAW buffers); eight warps split them
+// into the B operands (NB buffers, hi and lo columns side by side); one
+// thread issues per K step of 8 and part (cos or -sin) an MMA of table hi x
+// (B hi | B lo) with N = 64 and one of table lo x B hi with N = 32, M = 128,
+// into one of NACC accumulator sets, and commits them to mbarriers; four
+// warps read the accumulators with tcgen05.ld, add the hi x lo half, and
 // write 128-byte-swizzled output tiles, which one thread stores by TMA.  All
 // stages run concurrently on successive items, handing slots over through
 // full / empty mbarrier rings.  Tensor memory: 4 Q columns of tables (cos
-// hi, cos lo, -sin hi, -sin lo; lane = output row) and NACC x 2 x 32
-// accumulator columns (256 or 512 allocated).  Every wait is bounded and
+// hi, cos lo, -sin hi, -sin lo; lane = output row) and NACC x 2 x 64
+// accumulator columns (512 allocated).  Every wait is bounded and
 // gives up as soon as another thread of the CTA has given up; then bit 8 of
 // the device flag is set and the CTA drains its copies and products
 // (bounded), releases its tensor memory and leaves.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -33,7 +36,6 @@ using namespace tma;
 
 namespace {
 constexpr int UN = 32;        // kx columns per work item = N of the MMA
-constexpr int NRAW = 3;       // raw column buffers: copies of the next NRAW-1 items in flight
 
 __device__ __forceinline__ uint32_t u_tf32_rna(float x) {
   uint32_t r;
@@ -46,33 +48,38 @@ __device__ __forceinline__ void u_split(float x, uint32_t &hi, uint32_t &lo) {
   lo = u_tf32_rna(x - __uint_as_float(hi));
 }
 
-// B operand (K x N = 32), K-major without swizzle: core matrices of 8
-// columns n x 4 rows k (8 rows of 16 bytes, k fastest), the 4 column groups
-// of a 4-row slab 128 bytes apart (stride offset), slabs 512 bytes apart
-// (leading offset); one MMA (K = 8) reads two slabs, 1 KB
-__device__ __forceinline__ uint32_t b_off4(int k4, int n) {  // 16-byte chunk of rows 4 k4 .. 4 k4 + 3
-  return ((uint32_t)k4 << 9) + ((uint32_t)(n >> 3) << 7) + ((uint32_t)(n & 7) << 4);
+// B operand of one part (S or D: K x 64 = hi columns 0..31 | lo columns
+// 32..63), K-major without swizzle: core matrices of 8 columns x 4 rows k
+// (8 rows of 16 bytes, k fastest), the 8 column groups of a 4-row slab 128
+// bytes apart (stride offset), slabs 1 KB apart (leading offset); one MMA
+// (K = 8) reads two slabs.  The table's hi rows multiply hi | lo at once
+// (N = 64), its lo rows the hi columns (N = 32).
+__device__ __forceinline__ uint32_t b_off4(int k4, int n, int lo) {  // 16-byte chunk of rows 4 k4 .. 4 k4 + 3
+  return ((uint32_t)k4 << 10) + ((uint32_t)(4 * lo + (n >> 3)) << 7) + ((uint32_t)(n & 7) << 4);
 }
-// shared-memory matrix descriptor: start address, leading offset 512 B (next
+// shared-memory matrix descriptor: start address, leading offset 1 KB (next
 // core matrix along K), stride offset 128 B (next one along N), version 1,
 // no swizzle
 __device__ __forceinline__ uint64_t b_desc(uint32_t saddr) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((512u >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
   return d;
 }
-// instruction descriptor: F32 accumulate, A and B TF32, both K-major (A in
-// tensor memory), N = 32, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(UN >> 3) << 17) |
-                           ((uint32_t)(128 >> 4) << 24);
+// instruction descriptors: F32 accumulate, A and B TF32, both K-major (A in
+// tensor memory), M = 128, N = 64 or 32
+constexpr uint32_t idesc_n(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+constexpr uint32_t IDESC64 = idesc_n(2 * UN), IDESC32 = idesc_n(UN);
 
+template <uint32_t ID>
 __device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %4, p;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(bdesc), "r"(acc), "r"(IDESC)
+      "r"(a_tmem), "l"(bdesc), "r"(acc), "n"(ID)
       : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -114,33 +121,38 @@ __host__ __device__ inline uint32_t u_otile_bytes(int M, int MH) {
 // byte offset of 16-byte chunk c of row r in a 128-byte-swizzled tile
 __device__ __forceinline__ uint32_t sw128(int r, int c) { return ((uint32_t)r << 7) + ((uint32_t)((c ^ r) & 7) << 4); }
 
-// Warp roles (12 warps): warp 0 lane 0 issues the TMA copies of the raw
+// Warp roles (16 warps): warp 0 lane 0 issues the TMA copies of the raw
 // columns, warp 1 lane 0 the MMAs, warp 2 lane 0 the TMA stores of the
-// output tiles; warps 4-7 split raw columns into B operands, warps 8-11 (one
-// per 32 tensor-memory lanes) read the accumulators and write the output
-// tiles.  Every hand-off is an mbarrier ring: raw (NRAW), B (NB), accumulator
+// output tiles; warps 4-11 split raw columns into B operands, warps 12-15
+// (one per 32 tensor-memory lanes) read the accumulators and write the
+// output tiles.  Every hand-off is an mbarrier ring: raw (NRAW), B (NB), accumulator
 // pairs (NACC), output tiles (NOUT), each with a "full" and an "empty"
 // barrier; a producer waits for the empty phase before reusing a slot.
-constexpr int NB = 2, NACC = 2, NOUT = 2;
-constexpr int WS_WARPS = 12, WS_THREADS = WS_WARPS * 32;
+constexpr int NB = 2;
+constexpr int SPLIT_W = 8;                          // warps that split raw columns
+constexpr int EPI_W0 = 4 + SPLIT_W;                 // first of the four epilogue warps
+constexpr int WS_WARPS = EPI_W0 + 4, WS_THREADS = WS_WARPS * 32;
+static_assert(EPI_W0 % 4 == 0, "epilogue warp w serves tensor-memory lanes 32 (w % 4) ..");
 
 // Shared memory, from a 1 KB aligned base: B[NB][4 operands][Q/8 K-steps of
 // 1 KB] | raw[NRAW][rawf floats] | output tiles[NOUT] (1 KB aligned) |
 // mbarriers | tmem slot and failure flag.
-template <int QP>
+template <int QP, int NRAW, int NOUT>
 __global__ void __launch_bounds__(WS_THREADS, 1)
     k_zdft_umma(const __grid_constant__ CUtensorMap mapR, const __grid_constant__ CUtensorMap mapC,
                 const __grid_constant__ CUtensorMap mapRs, const __grid_constant__ CUtensorMap mapCs, Spec s,
                 const uint32_t *__restrict__ tab, int inverse, int rawf, int *__restrict__ err) {
-  constexpr int KS = QP / 8;                    // K steps (1 KB of B each) per product
-  constexpr uint32_t OPB = (uint32_t)KS << 10;  // bytes of one B operand
+  constexpr int KS = QP / 8;                    // K steps (2 KB of B each) per product
+  constexpr uint32_t OPB = (uint32_t)KS << 11;  // bytes of one part (hi | lo) of B
+  // accumulator sets of 2 parts x 64 columns: two where the tables leave room
+  constexpr int NACC = 4 * QP + 2 * 128 <= 512 ? 2 : 1;
   // tensor-memory columns: tables and accumulators, rounded up to a power of two
-  constexpr uint32_t TCOLS = (4 * QP + 2 * NACC * UN) <= 256 ? 256u : 512u;
+  constexpr uint32_t TCOLS = (4 * QP + NACC * 128) <= 256 ? 256u : 512u;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t s0 = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
-  unsigned char *Bb = sm;                                          // NB x 4 x OPB
-  float *raw0 = reinterpret_cast<float *>(sm + NB * 4 * OPB);      // [NRAW][rawf]
+  unsigned char *Bb = sm;                                          // NB x 2 x OPB
+  float *raw0 = reinterpret_cast<float *>(sm + NB * 2 * OPB);      // [NRAW][rawf]
   const uint32_t ohb = ((uint32_t)s.MH * 128u + 1023u) & ~1023u;  // one forward half
   const uint32_t otb = u_otile_bytes(s.M, s.MH);
   unsigned char *ot0 = reinterpret_cast<unsigned char *>(raw0 + NRAW * (size_t)rawf);
@@ -170,10 +182,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     *fail_s = 0;
     for (int q = 0; q < NRAW; ++q) {
       mbar_init(&raw_full[q], 1);
-      mbar_init(&raw_empty[q], 4);
+      mbar_init(&raw_empty[q], SPLIT_W);
     }
     for (int q = 0; q < NB; ++q) {
-      mbar_init(&b_full[q], 4);
+      mbar_init(&b_full[q], SPLIT_W);
       mbar_init(&b_empty[q], 1);
     }
     for (int q = 0; q < NACC; ++q) {
@@ -191,7 +203,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   tc_fence_after();
   const uint32_t tmem = *slot;
   const uint32_t tab_col = 0, acc_col = 4 * QP;  // tables, then the accumulator pairs
-  if (warp >= 8) {
+  if (warp >= EPI_W0) {
     // table t (0 cos hi, 1 cos lo, 2 -sin hi, 3 -sin lo) in columns t*QP.. of
     // lane = output row, by the warp of that lane quarter
     const int row = 32 * (warp & 3) + lane;
@@ -231,20 +243,19 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       if (!mbar_wait_or_fail(&b_full[bs], (uint32_t)(i / NB) & 1u, fail_s)) break;
       if (!mbar_wait_or_fail(&acc_empty[a], ((uint32_t)(i / NACC) & 1u) ^ 1u, fail_s)) break;
       tc_fence_after();
-      const uint32_t sB = smem_u32(Bb + (size_t)bs * 4 * OPB);
+      const uint32_t sB = smem_u32(Bb + (size_t)bs * 2 * OPB);
 #pragma unroll
       for (int part = 0; part < 2; ++part) {  // 0: cos x S (or Re), 1: -sin x D (or Im)
-        const uint32_t d = tmem + acc_col + (uint32_t)(a * 2 * UN + part * UN);
+        // columns 0..31: table hi x B hi + table lo x B hi; 32..63: table hi x B lo
+        const uint32_t d = tmem + acc_col + (uint32_t)(a * 128 + part * 64);
         const uint32_t ahi = tmem + tab_col + (uint32_t)((2 * part) * QP);
         const uint32_t alo = ahi + QP;
-        uint64_t dh = b_desc(sB + (uint32_t)(2 * part) * OPB), dl = dh + (OPB >> 4);
+        uint64_t db = b_desc(sB + (uint32_t)part * OPB);
 #pragma unroll
         for (int ks = 0; ks < KS; ++ks) {
-          umma_tf32(d, alo + 8 * ks, dh, ks > 0 ? 1u : 0u);  // lo x hi
-          umma_tf32(d, ahi + 8 * ks, dl, 1u);                // hi x lo
-          umma_tf32(d, ahi + 8 * ks, dh, 1u);                // hi x hi
-          dh += 64;
-          dl += 64;
+          umma_tf32<IDESC64>(d, ahi + 8 * ks, db, ks > 0 ? 1u : 0u);  // hi x (hi | lo)
+          umma_tf32<IDESC32>(d, alo + 8 * ks, db, 1u);                // lo x hi
+          db += 128;                                                   // 2 KB
         }
       }
       umma_commit(&b_empty[bs]);   // B[bs] free once these products are done
@@ -270,13 +281,14 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       mbar_arrive(&out_empty[o]);
     }
     store_wait_all();  // no store reads shared memory after this CTA leaves
-  } else if (warp >= 4 && warp < 8) {
+  } else if (warp >= 4 && warp < EPI_W0) {
     // ---- split raw columns into the B operands ----
-    // thread: column n = lane, rows k = 4 k4 .. 4 k4 + 3 for k4 = sw, sw + 4, ..;
+    // thread: column n = lane, rows k = 4 k4 .. 4 k4 + 3 for k4 = sw, sw + SPLIT_W, ..;
     // one 16-byte chunk per operand.  The f_{M/2} term (forward, even M) and
     // the c0 and Nyquist terms (inverse, halved) ride in the products as rows
     // 0 and M/2 of the tables, so the epilogue needs nothing else.
     const int sw = warp - 4, n = lane;
+    constexpr int NJ = (QP / 4 + SPLIT_W - 1) / SPLIT_W;  // slabs per warp
     for (int i = 0; i < nmine; ++i) {
       const int r = i % NRAW, bs = i % NB;
       const int item = blockIdx.x + i * G;
@@ -285,8 +297,11 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       if (!mbar_wait_or_fail(&raw_full[r], (uint32_t)(i / NRAW) & 1u, fail_s)) break;
       if (!mbar_wait_or_fail(&b_empty[bs], ((uint32_t)(i / NB) & 1u) ^ 1u, fail_s)) break;
       const float *rw = raw0 + (size_t)r * rawf;
-      unsigned char *Bi = Bb + (size_t)bs * 4 * OPB;
-      for (int k4 = sw; k4 < QP / 4; k4 += 4) {
+      unsigned char *Bi = Bb + (size_t)bs * 2 * OPB;
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        const int k4 = sw + SPLIT_W * j;
+        if (k4 >= QP / 4) break;
         uint4 h0, l0, h1, l1;
         uint32_t *ph0 = &h0.x, *pl0 = &l0.x, *ph1 = &h1.x, *pl1 = &l1.x;
 #pragma unroll
@@ -318,11 +333,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           u_split(x0, ph0[e], pl0[e]);
           u_split(x1, ph1[e], pl1[e]);
         }
-        const uint32_t off = b_off4(k4, n);
-        *reinterpret_cast<uint4 *>(Bi + 0 * OPB + off) = h0;
-        *reinterpret_cast<uint4 *>(Bi + 1 * OPB + off) = l0;
-        *reinterpret_cast<uint4 *>(Bi + 2 * OPB + off) = h1;
-        *reinterpret_cast<uint4 *>(Bi + 3 * OPB + off) = l1;
+        *reinterpret_cast<uint4 *>(Bi + b_off4(k4, n, 0)) = h0;
+        *reinterpret_cast<uint4 *>(Bi + b_off4(k4, n, 1)) = l0;
+        *reinterpret_cast<uint4 *>(Bi + OPB + b_off4(k4, n, 0)) = h1;
+        *reinterpret_cast<uint4 *>(Bi + OPB + b_off4(k4, n, 1)) = l1;
       }
       fence_async_shared();  // the B operands before the tensor cores read them
       __syncwarp();
@@ -331,7 +345,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         mbar_arrive(&b_full[bs]);
       }
     }
-  } else if (warp >= 8) {
+  } else if (warp >= EPI_W0) {
     // ---- epilogue: accumulators -> swizzled output tile ----
     const int row = 32 * (warp & 3) + lane;
     const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
@@ -340,45 +354,51 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       const int a = i % NACC, o = i % NOUT;
       if (!mbar_wait_or_fail(&acc_full[a], (uint32_t)(i / NACC) & 1u, fail_s)) break;
       tc_fence_after();
-      float re[32], im[32];
-      const uint32_t acc = tmem + lb + acc_col + (uint32_t)(a * 2 * UN);
-      tmem_ld16(acc, *reinterpret_cast<float(*)[16]>(re));
-      tmem_ld16(acc + 16, *reinterpret_cast<float(*)[16]>(re + 16));
-      tmem_ld16(acc + UN, *reinterpret_cast<float(*)[16]>(im));
-      tmem_ld16(acc + UN + 16, *reinterpret_cast<float(*)[16]>(im + 16));
-      tmem_wait_ld();
+      if (!mbar_wait_or_fail(&out_empty[o], ((uint32_t)(i / NOUT) & 1u) ^ 1u, fail_s)) break;
+      unsigned char *ot = ot0 + (size_t)o * otb;
+      const uint32_t acc = tmem + lb + acc_col + (uint32_t)(a * 128);
+      // column halves h of 16: re = cos part, im = -sin part, each the sum of
+      // (table hi x B hi + table lo x B hi) and (table hi x B lo)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float re[16], im[16];
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          float x[16], y[16];
+          tmem_ld16(acc + part * 64 + 16 * h, x);
+          tmem_ld16(acc + part * 64 + 32 + 16 * h, y);
+          tmem_wait_ld();
+          float *v = part ? im : re;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = x[j] + y[j];
+        }
+        if (!inverse) {
+          if (row < MH) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c)  // chunk c of half h: complex values 16h + 2c, 16h + 2c + 1
+              *reinterpret_cast<float4 *>(ot + h * ohb + sw128(row, c)) =
+                  make_float4(re[2 * c], im[2 * c], re[2 * c + 1], im[2 * c + 1]);
+          }
+        } else if (row <= M / 2) {
+          const int pm = M - row;
+          const bool two = pm != row && pm < M;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {  // chunk 4h + c: values 16h + 4c .. 16h + 4c + 3
+            float f1[4], f2[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              f1[e] = (re[4 * c + e] + im[4 * c + e]) * scale;
+              f2[e] = (re[4 * c + e] - im[4 * c + e]) * scale;
+            }
+            *reinterpret_cast<float4 *>(ot + sw128(row, 4 * h + c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
+            if (two)
+              *reinterpret_cast<float4 *>(ot + sw128(pm, 4 * h + c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
+          }
+        }
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[a]);
-      if (!mbar_wait_or_fail(&out_empty[o], ((uint32_t)(i / NOUT) & 1u) ^ 1u, fail_s)) break;
-      unsigned char *ot = ot0 + (size_t)o * otb;
-      if (!inverse) {
-        if (row < MH) {
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {  // chunk c of half h: complex values 16h + 2c, 16h + 2c + 1
-              const int q = 16 * h + 2 * c;
-              *reinterpret_cast<float4 *>(ot + h * ohb + sw128(row, c)) =
-                  make_float4(re[q], im[q], re[q + 1], im[q + 1]);
-            }
-        }
-      } else if (row <= M / 2) {
-        const int pm = M - row;
-        const bool two = pm != row && pm < M;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {  // chunk c: values 4c .. 4c + 3
-          float f1[4], f2[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int q = 4 * c + e;
-            f1[e] = (re[q] + im[q]) * scale;
-            f2[e] = (re[q] - im[q]) * scale;
-          }
-          *reinterpret_cast<float4 *>(ot + sw128(row, c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
-          if (two) *reinterpret_cast<float4 *>(ot + sw128(pm, c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
-        }
-      }
       fence_async_shared();  // the tile's writes before the TMA store reads them
       __syncwarp();
       if (lane == 0) mbar_arrive(&out_full[o]);
@@ -412,10 +432,10 @@ int u_raw_floats(const Spec &s) {
   const int f = s.M * UN > s.MH * 2 * UN ? s.M * UN : s.MH * 2 * UN;
   return (f + 31) / 32 * 32;
 }
-size_t u_smem_bytes(const Spec &s, int qp) {
+size_t u_smem_bytes(const Spec &s, int qp, int NRAW, int NOUT) {
   // the output tiles start at the next 1 KB boundary after raw (at most 1 KB on)
   return 1024 + (size_t)NB * 4 * (qp / 8) * 1024 + (size_t)NRAW * u_raw_floats(s) * sizeof(float) + 1024 +
-         NOUT * (size_t)u_otile_bytes(s.M, s.MH) + 2 * (NRAW + NB + NACC + NOUT) * sizeof(uint64_t) +
+         NOUT * (size_t)u_otile_bytes(s.M, s.MH) + 2 * (NRAW + NB + 2 + NOUT) * sizeof(uint64_t) +
          16;  // the last 16: tensor-memory slot and failure flag
 }
 uint32_t tf32_host_rna(float x) {
@@ -431,8 +451,24 @@ uint32_t tf32_host_rna(float x) {
 int zdft_umma_qp(const Spec &s) {
   const int qp = zdft_tc_qp(s);
   if (!qp) return 0;
-  if (u_smem_bytes(s, qp) > 227 * 1024) return 0;
+  if (u_smem_bytes(s, qp, 2, 1) > 227 * 1024) return 0;
   return qp;
+}
+
+// ring depths (raw buffers, output tiles) for the box: the deepest of the
+// configurations tried that fits the shared memory
+static void u_rings(const Spec &s, int qp, int *nraw, int *nout) {
+  static const int cfg[][2] = {{4, 2}, {4, 1}, {3, 2}, {2, 2}, {2, 1}};
+  const char *e = getenv("BLGPU_U_RINGS");
+  int first = e ? atoi(e) : 0;
+  for (int c = first; c < 5; ++c)
+    if (u_smem_bytes(s, qp, cfg[c][0], cfg[c][1]) <= 227 * 1024) {
+      *nraw = cfg[c][0];
+      *nout = cfg[c][1];
+      return;
+    }
+  *nraw = 2;
+  *nout = 1;
 }
 
 // tables [4][128][QP] of TF32 bit patterns: cos hi, cos lo, -sin hi, -sin lo
@@ -478,11 +514,11 @@ bool zdft_umma_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out) {
   return true;
 }
 
-template <int QP>
-static void launch_u(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, const uint32_t *tab, int inverse,
-                     int nsm, int *err, cudaStream_t st) {
-  const size_t sm = u_smem_bytes(s, QP);
-  cudaFuncSetAttribute(k_zdft_umma<QP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+template <int QP, int NRAW, int NOUT>
+static void launch_r(const Spec &s, const ZdftMaps &mp, const uint32_t *tab, int inverse, int nsm, int *err,
+                     cudaStream_t st) {
+  const size_t sm = u_smem_bytes(s, QP, NRAW, NOUT);
+  cudaFuncSetAttribute(k_zdft_umma<QP, NRAW, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int nitems = s.NM * ((s.N + UN - 1) / UN);
   const int grid = nitems < nsm ? nitems : nsm;
   CUtensorMap mr, mc, mrs, mcs;
@@ -490,9 +526,21 @@ static void launch_u(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, con
   memcpy(&mc, mp.c, sizeof mc);
   memcpy(&mrs, mp.rs, sizeof mrs);
   memcpy(&mcs, mp.cs, sizeof mcs);
+  k_zdft_umma<QP, NRAW, NOUT><<<grid, WS_THREADS, sm, st>>>(mr, mc, mrs, mcs, s, tab, inverse, u_raw_floats(s), err);
+}
+
+template <int QP>
+static void launch_u(const Spec &s, const ZdftMaps &mp, float *R, float2 *C, const uint32_t *tab, int inverse,
+                     int nsm, int *err, cudaStream_t st) {
   (void)R;
   (void)C;
-  k_zdft_umma<QP><<<grid, WS_THREADS, sm, st>>>(mr, mc, mrs, mcs, s, tab, inverse, u_raw_floats(s), err);
+  int nraw = 2, nout = 1;
+  u_rings(s, QP, &nraw, &nout);
+  if (nraw == 4 && nout == 2) launch_r<QP, 4, 2>(s, mp, tab, inverse, nsm, err, st);
+  else if (nraw == 4) launch_r<QP, 4, 1>(s, mp, tab, inverse, nsm, err, st);
+  else if (nraw == 3) launch_r<QP, 3, 2>(s, mp, tab, inverse, nsm, err, st);
+  else if (nout == 2) launch_r<QP, 2, 2>(s, mp, tab, inverse, nsm, err, st);
+  else launch_r<QP, 2, 1>(s, mp, tab, inverse, nsm, err, st);
 }
 
 void launch_zdft_umma(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *tab, int inverse,
