@@ -42,10 +42,11 @@ __device__ __forceinline__ uint32_t u_tf32_rna(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
 }
-// x -> (hi, lo) as TF32 bit patterns, x ~ hi + lo to ~2^-22
+// x -> (hi, lo) as TF32 bit patterns, x ~ hi + lo to ~2^-21: hi rounded to
+// nearest, lo (exact in FP32) truncated to TF32
 __device__ __forceinline__ void u_split(float x, uint32_t &hi, uint32_t &lo) {
   hi = u_tf32_rna(x);
-  lo = u_tf32_rna(x - __uint_as_float(hi));
+  lo = __float_as_uint(x - __uint_as_float(hi)) & 0xffffe000u;
 }
 
 // B operand of one part (S or D: K x 64 = hi columns 0..31 | lo columns
