@@ -355,51 +355,54 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       const int a = i % NACC, o = i % NOUT;
       if (!mbar_wait_or_fail(&acc_full[a], (uint32_t)(i / NACC) & 1u, fail_s)) break;
       tc_fence_after();
-      if (!mbar_wait_or_fail(&out_empty[o], ((uint32_t)(i / NOUT) & 1u) ^ 1u, fail_s)) break;
-      unsigned char *ot = ot0 + (size_t)o * otb;
       const uint32_t acc = tmem + lb + acc_col + (uint32_t)(a * 128);
-      // column halves h of 16: re = cos part, im = -sin part, each the sum of
-      // (table hi x B hi + table lo x B hi) and (table hi x B lo)
+      // re = cos part, im = -sin part, each the sum of (table hi x B hi +
+      // table lo x B hi) and (table hi x B lo); the accumulators are free for
+      // the next item's products as soon as they are read
+      float re[32], im[32];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        float re[16], im[16];
+      for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int part = 0; part < 2; ++part) {
           float x[16], y[16];
           tmem_ld16(acc + part * 64 + 16 * h, x);
           tmem_ld16(acc + part * 64 + 32 + 16 * h, y);
           tmem_wait_ld();
-          float *v = part ? im : re;
+          float *v = (part ? im : re) + 16 * h;
 #pragma unroll
           for (int j = 0; j < 16; ++j) v[j] = x[j] + y[j];
         }
-        if (!inverse) {
-          if (row < MH) {
-#pragma unroll
-            for (int c = 0; c < 8; ++c)  // chunk c of half h: complex values 16h + 2c, 16h + 2c + 1
-              *reinterpret_cast<float4 *>(ot + h * ohb + sw128(row, c)) =
-                  make_float4(re[2 * c], im[2 * c], re[2 * c + 1], im[2 * c + 1]);
-          }
-        } else if (row <= M / 2) {
-          const int pm = M - row;
-          const bool two = pm != row && pm < M;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {  // chunk 4h + c: values 16h + 4c .. 16h + 4c + 3
-            float f1[4], f2[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              f1[e] = (re[4 * c + e] + im[4 * c + e]) * scale;
-              f2[e] = (re[4 * c + e] - im[4 * c + e]) * scale;
-            }
-            *reinterpret_cast<float4 *>(ot + sw128(row, 4 * h + c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
-            if (two)
-              *reinterpret_cast<float4 *>(ot + sw128(pm, 4 * h + c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
-          }
-        }
-      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[a]);
+      if (!mbar_wait_or_fail(&out_empty[o], ((uint32_t)(i / NOUT) & 1u) ^ 1u, fail_s)) break;
+      unsigned char *ot = ot0 + (size_t)o * otb;
+      if (!inverse) {
+        if (row < MH) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {  // chunk c of half h: complex values 16h + 2c, 16h + 2c + 1
+              const int q = 16 * h + 2 * c;
+              *reinterpret_cast<float4 *>(ot + h * ohb + sw128(row, c)) =
+                  make_float4(re[q], im[q], re[q + 1], im[q + 1]);
+            }
+        }
+      } else if (row <= M / 2) {
+        const int pm = M - row;
+        const bool two = pm != row && pm < M;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {  // chunk c: values 4c .. 4c + 3
+          float f1[4], f2[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            f1[e] = (re[4 * c + e] + im[4 * c + e]) * scale;
+            f2[e] = (re[4 * c + e] - im[4 * c + e]) * scale;
+          }
+          *reinterpret_cast<float4 *>(ot + sw128(row, c)) = make_float4(f1[0], f1[1], f1[2], f1[3]);
+          if (two) *reinterpret_cast<float4 *>(ot + sw128(pm, c)) = make_float4(f2[0], f2[1], f2[2], f2[3]);
+        }
+      }
       fence_async_shared();  // the tile's writes before the TMA store reads them
       __syncwarp();
       if (lane == 0) mbar_arrive(&out_full[o]);
