@@ -124,6 +124,22 @@ def test_compute_dt_exact(gpu, grid):
     s.close()
 
 
+@pytest.mark.parametrize("grid", GRIDS)
+def test_compute_dt_mixed(gpu, grid):
+    """The mixed form's compute_dt (four points per thread, 16-byte loads)
+    against the oracle on the FP32-rounded fields; the w bound is taken as
+    1 / min(|w| / C) there, so agreement is to rounding, not bitwise."""
+    c = noisy_laminar(*grid, seed=9, amp=0.3)
+    c.U = np.asfortranarray((c.U + 2.0).astype(np.float32).astype(np.float64))
+    c.V = np.asfortranarray((c.V + 1.0).astype(np.float32).astype(np.float64))
+    c.W = np.asfortranarray((c.W + 1.0).astype(np.float32).astype(np.float64))
+    c.cfl = 0.37
+    s = cases.solver_for(c, precision=MIXED)
+    o = oracle.oracle_for(c)
+    assert s.compute_dt() == pytest.approx(o.compute_dt(), rel=1e-14)
+    s.close()
+
+
 def test_laminar_cfg1_10_steps(gpu):
     """Config 1 (128x64x32 laminar Blasius, RK3, CFL 0.5): 10 steps."""
     c = cases.laminar_case()
