@@ -1138,13 +1138,13 @@ __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, c
 // p0[b][i] = sum_{kx < K} H[b][kx] cm[kx][i]: 32 x 64 output tiles, k-tiles of 32
 __global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restrict__ H, int K,
                                                   const double *__restrict__ cm, double *__restrict__ p0) {
-  constexpr int BM = 32, BN = 64, BK = 32;
+  constexpr int BM = 16, BN = 64, BK = 32;  // 16-row tiles: 208 CTAs at 812 x 256
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN];
   const int N = s.N, NM = s.NM;
   const int b0 = blockIdx.y * BM, i0 = blockIdx.x * BN;
   const int t = threadIdx.x, tr = t >> 4, tc = t & 15;
-  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int k0 = 0; k0 < K; k0 += BK) {
     for (int q = t; q < BM * BK; q += 256) {
       const int r = q / BK, c = q % BK;
@@ -1157,23 +1157,17 @@ __global__ void __launch_bounds__(256) k_kz0_idct(Spec s, const double *__restri
     __syncthreads();
 #pragma unroll 8
     for (int kk = 0; kk < BK; ++kk) {
-      const double a0 = As[kk][2 * tr], a1 = As[kk][2 * tr + 1];
+      const double a0 = As[kk][tr];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double bv = Bs[kk][tc + 16 * q];
-        acc[0][q] += a0 * bv;
-        acc[1][q] += a1 * bv;
-      }
+      for (int q = 0; q < 4; ++q) acc[q] += a0 * Bs[kk][tc + 16 * q];
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int b = b0 + 2 * tr + r, i = i0 + tc + 16 * q;
-      if (b < NM && i < N) p0[(long long)b * N + i] = acc[r][q];
-    }
+  for (int q = 0; q < 4; ++q) {
+    const int b = b0 + tr, i = i0 + tc + 16 * q;
+    if (b < NM && i < N) p0[(long long)b * N + i] = acc[q];
+  }
 }
 
 // FP32 copies of the p0 differences the projection uses (taken in FP64):
@@ -1363,7 +1357,7 @@ void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const d
 
 void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm, double *p0, float *grad,
                      cudaStream_t st) {
-  k_kz0_idct<<<dim3((s.N + 63) / 64, (s.NM + 31) / 32), 256, 0, st>>>(s, H0, klow, cm, p0);
+  k_kz0_idct<<<dim3((s.N + 63) / 64, (s.NM + 15) / 16), 256, 0, st>>>(s, H0, klow, cm, p0);
   k_kz0_grad<<<(s.N * s.NM + 255) / 256, 256, 0, st>>>(s, p0, grad, grad + (long long)s.N * s.NM);
 }
 

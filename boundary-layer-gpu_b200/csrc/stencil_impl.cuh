@@ -1381,10 +1381,16 @@ __global__ void __launch_bounds__(128) k_lund_sums(Geo g, LundData L, const T *_
   if (threadIdx.x == 0) L.inst[r] = red[0] / (double)(g.nzg - 2);
 }
 
+// one warp: the first row j with Um >= Umean99 by ballots over 32 rows at a
+// time (the same row as a serial scan), then the interpolation
 __device__ double lund_delta99(const double *Um, const double *yg, int nyg, double Umean99) {
+  const int lane = threadIdx.x & 31;
   int jref = 0;
-  for (int j = 1; j <= nyg; ++j)
-    if (Um[j - 1] >= Umean99) { jref = j; break; }
+  for (int j0 = 1; j0 <= nyg && !jref; j0 += 32) {
+    const int j = j0 + lane;
+    const unsigned hit = __ballot_sync(0xffffffffu, j <= nyg && Um[j - 1] >= Umean99);
+    if (hit) jref = j0 + __ffs(hit) - 1;
+  }
   if (jref < 2) jref = nyg / 2;
   const double w1 = (Umean99 - Um[jref - 2]) / (Um[jref - 1] - Um[jref - 2]);
   const double w0 = 1.0 - w1;
@@ -1392,12 +1398,16 @@ __device__ double lund_delta99(const double *Um, const double *yg, int nyg, doub
   return d < 0 ? fabs(d) : d;
 }
 
+// one warp: trapezoidal momentum thickness, lane partial sums combined by a
+// butterfly (every lane returns the same value)
 __device__ double lund_theta(const double *Um, const double *yg, int nyg, double Uinf) {
+  const int lane = threadIdx.x & 31;
   double th = 0.0;
-  for (int j = 2; j <= nyg; ++j) {
+  for (int j = 2 + lane; j <= nyg; j += 32) {
     const double a = Um[j - 1] / Uinf * (1.0 - Um[j - 1] / Uinf), b = Um[j - 2] / Uinf * (1.0 - Um[j - 2] / Uinf);
     th = th + 0.5 * (a + b) * (yg[j] - yg[j - 1]);
   }
+  for (int o = 16; o > 0; o >>= 1) th += __shfl_xor_sync(0xffffffffu, th, o);
   return th < 0 ? fabs(th) : th;
 }
 
@@ -1420,10 +1430,15 @@ __global__ void __launch_bounds__(256) k_lund_rows(Geo g, LundData L, const Scal
   const double *Umr = L.mean, *Umi = L.mean + nyg, *Vmr = L.mean + 2 * nyg;
   // the four serial scans run on four warps at once
   const double Uinf = L.inst[nyg - 1];
-  if (tid == 0) sh[1] = lund_delta99(Umr, g.yg, nyg, 0.99 * Uinf);
-  if (tid == 32) sh[2] = lund_delta99(Umi, g.yg, nyg, 0.99 * Uinf);
-  if (tid == 64) sh[3] = lund_theta(Umr, g.yg, nyg, Uinf);
-  if (tid == 96) sh[4] = lund_theta(Umi, g.yg, nyg, Uinf);
+  {
+    const int w = tid >> 5;  // warps 0-3, one scan each
+    double r = 0.0;
+    if (w == 0) r = lund_delta99(Umr, g.yg, nyg, 0.99 * Uinf);
+    if (w == 1) r = lund_delta99(Umi, g.yg, nyg, 0.99 * Uinf);
+    if (w == 2) r = lund_theta(Umr, g.yg, nyg, Uinf);
+    if (w == 3) r = lund_theta(Umi, g.yg, nyg, Uinf);
+    if (w < 4 && (tid & 31) == 0) sh[1 + w] = r;
+  }
   __syncthreads();
   if (tid == 0) {
     const double th_r = sh[3], th_i = sh[4];
