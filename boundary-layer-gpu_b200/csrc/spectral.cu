@@ -968,9 +968,11 @@ __global__ void k_thomas_factors(Spec s, double *__restrict__ piv, const double 
 }
 
 // One thread per complex mode (a CTA takes 128 consecutive kx of one kz, so
-// each row step reads 1 KB runs of C and of piv), both sweeps down the NM rows b with a ring of PF rows in flight:
-// row b+PF is requested when row b is consumed.  Rows are reached by
-// stepping one pointer into C and one into piv by the row stride.
+// each row step reads 1 KB runs of C and of piv), both sweeps down the NM
+// rows b with a ring of PF rows in flight: row b+PF is requested when row b
+// is consumed.  Rows are reached by stepping one pointer into C and one into
+// piv by the row stride; the row loads are cached in L2 only (each is read
+// once per sweep), so the ring is not bounded by the L1 capacity.
 template <typename T, int PF>
 __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const double *__restrict__ pm, long long rs,
                                               int NM, const double *__restrict__ dl, const double *__restrict__ du) {
@@ -981,8 +983,8 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
   const double *pn = pm;
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
-    cr[u] = u < NM ? cn[0] : mk<T>((T)0, (T)0);
-    pr[u] = u < NM ? pn[0] : 0.0;
+    cr[u] = u < NM ? __ldcg(cn) : mk<T>((T)0, (T)0);
+    pr[u] = u < NM ? __ldcg(pn) : 0.0;
     if (u < NM) { cn += rs; pn += rs; }
   }
   double gx = 0.0, gy = 0.0, rprev = 0.0;
@@ -995,8 +997,8 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
         const T2<T> cv = cr[u];
         const double pv = pr[u];
         if (b + PF < NM) {
-          cr[u] = cn[0];
-          pr[u] = pn[0];
+          cr[u] = __ldcg(cn);
+          pr[u] = __ldcg(pn);
           cn += rs;
           pn += rs;
         }
@@ -1020,8 +1022,8 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
   const double *pb = pm + (long long)top * rs;
 #pragma unroll
   for (int u = 0; u < PF; ++u) {
-    cr[u] = u < NM ? cb[0] : mk<T>((T)0, (T)0);
-    pr[u] = u < NM ? pb[0] : 0.0;
+    cr[u] = u < NM ? __ldcg(cb) : mk<T>((T)0, (T)0);
+    pr[u] = u < NM ? __ldcg(pb) : 0.0;
     if (u < NM) { cb -= rs; pb -= rs; }
   }
   double xx = 0.0, xy = 0.0;
@@ -1034,8 +1036,8 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
         const T2<T> cv = cr[u];
         const double pv = pr[u];
         if (b - PF >= 0) {
-          cr[u] = cb[0];
-          pr[u] = pb[0];
+          cr[u] = __ldcg(cb);
+          pr[u] = __ldcg(pb);
           cb -= rs;
           pb -= rs;
         }
@@ -1344,10 +1346,11 @@ void launch_dft_z(const Spec &s, const T *R, T2<T> *C, const T2<T> *tz, int inve
 template <typename T>
 void launch_thomas(const Spec &s, T2<T> *C, const double *piv, const double *dl, const double *du, double *H0,
                    int klow, cudaStream_t st) {
-  // rows in flight per thread: 12 in FP32 (80 registers; 4, 6 and 8 measured
-  // slower at 814 x 257 x 193), 16 in FP64
+  // rows in flight per thread: 24 in FP32 (the row loads bypass L1, whose
+  // capacity capped the ring at 12 rows: 0.75 -> 0.67 ms per step at
+  // 814 x 257 x 193; more rows would cost the one-wave occupancy), 16 in FP64
   dim3 grid((s.N + 127) / 128, s.MH);  // 128 kx of one kz per CTA
-  k_thomas<T, sizeof(T) == 4 ? 12 : 16><<<grid, 128, 0, st>>>(s, C, piv, dl, du, H0, klow);
+  k_thomas<T, sizeof(T) == 4 ? 24 : 16><<<grid, 128, 0, st>>>(s, C, piv, dl, du, H0, klow);
 }
 
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
