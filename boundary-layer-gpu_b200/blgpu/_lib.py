@@ -73,6 +73,8 @@ _SIGS = {
     "blgpu_set_nu_t": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "blgpu_upload_state": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, ctypes.c_double]),
     "blgpu_download_state": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 5),
+    "blgpu_upload_state_async": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, ctypes.c_double]),
+    "blgpu_download_state_async": (ctypes.c_int, [ctypes.c_void_p] + [c_double_p] * 3),
     "blgpu_compute_dt": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "blgpu_set_dt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "blgpu_get_time": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),

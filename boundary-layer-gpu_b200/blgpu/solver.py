@@ -132,6 +132,23 @@ class Solver:
         self._ck(self.lib.blgpu_download_state(self.ctx, _p(U), _p(V), _p(W), _p(P), ctypes.byref(t)))
         return U, V, W, P, t.value
 
+    def upload_state_async(self, U, V, W, t=0.0):
+        """Streamed upload (returns at once): U, V, W must be Fortran-ordered
+        float64 arrays of the state's shapes, pinned for the copy to overlap,
+        and left untouched until sync()."""
+        for a, sh in ((U, (self.nx, self.nyg, self.nzg)), (V, (self.nxg, self.ny, self.nzg)),
+                      (W, (self.nxg, self.nyg, self.nz))):
+            assert a.dtype == np.float64 and a.flags.f_contiguous and a.shape == sh
+        self._ck(self.lib.blgpu_upload_state_async(self.ctx, _p(U), _p(V), _p(W), float(t)))
+
+    def download_state_async(self, U, V, W):
+        """Streamed download of U, V, W into the given arrays (as
+        upload_state_async), complete after sync()."""
+        for a, sh in ((U, (self.nx, self.nyg, self.nzg)), (V, (self.nxg, self.ny, self.nzg)),
+                      (W, (self.nxg, self.nyg, self.nz))):
+            assert a.dtype == np.float64 and a.flags.f_contiguous and a.shape == sh
+        self._ck(self.lib.blgpu_download_state_async(self.ctx, _p(U), _p(V), _p(W)))
+
     # -- the reference's files -------------------------------------------------
     def output_data(self, fileout, step, rescaling=False):
         """output_data: writes fileout.<step> (one-process layout), links

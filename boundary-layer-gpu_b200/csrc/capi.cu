@@ -72,6 +72,11 @@ struct blgpu_ctx {
   FftPlan<double> pl64{};
   FftPlan<float> pl32{};
   double *stage = nullptr;  // FP64 staging of one host-layout field
+  // streamed transfers: H2D and D2H streams, per-field staging buffers and
+  // the events that order them against st
+  cudaStream_t xin = nullptr, xout = nullptr;
+  double *stage_in[3] = {nullptr, nullptr, nullptr}, *stage_out[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_free = nullptr;
   double *d_cs2 = nullptr;  // (Cs Delta_j f)^2 of the Smagorinsky model, j = 0..nyg
   double *d_stats = nullptr;
   double *d_utau = nullptr;
@@ -404,8 +409,14 @@ int blgpu_destroy(blgpu_ctx *ctx) {
   for (int r = 0; r < 3; ++r)
     if (ctx->graph[r]) cudaGraphExecDestroy(ctx->graph[r]);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->xin) cudaStreamSynchronize(ctx->xin);
+  if (ctx->xout) cudaStreamSynchronize(ctx->xout);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->st) cudaStreamDestroy(ctx->st);
+  if (ctx->xin) cudaStreamDestroy(ctx->xin);
+  if (ctx->xout) cudaStreamDestroy(ctx->xout);
+  for (cudaEvent_t e : {ctx->ev_in_ready, ctx->ev_in_free, ctx->ev_out_ready, ctx->ev_out_free})
+    if (e) cudaEventDestroy(e);
   delete ctx;
   return BLGPU_OK;
 }
@@ -797,6 +808,99 @@ int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const d
   return BLGPU_OK;
 }
 
+// t, to and the dt maxima of a newly uploaded state, on the compute stream
+static __global__ void k_reset_scalars(Scalars *sc, double t) {
+  sc->t = t;
+  sc->to = t;
+  sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
+}
+
+// streams, staging buffers and events of the streamed transfers (first use)
+static int xfer_setup(blgpu_ctx *ctx) {
+  if (ctx->xin) return BLGPU_OK;
+  const size_t n = (size_t)ctx->nxg * ctx->nyg * ctx->nzg * sizeof(double);
+  for (int f = 0; f < 3; ++f) {
+    int rc = dalloc(ctx, (void **)&ctx->stage_in[f], n);
+    if (!rc) rc = dalloc(ctx, (void **)&ctx->stage_out[f], n);
+    if (rc) return rc;
+  }
+  for (cudaEvent_t *e : {&ctx->ev_in_ready, &ctx->ev_in_free, &ctx->ev_out_ready, &ctx->ev_out_free})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  // the "free" events start completed, so the first transfers do not wait
+  CK(cudaEventRecord(ctx->ev_in_free, ctx->st));
+  CK(cudaEventRecord(ctx->ev_out_free, ctx->st));
+  CK(cudaStreamCreateWithFlags(&ctx->xout, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->xin, cudaStreamNonBlocking));
+  return BLGPU_OK;
+}
+
+int blgpu_upload_state_async(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t) {
+  if (!ctx || !U || !V || !W) return set_err(ctx, BLGPU_EINVAL, "blgpu_upload_state_async: null argument");
+  CK(cudaSetDevice(ctx->cfg.device));
+  int rc = xfer_setup(ctx);
+  if (rc) return rc;
+  const double *src[3] = {U, V, W};
+  const int dims[3][3] = {{ctx->nx, ctx->nyg, ctx->nzg}, {ctx->nxg, ctx->ny, ctx->nzg}, {ctx->nxg, ctx->nyg, ctx->nz}};
+  // H2D once the previous upload's repack has read the staging buffers
+  CK(cudaStreamWaitEvent(ctx->xin, ctx->ev_in_free, 0));
+  for (int f = 0; f < 3; ++f)
+    CK(cudaMemcpyAsync(ctx->stage_in[f], src[f], (size_t)dims[f][0] * dims[f][1] * dims[f][2] * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->xin));
+  CK(cudaEventRecord(ctx->ev_in_ready, ctx->xin));
+  // repack on the compute stream, after whatever it was doing
+  CK(cudaStreamWaitEvent(ctx->st, ctx->ev_in_ready, 0));
+  ctx->cur = 0;
+  ctx->old = 1;
+  for (int f = 0; f < 3; ++f) {
+    if (ctx->fp64)
+      launch_repack<double>(ctx->geo_box(), 0, ctx->stage_in[f], (double *)ctx->S[0][f], dims[f][0], dims[f][1],
+                            dims[f][2], ctx->st);
+    else
+      launch_repack<float>(ctx->geo_box(), 0, ctx->stage_in[f], (float *)ctx->S[0][f], dims[f][0], dims[f][1],
+                           dims[f][2], ctx->st);
+    ctx->launches += 1;
+  }
+  CK(cudaEventRecord(ctx->ev_in_free, ctx->st));
+  for (int q = 0; q < 3; ++q)
+    CK(cudaMemcpyAsync(ctx->S[1][q], ctx->S[0][q], (size_t)ctx->boxn * ctx->esz, cudaMemcpyDeviceToDevice, ctx->st));
+  k_reset_scalars<<<1, 1, 0, ctx->st>>>(ctx->sc, t);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  ctx->have_state = true;
+  return BLGPU_OK;
+}
+
+int blgpu_download_state_async(blgpu_ctx *ctx, double *U, double *V, double *W) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  if (!ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_download_state_async: no state uploaded");
+  CK(cudaSetDevice(ctx->cfg.device));
+  int rc = xfer_setup(ctx);
+  if (rc) return rc;
+  double *dst[3] = {U, V, W};
+  const int dims[3][3] = {{ctx->nx, ctx->nyg, ctx->nzg}, {ctx->nxg, ctx->ny, ctx->nzg}, {ctx->nxg, ctx->nyg, ctx->nz}};
+  // repack into the staging buffers once the previous download has read them
+  CK(cudaStreamWaitEvent(ctx->st, ctx->ev_out_free, 0));
+  for (int f = 0; f < 3; ++f) {
+    if (!dst[f]) continue;
+    if (ctx->fp64)
+      launch_repack<double>(ctx->geo_box(), 1, ctx->stage_out[f], (double *)ctx->S[ctx->cur][f], dims[f][0],
+                            dims[f][1], dims[f][2], ctx->st);
+    else
+      launch_repack<float>(ctx->geo_box(), 1, ctx->stage_out[f], (float *)ctx->S[ctx->cur][f], dims[f][0],
+                           dims[f][1], dims[f][2], ctx->st);
+    ctx->launches += 1;
+  }
+  CK(cudaEventRecord(ctx->ev_out_ready, ctx->st));
+  CK(cudaStreamWaitEvent(ctx->xout, ctx->ev_out_ready, 0));
+  for (int f = 0; f < 3; ++f)
+    if (dst[f])
+      CK(cudaMemcpyAsync(dst[f], ctx->stage_out[f], (size_t)dims[f][0] * dims[f][1] * dims[f][2] * sizeof(double),
+                         cudaMemcpyDeviceToHost, ctx->xout));
+  CK(cudaEventRecord(ctx->ev_out_free, ctx->xout));
+  CK(cudaGetLastError());
+  return BLGPU_OK;
+}
+
 int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double *P, double *t) {
   if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
   if (!ctx->have_state) return set_err(ctx, BLGPU_ESTATE, "blgpu_download_state: no state uploaded");
@@ -1055,6 +1159,8 @@ int blgpu_sync(blgpu_ctx *ctx) {
   if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
   CK(cudaSetDevice(ctx->cfg.device));
   CK(cudaStreamSynchronize(ctx->st));
+  if (ctx->xin) CK(cudaStreamSynchronize(ctx->xin));
+  if (ctx->xout) CK(cudaStreamSynchronize(ctx->xout));
   return device_flag(ctx);
 }
 

@@ -122,6 +122,17 @@ int blgpu_get_grid(blgpu_ctx *ctx, double *x, double *y, double *z);
  * Upload also sets Uo = U as read_input_data does (input_output.f90:476-478). */
 int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
 int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double *P, double *t);
+/* Streamed variants for passing a sequence of states through the solver:
+ * they return at once; the host-to-device copies run on their own stream,
+ * the device-to-host copies on another, each through its own device staging
+ * buffers, ordered against the context's compute stream by events, so that
+ * the upload of the next state, the steps of the current one and the
+ * download of the previous one overlap (PCIe is full duplex).  Host arrays
+ * must be pinned for the copies to be asynchronous and must not be touched
+ * until blgpu_sync returns; the state semantics are those of
+ * blgpu_upload_state / blgpu_download_state (U, V, W; no pressure, no time). */
+int blgpu_upload_state_async(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
+int blgpu_download_state_async(blgpu_ctx *ctx, double *U, double *V, double *W);
 
 /* compute_dt (time_integration.f90:528-591): device reduction, no host copy
  * of the fields; the resulting dt is returned and kept on the device */
