@@ -679,7 +679,8 @@ __device__ __forceinline__ double mode_sum(const double2 *__restrict__ q, int ld
 template <typename T>
 __global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W,
                        const T *__restrict__ Uo, const T *__restrict__ Vo, const T *__restrict__ Wo,
-                       const Scalars *__restrict__ sc, double rkt, double *__restrict__ qx_part) {
+                       Scalars *__restrict__ sc, double rkt, double *__restrict__ qx_part, double qy,
+                       double length_y) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;  // 1..nyg
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;  // 1..nzg
   double q = 0.0;
@@ -756,7 +757,22 @@ __global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T
     if (tid < s) red[tid] += red[tid + s];
     __syncthreads();
   }
-  if (tid == 0) qx_part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+  // the last block to finish sums the partials in block order (the same
+  // fixed order for every launch) and leaves the flux correction in sc->dU
+  // (:240-260); the arrival counter sits after the partials
+  const int nparts = gridDim.x * gridDim.y;
+  unsigned int *arrived = reinterpret_cast<unsigned int *>(qx_part + nparts);
+  if (tid == 0) {
+    qx_part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+    __threadfence();
+    if (atomicAdd(arrived, 1u) == (unsigned)(nparts - 1)) {
+      __threadfence();
+      double qx = 0.0;
+      for (int p = 0; p < nparts; ++p) qx += __ldcg(qx_part + p);
+      sc->dU = (qx + qy) / length_y / (double)(g.nzg - 3);
+      *arrived = 0u;
+    }
+  }
 }
 
 template <typename T>
@@ -813,18 +829,9 @@ __global__ void k_bc_y(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T
 }
 
 template <typename T>
-__global__ void k_bc_mass(Geo g, T *__restrict__ U, const double *__restrict__ qx_part, int nparts, double qy,
-                          double length_y, Scalars *__restrict__ sc) {
-  // :240-260.  Every block sums the partials in the same fixed order.
-  __shared__ double s_du;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    double qx = 0.0;
-    for (int p = 0; p < nparts; ++p) qx += qx_part[p];
-    double du = (qx + qy) / length_y / (double)(g.nzg - 3);
-    s_du = du;
-    if (blockIdx.x == 0 && blockIdx.y == 0) sc->dU = du;
-  }
-  __syncthreads();
+__global__ void k_bc_mass(Geo g, T *__restrict__ U, const Scalars *__restrict__ sc) {
+  // :240-260: the correction k_bc_x's last block left in sc->dU
+  const double s_du = sc->dU;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
   if (j > g.nyg || k > g.nzg) return;
@@ -1230,10 +1237,10 @@ void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, co
                Scalars *sc, double rkt, double *qx_part, double qy, double length_y, cudaStream_t st) {
   dim3 b(32, 8);
   dim3 gx((g.nyg + 31) / 32, (g.nzg + 7) / 8);
-  k_bc_x<T><<<gx, b, 0, st>>>(g, bc, U, V, W, Uo, Vo, Wo, sc, rkt, qx_part);
+  k_bc_x<T><<<gx, b, 0, st>>>(g, bc, U, V, W, Uo, Vo, Wo, sc, rkt, qx_part, qy, length_y);
   k_bc_z<T><<<dim3((g.nxg + 31) / 32, (g.nyg + 7) / 8), b, 0, st>>>(g, U, V, W);
   k_bc_y<T><<<dim3((g.nxg + 31) / 32, (g.nzg + 7) / 8), b, 0, st>>>(g, bc, U, V, W);
-  k_bc_mass<T><<<gx, b, 0, st>>>(g, U, qx_part, (int)(gx.x * gx.y), qy, length_y, sc);
+  k_bc_mass<T><<<gx, b, 0, st>>>(g, U, sc);
 }
 
 template <typename T>
