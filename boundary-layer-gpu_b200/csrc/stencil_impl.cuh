@@ -760,15 +760,28 @@ __global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T
   // the last block to finish sums the partials in block order (the same
   // fixed order for every launch) and leaves the flux correction in sc->dU
   // (:240-260); the arrival counter sits after the partials
-  const int nparts = gridDim.x * gridDim.y;
+  const int nparts = gridDim.x * gridDim.y, nt = blockDim.x * blockDim.y;
   unsigned int *arrived = reinterpret_cast<unsigned int *>(qx_part + nparts);
+  __shared__ int last;
   if (tid == 0) {
     qx_part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
     __threadfence();
-    if (atomicAdd(arrived, 1u) == (unsigned)(nparts - 1)) {
-      __threadfence();
-      double qx = 0.0;
-      for (int p = 0; p < nparts; ++p) qx += __ldcg(qx_part + p);
+    last = atomicAdd(arrived, 1u) == (unsigned)(nparts - 1);
+  }
+  __syncthreads();
+  if (last) {
+    // the block loads the partials in parallel, thread 0 adds them in order
+    __threadfence();
+    double qx = 0.0;
+    for (int p0 = 0; p0 < nparts; p0 += nt) {
+      const int n = min(nt, nparts - p0);
+      if (tid < n) red[tid] = __ldcg(qx_part + p0 + tid);
+      __syncthreads();
+      if (tid == 0)
+        for (int p = 0; p < n; ++p) qx += red[p];
+      __syncthreads();
+    }
+    if (tid == 0) {
       sc->dU = (qx + qy) / length_y / (double)(g.nzg - 3);
       *arrived = 0u;
     }
