@@ -70,8 +70,9 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % index) if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else "/tmp/blgpu_clocks_%d_%d.csv" % (os.getpid(), index)
+        d = os.environ.get("BLGPU_CLOCKS_DIR")  # where to keep the raw samples (default: a temporary file)
+        self.out = os.path.join(d, "clocks_rank%d.csv" % index) if d and os.path.isdir(d) else \
+            "/tmp/blgpu_clocks_%d_%d.csv" % (os.getpid(), index)
 
     def start(self):
         try:

@@ -6,7 +6,7 @@ divergence free and stepped by the solver; at a few early snapshots every
 wall point of the rows between `lo` and `hi` (delta99 units) gives a sample
 (u, w, ln(h|u|/nu)/10, 100 h dP/dx) -> 1000 (tau_x, tau_z), the stress of
 the resolved wall gradient.  The WallNet is trained on those samples on the
-GPU.  It is judged against the equilibrium law of the wall
+GPU.  It is checked against the equilibrium law of the wall
 (wallmodel.f90:1951-1985) on a coarse wall-modelled grid: the mean skin
 friction 2 <tau_x> of the two models on the same states, and of runs that
 use each model as the Neumann wall condition.  The same grid with the
@@ -18,7 +18,7 @@ from . import cases
 from ._lib import MIXED
 
 # mean profiles whose log layer follows the equilibrium model's law
-# u+ = ln(y+)/0.38 + 5.2, so the judge compares like with like
+# u+ = ln(y+)/0.38 + 5.2, so the comparison is like with like
 LOG_LAW = dict(kappa=cases.KAPPA_WM, C=cases.reichardt_c(cases.KAPPA_WM, cases.B_WM))
 
 

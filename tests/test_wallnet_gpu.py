@@ -1,7 +1,7 @@
 """The learned wall-stress model on the GPU: the tensor-core network against
 the CPU oracle (forward pass and gradient), deterministic training, the
 training-sample extractor, the wall-model hooks of the step against the
-oracle, and the learned model judged by the equilibrium law of the wall
+oracle, and the learned model checked against the equilibrium law of the wall
 (wallmodel.f90:1951-1985): mean skin friction within 2 % of it on a coarse
 wall-modelled grid, and what it gains over the no-slip wall there."""
 import numpy as np
