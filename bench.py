@@ -37,7 +37,7 @@ PASSES_PER_STEP = 73
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nx", type=int, default=814)
@@ -81,12 +81,15 @@ class Clocks:
                 ["nvidia-smi", "-i", str(self.index),
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,timestamp",
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
+        """Median SM clock, its maximum and the throttle reasons seen, over
+        the samples taken between the host times t0 and t1 (the timed region;
+        all samples when none fall inside)."""
         if not self.proc:
             return None
         self.proc.terminate()
@@ -95,24 +98,25 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.fh.close()
-        sm, mx, reasons = [], [], set()
+        import datetime
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.out):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[9], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[1]), float(f[2]), {n for n, v in zip(names, f[5:9]) if v.lower() == "active"}))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        inside = [r for r in rows if t0 is not None and t0 <= r[0] <= t1]
+        use = inside if inside else rows
+        if not use:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = set().union(*(r[3] for r in use))
+        return {"sm_mhz": float(np.median([r[1] for r in use])), "sm_max_mhz": float(max(r[2] for r in use)),
+                "reasons": sorted(reasons), "samples": len(use), "in_timed_region": bool(inside)}
 
 
 def dist_setup(args):
@@ -185,7 +189,10 @@ def run_reference(args, rank, world, pg):
     o.compute_dt()
     stage = 1
     times = []
-    for it in range(args.warmup + args.steps):
+    # at most 24 timed substeps (about 2.2 s each on 16 cores at 814x257x193), so
+    # that any --steps keeps the run within a few minutes
+    nt = min(args.steps, 24)
+    for it in range(args.warmup + nt):
         t0 = time.perf_counter()
         o.rk3_stage(stage)
         el = time.perf_counter() - t0
@@ -203,7 +210,7 @@ def run_reference(args, rank, world, pg):
             "config": {"workload": "turbulent BL %dx%dx%d RK3 CFL 0.5, Lund inflow (flag 3), CPU restatement of "
                                    "the reference step" % (args.nx, args.ny, args.nz), "cells": case.cells},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "one RK3 substep of the full box per timed step, x3 per step"},
+                             "sample": "one RK3 substep of the full box per timed step (%d timed), x3 per step" % nt},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -321,13 +328,17 @@ def main():
     N, M, NM = case.nx - 2, case.nz - 2, case.ny - 1
     spectral_cells = N * M * NM
 
+    span = {}
+
     def timed_run(precision):
         s = cases.solver_for(case, precision=precision, device=dev)
         s.advance(args.warmup)
         s.sync()
         barrier(pg, local)
         l0 = s.kernel_launches()
+        t0 = time.time()
         ms = s.advance_timed(args.steps)
+        span[precision] = (t0, time.time())
         launches = s.kernel_launches() - l0
         barrier(pg, local)
         return s, ms, launches
@@ -337,7 +348,7 @@ def main():
     # ---- mixed form (headline) ----
     clocks.start()
     smix, ms_mix, launches = timed_run(blgpu.MIXED)
-    clk = clocks.stop()
+    clk = clocks.stop(*span[blgpu.MIXED])
     ms_mix = allmax(pg, ms_mix, local)
     ms_step_mix = ms_mix / args.steps
     value = ms_step_mix * 1e6 / (cells * world)
