@@ -1192,6 +1192,8 @@ int xfft_split(int n) {
   switch (n) {
     case 812: return 29;  // 29 x 28
     case 510: return 17;  // 17 x 30
+    case 190: return 19;  // 19 x 10 (ensemble boxes nx = 192)
+    case 126: return 14;  // 14 x 9 (ensemble boxes nx = 128)
     default: return 0;
   }
 }
@@ -1271,6 +1273,8 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
   if constexpr (sizeof(T) == 4) {
     if (split == 29) return launch_div_dct_e<T, TwoPassX<29, 28>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
     if (split == 17) return launch_div_dct_e<T, TwoPassX<17, 30>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
+    if (split == 19) return launch_div_dct_e<T, TwoPassX<19, 10>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
+    if (split == 14) return launch_div_dct_e<T, TwoPassX<14, 9>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
   }
   switch (radix_class(pl.rad, pl.nst)) {
     case 7: launch_div_dct_e<T, StockhamX<T, 7>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
@@ -1306,8 +1310,12 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
     const bool fused = idct2_fits(s, split) && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
     if (split == 29 && fused) return launch_idct2<29, 28>(g, s, pl, R, p, nw, sm, grid, err, st);
     if (split == 17 && fused) return launch_idct2<17, 30>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 19 && fused) return launch_idct2<19, 10>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 14 && fused) return launch_idct2<14, 9>(g, s, pl, R, p, nw, sm, grid, err, st);
     if (split == 29) return launch_idct_e<T, TwoPassX<29, 28>>(g, s, pl, R, p, nw, sm, grid, st);
     if (split == 17) return launch_idct_e<T, TwoPassX<17, 30>>(g, s, pl, R, p, nw, sm, grid, st);
+    if (split == 19) return launch_idct_e<T, TwoPassX<19, 10>>(g, s, pl, R, p, nw, sm, grid, st);
+    if (split == 14) return launch_idct_e<T, TwoPassX<14, 9>>(g, s, pl, R, p, nw, sm, grid, st);
   }
   switch (radix_class(pl.rad, pl.nst)) {
     case 7: launch_idct_e<T, StockhamX<T, 7>>(g, s, pl, R, p, nw, sm, grid, st); break;

@@ -238,7 +238,8 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
  * in shared memory, any N; 2 = two-pass register FFT, built for
- * N = nx-2 = 812 (29 x 28) and 510 (17 x 30)); 0 = the built-in choice.
+ * N = nx-2 = 812 (29 x 28), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9));
+ * 0 = the built-in choice.
  * Values not passed keep their current setting.  All but zdft, rhs_pts and
  * xfft leave results unchanged; those change them at FP32 rounding level.  No counterpart in the
  * reference (its OpenACC loops take compiler-chosen gangs). */

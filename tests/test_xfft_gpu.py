@@ -1,7 +1,8 @@
 """The mixed form's x transforms (divergence + DCT-II, inverse DCT): the
 two-pass register FFT (N = nx-2 = A B, compile-time indices) against the
-Stockham shared-memory FFT and the FP64 path, at the two built lengths
-(812 = 29 x 28, 510 = 17 x 30), for one projection and for a few steps."""
+Stockham shared-memory FFT and the FP64 path, at the built lengths
+(812 = 29 x 28, 510 = 17 x 30, 190 = 19 x 10, 126 = 14 x 9), for one
+projection and for a few steps."""
 import numpy as np
 import pytest
 
@@ -25,7 +26,8 @@ def noisy(nx, ny, nz, seed):
 
 
 # (814, 10, 13): an odd number of lines (9 x 11), so the last warp holds one real line
-@pytest.mark.parametrize("nx,ny,nz", [(814, 9, 12), (814, 17, 33), (512, 13, 20), (814, 10, 13)])
+@pytest.mark.parametrize("nx,ny,nz", [(814, 9, 12), (814, 17, 33), (512, 13, 20), (814, 10, 13), (192, 9, 12),
+                                      (128, 11, 14)])
 def test_two_pass_x_transform_matches_stockham_and_fp64(gpu, nx, ny, nz):
     c = noisy(nx, ny, nz, nx + ny)
     out = {}
