@@ -1,7 +1,7 @@
 """Build of the sm_100a shared library (libblgpu.so) from csrc/*.cu.
 
-nvcc cross-compiles for sm_100a without a GPU.  stencil64.cu is compiled
-with -fmad=false so that the FP64 stencil kernels evaluates each expression with the
+nvcc cross-compiles for sm_100a without a GPU.  stencil64.cu and
+dynsgs.cu are compiled with -fmad=false so that the FP64 stencil kernels evaluate each expression with the
 rounding of the Fortran source; the transform kernels keep fused multiply-adds.
 The library is written in-tree (lib/libblgpu.so) so that it ships with the
 source tree to the GPU host.
@@ -20,6 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 SOURCES = {
     "stencil64.cu": ["-fmad=false"],
+    "dynsgs.cu": ["-fmad=false"],
     "stencil32.cu": [],
     "spectral.cu": [],
     "capi.cu": [],

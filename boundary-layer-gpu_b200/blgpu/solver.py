@@ -226,7 +226,8 @@ class Solver:
 
     # -- models and diagnostics -------------------------------------------
     def compute_eddy_viscosity(self):
-        """sgs_Smagorinsky on the resident state; returns nu_t(nxg,nyg,nzg)."""
+        """The context's LES model on the resident state (LES = 1
+        sgs_Smagorinsky; 2, 3 the dynamic model); returns nu_t(nxg,nyg,nzg)."""
         self._ck(self.lib.blgpu_eddy_viscosity(self.ctx))
         return self.nu_t()
 

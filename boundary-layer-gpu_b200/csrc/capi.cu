@@ -53,6 +53,7 @@ struct blgpu_ctx {
   void *S[3][3] = {};  // state buffers [buffer][u,v,w]
   void *F1[3] = {};
   void *P = nullptr, *nut = nullptr, *rhs_p = nullptr, *R = nullptr, *C = nullptr;
+  double *dyn = nullptr;  // LES = 2, 3: dynamic-model work arrays (FP64)
   double *piv = nullptr, *qx_part = nullptr;
   // mixed form: the low-kx kz = 0 part of the pressure in FP64: p0 [NM][N], its modes
   // H0 [NM][klow], FP32 differences [2][NM][N], inverse-cosine matrix cm [klow][N]
@@ -227,11 +228,9 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   if (cfg->rk_scheme < 1 || cfg->rk_scheme > 3)
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: RKscheme %d not in {1,2,3}", cfg->rk_scheme);
   // LES as in compute_eddy_viscosity (subgrid.f90:23-47): 0 none, 1 constant-coefficient
-  // Smagorinsky; 2 and 3 (dynamic Smagorinsky) are not built; BLGPU_LES_HOST: nu_t from the host
-  if (cfg->les_model == 2 || cfg->les_model == 3)
-    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: LES=%d (dynamic Smagorinsky, subgrid.f90:261-583) is not built",
-                   cfg->les_model);
-  if (cfg->les_model != 0 && cfg->les_model != 1 && cfg->les_model != BLGPU_LES_HOST)
+  // Smagorinsky, 2 dynamic Smagorinsky with the coefficient averaged in z, 3 dynamic
+  // Smagorinsky pointwise; BLGPU_LES_HOST: nu_t from the host
+  if (cfg->les_model != BLGPU_LES_HOST && (cfg->les_model < 0 || cfg->les_model > 3))
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown LES model %d", cfg->les_model);
   if (cfg->precision != BLGPU_FP64 && cfg->precision != BLGPU_MIXED)
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown precision %d", cfg->precision);
@@ -265,6 +264,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, &ctx->P, box));
   TRY(dalloc(ctx, &ctx->rhs_p, box));
   if (cfg->les_model) TRY(dalloc(ctx, &ctx->nut, box));
+  if (cfg->les_model == 2 || cfg->les_model == 3)
+    TRY(dalloc(ctx, (void **)&ctx->dyn, dyn_smagorinsky_work_bytes(ctx->nxg, ctx->nyg, ctx->nzg)));
   Spec &s = ctx->spec;
   s.N = ctx->nx - 2;
   s.M = ctx->nz - 2;
@@ -1073,6 +1074,11 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
       ph_begin(ctx, PH_MISC);
       launch_smagorinsky<T>(ctx->geo, Si[0], Si[1], Si[2], ctx->d_cs2, (T *)ctx->nut, ctx->st);
       ph_end(ctx, 1);
+    } else if (ctx->dyn) {  // dynamic Smagorinsky, same place (LES = 2, 3)
+      T **Si = reinterpret_cast<T **>(ctx->S[in]);
+      ph_begin(ctx, PH_MISC);
+      ph_end(ctx, launch_dyn_smagorinsky<T>(ctx->geo, Si[0], Si[1], Si[2], ctx->dyn, ctx->cfg.les_model,
+                                            (T *)ctx->nut, ctx->st));
     }
     if (ctx->wm_mode) {  // wall model from the substep's state (time_integration.f90:341-346)
       T **Si = reinterpret_cast<T **>(ctx->S[in]);
@@ -1357,12 +1363,20 @@ int blgpu_eddy_viscosity(blgpu_ctx *ctx) {
   CK(cudaSetDevice(ctx->cfg.device));
   if (ctx->fp64) {
     double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
-    launch_smagorinsky<double>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (double *)ctx->nut, ctx->st);
+    if (ctx->dyn)
+      ctx->launches += launch_dyn_smagorinsky<double>(ctx->geo, S[0], S[1], S[2], ctx->dyn, ctx->cfg.les_model,
+                                                      (double *)ctx->nut, ctx->st);
+    else
+      launch_smagorinsky<double>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (double *)ctx->nut, ctx->st);
   } else {
     float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
-    launch_smagorinsky<float>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (float *)ctx->nut, ctx->st);
+    if (ctx->dyn)
+      ctx->launches += launch_dyn_smagorinsky<float>(ctx->geo, S[0], S[1], S[2], ctx->dyn, ctx->cfg.les_model,
+                                                     (float *)ctx->nut, ctx->st);
+    else
+      launch_smagorinsky<float>(ctx->geo, S[0], S[1], S[2], ctx->d_cs2, (float *)ctx->nut, ctx->st);
   }
-  ctx->launches += 1;
+  if (!ctx->dyn) ctx->launches += 1;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));
   return BLGPU_OK;

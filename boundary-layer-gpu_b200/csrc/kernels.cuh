@@ -82,6 +82,12 @@ void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned lo
 
 template <typename T>
 void launch_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, const double *cs2, T *nut, cudaStream_t st);
+// dynamic Smagorinsky (LES = 2 z-averaged, 3 pointwise), FP64 on dense work arrays;
+// returns the number of kernels launched
+size_t dyn_smagorinsky_work_bytes(int nxg, int nyg, int nzg);
+template <typename T>
+int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, double *work, int model, T *nut,
+                           cudaStream_t st);
 template <typename T>
 void launch_stats(const Geo &g, const T *U, const T *V, const T *W, const T *P, const T *nut, double *out,
                   cudaStream_t st);

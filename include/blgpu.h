@@ -50,10 +50,12 @@ typedef struct blgpu_config {
   double cfl;         /* CFL; < 0 means fixed dt = -CFL (time_integration.f90:539) */
   double dpdx, dpdz;  /* dPdx, dPdz (params.f90:152-153) */
   int rk_scheme;      /* RKscheme: 1 Euler, 2 RK2, 3 RK3 (params.f90:195) */
-  int les_model;      /* LES: 0 DNS; 1 constant-coefficient Smagorinsky computed on the device
-                         before every substep (subgrid.f90:609-730); BLGPU_LES_HOST: eddy
-                         viscosity given by blgpu_set_nu_t and held fixed.  The reference's
-                         2 and 3 (dynamic Smagorinsky) are refused with BLGPU_EINVAL */
+  int les_model;      /* LES, nu_t computed on the device before every substep: 0 DNS;
+                         1 constant-coefficient Smagorinsky (subgrid.f90:609-730); 2 dynamic
+                         Smagorinsky, coefficient averaged in z (subgrid.f90:261-414); 3 dynamic
+                         Smagorinsky, pointwise (subgrid.f90:420-583); 2 and 3 hold 29 FP64
+                         work arrays of nxg*nyg*nzg.  BLGPU_LES_HOST: eddy viscosity given by
+                         blgpu_set_nu_t and held fixed */
   int precision;      /* BLGPU_FP64 | BLGPU_MIXED */
   int poisson;        /* BLGPU_POISSON_NATIVE | BLGPU_POISSON_CUFFT */
   int device;         /* CUDA device ordinal */
@@ -185,8 +187,11 @@ long long blgpu_device_bytes(const blgpu_ctx *ctx);
  * nphase must be >= 10; kernels may be NULL. */
 int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels, int nphase);
 
-/* sgs_Smagorinsky (subgrid.f90:609-730) on the resident state: nu_t on the
- * interior i=2..nxg-1, j=2..nyg-1, k=2..nzg-1 (Cs = 0.11, f = 1) */
+/* the context's LES model on the resident state.  LES = 1: sgs_Smagorinsky
+ * (subgrid.f90:609-730), nu_t on the interior i=2..nxg-1, j=2..nyg-1,
+ * k=2..nzg-1 (Cs = 0.11, f = 1).  LES = 2, 3: the dynamic model
+ * (subgrid.f90:261-583), nu_t on the whole (nxg,nyg,nzg) array after clipping
+ * and the Neumann y ghosts. */
 int blgpu_eddy_viscosity(blgpu_ctx *ctx);
 /* nu_t(nxg,nyg,nzg); zeros for a context created with LES = 0 */
 int blgpu_get_nu_t(blgpu_ctx *ctx, double *nu_t);

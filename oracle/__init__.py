@@ -81,6 +81,7 @@ def load():
         lib.blo_zgtsv.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         lib.blo_dct2.argtypes = [ctypes.c_int, _dp, _dp]
         lib.blo_smagorinsky.argtypes = [ctypes.c_void_p]
+        lib.blo_dynamic_smagorinsky.argtypes = [ctypes.c_void_p]
         lib.blo_set_les.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.blo_get_nu_t.argtypes = [ctypes.c_void_p, _dp]
         lib.blo_statistics.argtypes = [ctypes.c_void_p] + [_dp] * 5
@@ -240,6 +241,18 @@ class Oracle:
         a = np.zeros((self.nxg, self.nyg, self.nzg), order="F")
         self.lib.blo_get_nu_t(self.h, _p(a))
         return a
+
+    def nu_t(self):
+        a = np.zeros((self.nxg, self.nyg, self.nzg), order="F")
+        self.lib.blo_get_nu_t(self.h, _p(a))
+        return a
+
+    def dynamic_smagorinsky(self, model):
+        """nu_t of the dynamic model (subgrid.f90:261-583): model 2 with the
+        coefficient averaged in z, 3 without; the oracle's LES flag is set to it."""
+        self.lib.blo_set_les(self.h, int(model))
+        self.lib.blo_dynamic_smagorinsky(self.h)
+        return self.nu_t()
 
     def statistics(self):
         nx, ny = self.nx, self.ny

@@ -1436,11 +1436,13 @@ void blo_get_rescaling(const blo_t *o, double *Umean_resc, double *Vmean_resc, d
 }
 
 void blo_smagorinsky(blo_t *o);
+void blo_dynamic_smagorinsky(blo_t *o);
 static void wall_model_eval(blo_t *o);
 static void substep(blo_t *o, int s, int rk_step, const double *coef, int nterms,
                     double tnew) {
   o->rk_step = rk_step;
   if (o->les == 1) blo_smagorinsky(o); /* time_integration.f90:341-346 */
+  else if (o->les >= 2) blo_dynamic_smagorinsky(o);
   if (o->wm) wall_model_eval(o);
   rhs_u_impl(o, o->U, o->V, o->W, o->Fu[s]);
   rhs_v_impl(o, o->U, o->V, o->W, o->Fv[s]);
@@ -1473,6 +1475,7 @@ void blo_step(blo_t *o) {
     /* Euler: U = Uo + dt*rhs(Uo); rk_step = 3 (time_integration.f90:24-114) */
     o->rk_step = 3;
     if (o->les == 1) blo_smagorinsky(o);
+    else if (o->les >= 2) blo_dynamic_smagorinsky(o);
     if (o->wm) wall_model_eval(o);
     rhs_u_impl(o, o->Uo, o->Vo, o->Wo, o->Fu[0]);
     rhs_v_impl(o, o->Uo, o->Vo, o->Wo, o->Fv[0]);
@@ -1561,6 +1564,230 @@ void blo_smagorinsky(blo_t *o) {
         NUT(i, j, k) = c2 * S;
       }
   }
+}
+
+/* ------------------------------------------------------------------------ */
+/* dynamic Smagorinsky, subgrid.f90:261-583: sgs_dynamic_Smagorinsky (LES=2, */
+/* z-averaged coefficient) and _noaverage (LES=3), with the filters of      */
+/* :69-184 (filter_xzy, fil_size = 2), compute_Sij (:672-730), the          */
+/* interpolations of interpolation.f90:24-114 and the x / z helpers of      */
+/* boundary_conditions.f90:295-344,732-888 for one process (the interior-    */
+/* plane exchange is then empty).  Every work array is a dense              */
+/* (nxg,nyg,nzg) array indexed 1-based like its Fortran counterpart (the    */
+/* velocity-shaped ones use the AU / AV / AW shapes); entries the source    */
+/* never sets stay zero here and never reach the output.                     */
+/* ------------------------------------------------------------------------ */
+#define AG(a, i, j, k) (a)[IX3(i, j, k, o->nxg, o->nyg)]
+
+/* apply_Neumann_bc_x / apply_periodic_bc_x (:295-344) on a dense array of first dimension d1 */
+static void dyn_bc_x(const blo_t *o, double *a, int d1, int d2, int d3, int id, int periodic) {
+  for (int k = 1; k <= d3; ++k)
+    for (int j = 1; j <= d2; ++j) {
+      double *r = a + IX3(1, j, k, d1, d2);
+      if (!periodic) {
+        if (id == 1) { r[0] = r[1]; r[o->nx - 1] = r[o->nx - 2]; }
+        else { r[0] = r[1]; r[o->nxg - 1] = r[o->nxg - 2]; }
+      } else {
+        if (id == 1) { r[0] = r[o->nx - 2]; r[o->nx - 1] = r[1]; }
+        else { r[0] = r[o->nxg - 3]; r[o->nxg - 2] = r[1]; r[o->nxg - 1] = r[2]; }
+      }
+    }
+}
+/* apply_periodic_bc_z (:732-760, one process) */
+static void dyn_bc_z(const blo_t *o, double *a, int d1, int d2, int id) {
+  const size_t pl = (size_t)d1 * d2;
+  if (id == 3) {
+    memcpy(a, a + (size_t)(o->nz - 2) * pl, pl * sizeof(double));
+    memcpy(a + (size_t)(o->nz - 1) * pl, a + pl, pl * sizeof(double));
+  } else {
+    memcpy(a, a + (size_t)(o->nzg - 3) * pl, pl * sizeof(double));
+    memcpy(a + (size_t)(o->nzg - 2) * pl, a + pl, pl * sizeof(double));
+    memcpy(a + (size_t)(o->nzg - 1) * pl, a + 2 * pl, pl * sizeof(double));
+  }
+}
+/* filter_xzy (:140-184) of the section a(1:n1, ja:jb, 1:n3) of a dense array
+ * of dims (d1,d2,*): g(i,j,k), i = 2..n1-1, j = ja..jb, k = 2..n3-1 (the
+ * section's own indices, which are the output's in every call of the model) */
+static void dyn_filter(const double *a, int d1, int d2, int n1, int ja, int jb, int n3, double *g, int e1, int e2) {
+  static const double fil[3][3] = {{1.0 / 36.0, 1.0 / 9.0, 1.0 / 36.0},
+                                   {1.0 / 9.0, 4.0 / 9.0, 1.0 / 9.0},
+                                   {1.0 / 36.0, 1.0 / 9.0, 1.0 / 36.0}};
+  for (int k = 2; k <= n3 - 1; ++k)
+    for (int j = ja; j <= jb; ++j)
+      for (int i = 2; i <= n1 - 1; ++i) {
+        double s = 0.0;
+        for (int di = -1; di <= 1; ++di)
+          for (int dk = -1; dk <= 1; ++dk) {
+            const int ii = i + di, kk = k + dk;
+            double y;
+            if (j == ja)
+              y = 2.0 / 3.0 * a[IX3(ii, j, kk, d1, d2)] + 1.0 / 3.0 * a[IX3(ii, j + 1, kk, d1, d2)];
+            else if (j == jb)
+              y = 1.0 / 3.0 * a[IX3(ii, j - 1, kk, d1, d2)] + 2.0 / 3.0 * a[IX3(ii, j, kk, d1, d2)];
+            else
+              y = 1.0 / 6.0 * a[IX3(ii, j - 1, kk, d1, d2)] + 2.0 / 3.0 * a[IX3(ii, j, kk, d1, d2)] +
+                  1.0 / 6.0 * a[IX3(ii, j + 1, kk, d1, d2)];
+            s = s + y * fil[di + 1][dk + 1];
+          }
+        g[IX3(i, j, k, e1, e2)] = s;
+      }
+}
+/* compute_Sij (:672-730) of (U_,V_,W_) shaped like U, V, W into Sg[6]
+ * (Sij(2:nxg,2:nyg,2:nzg,6)) and S (2:nxg-1,2:nyg-1,2:nzg-1); the corner
+ * averages run in place in the source's loop order */
+static void dyn_sij(const blo_t *o, const double *U_, const double *V_, const double *W_, double **Sg, double *S) {
+  const int nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        AG(Sg[0], i, j, k) = (AU(U_, i, j, k) - AU(U_, i - 1, j, k)) / (o->x[i] - o->x[i - 1]);
+        AG(Sg[1], i, j, k) = (AV(V_, i, j, k) - AV(V_, i, j - 1, k)) / (o->y[j] - o->y[j - 1]);
+        AG(Sg[2], i, j, k) = (AW(W_, i, j, k) - AW(W_, i, j, k - 1)) / (o->z[k] - o->z[k - 1]);
+      }
+  for (int k = 2; k <= nzg; ++k)
+    for (int j = 2; j <= nyg; ++j)
+      for (int i = 2; i <= nxg; ++i) {
+        AG(Sg[3], i, j, k) = sij_edge4(o, U_, V_, i, j, k);
+        AG(Sg[4], i, j, k) = sij_edge5(o, U_, W_, i, j, k);
+        AG(Sg[5], i, j, k) = sij_edge6(o, V_, W_, i, j, k);
+      }
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        AG(Sg[3], i, j, k) = 0.25 * (AG(Sg[3], i, j, k) + AG(Sg[3], i + 1, j, k) + AG(Sg[3], i, j + 1, k) +
+                                     AG(Sg[3], i + 1, j + 1, k));
+        AG(Sg[4], i, j, k) = 0.25 * (AG(Sg[4], i, j, k) + AG(Sg[4], i + 1, j, k) + AG(Sg[4], i, j, k + 1) +
+                                     AG(Sg[4], i + 1, j, k + 1));
+        AG(Sg[5], i, j, k) = 0.25 * (AG(Sg[5], i, j, k) + AG(Sg[5], i, j + 1, k) + AG(Sg[5], i, j, k + 1) +
+                                     AG(Sg[5], i, j + 1, k + 1));
+      }
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double s = 0.0;
+        for (int c = 0; c < 6; ++c) {
+          const double v = AG(Sg[c], i, j, k);
+          s = s + (c < 3 ? 2.0 : 4.0) * v * v;
+        }
+        AG(S, i, j, k) = pow(s, 0.5);
+      }
+}
+
+void blo_dynamic_smagorinsky(blo_t *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz, nxg = o->nxg, nyg = o->nyg, nzg = o->nzg;
+  const int avg = o->les == 2, per = o->les == 3;  /* LES = 3: x-periodic helpers */
+  const size_t n = (size_t)nxg * nyg * nzg;
+  double *term = dalloc(n), *term1 = dalloc(n), *term2 = dalloc(n), *S = dalloc(n);
+  double *Uf = dalloc(n), *Vf = dalloc(n), *Wf = dalloc(n);
+  double *tb[6], *L[6], *Sg[6], *M[6];
+  for (int c = 0; c < 6; ++c) { tb[c] = dalloc(n); L[c] = dalloc(n); Sg[c] = dalloc(n); M[c] = dalloc(n); }
+  const double *U = o->U, *V = o->V, *W = o->W;
+  /* Part 1: cell-centre velocities (interpolate_x/y/z, faces to centres) */
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 1; j <= nyg; ++j)
+      for (int i = 2; i <= nx; ++i) AG(term, i, j, k) = 0.5 * (AU(U, i - 1, j, k) + AU(U, i, j, k));
+  for (int k = 1; k <= nzg; ++k)
+    for (int j = 2; j <= ny; ++j)
+      for (int i = 1; i <= nxg; ++i) AG(term1, i, j, k) = 0.5 * (AV(V, i, j - 1, k) + AV(V, i, j, k));
+  for (int k = 2; k <= nz; ++k)
+    for (int j = 1; j <= nyg; ++j)
+      for (int i = 1; i <= nxg; ++i) AG(term2, i, j, k) = 0.5 * (AW(W, i, j, k - 1) + AW(W, i, j, k));
+  for (int j = 1; j <= nyg; ++j)
+    for (int i = 1; i <= nxg; ++i) AG(term2, i, j, nzg) = 0.0;  /* ui = 0 of interpolate_z */
+  dyn_bc_x(o, term, nxg, nyg, nzg, 2, per);
+  dyn_bc_z(o, term2, nxg, nyg, 4);
+  /* ui*uj at centres into ten_buf(2:nxg,2:nyg-1,2:nzg), its x / z ghosts, filtered */
+  const double *pa[6] = {term, term1, term2, term, term, term1}, *pb[6] = {term, term1, term2, term1, term2, term2};
+  for (int c = 0; c < 6; ++c) {
+    for (int k = 2; k <= nzg; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg; ++i) AG(tb[c], i, j, k) = AG(pa[c], i, j, k) * AG(pb[c], i, j, k);
+    dyn_bc_x(o, tb[c], nxg, nyg, nzg, 2, per);
+    dyn_bc_z(o, tb[c], nxg, nyg, 4);
+    dyn_filter(tb[c], nxg, nyg, nxg, 2, nyg - 1, nzg, L[c], nxg, nyg);  /* hat(ui uj) */
+  }
+  /* hat(ui) of the centre velocities into Sij(:,:,:,1:3) */
+  dyn_filter(term, nxg, nyg, nxg, 2, nyg - 1, nzg, Sg[0], nxg, nyg);
+  dyn_filter(term1, nxg, nyg, nxg, 2, nyg - 1, nzg, Sg[1], nxg, nyg);
+  dyn_filter(term2, nxg, nyg, nxg, 2, nyg - 1, nzg, Sg[2], nxg, nyg);
+  const int la[6] = {0, 1, 2, 0, 0, 1}, lb[6] = {0, 1, 2, 1, 2, 2};
+  for (int c = 0; c < 6; ++c)
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i)
+          AG(L[c], i, j, k) = AG(L[c], i, j, k) - AG(Sg[la[c]], i, j, k) * AG(Sg[lb[c]], i, j, k);
+  /* Part 2: filtered velocities, their x / z ghosts, hat(Sij), |hat(S)| */
+  dyn_filter(U, nx, nyg, nx, 1, nyg, nzg, Uf, nx, nyg);
+  dyn_filter(V, nxg, ny, nxg, 1, ny, nzg, Vf, nxg, ny);
+  dyn_filter(W, nxg, nyg, nxg, 1, nyg, nz, Wf, nxg, nyg);
+  dyn_bc_x(o, Uf, nx, nyg, nzg, 1, per);
+  dyn_bc_z(o, Uf, nx, nyg, 1);
+  dyn_bc_x(o, Vf, nxg, ny, nzg, 2, per);
+  dyn_bc_z(o, Vf, nxg, ny, 2);
+  dyn_bc_x(o, Wf, nxg, nyg, nz, 2, per);
+  dyn_bc_z(o, Wf, nxg, nyg, 3);
+  dyn_sij(o, Uf, Vf, Wf, Sg, S);
+  const double fs2 = pow(2.0, 2.0);  /* fil_size**2d0, fil_size = 2 after filter_xzy */
+  for (int c = 0; c < 6; ++c)
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AG(M[c], i, j, k) = fs2 * AG(S, i, j, k) * AG(Sg[c], i, j, k);
+  dyn_sij(o, U, V, W, Sg, S);
+  for (int c = 0; c < 6; ++c) {
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AG(term, i, j, k) = AG(S, i, j, k) * AG(Sg[c], i, j, k);
+    dyn_bc_x(o, term, nxg, nyg, nzg, 2, per);
+    dyn_bc_z(o, term, nxg, nyg, 4);
+    dyn_filter(term, nxg, nyg, nxg, 2, nyg - 1, nzg, Sg[c], nxg, nyg);  /* hat(|S| Sij) */
+  }
+  for (int c = 0; c < 6; ++c)
+    for (int k = 2; k <= nzg - 1; ++k)
+      for (int j = 2; j <= nyg - 1; ++j)
+        for (int i = 2; i <= nxg - 1; ++i) AG(M[c], i, j, k) = AG(M[c], i, j, k) - AG(Sg[c], i, j, k);
+  /* Part 3: nu_t = -1/2 (Mij Lij)/(Mij Mij) |S|, averaged in z for LES = 2 */
+  double *nut = o->nu_t;
+  memset(nut, 0, n * sizeof(double));
+  for (int k = 2; k <= nzg - 1; ++k)
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double ml = 0.0;
+        for (int c = 0; c < 6; ++c) {
+          if (c < 3) ml = ml + AG(M[c], i, j, k) * AG(L[c], i, j, k);
+          else ml = ml + 2.0 * AG(M[c], i, j, k) * AG(L[c], i, j, k);
+        }
+        const double mm = AG(M[0], i, j, k) * AG(M[0], i, j, k) + AG(M[1], i, j, k) * AG(M[1], i, j, k) +
+                          AG(M[2], i, j, k) * AG(M[2], i, j, k) +
+                          2.0 * (AG(M[3], i, j, k) * AG(M[3], i, j, k) + AG(M[4], i, j, k) * AG(M[4], i, j, k) +
+                                 AG(M[5], i, j, k) * AG(M[5], i, j, k));
+        if (avg) {
+          AG(L[0], i, j, k) = ml;  /* kept for the z averages */
+          AG(L[1], i, j, k) = mm;
+        } else {
+          AG(nut, i, j, k) = -0.5 * (ml / mm) * AG(S, i, j, k);
+        }
+      }
+  if (avg) {
+    for (int j = 2; j <= nyg - 1; ++j)
+      for (int i = 2; i <= nxg - 1; ++i) {
+        double a = 0.0, b = 0.0;
+        for (int k = 2; k <= nzg - 2; ++k) a += AG(L[0], i, j, k);
+        for (int k = 2; k <= nzg - 2; ++k) b += AG(L[1], i, j, k);
+        const double c = (a / (double)(nzg - 3)) / (b / (double)(nzg - 3));
+        for (int k = 2; k <= nzg - 1; ++k) AG(nut, i, j, k) = -0.5 * c * AG(S, i, j, k);
+      }
+  } else {
+    dyn_bc_x(o, nut, nxg, nyg, nzg, 4, 1);
+    dyn_bc_z(o, nut, nxg, nyg, 4);
+  }
+  for (size_t q = 0; q < n; ++q) nut[q] = nut[q] > 0.0 ? nut[q] : 0.0;  /* clipping */
+  for (int k = 1; k <= nzg; ++k)
+    for (int i = 1; i <= nxg; ++i) {  /* apply_Neumann_bc_y(nu_t, 2), Dirichlet_nu_t = 0 */
+      AG(nut, i, 1, k) = AG(nut, i, 2, k);
+      AG(nut, i, nyg, k) = AG(nut, i, nyg - 1, k);
+    }
+  free(term); free(term1); free(term2); free(S); free(Uf); free(Vf); free(Wf);
+  for (int c = 0; c < 6; ++c) { free(tb[c]); free(L[c]); free(Sg[c]); free(M[c]); }
 }
 
 void blo_get_nu_t(const blo_t *o, double *nu_t) {

@@ -70,6 +70,7 @@ void blo_get_rhs_p(const blo_t *o, double *rhs_p);
 
 /* models and diagnostics */
 void blo_smagorinsky(blo_t *o);          /* subgrid.f90:609-730 */
+void blo_dynamic_smagorinsky(blo_t *o);  /* subgrid.f90:261-583, LES = 2 or 3 from blo_set_les */
 void blo_get_nu_t(const blo_t *o, double *nu_t);
 void blo_statistics(const blo_t *o, double *means, double *nu_t_mean, double *Cf,
                     double *dUdy_wall, double *sc); /* statistics.f90:26-201 */

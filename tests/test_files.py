@@ -199,7 +199,7 @@ def test_snapshot_name():
 
 
 def test_params_les_flag_maps_to_config(tmp_path):
-    """The .turbb LES flag goes to blgpu_config.les_model unchanged; the
-    dynamic models (2, 3) are then refused by blgpu_create (not built)."""
+    """The .turbb LES flag goes to blgpu_config.les_model unchanged (2: the
+    dynamic model with the coefficient averaged in z)."""
     p = files.read_params(write_turbb(tmp_path / "l.turbb", "inflow_file = a\nLES = 2\n"))
     assert p["LES"] == 2 and p["config"]["les_model"] == 2

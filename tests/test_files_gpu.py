@@ -47,10 +47,10 @@ def test_rescaling_means_file(gpu, tmp_path):
     a.close()
 
 
-def test_dynamic_les_models_refused(gpu):
-    """LES = 2, 3 (dynamic Smagorinsky) are not built: blgpu_create says so
-    instead of running another model."""
+def test_unknown_les_model_refused(gpu):
+    """An LES flag outside 0..3 (and the host-supplied -1) is refused by
+    blgpu_create instead of running another model."""
     from blgpu import Solver, BlgpuError
-    for les in (2, 3):
-        with pytest.raises(BlgpuError, match="dynamic Smagorinsky"):
+    for les in (4, -2):
+        with pytest.raises(BlgpuError, match="unknown LES model"):
             Solver(34, 17, 12, 1e-3, -0.01, les_model=les)

@@ -165,3 +165,50 @@ def test_wall_model_law_of_the_wall_on_log_profile():
     tx, tz = o.wall_stress()
     assert abs(tx.mean() / c.utau ** 2 - 1) < 0.02
     assert np.all(tz == 0.0)
+
+
+def _dyn_case(model, shift=0.0):
+    """Noisy fields whose U, V planes in z are periodic and whose V, W
+    columns in x follow the model's x helper (Neumann for 2, periodic for 3),
+    so that the centre velocities agree with the ghosts of their products."""
+    c = cases.laminar_case(nx=26, ny=14, nz=11, lx=20.0, ly=5.0, lz=3.0)
+    rng = np.random.default_rng(41)
+    U = c.U + 0.05 * rng.standard_normal(c.U.shape)
+    V = c.V + 0.05 * rng.standard_normal(c.V.shape)
+    W = c.W + 0.05 * rng.standard_normal(c.W.shape) + shift
+    for a in (U, V):
+        a[:, :, 0], a[:, :, -2], a[:, :, -1] = a[:, :, -3], a[:, :, 1], a[:, :, 2]
+    for a in (V, W):
+        if model == 2:
+            a[0], a[-1] = a[1], a[-2]
+        else:
+            a[0], a[-2], a[-1] = a[-3], a[1], a[2]
+    c.U, c.V, c.W = (np.asfortranarray(a) for a in (U, V, W))
+    return c
+
+
+def test_dynamic_smagorinsky_structure():
+    """The oracle's dynamic model (subgrid.f90:261-583): nu_t >= 0 with
+    Neumann y ghosts; LES = 2 keeps one coefficient per (i,j) column, so each
+    column is all zero or all positive, and leaves the x / z ghosts at zero;
+    LES = 3 has periodic x / z ghosts."""
+    a = oracle.oracle_for(_dyn_case(2)).dynamic_smagorinsky(2)
+    assert np.isfinite(a).all() and (a >= 0).all() and a.max() > 0
+    assert np.array_equal(a[:, 0], a[:, 1]) and np.array_equal(a[:, -1], a[:, -2])
+    assert not a[0].any() and not a[-1].any() and not a[:, :, 0].any() and not a[:, :, -1].any()
+    col = a[1:-1, 1:-1, 1:-1] > 0
+    assert np.all(col.all(axis=2) | ~col.any(axis=2)) and col.any() and not col.all()
+    b = oracle.oracle_for(_dyn_case(3)).dynamic_smagorinsky(3)
+    assert np.isfinite(b).all() and (b >= 0).all() and b.max() > 0
+    assert np.array_equal(b[0], b[-3]) and np.array_equal(b[-2], b[1]) and np.array_equal(b[-1], b[2])
+    assert np.array_equal(b[:, :, 0], b[:, :, -3]) and np.array_equal(b[:, :, -1], b[:, :, 2])
+    assert np.array_equal(b[:, 0], b[:, 1])
+
+
+@pytest.mark.parametrize("model", [2, 3])
+def test_dynamic_smagorinsky_galilean_in_z(model):
+    """A uniform shift of W changes neither the Leonard term (the filter
+    weights sum to one) nor Mij (gradients only): nu_t moves by rounding."""
+    a = oracle.oracle_for(_dyn_case(model)).dynamic_smagorinsky(model)
+    b = oracle.oracle_for(_dyn_case(model, 0.3)).dynamic_smagorinsky(model)
+    assert np.abs(a - b).max() <= 1e-8 * a.max()
