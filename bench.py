@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-les", action="store_true")
     ap.add_argument("--ens-boxes", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--profile", default=None, choices=["mixed", "fp64", "ensemble"],
@@ -276,6 +277,33 @@ def run_ensemble(args, dev, pg, local, world):
     return out
 
 
+def run_les(args, dev):
+    """LES legs on the headline box in the mixed form: the device Smagorinsky
+    (LES = 1) and dynamic Smagorinsky (LES = 2 z-averaged, 3 pointwise) eddy
+    viscosity evaluated before every substep.  Fixed dt = 2e-4 so that the
+    synthetic field stays finite under the eddy viscosity; the step is timed
+    with CUDA events (advance_timed), one eddy-viscosity evaluation by wall
+    clock around the synchronising blgpu_eddy_viscosity call."""
+    import blgpu
+    from blgpu import cases
+    case = cases.turbulent_case(nx=args.nx, ny=args.ny, nz=args.nz)
+    case.cfl = -2e-4
+    out = {}
+    for model in (1, 2, 3):
+        s = cases.solver_for(case, precision=blgpu.MIXED, les_model=model, device=dev)
+        s.advance(2)
+        step = s.advance_timed(3) / 3
+        s._ck(s.lib.blgpu_eddy_viscosity(s.ctx))
+        t0 = time.perf_counter()
+        for _ in range(3):
+            s._ck(s.lib.blgpu_eddy_viscosity(s.ctx))
+        ev = (time.perf_counter() - t0) / 3 * 1e3
+        out["les%d" % model] = {"step_ms": step, "eddy_viscosity_ms": ev,
+                                "nu_t_finite": bool(np.isfinite(s.nu_t()).all())}
+        s.close()
+    return out
+
+
 def run_profile(args):
     """Small driver for ncu: set-up and warm-up outside the profiled range."""
     import torch
@@ -433,6 +461,9 @@ def main():
     ens = None
     if not args.no_ensemble:
         ens = run_ensemble(args, dev, pg, local, world)
+    les = None
+    if world == 1 and not args.no_les:
+        les = run_les(args, dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -452,7 +483,7 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk, "phases_ms_per_step_mixed": {k: v[0] / 2.0 for k, v in ph.items()},
                 "phases_ms_per_step_fp64": ({k: v[0] for k, v in ph64.items()} if fp64 else None),
-                "eager_step_ms_mixed": step_ms, "ensemble": ens}
+                "eager_step_ms_mixed": step_ms, "ensemble": ens, "les_mixed": les}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

@@ -230,6 +230,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   // LES as in compute_eddy_viscosity (subgrid.f90:23-47): 0 none, 1 constant-coefficient
   // Smagorinsky, 2 dynamic Smagorinsky with the coefficient averaged in z, 3 dynamic
   // Smagorinsky pointwise; BLGPU_LES_HOST: nu_t from the host
+  if ((cfg->les_model == 2 || cfg->les_model == 3) && (cfg->ny >= 65535 || cfg->nz >= 65535))
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: dynamic LES needs ny, nz < 65535");
   if (cfg->les_model != BLGPU_LES_HOST && (cfg->les_model < 0 || cfg->les_model > 3))
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown LES model %d", cfg->les_model);
   if (cfg->precision != BLGPU_FP64 && cfg->precision != BLGPU_MIXED)

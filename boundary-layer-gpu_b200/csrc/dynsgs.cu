@@ -5,8 +5,8 @@
 // The model runs in FP64 in both precisions, on dense (nxg,nyg,nzg) work
 // arrays indexed 1-based like the source's module arrays (i fastest); the
 // velocity-shaped ones use the U (nx,nyg), V (nxg,ny), W (nxg,nyg) plane
-// shapes.  Every step of the source is one grid-stride kernel in the source's
-// order, with the source's evaluation order in each expression (the file is
+// shapes.  Every step of the source is one kernel (one thread per point) in
+// the source's order, with the source's evaluation order in each expression (the file is
 // compiled with -fmad=false):
 //   interpolate_x/y/z (interpolation.f90:24-114) to cell centres;
 //   the x helpers apply_Neumann_bc_x / apply_periodic_bc_x
@@ -32,22 +32,21 @@ struct P6 {
   double *p[6];
 };
 
-// index range i0..i0+ni-1, j0.., k0.. walked by a flat grid-stride loop
+// index range i0..i0+ni-1, j0.., k0..: one thread per point, i along
+// blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z
+// (nj, nk <= 65535, checked at blgpu_create)
 struct Rng {
   int i0, ni, j0, nj, k0, nk;
-  __host__ __device__ long long n() const { return (long long)ni * nj * nk; }
 };
 
 __device__ __forceinline__ long long dix(int i, int j, int k, int d1, int d2) {
   return ((long long)(k - 1) * d2 + (j - 1)) * (long long)d1 + (i - 1);
 }
 
-#define FOR_RNG(R)                                                                                        \
-  for (long long q_ = blockIdx.x * (long long)blockDim.x + threadIdx.x; q_ < (R).n();                    \
-       q_ += (long long)gridDim.x * blockDim.x)                                                           \
-    if (const int i = (R).i0 + (int)(q_ % (R).ni), j = (R).j0 + (int)((q_ / (R).ni) % (R).nj),            \
-        k = (R).k0 + (int)(q_ / ((long long)(R).ni * (R).nj));                                            \
-        true)
+#define FOR_RNG(R)                                                                                 \
+  if (const int i = (R).i0 + (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (R).j0 + (int)blockIdx.y, \
+      k = (R).k0 + (int)blockIdx.z;                                                                      \
+      i < (R).i0 + (R).ni)
 
 template <typename T>
 __global__ void k_gather(Geo g, Rng R, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
@@ -74,10 +73,9 @@ __global__ void k_interp(Geo g, Rng R, const double *__restrict__ Ud, const doub
 }
 
 // x ghosts of every row (j,k) of a dense array with first dimension d1
-__global__ void k_bc_x(Rng R, double *__restrict__ a, int d1, int d2, int id, int periodic, int nx, int nxg) {
-  FOR_RNG(R) {
-    (void)i;
-    double *r = a + dix(1, j, k, d1, d2);
+__global__ void k_bc_x(long long rows, double *__restrict__ a, int d1, int id, int periodic, int nx, int nxg) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < rows; q += (long long)gridDim.x * blockDim.x) {
+    double *r = a + q * d1;
     if (!periodic) {
       if (id == 1) { r[0] = r[1]; r[nx - 1] = r[nx - 2]; }
       else { r[0] = r[1]; r[nxg - 1] = r[nxg - 2]; }
@@ -263,7 +261,7 @@ __global__ void k_store(Geo g, Rng R, const double *__restrict__ nd, T *__restri
   }
 }
 
-// grid-stride launches of 256 threads, at most 16 blocks per SM of 148
+// grid-stride launches of 256 threads (x / z ghosts), at most 16 blocks per SM of 148
 inline unsigned blocks(long long n) {
   const long long b = (n + 255) / 256, cap = 148LL * 16;
   return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
@@ -290,10 +288,11 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   for (int m = 0; m < 6; ++m) { L.p[m] = w[W_L + m]; G.p[m] = w[W_G + m]; M.p[m] = w[W_M + m]; }
   const int per = model == 3;
   int launches = 0;
-  auto go = [&](const Rng &R) { ++launches; return dim3(blocks(R.n())); };
+  auto go = [&](const Rng &R) { ++launches; return dim3((R.ni + 127) / 128, R.nj, R.nk); };
   auto bcx = [&](double *a, int d1, int d2, int d3, int id, int periodic) {
-    const Rng R = rng(1, 1, 1, d2, 1, d3);
-    k_bc_x<<<go(R), 256, 0, st>>>(R, a, d1, d2, id, periodic, nx, nxg);
+    const long long rows = (long long)d2 * d3;
+    ++launches;
+    k_bc_x<<<blocks(rows), 256, 0, st>>>(rows, a, d1, id, periodic, nx, nxg);
   };
   auto bcz = [&](double *a, int d1, int d2, int id) {
     const long long pl = (long long)d1 * d2;
@@ -302,20 +301,20 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   };
   auto filt = [&](const double *a, int d1, int d2, int n1, int ja, int jb, int n3, double *o, int e1, int e2) {
     const Rng R = rng(2, n1 - 1, ja, jb, 2, n3 - 1);
-    k_filter<<<go(R), 256, 0, st>>>(R, a, d1, d2, ja, jb, o, e1, e2);
+    k_filter<<<go(R), 128, 0, st>>>(R, a, d1, d2, ja, jb, o, e1, e2);
   };
   const Rng all = rng(1, nxg, 1, nyg, 1, nzg), in = rng(2, nxg - 1, 2, nyg - 1, 2, nzg - 1);
   double *Ud = w[W_U], *Vd = w[W_V], *Wd = w[W_W], *t0 = w[W_T0], *t1 = w[W_T1], *t2 = w[W_T2], *S = w[W_S];
   double *Uf = w[W_UF], *Vf = w[W_VF], *Wf = w[W_WF], *tb = w[W_TB];
-  k_gather<T><<<go(all), 256, 0, st>>>(g, all, U, V, W, Ud, Vd, Wd);
+  k_gather<T><<<go(all), 128, 0, st>>>(g, all, U, V, W, Ud, Vd, Wd);
   // Part 1: Leonard term
-  k_interp<<<go(all), 256, 0, st>>>(g, all, Ud, Vd, Wd, t0, t1, t2);
+  k_interp<<<go(all), 128, 0, st>>>(g, all, Ud, Vd, Wd, t0, t1, t2);
   bcx(t0, nxg, nyg, nzg, 2, per);
   bcz(t2, nxg, nyg, 4);
   const double *pa[6] = {t0, t1, t2, t0, t0, t1}, *pb[6] = {t0, t1, t2, t1, t2, t2};
   const Rng rp = rng(2, nxg, 2, nyg - 1, 2, nzg);
   for (int m = 0; m < 6; ++m) {
-    k_prod<<<go(rp), 256, 0, st>>>(g, rp, tb, pa[m], pb[m]);
+    k_prod<<<go(rp), 128, 0, st>>>(g, rp, tb, pa[m], pb[m]);
     bcx(tb, nxg, nyg, nzg, 2, per);
     bcz(tb, nxg, nyg, 4);
     filt(tb, nxg, nyg, nxg, 2, nyg - 1, nzg, L.p[m], nxg, nyg);
@@ -323,7 +322,7 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   filt(t0, nxg, nyg, nxg, 2, nyg - 1, nzg, G.p[0], nxg, nyg);
   filt(t1, nxg, nyg, nxg, 2, nyg - 1, nzg, G.p[1], nxg, nyg);
   filt(t2, nxg, nyg, nxg, 2, nyg - 1, nzg, G.p[2], nxg, nyg);
-  k_leonard<<<go(in), 256, 0, st>>>(g, in, L, G);
+  k_leonard<<<go(in), 128, 0, st>>>(g, in, L, G);
   // Part 2: Mij
   filt(Ud, nx, nyg, nx, 1, nyg, nzg, Uf, nx, nyg);
   filt(Vd, nxg, ny, nxg, 1, ny, nzg, Vf, nxg, ny);
@@ -334,28 +333,28 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   bcz(Vf, nxg, ny, 2);
   bcx(Wf, nxg, nyg, nz, 2, per);
   bcz(Wf, nxg, nyg, 3);
-  k_sij<<<go(in), 256, 0, st>>>(g, in, DV{Uf, Vf, Wf, nx, ny, nxg, nyg}, G, S);
-  k_mij<<<go(in), 256, 0, st>>>(g, in, M, G, S);
-  k_sij<<<go(in), 256, 0, st>>>(g, in, DV{Ud, Vd, Wd, nx, ny, nxg, nyg}, G, S);
+  k_sij<<<go(in), 128, 0, st>>>(g, in, DV{Uf, Vf, Wf, nx, ny, nxg, nyg}, G, S);
+  k_mij<<<go(in), 128, 0, st>>>(g, in, M, G, S);
+  k_sij<<<go(in), 128, 0, st>>>(g, in, DV{Ud, Vd, Wd, nx, ny, nxg, nyg}, G, S);
   for (int m = 0; m < 6; ++m) {
-    k_ssij<<<go(in), 256, 0, st>>>(g, in, t0, S, G.p[m]);
+    k_ssij<<<go(in), 128, 0, st>>>(g, in, t0, S, G.p[m]);
     bcx(t0, nxg, nyg, nzg, 2, per);
     bcz(t0, nxg, nyg, 4);
     filt(t0, nxg, nyg, nxg, 2, nyg - 1, nzg, G.p[m], nxg, nyg);
   }
-  k_msub<<<go(in), 256, 0, st>>>(g, in, M, G);
+  k_msub<<<go(in), 128, 0, st>>>(g, in, M, G);
   // Part 3: nu_t (tb holds it; entries the source leaves at zero stay zero)
   cudaMemsetAsync(tb, 0, n * sizeof(double), st);
   if (model == 2) {
-    k_contract<<<go(in), 256, 0, st>>>(g, in, M, L, S, tb, t1, t2, 1);
+    k_contract<<<go(in), 128, 0, st>>>(g, in, M, L, S, tb, t1, t2, 1);
     const Rng ij = rng(2, nxg - 1, 2, nyg - 1, 1, 1);
-    k_zavg<<<go(ij), 256, 0, st>>>(g, ij, t1, t2, S, tb);
+    k_zavg<<<go(ij), 128, 0, st>>>(g, ij, t1, t2, S, tb);
   } else {
-    k_contract<<<go(in), 256, 0, st>>>(g, in, M, L, S, tb, nullptr, nullptr, 0);
+    k_contract<<<go(in), 128, 0, st>>>(g, in, M, L, S, tb, nullptr, nullptr, 0);
     bcx(tb, nxg, nyg, nzg, 4, 1);
     bcz(tb, nxg, nyg, 4);
   }
-  k_store<T><<<go(all), 256, 0, st>>>(g, all, tb, nut);
+  k_store<T><<<go(all), 128, 0, st>>>(g, all, tb, nut);
   return launches;
 }
 
