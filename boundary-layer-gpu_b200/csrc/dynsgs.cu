@@ -110,17 +110,30 @@ __global__ void k_prod(Geo g, Rng R, double *__restrict__ tb, const double *__re
 
 // filter_xzy of the section a(1:n1, ja:jb, 1:n3) of a dense (d1,d2,*) array
 // into o(i,j,k), i = 2..n1-1, j = ja..jb, k = 2..n3-1 (output dims e1,e2);
-// the range R carries those output indices
-__global__ void k_filter(Rng R, const double *__restrict__ a, int d1, int d2, int ja, int jb,
-                         double *__restrict__ o, int e1, int e2) {
+// the range R carries those output indices.  A block of FK_I threads takes
+// FK_I outputs along i at one j and marches over FK_K planes in k: the
+// y-combined values of input columns i-1..i+FK_I of plane kk go to a ring of
+// three shared rows, and each output sums its 3 x 3 (x,z) neighbourhood from
+// the ring in the source's order (x outer, z inner).
+constexpr int FK_I = 128, FK_K = 16;
+
+__global__ void __launch_bounds__(FK_I) k_filter(Rng R, const double *__restrict__ a, int d1, int d2, int ja,
+                                                 int jb, double *__restrict__ o, int e1, int e2) {
   const double fil[3][3] = {{1.0 / 36.0, 1.0 / 9.0, 1.0 / 36.0},
                             {1.0 / 9.0, 4.0 / 9.0, 1.0 / 9.0},
                             {1.0 / 36.0, 1.0 / 9.0, 1.0 / 36.0}};
-  FOR_RNG(R) {
-    double s = 0.0;
-    for (int di = -1; di <= 1; ++di)
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int ii = i + di, kk = k + dk;
+  __shared__ double ys[3][FK_I + 2];
+  const int t = threadIdx.x;
+  const int ib = R.i0 + (int)blockIdx.x * FK_I;  // first output i of the block
+  const int i = ib + t, ilast = R.i0 + R.ni - 1;
+  const int j = R.j0 + (int)blockIdx.y;
+  const int kb = R.k0 + (int)blockIdx.z * FK_K;
+  const int ke = min(kb + FK_K - 1, R.k0 + R.nk - 1);
+  for (int kk = kb - 1; kk <= ke + 1; ++kk) {
+    double *row = ys[(kk - kb + 1) % 3];
+    for (int x = t; x < FK_I + 2; x += FK_I) {
+      const int ii = ib - 1 + x;
+      if (ii <= ilast + 1) {
         double y;
         if (j == ja)
           y = 2.0 / 3.0 * a[dix(ii, j, kk, d1, d2)] + 1.0 / 3.0 * a[dix(ii, j + 1, kk, d1, d2)];
@@ -129,9 +142,18 @@ __global__ void k_filter(Rng R, const double *__restrict__ a, int d1, int d2, in
         else
           y = 1.0 / 6.0 * a[dix(ii, j - 1, kk, d1, d2)] + 2.0 / 3.0 * a[dix(ii, j, kk, d1, d2)] +
               1.0 / 6.0 * a[dix(ii, j + 1, kk, d1, d2)];
-        s = s + y * fil[di + 1][dk + 1];
+        row[x] = y;
       }
-    o[dix(i, j, k, e1, e2)] = s;
+    }
+    __syncthreads();
+    if (kk >= kb + 1 && i <= ilast) {  // output plane k = kk-1 from planes kk-2, kk-1, kk
+      const int k = kk - 1;
+      double s = 0.0;
+      for (int di = -1; di <= 1; ++di)
+        for (int dk = -1; dk <= 1; ++dk) s = s + ys[(k + dk - kb + 1) % 3][t + 1 + di] * fil[di + 1][dk + 1];
+      o[dix(i, j, k, e1, e2)] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -301,7 +323,9 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   };
   auto filt = [&](const double *a, int d1, int d2, int n1, int ja, int jb, int n3, double *o, int e1, int e2) {
     const Rng R = rng(2, n1 - 1, ja, jb, 2, n3 - 1);
-    k_filter<<<go(R), 128, 0, st>>>(R, a, d1, d2, ja, jb, o, e1, e2);
+    ++launches;
+    k_filter<<<dim3((R.ni + FK_I - 1) / FK_I, R.nj, (R.nk + FK_K - 1) / FK_K), FK_I, 0, st>>>(R, a, d1, d2, ja, jb, o,
+                                                                                            e1, e2);
   };
   const Rng all = rng(1, nxg, 1, nyg, 1, nzg), in = rng(2, nxg - 1, 2, nyg - 1, 2, nzg - 1);
   double *Ud = w[W_U], *Vd = w[W_V], *Wd = w[W_W], *t0 = w[W_T0], *t1 = w[W_T1], *t2 = w[W_T2], *S = w[W_S];
