@@ -14,7 +14,7 @@
 //   one process, where update_ghost_interior_planes is empty;
 //   filter_xzy (subgrid.f90:140-184, fil_size = 2);
 //   compute_Sij (subgrid.f90:672-730), with the in-place corner averages
-//   read from edge values recomputed per point (the source's loop order
+//   taken from a separate array of edge values (the source's loop order
 //   reads only not-yet-averaged neighbours, so the values are the same);
 //   the Lij, Mij contractions, the z average (LES = 2), clipping and
 //   Neumann y (Dirichlet_nu_t = 0).
@@ -193,17 +193,30 @@ __device__ __forceinline__ double e6(const Geo &g, const DV &d, int i, int j, in
                 (d.w(i, j, k - 1) - d.w(i, j - 1, k - 1)) / (g.yg[j] - g.yg[j - 1]));
 }
 
-// Sij (cell centres) and |S| of the velocity triple d
-__global__ void k_sij(Geo g, Rng R, DV d, P6 G, double *__restrict__ S) {
+// compute_Sij's edge values at i = 2..nxg, j = 2..nyg, k = 2..nzg (dense (nxg,nyg) planes)
+__global__ void k_edges(Geo g, Rng R, DV d, double *__restrict__ E4, double *__restrict__ E5,
+                        double *__restrict__ E6) {
   FOR_RNG(R) {
     const long long c = dix(i, j, k, g.nxg, g.nyg);
+    E4[c] = e4(g, d, i, j, k);
+    E5[c] = e5(g, d, i, j, k);
+    E6[c] = e6(g, d, i, j, k);
+  }
+}
+
+// Sij (cell centres) and |S| of the velocity triple d, the off-diagonal terms
+// as the source's corner averages of the edge values E4..E6
+__global__ void k_sij(Geo g, Rng R, DV d, const double *__restrict__ E4, const double *__restrict__ E5,
+                      const double *__restrict__ E6, P6 G, double *__restrict__ S) {
+  FOR_RNG(R) {
+    const long long c = dix(i, j, k, g.nxg, g.nyg), sj = g.nxg, sk = (long long)g.nxg * g.nyg;
     double s[6];
     s[0] = (d.u(i, j, k) - d.u(i - 1, j, k)) / (g.x[i] - g.x[i - 1]);
     s[1] = (d.v(i, j, k) - d.v(i, j - 1, k)) / (g.y[j] - g.y[j - 1]);
     s[2] = (d.w(i, j, k) - d.w(i, j, k - 1)) / (g.z[k] - g.z[k - 1]);
-    s[3] = 0.25 * (e4(g, d, i, j, k) + e4(g, d, i + 1, j, k) + e4(g, d, i, j + 1, k) + e4(g, d, i + 1, j + 1, k));
-    s[4] = 0.25 * (e5(g, d, i, j, k) + e5(g, d, i + 1, j, k) + e5(g, d, i, j, k + 1) + e5(g, d, i + 1, j, k + 1));
-    s[5] = 0.25 * (e6(g, d, i, j, k) + e6(g, d, i, j + 1, k) + e6(g, d, i, j, k + 1) + e6(g, d, i, j + 1, k + 1));
+    s[3] = 0.25 * (E4[c] + E4[c + 1] + E4[c + sj] + E4[c + 1 + sj]);
+    s[4] = 0.25 * (E5[c] + E5[c + 1] + E5[c + sk] + E5[c + 1 + sk]);
+    s[5] = 0.25 * (E6[c] + E6[c + sj] + E6[c + sk] + E6[c + sj + sk]);
     double q = 0.0;
     for (int m = 0; m < 6; ++m) {
       G.p[m][c] = s[m];
@@ -357,9 +370,14 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   bcz(Vf, nxg, ny, 2);
   bcx(Wf, nxg, nyg, nz, 2, per);
   bcz(Wf, nxg, nyg, 3);
-  k_sij<<<go(in), 128, 0, st>>>(g, in, DV{Uf, Vf, Wf, nx, ny, nxg, nyg}, G, S);
+  // t0..t2 are free here: they hold the edge values of each compute_Sij
+  const Rng re = rng(2, nxg, 2, nyg, 2, nzg);
+  const DV df{Uf, Vf, Wf, nx, ny, nxg, nyg}, du{Ud, Vd, Wd, nx, ny, nxg, nyg};
+  k_edges<<<go(re), 128, 0, st>>>(g, re, df, t0, t1, t2);
+  k_sij<<<go(in), 128, 0, st>>>(g, in, df, t0, t1, t2, G, S);
   k_mij<<<go(in), 128, 0, st>>>(g, in, M, G, S);
-  k_sij<<<go(in), 128, 0, st>>>(g, in, DV{Ud, Vd, Wd, nx, ny, nxg, nyg}, G, S);
+  k_edges<<<go(re), 128, 0, st>>>(g, re, du, t0, t1, t2);
+  k_sij<<<go(in), 128, 0, st>>>(g, in, du, t0, t1, t2, G, S);
   for (int m = 0; m < 6; ++m) {
     k_ssij<<<go(in), 128, 0, st>>>(g, in, t0, S, G.p[m]);
     bcx(t0, nxg, nyg, nzg, 2, per);
