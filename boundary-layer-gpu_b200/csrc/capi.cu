@@ -181,10 +181,12 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 // the sticky device flag of the step kernels (stream already synchronized);
 // bit 2: a TMA copy of the tensor-core z transform missed its wait limit;
 // bit 4: one of the tiled y-solve; bit 8: one of the tcgen05 z transform;
-// bit 16: a row copy of the two-pass inverse x transform
+// bit 16: a row copy of the two-pass inverse x transform; bit 32: a streamed
+// upload (blgpu_upload_state_async) held a NaN or an infinity
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
+  if (f & 32) return set_err(ctx, BLGPU_EDEVICE, "an uploaded state held a NaN or an infinity");
   if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
   if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
   if (f & 8) return set_err(ctx, BLGPU_EDEVICE, "z transform (tcgen05): a copy or a product missed its wait limit");
@@ -760,20 +762,31 @@ int blgpu_get_rescaling(blgpu_ctx *ctx, double *Umean_resc, double *Vmean_resc, 
 // ---- host <-> box layout (staged through device memory, repacked on the GPU) ----
 static int upload_field(blgpu_ctx *ctx, void *dst, const double *a, int n1, int n2, int n3) {
   CK(cudaMemcpyAsync(ctx->stage, a, (size_t)n1 * n2 * n3 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 0, ctx->stage, (double *)dst, n1, n2, n3, ctx->st);
-  else launch_repack<float>(ctx->geo_box(), 0, ctx->stage, (float *)dst, n1, n2, n3, ctx->st);
+  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 0, ctx->stage, (double *)dst, n1, n2, n3, &ctx->sc->err, ctx->st);
+  else launch_repack<float>(ctx->geo_box(), 0, ctx->stage, (float *)dst, n1, n2, n3, &ctx->sc->err, ctx->st);
   ctx->launches += 1;
   CK(cudaGetLastError());
   return BLGPU_OK;
 }
 
 static int download_field(blgpu_ctx *ctx, const void *src, double *a, int n1, int n2, int n3) {
-  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 1, ctx->stage, (double *)src, n1, n2, n3, ctx->st);
-  else launch_repack<float>(ctx->geo_box(), 1, ctx->stage, (float *)src, n1, n2, n3, ctx->st);
+  if (ctx->fp64) launch_repack<double>(ctx->geo_box(), 1, ctx->stage, (double *)src, n1, n2, n3, nullptr, ctx->st);
+  else launch_repack<float>(ctx->geo_box(), 1, ctx->stage, (float *)src, n1, n2, n3, nullptr, ctx->st);
   ctx->launches += 1;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(a, ctx->stage, (size_t)n1 * n2 * n3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
   return BLGPU_OK;
+}
+
+// after a synchronous upload: a non-finite host value (bit 32 of the device
+// flag, set by the repack kernel) is reported and the bit cleared
+static int take_upload_flag(blgpu_ctx *ctx, const char *what) {
+  int f = 0;
+  CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
+  if (!(f & 32)) return BLGPU_OK;
+  f &= ~32;
+  CK(cudaMemcpy(&ctx->sc->err, &f, sizeof f, cudaMemcpyHostToDevice));
+  return set_err(ctx, BLGPU_EDEVICE, "%s: the host arrays hold a NaN or an infinity", what);
 }
 
 extern "C" {
@@ -785,7 +798,7 @@ int blgpu_set_nu_t(blgpu_ctx *ctx, const double *nu_t) {
   int rc = upload_field(ctx, ctx->nut, nu_t, ctx->nxg, ctx->nyg, ctx->nzg);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->st));
-  return BLGPU_OK;
+  return take_upload_flag(ctx, "blgpu_set_nu_t");
 }
 
 int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t) {
@@ -801,6 +814,11 @@ int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const d
   for (int q = 0; q < 3; ++q)
     CK(cudaMemcpyAsync(ctx->S[1][q], ctx->S[0][q], (size_t)ctx->boxn * ctx->esz, cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
+  rc = take_upload_flag(ctx, "blgpu_upload_state");
+  if (rc) {
+    ctx->have_state = false;
+    return rc;
+  }
   Scalars h{};
   CK(cudaMemcpy(&h, ctx->sc, sizeof h, cudaMemcpyDeviceToHost));
   h.t = t;
@@ -857,10 +875,10 @@ int blgpu_upload_state_async(blgpu_ctx *ctx, const double *U, const double *V, c
   for (int f = 0; f < 3; ++f) {
     if (ctx->fp64)
       launch_repack<double>(ctx->geo_box(), 0, ctx->stage_in[f], (double *)ctx->S[0][f], dims[f][0], dims[f][1],
-                            dims[f][2], ctx->st);
+                            dims[f][2], &ctx->sc->err, ctx->st);
     else
       launch_repack<float>(ctx->geo_box(), 0, ctx->stage_in[f], (float *)ctx->S[0][f], dims[f][0], dims[f][1],
-                           dims[f][2], ctx->st);
+                           dims[f][2], &ctx->sc->err, ctx->st);
     ctx->launches += 1;
   }
   CK(cudaEventRecord(ctx->ev_in_free, ctx->st));
@@ -887,10 +905,10 @@ int blgpu_download_state_async(blgpu_ctx *ctx, double *U, double *V, double *W) 
     if (!dst[f]) continue;
     if (ctx->fp64)
       launch_repack<double>(ctx->geo_box(), 1, ctx->stage_out[f], (double *)ctx->S[ctx->cur][f], dims[f][0],
-                            dims[f][1], dims[f][2], ctx->st);
+                            dims[f][1], dims[f][2], nullptr, ctx->st);
     else
       launch_repack<float>(ctx->geo_box(), 1, ctx->stage_out[f], (float *)ctx->S[ctx->cur][f], dims[f][0],
-                           dims[f][1], dims[f][2], ctx->st);
+                           dims[f][1], dims[f][2], nullptr, ctx->st);
     ctx->launches += 1;
   }
   CK(cudaEventRecord(ctx->ev_out_ready, ctx->st));
@@ -1204,6 +1222,9 @@ int blgpu_compute_rhs(blgpu_ctx *ctx, const double *U, const double *V, const do
   int rc = upload_field(ctx, ctx->S[sb][0], U, ctx->nx, ctx->nyg, ctx->nzg);
   if (!rc) rc = upload_field(ctx, ctx->S[sb][1], V, ctx->nxg, ctx->ny, ctx->nzg);
   if (!rc) rc = upload_field(ctx, ctx->S[sb][2], W, ctx->nxg, ctx->nyg, ctx->nz);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  rc = take_upload_flag(ctx, "blgpu_compute_rhs");
   if (rc) return rc;
   if (ctx->fp64) enq_rhs<double>(ctx, 0, sb, sb, sb, 0.0, 0.0);
   else enq_rhs<float>(ctx, 0, sb, sb, sb, 0.0, 0.0);

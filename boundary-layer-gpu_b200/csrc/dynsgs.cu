@@ -387,6 +387,7 @@ int launch_dyn_smagorinsky(const Geo &g, const T *U, const T *V, const T *W, dou
   k_msub<<<go(in), 128, 0, st>>>(g, in, M, G);
   // Part 3: nu_t (tb holds it; entries the source leaves at zero stay zero)
   cudaMemsetAsync(tb, 0, n * sizeof(double), st);
+  ++launches;  // the memset is one stream operation (one graph node) like a kernel
   if (model == 2) {
     k_contract<<<go(in), 128, 0, st>>>(g, in, M, L, S, tb, t1, t2, 1);
     const Rng ij = rng(2, nxg - 1, 2, nyg - 1, 1, 1);

@@ -96,8 +96,10 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int 
 template <typename T>
 void launch_lund(const Geo &g, const LundData &L, const T *U, const T *V, const T *W, const Scalars *sc, int phase,
                  cudaStream_t st);
+// dir 0: host-layout FP64 stage -> box (bit 32 of *flag set on a NaN or infinity; flag may be null);
+// dir 1: box -> stage
 template <typename T>
-void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st);
+void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, int *flag, cudaStream_t st);
 
 // ---- spectral.cu ----
 // Transform plan of one axis length n (device tables)

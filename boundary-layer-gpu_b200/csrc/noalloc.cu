@@ -20,7 +20,8 @@
 //  - all calls share the one scratch array: calls that overlap on the GPU
 //    (different streams, different host threads) race; every row slot a call
 //    reads is written by the same call first, so stale contents of an earlier
-//    call are never used.
+//    call are never used;
+//  - a NaN anywhere in the divergence gives a NaN result.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,6 +42,10 @@ __device__ __align__(256) double g_row_max[kMaxRows];
 std::mutex g_setup_mutex;
 double *g_row_max_addr[kMaxDevices] = {};
 
+// max that keeps a NaN (fmax would drop it), so that a NaN divergence reads as
+// NaN, as it does through the context's check (blgpu_max_divergence)
+__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
+
 // one warp per (j,k) row: max over i = 2..nxg-2 of |div u| (projection.f90:399-408)
 __global__ void k_row_divmax(const double *__restrict__ U, const double *__restrict__ V,
                              const double *__restrict__ W, const double *__restrict__ x,
@@ -60,22 +65,22 @@ __global__ void k_row_divmax(const double *__restrict__ U, const double *__restr
   for (int i = 2 + lane; i <= nxg - 2; i += 32) {
     const double d = (U[ub + i - 1] - U[ub + i - 2]) / (x[i - 1] - x[i - 2]) + (V[vb + i - 1] - V[vbs + i - 1]) / dy +
                      (W[wb + i - 1] - W[wbs + i - 1]) / dz;
-    m = fmax(m, fabs(d));
+    m = max_nan(m, fabs(d));
   }
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0) rows[warp] = m;
 }
 
 __global__ void k_rows_max(const double *__restrict__ rows, int nrows, double *__restrict__ out) {
   __shared__ double red[32];
   double m = 0.0;
-  for (int r = threadIdx.x; r < nrows; r += blockDim.x) m = fmax(m, rows[r]);
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x) m = max_nan(m, rows[r]);
+  for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x < 32) {
     m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
     if (threadIdx.x == 0) out[0] = m;
   }
 }

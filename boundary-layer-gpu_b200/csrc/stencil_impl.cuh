@@ -1334,14 +1334,20 @@ namespace blgpu {
 // staged as FP64 in device memory, to and from the padded box in precision T)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_repack_in(Geo g, const double *__restrict__ src, int n1, int n2, int n3, T *__restrict__ dst) {
+__global__ void k_repack_in(Geo g, const double *__restrict__ src, int n1, int n2, int n3, T *__restrict__ dst,
+                            int *flag) {
   const long long tot = (long long)n1 * n2 * n3;
+  bool bad = false;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % n1);
     const long long r = q / n1;
     const int j = (int)(r % n2), k = (int)(r / n2);
-    dst[bidx(g, i + 1, j + 1, k + 1)] = (T)src[q];
+    const double v = src[q];
+    bad |= !isfinite(v);
+    dst[bidx(g, i + 1, j + 1, k + 1)] = (T)v;
   }
+  // a NaN or infinity in the host state: bit 32 of the device flag
+  if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 32);
 }
 
 template <typename T>
@@ -1356,12 +1362,13 @@ __global__ void k_repack_out(Geo g, const T *__restrict__ src, int n1, int n2, i
 }
 
 template <typename T>
-void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, cudaStream_t st) {
+void launch_repack(const Geo &g, int dir, double *stage, T *box, int n1, int n2, int n3, int *flag, cudaStream_t st) {
   const int blocks = 148 * 8;
-  if (dir == 0) k_repack_in<T><<<blocks, 256, 0, st>>>(g, stage, n1, n2, n3, box);
+  if (dir == 0) k_repack_in<T><<<blocks, 256, 0, st>>>(g, stage, n1, n2, n3, box, flag);
   else k_repack_out<T><<<blocks, 256, 0, st>>>(g, box, n1, n2, n3, stage);
 }
-template void launch_repack<BLGPU_STENCIL_T>(const Geo &, int, double *, BLGPU_STENCIL_T *, int, int, int, cudaStream_t);
+template void launch_repack<BLGPU_STENCIL_T>(const Geo &, int, double *, BLGPU_STENCIL_T *, int, int, int, int *,
+                                             cudaStream_t);
 
 }  // namespace blgpu
 

@@ -6,7 +6,7 @@
  * (time_integration.f90), the boundary-condition pass of the GPU build
  * (boundary_conditions.f90:127-262) and the fractional-step projection
  * (projection.f90).  Plain C types only, so a Fortran host binds it with
- * ISO_C_BINDING (see INTEGRATION.md) and Python with ctypes.
+ * ISO_C_BINDING and Python with ctypes.
  *
  * Conventions
  *  - Every entry point returns 0 on success and a negative BLGPU_E* code on
@@ -121,7 +121,10 @@ int blgpu_box(const blgpu_ctx *ctx, int *nx, int *ny, int *nz, double *nu);
 int blgpu_get_grid(blgpu_ctx *ctx, double *x, double *y, double *z);
 
 /* state in/out (main.f90:61-81 copy-in; main.f90:99-101 update self).
- * Upload also sets Uo = U as read_input_data does (input_output.f90:476-478). */
+ * Upload also sets Uo = U as read_input_data does (input_output.f90:476-478).
+ * A NaN or an infinity in the host arrays is rejected with BLGPU_EDEVICE
+ * (the context then holds no state); blgpu_set_nu_t and blgpu_compute_rhs
+ * check their host arrays the same way. */
 int blgpu_upload_state(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
 int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double *P, double *t);
 /* Streamed variants for passing a sequence of states through the solver:
@@ -132,7 +135,9 @@ int blgpu_download_state(blgpu_ctx *ctx, double *U, double *V, double *W, double
  * download of the previous one overlap (PCIe is full duplex).  Host arrays
  * must be pinned for the copies to be asynchronous and must not be touched
  * until blgpu_sync returns; the state semantics are those of
- * blgpu_upload_state / blgpu_download_state (U, V, W; no pressure, no time). */
+ * blgpu_upload_state / blgpu_download_state (U, V, W; no pressure, no time);
+ * a NaN or an infinity in a streamed upload is reported by the next
+ * blgpu_sync as BLGPU_EDEVICE. */
 int blgpu_upload_state_async(blgpu_ctx *ctx, const double *U, const double *V, const double *W, double t);
 int blgpu_download_state_async(blgpu_ctx *ctx, double *U, double *V, double *W);
 

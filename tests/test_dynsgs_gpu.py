@@ -26,8 +26,11 @@ def noisy(nx, ny, nz, seed, amp, **kw):
 
 
 @pytest.mark.parametrize("model", [2, 3])
-@pytest.mark.parametrize("grid", [(26, 14, 11), (61, 17, 16)])
+@pytest.mark.parametrize("grid", [(26, 14, 11), (61, 17, 16), (300, 9, 40)])
 def test_dynamic_nu_t_matches_oracle(gpu, model, grid):
+    """300 x 9 x 40: several 128-point x blocks of the filter kernel (the
+    halo at ib-1 and ib+128 and the guard at the last block) and three
+    16-plane k blocks, against the oracle."""
     c = noisy(*grid, seed=31, amp=0.05)
     s = cases.solver_for(c, les_model=model)
     o = oracle.oracle_for(c)

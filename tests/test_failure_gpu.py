@@ -1,0 +1,50 @@
+"""Failure detection on the device, without faulting it.
+
+A NaN or an infinity in host arrays handed to the upload entry points is
+found by the repack kernel (a flag bit, no trap) and reported as
+BLGPU_EDEVICE; the context stays usable and takes a clean state afterwards.
+"""
+import numpy as np
+import pytest
+
+from blgpu import cases, BlgpuError, FP64, MIXED
+
+pytestmark = pytest.mark.gpu
+
+
+def _case():
+    c = cases.laminar_case(nx=40, ny=13, nz=18, lx=20.0, ly=5.0, lz=3.0)
+    rng = np.random.default_rng(3)
+    c.W = np.asfortranarray(c.W + 1e-3 * rng.standard_normal(c.W.shape))
+    return c
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_upload_rejects_non_finite(gpu, precision, bad):
+    c = _case()
+    s = cases.solver_for(c, precision=precision)
+    V = np.array(c.V, order="F")
+    V[7, 4, 9] = bad
+    with pytest.raises(BlgpuError, match="NaN or an infinity"):
+        s.upload_state(c.U, V, c.W)
+    # the context still works: a clean state steps and matches a fresh context
+    s.upload_state(c.U, c.V, c.W)
+    s.advance(2)
+    r = cases.solver_for(c, precision=precision)
+    r.advance(2)
+    for a, b in zip(s.download_state()[:3], r.download_state()[:3]):
+        assert np.array_equal(a, b)
+    s.close()
+    r.close()
+
+
+def test_streamed_upload_reports_non_finite_at_sync(gpu):
+    c = _case()
+    s = cases.solver_for(c)
+    U = np.array(c.U, order="F")
+    U[3, 2, 1] = np.nan
+    s.upload_state_async(U, c.V, c.W)
+    with pytest.raises(BlgpuError, match="NaN or an infinity"):
+        s.sync()
+    s.close()

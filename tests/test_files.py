@@ -10,7 +10,8 @@ import pytest
 
 from blgpu import files, BlgpuError
 
-REF = "/root/reference"
+# the reference source tree (its .turbb files), when present on this machine
+REF = os.environ.get("BLGPU_REFERENCE_DIR", "")
 
 
 def write_turbb(path, text):
@@ -62,7 +63,7 @@ def test_turbb_errors(tmp_path):
         files.read_params(write_turbb(tmp_path / "e.turbb", "inflow_file = a\nnxyz = 4 4\n"))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="BLGPU_REFERENCE_DIR not set")
 def test_reference_turbb_files():
     p = files.read_params(os.path.join(REF, "laminar_test", "laminar.turbb"))
     assert p["nxyz"] == [302, 64, 8] and p["CFL"] == -5e-5 and p["nu"] == 1e-5

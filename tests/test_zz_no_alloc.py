@@ -59,3 +59,22 @@ def test_noalloc_rejects_oversized_grid(gpu):
     rc = lib.blgpu_check_divergence_noalloc(dummy, dummy, dummy, dummy, dummy, dummy, 64, 300, 300, dummy, None)
     assert rc == -1
     assert b"65536" in lib.blgpu_last_error(None)
+
+
+def test_noalloc_divergence_keeps_nan(gpu):
+    """A NaN in the velocity field gives a NaN maximum, as the context's check does."""
+    import torch
+    lib = _lib.load()
+    dev = torch.device("cuda:0")
+    out = torch.zeros(1, dtype=torch.float64, device=dev)
+    c = _state(13, 1e-2)
+    U = np.array(c.U, order="F")
+    U[20, 7, 5] = np.nan
+    t = [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev) for a in (U, c.V, c.W)]
+    g = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (c.x, c.y, c.z)]
+    torch.cuda.synchronize()
+    rc = lib.blgpu_check_divergence_noalloc(*[ctypes.c_void_p(a.data_ptr()) for a in t + g],
+                                            c.nx, c.ny, c.nz, ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 0, lib.blgpu_last_error(None)
+    torch.cuda.synchronize()
+    assert np.isnan(float(out.item()))
