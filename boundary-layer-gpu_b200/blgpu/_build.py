@@ -31,6 +31,7 @@ SOURCES = {
     "zdft_umma.cu": [],
     "snapshot.cpp": [],
     "thomas_tma.cu": [],
+    "cufft_path.cu": [],
 }
 
 

@@ -368,12 +368,13 @@ def ensemble_cases(nbox=64, seed=2024, nx_set=(128, 192, 256), ny=65, nz_set=(64
     return out
 
 
-def solver_for(case, precision=0, device=0, les_model=0, inflow=True):
+def solver_for(case, precision=0, device=0, les_model=0, inflow=True, poisson=0):
     """Create a Solver loaded with a case (grid, boundary vectors, state and,
-    unless inflow=False, the case's Lund recycling inflow)."""
+    unless inflow=False, the case's Lund recycling inflow).  poisson = 1
+    selects the cuFFT comparison path of the Poisson solve."""
     from .solver import Solver
     s = Solver(case.nx, case.ny, case.nz, case.nu, case.cfl, case.dpdx, case.dpdz, case.rk_scheme,
-               les_model=les_model, precision=precision, device=device)
+               les_model=les_model, precision=precision, device=device, poisson=poisson)
     s.set_grid(case.x, case.y, case.z)
     s.set_boundary(*case.bc)
     s.upload_state(case.U, case.V, case.W, case.t)

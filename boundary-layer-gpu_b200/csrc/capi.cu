@@ -65,6 +65,8 @@ struct blgpu_ctx {
   uint32_t *utab = nullptr;   // mixed form: tcgen05 z transforms, tables (or null)
   ZdftMaps umaps{};           // and their TMA maps
   ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
+  CufftPath *cf = nullptr;    // poisson = BLGPU_POISSON_CUFFT: plans and work arrays
+  int cf_status = 0;          // first failing cufftExec status of an enqueued step (0: none)
   bool have_tmaps = false;
   int nsm = 148;
   Scalars *sc = nullptr;
@@ -238,8 +240,8 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown LES model %d", cfg->les_model);
   if (cfg->precision != BLGPU_FP64 && cfg->precision != BLGPU_MIXED)
     return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown precision %d", cfg->precision);
-  if (cfg->poisson != BLGPU_POISSON_NATIVE)
-    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: poisson backend %d not available", cfg->poisson);
+  if (cfg->poisson != BLGPU_POISSON_NATIVE && cfg->poisson != BLGPU_POISSON_CUFFT)
+    return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: unknown poisson backend %d", cfg->poisson);
   if (!(cfg->nu > 0)) return set_err(nullptr, BLGPU_EINVAL, "blgpu_create: nu must be > 0");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -281,6 +283,11 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   TRY(dalloc(ctx, (void **)&ctx->piv, (size_t)s.NM * s.MH * s.rx * sizeof(double)));
   ctx->have_tmaps = ctx->fp64 ? thomas_maps<double>(s, ctx->C, ctx->piv, &ctx->tmaps)
                               : thomas_maps<float>(s, ctx->C, ctx->piv, &ctx->tmaps);
+  if (cfg->poisson == BLGPU_POISSON_CUFFT) {  // cufft_init_plans (cufft_solver.f90:26-62)
+    char msg[256];
+    if (cufft_path_create(s, ctx->fp64, ctx->st, &ctx->cf, msg, sizeof msg)) TRY(set_err(ctx, BLGPU_ECUDA, "%s", msg));
+    ctx->bytes += (long long)cufft_path_bytes(ctx->cf);
+  }
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
   TRY(upload_dft_constants() == 0 ? BLGPU_OK : set_err(ctx, BLGPU_ECUDA, "DFT constants upload failed"));
   if (!ctx->fp64 && zdft_tc_qp(s)) {
@@ -417,6 +424,7 @@ int blgpu_destroy(blgpu_ctx *ctx) {
   if (ctx->xin) cudaStreamSynchronize(ctx->xin);
   if (ctx->xout) cudaStreamSynchronize(ctx->xout);
   for (void *p : ctx->allocs) cudaFree(p);
+  cufft_path_destroy(ctx->cf);  // cufft_destroy_plans (cufft_solver.f90:64-72)
   if (ctx->st) cudaStreamDestroy(ctx->st);
   if (ctx->xin) cudaStreamDestroy(ctx->xin);
   if (ctx->xout) cudaStreamDestroy(ctx->xout);
@@ -1001,6 +1009,33 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const Spec &s = ctx->spec;
   const FftPlan<T> &pl = *reinterpret_cast<const FftPlan<T> *>(ctx->fp64 ? (const void *)&ctx->pl64 : (const void *)&ctx->pl32);
   const bool mixed = !ctx->fp64;
+  if (ctx->cf) {  // cuFFT comparison path (solve_poisson_gpu, projection.f90:93-204)
+    const double *sp = ctx->d_spec;
+    int r;
+    ph_begin(ctx, PH_DIVDCT);
+    r = cufft_path_forward<T>(ctx->cf, ctx->geo, s, S[0], S[1], S[2], ctx->st);
+    if (r && !ctx->cf_status) ctx->cf_status = r;
+    ph_end(ctx, 2);
+    ph_begin(ctx, PH_THOMAS);
+    cufft_path_extract_solve<T>(ctx->cf, s, ctx->post, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr,
+                                ctx->klow, ctx->st);
+    if (mixed) launch_kz0_idct(s, ctx->kz0h, ctx->klow, ctx->cmat, ctx->kz0, ctx->kz0g, ctx->st);
+    ph_end(ctx, mixed ? 4 : 2);
+    ph_begin(ctx, PH_IDFTZ);
+    r = cufft_path_inverse_z<T>(ctx->cf);
+    if (r && !ctx->cf_status) ctx->cf_status = r;
+    ph_end(ctx, 1);
+    ph_begin(ctx, PH_IDCT);
+    r = cufft_path_inverse_x<T>(ctx->cf, ctx->geo, s, ctx->post, (T *)ctx->rhs_p, ctx->st);
+    if (r && !ctx->cf_status) ctx->cf_status = r;
+    ph_end(ctx, 3);
+    const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
+    ph_begin(ctx, PH_PROJECT);
+    launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, mixed ? ctx->kz0g : nullptr,
+                      S[0], S[1], S[2], (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
+    ph_end(ctx, rk_step == 1 ? 4 : 1);
+    return;
+  }
   ph_begin(ctx, PH_DIVDCT);
   launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->tiles.xfft, ctx->st);
   ph_end(ctx, 1);
@@ -1129,11 +1164,19 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
   }
 }
 
+// a cufftExec of the cuFFT comparison path refused work that was enqueued
+static int cf_check(blgpu_ctx *ctx) {
+  if (!ctx->cf_status) return BLGPU_OK;
+  const int r = ctx->cf_status;
+  ctx->cf_status = 0;
+  return set_err(ctx, BLGPU_ECUDA, "cuFFT comparison path: cufftExec failed (cufftResult %d)", r);
+}
+
 static int step_once(blgpu_ctx *ctx, bool with_dt) {
   int nb = ctx->fp64 ? enq_step<double>(ctx, ctx->cur, with_dt) : enq_step<float>(ctx, ctx->cur, with_dt);
   ctx->old = ctx->cur;
   ctx->cur = nb;
-  return BLGPU_OK;
+  return cf_check(ctx);
 }
 
 extern "C" {
@@ -1143,7 +1186,8 @@ int blgpu_time_step(blgpu_ctx *ctx) {
   if (!ctx->have_grid || !ctx->have_bc || !ctx->have_state)
     return set_err(ctx, BLGPU_ESTATE, "blgpu_time_step: grid, boundary and state must be set first");
   CK(cudaSetDevice(ctx->cfg.device));
-  step_once(ctx, false);
+  int rc = step_once(ctx, false);
+  if (rc) return rc;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));
   return BLGPU_OK;
@@ -1166,6 +1210,10 @@ int blgpu_advance(blgpu_ctx *ctx, int nsteps) {
       ctx->launches = l0;
       cudaError_t e = cudaStreamEndCapture(ctx->st, &gr);
       if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
+      if (ctx->cf_status) {
+        cudaGraphDestroy(gr);
+        return cf_check(ctx);
+      }
       e = cudaGraphInstantiate(&ctx->graph[a], gr, 0);
       cudaGraphDestroy(gr);
       if (e != cudaSuccess) return check_cuda(ctx, e, "cudaGraphInstantiate");
@@ -1271,6 +1319,8 @@ int blgpu_projection(blgpu_ctx *ctx, int rk_step) {
   CK(cudaSetDevice(ctx->cfg.device));
   if (ctx->fp64) enq_projection<double>(ctx, ctx->cur, rk_step);
   else enq_projection<float>(ctx, ctx->cur, rk_step);
+  int rc = cf_check(ctx);
+  if (rc) return rc;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));
   return BLGPU_OK;
@@ -1336,7 +1386,8 @@ int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels
   }
   ctx->prof_on = true;
   ctx->marks.clear();
-  for (int n = 0; n < nsteps; ++n) step_once(ctx, true);
+  int rc = 0;
+  for (int n = 0; n < nsteps && !rc; ++n) rc = step_once(ctx, true);
   ctx->prof_on = false;
   cudaError_t e = cudaStreamSynchronize(ctx->st);
   for (auto &mk : ctx->marks) {
@@ -1349,7 +1400,7 @@ int blgpu_phase_times(blgpu_ctx *ctx, int nsteps, double *ms, long long *kernels
   }
   ctx->marks.clear();
   CK(e);
-  return BLGPU_OK;
+  return rc;
 }
 
 long long blgpu_kernel_launches(const blgpu_ctx *ctx) { return ctx ? ctx->launches : 0; }

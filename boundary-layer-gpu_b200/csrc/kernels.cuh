@@ -160,6 +160,23 @@ bool zdft_tc_maps(const Spec &s, float *R, float2 *C, ZdftMaps *out);
 // flag, bit 2 set when a TMA copy did not complete within the wait limit
 void launch_zdft_tc(const Spec &s, const ZdftMaps &maps, float *R, float2 *C, const uint32_t *frag, int inverse,
                     int nsm, int *err, cudaStream_t st);
+// ---- cufft_path.cu: the cuFFT comparison path (solve_poisson_gpu with cuFFT plans) ----
+struct CufftPath;
+// plans (set to stream st) and the 2N plane / mode arrays; 0 or -1 with msg
+int cufft_path_create(const Spec &s, bool fp64, cudaStream_t st, CufftPath **out, char *msg, size_t cap);
+void cufft_path_destroy(CufftPath *c);
+size_t cufft_path_bytes(const CufftPath *c);
+// divergence + symmetric pack + 2D forward transform; returns the cufftResult
+template <typename T>
+int cufft_path_forward(CufftPath *c, const Geo &g, const Spec &s, const T *U, const T *V, const T *W, cudaStream_t st);
+// twiddle extract + y-solve (post = the DCT twiddles exp(-i pi i/2N) in T)
+template <typename T>
+void cufft_path_extract_solve(CufftPath *c, const Spec &s, const void *post, const double *piv, const double *dl,
+                              const double *du, double *H0, int klow, cudaStream_t st);
+template <typename T> int cufft_path_inverse_z(CufftPath *c);
+// untwiddle + Hermitian extension + inverse x transform + rhs_p into the box
+template <typename T>
+int cufft_path_inverse_x(CufftPath *c, const Geo &g, const Spec &s, const void *post, T *p, cudaStream_t st);
 // ---- thomas_tma.cu: the y-solve as one TMA-fed pass over tiles ----
 struct ThomasMaps {  // CUtensorMap bytes of C and of the pivots
   alignas(64) unsigned char c[128];

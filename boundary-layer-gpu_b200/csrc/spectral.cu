@@ -18,6 +18,7 @@
 //               z-periodic copies of apply_periodic_z_pressure
 //               (projection.f90:295-303).
 #include "kernels.cuh"
+#include "divergence.cuh"
 #include "tma.cuh"
 
 namespace blgpu {
@@ -462,19 +463,6 @@ template <int A, int B> struct TwoPassX {
 // the real lines q and q+1 (q = b*M + k').  R[q][kx] receives
 // c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
 // ---------------------------------------------------------------------------
-// FP64: the source's divisions; FP32: products with the reciprocal spacing
-__device__ __forceinline__ double dq(double a, double F, double) { return a / F; }
-__device__ __forceinline__ float dq(float a, double, double rF) { return a * (float)rF; }
-
-template <typename T>
-__device__ __forceinline__ T div_at(const Geo &g, const T *__restrict__ U, const T *__restrict__ V,
-                                    const T *__restrict__ W, long long c, int i, int j, int k) {
-  // projection.f90:42-44
-  return dq(__ldg(U + c) - __ldg(U + c - 1), g.ax.F[i], g.ax.rF[i]) +
-         dq(__ldg(V + c) - __ldg(V + c - g.px), g.ay.F[j], g.ay.rF[j]) +
-         dq(__ldg(W + c) - __ldg(W + c - g.plane), g.az.F[k], g.az.rF[k]);
-}
-
 // FP32 CTAs take up to 16 lines (one CTA fills an SM's shared memory); the
 // FP64 kernels need more registers per thread and stop at 8
 template <typename T> struct DctCta { static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256; };
