@@ -3,17 +3,18 @@
 The FP64 form after 10 RK3 steps (CFL 0.5, Lund inflow, flag 3, from
 i = 81) against the CPU oracle's restatement of the reference step
 (time_integration.f90:305-465, projection.f90:21-386,
-rescaled_inlet_bc.f90:60-345): relative L2 <= 1e-10 per component, and the
-maximum divergence (check_divergence, projection.f90:391-413) equal to the
-oracle's within 1e-12.  The shape exercises what the small grids do not:
+rescaled_inlet_bc.f90:60-345): relative L2 <= 1e-10 per component, the
+maximum divergence (check_divergence, projection.f90:391-413) of the same
+size as the oracle's, and <= 1e-12 after a projection.  The shape exercises what the small grids do not:
 the x transform of N = 812 (29 x 28), the prime z length M = 191 (Q = 96),
 256 unknowns per y-solve and the Lund station.
 
-The maximum divergence after a step is not at rounding level in either
-code: the boundary pass that follows the projection (time_integration.f90:
-379-381) moves the outflow plane and adds the mass-flux correction to
-U(nx-1), which the recycled inflow makes non-zero every step; the oracle
-shows the same value.
+The maximum divergence at the end of a step is not the projection's: the
+boundary pass that follows the projection (time_integration.f90:379-381)
+adds the mass-flux correction to U(nx-1), which after the projection is the
+rounding of the flux sums over the inflow and outflow planes (about 3e-10
+here, in both codes).  The projection itself is checked by one more
+projection after the 10 steps: maximum divergence <= 1e-12.
 
 The mixed form is checked against the same oracle run: relative L2 <= 1e-5
 (u, w) after 10 steps.
@@ -42,26 +43,37 @@ def reference_run():
     o.advance(STEPS)
     U, V, W, P, t = o.state()
     div = o.max_divergence()
+    # one more projection (no boundary pass after it): the divergence the
+    # projection itself leaves
+    o.projection(2)
+    div_proj = o.max_divergence()
     o.close()
-    return c, (U, V, W, P, t), div
+    return c, (U, V, W, P, t), div, div_proj
 
 
 def test_fp64_full_shape_10_steps(gpu, reference_run):
-    c, (Ur, Vr, Wr, Pr, tr), div_ref = reference_run
+    c, (Ur, Vr, Wr, Pr, tr), div_ref, div_proj_ref = reference_run
     s = cases.solver_for(c, precision=FP64)
     s.advance(STEPS)
     U, V, W, P, t = s.download_state()
     div = s.check_divergence()
+    s.compute_projection_step(2)
+    div_proj = s.check_divergence()
     s.close()
     errs = {"u": rel(U, Ur), "v": rel(V, Vr), "w": rel(W, Wr)}
-    print("fp64 814x257x193 after %d steps: rel L2 %s, max div %.3e (oracle %.3e)" % (STEPS, errs, div, div_ref))
+    print("fp64 814x257x193 after %d steps: rel L2 %s; max div %.3e (oracle %.3e); after one more projection "
+          "%.3e (oracle %.3e)" % (STEPS, errs, div, div_ref, div_proj, div_proj_ref))
     assert max(errs.values()) <= 1e-10, errs
-    assert abs(div - div_ref) <= 1e-12, (div, div_ref)
     assert t == pytest.approx(tr, rel=1e-14)
+    # end of step: the rounding of the mass-flux sums, the same size in both codes
+    assert div <= 1e-9 and div_ref <= 1e-9
+    assert div <= 1.5 * div_ref and div_ref <= 1.5 * div
+    # the projection itself leaves the field divergence free to 1e-12
+    assert div_proj <= 1e-12, div_proj
 
 
 def test_mixed_full_shape_10_steps(gpu, reference_run):
-    c, (Ur, Vr, Wr, Pr, tr), _ = reference_run
+    c, (Ur, Vr, Wr, Pr, tr), _, _ = reference_run
     s = cases.solver_for(c, precision=MIXED)
     s.advance(STEPS)
     U, V, W, P, t = s.download_state()
