@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-les", action="store_true")
+    ap.add_argument("--no-cufft", action="store_true")
     ap.add_argument("--ens-boxes", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--profile", default=None, choices=["mixed", "fp64", "ensemble"],
@@ -319,6 +320,27 @@ def run_les(args, dev):
     return out
 
 
+def run_cufft(args, case, dev):
+    """The cuFFT comparison path (poisson = BLGPU_POISSON_CUFFT) against the
+    hand-written transforms on the same box: graph-replayed step time and the
+    per-phase device times (CUDA events) of the Poisson solve, FP64 and mixed."""
+    import blgpu
+    from blgpu import cases
+    out = {}
+    for name, prec in (("fp64", blgpu.FP64), ("mixed", blgpu.MIXED)):
+        s = cases.solver_for(case, precision=prec, device=dev, poisson=blgpu.POISSON_CUFFT)
+        s.advance(2)
+        n = 5
+        ms = s.advance_timed(n) / n
+        ph = s.phase_times(1)
+        keep = ("div_dct", "dft_z", "thomas", "idft_z", "idct", "project")
+        out[name] = {"ms_per_step": round(ms, 4),
+                     "poisson_ms_per_step": round(sum(ph[k][0] for k in keep), 4),
+                     "phases": {k: round(ph[k][0], 4) for k in keep}}
+        s.close()
+    return out
+
+
 def run_profile(args):
     """Small driver for ncu: set-up and warm-up outside the profiled range."""
     import torch
@@ -473,6 +495,12 @@ def main():
            "what": "upload_state_async + advance(1) + download_state_async per step (FP64 Fortran-layout pinned "
                    "host arrays, copies overlapping the steps), wall clock to the final blgpu_sync"}
     smix.close()
+    cufft = None
+    if not args.no_cufft:
+        cufft = run_cufft(args, case, dev)
+        keep = ("div_dct", "dft_z", "thomas", "idft_z", "idct", "project")
+        cufft["native_poisson_ms_per_step"] = {"mixed": round(sum(ph[k][0] for k in keep) / 2.0, 4),
+                                               "fp64": round(sum(ph64[k][0] for k in keep), 4) if fp64 else None}
     ens = None
     if not args.no_ensemble:
         ens = run_ensemble(args, dev, pg, local, world)
@@ -494,7 +522,7 @@ def main():
                                                   % (smix_bytes(case, 4) / 1e6),
                            "replicas_per_gpu": 1},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk, "ensemble": ens, "les_mixed": les,
+                "clocks": clk, "ensemble": ens, "les_mixed": les, "cufft_path": cufft,
                 "phases_ms_per_step_mixed": {k: round(v[0] / 2.0, 4) for k, v in ph.items()},
                 "phases_ms_per_step_fp64": ({k: round(v[0], 4) for k, v in ph64.items()} if fp64 else None),
                 "eager_step_ms_mixed": step_ms,

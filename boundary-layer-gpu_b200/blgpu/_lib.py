@@ -47,6 +47,11 @@ PARAM_KEYS = ["nu", "CFL", "Vmax", "x0", "sigma", "phi", "nsteps", "nsave", "nst
               "init_rand", "filein", "fileout", "timeinflow_file", "RKscheme", "alphas"]
 
 
+class ModesInfo(ctypes.Structure):
+    _fields_ = [("ny_inlet", ctypes.c_int), ("n_modes", ctypes.c_int), ("m_modes", ctypes.c_int),
+                ("beta", ctypes.c_double), ("omega", ctypes.c_double)]
+
+
 class SnapshotInfo(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("nu", ctypes.c_double), ("step", ctypes.c_int),
                 ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -143,6 +148,8 @@ _SIGS = {
     "blgpu_snapshot_name": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "blgpu_output_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "blgpu_read_input_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "blgpu_read_temporal_modes_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ModesInfo)]),
+    "blgpu_read_temporal_modes": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int] + [c_double_p] * 7),
 }
 
 PHASES = ["rhs_rk", "bc", "div_dct", "dft_z", "thomas", "idft_z", "idct", "project", "compute_dt", "time"]

@@ -6,12 +6,14 @@ write_snapshot    flow snapshot in the one-process layout (output_data, input_ou
 read_rescaling,
 write_rescaling   <snapshot>.mean.rescaling Lund means (input_output.f90:440-458, 668-676)
 snapshot_name     fileout.%08d
+read_temporal_modes  the binary temporal inflow-mode file of the transition case
+                  (compute_blasius_solution_for_bc, boundary_conditions.f90:1652-1797)
 """
 import ctypes
 
 import numpy as np
 
-from ._lib import Config, Params, PARAM_KEYS, SnapshotInfo, check_io, load
+from ._lib import Config, ModesInfo, Params, PARAM_KEYS, SnapshotInfo, check_io, load
 
 
 def _p(a):
@@ -102,3 +104,26 @@ def snapshot_name(fileout, step):
     buf = ctypes.create_string_buffer(4096)
     check_io(load().blgpu_snapshot_name(str(fileout).encode(), int(step), buf, 4096))
     return buf.value.decode()
+
+
+def temporal_modes_info(path):
+    h = ModesInfo()
+    check_io(load().blgpu_read_temporal_modes_info(str(path).encode(), ctypes.byref(h)))
+    return dict(ny_inlet=h.ny_inlet, n_modes=h.n_modes, m_modes=h.m_modes, beta=h.beta, omega=h.omega)
+
+
+def read_temporal_modes(path, y):
+    """The file's modes on the face grid y(ny) and its centres: zmode (n,),
+    tmode (m,) already scaled by beta / omega; qu (ny+1, n, m), qv (ny, n, m),
+    qw (ny+1, n, m) complex; ymesh (ny_inlet,).  The arguments of
+    Solver.set_inflow_modes."""
+    h = temporal_modes_info(path)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    ny, n, m = len(y), h["n_modes"], h["m_modes"]
+    zm, tm = np.zeros(n), np.zeros(m)
+    qu, qw = np.zeros(2 * (ny + 1) * n * m), np.zeros(2 * (ny + 1) * n * m)
+    qv, ym = np.zeros(2 * ny * n * m), np.zeros(h["ny_inlet"])
+    check_io(load().blgpu_read_temporal_modes(str(path).encode(), ny, _p(y), _p(zm), _p(tm), _p(qu), _p(qv),
+                                              _p(qw), _p(ym)))
+    cplx = lambda a, n1: a.view(np.complex128).reshape((n1, n, m), order="F")
+    return dict(zmode=zm, tmode=tm, qu=cplx(qu, ny + 1), qv=cplx(qv, ny), qw=cplx(qw, ny + 1), ymesh=ym, info=h)

@@ -590,4 +590,101 @@ int blgpu_read_input_data(blgpu_ctx *ctx, const char *filein, int *step) {
   return BLGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Temporal inflow modes (the inflow_flag = 1 branch of
+// compute_blasius_solution_for_bc, boundary_conditions.f90:1652-1797).  The
+// file is a native-order stream: ny_inlet, n, m (int32), beta, omega (f64),
+// ymesh(ny_inlet), zmode(n), tmode(m), then qu_r, qu_i, qv_r, qv_i, qw_r,
+// qw_i, each (ny_inlet, n, m) in Fortran order.
+// ---------------------------------------------------------------------------
+int blgpu_read_temporal_modes_info(const char *path, blgpu_modes_info *h) {
+  if (!path || !h) return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes_info: null argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return io_err(BLGPU_EINVAL, "cannot open %s: %s", path, strerror(errno));
+  int32_t iv[3];
+  double dv[2];
+  const bool ok = rd(f, iv, sizeof iv) && rd(f, dv, sizeof dv);
+  fseek(f, 0, SEEK_END);
+  const long long size = ftell(f);
+  fclose(f);
+  if (!ok) return io_err(BLGPU_EINVAL, "%s: short header", path);
+  if (iv[0] < 2 || iv[1] < 1 || iv[2] < 1 || iv[0] > (1 << 24) || iv[1] > 4096 || iv[2] > 4096)
+    return io_err(BLGPU_EINVAL, "%s: implausible sizes ny_inlet %d, n %d, m %d", path, iv[0], iv[1], iv[2]);
+  const long long nq = (long long)iv[0] * iv[1] * iv[2];
+  const long long want = 12 + 16 + 8LL * (iv[0] + iv[1] + iv[2]) + 6 * 8 * nq;
+  if (size != want)
+    return io_err(BLGPU_EINVAL, "%s: %lld bytes, the header's sizes need %lld", path, size, want);
+  h->ny_inlet = iv[0];
+  h->n_modes = iv[1];
+  h->m_modes = iv[2];
+  h->beta = dv[0];
+  h->omega = dv[1];
+  return BLGPU_OK;
+}
+
+int blgpu_read_temporal_modes(const char *path, int ny, const double *y, double *zmode, double *tmode, double *qu,
+                              double *qv, double *qw, double *ymesh) {
+  blgpu_modes_info h{};
+  int rc = blgpu_read_temporal_modes_info(path, &h);
+  if (rc) return rc;
+  if (!y || ny < 3 || !zmode || !tmode || !qu || !qv || !qw)
+    return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes: bad argument");
+  for (int j = 1; j < ny; ++j)
+    if (!(y[j] > y[j - 1])) return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes: y not increasing at %d", j + 1);
+  const int nyi = h.ny_inlet, n = h.n_modes, m = h.m_modes;
+  const long long nq = (long long)nyi * n * m;
+  std::vector<double> ym(nyi), zm(n), tm(m), q(6 * nq);
+  FILE *f = fopen(path, "rb");
+  if (!f) return io_err(BLGPU_EINVAL, "cannot open %s: %s", path, strerror(errno));
+  fseek(f, 28, SEEK_SET);
+  const bool ok = rd(f, ym.data(), 8 * nyi) && rd(f, zm.data(), 8 * n) && rd(f, tm.data(), 8 * m) &&
+                  rd(f, q.data(), 8 * 6 * nq);
+  fclose(f);
+  if (!ok) return io_err(BLGPU_EINVAL, "%s: short read", path);
+  for (int a = 0; a < n; ++a) zmode[a] = h.beta * zm[a];   // zmode_inlet = beta_inlet*zmode_inlet
+  for (int b = 0; b < m; ++b) tmode[b] = h.omega * tm[b];  // tmode_inlet = omega_inlet*tmode_inlet
+  if (ymesh)
+    for (int j = 0; j < nyi; ++j) ymesh[j] = ym[j];
+  // centres with mirrored ghosts (initialization.f90:174-222): yg(1..ny+1)
+  const int nyg = ny + 1;
+  std::vector<double> yc(ny - 1), yg(nyg);
+  for (int j = 0; j < ny - 1; ++j) yc[j] = 0.5 * (y[j] + y[j + 1]);
+  for (int j = 0; j < ny - 1; ++j) yg[j + 1] = yc[j];
+  yg[0] = yc[0] - 2.0 * (yc[0] - y[0]);
+  yg[ny] = yc[ny - 2] + 2.0 * (y[ny - 1] - yc[ny - 2]);
+  // linear interpolation of the modes onto target rows (boundary_conditions.f90:1730-1774):
+  // j1 = first jj >= 2 with ymesh(jj) >= target, else ny_inlet; rows at or past the
+  // mesh end are zero
+  auto interp = [&](const double *re, const double *im, const std::vector<double> &tgt, double *out) {
+    const int nt = (int)tgt.size();
+    for (int j = 0; j < nt; ++j) {
+      int j1 = nyi;  // 1-based
+      for (int jj = 2; jj <= nyi; ++jj)
+        if (ym[jj - 1] >= tgt[j]) {
+          j1 = jj;
+          break;
+        }
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < m; ++b) {
+          double *o = out + 2 * ((long long)j + (long long)nt * (a + (long long)n * b));
+          if (j1 == nyi) {
+            o[0] = o[1] = 0.0;
+            continue;
+          }
+          const int j0 = j1 - 1;
+          const long long i0 = (j0 - 1) + (long long)nyi * (a + (long long)n * b), i1 = i0 + 1;
+          // q(j0) + (y - ymesh(j0)) (q(j1) - q(j0)) / (ymesh(j1) - ymesh(j0)), per component
+          const double dy = tgt[j] - ym[j0 - 1], span = ym[j1 - 1] - ym[j0 - 1];
+          o[0] = re[i0] + dy * (re[i1] - re[i0]) / span;
+          o[1] = im[i0] + dy * (im[i1] - im[i0]) / span;
+        }
+    }
+  };
+  std::vector<double> yv(y, y + ny);
+  interp(q.data(), q.data() + nq, yg, qu);
+  interp(q.data() + 2 * nq, q.data() + 3 * nq, yv, qv);
+  interp(q.data() + 4 * nq, q.data() + 5 * nq, yg, qw);
+  return BLGPU_OK;
+}
+
 }  // extern "C"

@@ -415,6 +415,27 @@ int blgpu_output_data(blgpu_ctx *ctx, const char *fileout, int step, int rescali
  * blgpu_read_rescaling. */
 int blgpu_read_input_data(blgpu_ctx *ctx, const char *filein, int *step);
 
+/* Temporal inflow modes of the transition case (inflow_flag = 1): the binary
+ * mode file read by compute_blasius_solution_for_bc
+ * (boundary_conditions.f90:1652-1797), a native-order stream of ny_inlet,
+ * n, m (int32), beta, omega (f64), ymesh(ny_inlet), zmode(n), tmode(m) and
+ * the real and imaginary parts of qu, qv, qw (ny_inlet, n, m).  The info
+ * call reads the header and checks the file size against it. */
+typedef struct blgpu_modes_info {
+  int ny_inlet, n_modes, m_modes;
+  double beta, omega;
+} blgpu_modes_info;
+int blgpu_read_temporal_modes_info(const char *path, blgpu_modes_info *h);
+/* The modes on the solver's mesh, ready for blgpu_set_inflow_modes:
+ * zmode(n) = beta * file zmode, tmode(m) = omega * file tmode; qu(nyg,n,m)
+ * and qw(nyg,n,m) interpolated linearly to the cell centres yg, qv(ny,n,m)
+ * to the faces y (the face grid y(ny) is given; centres and ghosts as in
+ * initialization.f90:174-222); rows at or above the file's last ymesh point
+ * are zero, as in the reference.  Complex values as interleaved (re, im)
+ * doubles; ymesh (may be NULL) receives the file's mesh. */
+int blgpu_read_temporal_modes(const char *path, int ny, const double *y, double *zmode, double *tmode, double *qu,
+                              double *qv, double *qw, double *ymesh);
+
 #ifdef __cplusplus
 }
 #endif
