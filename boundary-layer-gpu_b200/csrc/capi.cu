@@ -999,7 +999,7 @@ static void enq_bc(blgpu_ctx *ctx, int b, int o, int rk_step) {
   ph_begin(ctx, PH_BC);
   launch_bc<T>(ctx->geo, ctx->bc, S[0], S[1], S[2], So[0], So[1], So[2], ctx->sc, ctx->rk_t[rk_step], ctx->qx_part,
                ctx->qy, ctx->length_y, ctx->st);
-  ph_end(ctx, 4);
+  ph_end(ctx, 2);
 }
 
 template <typename T>

@@ -656,9 +656,9 @@ __global__ void k_p_ghost(Geo g, T *__restrict__ P, int phase) {
 }
 
 // ---------------------------------------------------------------------------
-// Boundary conditions, boundary_conditions.f90:127-262, in four ordered
-// launches: (1) inflow + convective outflow planes (+ the x mass-flux
-// partial sums), (2) z periodicity, (3) top and wall, (4) mass correction.
+// Boundary conditions, boundary_conditions.f90:127-262, in two ordered
+// launches: k_bc_all (every boundary value but the mass correction, and the
+// x mass-flux sum) and k_bc_mass (the correction of U(nx-1), U(nx)).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double mode_sum(const double2 *__restrict__ q, int ld, int j, int nm, int mm,
                                            const double *__restrict__ zmode, const double *__restrict__ tmode,
@@ -676,174 +676,241 @@ __device__ __forceinline__ double mode_sum(const double2 *__restrict__ q, int ld
   return acc;
 }
 
-template <typename T>
-__global__ void k_bc_x(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W,
-                       const T *__restrict__ Uo, const T *__restrict__ Vo, const T *__restrict__ Wo,
-                       Scalars *__restrict__ sc, double rkt, double *__restrict__ qx_part, double qy,
-                       double length_y) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;  // 1..nyg
-  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;  // 1..nzg
-  double q = 0.0;
-  if (j <= g.nyg && k <= g.nzg) {
-    const double t = sc->t, dt = sc->dt;
-    const int nx = g.nx, nxg = g.nxg;
-    // inflow (:182-190), with the temporal modes of :137-180
-    // or the Lund planes of the step: flag 3 replaces the whole plane
-    // (boundary_conditions.f90:586-594), flag 5 adds the fluctuations to the
-    // inlet profile with W taken at ks = mod(k+16,nz)+1 (:527-553)
-    double u1d, v1d = 0.0, w1d = 0.0;
-    if (bc.lund == 3) {
-      u1d = bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
-      if (k <= g.nz) w1d = bc.lw[(long long)(k - 1) * g.nyg + (j - 1)];
-      if (j <= g.ny) v1d = bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
-    } else if (bc.lund == 5) {
-      u1d = bc.U_inlet[j] + bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
-      if (k <= g.nz) {
-        const int ks = (k + 16) % g.nz + 1;
-        w1d = bc.W_inlet[j] + bc.lw[(long long)(ks - 1) * g.nyg + (j - 1)];
-      }
-      if (j <= g.ny) v1d = bc.V_inlet[j] + bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
-    } else {
-      double ut = 0.0, vt = 0.0, wt = 0.0;
-      if (bc.n_modes > 0) {
-        ut = mode_sum(bc.qu, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
-        if (j <= g.ny) vt = mode_sum(bc.qv, g.ny, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
-        if (k <= g.nz) wt = mode_sum(bc.qw, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.z[k], t);
-      } else if (bc.ut) {
-        ut = bc.ut[(long long)(k - 1) * g.nyg + (j - 1)];
-        if (j <= g.ny) vt = bc.vt[(long long)(k - 1) * g.ny + (j - 1)];
-        if (k <= g.nz) wt = bc.wt[(long long)(k - 1) * g.nyg + (j - 1)];
-      }
-      u1d = bc.U_inlet[j] + ut;
-      if (k <= g.nz) w1d = bc.W_inlet[j] + wt;
-      if (j <= g.ny) v1d = bc.V_inlet[j] + vt;
-    }
-    const T u1 = (T)u1d;
-    U[bidx(g, 1, j, k)] = u1;
-    if (k <= g.nz) W[bidx(g, 1, j, k)] = (T)w1d;
-    if (j <= g.ny) V[bidx(g, 1, j, k)] = (T)v1d;
-    // outflow (:193-201): rk_t(rk_step)*dt*Uc*(Uo(nx-1)-Uo(nx-2))/(x(nx-1)-x(nx-2))
-    const double cc = rkt * dt * bc.U_top[nx];
-    {
-      long long a = bidx(g, nx - 1, j, k);
-      T uo1 = Uo[a], uo2 = Uo[a - 1];
-      const T un = (T)((double)uo1 - cc * (double)(uo1 - uo2) / g.ax.F[nx - 1]);
-      U[a] = un;
-      U[a + 1] = un;
-      if (j >= 2 && j <= g.nyg - 1 && k >= 2 && k <= g.nzg - 2)
-        q = ((double)u1 - (double)un) * g.ay.F[j];
-    }
-    if (j <= g.ny) {
-      long long a = bidx(g, nxg - 1, j, k);
-      T vo1 = Vo[a], vo2 = Vo[a - 1];
-      const T vn = (T)((double)vo1 - cc * (double)(vo1 - vo2) / g.ax.C[nxg - 2]);
-      V[a] = vn;
-      V[a + 1] = vn;
-    }
-    if (k <= g.nz) {
-      long long a = bidx(g, nxg - 1, j, k);
-      T wo1 = Wo[a], wo2 = Wo[a - 1];
-      const T wn = (T)((double)wo1 - cc * (double)(wo1 - wo2) / g.ax.C[nxg - 2]);
-      W[a] = wn;
-      W[a + 1] = wn;
-    }
+// Every boundary value the routine leaves before its mass correction is a
+// function of the inflow data, the step's start fields Uo, Vo, Wo and the
+// interior of the current fields, evaluated in the routine's order:
+//   x planes (1) inflow at i = 1, (2) convective outflow at i = nx-1 (U) and
+//     nxg-1 (V, W) with the plane beyond it equal;
+//   (3) z ghosts: U, V: k = 1 <- nzg-2, nzg-1 <- 2, nzg <- 3; W: 1 <- nz-1,
+//     nz <- 2 (copies of what (1), (2) left there);
+//   (4) top rows U(:,nyg,:), V(:,ny,:), W(:,nyg,:) = U_top, V_top, W_top;
+//   (5) wall rows U(:,1,:) = -U(:,2,:), V(:,1,:) = 0, W(:,1,:) = -W(:,2,:)
+//     (or the wall model's Neumann rows) from what (1)-(3) left in row 2.
+// k_bc_all writes each boundary point once with that final value, so its
+// three segments of blocks (x planes; z ghosts of interior columns; y rows of
+// interior columns) read nothing another thread writes.  The x-plane blocks
+// also form the x mass-flux partials; the last of them sums the partials in
+// block order and leaves the correction in sc->dU for k_bc_mass (6).
+template <typename T> struct BcX {
+  // (1): U, V, W at i = 1 of row j, plane k
+  __device__ static double in_u(const Geo &g, const BcData &bc, int j, int k, double t) {
+    if (bc.lund == 3) return bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
+    if (bc.lund == 5) return bc.U_inlet[j] + bc.lu[(long long)(k - 1) * g.nyg + (j - 1)];
+    double ut = 0.0;
+    if (bc.n_modes > 0) ut = mode_sum(bc.qu, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+    else if (bc.ut) ut = bc.ut[(long long)(k - 1) * g.nyg + (j - 1)];
+    return bc.U_inlet[j] + ut;
   }
-  // deterministic block reduction of the x mass-flux partials (:242-246)
-  __shared__ double red[256];
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  red[tid] = q;
-  __syncthreads();
-  for (int s = (blockDim.x * blockDim.y) / 2; s > 0; s >>= 1) {
-    if (tid < s) red[tid] += red[tid + s];
-    __syncthreads();
+  __device__ static double in_v(const Geo &g, const BcData &bc, int j, int k, double t) {  // j <= ny
+    if (bc.lund == 3) return bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
+    if (bc.lund == 5) return bc.V_inlet[j] + bc.lv[(long long)(k - 1) * g.ny + (j - 1)];
+    double vt = 0.0;
+    if (bc.n_modes > 0) vt = mode_sum(bc.qv, g.ny, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.zg[k], t);
+    else if (bc.ut) vt = bc.vt[(long long)(k - 1) * g.ny + (j - 1)];
+    return bc.V_inlet[j] + vt;
   }
-  // the last block to finish sums the partials in block order (the same
-  // fixed order for every launch) and leaves the flux correction in sc->dU
-  // (:240-260); the arrival counter sits after the partials
-  const int nparts = gridDim.x * gridDim.y, nt = blockDim.x * blockDim.y;
-  unsigned int *arrived = reinterpret_cast<unsigned int *>(qx_part + nparts);
-  __shared__ int last;
-  if (tid == 0) {
-    qx_part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
-    __threadfence();
-    last = atomicAdd(arrived, 1u) == (unsigned)(nparts - 1);
-  }
-  __syncthreads();
-  if (last) {
-    // the block loads the partials in parallel, thread 0 adds them in order
-    __threadfence();
-    double qx = 0.0;
-    for (int p0 = 0; p0 < nparts; p0 += nt) {
-      const int n = min(nt, nparts - p0);
-      if (tid < n) red[tid] = __ldcg(qx_part + p0 + tid);
-      __syncthreads();
-      if (tid == 0)
-        for (int p = 0; p < n; ++p) qx += red[p];
-      __syncthreads();
+  __device__ static double in_w(const Geo &g, const BcData &bc, int j, int k, double t) {  // k <= nz
+    if (bc.lund == 3) return bc.lw[(long long)(k - 1) * g.nyg + (j - 1)];
+    if (bc.lund == 5) {
+      const int ks = (k + 16) % g.nz + 1;  // boundary_conditions.f90:527-553
+      return bc.W_inlet[j] + bc.lw[(long long)(ks - 1) * g.nyg + (j - 1)];
     }
-    if (tid == 0) {
-      sc->dU = (qx + qy) / length_y / (double)(g.nzg - 3);
-      *arrived = 0u;
-    }
+    double wt = 0.0;
+    if (bc.n_modes > 0) wt = mode_sum(bc.qw, g.nyg, j, bc.n_modes, bc.m_modes, bc.zmode, bc.tmode, g.z[k], t);
+    else if (bc.ut) wt = bc.wt[(long long)(k - 1) * g.nyg + (j - 1)];
+    return bc.W_inlet[j] + wt;
   }
-}
-
-template <typename T>
-__global__ void k_bc_z(Geo g, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W) {
-  // :204-216
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  if (i > g.nxg || j > g.nyg) return;
-  const long long P = g.plane;
-  const long long c1 = bidx(g, i, j, 1);
-  const int nzg = g.nzg, nz = g.nz;
-  if (i <= g.nx) {
-    U[c1] = U[c1 + (nzg - 3) * P];
-    U[c1 + (nzg - 2) * P] = U[c1 + 1 * P];
-    U[c1 + (nzg - 1) * P] = U[c1 + 2 * P];
+  // (2): rk_t(rk_step) dt Uc (Fo(n-1) - Fo(n-2)) / spacing, cc = rk_t dt Uc
+  __device__ static T out_u(const Geo &g, const T *__restrict__ Uo, int j, int k, double cc) {
+    const long long a = bidx(g, g.nx - 1, j, k);
+    const T uo1 = Uo[a], uo2 = Uo[a - 1];
+    return (T)((double)uo1 - cc * (double)(uo1 - uo2) / g.ax.F[g.nx - 1]);
   }
-  if (j <= g.ny) {
-    V[c1] = V[c1 + (nzg - 3) * P];
-    V[c1 + (nzg - 2) * P] = V[c1 + 1 * P];
-    V[c1 + (nzg - 1) * P] = V[c1 + 2 * P];
+  __device__ static T out_vw(const Geo &g, const T *__restrict__ Fo, int j, int k, double cc) {
+    const long long a = bidx(g, g.nxg - 1, j, k);
+    const T f1 = Fo[a], f2 = Fo[a - 1];
+    return (T)((double)f1 - cc * (double)(f1 - f2) / g.ax.C[g.nxg - 2]);
   }
-  W[c1] = W[c1 + (nz - 2) * P];
-  W[c1 + (nz - 1) * P] = W[c1 + 1 * P];
-}
-
-template <typename T>
-__global__ void k_bc_y(Geo g, BcData bc, T *__restrict__ U, T *__restrict__ V, T *__restrict__ W) {
-  // top (:219-227) then wall (:230-237)
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  if (i > g.nxg || k > g.nzg) return;
-  if (i <= g.nx) U[bidx(g, i, g.nyg, k)] = (T)bc.U_top[i];
-  V[bidx(g, i, g.ny, k)] = (T)bc.V_top[i];
-  if (k <= g.nz) W[bidx(g, i, g.nyg, k)] = (T)bc.W_top[i];
-  // a wall model replaces the no-slip U (and W) rows by the non-zero Neumann
-  // condition F(:,1,:) = F(:,2,:) - alpha (yg(2) - yg(1)) of
-  // boundary_conditions.f90:359-372, alpha = tau_wall / nu_wall per wall
-  // point (i = 2..nx-1, k = 2..nzg-2; ghost rows take their periodic / end value)
-  if (bc.wm_ax) {
+  // z source plane of a ghost plane, (3)
+  __device__ static int ks_uv(const Geo &g, int k) {
+    return k == 1 ? g.nzg - 2 : (k == g.nzg - 1 ? 2 : (k == g.nzg ? 3 : k));
+  }
+  __device__ static int ks_w(const Geo &g, int k) { return k == 1 ? g.nz - 1 : (k == g.nz ? 2 : k); }
+  // (5) with the wall model: F(i,1,k) = F(i,2,k) - alpha (yg(2) - yg(1)) at the
+  // wall point (ic, kc) that column i, plane k takes (boundary_conditions.f90:359-372)
+  __device__ static long long wm_index(const Geo &g, int i, int k) {
     const int ic = min(max(i, 2), g.nx - 1);
     const int kc = k == 1 ? g.nzg - 2 : (k == g.nzg - 1 ? 2 : (k == g.nzg ? 3 : k));
-    const long long q = (long long)(kc - 2) * (g.nx - 2) + (ic - 2);
-    const double dy = g.yg[2] - g.yg[1];
-    if (i <= g.nx) U[bidx(g, i, 1, k)] = (T)((double)U[bidx(g, i, 2, k)] - bc.wm_ax[q] * dy);
-    if (k <= g.nz) {
-      if (bc.wm_az) W[bidx(g, i, 1, k)] = (T)((double)W[bidx(g, i, 2, k)] - bc.wm_az[q] * dy);
-      else W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
-    }
-  } else {
-    if (i <= g.nx) U[bidx(g, i, 1, k)] = -U[bidx(g, i, 2, k)];
-    if (k <= g.nz) W[bidx(g, i, 1, k)] = -W[bidx(g, i, 2, k)];
+    return (long long)(kc - 2) * (g.nx - 2) + (ic - 2);
   }
+  __device__ static T wall_u(const Geo &g, const BcData &bc, T row2, int i, int k) {
+    if (bc.wm_ax) return (T)((double)row2 - bc.wm_ax[wm_index(g, i, k)] * (g.yg[2] - g.yg[1]));
+    return -row2;
+  }
+  __device__ static T wall_w(const Geo &g, const BcData &bc, T row2, int i, int k) {
+    if (bc.wm_ax && bc.wm_az) return (T)((double)row2 - bc.wm_az[wm_index(g, i, k)] * (g.yg[2] - g.yg[1]));
+    return -row2;
+  }
+};
+
+struct BcGrid {  // block counts of the three segments (32 x 8 tiles)
+  int nx_blocks, nz_blocks, ny_blocks;
+  int x_tiles, zi_tiles, yi_tiles;  // tiles along the first dimension of each segment
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_bc_all(Geo g, BcData bc, BcGrid G, T *__restrict__ U, T *__restrict__ V,
+                                                T *__restrict__ W, const T *__restrict__ Uo,
+                                                const T *__restrict__ Vo, const T *__restrict__ Wo,
+                                                Scalars *__restrict__ sc, double rkt, double *__restrict__ qx_part,
+                                                double qy, double length_y) {
+  int blk = blockIdx.x;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nx = g.nx, nxg = g.nxg, ny = g.ny, nyg = g.nyg, nz = g.nz, nzg = g.nzg;
+  typedef BcX<T> X;
+  if (blk < G.nx_blocks) {
+    // ---- x planes, thread (j, k) ----
+    const int j = (blk % G.x_tiles) * 32 + tx + 1, k = (blk / G.x_tiles) * 8 + ty + 1;
+    double q = 0.0;
+    if (j <= nyg && k <= nzg) {
+      const double t = sc->t, cc = rkt * sc->dt * bc.U_top[nx];
+      // U at i = 1 and nx-1 (k_bc_mass sets i = nx)
+      {
+        const int ku = X::ks_uv(g, k);
+        T u1, un;
+        if (j == nyg) {
+          u1 = (T)bc.U_top[1];
+          un = (T)bc.U_top[nx - 1];
+        } else if (j == 1) {
+          u1 = X::wall_u(g, bc, (T)X::in_u(g, bc, 2, ku, t), 1, k);
+          un = X::wall_u(g, bc, X::out_u(g, Uo, 2, ku, cc), nx - 1, k);
+        } else {
+          u1 = (T)X::in_u(g, bc, j, ku, t);
+          un = X::out_u(g, Uo, j, ku, cc);
+          if (j <= nyg - 1 && k >= 2 && k <= nzg - 2) q = ((double)u1 - (double)un) * g.ay.F[j];  // (:242-246)
+        }
+        U[bidx(g, 1, j, k)] = u1;
+        U[bidx(g, nx - 1, j, k)] = un;
+      }
+      if (j <= ny) {  // V at i = 1, nxg-1, nxg
+        const int kv = X::ks_uv(g, k);
+        T v1, vn, vn1;
+        if (j == 1) {
+          v1 = vn = vn1 = (T)0;
+        } else if (j == ny) {
+          v1 = (T)bc.V_top[1];
+          vn = (T)bc.V_top[nxg - 1];
+          vn1 = (T)bc.V_top[nxg];
+        } else {
+          v1 = (T)X::in_v(g, bc, j, kv, t);
+          vn = vn1 = X::out_vw(g, Vo, j, kv, cc);
+        }
+        const long long a = bidx(g, nxg - 1, j, k);
+        V[bidx(g, 1, j, k)] = v1;
+        V[a] = vn;
+        V[a + 1] = vn1;
+      }
+      if (k <= nz) {  // W at i = 1, nxg-1, nxg
+        const int kw = X::ks_w(g, k);
+        T w1, wn, wn1;
+        if (j == nyg) {
+          w1 = (T)bc.W_top[1];
+          wn = (T)bc.W_top[nxg - 1];
+          wn1 = (T)bc.W_top[nxg];
+        } else if (j == 1) {
+          w1 = X::wall_w(g, bc, (T)X::in_w(g, bc, 2, kw, t), 1, k);
+          const T o2 = X::out_vw(g, Wo, 2, kw, cc);
+          wn = X::wall_w(g, bc, o2, nxg - 1, k);
+          wn1 = X::wall_w(g, bc, o2, nxg, k);
+        } else {
+          w1 = (T)X::in_w(g, bc, j, kw, t);
+          wn = wn1 = X::out_vw(g, Wo, j, kw, cc);
+        }
+        const long long a = bidx(g, nxg - 1, j, k);
+        W[bidx(g, 1, j, k)] = w1;
+        W[a] = wn;
+        W[a + 1] = wn1;
+      }
+    }
+    // deterministic block reduction of the x mass-flux partials (:242-246)
+    __shared__ double red[256];
+    const int tid = threadIdx.x;
+    red[tid] = q;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+      if (tid < s) red[tid] += red[tid + s];
+      __syncthreads();
+    }
+    // the last x-plane block to finish sums the partials in block order (the
+    // same fixed order for every launch) and leaves the flux correction in
+    // sc->dU (:240-260); the arrival counter sits after the partials
+    const int nparts = G.nx_blocks;
+    unsigned int *arrived = reinterpret_cast<unsigned int *>(qx_part + nparts);
+    __shared__ int last;
+    if (tid == 0) {
+      qx_part[blk] = red[0];
+      __threadfence();
+      last = atomicAdd(arrived, 1u) == (unsigned)(nparts - 1);
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      double qx = 0.0;
+      for (int p0 = 0; p0 < nparts; p0 += 256) {
+        const int n = min(256, nparts - p0);
+        if (tid < n) red[tid] = __ldcg(qx_part + p0 + tid);
+        __syncthreads();
+        if (tid == 0)
+          for (int p = 0; p < n; ++p) qx += red[p];
+        __syncthreads();
+      }
+      if (tid == 0) {
+        sc->dU = (qx + qy) / length_y / (double)(nzg - 3);
+        *arrived = 0u;
+      }
+    }
+    return;
+  }
+  blk -= G.nx_blocks;
+  const long long P = g.plane;
+  if (blk < G.nz_blocks) {
+    // ---- z ghost planes of the interior columns, thread (i, j): (3) ----
+    const int i = (blk % G.zi_tiles) * 32 + tx + 2, j = (blk / G.zi_tiles) * 8 + ty + 2;
+    if (i > nxg - 2 || j > nyg - 1) return;
+    const long long c1 = bidx(g, i, j, 1);
+    if (i <= nx - 2) {
+      U[c1] = U[c1 + (nzg - 3) * P];
+      U[c1 + (nzg - 2) * P] = U[c1 + 1 * P];
+      U[c1 + (nzg - 1) * P] = U[c1 + 2 * P];
+    }
+    if (j <= ny - 1) {
+      V[c1] = V[c1 + (nzg - 3) * P];
+      V[c1 + (nzg - 2) * P] = V[c1 + 1 * P];
+      V[c1 + (nzg - 1) * P] = V[c1 + 2 * P];
+    }
+    W[c1] = W[c1 + (nz - 2) * P];
+    W[c1 + (nz - 1) * P] = W[c1 + 1 * P];
+    return;
+  }
+  blk -= G.nz_blocks;
+  // ---- top and wall rows of the interior columns, thread (i, k): (4), (5) ----
+  const int i = (blk % G.yi_tiles) * 32 + tx + 2, k = (blk / G.yi_tiles) * 8 + ty + 1;
+  if (i > nxg - 2 || k > nzg) return;
+  if (i <= nx - 2) {
+    U[bidx(g, i, nyg, k)] = (T)bc.U_top[i];
+    U[bidx(g, i, 1, k)] = X::wall_u(g, bc, U[bidx(g, i, 2, X::ks_uv(g, k))], i, k);
+  }
+  V[bidx(g, i, ny, k)] = (T)bc.V_top[i];
   V[bidx(g, i, 1, k)] = (T)0;
+  if (k <= nz) {
+    W[bidx(g, i, nyg, k)] = (T)bc.W_top[i];
+    W[bidx(g, i, 1, k)] = X::wall_w(g, bc, W[bidx(g, i, 2, X::ks_w(g, k))], i, k);
+  }
 }
 
 template <typename T>
 __global__ void k_bc_mass(Geo g, T *__restrict__ U, const Scalars *__restrict__ sc) {
-  // :240-260: the correction k_bc_x's last block left in sc->dU
+  // :240-260: the correction the last x-plane block of k_bc_all left in sc->dU
   const double s_du = sc->dU;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -1248,12 +1315,16 @@ int bc_x_parts(const Geo &g) { return ((g.nyg + 31) / 32) * ((g.nzg + 7) / 8); }
 template <typename T>
 void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
                Scalars *sc, double rkt, double *qx_part, double qy, double length_y, cudaStream_t st) {
-  dim3 b(32, 8);
-  dim3 gx((g.nyg + 31) / 32, (g.nzg + 7) / 8);
-  k_bc_x<T><<<gx, b, 0, st>>>(g, bc, U, V, W, Uo, Vo, Wo, sc, rkt, qx_part, qy, length_y);
-  k_bc_z<T><<<dim3((g.nxg + 31) / 32, (g.nyg + 7) / 8), b, 0, st>>>(g, U, V, W);
-  k_bc_y<T><<<dim3((g.nxg + 31) / 32, (g.nzg + 7) / 8), b, 0, st>>>(g, bc, U, V, W);
-  k_bc_mass<T><<<gx, b, 0, st>>>(g, U, sc);
+  BcGrid G;
+  G.x_tiles = (g.nyg + 31) / 32;
+  G.nx_blocks = G.x_tiles * ((g.nzg + 7) / 8);  // = bc_x_parts(g)
+  G.zi_tiles = (g.nxg - 3 + 31) / 32;           // interior columns i = 2..nxg-2
+  G.nz_blocks = G.zi_tiles * ((g.nyg - 2 + 7) / 8);
+  G.yi_tiles = G.zi_tiles;
+  G.ny_blocks = G.yi_tiles * ((g.nzg + 7) / 8);
+  k_bc_all<T><<<G.nx_blocks + G.nz_blocks + G.ny_blocks, 256, 0, st>>>(g, bc, G, U, V, W, Uo, Vo, Wo, sc, rkt,
+                                                                         qx_part, qy, length_y);
+  k_bc_mass<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), dim3(32, 8), 0, st>>>(g, U, sc);
 }
 
 template <typename T>
