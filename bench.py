@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-les", action="store_true")
     ap.add_argument("--no-cufft", action="store_true")
+    ap.add_argument("--no-transition", action="store_true")
+    ap.add_argument("--ts-steps", type=int, default=2000)
     ap.add_argument("--ens-boxes", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--profile", default=None, choices=["mixed", "fp64", "ensemble"],
@@ -341,6 +343,32 @@ def run_cufft(args, case, dev):
     return out
 
 
+def run_transition(args, dev):
+    """Tollmien-Schlichting transition on the 1024 x 129 x 128 box (400 x 20 x 40
+    delta*, Re_delta* = 1000 at the inflow): a 2-D TS wave at omega = 0.1
+    (amplitude 1e-3) and an oblique pair (1e-4, seeded phases) from the
+    Orr-Sommerfeld solve, forced through the reference-format mode file, 2000
+    steps at a fixed dt of 1/400 forcing period (CFL 0.4 on the x spacing);
+    the spatial growth rate of the wave envelope, mixed against FP64."""
+    import tempfile
+    import blgpu
+    from blgpu import files, transition
+    lz = 40.0
+    beta = 2.0 * np.pi / lz  # the box's spanwise wavenumber closest to 0.2
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "ts_modes.dat")
+        info = transition.ts_mode_file(path, beta=beta)
+        c = transition.transition_case(nx=1024, ny=129, nz=128, lx=400.0, ly=20.0, lz=lz)
+        modes = files.read_temporal_modes(path, c.y)
+    out = {"grid": [1024, 129, 128], "steps": args.ts_steps, "beta": beta, "os": info}
+    t0 = time.perf_counter()
+    g64, _, _ = transition.run_growth(c, modes, blgpu.FP64, steps=args.ts_steps, device=dev, x_fit=(20.0, 90.0))
+    g32, _, _ = transition.run_growth(c, modes, blgpu.MIXED, steps=args.ts_steps, device=dev, x_fit=(20.0, 90.0))
+    out.update({"growth_fp64": g64, "growth_mixed": g32, "rel_diff": abs(g32 - g64) / abs(g64),
+                "wall_s": round(time.perf_counter() - t0, 1)})
+    return out
+
+
 def run_profile(args):
     """Small driver for ncu: set-up and warm-up outside the profiled range."""
     import torch
@@ -504,6 +532,9 @@ def main():
     ens = None
     if not args.no_ensemble:
         ens = run_ensemble(args, dev, pg, local, world)
+    ts = None
+    if world == 1 and not args.no_transition:
+        ts = run_transition(args, dev)
     les = None
     if world == 1 and not args.no_les:
         les = run_les(args, dev)
@@ -522,7 +553,7 @@ def main():
                                                   % (smix_bytes(case, 4) / 1e6),
                            "replicas_per_gpu": 1},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk, "ensemble": ens, "les_mixed": les, "cufft_path": cufft,
+                "clocks": clk, "ensemble": ens, "les_mixed": les, "cufft_path": cufft, "transition": ts,
                 "phases_ms_per_step_mixed": {k: round(v[0] / 2.0, 4) for k, v in ph.items()},
                 "phases_ms_per_step_fp64": ({k: round(v[0], 4) for k, v in ph64.items()} if fp64 else None),
                 "eager_step_ms_mixed": step_ms,
