@@ -105,3 +105,62 @@ def run_cf(case, mode, net=None, jh=3, steps=40, precision=MIXED, device=0):
             cfs.append(mean_cf(s.wall_stress()[0]) if mode else resolved_cf(s))
     s.close()
     return float(np.mean(cfs))
+
+
+def row_at(case, h):
+    """1-based centre row whose yg is closest to h (delta99 units)"""
+    yg = cases.centres_ghost(case.y)
+    return int(np.argmin(np.abs(yg[1:-1] - h))) + 2
+
+
+def config2_training(net, holdout, h=0.1, spinup=300, snaps=12, every=25, held=2, precision=MIXED, device=0,
+                     **case_kw):
+    """Training data from the turbulent DNS recipe (814 x 257 x 193 by default:
+    composite mean profile with the equilibrium law's log layer, 10 % U_inf
+    divergence-free noise, Lund inflow), run `spinup` steps past the noisy
+    initial field and then sampled every `every` steps: `snaps` snapshots of
+    every wall point of the row at h = 0.1 delta go to `net`'s training set,
+    the `held` snapshots after them to `holdout` (never trained on), together
+    with the equilibrium model's stress at the same row on those states.
+    Returns a dict: jh, steps run, samples, and the held-out equilibrium
+    stresses tau_eq (flattened in the sample order)."""
+    case = cases.turbulent_case(noise=0.10, **LOG_LAW, **case_kw)
+    cases.project_initial(case, device=device)
+    s = cases.solver_for(case, precision=precision, device=device)
+    jh = row_at(case, h)
+    s.advance(spinup)
+    n0 = net.num_samples
+    for _ in range(snaps):
+        s.advance(every)
+        net.sample(s, jh)
+    tau_eq = []
+    for _ in range(held):
+        s.advance(every)
+        holdout.sample(s, jh)
+        s.set_wall_model(1, jh)  # the equilibrium law on this state (no step taken)
+        tau_eq.append(s.wall_stress()[0].ravel())
+        s.set_wall_model(0, jh)
+    s.close()
+    return dict(jh=jh, h=float(cases.centres_ghost(case.y)[jh - 1]), steps=spinup + (snaps + held) * every,
+                samples=net.num_samples - n0, held_samples=holdout.num_samples, tau_eq=np.concatenate(tau_eq),
+                grid=(case.nx, case.ny, case.nz))
+
+
+def holdout_errors(net, holdout, tau_eq):
+    """The network and the equilibrium model against the resolved wall stress
+    of the held-out states: rms pointwise error, mean Cf and their errors."""
+    X, T = holdout.data()
+    tau = T[:, 0].astype(np.float64) / 1000.0
+    tau_net = net.forward(X)[:, 0].astype(np.float64) / 1000.0
+    rms = lambda a: float(np.sqrt(np.mean((a - tau) ** 2)))
+    cf, cf_net, cf_eq = mean_cf(tau), mean_cf(tau_net), mean_cf(tau_eq)
+    return dict(cf_dns=cf, cf_net=cf_net, cf_eq=cf_eq, rms_net=rms(tau_net), rms_eq=rms(tau_eq),
+                cf_err_net=abs(cf_net / cf - 1.0), cf_err_eq=abs(cf_eq / cf - 1.0))
+
+
+def config4_case(retheta=2000.0, nx=512, ny=96, nz=256, seed=5):
+    """The wall-modelled LES grid of the closure's judge: 512 x 96 x 256 over
+    64 x 2 x 16 delta99, nearly uniform y (dy = delta/48), so h = 0.1 delta is
+    the fifth or sixth row and the first cell centre sits at y+ ~ 7 (Re_theta
+    2000), far from resolving the wall gradient."""
+    return wmles_case(retheta=retheta, nx=nx, ny=ny, nz=nz, seed=seed)

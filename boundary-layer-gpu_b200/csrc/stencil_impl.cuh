@@ -20,6 +20,9 @@ namespace blgpu {
 // the FP32 path multiplies by the reciprocal table instead.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double qdiv(double a, double b, double) { return a / b; }
+// maximum that keeps a NaN (fmax drops it): check_divergence of a field that
+// holds a NaN reads NaN
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (a > b || a != a) ? a : b; }
 __device__ __forceinline__ float qdiv(float a, float, float rb) { return a * rb; }
 
 template <typename T> struct Ld {
@@ -1087,10 +1090,12 @@ __global__ void __launch_bounds__(256) k_maxdiv(Geo g, const T *__restrict__ U, 
       long long c = bidx(g, i, j, k);
       double d = ((double)U[c] - (double)U[c - 1]) / g.ax.F[i] + ((double)V[c] - (double)V[c - g.px]) / g.ay.F[j] +
                  ((double)W[c] - (double)W[c - g.plane]) / g.az.F[k];
-      mx = fmax(mx, fabs(d));
+      mx = max_keep_nan(mx, fabs(d));
     }
   }
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  for (int o = 16; o > 0; o >>= 1) mx = max_keep_nan(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  // |d| >= 0 and a positive NaN's bit pattern is above +Inf's, so the largest
+  // pattern is the maximum and a NaN anywhere wins
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
 }
 

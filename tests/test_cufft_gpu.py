@@ -27,22 +27,25 @@ def noisy(nx, ny, nz, seed=0, amp=1e-2, **kw):
 
 @pytest.mark.parametrize("grid", [(26, 14, 11), (60, 17, 15), (37, 9, 24), (131, 33, 24)])
 def test_cufft_projection_fp64(gpu, grid):
-    """One projection: rhs_p and the projected fields within 1e-12 of the
-    oracle and of the native kernels."""
+    """Boundary pass, projection, boundary pass (the substep's order): rhs_p
+    and the projected fields within 1e-12 of the oracle and of the native
+    kernels, and the field divergence free to 1e-12."""
     c = noisy(*grid, seed=4)
     out = {}
     for name, po in (("cufft", POISSON_CUFFT), ("native", POISSON_NATIVE)):
         s = cases.solver_for(c, poisson=po)
         s.set_dt(0.01)
+        s.apply_boundary_conditions(2)
         s.compute_projection_step(2)
-        out[name] = (s.rhs_p(),) + tuple(s.download_state()[:3])
-        div = s.check_divergence()
+        out[name] = (s.rhs_p()[:, :, :-1],) + tuple(s.download_state()[:3])
+        s.apply_boundary_conditions(2)
+        assert s.check_divergence() < 1e-12
         s.close()
-        assert div < 1e-11
     o = oracle.oracle_for(c)
     o.set_dt(0.01)
+    o.apply_bc(2)
     o.projection(2)
-    ref = (o.rhs_p(),) + tuple(o.state()[:3])
+    ref = (o.rhs_p()[:, :, :-1],) + tuple(o.state()[:3])
     for a, b, r in zip(out["cufft"], out["native"], ref):
         assert rel(a, r) < 1e-12, rel(a, r)
         assert rel(a, b) < 1e-12, rel(a, b)
@@ -58,7 +61,9 @@ def test_cufft_steps_fp64(gpu):
     o.advance(10)
     U, V, W, P, t = s.download_state()
     Ur, Vr, Wr, Pr, tr = o.state()
-    assert rel(U, Ur) < 1e-10 and rel(V, Vr) < 1e-10 and rel(W, Wr) < 1e-10
+    # W stays at round-off size in this z-independent flow: compared absolutely
+    assert rel(U, Ur) < 1e-10 and rel(V, Vr) < 1e-10 and np.abs(W - Wr).max() < 1e-12
+    assert rel(P, Pr) < 1e-8
     assert s.check_divergence() <= 1e-12
     s.close()
 
@@ -67,7 +72,9 @@ def test_cufft_mixed_turbulent(gpu):
     """Mixed form with C2C plans on a turbulent box with Lund inflow: within
     the mixed form's tolerance of the FP64 oracle after 5 steps, and of the
     native mixed path."""
-    c = cases.turbulent_case(nx=130, ny=33, nz=34, lx=16.0, ly=2.0, lz=3.0, seed=11)
+    # fixed dt: on this coarse y grid the CFL dt of compute_dt (the viscous
+    # limit, time_integration.f90:546-575) would be far above the convective one
+    c = cases.turbulent_case(nx=130, ny=33, nz=34, lx=16.0, ly=2.0, lz=3.0, seed=11, cfl=-0.01)
     res = {}
     for po in (POISSON_CUFFT, POISSON_NATIVE):
         s = cases.solver_for(c, precision=MIXED, poisson=po)
