@@ -148,6 +148,7 @@ _SIGS = {
     "blgpu_snapshot_name": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "blgpu_output_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "blgpu_read_input_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "blgpu_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "blgpu_read_temporal_modes_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ModesInfo)]),
     "blgpu_read_temporal_modes": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int] + [c_double_p] * 7),
 }

@@ -265,6 +265,11 @@ class Solver:
         return int(self.lib.blgpu_kernel_launches(self.ctx))
 
     # -- wall model ----------------------------------------------------------
+    def set_wait_limit(self, polls):
+        """Test hook: mbarrier polls of the tiled y-solve before a copy counts
+        as lost (< 0: the built-in limit)."""
+        self._ck(self.lib.blgpu_set_wait_limit(self.ctx, int(polls)))
+
     def set_wall_model(self, mode, jh=3, net=None):
         """0 no-slip, 1 law of the wall at row jh, 2 the WallNet `net` at row jh."""
         self._wall_net = net  # the solver reads the network's device weights every substep

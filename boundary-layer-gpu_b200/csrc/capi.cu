@@ -67,6 +67,7 @@ struct blgpu_ctx {
   ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
   CufftPath *cf = nullptr;    // poisson = BLGPU_POISSON_CUFFT: plans and work arrays
   int cf_status = 0;          // first failing cufftExec status of an enqueued step (0: none)
+  int wait_limit = -1;        // mbarrier polls of the tiled y-solve (< 0: built-in), a test hook
   bool have_tmaps = false;
   int nsm = 148;
   Scalars *sc = nullptr;
@@ -188,6 +189,10 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
+  if (f) {  // reported once: the next call starts clean
+    const int z = 0;
+    CK(cudaMemcpy(&ctx->sc->err, &z, sizeof z, cudaMemcpyHostToDevice));
+  }
   if (f & 32) return set_err(ctx, BLGPU_EDEVICE, "an uploaded state held a NaN or an infinity");
   if (f & 2) return set_err(ctx, BLGPU_EDEVICE, "z transform: a TMA copy did not complete within the wait limit");
   if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
@@ -1053,7 +1058,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   const bool tiled = ctx->have_tmaps && (ctx->tiles.thomas == 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
   if (tiled)
     launch_thomas_tile<T>(s, ctx->tmaps, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
-                          &ctx->sc->err, ctx->st);
+                          &ctx->sc->err, ctx->wait_limit, ctx->st);
   else
     launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
                      ctx->st);
@@ -1371,6 +1376,13 @@ int blgpu_max_divergence(blgpu_ctx *ctx, double *max_div) {
   double v;
   memcpy(&v, &bits, sizeof v);
   *max_div = v;
+  return BLGPU_OK;
+}
+
+int blgpu_set_wait_limit(blgpu_ctx *ctx, int polls) {
+  if (!ctx) return set_err(ctx, BLGPU_EINVAL, "null ctx");
+  ctx->wait_limit = polls < 0 ? -1 : polls;
+  drop_graphs(ctx);  // the limit is a kernel argument of the captured steps
   return BLGPU_OK;
 }
 

@@ -186,10 +186,11 @@ struct ThomasMaps {  // CUtensorMap bytes of C and of the pivots
 // k_thomas then serves the box)
 template <typename T>
 bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out);
-// err: device flag, bit 4 set when a tile copy missed its wait limit
+// err: device flag, bit 4 set when a tile copy missed its wait limit;
+// wait_limit: mbarrier polls before giving up (< 0: the built-in limit)
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
-                        int klow, int *err, cudaStream_t st);
+                        int klow, int *err, int wait_limit, cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);

@@ -1207,6 +1207,9 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
   int w = (int)((budget > fixed ? budget - fixed : 0) / line);
   if (w < 1) w = 1;
   if (w > cap) w = cap;
+  // the whole allocation (with the reciprocal spacings and the mbarriers)
+  // within the 227 KB a CTA may hold
+  while (w > 1 && dct_smem_bytes(n, elem_bytes, w, split) > 227 * 1024) --w;
   return w;
 }
 

@@ -49,7 +49,8 @@ template <typename T>
 __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUtensorMap mapC,
                                                     const __grid_constant__ CUtensorMap mapP, Spec s,
                                                     const double *__restrict__ dl, const double *__restrict__ du,
-                                                    double *__restrict__ H0, int klow, int *__restrict__ err) {
+                                                    double *__restrict__ H0, int klow, int *__restrict__ err,
+                                                    int wait_limit) {
   constexpr int MT = ThomasTile<T>::MT;
   typedef T2t<T> V2;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -73,11 +74,14 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
     dus[b] = du[b];
   }
   __syncwarp();
-  const bool ok = mbar_wait(bar, 0);
+  // wait_limit polls (the context's test hook may shorten it); after giving
+  // up, the drain waits with the normal limit, so no copy into this CTA's
+  // shared memory is in flight when it leaves
+  const bool ok = mbar_wait(bar, 0, wait_limit);
   if (!__all_sync(0xffffffffu, ok)) {
     if (lane == 0) {
       atomicOr(err, 4);
-      mbar_wait(bar, 0);  // let the copies finish (bounded) before leaving
+      mbar_wait(bar, 0);
     }
     return;
   }
@@ -190,7 +194,7 @@ bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out) {
 
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
-                        int klow, int *err, cudaStream_t st) {
+                        int klow, int *err, int wait_limit, cudaStream_t st) {
   constexpr int MT = ThomasTile<T>::MT;
   const size_t sm = thomas_tile_smem<T>(s.NM);
   cudaFuncSetAttribute(k_thomas_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -198,14 +202,14 @@ void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl,
   memcpy(&mc, maps.c, sizeof mc);
   memcpy(&mp, maps.p, sizeof mp);
   dim3 grid((s.N + MT - 1) / MT, s.MH);
-  k_thomas_tile<T><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err);
+  k_thomas_tile<T><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wait_limit < 0 ? WAIT_LIMIT : wait_limit);
 }
 
 template bool thomas_maps<float>(const Spec &, void *, double *, ThomasMaps *);
 template bool thomas_maps<double>(const Spec &, void *, double *, ThomasMaps *);
 template void launch_thomas_tile<float>(const Spec &, const ThomasMaps &, const double *, const double *, double *,
-                                        int, int *, cudaStream_t);
+                                        int, int *, int, cudaStream_t);
 template void launch_thomas_tile<double>(const Spec &, const ThomasMaps &, const double *, const double *, double *,
-                                         int, int *, cudaStream_t);
+                                         int, int *, int, cudaStream_t);
 
 }  // namespace blgpu

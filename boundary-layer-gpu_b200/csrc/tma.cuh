@@ -34,9 +34,10 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait for phase `parity`; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < WAIT_LIMIT; ++it) {
+// bounded wait for phase `parity`: at most `limit` polls; false when the
+// limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit = WAIT_LIMIT) {
+  for (int it = 0; it < limit; ++it) {
     if (mbar_test(bar, parity)) return true;
     if (it >= 32) __nanosleep(64);
   }

@@ -219,6 +219,15 @@ int blgpu_law_of_wall(blgpu_ctx *ctx, double *utau, int *iters_max);
  * stream; *ms = device time of the nsteps (graph captured beforehand) */
 int blgpu_advance_timed(blgpu_ctx *ctx, int nsteps, double *ms);
 
+/* Test hook of the failure path, no counterpart in the reference: the
+ * number of mbarrier polls the tiled y-solve's CTAs make before a tile copy
+ * counts as lost (polls < 0 restores the built-in limit of 2^24).  A wait
+ * that gives up sets bit 4 of the device flag; the CTA still waits, with the
+ * built-in limit, for its copy to land before it leaves, and the next
+ * blgpu_sync / blgpu_advance_timed reports BLGPU_EDEVICE (once; the flag is
+ * cleared when reported).  The state of such a step is not valid. */
+int blgpu_set_wait_limit(blgpu_ctx *ctx, int polls);
+
 /* number of kernels this context has launched (graph replays included) */
 long long blgpu_kernel_launches(const blgpu_ctx *ctx);
 

@@ -48,3 +48,32 @@ def test_streamed_upload_reports_non_finite_at_sync(gpu):
     with pytest.raises(BlgpuError, match="NaN or an infinity"):
         s.sync()
     s.close()
+
+
+def test_y_solve_wait_limit_reports_and_recovers(gpu):
+    """The tiled y-solve's mbarrier wait given zero polls: every tile's wait
+    gives up at once, the CTAs drain their copies (normal limit) and leave,
+    the step reports BLGPU_EDEVICE through the device flag; with the limit
+    restored and the state uploaded again the context steps exactly as a
+    fresh one."""
+    c = _case()
+    c.cfl = -1e-3
+    s = cases.solver_for(c, precision=FP64)
+    assert s.tiles()["thomas"] in (0, 2)
+    s.set_tiles(thomas=2)
+    s.set_wait_limit(0)
+    s.time_step()
+    with pytest.raises(BlgpuError, match="y-solve"):
+        s.sync()
+    s.sync()  # reported once
+    s.set_wait_limit(-1)
+    s.upload_state(c.U, c.V, c.W)
+    s.set_dt(1e-3)
+    s.advance(2)
+    r = cases.solver_for(c, precision=FP64)
+    r.set_tiles(thomas=2)
+    r.advance(2)
+    for a, b in zip(s.download_state()[:3], r.download_state()[:3]):
+        assert np.array_equal(a, b)
+    s.close()
+    r.close()
