@@ -113,8 +113,8 @@ def row_at(case, h):
     return int(np.argmin(np.abs(yg[1:-1] - h))) + 2
 
 
-def config2_training(net, holdout, h=0.1, spinup=300, snaps=12, every=25, held=2, precision=MIXED, device=0,
-                     **case_kw):
+def config2_training(net, holdout, h=0.1, spinup=300, snaps=12, every=25, held=2, dt=0.012, precision=MIXED,
+                     device=0, **case_kw):
     """Training data from the turbulent DNS recipe (814 x 257 x 193 by default:
     composite mean profile with the equilibrium law's log layer, 10 % U_inf
     divergence-free noise, Lund inflow), run `spinup` steps past the noisy
@@ -122,9 +122,13 @@ def config2_training(net, holdout, h=0.1, spinup=300, snaps=12, every=25, held=2
     every wall point of the row at h = 0.1 delta go to `net`'s training set,
     the `held` snapshots after them to `holdout` (never trained on), together
     with the equilibrium model's stress at the same row on those states.
+    The steps use a fixed dt (delta99 / U_inf units): compute_dt's CFL mode
+    takes the largest spacing/|u| (time_integration.f90:546-558), so at
+    CFL 0.5 its dt is the viscous limit and this noisy field breaks up after
+    about 130 steps; 0.012 keeps the convective CFL below about 0.5.
     Returns a dict: jh, steps run, samples, and the held-out equilibrium
     stresses tau_eq (flattened in the sample order)."""
-    case = cases.turbulent_case(noise=0.10, **LOG_LAW, **case_kw)
+    case = cases.turbulent_case(noise=0.10, cfl=-dt, **LOG_LAW, **case_kw)
     cases.project_initial(case, device=device)
     s = cases.solver_for(case, precision=precision, device=device)
     jh = row_at(case, h)
@@ -158,9 +162,13 @@ def holdout_errors(net, holdout, tau_eq):
                 cf_err_net=abs(cf_net / cf - 1.0), cf_err_eq=abs(cf_eq / cf - 1.0))
 
 
-def config4_case(retheta=2000.0, nx=512, ny=96, nz=256, seed=5):
+def config4_case(retheta=2000.0, nx=512, ny=96, nz=256, seed=5, dt=0.04):
     """The wall-modelled LES grid of the closure's judge: 512 x 96 x 256 over
     64 x 2 x 16 delta99, nearly uniform y (dy = delta/48), so h = 0.1 delta is
-    the fifth or sixth row and the first cell centre sits at y+ ~ 7 (Re_theta
-    2000), far from resolving the wall gradient."""
-    return wmles_case(retheta=retheta, nx=nx, ny=ny, nz=nz, seed=seed)
+    the sixth row and the first cell centre sits at y+ ~ 7 (Re_theta 2000),
+    far from resolving the wall gradient.  Fixed dt = 0.04 delta99/U_inf
+    (convective CFL about 0.35 in x): compute_dt's CFL mode would take the
+    viscous limit, about 4 on this grid."""
+    c = wmles_case(retheta=retheta, nx=nx, ny=ny, nz=nz, seed=seed)
+    c.cfl = -dt
+    return c
