@@ -1055,12 +1055,8 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
-  const bool rcp = ctx->tmaps.have_rc && ctx->tiles.thomas == 3;
-  const bool tiled = !rcp && ctx->have_tmaps && (ctx->tiles.thomas == 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
-  if (rcp)
-    launch_thomas_rc<T>(s, ctx->tmaps, sp, sp + s.NM, sp + 2 * s.NM, sp + 3 * s.NM, sp + 3 * s.NM + s.N,
-                        mixed ? ctx->kz0h : nullptr, ctx->klow, &ctx->sc->err, ctx->wait_limit, ctx->st);
-  else if (tiled)
+  const bool tiled = ctx->have_tmaps && (ctx->tiles.thomas == 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
+  if (tiled)
     launch_thomas_tile<T>(s, ctx->tmaps, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
                           &ctx->sc->err, ctx->wait_limit, ctx->st);
   else
@@ -1686,9 +1682,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   }
   if (t.zdft < 0 || t.zdft > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1,2,3}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
-  if (t.thomas < 0 || t.thomas > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2,3}", t.thomas);
-  if ((t.thomas == 2 && !ctx->have_tmaps) || (t.thomas == 3 && !ctx->tmaps.have_rc))
-    return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d needs TMA tiles (ny-1 <= 256)", t.thomas);
+  if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
   return BLGPU_OK;
 }
 
@@ -1804,7 +1798,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {4, 8},                                                                  // proj_by
       {1, 2, 3},                                                               // zdft
       {1, 2},                                                                  // rhs_pts
-      {1, 2, 3},                                                               // thomas
+      {1, 2},                                                                  // thomas
       {0, 4, 8, 12, 16},                                                       // idct_nw
       {1, 2}};                                                                 // xfft
   auto measure = [&](const Tiles &t, double *ms) -> int {

@@ -34,7 +34,6 @@
 
 #include "divergence.cuh"
 #include "kernels.cuh"
-#include "ysolve.cuh"
 
 namespace blgpu {
 
@@ -106,9 +105,9 @@ __global__ void __launch_bounds__(128) k_cf_thomas(Spec s, C2<T> *__restrict__ h
     const C2<T> c = h[b * hs];
     double rx = (double)c.x, ry = (double)c.y;
     if (b > 0) {
-      const double w = ys_w(dl[b], rprev);
-      rx = ys_fwd(rx, w, gx);
-      ry = ys_fwd(ry, w, gy);
+      const double w = dl[b] * rprev;
+      rx = rx - w * gx;
+      ry = ry - w * gy;
     }
     rprev = pv[b * ps];
     gx = rx;
@@ -135,11 +134,11 @@ __global__ void __launch_bounds__(128) k_cf_thomas(Spec s, C2<T> *__restrict__ h
     }
     const double p = pv[b * ps];
     if (b == NM - 1) {
-      xx = ys_top(cx, p);
-      xy = ys_top(cy, p);
+      xx = cx * p;
+      xy = cy * p;
     } else {
-      xx = ys_bwd(cx, du[b], xx, p);
-      xy = ys_bwd(cy, du[b], xy, p);
+      xx = (cx - du[b] * xx) * p;
+      xy = (cy - du[b] * xy) * p;
     }
     C2<T> o;
     if (kz0) {

@@ -25,8 +25,7 @@ struct Tiles {
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
   int rhs_pts;  // FP32 DNS RHS: x-points per thread, 1 or 2 (0: 2)
-  int thomas;   // y-solve: 1 register ring, 2 TMA tiles, 3 TMA tiles with pivots formed in the kernel
-                //   (2, 3 where the box allows; 0: tiles in FP64, ring in FP32)
+  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
   int xfft;     // FP32 x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N)
 };
@@ -182,8 +181,6 @@ int cufft_path_inverse_x(CufftPath *c, const Geo &g, const Spec &s, const void *
 struct ThomasMaps {  // CUtensorMap bytes of C and of the pivots
   alignas(64) unsigned char c[128];
   alignas(64) unsigned char p[128];
-  alignas(64) unsigned char rc[128];  // C in the tiles of the recomputing kernel
-  bool have_rc = false;
 };
 // false when the maps cannot be encoded or NM > 256 (the register-ring
 // k_thomas then serves the box)
@@ -194,12 +191,6 @@ bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out);
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
                         int klow, int *err, int wait_limit, cudaStream_t st);
-// the y-solve with the pivots formed in the kernel from dd, dl, du, kxx, kzz
-// (bit-identical to the pivot-table kernels; needs maps.have_rc)
-template <typename T>
-void launch_thomas_rc(const Spec &s, const ThomasMaps &maps, const double *dd, const double *dl, const double *du,
-                      const double *kxx, const double *kzz, double *H0, int klow, int *err, int wait_limit,
-                      cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);

@@ -19,7 +19,6 @@
 //               (projection.f90:295-303).
 #include "kernels.cuh"
 #include "divergence.cuh"
-#include "ysolve.cuh"
 #include "tma.cuh"
 
 namespace blgpu {
@@ -945,8 +944,13 @@ __global__ void k_thomas_factors(Spec s, double *__restrict__ piv, const double 
   const double kk = kxx[kx], kzv = kzz[kz];
   double rinv = 0.0;
   for (int b = 0; b < s.NM; ++b) {
-    const double d = ys_diag(dd[b], kk, kzv, kx == 0 && kz == 0 && b == 0);
-    rinv = b > 0 ? ys_piv(d, ys_w(dl[b], rinv), du[b - 1], false) : ys_piv(d, 0.0, 0.0, true);
+    double d = (dd[b] + kk) + kzv;
+    if (kx == 0 && kz == 0 && b == 0) d = 3.0 / 2.0 * d;
+    if (b > 0) {
+      const double w = dl[b] * rinv;
+      d = d - w * du[b - 1];
+    }
+    rinv = 1.0 / d;
     piv[base + b * rs] = rinv;
   }
 }
@@ -988,9 +992,9 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
         }
         double rx = (double)cv.x, ry = (double)cv.y;
         if (b > 0) {
-          const double w = ys_w(dl[b], rprev);  // l_b / d'_{b-1}
-          rx = ys_fwd(rx, w, gx);
-          ry = ys_fwd(ry, w, gy);
+          const double w = dl[b] * rprev;  // l_b / d'_{b-1}
+          rx = rx - w * gx;
+          ry = ry - w * gy;
         }
         rprev = pv;
         gx = rx;
@@ -1026,11 +1030,11 @@ __device__ __forceinline__ void thomas_sweeps(T2<T> *__restrict__ Cm, const doub
           pb -= rs;
         }
         if (b == top) {
-          xx = ys_top((double)cv.x, pv);
-          xy = ys_top((double)cv.y, pv);
+          xx = (double)cv.x * pv;
+          xy = (double)cv.y * pv;
         } else {
-          xx = ys_bwd((double)cv.x, du[b], xx, pv);
-          xy = ys_bwd((double)cv.y, du[b], xy, pv);
+          xx = ((double)cv.x - du[b] * xx) * pv;
+          xy = ((double)cv.y - du[b] * xy) * pv;
         }
         *cw = mk<T>((T)xx, (T)xy);
         cw -= rs;
@@ -1073,7 +1077,10 @@ __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, c
         const int b = b0 + u;
         if (b < NM) {
           double r = rv[u];
-          if (b > 0) r = ys_fwd(r, ys_w(dl[b], rprev), g);
+          if (b > 0) {
+            const double w = dl[b] * rprev;
+            r = r - w * g;
+          }
           rprev = pvv[u];
           g = r;
           Hd[(long long)b * klow] = r;
@@ -1093,7 +1100,7 @@ __global__ void __launch_bounds__(128) k_thomas(Spec s, T2<T> *__restrict__ C, c
       for (int u = 0; u < PB; ++u) {
         const int b = b0 - u;
         if (b >= 0) {
-          x = (b == NM - 1) ? ys_top(hv[u], pvv[u]) : ys_bwd(hv[u], du[b], x, pvv[u]);
+          x = (b == NM - 1) ? hv[u] * pvv[u] : (hv[u] - du[b] * x) * pvv[u];
           Hd[(long long)b * klow] = x;
         }
       }

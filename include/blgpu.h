@@ -254,8 +254,7 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * sums, 2 = mma.sync TF32 tensor cores, 3 = tcgen05 tensor cores with the
  * accumulators in tensor memory), rhs_pts (mixed-form DNS
  * RHS: x-points per thread, 1 or 2), thomas (y-solve: 1 = register ring,
- * 2 = TMA-fed tiles where ny-1 <= 256, 3 = TMA-fed tiles with the pivots
- * formed in the kernel, no pivot table read, ny-1 <= 256), idct_nw (lines per CTA of the
+ * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
  * in shared memory, any N; 2 = two-pass register FFT, built for
  * N = nx-2 = 812 (29 x 28), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9));
