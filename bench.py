@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-les", action="store_true")
     ap.add_argument("--no-cufft", action="store_true")
     ap.add_argument("--no-transition", action="store_true")
+    ap.add_argument("--no-closure", action="store_true")
+    ap.add_argument("--les-steps", type=int, default=200)
     ap.add_argument("--ts-steps", type=int, default=2000)
     ap.add_argument("--ens-boxes", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
@@ -369,6 +371,33 @@ def run_transition(args, dev):
     return out
 
 
+def run_closure(args, dev):
+    """The learned wall-stress closure: trained on the turbulent DNS recipe's
+    own wall samples (814 x 257 x 193, 12 snapshots of the row at h = 0.1
+    delta99 after 300 steps, 2 more held out), judged on the held-out states
+    against the resolved wall stress beside the equilibrium law of the wall,
+    then both as the wall condition of the 512 x 96 x 256 wall-modelled LES."""
+    from blgpu import wallmodel, WallNet
+    t0 = time.perf_counter()
+    net, hold = WallNet(seed=11), WallNet(seed=12)
+    info = wallmodel.config2_training(net, hold, device=dev)
+    l0 = net.eval()
+    wallmodel.train(net)
+    l1 = net.eval()
+    e = wallmodel.holdout_errors(net, hold, info["tau_eq"])
+    c = wallmodel.config4_case()
+    jh = wallmodel.row_at(c, 0.1)
+    cf_eq = wallmodel.run_cf(c, 1, jh=jh, steps=args.les_steps, device=dev)
+    cf_net = wallmodel.run_cf(c, 2, net, jh=jh, steps=args.les_steps, device=dev)
+    r = lambda v: float("%.5g" % v)
+    return {"samples": info["samples"], "held_out": info["held_samples"], "dns_steps": info["steps"],
+            "h": r(info["h"]), "loss": [r(l0), r(l1)],
+            "held_out_cf": {"dns": r(e["cf_dns"]), "network": r(e["cf_net"]), "equilibrium": r(e["cf_eq"])},
+            "held_out_rms_tau": {"network": r(e["rms_net"]), "equilibrium": r(e["rms_eq"])},
+            "les_512x96x256_cf": {"equilibrium": r(cf_eq), "network": r(cf_net), "steps": args.les_steps},
+            "wall_s": round(time.perf_counter() - t0, 1)}
+
+
 def run_profile(args):
     """Small driver for ncu: set-up and warm-up outside the profiled range."""
     import torch
@@ -535,6 +564,9 @@ def main():
     ts = None
     if world == 1 and not args.no_transition:
         ts = run_transition(args, dev)
+    closure = None
+    if world == 1 and not args.no_closure:
+        closure = run_closure(args, dev)
     les = None
     if world == 1 and not args.no_les:
         les = run_les(args, dev)
@@ -553,7 +585,7 @@ def main():
                                                   % (smix_bytes(case, 4) / 1e6),
                            "replicas_per_gpu": 1},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk, "ensemble": ens, "les_mixed": les, "cufft_path": cufft, "transition": ts,
+                "clocks": clk, "ensemble": ens, "les_mixed": les, "cufft_path": cufft, "transition": ts, "closure": closure,
                 "phases_ms_per_step_mixed": {k: round(v[0] / 2.0, 4) for k, v in ph.items()},
                 "phases_ms_per_step_fp64": ({k: round(v[0], 4) for k, v in ph64.items()} if fp64 else None),
                 "eager_step_ms_mixed": step_ms,
