@@ -284,11 +284,11 @@ class Solver:
 
     # -- launch shapes -----------------------------------------------------
     TILE_NAMES = ("rhs_kc", "rhs_by", "dct_nw", "dftz_rk", "proj_by", "zdft", "rhs_pts", "thomas", "idct_nw",
-                  "xfft", "xrad")
+                  "xfft")
 
     def tiles(self):
-        t = (ctypes.c_int * 11)()
-        self._ck(self.lib.blgpu_get_tiles(self.ctx, t, 11))
+        t = (ctypes.c_int * 10)()
+        self._ck(self.lib.blgpu_get_tiles(self.ctx, t, 10))
         return dict(zip(self.TILE_NAMES, list(t)))
 
     def set_tiles(self, **kw):
@@ -297,8 +297,8 @@ class Solver:
             if k not in cur:
                 raise KeyError(k)
             cur[k] = int(v)
-        t = (ctypes.c_int * 11)(*[cur[k] for k in self.TILE_NAMES])
-        self._ck(self.lib.blgpu_set_tiles(self.ctx, t, 11))
+        t = (ctypes.c_int * 10)(*[cur[k] for k in self.TILE_NAMES])
+        self._ck(self.lib.blgpu_set_tiles(self.ctx, t, 10))
 
     def autotune(self, steps=3):
         """Choose the launch shapes by timing; returns (ms/step before, after)."""

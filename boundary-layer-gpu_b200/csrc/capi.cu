@@ -1042,8 +1042,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
     return;
   }
   ph_begin(ctx, PH_DIVDCT);
-  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->tiles.xfft,
-                    ctx->tiles.xrad, ctx->st);
+  launch_div_dct<T>(ctx->geo, s, pl, S[0], S[1], S[2], (T *)ctx->R, ctx->tiles.dct_nw, ctx->tiles.xfft, ctx->st);
   ph_end(ctx, 1);
   // z transforms: tcgen05 (zdft 0 or 3), mma.sync TF32 (0 without tcgen05, or 2), FP32/FP64 sums (1)
   const int zd = ctx->tiles.zdft;
@@ -1073,7 +1072,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);
   launch_idct<T>(ctx->geo, s, pl, (const T *)ctx->R, (T *)ctx->rhs_p, ctx->tiles.idct_nw, ctx->tiles.xfft,
-                 ctx->tiles.xrad, &ctx->sc->err, ctx->st);
+                 &ctx->sc->err, ctx->st);
   ph_end(ctx, 1);
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_PROJECT);
@@ -1684,8 +1683,6 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   if (t.zdft < 0 || t.zdft > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1,2,3}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
   if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
-  if (t.xrad != 0 && t.xrad != 7 && t.xrad != 13 && t.xrad != 19 && t.xrad != 29 && t.xrad != 31)
-    return set_err(ctx, BLGPU_EINVAL, "tiles: xrad %d not in {0,7,13,19,29,31}", t.xrad);
   return BLGPU_OK;
 }
 
@@ -1748,7 +1745,7 @@ static int time_steps(blgpu_ctx *ctx, int steps, double *ms) {
 extern "C" {
 
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
-  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 11 values");
+  if (!ctx || !tiles || n < 5) return set_err(ctx, BLGPU_EINVAL, "blgpu_set_tiles: need 5 to 10 values");
   Tiles t{tiles[0],
           tiles[1],
           tiles[2],
@@ -1758,8 +1755,7 @@ int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n) {
           n >= 7 ? tiles[6] : ctx->tiles.rhs_pts,
           n >= 8 ? tiles[7] : ctx->tiles.thomas,
           n >= 9 ? tiles[8] : ctx->tiles.idct_nw,
-          n >= 10 ? tiles[9] : ctx->tiles.xfft,
-          n >= 11 ? tiles[10] : ctx->tiles.xrad};
+          n >= 10 ? tiles[9] : ctx->tiles.xfft};
   int rc = tiles_check(ctx, t);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->cfg.device));
@@ -1782,7 +1778,6 @@ int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n) {
   if (n >= 8) tiles[7] = t.thomas;
   if (n >= 9) tiles[8] = t.idct_nw;
   if (n >= 10) tiles[9] = t.xfft;
-  if (n >= 11) tiles[10] = t.xrad;
   return BLGPU_OK;
 }
 
@@ -1805,8 +1800,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {1, 2},                                                                  // rhs_pts
       {1, 2},                                                                  // thomas
       {0, 4, 8, 12, 16},                                                       // idct_nw
-      {1, 2},                                                                  // xfft
-      {7, 13, 19, 29}};                                                        // xrad
+      {1, 2}};                                                                 // xfft
   auto measure = [&](const Tiles &t, double *ms) -> int {
     int r = snap_restore(ctx, sn);
     if (r) return r;
@@ -1823,16 +1817,15 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   double best_ms = 0;
   rc = measure(best, &best_ms);
   const double def_ms = best_ms;
-  for (int knob = 0; knob < 11 && !rc; ++knob) {  // one pass of coordinate descent
+  for (int knob = 0; knob < 10 && !rc; ++knob) {  // one pass of coordinate descent
     if (knob == 5 && !ctx->zfrag && !ctx->utab) continue;  // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
     if (knob == 9 && (ctx->fp64 || !xfft_split(ctx->spec.N))) continue;  // one x-transform kernel
-    if (knob == 10 && !ctx->fp64 && xfft_split(ctx->spec.N) && best.xfft != 1) continue;  // two-pass: no radix classes
     for (int v : cand[knob]) {
       Tiles t = best;
-      int *f[11] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,
-                    &t.idct_nw, &t.xfft, &t.xrad};
+      int *f[10] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,
+                    &t.idct_nw, &t.xfft};
       if (*f[knob] == v) continue;
       *f[knob] = v;
       if (tiles_check(ctx, t)) continue;

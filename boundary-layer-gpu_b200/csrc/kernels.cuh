@@ -28,8 +28,6 @@ struct Tiles {
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
   int xfft;     // FP32 x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N)
-  int xrad;     // Stockham x transforms: largest radix with a register butterfly, 7/13/19/29/31; larger
-                //   radices take the shared-memory summation path (0: 7 in FP64, every radix up to 31 in FP32)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)
@@ -123,7 +121,7 @@ struct Spec {  // spectral layout of the Poisson solve
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    int nw, int xfft, int xrad, cudaStream_t st);
+                    int nw, int xfft, cudaStream_t st);
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
                   int rk, cudaStream_t st);
@@ -198,8 +196,8 @@ void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const d
                            const double *kxx, const double *kzz, cudaStream_t st);
 template <typename T>
 // err: device flag, bit 16 set when a row copy of the two-pass kernel missed its wait limit
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, int xfft, int xrad,
-                 int *err, cudaStream_t st);
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, int xfft, int *err,
+                 cudaStream_t st);
 // shared memory of a DCT CTA of `lines` warps; split: that of xfft_split, 0 for the Stockham kernels
 size_t dct_smem_bytes(int n, int elem_bytes, int lines, int split);
 // the split A of N = A B served by the two-pass FP32 x transforms, 0 if none

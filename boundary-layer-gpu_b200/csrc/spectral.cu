@@ -1226,17 +1226,10 @@ size_t dct_smem_bytes(int n, int elem_bytes, int warps, int split) {
 // kernel to that of the largest radix compiled in, so the transform kernels
 // are instantiated per largest radix class; radices above the class (and
 // primes above 31) take the shared-memory summation path.
-// the register-class cap of the Stockham x transforms: tiles value, or the
-// built-in 7 in FP64 (no cap in FP32)
-template <typename T> static int xrad_cap(int xrad) { return xrad > 0 ? xrad : (sizeof(T) == 8 ? 7 : 0); }
-
-// cap (0: none): the largest register class to use; radices above it take the
-// shared-memory summation path (FP64 butterflies of radix 19 and up hold
-// 200-255 registers, which leaves eight warps per SM)
-static int radix_class(const int *rad, int nst, int cap) {
+static int radix_class(const int *rad, int nst) {
   int mx = 2;
   for (int i = 0; i < nst; ++i)
-    if (rad[i] <= 31 && (cap <= 0 || rad[i] <= cap)) mx = rad[i] > mx ? rad[i] : mx;
+    if (rad[i] <= 31) mx = rad[i] > mx ? rad[i] : mx;
   if (mx <= 7) return 7;
   if (mx <= 13) return 13;
   if (mx <= 19) return 19;
@@ -1262,7 +1255,7 @@ static void launch_idct_e(const Geo &g, const Spec &s, const FftPlan<T> &pl, con
 
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
-                    int nw_req, int xfft, int xrad, cudaStream_t st) {
+                    int nw_req, int xfft, cudaStream_t st) {
   const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
@@ -1274,7 +1267,7 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
     if (split == 19) return launch_div_dct_e<T, TwoPassX<19, 10>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
     if (split == 14) return launch_div_dct_e<T, TwoPassX<14, 9>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
   }
-  switch (radix_class(pl.rad, pl.nst, xrad_cap<T>(xrad))) {
+  switch (radix_class(pl.rad, pl.nst)) {
     case 7: launch_div_dct_e<T, StockhamX<T, 7>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
     case 13: launch_div_dct_e<T, StockhamX<T, 13>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
     case 19: launch_div_dct_e<T, StockhamX<T, 19>>(g, s, pl, U, V, W, R, nw, sm, grid, st); break;
@@ -1297,8 +1290,8 @@ static bool idct2_fits(const Spec &s, int split) {
 }
 
 template <typename T>
-void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft, int xrad,
-                 int *err, cudaStream_t st) {
+void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft, int *err,
+                 cudaStream_t st) {
   const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
@@ -1315,7 +1308,7 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
     if (split == 19) return launch_idct_e<T, TwoPassX<19, 10>>(g, s, pl, R, p, nw, sm, grid, st);
     if (split == 14) return launch_idct_e<T, TwoPassX<14, 9>>(g, s, pl, R, p, nw, sm, grid, st);
   }
-  switch (radix_class(pl.rad, pl.nst, xrad_cap<T>(xrad))) {
+  switch (radix_class(pl.rad, pl.nst)) {
     case 7: launch_idct_e<T, StockhamX<T, 7>>(g, s, pl, R, p, nw, sm, grid, st); break;
     case 13: launch_idct_e<T, StockhamX<T, 13>>(g, s, pl, R, p, nw, sm, grid, st); break;
     case 19: launch_idct_e<T, StockhamX<T, 19>>(g, s, pl, R, p, nw, sm, grid, st); break;
@@ -1372,9 +1365,9 @@ void launch_kz0_idct(const Spec &s, const double *H0, int klow, const double *cm
 
 #define BLGPU_SPEC_INST(T)                                                                                        \
   template void launch_div_dct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, const T *, const T *, \
-                                  T *, int, int, int, cudaStream_t);                                              \
-  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, int, int,     \
-                               int *, cudaStream_t);                                                             \
+                                  T *, int, int, cudaStream_t);                                                   \
+  template void launch_idct<T>(const Geo &, const Spec &, const FftPlan<T> &, const T *, T *, int, int, int *,   \
+                               cudaStream_t);                                                                    \
   template void launch_dft_z<T>(const Spec &, const T *, T2<T> *, const T2<T> *, int, int, cudaStream_t);        \
   template void launch_thomas<T>(const Spec &, T2<T> *, const double *, const double *, const double *,          \
                                  double *, int, cudaStream_t);

@@ -246,7 +246,7 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
                                    void *stream);
 
 /* ---- launch shapes and the autotuner ----
- * tiles[5 to 11] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS
+ * tiles[5 to 10] = rhs_kc (k-planes per CTA of the RHS kernel), rhs_by (RHS
  * block 32 x rhs_by), dct_nw (complex lines per CTA of the forward DCT, up
  * to 16 in the mixed form (8 with the two-pass x transforms) and 8 in FP64),
  * dftz_rk (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection
@@ -257,14 +257,10 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
  * in shared memory, any N; 2 = two-pass register FFT, built for
- * N = nx-2 = 812 (29 x 28), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9)),
- * xrad (Stockham x transforms, FP64 and FP32 Stockham: the largest radix
- * with a register butterfly, 7, 13, 19, 29 or 31; larger radices are summed
- * from shared memory; built-in 7 in FP64, every radix up to 31 in FP32);
+ * N = nx-2 = 812 (29 x 28), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9));
  * 0 = the built-in choice.
- * Values not passed keep their current setting.  All but zdft, rhs_pts,
- * xfft and xrad leave results unchanged; those change them at rounding
- * level (FP32 or FP64).  No counterpart in the
+ * Values not passed keep their current setting.  All but zdft, rhs_pts and
+ * xfft leave results unchanged; those change them at FP32 rounding level.  No counterpart in the
  * reference (its OpenACC loops take compiler-chosen gangs). */
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n);
 int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n);
