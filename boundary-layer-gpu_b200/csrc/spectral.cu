@@ -463,6 +463,90 @@ template <int A, int B> struct TwoPassX {
 // the real lines q and q+1 (q = b*M + k').  R[q][kx] receives
 // c_k = sum_i f_i cos(pi k (2i+1) / (2N)).
 // ---------------------------------------------------------------------------
+// Divergence of the real lines q and q+1 (q = b*M + k') into the complex line
+// buffer in the DCT's reordered positions (point i at i/2 when even, at
+// N-1-i/2 when odd), FP32, four consecutive points per lane with 16-byte
+// loads (the box rows start 16-byte aligned at i = 2); U at i-1 of the first
+// point comes from the previous lane, or from the previous round for lane 0.
+// rfx: the FP32 reciprocal x spacings of the points, N rounded up to 4.
+__device__ __forceinline__ void div_pair_vec(const Geo &g, const Spec &s, const float *__restrict__ U,
+                                             const float *__restrict__ V, const float *__restrict__ W,
+                                             const float *rfx, float2 *bufA, int q, int lane) {
+  const int N = s.N, N4 = (N + 3) & ~3;
+  const int nlines = s.NM * s.M;
+  const bool hb = q + 1 < nlines;
+  const int ba = q / s.M, ka = q - ba * s.M;
+  const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
+  const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
+  // line B aliases line A when it does not exist, so every load is valid
+  const long long cbb = hb ? cb : ca;
+  const int jb = hb ? bb + 2 : ba + 2, kbb = hb ? kb + 2 : ka + 2;
+  const float ryA = (float)g.ay.rF[ba + 2], rzA = (float)g.az.rF[ka + 2];
+  const float ryB = (float)g.ay.rF[jb], rzB = (float)g.az.rF[kbb];
+  float carA = __ldg(U + ca - 1), carB = __ldg(U + cbb - 1);
+  for (int base = 0; base < N; base += 128) {
+    const int i4 = base + 4 * lane, ic = i4 < N4 ? i4 : N4 - 4;  // in-row address for idle lanes
+    const float4 rx = *reinterpret_cast<const float4 *>(rfx + ic);
+    float fa[4], fb[4];
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const long long c = (l ? cbb : ca) + ic;
+      const float4 u = __ldg(reinterpret_cast<const float4 *>(U + c));
+      const float4 v = __ldg(reinterpret_cast<const float4 *>(V + c));
+      const float4 vm = __ldg(reinterpret_cast<const float4 *>(V + c - g.px));
+      const float4 w = __ldg(reinterpret_cast<const float4 *>(W + c));
+      const float4 wm = __ldg(reinterpret_cast<const float4 *>(W + c - g.plane));
+      float um0 = __shfl_up_sync(0xffffffffu, u.w, 1);
+      const float car = l ? carB : carA;
+      if (lane == 0) um0 = car;
+      const float nc = __shfl_sync(0xffffffffu, u.w, 31);
+      if (l) carB = nc;
+      else carA = nc;
+      const float ry = l ? ryB : ryA, rz = l ? rzB : rzA;
+      float *f = l ? fb : fa;
+      // projection.f90:42-44, as div_at
+      f[0] = (u.x - um0) * rx.x + (v.x - vm.x) * ry + (w.x - wm.x) * rz;
+      f[1] = (u.y - u.x) * rx.y + (v.y - vm.y) * ry + (w.y - wm.y) * rz;
+      f[2] = (u.z - u.y) * rx.z + (v.z - vm.z) * ry + (w.z - wm.z) * rz;
+      f[3] = (u.w - u.z) * rx.w + (v.w - vm.w) * ry + (w.w - wm.w) * rz;
+    }
+    if (!hb) fb[0] = fb[1] = fb[2] = fb[3] = 0.f;
+    if (i4 + 3 < N && (N & 1) == 0) {
+      // points i4, i4+2 go to the adjacent slots i4/2, i4/2+1; points
+      // i4+3, i4+1 to N-2-i4/2, N-1-i4/2
+      float *b = reinterpret_cast<float *>(bufA);
+      *reinterpret_cast<float4 *>(b + i4) = make_float4(fa[0], fb[0], fa[2], fb[2]);
+      *reinterpret_cast<float4 *>(b + 2 * (N - 2 - i4 / 2)) = make_float4(fa[3], fb[3], fa[1], fb[1]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int ip = i4 + e;
+        if (ip < N) {
+          const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
+          bufA[pos] = make_float2(fa[e], fb[e]);
+        }
+      }
+    }
+  }
+}
+
+// The DCT coefficients of the two lines from their packed transform res:
+// V_A = (Z_k + conj Z_{N-k})/2, V_B = (Z_k - conj Z_{N-k})/(2i), c = Re(e^{-i pi k/2N} V)
+template <typename T>
+__device__ __forceinline__ void dct_pair_out(const T2<T> *res, const T2<T> *post, T *ra, int rx, int N, bool hb,
+                                             int lane) {
+  T *rb = ra + rx;
+  for (int k = lane; k < N; k += 32) {
+    const T2<T> z = res[k];
+    const T2<T> zr = res[k == 0 ? 0 : N - k];
+    const T2<T> p = post[k];
+    const T vax = (T)0.5 * (z.x + zr.x), vay = (T)0.5 * (z.y - zr.y);
+    const T vbx = (T)0.5 * (z.y + zr.y), vby = (T)0.5 * (zr.x - z.x);
+    ra[k] = p.x * vax - p.y * vay;
+    if (hb) rb[k] = p.x * vbx - p.y * vby;
+  }
+}
+
 // FP32 CTAs take up to 16 lines (one CTA fills an SM's shared memory); the
 // FP64 kernels need more registers per thread and stop at 8
 template <typename T> struct DctCta { static constexpr int max_threads = sizeof(T) == 4 ? 512 : 256; };
@@ -499,58 +583,7 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_div_dct(Geo g
                    ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(W)) &
                     15) == 0 && (g.px & 3) == 0;
   if constexpr (sizeof(T) == 4) {
-    if (vec) {
-      // four consecutive points per lane, 16-byte loads (the box rows start
-      // 16-byte aligned at i = 2); U at i-1 of the first point comes from the
-      // previous lane, or from the previous round for lane 0
-      const float ryA = (float)g.ay.rF[ba + 2], rzA = (float)g.az.rF[ka + 2];
-      const float ryB = (float)g.ay.rF[jb], rzB = (float)g.az.rF[kbb];
-      float carA = __ldg(U + ca - 1), carB = __ldg(U + cbb - 1);
-      for (int base = 0; base < N; base += 128) {
-        const int i4 = base + 4 * lane, ic = i4 < N4 ? i4 : N4 - 4;  // in-row address for idle lanes
-        const float4 rx = *reinterpret_cast<const float4 *>(rfx + ic);
-        float fa[4], fb[4];
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-          const long long c = (l ? cbb : ca) + ic;
-          const float4 u = __ldg(reinterpret_cast<const float4 *>(U + c));
-          const float4 v = __ldg(reinterpret_cast<const float4 *>(V + c));
-          const float4 vm = __ldg(reinterpret_cast<const float4 *>(V + c - g.px));
-          const float4 w = __ldg(reinterpret_cast<const float4 *>(W + c));
-          const float4 wm = __ldg(reinterpret_cast<const float4 *>(W + c - g.plane));
-          float um0 = __shfl_up_sync(0xffffffffu, u.w, 1);
-          const float car = l ? carB : carA;
-          if (lane == 0) um0 = car;
-          const float nc = __shfl_sync(0xffffffffu, u.w, 31);
-          if (l) carB = nc;
-          else carA = nc;
-          const float ry = l ? ryB : ryA, rz = l ? rzB : rzA;
-          float *f = l ? fb : fa;
-          // projection.f90:42-44, as div_at
-          f[0] = (u.x - um0) * rx.x + (v.x - vm.x) * ry + (w.x - wm.x) * rz;
-          f[1] = (u.y - u.x) * rx.y + (v.y - vm.y) * ry + (w.y - wm.y) * rz;
-          f[2] = (u.z - u.y) * rx.z + (v.z - vm.z) * ry + (w.z - wm.z) * rz;
-          f[3] = (u.w - u.z) * rx.w + (v.w - vm.w) * ry + (w.w - wm.w) * rz;
-        }
-        if (!hb) fb[0] = fb[1] = fb[2] = fb[3] = 0.f;
-        if (i4 + 3 < N && (N & 1) == 0) {
-          // points i4, i4+2 go to the adjacent slots i4/2, i4/2+1; points
-          // i4+3, i4+1 to N-2-i4/2, N-1-i4/2
-          float *b = reinterpret_cast<float *>(bufA);
-          *reinterpret_cast<float4 *>(b + i4) = make_float4(fa[0], fb[0], fa[2], fb[2]);
-          *reinterpret_cast<float4 *>(b + 2 * (N - 2 - i4 / 2)) = make_float4(fa[3], fb[3], fa[1], fb[1]);
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int ip = i4 + e;
-            if (ip < N) {
-              const int pos = (ip & 1) ? (N - 1 - (ip >> 1)) : (ip >> 1);
-              bufA[pos] = mk<T>(fa[e], fb[e]);
-            }
-          }
-        }
-      }
-    }
+    if (vec) div_pair_vec(g, s, U, V, W, rfx, bufA, q, lane);
   }
   // batches of 4 points per lane: all 48 loads issued before any use
   for (int base = 0; base < N && !vec; base += 128) {
@@ -573,18 +606,7 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_div_dct(Geo g
   }
   __syncwarp();
   const T2<T> *res = E::template run<false>(bufA, pl, tw, lane);
-  T *ra = R + (long long)q * s.rx;
-  T *rb = ra + s.rx;
-  for (int k = lane; k < N; k += 32) {
-    const T2<T> z = res[k];
-    const T2<T> zr = res[k == 0 ? 0 : N - k];
-    // V_A = (Z_k + conj Z_{N-k})/2, V_B = (Z_k - conj Z_{N-k})/(2i), c = Re(e^{-i pi k/2N} V)
-    const T2<T> p = post[k];
-    const T vax = (T)0.5 * (z.x + zr.x), vay = (T)0.5 * (z.y - zr.y);
-    const T vbx = (T)0.5 * (z.y + zr.y), vby = (T)0.5 * (zr.x - z.x);
-    ra[k] = p.x * vax - p.y * vay;
-    if (hb) rb[k] = p.x * vbx - p.y * vby;
-  }
+  dct_pair_out<T>(res, post, R + (long long)q * s.rx, s.rx, N, hb, lane);
 }
 
 // ---------------------------------------------------------------------------
