@@ -553,7 +553,7 @@ def main():
                    "host arrays, copies overlapping the steps), wall clock to the final blgpu_sync"}
     smix.close()
     cufft = None
-    if not args.no_cufft:
+    if world == 1 and not args.no_cufft:
         cufft = run_cufft(args, case, dev)
         keep = ("div_dct", "dft_z", "thomas", "idft_z", "idct", "project")
         cufft["native_poisson_ms_per_step"] = {"mixed": round(sum(ph[k][0] for k in keep) / 2.0, 4),
