@@ -65,9 +65,11 @@ struct blgpu_ctx {
   uint32_t *utab = nullptr;   // mixed form: tcgen05 z transforms, tables (or null)
   ZdftMaps umaps{};           // and their TMA maps
   ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
+  RhsMaps rmaps[4]{};         // TMA maps of U, V, W of each state buffer and of F1 (mixed form)
+  bool have_rmaps = false;
   CufftPath *cf = nullptr;    // poisson = BLGPU_POISSON_CUFFT: plans and work arrays
   int cf_status = 0;          // first failing cufftExec status of an enqueued step (0: none)
-  int wait_limit = -1;        // mbarrier polls of the tiled y-solve (< 0: built-in), a test hook
+  int wait_limit = -1;        // mbarrier polls of the tiled y-solve and the TMA-fed RHS (< 0: built-in), a test hook
   bool have_tmaps = false;
   int nsm = 148;
   Scalars *sc = nullptr;
@@ -185,7 +187,8 @@ static int dalloc(blgpu_ctx *ctx, void **p, size_t bytes) {
 // bit 2: a TMA copy of the tensor-core z transform missed its wait limit;
 // bit 4: one of the tiled y-solve; bit 8: one of the tcgen05 z transform;
 // bit 16: a row copy of the two-pass inverse x transform; bit 32: a streamed
-// upload (blgpu_upload_state_async) held a NaN or an infinity
+// upload (blgpu_upload_state_async) held a NaN or an infinity; bit 64: a
+// plane copy of the TMA-fed RHS
 static int device_flag(blgpu_ctx *ctx) {
   int f = 0;
   CK(cudaMemcpy(&f, &ctx->sc->err, sizeof f, cudaMemcpyDeviceToHost));
@@ -198,6 +201,7 @@ static int device_flag(blgpu_ctx *ctx) {
   if (f & 4) return set_err(ctx, BLGPU_EDEVICE, "y-solve: a TMA tile copy did not complete within the wait limit");
   if (f & 8) return set_err(ctx, BLGPU_EDEVICE, "z transform (tcgen05): a copy or a product missed its wait limit");
   if (f & 16) return set_err(ctx, BLGPU_EDEVICE, "inverse x transform: a row copy did not complete within the wait limit");
+  if (f & 64) return set_err(ctx, BLGPU_EDEVICE, "RHS: a plane copy did not complete within the wait limit");
   if (f) return set_err(ctx, BLGPU_EDEVICE, "device flag %d set by a step kernel", f);
   return BLGPU_OK;
 }
@@ -272,6 +276,16 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   for (int b = 0; b < 3; ++b)
     for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->S[b][q], box));
   for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->F1[q], box));
+  if (!ctx->fp64) {  // plane maps of the TMA-fed RHS: each state buffer and F1
+    const Geo gb = ctx->geo_box();
+    ctx->have_rmaps = true;
+    for (int b = 0; b < 3; ++b)
+      if (!rhs_maps(gb, (const float *)ctx->S[b][0], (const float *)ctx->S[b][1], (const float *)ctx->S[b][2],
+                    &ctx->rmaps[b]))
+        ctx->have_rmaps = false;
+    if (!rhs_maps(gb, (const float *)ctx->F1[0], (const float *)ctx->F1[1], (const float *)ctx->F1[2], &ctx->rmaps[3]))
+      ctx->have_rmaps = false;
+  }
   TRY(dalloc(ctx, &ctx->P, box));
   TRY(dalloc(ctx, &ctx->rhs_p, box));
   if (cfg->les_model) TRY(dalloc(ctx, &ctx->nut, box));
@@ -1091,7 +1105,9 @@ static void enq_rhs(blgpu_ctx *ctx, int mode, int in, int o, int outb, double c1
   const MetT<T> &m = *reinterpret_cast<const MetT<T> *>(ctx->fp64 ? (const void *)&ctx->m64 : (const void *)&ctx->m32);
   ph_begin(ctx, PH_RHS);
   launch_rhs_rk<T>(ctx->geo, m, mode, ctx->cfg.les_model != 0, Si[0], Si[1], Si[2], (const T *)ctx->nut, So[0], So[1],
-                   So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->tiles, ctx->st);
+                   So[2], F[0], F[1], F[2], Sn[0], Sn[1], Sn[2], ctx->sc, c1, c2, ctx->tiles,
+                   ctx->have_rmaps ? &ctx->rmaps[in] : nullptr, ctx->have_rmaps ? &ctx->rmaps[o] : nullptr,
+                   ctx->have_rmaps ? &ctx->rmaps[3] : nullptr, &ctx->sc->err, ctx->wait_limit, ctx->st);
   ph_end(ctx, 1);
 }
 
@@ -1681,7 +1697,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
     }
   }
   if (t.zdft < 0 || t.zdft > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1,2,3}", t.zdft);
-  if (t.rhs_pts < 0 || t.rhs_pts > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,1,2}", t.rhs_pts);
+  if (t.rhs_pts < 0 || t.rhs_pts > 4) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,...,4}", t.rhs_pts);
   if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
   return BLGPU_OK;
 }
@@ -1797,7 +1813,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {4, 8},                                                                  // dftz_rk
       {4, 8},                                                                  // proj_by
       {1, 2, 3},                                                               // zdft
-      {1, 2},                                                                  // rhs_pts
+      {1, 2, 4},                                                               // rhs_pts
       {1, 2},                                                                  // thomas
       {0, 4, 8, 12, 16},                                                       // idct_nw
       {1, 2}};                                                                 // xfft

@@ -11,7 +11,10 @@
 //   k_bc_*        apply_boundary_conditions_gpu (boundary_conditions.f90:127-262)
 //   k_dt_*        compute_dt (time_integration.f90:528-591)
 //   k_maxdiv      check_divergence (projection.f90:391-413)
+#include <cstring>
+
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace blgpu {
 
@@ -556,6 +559,424 @@ __global__ void __launch_bounds__(256) k_rhs_rk_pair(Geo g, MetT<T> m, const T *
     ut = ut2; vt = vt2; vst = vst2; wt = wt2;
     oU = oU2; oV = oV2; oW = oW2; fU = fU2; fV = fV2; fW = fW2;
   }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 DNS form with the two x-points of a thread packed: every operation on
+// the pair (point i0 in .x, i0+1 in .y) is one FP32x2 instruction of sm_100
+// (__fadd2_rn, __fmul2_rn, __ffma2_rn), each with its rounding written out,
+// so a carried k-1 face term and one formed afresh at the first plane of a
+// chunk round alike.  Loads, shared face fluxes, carried terms and the
+// one-plane-ahead fetches are those of k_rhs_rk_pair; the x-shifted pairs
+// (i0-1, i0) and (i0+1, i0+2) are assembled from the pair and the scalar
+// neighbours.  The terms are those of rhs_*_at, grouped for fused
+// multiply-adds: a*x - b*y as fma(a, x, -b*y).
+// ---------------------------------------------------------------------------
+namespace pk {
+typedef float2 f2;
+__device__ __forceinline__ f2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ f2 sp(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 neg(f2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ f2 add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub(f2 a, f2 b) { return __fadd2_rn(a, neg(b)); }
+__device__ __forceinline__ f2 mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 lin(f2 a, f2 x, f2 b, f2 y) { return fma(a, x, mul(b, y)); }       // a x + b y
+__device__ __forceinline__ f2 dif(f2 a, f2 x, f2 b, f2 y) { return fma(a, x, mul(neg(b), y)); }  // a x - b y
+__device__ __forceinline__ f2 ld(const float *__restrict__ p, long long c) {
+  return __ldg(reinterpret_cast<const float2 *>(p + c));
+}
+// the carried terms, formed by one expression whether carried or fresh
+__device__ __forceinline__ f2 fxz(f2 H, f2 u0, f2 u1, f2 w0, f2 w1) { return mul(mul(H, add(u0, u1)), mul(H, add(w0, w1))); }
+__device__ __forceinline__ f2 fyz(f2 H, f2 W0, f2 W1, f2 v0, f2 v1, f2 w, f2 wn) {
+  return mul(mul(H, add(v0, v1)), lin(W0, w, W1, wn));
+}
+__device__ __forceinline__ void st(float *__restrict__ p, long long c, f2 f, bool sa, bool sb) {
+  if (sb) *reinterpret_cast<f2 *>(p + c) = f;
+  else if (sa) p[c] = f.x;
+}
+template <int MODE>
+__device__ __forceinline__ void rk(float *__restrict__ F1, float *__restrict__ Un, long long c, f2 f, f2 o, f2 f1,
+                                   f2 CDT1, f2 TDT, f2 TC1, f2 TC2, bool sa, bool sb) {
+  if (MODE == 0) {
+    st(F1, c, f, sa, sb);
+  } else if (MODE == 1) {
+    st(F1, c, f, sa, sb);
+    st(Un, c, fma(CDT1, f, o), sa, sb);
+  } else {
+    st(Un, c, fma(TDT, fma(TC1, f1, mul(TC2, f)), o), sa, sb);
+  }
+}
+}  // namespace pk
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 2) k_rhs_rk_pk(Geo g, MetT<float> m, const float *__restrict__ U,
+                                                   const float *__restrict__ V, const float *__restrict__ W,
+                                                   const float *__restrict__ Uo, const float *__restrict__ Vo,
+                                                   const float *__restrict__ Wo, float *__restrict__ F1u,
+                                                   float *__restrict__ F1v, float *__restrict__ F1w,
+                                                   float *__restrict__ Un, float *__restrict__ Vn,
+                                                   float *__restrict__ Wn, const Scalars *__restrict__ sc, double c1,
+                                                   double c2, int kchunk) {
+  using namespace pk;
+  const int i0 = 2 + 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (i0 > g.nx || j > g.ny) return;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  if (k0 > k1) return;
+  const long long px = g.px, pl = g.plane;
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  const f2 CDT1 = sp((float)(dt * c1)), TDT = sp((float)dt), TC1 = sp((float)c1), TC2 = sp((float)c2);
+  const int ib = i0 + 1;
+  const bool su_a = i0 <= g.nx - 1, su_b = ib <= g.nx - 1;
+  const bool sv_a = true, sv_b = ib <= g.nx;
+  const bool dv = (j <= g.ny - 1);
+  const bool zu_a = (i0 == g.nx - 1), zu_b = (ib == g.nx - 1);
+  const bool zx_a = (i0 == g.nx), zx_b = (ib == g.nx);
+  const f2 H = sp(0.5f);
+  const f2 XRC_P = mk(m.xrC[i0], m.xrC[ib]), XRF_P = mk(m.xrF[i0], m.xrF[ib]);
+  const f2 XRF_R = mk(m.xrF[ib], m.xrF[i0 + 2]), XRC_L = mk(m.xrC[i0 - 1], m.xrC[i0]);
+  const f2 YRF = sp(m.yrF[j]), YRC = sp(m.yrC[j]), YRCM = sp(m.yrC[j - 1]), YRFP = sp(m.yrF[j + 1]);
+  const f2 W0 = sp(m.w0[j]), W1 = sp(m.w1[j]), W0M = sp(m.w0[j - 1]), W1M = sp(m.w1[j - 1]);
+  const f2 NU = sp(m.nu), DPDX = sp(m.dpdx), DPDZ = sp(m.dpdz);
+  long long c = bidx(g, i0, j, k0);
+  // window at k0 (pairs P, scalar neighbours i0-1 and i0+2)
+  float um = __ldg(U + c - 1), up = __ldg(U + c + 2);
+  float vm = __ldg(V + c - 1), vp = __ldg(V + c + 2);
+  float wm = __ldg(W + c - 1), wp = __ldg(W + c + 2);
+  f2 uP = ld(U, c), vP = ld(V, c), wP = ld(W, c);
+  float unm = __ldg(U + c + px - 1), utm = __ldg(U + c + pl - 1);
+  f2 unP = ld(U, c + px), utP = ld(U, c + pl), usP = ld(U, c - px);
+  f2 vnP = ld(V, c + px), vtP = ld(V, c + pl), vstP = ld(V, c - px + pl), vsP = ld(V, c - px);
+  float vs_p = __ldg(V + c - px + 2);
+  f2 wnP = ld(W, c + px), wsP = ld(W, c - px), wtP = ld(W, c + pl);
+  f2 FxzB, FyzB, dUz, dVz, dWz, WbA;
+  {
+    const f2 ubP = ld(U, c - pl), vbP = ld(V, c - pl), wbP = ld(W, c - pl), wnbP = ld(W, c + px - pl);
+    const float wb_p = __ldg(W + c + 2 - pl);
+    FxzB = fxz(H, ubP, uP, wbP, mk(wbP.y, wb_p));
+    FyzB = fyz(H, W0, W1, vbP, vP, wbP, wnbP);
+    dUz = sub(uP, ubP);
+    dVz = sub(vP, vbP);
+    dWz = sub(wP, wbP);
+    WbA = mul(H, add(wbP, wP));
+  }
+  f2 oU{}, oV{}, oW{}, fU{}, fV{}, fW{};
+  if (MODE != 0 && MODE != 1) { fU = ld(F1u, c); fV = ld(F1v, c); fW = ld(F1w, c); }
+  if (MODE != 0) { oU = ld(Uo, c); oV = ld(Vo, c); oW = ld(Wo, c); }
+  for (int k = k0;; ++k) {
+    const bool more = k < k1;
+    float utm2 = 0.f;
+    f2 utP2{}, vtP2{}, vstP2{}, wtP2{}, oU2{}, oV2{}, oW2{}, fU2{}, fV2{}, fW2{};
+    if (more) {
+      const long long c2p = c + 2 * pl, c1p = c + pl;
+      utm2 = __ldg(U + c2p - 1);
+      utP2 = ld(U, c2p);
+      vtP2 = ld(V, c2p);
+      vstP2 = ld(V, c2p - px);
+      wtP2 = ld(W, c2p);
+      if (MODE != 0) { oU2 = ld(Uo, c1p); oV2 = ld(Vo, c1p); oW2 = ld(Wo, c1p); }
+      if (MODE != 0 && MODE != 1) { fU2 = ld(F1u, c1p); fV2 = ld(F1v, c1p); fW2 = ld(F1w, c1p); }
+    }
+    const f2 ZRF = sp(m.zrF[k]), ZRC = sp(m.zrC[k]), ZRCM = sp(m.zrC[k - 1]), ZRFP = sp(m.zrF[k + 1]);
+    // x-shifted pairs
+    const f2 uL = mk(um, uP.x), uR = mk(uP.y, up);
+    const f2 vL = mk(vm, vP.x), vR = mk(vP.y, vp);
+    const f2 wL = mk(wm, wP.x), wR = mk(wP.y, wp);
+    // shared face fluxes of this plane
+    const f2 XL = mul(H, add(uL, uP)), XR = mul(H, add(uP, uR));
+    const f2 FxyP = mul(lin(W0, uP, W1, unP), mul(H, add(vP, vR)));
+    const f2 FxyL = mul(lin(W0, uL, W1, mk(unm, unP.x)), mul(H, add(vL, vP)));
+    const f2 FxzP = fxz(H, uP, utP, wP, wR);
+    const f2 FxzL = fxz(H, uL, mk(utm, utP.x), wL, wP);
+    const f2 FyzP = fyz(H, W0, W1, vP, vtP, wP, wnP);
+    const f2 dUt = sub(utP, uP), dVt = sub(vtP, vP), dWt = sub(wtP, wP);
+    const f2 WtA = mul(H, add(wP, wtP));
+    // u
+    {
+      const f2 ax = mul(dif(XR, XR, XL, XL), XRC_P);
+      const f2 ay = mul(sub(FxyP, mul(lin(W0M, usP, W1M, uP), mul(H, add(vsP, mk(vsP.y, vs_p))))), YRF);
+      const f2 az = mul(sub(FxzP, FxzB), ZRF);
+      const f2 vx = mul(dif(XRF_R, sub(uR, uP), XRF_P, sub(uP, uL)), XRC_P);
+      const f2 vy = mul(dif(sub(unP, uP), YRC, sub(uP, usP), YRCM), YRF);
+      const f2 vz = mul(dif(ZRC, dUt, ZRCM, dUz), ZRF);
+      f2 f = fma(NU, add(add(vx, vy), vz), sub(DPDX, add(add(ax, ay), az)));
+      if (zu_a) f.x = 0.f;
+      if (zu_b) f.y = 0.f;
+      rk<MODE>(F1u, Un, c, f, oU, fU, CDT1, TDT, TC1, TC2, su_a, su_b);
+    }
+    // v
+    if (dv) {
+      const f2 aa = mul(H, add(vP, vnP)), bb = mul(H, add(vsP, vP));
+      const f2 ay = mul(dif(aa, aa, bb, bb), YRC);
+      const f2 ax = mul(sub(FxyP, FxyL), XRF_P);
+      const f2 az = mul(sub(FyzP, FyzB), ZRF);
+      const f2 vx = mul(dif(XRC_P, sub(vR, vP), XRC_L, sub(vP, vL)), XRF_P);
+      const f2 vy = mul(dif(YRFP, sub(vnP, vP), YRF, sub(vP, vsP)), YRC);
+      const f2 vz = mul(dif(ZRC, dVt, ZRCM, dVz), ZRF);
+      f2 f = fma(NU, add(add(vx, vy), vz), neg(add(add(ay, ax), az)));
+      if (zx_a) f.x = 0.f;
+      if (zx_b) f.y = 0.f;
+      rk<MODE>(F1v, Vn, c, f, oV, fV, CDT1, TDT, TC1, TC2, sv_a, sv_b);
+    }
+    // w
+    if (k <= g.nz - 1) {
+      const f2 az = mul(dif(WtA, WtA, WbA, WbA), ZRC);
+      const f2 ax = mul(sub(FxzP, FxzL), XRF_P);
+      const f2 ay = mul(sub(FyzP, mul(mul(H, add(vsP, vstP)), lin(W0M, wsP, W1M, wP))), YRF);
+      const f2 vx = mul(dif(XRC_P, sub(wR, wP), XRC_L, sub(wP, wL)), XRF_P);
+      const f2 vy = mul(dif(sub(wnP, wP), YRC, sub(wP, wsP), YRCM), YRF);
+      const f2 vz = mul(dif(ZRFP, dWt, ZRF, dWz), ZRC);
+      f2 f = fma(NU, add(add(vx, vy), vz), sub(DPDZ, add(add(az, ax), ay)));
+      if (zx_a) f.x = 0.f;
+      if (zx_b) f.y = 0.f;
+      rk<MODE>(F1w, Wn, c, f, oW, fW, CDT1, TDT, TC1, TC2, sv_a, sv_b);
+    }
+    if (!more) break;
+    // carry the upper face terms down and slide the window to k+1
+    FxzB = FxzP;
+    FyzB = FyzP;
+    dUz = dUt; dVz = dVt; dWz = dWt; WbA = WtA;
+    c += pl;
+    um = utm; uP = utP; up = __ldg(U + c + 2);
+    vm = __ldg(V + c - 1); vP = vtP; vp = __ldg(V + c + 2);
+    wm = __ldg(W + c - 1); wP = wtP; wp = __ldg(W + c + 2);
+    vsP = vstP;
+    vs_p = __ldg(V + c - px + 2);
+    unm = __ldg(U + c + px - 1);
+    unP = ld(U, c + px);
+    usP = ld(U, c - px);
+    vnP = ld(V, c + px);
+    wnP = ld(W, c + px);
+    wsP = ld(W, c - px);
+    utm = utm2; utP = utP2; vtP = vtP2; vstP = vstP2; wtP = wtP2;
+    oU = oU2; oV = oV2; oW = oW2; fU = fU2; fV = fV2; fW = fW2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The packed FP32 DNS kernel fed by TMA.  A CTA of 32 x 8 threads owns 64
+// x-points (32 pairs) by 8 rows and walks a chunk of k-planes.  Plane p of
+// U, V and W reaches shared memory as one 72 x 10 x 1 tensor copy per field
+// (x from the CTA's first point - 4, rows j-1 .. j+8) and, for the planes the
+// CTA updates, the point-wise operands Uo, Vo, Wo (RK substeps) and F1
+// (substeps 2 and 3) as 64 x 8 x 1 copies.  A ring of 4 stages, each
+// completed on an mbarrier, holds plane p in stage (p - k0 + 1) mod 4: while
+// plane k is computed (from planes k and k+1), planes k+2 and k+3 are in
+// flight, and after a CTA barrier the stage of plane k takes plane k+4.  The
+// k loop is unrolled by the ring length, so every shared-memory operand sits
+// at a fixed offset from one per-thread base, and no global load sits on the
+// arithmetic's path.  Arithmetic and carried terms are those of k_rhs_rk_pk.
+// A wait that runs out of polls sets bit 64 of the device flag; the CTA then
+// stops at the next barrier and waits (bounded) for the copies it issued.
+// ---------------------------------------------------------------------------
+constexpr int RT_NS = 4, RT_TW = 72, RT_BY = 8, RT_TH = RT_BY + 2;
+constexpr int RT_FS = (RT_TH * RT_TW * 4 + 127) / 128 * 32;  // floats per field tile (a 128-byte multiple)
+constexpr int RT_PS = 64 * RT_BY;                            // floats per point-wise tile
+__host__ __device__ constexpr int rt_npw(int mode) { return mode == 0 ? 0 : mode == 1 ? 3 : 6; }
+__host__ __device__ constexpr int rt_stage(int mode) { return 3 * RT_FS + rt_npw(mode) * RT_PS; }  // floats
+__host__ __device__ constexpr size_t rt_smem(int mode) { return (size_t)RT_NS * rt_stage(mode) * 4 + RT_NS * 8 + 16; }
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * RT_BY, 2)
+    k_rhs_rk_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
+                 const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap mou,
+                 const __grid_constant__ CUtensorMap mov, const __grid_constant__ CUtensorMap mow,
+                 const __grid_constant__ CUtensorMap mfu, const __grid_constant__ CUtensorMap mfv,
+                 const __grid_constant__ CUtensorMap mfw, Geo g, MetT<float> m, float *__restrict__ F1u,
+                 float *__restrict__ F1v, float *__restrict__ F1w, float *__restrict__ Un, float *__restrict__ Vn,
+                 float *__restrict__ Wn, const Scalars *__restrict__ sc, double c1, double c2, int kchunk, int *err,
+                 int wait_limit) {
+  using namespace pk;
+  constexpr int NS = RT_NS, TW = RT_TW, NPW = rt_npw(MODE), SS = rt_stage(MODE);
+  constexpr uint32_t FIELD_BYTES = 3u * TW * RT_TH * 4u, PW_BYTES = (uint32_t)NPW * RT_PS * 4u;
+  extern __shared__ __align__(1024) float rt_sm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(rt_sm + NS * SS);
+  volatile int *bad = reinterpret_cast<volatile int *>(full + NS);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int istart = 2 + 64 * blockIdx.x, jstart = 2 + RT_BY * blockIdx.y;
+  const int i0 = istart + 2 * tx, j = jstart + ty;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  if (k0 > k1) return;  // whole CTA
+  const bool act = i0 <= g.nx && j <= g.ny;
+  const int jj = act ? j : jstart;  // metric row and column of idle threads: any valid one
+  const int ii = act ? i0 : istart;
+  if (tid == 0) {
+    // the copies need 128-byte aligned destinations
+    *bad = (tma::smem_u32(rt_sm) & 127u) ? 1 : 0;
+    for (int s = 0; s < NS; ++s) tma::mbar_init(&full[s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncthreads();
+  if (*bad) {
+    if (tid == 0) atomicOr(err, 64);
+    return;
+  }
+  auto issue = [&](int p) {  // thread 0: plane p into its stage
+    const int s = (p - k0 + 1) & (NS - 1);
+    float *st = rt_sm + s * SS;
+    const bool pw = NPW > 0 && p >= k0 && p <= k1;
+    tma::mbar_expect_tx(&full[s], FIELD_BYTES + (pw ? PW_BYTES : 0u));
+    tma::load_3d(st, &mu, istart - 2, jstart - 2, p - 1, &full[s]);
+    tma::load_3d(st + RT_FS, &mv, istart - 2, jstart - 2, p - 1, &full[s]);
+    tma::load_3d(st + 2 * RT_FS, &mw, istart - 2, jstart - 2, p - 1, &full[s]);
+    if (pw) {
+      float *pt = st + 3 * RT_FS;
+      tma::load_3d(pt, &mou, istart + 2, jstart - 1, p - 1, &full[s]);
+      tma::load_3d(pt + RT_PS, &mov, istart + 2, jstart - 1, p - 1, &full[s]);
+      tma::load_3d(pt + 2 * RT_PS, &mow, istart + 2, jstart - 1, p - 1, &full[s]);
+      if (NPW == 6) {
+        tma::load_3d(pt + 3 * RT_PS, &mfu, istart + 2, jstart - 1, p - 1, &full[s]);
+        tma::load_3d(pt + 4 * RT_PS, &mfv, istart + 2, jstart - 1, p - 1, &full[s]);
+        tma::load_3d(pt + 5 * RT_PS, &mfw, istart + 2, jstart - 1, p - 1, &full[s]);
+      }
+    }
+  };
+  int issued = k0 - 2;  // thread 0: last plane issued
+  if (tid == 0)
+    for (int p = k0 - 1; p <= min(k0 + 2, k1 + 1); ++p) {
+      issue(p);
+      issued = p;
+    }
+  auto wait_plane = [&](int p) {
+    if (!tma::mbar_wait(&full[(p - k0 + 1) & (NS - 1)], (uint32_t)(((p - k0 + 1) >> 2) & 1), wait_limit)) {
+      *bad = 1;
+      atomicOr(err, 64);
+    }
+  };
+  // per-thread offsets: field tiles at row j (tile row ty + 1), column of
+  // point i0; point-wise tiles at row ty, column 2 tx
+  const float *fo = rt_sm + (ty + 1) * TW + 4 + 2 * tx;
+  const float *po = rt_sm + 3 * RT_FS + ty * 64 + 2 * tx;
+#define RT_P2(S, q, dr) (*reinterpret_cast<const f2 *>(fo + (S) * SS + (q) * RT_FS + (dr) * TW))
+#define RT_S1(S, q, dr, dc) (fo[(S) * SS + (q) * RT_FS + (dr) * TW + (dc)])
+#define RT_PW(S, q) (*reinterpret_cast<const f2 *>(po + (S) * SS + (q) * RT_PS))
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  const f2 CDT1 = sp((float)(dt * c1)), TDT = sp((float)dt), TC1 = sp((float)c1), TC2 = sp((float)c2);
+  const int ib = i0 + 1;
+  const bool su_a = i0 <= g.nx - 1, su_b = ib <= g.nx - 1;
+  const bool sv_a = true, sv_b = ib <= g.nx;
+  const bool dv = (j <= g.ny - 1);
+  const bool zu_a = (i0 == g.nx - 1), zu_b = (ib == g.nx - 1);
+  const bool zx_a = (i0 == g.nx), zx_b = (ib == g.nx);
+  const f2 H = sp(0.5f);
+  const f2 XRC_P = mk(m.xrC[ii], m.xrC[ii + 1]), XRF_P = mk(m.xrF[ii], m.xrF[ii + 1]);
+  const f2 XRF_R = mk(m.xrF[ii + 1], m.xrF[ii + 2]), XRC_L = mk(m.xrC[ii - 1], m.xrC[ii]);
+  const f2 YRF = sp(m.yrF[jj]), YRC = sp(m.yrC[jj]), YRCM = sp(m.yrC[jj - 1]), YRFP = sp(m.yrF[jj + 1]);
+  const f2 W0 = sp(m.w0[jj]), W1 = sp(m.w1[jj]), W0M = sp(m.w0[jj - 1]), W1M = sp(m.w1[jj - 1]);
+  const f2 NU = sp(m.nu), DPDX = sp(m.dpdx), DPDZ = sp(m.dpdz);
+  long long c = bidx(g, ii, jj, k0);
+  // carried k-1 face terms from planes k0-1 (stage 0) and k0 (stage 1)
+  wait_plane(k0 - 1);
+  wait_plane(k0);
+  f2 FxzB, FyzB, dUz, dVz, dWz, WbA;
+  {
+    const f2 ubP = RT_P2(0, 0, 0), vbP = RT_P2(0, 1, 0), wbP = RT_P2(0, 2, 0), wnbP = RT_P2(0, 2, 1);
+    const f2 uP = RT_P2(1, 0, 0), vP = RT_P2(1, 1, 0), wP = RT_P2(1, 2, 0);
+    FxzB = fxz(H, ubP, uP, wbP, mk(wbP.y, RT_S1(0, 2, 0, 2)));
+    FyzB = fyz(H, W0, W1, vbP, vP, wbP, wnbP);
+    dUz = sub(uP, ubP);
+    dVz = sub(vP, vbP);
+    dWz = sub(wP, wbP);
+    WbA = mul(H, add(wbP, wP));
+  }
+  __syncthreads();  // plane k0-1 read by all: its stage takes plane k0+3
+  if (*bad) goto drain;
+  if (tid == 0 && k0 + 3 <= k1 + 1) {
+    issue(k0 + 3);
+    issued = k0 + 3;
+  }
+  for (int k = k0;;) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u) {
+      const int SC = (u + 1) & (NS - 1), SN = (u + 2) & (NS - 1);  // stages of planes k and k+1
+      wait_plane(k + 1);
+      const f2 ZRF = sp(m.zrF[k]), ZRC = sp(m.zrC[k]), ZRCM = sp(m.zrC[k - 1]), ZRFP = sp(m.zrF[k + 1]);
+      const f2 uP = RT_P2(SC, 0, 0), vP = RT_P2(SC, 1, 0), wP = RT_P2(SC, 2, 0);
+      const f2 uL = mk(RT_S1(SC, 0, 0, -1), uP.x), uR = mk(uP.y, RT_S1(SC, 0, 0, 2));
+      const f2 vL = mk(RT_S1(SC, 1, 0, -1), vP.x), vR = mk(vP.y, RT_S1(SC, 1, 0, 2));
+      const f2 wL = mk(RT_S1(SC, 2, 0, -1), wP.x), wR = mk(wP.y, RT_S1(SC, 2, 0, 2));
+      const f2 unP = RT_P2(SC, 0, 1), usP = RT_P2(SC, 0, -1), utP = RT_P2(SN, 0, 0);
+      const f2 vnP = RT_P2(SC, 1, 1), vsP = RT_P2(SC, 1, -1), vtP = RT_P2(SN, 1, 0), vstP = RT_P2(SN, 1, -1);
+      const f2 wnP = RT_P2(SC, 2, 1), wsP = RT_P2(SC, 2, -1), wtP = RT_P2(SN, 2, 0);
+      const f2 XL = mul(H, add(uL, uP)), XR = mul(H, add(uP, uR));
+      const f2 FxyP = mul(lin(W0, uP, W1, unP), mul(H, add(vP, vR)));
+      const f2 FxyL = mul(lin(W0, uL, W1, mk(RT_S1(SC, 0, 1, -1), unP.x)), mul(H, add(vL, vP)));
+      const f2 FxzP = fxz(H, uP, utP, wP, wR);
+      const f2 FxzL = fxz(H, uL, mk(RT_S1(SN, 0, 0, -1), utP.x), wL, wP);
+      const f2 FyzP = fyz(H, W0, W1, vP, vtP, wP, wnP);
+      const f2 dUt = sub(utP, uP), dVt = sub(vtP, vP), dWt = sub(wtP, wP);
+      const f2 WtA = mul(H, add(wP, wtP));
+      if (act) {
+        f2 oU{}, oV{}, oW{}, fU{}, fV{}, fW{};
+        if (NPW >= 3) { oU = RT_PW(SC, 0); oV = RT_PW(SC, 1); oW = RT_PW(SC, 2); }
+        if (NPW == 6) { fU = RT_PW(SC, 3); fV = RT_PW(SC, 4); fW = RT_PW(SC, 5); }
+        {  // u
+          const f2 ax = mul(dif(XR, XR, XL, XL), XRC_P);
+          const f2 ay = mul(sub(FxyP, mul(lin(W0M, usP, W1M, uP), mul(H, add(vsP, mk(vsP.y, RT_S1(SC, 1, -1, 2)))))), YRF);
+          const f2 az = mul(sub(FxzP, FxzB), ZRF);
+          const f2 vx = mul(dif(XRF_R, sub(uR, uP), XRF_P, sub(uP, uL)), XRC_P);
+          const f2 vy = mul(dif(sub(unP, uP), YRC, sub(uP, usP), YRCM), YRF);
+          const f2 vz = mul(dif(ZRC, dUt, ZRCM, dUz), ZRF);
+          f2 f = fma(NU, add(add(vx, vy), vz), sub(DPDX, add(add(ax, ay), az)));
+          if (zu_a) f.x = 0.f;
+          if (zu_b) f.y = 0.f;
+          rk<MODE>(F1u, Un, c, f, oU, fU, CDT1, TDT, TC1, TC2, su_a, su_b);
+        }
+        if (dv) {  // v
+          const f2 aa = mul(H, add(vP, vnP)), bb = mul(H, add(vsP, vP));
+          const f2 ay = mul(dif(aa, aa, bb, bb), YRC);
+          const f2 ax = mul(sub(FxyP, FxyL), XRF_P);
+          const f2 az = mul(sub(FyzP, FyzB), ZRF);
+          const f2 vx = mul(dif(XRC_P, sub(vR, vP), XRC_L, sub(vP, vL)), XRF_P);
+          const f2 vy = mul(dif(YRFP, sub(vnP, vP), YRF, sub(vP, vsP)), YRC);
+          const f2 vz = mul(dif(ZRC, dVt, ZRCM, dVz), ZRF);
+          f2 f = fma(NU, add(add(vx, vy), vz), neg(add(add(ay, ax), az)));
+          if (zx_a) f.x = 0.f;
+          if (zx_b) f.y = 0.f;
+          rk<MODE>(F1v, Vn, c, f, oV, fV, CDT1, TDT, TC1, TC2, sv_a, sv_b);
+        }
+        if (k <= g.nz - 1) {  // w
+          const f2 az = mul(dif(WtA, WtA, WbA, WbA), ZRC);
+          const f2 ax = mul(sub(FxzP, FxzL), XRF_P);
+          const f2 ay = mul(sub(FyzP, mul(mul(H, add(vsP, vstP)), lin(W0M, wsP, W1M, wP))), YRF);
+          const f2 vx = mul(dif(XRC_P, sub(wR, wP), XRC_L, sub(wP, wL)), XRF_P);
+          const f2 vy = mul(dif(sub(wnP, wP), YRC, sub(wP, wsP), YRCM), YRF);
+          const f2 vz = mul(dif(ZRFP, dWt, ZRF, dWz), ZRC);
+          f2 f = fma(NU, add(add(vx, vy), vz), sub(DPDZ, add(add(az, ax), ay)));
+          if (zx_a) f.x = 0.f;
+          if (zx_b) f.y = 0.f;
+          rk<MODE>(F1w, Wn, c, f, oW, fW, CDT1, TDT, TC1, TC2, sv_a, sv_b);
+        }
+      }
+      if (k == k1) goto drain;
+      FxzB = FxzP;
+      FyzB = FyzP;
+      dUz = dUt; dVz = dVt; dWz = dWt; WbA = WtA;
+      c += g.plane;
+      __syncthreads();  // plane k read by all: its stage takes plane k+4
+      if (*bad) goto drain;
+      if (tid == 0 && k + 4 <= k1 + 1) {
+        issue(k + 4);
+        issued = k + 4;
+      }
+      ++k;
+    }
+  }
+drain:
+#undef RT_P2
+#undef RT_S1
+#undef RT_PW
+  // after a missed wait: the copies this CTA issued complete before it exits
+  // (on the normal path every issued plane has been waited for)
+  __syncthreads();
+  if (tid == 0 && *bad)
+    for (int p = max(issued - NS + 1, k0 - 1); p <= issued; ++p)
+      tma::mbar_wait(&full[(p - k0 + 1) & (NS - 1)], (uint32_t)(((p - k0 + 1) >> 2) & 1));
 }
 
 // ---------------------------------------------------------------------------
@@ -1249,10 +1670,55 @@ static inline dim3 vol_grid(int ni, int nj, int nk, int kchunk, int by = 8) {
   return dim3((ni + 31) / 32, (nj + by - 1) / by, (nk + kchunk - 1) / kchunk);
 }
 
+#ifndef BLGPU_STENCIL_PRIMARY
+// planes of U, V, W as (px, py, nzg) FP32 tensors: boxes of 72 x 10 x 1
+// (neighbourhood tiles) and 64 x 8 x 1 (point-wise tiles)
+bool rhs_maps(const Geo &g, const float *U, const float *V, const float *W, RhsMaps *out) {
+  const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.nzg};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.plane * 4};
+  const cuuint32_t fbox[3] = {RT_TW, RT_TH, 1}, pbox[3] = {64, RT_BY, 1};
+  const float *a[3] = {U, V, W};
+  for (int q = 0; q < 3; ++q) {
+    CUtensorMap mf, mp;
+    if (!tma::encode(&mf, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(a[q]), dims, strides, fbox) ||
+        !tma::encode(&mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(a[q]), dims, strides, pbox))
+      return false;
+    static_assert(sizeof(CUtensorMap) == sizeof(out->f[0]), "tensor map size");
+    memcpy(out->f[q], &mf, sizeof mf);
+    memcpy(out->p[q], &mp, sizeof mp);
+  }
+  return true;
+}
+#endif
+
+template <int MODE>
+static void launch_rhs_tma(const Geo &g, const MetT<float> &m, const RhsMaps &mi, const RhsMaps &mo,
+                           const RhsMaps &mf, float *F1u, float *F1v, float *F1w, float *Un, float *Vn, float *Wn,
+                           const Scalars *sc, double c1, double c2, int kc, int *err, int wait_limit,
+                           cudaStream_t st) {
+  CUtensorMap t[9];
+  for (int q = 0; q < 3; ++q) {
+    memcpy(&t[q], mi.f[q], sizeof(CUtensorMap));
+    memcpy(&t[3 + q], mo.p[q], sizeof(CUtensorMap));
+    memcpy(&t[6 + q], mf.p[q], sizeof(CUtensorMap));
+  }
+  const size_t sm = rt_smem(MODE);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_rhs_rk_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
+  }
+  const dim3 grid = vol_grid(g.nx / 2, g.ny - 1, g.nz - 1, kc, RT_BY);
+  k_rhs_rk_tma<MODE><<<grid, dim3(32, RT_BY), sm, st>>>(t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], g, m,
+                                                        F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err,
+                                                        wait_limit < 0 ? tma::WAIT_LIMIT : wait_limit);
+}
+
 template <typename T>
 void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *U, const T *V, const T *W,
                    const T *nut, const T *Uo, const T *Vo, const T *Wo, T *F1u, T *F1v, T *F1w, T *Un, T *Vn, T *Wn,
-                   const Scalars *sc, double c1, double c2, const Tiles &tl, cudaStream_t st) {
+                   const Scalars *sc, double c1, double c2, const Tiles &tl, const RhsMaps *mi, const RhsMaps *mo,
+                   const RhsMaps *mf, int *err, int wait_limit, cudaStream_t st) {
   const int kchunk = tl.rhs_kc > 0 ? tl.rhs_kc : 8;
   const int by = tl.rhs_by > 0 ? tl.rhs_by : 8;
   dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kchunk, by), block(32, by);
@@ -1261,11 +1727,24 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
                                             c2, kchunk)
   if (!les && sizeof(T) == 4) {  // FP32: register-window kernel (FP64 keeps the lower-register form)
     const bool pair = tl.rhs_pts != 1;
-    const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : (pair ? 8 : 32);
+    // the TMA-fed kernel serves the default where its maps exist (16 planes
+    // per CTA: the two extra planes a chunk reads cost 1/8 of its loads)
+    const bool tma_fed = (tl.rhs_pts == 4 || tl.rhs_pts == 0) && mi && mo && mf;
+    const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : (tma_fed ? 16 : pair ? 8 : 32);
     // pairs cover i = 2..nx two points at a time
     dim3 gd = vol_grid(pair ? g.nx / 2 : g.nx - 1, g.ny - 1, g.nz - 1, kc, by);
 #define BLGPU_DNS_CASE(M)                                                                                           \
   do {                                                                                                              \
+    if constexpr (sizeof(T) == 4) {                                                                                 \
+      if (tma_fed) {                                                                                                \
+        launch_rhs_tma<M>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st);     \
+        break;                                                                                                      \
+      }                                                                                                             \
+      if (tl.rhs_pts == 3) {                                                                                        \
+        k_rhs_rk_pk<M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); \
+        break;                                                                                                      \
+      }                                                                                                             \
+    }                                                                                                               \
     if (pair)                                                                                                       \
       k_rhs_rk_pair<T, M><<<gd, block, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); \
     else                                                                                                            \
@@ -1386,7 +1865,8 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int 
 #define BLGPU_INST(T)                                                                                                \
   template void launch_rhs_rk<T>(const Geo &, const MetT<T> &, int, bool, const T *, const T *, const T *,          \
                                  const T *, const T *, const T *, const T *, T *, T *, T *, T *, T *, T *,          \
-                                 const Scalars *, double, double, const Tiles &, cudaStream_t);                     \
+                                 const Scalars *, double, double, const Tiles &, const RhsMaps *, const RhsMaps *,  \
+                                 const RhsMaps *, int *, int, cudaStream_t);                                        \
   template void launch_project<T>(const Geo &, const MetT<T> &, const T *, const double *, const float *, T *,    \
                                   T *, T *, T *,                                                                    \
                                   const Scalars *, int, const Tiles &, cudaStream_t);                               \

@@ -252,8 +252,10 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * dftz_rk (z wavenumbers per warp of the z-DFT, 4 or 8), proj_by (projection
  * block 32 x proj_by), zdft (mixed form, where M/2+1 <= 96: 1 = FP32 direct
  * sums, 2 = mma.sync TF32 tensor cores, 3 = tcgen05 tensor cores with the
- * accumulators in tensor memory), rhs_pts (mixed-form DNS
- * RHS: x-points per thread, 1 or 2), thomas (y-solve: 1 = register ring,
+ * accumulators in tensor memory), rhs_pts (mixed-form DNS RHS: 1 = one
+ * x-point per thread, 2 = two, 3 = two in packed FP32x2 instructions, 4 = as
+ * 3 with every plane staged in shared memory by TMA; rhs_by then fixed at
+ * 8), thomas (y-solve: 1 = register ring,
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
  * in shared memory, any N; 2 = two-pass register FFT, built for

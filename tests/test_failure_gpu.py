@@ -77,3 +77,30 @@ def test_y_solve_wait_limit_reports_and_recovers(gpu):
         assert np.array_equal(a, b)
     s.close()
     r.close()
+
+
+def test_rhs_plane_wait_limit_reports_and_recovers(gpu):
+    """The TMA-fed RHS (mixed form, rhs_pts 4) given zero polls: every CTA's
+    first plane wait gives up, the CTA drains the copies it issued and
+    leaves, the step reports BLGPU_EDEVICE; with the limit restored and the
+    state uploaded again the context steps exactly as a fresh one."""
+    c = _case()
+    c.cfl = -1e-3
+    s = cases.solver_for(c, precision=MIXED)
+    s.set_tiles(rhs_pts=4)
+    s.set_wait_limit(0)
+    s.time_step()
+    with pytest.raises(BlgpuError, match="RHS"):
+        s.sync()
+    s.sync()  # reported once
+    s.set_wait_limit(-1)
+    s.upload_state(c.U, c.V, c.W)
+    s.set_dt(1e-3)
+    s.advance(2)
+    r = cases.solver_for(c, precision=MIXED)
+    r.set_tiles(rhs_pts=4)
+    r.advance(2)
+    for a, b in zip(s.download_state()[:3], r.download_state()[:3]):
+        assert np.array_equal(a, b)
+    s.close()
+    r.close()
