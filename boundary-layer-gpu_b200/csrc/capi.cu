@@ -65,7 +65,7 @@ struct blgpu_ctx {
   uint32_t *utab = nullptr;   // mixed form: tcgen05 z transforms, tables (or null)
   ZdftMaps umaps{};           // and their TMA maps
   ThomasMaps tmaps{};         // TMA maps of C and the pivots for the tiled y-solve
-  RhsMaps rmaps[4]{};         // TMA maps of U, V, W of each state buffer and of F1 (mixed form)
+  RhsMaps rmaps[4]{};         // TMA maps of U, V, W of each state buffer and of F1 (TMA-fed RHS)
   bool have_rmaps = false;
   CufftPath *cf = nullptr;    // poisson = BLGPU_POISSON_CUFFT: plans and work arrays
   int cf_status = 0;          // first failing cufftExec status of an enqueued step (0: none)
@@ -276,15 +276,16 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
   for (int b = 0; b < 3; ++b)
     for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->S[b][q], box));
   for (int q = 0; q < 3; ++q) TRY(dalloc(ctx, &ctx->F1[q], box));
-  if (!ctx->fp64) {  // plane maps of the TMA-fed RHS: each state buffer and F1
+  {  // plane maps of the TMA-fed RHS: each state buffer and F1
     const Geo gb = ctx->geo_box();
+    auto enc = [&](void *const *f, RhsMaps *out) {
+      return ctx->fp64 ? rhs_maps64(gb, (const double *)f[0], (const double *)f[1], (const double *)f[2], out)
+                       : rhs_maps(gb, (const float *)f[0], (const float *)f[1], (const float *)f[2], out);
+    };
     ctx->have_rmaps = true;
     for (int b = 0; b < 3; ++b)
-      if (!rhs_maps(gb, (const float *)ctx->S[b][0], (const float *)ctx->S[b][1], (const float *)ctx->S[b][2],
-                    &ctx->rmaps[b]))
-        ctx->have_rmaps = false;
-    if (!rhs_maps(gb, (const float *)ctx->F1[0], (const float *)ctx->F1[1], (const float *)ctx->F1[2], &ctx->rmaps[3]))
-      ctx->have_rmaps = false;
+      if (!enc(ctx->S[b], &ctx->rmaps[b])) ctx->have_rmaps = false;
+    if (!enc(ctx->F1, &ctx->rmaps[3])) ctx->have_rmaps = false;
   }
   TRY(dalloc(ctx, &ctx->P, box));
   TRY(dalloc(ctx, &ctx->rhs_p, box));

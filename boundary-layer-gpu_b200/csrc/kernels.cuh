@@ -18,14 +18,15 @@ template <typename T> struct MetT {
 // Launch shapes of the main kernels.  0 selects the built-in choice; the
 // autotuner (blgpu_autotune) searches these per box.
 struct Tiles {
-  int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8; FP32 DNS 16 TMA-fed, 8 for two points, 32 for one)
+  int rhs_kc;   // k-planes walked by one CTA of the RHS kernel (0: 8; TMA-fed 16 in FP32, 32 in FP64; FP32 two points 8, one 32)
   int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
   int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 (8 two-pass) and 8 in FP64 (0: built-in)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
   int proj_by;  // projection block is 32 x proj_by threads (0: 8)
   int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
   int rhs_pts;  // FP32 DNS RHS: 1 one point per thread, 2 two points, 3 two points packed in FP32x2
-                // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2)
+                // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2);
+                // FP64 DNS: 1 the kernel of global loads, else the TMA-fed one where its maps exist
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
   int xfft;     // FP32 x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N)
@@ -69,8 +70,9 @@ struct RhsMaps {  // CUtensorMap bytes of the planes of U, V, W of one FP32 buff
 // false when a map cannot be encoded (the RHS then uses the kernels with
 // global loads)
 bool rhs_maps(const Geo &g, const float *U, const float *V, const float *W, RhsMaps *out);
-// mi, mo, mf: tensor maps of the buffers of U V W, Uo Vo Wo and F1 (FP32
-// DNS with rhs_pts 4), or null; err: device flag, bit 64 set when a plane
+bool rhs_maps64(const Geo &g, const double *U, const double *V, const double *W, RhsMaps *out);
+// mi, mo, mf: tensor maps of the buffers of U V W, Uo Vo Wo and F1 (the
+// TMA-fed DNS kernels: FP32 with rhs_pts 0 or 4, FP64 unless rhs_pts 1), or null; err: device flag, bit 64 set when a plane
 // copy missed its wait limit; wait_limit: mbarrier polls before giving up
 // (< 0: the built-in limit)
 template <typename T>

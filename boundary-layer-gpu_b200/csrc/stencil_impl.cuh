@@ -21,8 +21,22 @@ namespace blgpu {
 // ---------------------------------------------------------------------------
 // division policy: the FP64 path divides exactly where the source divides;
 // the FP32 path multiplies by the reciprocal table instead.
+// The FP64 quotient is formed from the table's reciprocal rb = RN(1/b)
+// (the host's correctly rounded 1.0/b) by Markstein's correction (P. W.
+// Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34 (1990); also "IA-64 and Elementary
+// Functions", 2000, Thm. 8.10): q = RN(a rb) is within one ulp of a/b, the
+// remainder r = a - b q is exact in one fused multiply-add, and RN(q + r rb)
+// is the correctly rounded a/b -- the value of the source's division, in one
+// multiply and two fused multiply-adds instead of a division sequence.  The
+// operands here (velocities, spacings) stay far from overflow and underflow,
+// where the theorem holds.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double qdiv(double a, double b, double) { return a / b; }
+__device__ __forceinline__ double qdiv(double a, double b, double rb) {
+  const double q = a * rb;
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, rb, q);
+}
 // maximum that keeps a NaN (fmax drops it): check_divergence of a field that
 // holds a NaN reads NaN
 __device__ __forceinline__ double max_keep_nan(double a, double b) { return (a > b || a != a) ? a : b; }
@@ -37,9 +51,9 @@ template <typename T> struct Ld {
 };
 
 // RHS of u at (i,j,k), equations.f90:53-91 (DNS) / :98-129 (LES)
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_u_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
-                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+template <typename T, bool LES, typename L = Ld<T>>
+__device__ __forceinline__ T rhs_u_at(const Geo &g, const MetT<T> &m, const L &U, const L &V, const L &W,
+                                      const L &N, long long c, int i, int j, int k) {
   const T h = (T)0.5;
   T uc = U(c, 0, 0, 0), ue = U(c, 1, 0, 0), uw = U(c, -1, 0, 0);
   T un = U(c, 0, 1, 0), us = U(c, 0, -1, 0), ut = U(c, 0, 0, 1), ub = U(c, 0, 0, -1);
@@ -75,9 +89,9 @@ __device__ __forceinline__ T rhs_u_at(const Geo &g, const MetT<T> &m, const Ld<T
 }
 
 // RHS of v at (i,j,k), equations.f90:188-227 (DNS) / :238-266 (LES)
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_v_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
-                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+template <typename T, bool LES, typename L = Ld<T>>
+__device__ __forceinline__ T rhs_v_at(const Geo &g, const MetT<T> &m, const L &U, const L &V, const L &W,
+                                      const L &N, long long c, int i, int j, int k) {
   const T h = (T)0.5;
   T vc = V(c, 0, 0, 0), ve = V(c, 1, 0, 0), vw = V(c, -1, 0, 0);
   T vn = V(c, 0, 1, 0), vs = V(c, 0, -1, 0), vt = V(c, 0, 0, 1), vb = V(c, 0, 0, -1);
@@ -109,9 +123,9 @@ __device__ __forceinline__ T rhs_v_at(const Geo &g, const MetT<T> &m, const Ld<T
 }
 
 // RHS of w at (i,j,k), equations.f90:328-363 (DNS) / :383-401 (LES)
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_w_at(const Geo &g, const MetT<T> &m, const Ld<T> &U, const Ld<T> &V,
-                                      const Ld<T> &W, const Ld<T> &N, long long c, int i, int j, int k) {
+template <typename T, bool LES, typename L = Ld<T>>
+__device__ __forceinline__ T rhs_w_at(const Geo &g, const MetT<T> &m, const L &U, const L &V, const L &W,
+                                      const L &N, long long c, int i, int j, int k) {
   const T h = (T)0.5;
   T wc = W(c, 0, 0, 0), we = W(c, 1, 0, 0), ww = W(c, -1, 0, 0);
   T wn = W(c, 0, 1, 0), ws = W(c, 0, -1, 0), wt = W(c, 0, 0, 1), wb = W(c, 0, 0, -1);
@@ -980,6 +994,158 @@ drain:
 }
 
 // ---------------------------------------------------------------------------
+// The FP64 DNS RHS fed by TMA.  The arithmetic is rhs_*_at and the RK update
+// of k_rhs_rk, term for term (the FP64 unit is compiled without contraction,
+// so the results are those of k_rhs_rk bit for bit); only the operands come
+// from shared memory.  A CTA of 32 x 8 threads owns 32 x-points (one per
+// thread) by 8 rows and walks a chunk of k-planes.  Plane p of U, V, W
+// arrives as one 36 x 10 x 1 tensor copy per field (x from the CTA's first
+// point - 2, so the copy starts on a 16-byte boundary; rows j-1 .. j+8) and,
+// for the planes the CTA updates, Uo, Vo, Wo and F1 as 32 x 8 x 1 copies.  A
+// ring of 5 stages holds plane p in stage (p - k0 + 1) mod 5: plane k is
+// computed from planes k-1, k and k+1 while k+2 and k+3 are in flight, and
+// after a CTA barrier the stage of plane k-1 takes plane k+4.  The k loop is
+// unrolled by the ring length.  Wait limits and the drain as in k_rhs_rk_tma.
+// ---------------------------------------------------------------------------
+constexpr int R64_NS = 5, R64_TW = 36, R64_BY = 8, R64_TH = R64_BY + 2;
+constexpr int R64_FS = (R64_TH * R64_TW * 8 + 127) / 128 * 16;  // doubles per field tile (a 128-byte multiple)
+constexpr int R64_PS = 32 * R64_BY;                             // doubles per point-wise tile
+__host__ __device__ constexpr int r64_stage(int mode) { return 3 * R64_FS + rt_npw(mode) * R64_PS; }  // doubles
+__host__ __device__ constexpr size_t r64_smem(int mode) {
+  return (size_t)R64_NS * r64_stage(mode) * 8 + R64_NS * 8 + 16;
+}
+
+// operand loader of rhs_*_at over the staged planes k-1, k, k+1 (pointers at
+// the thread's point; di, dj, dk in -1..1 are compile-time at every call)
+struct SmemLd64 {
+  const double *pb, *pc, *pt;
+  __device__ __forceinline__ double operator()(long long, int di, int dj, int dk) const {
+    return (dk < 0 ? pb : dk > 0 ? pt : pc)[di + dj * R64_TW];
+  }
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * R64_BY, 2)
+    k_rhs_rk_tma64(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
+                   const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap mou,
+                   const __grid_constant__ CUtensorMap mov, const __grid_constant__ CUtensorMap mow,
+                   const __grid_constant__ CUtensorMap mfu, const __grid_constant__ CUtensorMap mfv,
+                   const __grid_constant__ CUtensorMap mfw, Geo g, MetT<double> m, double *__restrict__ F1u,
+                   double *__restrict__ F1v, double *__restrict__ F1w, double *__restrict__ Un,
+                   double *__restrict__ Vn, double *__restrict__ Wn, const Scalars *__restrict__ sc, double c1,
+                   double c2, int kchunk, int *err, int wait_limit) {
+  constexpr int NS = R64_NS, TW = R64_TW, NPW = rt_npw(MODE), SS = r64_stage(MODE);
+  constexpr uint32_t FIELD_BYTES = 3u * TW * R64_TH * 8u, PW_BYTES = (uint32_t)NPW * R64_PS * 8u;
+  extern __shared__ __align__(1024) double r64_sm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(r64_sm + NS * SS);
+  volatile int *bad = reinterpret_cast<volatile int *>(full + NS);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int istart = 2 + 32 * blockIdx.x, jstart = 2 + R64_BY * blockIdx.y;
+  const int i = istart + tx, j = jstart + ty;
+  const int k0 = blockIdx.z * kchunk + 2;
+  const int k1 = min(k0 + kchunk - 1, g.nz);
+  if (k0 > k1) return;  // whole CTA
+  const bool act = i <= g.nx && j <= g.ny;
+  if (tid == 0) {
+    *bad = (tma::smem_u32(r64_sm) & 127u) ? 1 : 0;
+    for (int s = 0; s < NS; ++s) tma::mbar_init(&full[s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncthreads();
+  if (*bad) {
+    if (tid == 0) atomicOr(err, 64);
+    return;
+  }
+  auto issue = [&](int p) {  // thread 0: plane p into its stage
+    const int s = (p - k0 + 1) % NS;
+    double *st = r64_sm + s * SS;
+    const bool pw = NPW > 0 && p >= k0 && p <= k1;
+    tma::mbar_expect_tx(&full[s], FIELD_BYTES + (pw ? PW_BYTES : 0u));
+    tma::load_3d(st, &mu, istart, jstart - 2, p - 1, &full[s]);
+    tma::load_3d(st + R64_FS, &mv, istart, jstart - 2, p - 1, &full[s]);
+    tma::load_3d(st + 2 * R64_FS, &mw, istart, jstart - 2, p - 1, &full[s]);
+    if (pw) {
+      double *pt = st + 3 * R64_FS;
+      tma::load_3d(pt, &mou, istart + 2, jstart - 1, p - 1, &full[s]);
+      tma::load_3d(pt + R64_PS, &mov, istart + 2, jstart - 1, p - 1, &full[s]);
+      tma::load_3d(pt + 2 * R64_PS, &mow, istart + 2, jstart - 1, p - 1, &full[s]);
+      if (NPW == 6) {
+        tma::load_3d(pt + 3 * R64_PS, &mfu, istart + 2, jstart - 1, p - 1, &full[s]);
+        tma::load_3d(pt + 4 * R64_PS, &mfv, istart + 2, jstart - 1, p - 1, &full[s]);
+        tma::load_3d(pt + 5 * R64_PS, &mfw, istart + 2, jstart - 1, p - 1, &full[s]);
+      }
+    }
+  };
+  int issued = k0 - 2;  // thread 0: last plane issued
+  if (tid == 0)
+    for (int p = k0 - 1; p <= min(k0 + NS - 2, k1 + 1); ++p) {
+      issue(p);
+      issued = p;
+    }
+  auto wait_plane = [&](int p) {
+    if (!tma::mbar_wait(&full[(p - k0 + 1) % NS], (uint32_t)(((p - k0 + 1) / NS) & 1), wait_limit)) {
+      *bad = 1;
+      atomicOr(err, 64);
+    }
+  };
+  // per-thread offsets: field tiles at row j (tile row ty + 1), column of
+  // point i (tx + 2); point-wise tiles at row ty, column tx
+  const double *fo = r64_sm + (ty + 1) * TW + 2 + tx;
+  const double *po = r64_sm + 3 * R64_FS + ty * 32 + tx;
+  double dt = 0.0;
+  if (MODE != 0) dt = sc->dt;
+  const double cdt1 = dt * c1, tdt = dt, tc1 = c1, tc2 = c2;
+  const bool du = (i <= g.nx - 1), dv = (j <= g.ny - 1);
+  wait_plane(k0 - 1);
+  wait_plane(k0);
+  for (int k = k0;;) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u) {
+      const int SB = u, SC = (u + 1) % NS, ST = (u + 2) % NS;  // stages of planes k-1, k, k+1
+      wait_plane(k + 1);
+      if (act) {
+        const SmemLd64 LU{fo + SB * SS, fo + SC * SS, fo + ST * SS};
+        const SmemLd64 LV{fo + SB * SS + R64_FS, fo + SC * SS + R64_FS, fo + ST * SS + R64_FS};
+        const SmemLd64 LW{fo + SB * SS + 2 * R64_FS, fo + SC * SS + 2 * R64_FS, fo + ST * SS + 2 * R64_FS};
+        const double *pw = po + SC * SS;
+        const long long c = bidx(g, i, j, k);
+        if (du) {
+          double f = (i == g.nx - 1) ? 0.0 : rhs_u_at<double, false, SmemLd64>(g, m, LU, LV, LW, LU, c, i, j, k);
+          if (MODE == 0) F1u[c] = f;
+          else if (MODE == 1) { F1u[c] = f; Un[c] = pw[0] + cdt1 * f; }
+          else Un[c] = pw[0] + tdt * (tc1 * pw[3 * R64_PS] + tc2 * f);
+        }
+        if (dv) {
+          double f = (i == g.nx) ? 0.0 : rhs_v_at<double, false, SmemLd64>(g, m, LU, LV, LW, LU, c, i, j, k);
+          if (MODE == 0) F1v[c] = f;
+          else if (MODE == 1) { F1v[c] = f; Vn[c] = pw[R64_PS] + cdt1 * f; }
+          else Vn[c] = pw[R64_PS] + tdt * (tc1 * pw[4 * R64_PS] + tc2 * f);
+        }
+        if (k <= g.nz - 1) {
+          double f = (i == g.nx) ? 0.0 : rhs_w_at<double, false, SmemLd64>(g, m, LU, LV, LW, LU, c, i, j, k);
+          if (MODE == 0) F1w[c] = f;
+          else if (MODE == 1) { F1w[c] = f; Wn[c] = pw[2 * R64_PS] + cdt1 * f; }
+          else Wn[c] = pw[2 * R64_PS] + tdt * (tc1 * pw[5 * R64_PS] + tc2 * f);
+        }
+      }
+      if (k == k1) goto drain;
+      __syncthreads();  // plane k-1 read by all: its stage takes plane k+4
+      if (*bad) goto drain;
+      if (tid == 0 && k + NS - 1 <= k1 + 1) {
+        issue(k + NS - 1);
+        issued = k + NS - 1;
+      }
+      ++k;
+    }
+  }
+drain:
+  __syncthreads();
+  if (tid == 0 && *bad)
+    for (int p = max(issued - NS + 1, k0 - 1); p <= issued; ++p)
+      tma::mbar_wait(&full[(p - k0 + 1) % NS], (uint32_t)(((p - k0 + 1) / NS) & 1));
+}
+
+// ---------------------------------------------------------------------------
 // project_velocity (projection.f90:359-384) + pressure save at rk_step 1
 // (projection.f90:75-78, P(2:nxg-1,2:nyg-1,2:nzg-1) = rhs_p/(dt*rk2_coef(1,1))).
 // p holds rhs_p in the box layout (i=2..nx, j=2..ny, k=2..nz valid).
@@ -1691,6 +1857,49 @@ bool rhs_maps(const Geo &g, const float *U, const float *V, const float *W, RhsM
 }
 #endif
 
+#ifdef BLGPU_STENCIL_PRIMARY
+// planes of U, V, W as (px, py, nzg) FP64 tensors: boxes of 36 x 10 x 1
+// (neighbourhood tiles) and 32 x 8 x 1 (point-wise tiles)
+bool rhs_maps64(const Geo &g, const double *U, const double *V, const double *W, RhsMaps *out) {
+  const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.nzg};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.px * 8, (cuuint64_t)g.plane * 8};
+  const cuuint32_t fbox[3] = {R64_TW, R64_TH, 1}, pbox[3] = {32, R64_BY, 1};
+  const double *a[3] = {U, V, W};
+  for (int q = 0; q < 3; ++q) {
+    CUtensorMap mf, mp;
+    if (!tma::encode(&mf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(a[q]), dims, strides, fbox) ||
+        !tma::encode(&mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(a[q]), dims, strides, pbox))
+      return false;
+    memcpy(out->f[q], &mf, sizeof mf);
+    memcpy(out->p[q], &mp, sizeof mp);
+  }
+  return true;
+}
+#endif
+
+template <int MODE>
+static void launch_rhs_tma64(const Geo &g, const MetT<double> &m, const RhsMaps &mi, const RhsMaps &mo,
+                             const RhsMaps &mf, double *F1u, double *F1v, double *F1w, double *Un, double *Vn,
+                             double *Wn, const Scalars *sc, double c1, double c2, int kc, int *err, int wait_limit,
+                             cudaStream_t st) {
+  CUtensorMap t[9];
+  for (int q = 0; q < 3; ++q) {
+    memcpy(&t[q], mi.f[q], sizeof(CUtensorMap));
+    memcpy(&t[3 + q], mo.p[q], sizeof(CUtensorMap));
+    memcpy(&t[6 + q], mf.p[q], sizeof(CUtensorMap));
+  }
+  const size_t sm = r64_smem(MODE);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_rhs_rk_tma64<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
+  }
+  const dim3 grid = vol_grid(g.nx - 1, g.ny - 1, g.nz - 1, kc, R64_BY);
+  k_rhs_rk_tma64<MODE><<<grid, dim3(32, R64_BY), sm, st>>>(t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], g,
+                                                           m, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err,
+                                                           wait_limit < 0 ? tma::WAIT_LIMIT : wait_limit);
+}
+
 template <int MODE>
 static void launch_rhs_tma(const Geo &g, const MetT<float> &m, const RhsMaps &mi, const RhsMaps &mo,
                            const RhsMaps &mf, float *F1u, float *F1v, float *F1w, float *Un, float *Vn, float *Wn,
@@ -1758,6 +1967,20 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
     }
 #undef BLGPU_DNS_CASE
   } else if (!les) {
+    if constexpr (sizeof(T) == 8) {
+      // FP64 DNS: the TMA-fed kernel (results bit-identical to k_rhs_rk) where
+      // its maps exist, unless rhs_pts = 1 asks for the global-load kernel
+      if (tl.rhs_pts != 1 && mi && mo && mf) {
+        const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 32;
+        switch (mode) {
+          case 0: launch_rhs_tma64<0>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st); break;
+          case 1: launch_rhs_tma64<1>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st); break;
+          case 2: launch_rhs_tma64<2>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st); break;
+          default: launch_rhs_tma64<3>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st); break;
+        }
+        return;
+      }
+    }
     switch (mode) {
       case 0: BLGPU_RHS_CASE(0, false); break;
       case 1: BLGPU_RHS_CASE(1, false); break;

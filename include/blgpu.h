@@ -254,8 +254,9 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * sums, 2 = mma.sync TF32 tensor cores, 3 = tcgen05 tensor cores with the
  * accumulators in tensor memory), rhs_pts (mixed-form DNS RHS: 1 = one
  * x-point per thread, 2 = two, 3 = two in packed FP32x2 instructions, 4 = as
- * 3 with every plane staged in shared memory by TMA; rhs_by then fixed at
- * 8), thomas (y-solve: 1 = register ring,
+ * 3 with every plane staged in shared memory by TMA, rhs_by then fixed at
+ * 8; FP64 DNS: 1 = global loads, else TMA-fed planes, both bit-identical),
+ * thomas (y-solve: 1 = register ring,
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
  * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
  * in shared memory, any N; 2 = two-pass register FFT, built for
