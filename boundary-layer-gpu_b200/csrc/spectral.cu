@@ -195,25 +195,6 @@ __device__ __forceinline__ void bf_odd(const T2<T> *in, T2<T> *out, int jj, int 
   }
 }
 
-// any radix: output k of butterfly jj by direct summation from shared
-// memory (large primes).  e = tstep + k n/R < n, so one subtraction keeps
-// the table index q*e mod n in range.
-template <typename T, bool INV>
-__device__ __forceinline__ void bf_loop_out(const T2<T> *in, T2<T> *out, int R, int k, int jj, int nb, int tstep,
-                                            int idxD, int Ns, int n, const T2<T> *tw) {
-  const int e = tstep + k * (n / R);
-  T ax = 0, ay = 0;
-  int idx = 0;
-  for (int q = 0; q < R; ++q) {
-    T2<T> v = twm<T, INV>(in[jj + q * nb], tw[idx]);
-    ax += v.x;
-    ay += v.y;
-    idx += e;
-    if (idx >= n) idx -= n;
-  }
-  out[idxD + k * Ns] = mk<T>(ax, ay);
-}
-
 // radices with a dedicated butterfly in the kernel instantiated for MAXR
 template <int MAXR>
 __device__ __forceinline__ bool reg_radix(int R) {
@@ -233,12 +214,62 @@ __device__ __forceinline__ T2<T> *fft_warp(T2<T> *a, T2<T> *b, const FftPlan<T> 
     const int nb = n / R;
     const int tsc = n / (Ns * R);
     if (!reg_radix<MAXR>(R)) {
-      // a large prime has few butterflies (nb = n/R), so the lanes take
-      // (butterfly, output) pairs: n items of R terms each
-      for (int t = lane; t < n; t += 32) {
-        const int k = t / nb, jj = t - k * nb;
+      // a large prime R has few butterflies (nb = n/R), so the lanes take
+      // (butterfly, term pair) and (butterfly, output pair) items.  First the
+      // inputs of butterfly jj are twiddled (y_q = in_q W_n^{q tstep}) and
+      // folded in place: a[jj + q nb] <- s_q = y_q + y_{R-q},
+      // a[jj + (R-q) nb] <- d_q = y_q - y_{R-q}, q = 1 .. H (the stage's
+      // input is dead after it).  Then X_0 = y_0 + sum s_q and, for k = 1..H,
+      //   X_k, X_{R-k} = y_0 + sum_q s_q cos(2 pi qk/R) -+ i sum_q d_q sin(2 pi qk/R)
+      // (signs swapped for the inverse): H terms for two outputs instead of
+      // R terms for one.
+      const int H = (R - 1) / 2;
+      for (int t = lane; t < nb * H; t += 32) {
+        const int jj = t % nb, q = 1 + t / nb;
+        const int tstep = (jj % Ns) * tsc;
+        T2<T> y1 = a[jj + q * nb], y2 = a[jj + (R - q) * nb];
+        if (tstep) {
+          y1 = twm<T, INV>(y1, tw[q * tstep]);
+          y2 = twm<T, INV>(y2, tw[(R - q) * tstep]);
+        }
+        a[jj + q * nb] = add<T>(y1, y2);
+        a[jj + (R - q) * nb] = sub<T>(y1, y2);
+      }
+      __syncwarp();
+      for (int t = lane; t < nb * (H + 1); t += 32) {
+        const int jj = t % nb, k = t / nb;
         const int jm = jj % Ns;
-        bf_loop_out<T, INV>(a, b, R, k, jj, nb, jm * tsc, (jj - jm) * R + jm, Ns, n, tw);
+        const int idxD = (jj - jm) * R + jm;
+        const T2<T> y0 = a[jj];
+        T ax = y0.x, ay = y0.y;
+        if (k == 0) {
+          for (int q = 1; q <= H; ++q) {
+            const T2<T> sq = a[jj + q * nb];
+            ax += sq.x;
+            ay += sq.y;
+          }
+          b[idxD] = mk<T>(ax, ay);
+          continue;
+        }
+        T bx = 0, by = 0;  // sums of d_q times the table's imaginary part (-sin)
+        int m = 0;         // q k mod R
+        for (int q = 1; q <= H; ++q) {
+          m += k;
+          if (m >= R) m -= R;
+          const T2<T> w = tw[m * nb];  // W_R^m = (cos, -sin)(2 pi m / R)
+          const T2<T> sq = a[jj + q * nb], dq = a[jj + (R - q) * nb];
+          ax += sq.x * w.x;
+          ay += sq.y * w.x;
+          bx += dq.x * w.y;
+          by += dq.y * w.y;
+        }
+        if (!INV) {
+          b[idxD + k * Ns] = mk<T>(ax - by, ay + bx);
+          b[idxD + (R - k) * Ns] = mk<T>(ax + by, ay - bx);
+        } else {
+          b[idxD + k * Ns] = mk<T>(ax + by, ay - bx);
+          b[idxD + (R - k) * Ns] = mk<T>(ax - by, ay + bx);
+        }
       }
       __syncwarp();
       T2<T> *t = a;
