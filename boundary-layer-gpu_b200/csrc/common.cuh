@@ -39,6 +39,19 @@ struct Geo {
   double nu, dpdx, dpdz;
 };
 
+// a / b, correctly rounded, from rb = RN(1/b) (the host's 1.0/b) by
+// Markstein's correction (P. W. Markstein, IBM J. Res. Dev. 34, 1990; "IA-64
+// and Elementary Functions", 2000, Thm. 8.10): q = RN(a rb) is within one
+// ulp of a/b, the remainder a - b q is exact in one fused multiply-add, and
+// RN(q + (a - b q) rb) is RN(a/b), for operands far from overflow and
+// underflow.  One multiply and two fused multiply-adds in place of the
+// division sequence; the FP64 kernels divide through it wherever the source
+// divides by a grid spacing whose reciprocal is tabulated.
+__device__ __forceinline__ double mdiv(double a, double b, double rb) {
+  const double q = __dmul_rn(a, rb);
+  return __fma_rn(__fma_rn(-q, b, a), rb, q);
+}
+
 __host__ __device__ inline long long bidx(const Geo &g, int i, int j, int k) {
   return ((long long)(k - 1) * g.py + (j - 1)) * (long long)g.px + (i + 2);
 }

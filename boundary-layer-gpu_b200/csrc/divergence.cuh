@@ -7,8 +7,9 @@
 
 namespace blgpu {
 
-// FP64: the source's divisions; FP32: products with the reciprocal spacing
-__device__ __forceinline__ double dq(double a, double F, double) { return a / F; }
+// FP64: the source's divisions (correctly rounded, through mdiv); FP32:
+// products with the reciprocal spacing
+__device__ __forceinline__ double dq(double a, double F, double rF) { return mdiv(a, F, rF); }
 __device__ __forceinline__ float dq(float a, double, double rF) { return a * (float)rF; }
 
 // c = bidx(g, i, j, k)

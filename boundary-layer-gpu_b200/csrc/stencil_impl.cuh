@@ -21,22 +21,10 @@ namespace blgpu {
 // ---------------------------------------------------------------------------
 // division policy: the FP64 path divides exactly where the source divides;
 // the FP32 path multiplies by the reciprocal table instead.
-// The FP64 quotient is formed from the table's reciprocal rb = RN(1/b)
-// (the host's correctly rounded 1.0/b) by Markstein's correction (P. W.
-// Markstein, "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34 (1990); also "IA-64 and Elementary
-// Functions", 2000, Thm. 8.10): q = RN(a rb) is within one ulp of a/b, the
-// remainder r = a - b q is exact in one fused multiply-add, and RN(q + r rb)
-// is the correctly rounded a/b -- the value of the source's division, in one
-// multiply and two fused multiply-adds instead of a division sequence.  The
-// operands here (velocities, spacings) stay far from overflow and underflow,
-// where the theorem holds.
+// The FP64 quotient is the correctly rounded a/b formed from the table's
+// reciprocal by mdiv (common.cuh): the value of the source's division.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double qdiv(double a, double b, double rb) {
-  const double q = a * rb;
-  const double r = __fma_rn(-q, b, a);
-  return __fma_rn(r, rb, q);
-}
+__device__ __forceinline__ double qdiv(double a, double b, double rb) { return mdiv(a, b, rb); }
 // maximum that keeps a NaN (fmax drops it): check_divergence of a field that
 // holds a NaN reads NaN
 __device__ __forceinline__ double max_keep_nan(double a, double b) { return (a > b || a != a) ? a : b; }
