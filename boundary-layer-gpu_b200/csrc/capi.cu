@@ -75,6 +75,7 @@ struct blgpu_ctx {
   Scalars *sc = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   void *tw = nullptr, *post = nullptr, *ztab = nullptr;
+  void *ztab64 = nullptr;  // cos and sin tables of the FP64 z transforms on the FP64 MMA
   FftPlan<double> pl64{};
   FftPlan<float> pl32{};
   double *stage = nullptr;  // FP64 staging of one host-layout field
@@ -406,6 +407,13 @@ int blgpu_create(const blgpu_config *cfg, blgpu_ctx **out) {
       TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, tw.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
       TRY(check_cuda(ctx, cudaMemcpy(ctx->post, post.data(), N * es2, cudaMemcpyHostToDevice), "post"));
       TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab, zt.data(), (size_t)MH * MH * es2, cudaMemcpyHostToDevice), "ztab"));
+      if (s.M >= 8 && s.M <= 254) {  // FP64 z transforms on the FP64 MMA (rows to 128, 4 per lane group)
+        std::vector<double> t64;
+        zdft64_tables(s, t64);
+        TRY(dalloc(ctx, &ctx->ztab64, t64.size() * sizeof(double)));
+        TRY(check_cuda(ctx, cudaMemcpy(ctx->ztab64, t64.data(), t64.size() * sizeof(double), cudaMemcpyHostToDevice),
+                       "ztab64"));
+      }
     } else {
       std::vector<float> a(tw.begin(), tw.end()), b(post.begin(), post.end()), c(zt.begin(), zt.end());
       TRY(check_cuda(ctx, cudaMemcpy(ctx->tw, a.data(), N * es2, cudaMemcpyHostToDevice), "tw"));
@@ -1066,6 +1074,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_begin(ctx, PH_DFTZ);
   if (um) launch_zdft_umma(s, ctx->umaps, (float *)ctx->R, (float2 *)ctx->C, ctx->utab, 0, ctx->nsm, &ctx->sc->err, ctx->st);
   else if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 0, ctx->nsm, &ctx->sc->err, ctx->st);
+  else if (ctx->ztab64) launch_zdft64(s, (double *)ctx->R, (double2 *)ctx->C, (const double *)ctx->ztab64, 0, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 0, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
@@ -1083,6 +1092,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_begin(ctx, PH_IDFTZ);
   if (um) launch_zdft_umma(s, ctx->umaps, (float *)ctx->R, (float2 *)ctx->C, ctx->utab, 1, ctx->nsm, &ctx->sc->err, ctx->st);
   else if (tc) launch_zdft_tc(s, ctx->zmaps, (float *)ctx->R, (float2 *)ctx->C, ctx->zfrag, 1, ctx->nsm, &ctx->sc->err, ctx->st);
+  else if (ctx->ztab64) launch_zdft64(s, (double *)ctx->R, (double2 *)ctx->C, (const double *)ctx->ztab64, 1, ctx->st);
   else launch_dft_z<T>(s, (T *)ctx->R, (T2 *)ctx->C, (const T2 *)ctx->ztab, 1, ctx->tiles.dftz_rk, ctx->st);
   ph_end(ctx, 1);
   ph_begin(ctx, PH_IDCT);

@@ -140,6 +140,10 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
 template <typename T>
 void launch_dft_z(const Spec &s, const T *R, typename vec2<T>::type *C, const typename vec2<T>::type *ztab, int inverse,
                   int rk, cudaStream_t st);
+// FP64 z transforms on the FP64 tensor-core MMA (8 <= M <= 254): the host
+// tables (cos, then sin, [rows][Kp] each) and the forward / inverse launch
+void zdft64_tables(const Spec &s, std::vector<double> &t);
+void launch_zdft64(const Spec &s, double *R, double2 *C, const double *tab, int inverse, cudaStream_t st);
 // H0 (mixed form): the kz = 0 modes kx < klow are solved in FP64 into
 // H0[NM][klow] and zeroed in C; null for the FP64 form
 template <typename T>

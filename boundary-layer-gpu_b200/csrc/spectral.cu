@@ -974,6 +974,213 @@ __global__ void __launch_bounds__(256) k_dft_z_inv(Spec s, const T2<T> *__restri
 }
 
 // ---------------------------------------------------------------------------
+// FP64 z transforms as products on the FP64 tensor-core MMA (mma.sync
+// m8n8k4 f64; the tcgen05 MMA has no FP64 kind).  The sums of the direct
+// transforms above, with H = (M-1)/2 and the half-spectrum rows r = 0..MH-1:
+//   forward  Re C_r = f_0 + sum_{k=1..H} S_k cos(2 pi r k/M) [+ (-1)^r f_{M/2}, M even]
+//            Im C_r = -sum_{k=1..H} D_k sin(2 pi r k/M),  S_k, D_k = f_k +- f_{M-k}
+//   inverse  f_p, f_{M-p} = (C_0 + 2 (P_p -+ Q_p) [+ (-1)^p C_{M/2}]) / M,
+//            P_p = sum_{k=1..H} Re C_k cos(2 pi p k/M), Q_p = sum Im C_k sin(...)
+// are each a product (rows r or p) x (K = H terms) x (32 x columns of a CTA)
+// with the tables tc[r][k-1] = cos, ts[r][k-1] = sin (rows to MHp = MH
+// rounded up to 16, columns to Kp = H rounded up to 4, zero beyond H and
+// MH).  A CTA owns one row b and 32 kx; its column data sit in shared memory
+// transposed ([x][k], pitch PZ = 4 mod 16 doubles, so the B fragments meet
+// two wavefronts); the forward folds S_k, D_k in place (F[x][k], F[x][M-k]).
+// Warp w computes rows 16w .. 16w+15 by 2 x 4 MMA tiles of 8 x 8, K in steps
+// of 4.  Fragments (PTX m8n8k4 .f64): A a0 at (row lane/4, col lane%4), B b0
+// at (row lane%4, col lane/4), C c0, c1 at (row lane/4, cols 2 (lane%4) + i).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+__host__ __device__ inline int zd64_kp(int M) { return ((M - 1) / 2 + 3) / 4 * 4; }
+__host__ __device__ inline int zd64_rows(int M) { return (M / 2 + 1 + 15) / 16 * 16; }
+// pitch of the transposed column data: >= the larger of M and Kp + 1, = 4 mod 16
+__host__ __device__ inline int zd64_pitch(int len) { return (len + 11) / 16 * 16 + 4; }
+
+__global__ void __launch_bounds__(256) k_zdft64_fwd(Spec s, const double *__restrict__ R, double2 *__restrict__ C,
+                                                    const double *__restrict__ tc, const double *__restrict__ ts) {
+  extern __shared__ double zf[];  // [32][PZ]
+  const int M = s.M, MH = s.MH, H = (M - 1) / 2, Kp = zd64_kp(M), PZ = zd64_pitch(M);
+  const int b = blockIdx.y, x0 = blockIdx.x * 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const bool xin = x0 + lane < s.N;
+  // rows in batches of 8 per warp, every load of a batch issued before the
+  // stores (the slab comes from DRAM)
+  for (int k8 = warp * 8; k8 < PZ; k8 += nw * 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k8 + u;
+      v[u] = (k < M && xin) ? __ldcs(R + ((long long)b * M + k) * s.rx + x0 + lane) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k8 + u < PZ) zf[lane * PZ + k8 + u] = v[u];
+  }
+  __syncthreads();
+  for (int t = tid; t < 32 * H; t += blockDim.x) {
+    const int x = t & 31, k = 1 + (t >> 5);
+    const double a = zf[x * PZ + k], c = zf[x * PZ + M - k];
+    zf[x * PZ + k] = a + c;
+    zf[x * PZ + M - k] = a - c;
+  }
+  __syncthreads();
+  const int r0 = 16 * warp;
+  if (r0 >= MH) return;
+  const int g = lane >> 2, q = lane & 3;
+  double re[2][4][2] = {}, im[2][4][2] = {};
+  // table fragments of the next K step fetched one step ahead
+  const double *tcr = tc + (r0 + g) * Kp + q, *tsr = ts + (r0 + g) * Kp + q;
+  double nc[2] = {__ldg(tcr), __ldg(tcr + 8 * Kp)}, ns[2] = {__ldg(tsr), __ldg(tsr + 8 * Kp)};
+  for (int k0 = 1; k0 <= Kp; k0 += 4) {
+    const int k = k0 + q;  // 1 .. Kp: S_k at zf[x][k], D_k at zf[x][M-k] (table zero for k > H)
+    double ac[2] = {nc[0], nc[1]}, as[2] = {ns[0], ns[1]}, bs[4], bd[4];
+    if (k0 + 4 <= Kp) {
+      nc[0] = __ldg(tcr + k0 + 3);
+      nc[1] = __ldg(tcr + 8 * Kp + k0 + 3);
+      ns[0] = __ldg(tsr + k0 + 3);
+      ns[1] = __ldg(tsr + 8 * Kp + k0 + 3);
+    }
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) {
+      bs[ct] = zf[(8 * ct + g) * PZ + k];
+      bd[ct] = zf[(8 * ct + g) * PZ + M - k];
+    }
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) {
+        dmma(re[rt][ct], ac[rt], bs[ct]);
+        dmma(im[rt][ct], as[rt], bd[ct]);
+      }
+  }
+  const bool even = (M & 1) == 0;
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt) {
+    const int r = r0 + 8 * rt + g;
+    if (r >= MH) continue;
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int x = 8 * ct + 2 * q + i;
+        if (x0 + x >= s.N) continue;
+        double a = zf[x * PZ] + re[rt][ct][i];
+        if (even) a += (r & 1) ? -zf[x * PZ + M / 2] : zf[x * PZ + M / 2];
+        C[((long long)b * MH + r) * s.rx + x0 + x] = make_double2(a, -im[rt][ct][i]);
+      }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_zdft64_inv(Spec s, const double2 *__restrict__ C, double *__restrict__ R,
+                                                    const double *__restrict__ tc, const double *__restrict__ ts) {
+  extern __shared__ double zf[];  // Re [32][PZ], then Im [32][PZ]
+  const int M = s.M, MH = s.MH, Kp = zd64_kp(M), PZ = zd64_pitch(Kp + 1 > MH ? Kp + 1 : MH);
+  double *zr = zf, *zi = zf + 32 * PZ;
+  const int b = blockIdx.y, x0 = blockIdx.x * 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const bool xin = x0 + lane < s.N;
+  for (int k8 = warp * 8; k8 < PZ; k8 += nw * 8) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k8 + u;
+      v[u] = (k < MH && xin) ? __ldcs(C + ((long long)b * MH + k) * s.rx + x0 + lane) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k8 + u < PZ) {
+        zr[lane * PZ + k8 + u] = v[u].x;
+        zi[lane * PZ + k8 + u] = v[u].y;
+      }
+  }
+  __syncthreads();
+  const int npairs = M / 2 + 1;
+  const int p0 = 16 * warp;
+  if (p0 >= npairs) return;
+  const int g = lane >> 2, q = lane & 3;
+  double P[2][4][2] = {}, Q[2][4][2] = {};
+  const double *tcr = tc + (p0 + g) * Kp + q, *tsr = ts + (p0 + g) * Kp + q;
+  double nc[2] = {__ldg(tcr), __ldg(tcr + 8 * Kp)}, ns[2] = {__ldg(tsr), __ldg(tsr + 8 * Kp)};
+  for (int k0 = 1; k0 <= Kp; k0 += 4) {
+    const int k = k0 + q;
+    double ac[2] = {nc[0], nc[1]}, as[2] = {ns[0], ns[1]}, br[4], bi[4];
+    if (k0 + 4 <= Kp) {
+      nc[0] = __ldg(tcr + k0 + 3);
+      nc[1] = __ldg(tcr + 8 * Kp + k0 + 3);
+      ns[0] = __ldg(tsr + k0 + 3);
+      ns[1] = __ldg(tsr + 8 * Kp + k0 + 3);
+    }
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) {
+      br[ct] = zr[(8 * ct + g) * PZ + k];
+      bi[ct] = zi[(8 * ct + g) * PZ + k];
+    }
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) {
+        dmma(P[rt][ct], ac[rt], br[ct]);
+        dmma(Q[rt][ct], as[rt], bi[ct]);
+      }
+  }
+  const bool even = (M & 1) == 0;
+  const double invM = 1.0 / (double)M;
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt) {
+    const int pp = p0 + 8 * rt + g;
+    if (pp >= npairs) continue;
+    const int pm = M - pp;
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int x = 8 * ct + 2 * q + i;
+        if (x0 + x >= s.N) continue;
+        const double c0 = zr[x * PZ];
+        const double ny = even ? zr[x * PZ + M / 2] : 0.0;
+        const double y = (pp & 1) ? -ny : ny;
+        const double pv = P[rt][ct][i], qv = Q[rt][ct][i];
+        R[((long long)b * M + pp) * s.rx + x0 + x] = (c0 + 2.0 * (pv - qv) + y) * invM;
+        if (pm != pp && pm < M) R[((long long)b * M + pm) * s.rx + x0 + x] = (c0 + 2.0 * (pv + qv) + y) * invM;
+      }
+  }
+}
+
+// tables tc, ts ([MHp][Kp] each, in that order) of the FP64 z transforms
+void zdft64_tables(const Spec &s, std::vector<double> &t) {
+  const int M = s.M, H = (M - 1) / 2, rows = zd64_rows(M), Kp = zd64_kp(M), MH = s.MH;
+  t.assign(2 * (size_t)rows * Kp, 0.0);
+  for (int r = 0; r < MH && r < rows; ++r)
+    for (int k = 1; k <= H; ++k) {
+      const double a = 2.0 * M_PI * (double)(((long long)r * k) % M) / (double)M;
+      t[(size_t)r * Kp + (k - 1)] = cos(a);
+      t[(size_t)rows * Kp + (size_t)r * Kp + (k - 1)] = sin(a);
+    }
+}
+
+void launch_zdft64(const Spec &s, double *R, double2 *C, const double *tab, int inverse, cudaStream_t st) {
+  const int rows = zd64_rows(s.M), Kp = zd64_kp(s.M);
+  const double *tc = tab, *ts = tab + (size_t)rows * Kp;
+  const dim3 grid((s.N + 31) / 32, s.NM);
+  const int threads = 32 * (rows / 16);
+  if (!inverse) {
+    const size_t sm = (size_t)32 * zd64_pitch(s.M) * sizeof(double);
+    cudaFuncSetAttribute(k_zdft64_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_zdft64_fwd<<<grid, threads, sm, st>>>(s, R, C, tc, ts);
+  } else {
+    const int len = Kp + 1 > s.MH ? Kp + 1 : s.MH;
+    const size_t sm = (size_t)2 * 32 * zd64_pitch(len) * sizeof(double);
+    cudaFuncSetAttribute(k_zdft64_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_zdft64_inv<<<grid, threads, sm, st>>>(s, C, R, tc, ts);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Tridiagonal solve in y for every (kx, kz) mode, FP64 arithmetic.
 // Row b (= j-2) of the operator: diag dd[b] + kxx[kx] + kzz[kz] (row 0 of
 // mode (0,0) scaled by 3/2, initialization.f90:454), sub dl[b] = Dyy(j,j-1),
