@@ -1958,6 +1958,18 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
     if constexpr (sizeof(T) == 8) {
       // FP64 DNS: the TMA-fed kernel (results bit-identical to k_rhs_rk) where
       // its maps exist, unless rhs_pts = 1 asks for the global-load kernel
+      if (tl.rhs_pts == 2) {
+        const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 8;
+        dim3 gd = vol_grid(g.nx / 2, g.ny - 1, g.nz - 1, kc, 8);
+        dim3 blk(32, 8);
+        switch (mode) {
+          case 0: k_rhs_rk_pair<T, 0><<<gd, blk, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); break;
+          case 1: k_rhs_rk_pair<T, 1><<<gd, blk, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); break;
+          case 2: k_rhs_rk_pair<T, 2><<<gd, blk, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); break;
+          default: k_rhs_rk_pair<T, 3><<<gd, blk, 0, st>>>(g, m, U, V, W, Uo, Vo, Wo, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc); break;
+        }
+        return;
+      }
       if (tl.rhs_pts != 1 && mi && mo && mf) {
         const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 32;
         switch (mode) {
