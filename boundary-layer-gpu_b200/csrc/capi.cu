@@ -1690,7 +1690,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   if (t.dftz_rk != 0 && t.dftz_rk != 4 && t.dftz_rk != 8)
     return set_err(ctx, BLGPU_EINVAL, "tiles: dftz_rk %d not in {4,8}", t.dftz_rk);
   if (t.xfft < 0 || t.xfft > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: xfft %d not in {0,1,2}", t.xfft);
-  const int split = (ctx->fp64 || t.xfft == 1) ? 0 : xfft_split(ctx->spec.N);
+  const int split = t.xfft == 1 ? 0 : ctx->fp64 ? (xfft_split(ctx->spec.N) == 29 ? 29 : 0) : xfft_split(ctx->spec.N);
   if (t.xfft == 2 && !split)
     return set_err(ctx, BLGPU_EINVAL, "tiles: xfft 2 (two-pass x transforms) not built for N = %d in %s", ctx->spec.N,
                    ctx->fp64 ? "FP64" : "FP32");

@@ -107,17 +107,24 @@ template <> __device__ __forceinline__ const float2 *dft_consts<float>() { retur
 // root_off<R>(): the constants of the in-register DFTs of the two-pass FFT
 constexpr int ROOTS_N = 33 * 32 / 2 - 1;
 __constant__ float2 c_roots32[ROOTS_N];
+__constant__ double2 c_roots64[ROOTS_N];
 template <int R> __host__ __device__ constexpr int root_off() { return R * (R - 1) / 2 - 1; }
+template <typename V> __device__ __forceinline__ const V *roots();
+template <> __device__ __forceinline__ const float2 *roots<float2>() { return c_roots32; }
+template <> __device__ __forceinline__ const double2 *roots<double2>() { return c_roots64; }
 
 int upload_dft_constants() {
   {
     float2 h[ROOTS_N];
+    double2 hd[ROOTS_N];
     for (int R = 2; R <= 32; ++R)
       for (int e = 0; e < R; ++e) {
         const double a = 2.0 * M_PI * (double)e / (double)R;
         h[R * (R - 1) / 2 - 1 + e] = make_float2((float)cos(a), (float)sin(a));
+        hd[R * (R - 1) / 2 - 1 + e] = make_double2(cos(a), sin(a));
       }
     if (cudaMemcpyToSymbol(c_roots32, h, sizeof h) != cudaSuccess) return -1;
+    if (cudaMemcpyToSymbol(c_roots64, hd, sizeof hd) != cudaSuccess) return -1;
   }
   const int rad[9] = {5, 7, 11, 13, 17, 19, 23, 29, 31};
   double2 h64[DFT_RSUM];
@@ -325,81 +332,89 @@ __host__ __device__ constexpr int first_factor(int R) {
   return R;
 }
 
-// a * W_R^e (W_R = exp(-2 pi i / R)), or a * conj(W_R^e) for the inverse
-template <int R, bool INV>
-__device__ __forceinline__ float2 twr(float2 a, int e) {
-  if (e == 0) return a;
-  if (2 * e == R) return make_float2(-a.x, -a.y);
-  if (4 * e == R) return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
-  if (4 * e == 3 * R) return INV ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
-  const float2 w = c_roots32[root_off<R>() + e];  // (cos, sin)
-  return INV ? make_float2(a.x * w.x - a.y * w.y, a.y * w.x + a.x * w.y)
-             : make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+template <typename V, typename S> __device__ __forceinline__ V mkv(S a, S b) {
+  V r;
+  r.x = a;
+  r.y = b;
+  return r;
 }
 
-template <int R, bool INV>
-__device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
+// a * W_R^e (W_R = exp(-2 pi i / R)), or a * conj(W_R^e) for the inverse
+template <int R, bool INV, typename V>
+__device__ __forceinline__ V twr(V a, int e) {
+  if (e == 0) return a;
+  if (2 * e == R) return mkv<V>(-a.x, -a.y);
+  if (4 * e == R) return INV ? mkv<V>(-a.y, a.x) : mkv<V>(a.y, -a.x);
+  if (4 * e == 3 * R) return INV ? mkv<V>(a.y, -a.x) : mkv<V>(-a.y, a.x);
+  const V w = roots<V>()[root_off<R>() + e];  // (cos, sin)
+  return INV ? mkv<V>(a.x * w.x - a.y * w.y, a.y * w.x + a.x * w.y)
+             : mkv<V>(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+template <int R, bool INV, typename V>
+__device__ __forceinline__ void dft_reg(V (&x)[R]) {
+  typedef decltype(V().x) S;
   if constexpr (R == 2) {
-    const float2 a = x[0], b = x[1];
-    x[0] = make_float2(a.x + b.x, a.y + b.y);
-    x[1] = make_float2(a.x - b.x, a.y - b.y);
+    const V a = x[0], b = x[1];
+    x[0] = mkv<V>(a.x + b.x, a.y + b.y);
+    x[1] = mkv<V>(a.x - b.x, a.y - b.y);
   } else if constexpr (R == 3) {
-    const float s60 = 0.86602540378443864676f;
-    const float2 a0 = x[0], t1 = make_float2(x[1].x + x[2].x, x[1].y + x[2].y);
-    const float2 t2 = make_float2(x[1].x - x[2].x, x[1].y - x[2].y);
-    const float2 m = make_float2(a0.x - 0.5f * t1.x, a0.y - 0.5f * t1.y);
-    const float2 it = INV ? make_float2(-s60 * t2.y, s60 * t2.x) : make_float2(s60 * t2.y, -s60 * t2.x);
-    x[0] = make_float2(a0.x + t1.x, a0.y + t1.y);
-    x[1] = make_float2(m.x + it.x, m.y + it.y);
-    x[2] = make_float2(m.x - it.x, m.y - it.y);
+    const S s60 = (S)0.86602540378443864676;
+    const V a0 = x[0], t1 = mkv<V>(x[1].x + x[2].x, x[1].y + x[2].y);
+    const V t2 = mkv<V>(x[1].x - x[2].x, x[1].y - x[2].y);
+    const V m = mkv<V>(a0.x - (S)0.5 * t1.x, a0.y - (S)0.5 * t1.y);
+    const V it = INV ? mkv<V>(-s60 * t2.y, s60 * t2.x) : mkv<V>(s60 * t2.y, -s60 * t2.x);
+    x[0] = mkv<V>(a0.x + t1.x, a0.y + t1.y);
+    x[1] = mkv<V>(m.x + it.x, m.y + it.y);
+    x[2] = mkv<V>(m.x - it.x, m.y - it.y);
   } else if constexpr (R == 4) {
-    const float2 s0 = make_float2(x[0].x + x[2].x, x[0].y + x[2].y), s1 = make_float2(x[0].x - x[2].x, x[0].y - x[2].y);
-    const float2 s2 = make_float2(x[1].x + x[3].x, x[1].y + x[3].y), s3 = make_float2(x[1].x - x[3].x, x[1].y - x[3].y);
-    const float2 r3 = INV ? make_float2(-s3.y, s3.x) : make_float2(s3.y, -s3.x);  // +-i s3
-    x[0] = make_float2(s0.x + s2.x, s0.y + s2.y);
-    x[1] = make_float2(s1.x + r3.x, s1.y + r3.y);
-    x[2] = make_float2(s0.x - s2.x, s0.y - s2.y);
-    x[3] = make_float2(s1.x - r3.x, s1.y - r3.y);
+    const V s0 = mkv<V>(x[0].x + x[2].x, x[0].y + x[2].y), s1 = mkv<V>(x[0].x - x[2].x, x[0].y - x[2].y);
+    const V s2 = mkv<V>(x[1].x + x[3].x, x[1].y + x[3].y), s3 = mkv<V>(x[1].x - x[3].x, x[1].y - x[3].y);
+    const V r3 = INV ? mkv<V>(-s3.y, s3.x) : mkv<V>(s3.y, -s3.x);  // +-i s3
+    x[0] = mkv<V>(s0.x + s2.x, s0.y + s2.y);
+    x[1] = mkv<V>(s1.x + r3.x, s1.y + r3.y);
+    x[2] = mkv<V>(s0.x - s2.x, s0.y - s2.y);
+    x[3] = mkv<V>(s1.x - r3.x, s1.y - r3.y);
   } else if constexpr (first_factor(R) == R) {
     // prime R >= 5: X_k = x_0 + sum_q s_q cos - (+) i d_q sin, s, d = x_q +- x_{R-q}
     constexpr int H = (R - 1) / 2;
-    const float2 x0 = x[0];
-    float2 s[H], d[H];
+    const V x0 = x[0];
+    V s[H], d[H];
 #pragma unroll
     for (int q = 1; q <= H; ++q) {
-      s[q - 1] = make_float2(x[q].x + x[R - q].x, x[q].y + x[R - q].y);
-      d[q - 1] = make_float2(x[q].x - x[R - q].x, x[q].y - x[R - q].y);
+      s[q - 1] = mkv<V>(x[q].x + x[R - q].x, x[q].y + x[R - q].y);
+      d[q - 1] = mkv<V>(x[q].x - x[R - q].x, x[q].y - x[R - q].y);
     }
-    float2 y0 = x0;
+    V y0 = x0;
 #pragma unroll
-    for (int q = 0; q < H; ++q) y0 = make_float2(y0.x + s[q].x, y0.y + s[q].y);
+    for (int q = 0; q < H; ++q) y0 = mkv<V>(y0.x + s[q].x, y0.y + s[q].y);
     x[0] = y0;
-    const float2 *K = c_roots32 + root_off<R>();
+    const V *K = roots<V>() + root_off<R>();
 #pragma unroll
     for (int k = 1; k <= H; ++k) {
-      float ax = x0.x, ay = x0.y, bx = 0.f, by = 0.f;
+      S ax = x0.x, ay = x0.y, bx = 0, by = 0;
 #pragma unroll
       for (int q = 1; q <= H; ++q) {
         const int m = (q * k) % R;
-        const float c = K[m].x, sv = K[m].y;
+        const S c = K[m].x, sv = K[m].y;
         ax += s[q - 1].x * c;
         ay += s[q - 1].y * c;
         bx += d[q - 1].x * sv;
         by += d[q - 1].y * sv;
       }
       if (!INV) {
-        x[k] = make_float2(ax + by, ay - bx);
-        x[R - k] = make_float2(ax - by, ay + bx);
+        x[k] = mkv<V>(ax + by, ay - bx);
+        x[R - k] = mkv<V>(ax - by, ay + bx);
       } else {
-        x[k] = make_float2(ax - by, ay + bx);
-        x[R - k] = make_float2(ax + by, ay - bx);
+        x[k] = mkv<V>(ax - by, ay + bx);
+        x[R - k] = mkv<V>(ax + by, ay - bx);
       }
     }
   } else {
     // R = p m: m-point DFTs of the p decimated sequences x[p j + r], twiddles
     // W_R^{r k}, p-point DFTs across r: X[k + m q]
     constexpr int p = first_factor(R), m = R / p;
-    float2 y[p][m];
+    V y[p][m];
 #pragma unroll
     for (int r = 0; r < p; ++r)
 #pragma unroll
@@ -412,7 +427,7 @@ __device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
       for (int k = 1; k < m; ++k) y[r][k] = twr<R, INV>(y[r][k], r * k);
 #pragma unroll
     for (int k = 0; k < m; ++k) {
-      float2 t[p];
+      V t[p];
 #pragma unroll
       for (int r = 0; r < p; ++r) t[r] = y[r][k];
       dft_reg<p, INV>(t);
@@ -440,31 +455,32 @@ template <typename T, int MAXR> struct StockhamX {
 
 // Two-pass: N = A B (A, B <= 32), one buffer of max(N, A (B | 1)) values;
 // the table holds W_N^{n2 k1} at [k1][n2] (row pitch B)
-template <int A, int B> struct TwoPassX {
+template <int A, int B, typename T = float> struct TwoPassX {
   // LINE even keeps every line buffer 16-byte aligned
   static constexpr int N = A * B, SB = B | 1, LINE = ((N > A * SB ? N : A * SB) + 1) & ~1;
   static_assert(A <= 32 && B <= 32, "one lane per butterfly");
-  // up to 8 lines per CTA and three CTAs of 8 per SM: 80 registers, which
-  // hold the 29-point pass without spills and leave room for 24 warps per SM
-  static constexpr int max_threads = 256, min_blocks = 3;
+  // FP32: up to 8 lines per CTA and three CTAs of 8 per SM: 80 registers,
+  // which hold the 29-point pass without spills and leave room for 24 warps
+  // per SM; FP64: the pass's doubled registers, one CTA of up to 8 lines
+  static constexpr int max_threads = 256, min_blocks = sizeof(T) == 4 ? 3 : 1;
   static size_t line(int) { return LINE; }
   __device__ static size_t dline(int) { return LINE; }
-  __device__ static void fill(float2 *tw, const FftPlan<float> &pl, int tid, int nt) {
+  __device__ static void fill(T2<T> *tw, const FftPlan<T> &pl, int tid, int nt) {
     for (int t = tid; t < N; t += nt) {
       const int k1 = t / B, n2 = t - k1 * B;
       tw[t] = pl.tw[n2 * k1];  // n2 k1 < N
     }
   }
   template <bool INV>
-  __device__ static float2 *run(float2 *buf, const FftPlan<float> &, const float2 *tw, int lane) {
+  __device__ static T2<T> *run(T2<T> *buf, const FftPlan<T> &, const T2<T> *tw, int lane) {
     {
-      float2 x[A];
+      T2<T> x[A];
       if (lane < B) {
 #pragma unroll
         for (int n1 = 0; n1 < A; ++n1) x[n1] = buf[B * n1 + lane];
         dft_reg<A, INV>(x);
 #pragma unroll
-        for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<float, INV>(x[k1], tw[k1 * B + lane]);
+        for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<T, INV>(x[k1], tw[k1 * B + lane]);
       }
       __syncwarp();
       if (lane < B) {
@@ -473,7 +489,7 @@ template <int A, int B> struct TwoPassX {
       }
       __syncwarp();
     }
-    float2 y[B];
+    T2<T> y[B];
     if (lane < A) {
 #pragma unroll
       for (int n2 = 0; n2 < B; ++n2) y[n2] = buf[lane * SB + n2];
@@ -1516,11 +1532,14 @@ static void launch_idct_e(const Geo &g, const Spec &s, const FftPlan<T> &pl, con
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
                     int nw_req, int xfft, cudaStream_t st) {
-  const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
+  const int split = ((sizeof(T) == 4 && xfft != 1) || (sizeof(T) == 8 && xfft == 2)) ? xfft_split(s.N) : 0;
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
   const int grid = (ncl + nw - 1) / nw;
+  if constexpr (sizeof(T) == 8) {
+    if (split == 29) return launch_div_dct_e<T, TwoPassX<29, 28, T>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
+  }
   if constexpr (sizeof(T) == 4) {
     if (split == 29) return launch_div_dct_e<T, TwoPassX<29, 28>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
     if (split == 17) return launch_div_dct_e<T, TwoPassX<17, 30>>(g, s, pl, U, V, W, R, nw, sm, grid, st);
@@ -1552,11 +1571,14 @@ static bool idct2_fits(const Spec &s, int split) {
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft, int *err,
                  cudaStream_t st) {
-  const int split = (sizeof(T) == 4 && xfft != 1) ? xfft_split(s.N) : 0;
+  const int split = ((sizeof(T) == 4 && xfft != 1) || (sizeof(T) == 8 && xfft == 2)) ? xfft_split(s.N) : 0;
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;
+  if constexpr (sizeof(T) == 8) {
+    if (split == 29) return launch_idct_e<T, TwoPassX<29, 28, T>>(g, s, pl, R, p, nw, sm, grid, st);
+  }
   if constexpr (sizeof(T) == 4) {
     const bool fused = idct2_fits(s, split) && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
     if (split == 29 && fused) return launch_idct2<29, 28>(g, s, pl, R, p, nw, sm, grid, err, st);
