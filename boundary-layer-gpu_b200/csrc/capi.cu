@@ -1816,7 +1816,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
   Snapshot sn;
   int rc = snap_take(ctx, sn);
   if (rc) { snap_free(sn); return rc; }
-  const bool window = !ctx->fp64 && ctx->cfg.les_model == 0;  // FP32 register-window RHS kernel
+  const bool window = ctx->cfg.les_model == 0;  // DNS: register-window and TMA-fed RHS kernels
   std::vector<std::vector<int>> cand = {
       window ? std::vector<int>{8, 16, 32, 64} : std::vector<int>{4, 8, 16},  // rhs_kc
       {4, 8},                                                                  // rhs_by
@@ -1848,7 +1848,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
     if (knob == 5 && !ctx->zfrag && !ctx->utab) continue;  // no tensor-core z transform for this box
     if (knob == 6 && !window) continue;            // one RHS form outside the FP32 DNS path
     if (knob == 7 && !ctx->have_tmaps) continue;   // one y-solve without tensor maps
-    if (knob == 9 && (ctx->fp64 || !xfft_split(ctx->spec.N))) continue;  // one x-transform kernel
+    if (knob == 9 && (ctx->fp64 ? xfft_split(ctx->spec.N) != 29 : !xfft_split(ctx->spec.N))) continue;  // one x-transform kernel
     for (int v : cand[knob]) {
       Tiles t = best;
       int *f[10] = {&t.rhs_kc, &t.rhs_by, &t.dct_nw, &t.dftz_rk, &t.proj_by, &t.zdft, &t.rhs_pts, &t.thomas,

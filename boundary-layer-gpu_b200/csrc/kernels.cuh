@@ -26,10 +26,10 @@ struct Tiles {
   int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
   int rhs_pts;  // FP32 DNS RHS: 1 one point per thread, 2 two points, 3 two points packed in FP32x2
                 // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2);
-                // FP64 DNS: 1 the kernel of global loads, else the TMA-fed one where its maps exist
+                // FP64 DNS: 1 one point with global loads, 4 one point TMA-fed, 0 or 2 two points
   int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
-  int xfft;     // FP32 x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N)
+  int xfft;     // x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N; FP64: N = 812)
 };
 
 // boundary data (FP64, 1-based like the Fortran vectors)

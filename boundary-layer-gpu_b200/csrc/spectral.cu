@@ -1475,7 +1475,7 @@ int dct_lines_per_cta(int n, int elem_bytes, bool inverse, int split) {
   // of up to 4 lines per SM, FP64 (register-limited) two CTAs within 113 KB;
   // the two-pass kernels (80 registers, 24 warps per SM) take 6 lines per
   // CTA in both directions
-  if (split) return 6;
+  if (split) return elem_bytes == 8 ? 4 : 6;
   const size_t line = (size_t)n * 2 * elem_bytes * 2;  // ping-pong buffers of one complex line
   const size_t fixed = (size_t)n * 2 * elem_bytes * 2; // twiddle + DCT tables
   const size_t budget = elem_bytes == 8 ? 113 * 1024 : inverse ? 226 * 1024 : 75 * 1024;
@@ -1532,7 +1532,8 @@ static void launch_idct_e(const Geo &g, const Spec &s, const FftPlan<T> &pl, con
 template <typename T>
 void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *U, const T *V, const T *W, T *R,
                     int nw_req, int xfft, cudaStream_t st) {
-  const int split = ((sizeof(T) == 4 && xfft != 1) || (sizeof(T) == 8 && xfft == 2)) ? xfft_split(s.N) : 0;
+  int split = xfft != 1 ? xfft_split(s.N) : 0;
+  if (sizeof(T) == 8 && split != 29) split = 0;  // FP64 two-pass built for N = 812 only
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), false, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;  // complex lines
@@ -1571,7 +1572,8 @@ static bool idct2_fits(const Spec &s, int split) {
 template <typename T>
 void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw_req, int xfft, int *err,
                  cudaStream_t st) {
-  const int split = ((sizeof(T) == 4 && xfft != 1) || (sizeof(T) == 8 && xfft == 2)) ? xfft_split(s.N) : 0;
+  int split = xfft != 1 ? xfft_split(s.N) : 0;
+  if (sizeof(T) == 8 && split != 29) split = 0;  // FP64 two-pass built for N = 812 only
   const int nw = nw_req > 0 ? nw_req : dct_lines_per_cta(s.N, sizeof(T), true, split);
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;

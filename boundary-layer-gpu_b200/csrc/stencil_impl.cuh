@@ -1958,8 +1958,11 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
     if constexpr (sizeof(T) == 8) {
       // FP64 DNS: the TMA-fed kernel (results bit-identical to k_rhs_rk) where
       // its maps exist, unless rhs_pts = 1 asks for the global-load kernel
-      if (tl.rhs_pts == 2) {
-        const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 8;
+      // FP64 DNS: the two-point register window (rhs_pts 0 or 2, bit-identical to
+      // k_rhs_rk: its shared and carried terms are the same expressions), the
+      // TMA-fed one-point kernel (rhs_pts 4) or the global-load kernel (1)
+      if (tl.rhs_pts == 2 || tl.rhs_pts == 0) {
+        const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 16;
         dim3 gd = vol_grid(g.nx / 2, g.ny - 1, g.nz - 1, kc, 8);
         dim3 blk(32, 8);
         switch (mode) {
@@ -1970,7 +1973,7 @@ void launch_rhs_rk(const Geo &g, const MetT<T> &m, int mode, bool les, const T *
         }
         return;
       }
-      if (tl.rhs_pts != 1 && mi && mo && mf) {
+      if (tl.rhs_pts == 4 && mi && mo && mf) {
         const int kc = tl.rhs_kc > 0 ? tl.rhs_kc : 32;
         switch (mode) {
           case 0: launch_rhs_tma64<0>(g, m, *mi, *mo, *mf, F1u, F1v, F1w, Un, Vn, Wn, sc, c1, c2, kc, err, wait_limit, st); break;

@@ -255,12 +255,14 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * accumulators in tensor memory), rhs_pts (mixed-form DNS RHS: 1 = one
  * x-point per thread, 2 = two, 3 = two in packed FP32x2 instructions, 4 = as
  * 3 with every plane staged in shared memory by TMA, rhs_by then fixed at
- * 8; FP64 DNS: 1 = global loads, else TMA-fed planes, both bit-identical),
+ * 8; FP64 DNS, all bit-identical: 1 = one point, global loads, 4 = one point,
+ * TMA-fed planes, 2 = two points in a register window),
  * thomas (y-solve: 1 = register ring,
  * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
- * inverse DCT), xfft (mixed-form x transforms: 1 = Stockham mixed-radix FFT
- * in shared memory, any N; 2 = two-pass register FFT, built for
- * N = nx-2 = 812 (29 x 28), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9));
+ * inverse DCT), xfft (x transforms: 1 = Stockham mixed-radix FFT in shared
+ * memory, any N; 2 = two-pass register FFT, built for N = nx-2 = 812
+ * (29 x 28; both precisions), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9)
+ * (mixed form));
  * 0 = the built-in choice.
  * Values not passed keep their current setting.  All but zdft, rhs_pts and
  * xfft leave results unchanged; those change them at FP32 rounding level.  No counterpart in the

@@ -1,8 +1,8 @@
-"""The mixed form's x transforms (divergence + DCT-II, inverse DCT): the
-two-pass register FFT (N = nx-2 = A B, compile-time indices) against the
-Stockham shared-memory FFT and the FP64 path, at the built lengths
-(812 = 29 x 28, 510 = 17 x 30, 190 = 19 x 10, 126 = 14 x 9), for one
-projection and for a few steps."""
+"""The x transforms (divergence + DCT-II, inverse DCT): the two-pass
+register FFT (N = nx-2 = A B, compile-time indices) against the Stockham
+shared-memory FFT and the FP64 path, at the built lengths (812 = 29 x 28,
+510 = 17 x 30, 190 = 19 x 10, 126 = 14 x 9 in the mixed form; 812 in FP64),
+for one projection and for a few steps."""
 import numpy as np
 import pytest
 
@@ -87,7 +87,34 @@ def test_two_pass_refused_where_not_built(gpu):
         s.set_tiles(xfft=2)
     s.set_tiles(xfft=1)
     s.close()
-    f = cases.solver_for(noisy(814, 9, 12, 2), precision=FP64)
+    # FP64: the two-pass transform is built for N = 812 only
+    f = cases.solver_for(noisy(128, 9, 12, 2), precision=FP64)
     with pytest.raises(BlgpuError, match="xfft 2"):
         f.set_tiles(xfft=2)
     f.close()
+    f = cases.solver_for(noisy(814, 9, 12, 2), precision=FP64)
+    f.set_tiles(xfft=2)
+    assert f.tiles()["xfft"] == 2
+    f.close()
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(814, 9, 12), (814, 10, 13)])
+def test_fp64_two_pass_matches_stockham(gpu, nx, ny, nz):
+    """The FP64 instance of the two-pass transform (the FP64 default at
+    N = 812) against the FP64 Stockham transform: one projection agrees to
+    FP64 rounding, and every lines-per-CTA choice gives the same bits."""
+    c = noisy(nx, ny, nz, nx + 2 * ny)
+    out = {}
+    for name, t in (("two", dict(xfft=2)), ("stock", dict(xfft=1)), ("two3", dict(xfft=2, dct_nw=3, idct_nw=6))):
+        s = cases.solver_for(c, precision=FP64)
+        s.set_tiles(**t)
+        s.apply_boundary_conditions(1)
+        s.compute_projection_step(1)
+        out[name] = (s.download_state()[:3], s.rhs_p())
+        s.close()
+    (a, pa), (b, pb), (d, pd) = out["two"], out["stock"], out["two3"]
+    assert rel(pa, pb) < 1e-12
+    for x, y in zip(a, b):
+        assert rel(x, y) < 1e-13
+    for x, y in zip(a + (pa,), d + (pd,)):
+        assert np.array_equal(x, y)
