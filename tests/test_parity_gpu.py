@@ -49,13 +49,14 @@ def test_rhs_bit_identical(gpu, grid):
 
 @pytest.mark.parametrize("seed", [3, 4])
 def test_rhs_bit_identical_turbulent(gpu, seed):
-    """The FP64 RHS (TMA-fed kernel) on a stretched turbulent box: wall-refined
-    y spacings, 10 % noise, 15 M quotients, each formed from the reciprocal
-    tables by Markstein's correction, must equal the oracle's IEEE divisions
-    bit for bit; the global-load kernel (rhs_pts 1) too."""
+    """The FP64 RHS on a stretched turbulent box: wall-refined y spacings,
+    10 % noise, 15 M quotients, each formed from the reciprocal tables by
+    Markstein's correction, must equal the oracle's IEEE divisions bit for
+    bit, in every FP64 kernel: the two-point window (the default), the
+    one-point kernel of global loads (rhs_pts 1) and the TMA-fed one (4)."""
     c = cases.turbulent_case(nx=200, ny=65, nz=48, lx=20.0, ly=2.0, lz=3.0, seed=seed, cfl=-0.01)
     ref = oracle.oracle_for(c).rhs(c.U, c.V, c.W)
-    for pts in (0, 1):
+    for pts in (0, 1, 4):
         s = cases.solver_for(c)
         s.set_tiles(rhs_pts=pts)
         got = s.compute_rhs(c.U, c.V, c.W)
