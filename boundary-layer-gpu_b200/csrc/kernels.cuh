@@ -22,7 +22,7 @@ struct Tiles {
   int rhs_by;   // RHS block is 32 x rhs_by threads (0: 8)
   int dct_nw;   // complex lines (warps) per CTA of the forward DCT, up to 16 in FP32 (8 two-pass) and 8 in FP64 (0: built-in)
   int dftz_rk;  // z wavenumbers per warp in the z-DFT, 4 or 8 (0: 8)
-  int proj_by;  // projection block is 32 x proj_by threads (0: 8)
+  int proj_by;  // projection block is 32 x proj_by threads (0: 4)
   int zdft;     // mixed-form z transforms: 1 FP32 sums, 2 mma.sync TF32, 3 tcgen05 (0: tcgen05, else mma.sync, else sums)
   int rhs_pts;  // FP32 DNS RHS: 1 one point per thread, 2 two points, 3 two points packed in FP32x2
                 // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2);
