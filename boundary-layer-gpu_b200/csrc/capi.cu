@@ -1061,7 +1061,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
     ph_begin(ctx, PH_PROJECT);
     launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, mixed ? ctx->kz0g : nullptr,
                       S[0], S[1], S[2], (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
-    ph_end(ctx, rk_step == 1 ? 4 : 1);
+    ph_end(ctx, rk_step == 1 ? 2 : 1);
     return;
   }
   ph_begin(ctx, PH_DIVDCT);
@@ -1104,7 +1104,7 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   launch_project<T>(ctx->geo, m, (const T *)ctx->rhs_p, mixed ? ctx->kz0 : nullptr, mixed ? ctx->kz0g : nullptr,
                     S[0], S[1], S[2],
                     (T *)ctx->P, ctx->sc, rk_step == 1 ? 1 : 0, ctx->tiles, ctx->st);
-  ph_end(ctx, rk_step == 1 ? 4 : 1);
+  ph_end(ctx, rk_step == 1 ? 2 : 1);
 }
 
 template <typename T>

@@ -1213,24 +1213,45 @@ __global__ void __launch_bounds__(256) k_project_v(Geo g, MetT<T> m, const T *__
   }
 }
 
-// P ghost planes, projection.f90:78-83 (three ordered phases)
+// P ghost planes, projection.f90:78-83.  The source copies the x ghosts, then
+// the y ghosts (over every i, the x ghosts included), then the z ghosts (over
+// every i, j); each copy takes the neighbouring layer, so every ghost point
+// ends with the interior value at its clamped indices (1 -> 2, n -> n-1 in
+// each direction), which this launch writes in one pass: blocks take the x
+// faces over (j, k), the y faces over (i, k) and the z faces over (i, j);
+// edges and corners are written alike by each face they lie on, and no
+// source value is a ghost.
 template <typename T>
-__global__ void k_p_ghost(Geo g, T *__restrict__ P, int phase) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int b = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  if (phase == 0) {  // P(1,:,:)=P(2,:,:); P(nxg,:,:)=P(nxg-1,:,:) over (j,k)
-    if (a > g.nyg || b > g.nzg) return;
-    P[bidx(g, 1, a, b)] = P[bidx(g, 2, a, b)];
-    P[bidx(g, g.nxg, a, b)] = P[bidx(g, g.nxg - 1, a, b)];
-  } else if (phase == 1) {  // over (i,k)
-    if (a > g.nxg || b > g.nzg) return;
-    P[bidx(g, a, 1, b)] = P[bidx(g, a, 2, b)];
-    P[bidx(g, a, g.nyg, b)] = P[bidx(g, a, g.nyg - 1, b)];
-  } else {  // over (i,j)
-    if (a > g.nxg || b > g.nyg) return;
-    P[bidx(g, a, b, 1)] = P[bidx(g, a, b, 2)];
-    P[bidx(g, a, b, g.nzg)] = P[bidx(g, a, b, g.nzg - 1)];
+__global__ void k_p_ghost(Geo g, T *__restrict__ P, int bx, int by) {
+  int blk = blockIdx.x;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  auto cl = [](int v, int n) { return v == 1 ? 2 : v == n ? n - 1 : v; };
+  const int nxg = g.nxg, nyg = g.nyg, nzg = g.nzg;
+  if (blk < bx) {  // x faces, (j, k)
+    const int tj = (nyg + 31) / 32;
+    const int j = (blk % tj) * 32 + tx + 1, k = (blk / tj) * 8 + ty + 1;
+    if (j > nyg || k > nzg) return;
+    const int cj = cl(j, nyg), ck = cl(k, nzg);
+    P[bidx(g, 1, j, k)] = P[bidx(g, 2, cj, ck)];
+    P[bidx(g, nxg, j, k)] = P[bidx(g, nxg - 1, cj, ck)];
+    return;
   }
+  blk -= bx;
+  const int ti = (nxg + 31) / 32;
+  if (blk < by) {  // y faces, (i, k)
+    const int i = (blk % ti) * 32 + tx + 1, k = (blk / ti) * 8 + ty + 1;
+    if (i > nxg || k > nzg) return;
+    const int ci = cl(i, nxg), ck = cl(k, nzg);
+    P[bidx(g, i, 1, k)] = P[bidx(g, ci, 2, ck)];
+    P[bidx(g, i, nyg, k)] = P[bidx(g, ci, nyg - 1, ck)];
+    return;
+  }
+  blk -= by;  // z faces, (i, j)
+  const int i = (blk % ti) * 32 + tx + 1, j = (blk / ti) * 8 + ty + 1;
+  if (i > nxg || j > nyg) return;
+  const int ci = cl(i, nxg), cj = cl(j, nyg);
+  P[bidx(g, i, j, 1)] = P[bidx(g, ci, cj, 2)];
+  P[bidx(g, i, j, nzg)] = P[bidx(g, ci, cj, nzg - 1)];
 }
 
 // ---------------------------------------------------------------------------
@@ -2011,10 +2032,9 @@ void launch_project(const Geo &g, const MetT<T> &m, const T *p, const double *p0
   dim3 block(32, by), grid((ngrp + 31) / 32, (g.ny - 1 + by - 1) / by, g.nz - 1);
   k_project_v<T><<<grid, block, 0, st>>>(g, m, p, p0, p0g, U, V, W, P, sc, save_p);
   if (save_p) {
-    dim3 b2(32, 8);
-    k_p_ghost<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 0);
-    k_p_ghost<T><<<dim3((g.nxg + 31) / 32, (g.nzg + 7) / 8), b2, 0, st>>>(g, P, 1);
-    k_p_ghost<T><<<dim3((g.nxg + 31) / 32, (g.nyg + 7) / 8), b2, 0, st>>>(g, P, 2);
+    const int bx = ((g.nyg + 31) / 32) * ((g.nzg + 7) / 8), by = ((g.nxg + 31) / 32) * ((g.nzg + 7) / 8);
+    const int bz = ((g.nxg + 31) / 32) * ((g.nyg + 7) / 8);
+    k_p_ghost<T><<<bx + by + bz, 256, 0, st>>>(g, P, bx, by);
   }
 }
 
