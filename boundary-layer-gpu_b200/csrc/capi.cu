@@ -1144,7 +1144,7 @@ static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
     T **S = reinterpret_cast<T **>(ctx->S[a]);
     ph_begin(ctx, PH_DT);
     launch_dt<T>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
-    ph_end(ctx, 2);
+    ph_end(ctx, 1);
   }
   ph_begin(ctx, PH_MISC);
   launch_set_time(ctx->sc, 0, 0.0, ctx->st);

@@ -66,7 +66,7 @@ struct Scalars {
   double dU;       // last mass-flux correction
   unsigned long long lmax[3];  // compute_dt maxima (bit patterns of >=0 doubles)
   int err;         // sticky device error flag
-  int pad;
+  unsigned int dt_arrived;  // blocks of the compute_dt reduction that have finished (the last one resets it)
 };
 
 template <typename T> struct vec2;

@@ -1526,9 +1526,27 @@ __global__ void k_bc_mass(Geo g, T *__restrict__ U, const Scalars *__restrict__ 
 // maximum of their IEEE bit patterns is their maximum and atomicMax is exact
 // and order independent.
 // ---------------------------------------------------------------------------
+// dt from the maxima of the reduction (time_integration.f90:580-590), by the
+// last block to finish: the arrival counter after every block's atomics
+__device__ __forceinline__ void dt_finish_last(Scalars *sc, double cfl, double dtvis) {
+  __threadfence();
+  const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+  if (atomicAdd(&sc->dt_arrived, 1u) != nb - 1) return;
+  __threadfence();
+  const double cfla = fabs(cfl);
+  const double lu = __longlong_as_double((long long)atomicOr(&sc->lmax[0], 0ull));
+  const double lv = __longlong_as_double((long long)atomicOr(&sc->lmax[1], 0ull));
+  const double lw = __longlong_as_double((long long)atomicOr(&sc->lmax[2], 0ull));
+  const double dt_conv = fmin(fmin(cfla * lu, cfla * lv), cfla * lw);
+  sc->dt = fmin(dt_conv, dtvis);
+  sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
+  sc->dt_arrived = 0u;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ U, const T *__restrict__ V,
-                                                   const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk) {
+                                                   const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk,
+                                                   double cfl, double dtvis) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   double mu = 0.0, mv = 0.0, mw = 0.0;
@@ -1576,6 +1594,7 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
     atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
     atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
     atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
+    dt_finish_last(sc, cfl, dtvis);
   }
 }
 
@@ -1584,7 +1603,8 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
 // k loop unrolled, so that a thread keeps a dozen loads in flight.
 template <typename T>  // float
 __global__ void __launch_bounds__(256) k_dt_reduce4(Geo g, const T *__restrict__ U, const T *__restrict__ V,
-                                                    const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk) {
+                                                    const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk,
+                                                    double cfl, double dtvis) {
   const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x) + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   double mu = 0.0, mv = 0.0, mw = 0.0;
@@ -1648,20 +1668,12 @@ __global__ void __launch_bounds__(256) k_dt_reduce4(Geo g, const T *__restrict__
     atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
     atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
     atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
+    dt_finish_last(sc, cfl, dtvis);
   }
 }
 
 // time_integration.f90:560-575 (dt = min(dt_conv, dt_vis)); also arms the
 // accumulators for the next call and records to = t for the RK substeps.
-static __global__ void k_dt_finish(Scalars *sc, double cfl, double dtvis) {
-  double cfla = fabs(cfl);
-  double lu = __longlong_as_double((long long)sc->lmax[0]);
-  double lv = __longlong_as_double((long long)sc->lmax[1]);
-  double lw = __longlong_as_double((long long)sc->lmax[2]);
-  double dt_conv = fmin(fmin(cfla * lu, cfla * lv), cfla * lw);
-  sc->dt = fmin(dt_conv, dtvis);
-  sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
-}
 
 #ifdef BLGPU_STENCIL_PRIMARY
 __global__ void k_set_time(Scalars *sc, int phase, double coef) {
@@ -2067,14 +2079,13 @@ void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, do
   if constexpr (sizeof(T) == 4) {
     if (vec) {
       dim3 grid = vol_grid((g.nxg - 2 + 3) / 4, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
-      k_dt_reduce4<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk);
+      k_dt_reduce4<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis);
     }
   }
   if (!vec) {
     dim3 grid = vol_grid(g.nxg - 2, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
-    k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk);
+    k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis);
   }
-  k_dt_finish<<<1, 1, 0, st>>>(sc, cfl, dtvis);
 }
 
 #ifdef BLGPU_STENCIL_PRIMARY
