@@ -1140,15 +1140,16 @@ static int enq_wall_model(blgpu_ctx *ctx, const T *U, const T *W) {
 template <typename T>
 static int enq_step(blgpu_ctx *ctx, int a, bool with_dt) {
   const int b = (a + 1) % 3, c = (a + 2) % 3;
-  if (with_dt && ctx->cfg.cfl > 0) {
+  if (with_dt && ctx->cfg.cfl > 0) {  // dt, and the step's start time saved by the same launch
     T **S = reinterpret_cast<T **>(ctx->S[a]);
     ph_begin(ctx, PH_DT);
-    launch_dt<T>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+    launch_dt<T>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, true, ctx->st);
+    ph_end(ctx, 1);
+  } else {
+    ph_begin(ctx, PH_MISC);
+    launch_set_time(ctx->sc, 0, 0.0, ctx->st);
     ph_end(ctx, 1);
   }
-  ph_begin(ctx, PH_MISC);
-  launch_set_time(ctx->sc, 0, 0.0, ctx->st);
-  ph_end(ctx, 1);
   if (ctx->lund.mode) {  // Lund inflow once per step from the step's start fields
     T **S = reinterpret_cast<T **>(ctx->S[a]);
     ph_begin(ctx, PH_BC);
@@ -1280,10 +1281,10 @@ int blgpu_compute_dt(blgpu_ctx *ctx, double *dt) {
     CK(cudaMemcpy(&ctx->sc->dt, &v, sizeof v, cudaMemcpyHostToDevice));
   } else if (ctx->fp64) {
     double **S = reinterpret_cast<double **>(ctx->S[ctx->cur]);
-    launch_dt<double>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+    launch_dt<double>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, false, ctx->st);
   } else {
     float **S = reinterpret_cast<float **>(ctx->S[ctx->cur]);
-    launch_dt<float>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, ctx->st);
+    launch_dt<float>(ctx->geo, S[0], S[1], S[2], ctx->sc, ctx->cfg.cfl, ctx->dtvis, false, ctx->st);
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));

@@ -88,9 +88,11 @@ int bc_x_parts(const Geo &g);
 template <typename T>
 void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, const T *Vo, const T *Wo,
                Scalars *sc, double rkt, double *qx_part, double qy, double length_y, cudaStream_t st);
+// save_time: the reduction's last block also saves the step's start time
+// (sc->to = sc->t, what launch_set_time phase 0 does)
 template <typename T>
 void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
-               cudaStream_t st);
+               bool save_time, cudaStream_t st);
 void launch_set_time(Scalars *sc, int phase, double coef, cudaStream_t st);
 template <typename T>
 void launch_maxdiv(const Geo &g, const T *U, const T *V, const T *W, unsigned long long *out, cudaStream_t st);

@@ -1528,7 +1528,7 @@ __global__ void k_bc_mass(Geo g, T *__restrict__ U, const Scalars *__restrict__ 
 // ---------------------------------------------------------------------------
 // dt from the maxima of the reduction (time_integration.f90:580-590), by the
 // last block to finish: the arrival counter after every block's atomics
-__device__ __forceinline__ void dt_finish_last(Scalars *sc, double cfl, double dtvis) {
+__device__ __forceinline__ void dt_finish_last(Scalars *sc, double cfl, double dtvis, int save_time) {
   __threadfence();
   const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
   if (atomicAdd(&sc->dt_arrived, 1u) != nb - 1) return;
@@ -1541,12 +1541,13 @@ __device__ __forceinline__ void dt_finish_last(Scalars *sc, double cfl, double d
   sc->dt = fmin(dt_conv, dtvis);
   sc->lmax[0] = sc->lmax[1] = sc->lmax[2] = 0ull;
   sc->dt_arrived = 0u;
+  if (save_time) sc->to = sc->t;  // the step's start time (k_set_time phase 0)
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ U, const T *__restrict__ V,
                                                    const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk,
-                                                   double cfl, double dtvis) {
+                                                   double cfl, double dtvis, int save_time) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   double mu = 0.0, mv = 0.0, mw = 0.0;
@@ -1594,7 +1595,7 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
     atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
     atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
     atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
-    dt_finish_last(sc, cfl, dtvis);
+    dt_finish_last(sc, cfl, dtvis, save_time);
   }
 }
 
@@ -1604,7 +1605,7 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
 template <typename T>  // float
 __global__ void __launch_bounds__(256) k_dt_reduce4(Geo g, const T *__restrict__ U, const T *__restrict__ V,
                                                     const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk,
-                                                    double cfl, double dtvis) {
+                                                    double cfl, double dtvis, int save_time) {
   const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x) + 2;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   double mu = 0.0, mv = 0.0, mw = 0.0;
@@ -1668,7 +1669,7 @@ __global__ void __launch_bounds__(256) k_dt_reduce4(Geo g, const T *__restrict__
     atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
     atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
     atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
-    dt_finish_last(sc, cfl, dtvis);
+    dt_finish_last(sc, cfl, dtvis, save_time);
   }
 }
 
@@ -2071,7 +2072,7 @@ void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, co
 
 template <typename T>
 void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
-               cudaStream_t st) {
+               bool save_time, cudaStream_t st) {
   const int kchunk = 32;
   const bool vec = sizeof(T) == 4 && (g.px & 3) == 0 &&
                    ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(W)) &
@@ -2079,12 +2080,12 @@ void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, do
   if constexpr (sizeof(T) == 4) {
     if (vec) {
       dim3 grid = vol_grid((g.nxg - 2 + 3) / 4, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
-      k_dt_reduce4<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis);
+      k_dt_reduce4<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis, save_time ? 1 : 0);
     }
   }
   if (!vec) {
     dim3 grid = vol_grid(g.nxg - 2, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
-    k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis);
+    k_dt_reduce<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis, save_time ? 1 : 0);
   }
 }
 
@@ -2129,7 +2130,8 @@ void launch_law_of_wall(const Geo &g, const T *U, double *utau, int *iters, int 
                                   const Scalars *, int, const Tiles &, cudaStream_t);                               \
   template void launch_bc<T>(const Geo &, const BcData &, T *, T *, T *, const T *, const T *, const T *,         \
                              Scalars *, double, double *, double, double, cudaStream_t);                            \
-  template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, cudaStream_t); \
+  template void launch_dt<T>(const Geo &, const T *, const T *, const T *, Scalars *, double, double, bool,        \
+                             cudaStream_t);                                                                         \
   template void launch_maxdiv<T>(const Geo &, const T *, const T *, const T *, unsigned long long *, cudaStream_t); \
   template void launch_smagorinsky<T>(const Geo &, const T *, const T *, const T *, const double *, T *,            \
                                       cudaStream_t);                                                                \
