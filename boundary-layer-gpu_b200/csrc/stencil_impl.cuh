@@ -1286,10 +1286,12 @@ __device__ __forceinline__ double mode_sum(const double2 *__restrict__ q, int ld
 //   (5) wall rows U(:,1,:) = -U(:,2,:), V(:,1,:) = 0, W(:,1,:) = -W(:,2,:)
 //     (or the wall model's Neumann rows) from what (1)-(3) left in row 2.
 // k_bc_all writes each boundary point once with that final value, so its
-// three segments of blocks (x planes; z ghosts of interior columns; y rows of
-// interior columns) read nothing another thread writes.  The x-plane blocks
-// also form the x mass-flux partials; the last of them sums the partials in
-// block order and leaves the correction in sc->dU for k_bc_mass (6).
+// four segments of blocks (x planes of U; x planes of V and W; z ghosts of
+// interior columns; y rows of interior columns) read nothing another thread
+// writes.  The U x-plane blocks also form the x mass-flux partials; the last
+// of them sums the partials in block order and leaves the correction in
+// sc->dU for k_bc_mass (6).  A thread issues its loads before its stores, so
+// that it waits for memory about once.
 template <typename T> struct BcX {
   // (1): U, V, W at i = 1 of row j, plane k
   __device__ static double in_u(const Geo &g, const BcData &bc, int j, int k, double t) {
@@ -1352,9 +1354,9 @@ template <typename T> struct BcX {
   }
 };
 
-struct BcGrid {  // block counts of the three segments (32 x 8 tiles)
-  int nx_blocks, nz_blocks, ny_blocks;
-  int x_tiles, zi_tiles, yi_tiles;  // tiles along the first dimension of each segment
+struct BcGrid {  // block counts of the segments (32 x 8 tiles)
+  int nx_blocks, nz_blocks, ny_blocks;  // U x planes (V and W take 2 nx_blocks more); z ghosts; y rows
+  int x_tiles, zi_tiles, yi_tiles;      // tiles along the first dimension of each segment
 };
 
 template <typename T>
@@ -1367,69 +1369,76 @@ __global__ void __launch_bounds__(256) k_bc_all(Geo g, BcData bc, BcGrid G, T *_
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int nx = g.nx, nxg = g.nxg, ny = g.ny, nyg = g.nyg, nz = g.nz, nzg = g.nzg;
   typedef BcX<T> X;
+  if (blk >= G.nx_blocks && blk < 3 * G.nx_blocks) {
+    // ---- x planes of V (the first nx_blocks) and W, thread (j, k) ----
+    const int bb = (blk - G.nx_blocks) % G.nx_blocks;
+    const int j = (bb % G.x_tiles) * 32 + tx + 1, k = (bb / G.x_tiles) * 8 + ty + 1;
+    if (j > nyg || k > nzg) return;
+    const double t = sc->t, cc = rkt * sc->dt * bc.U_top[nx];
+    if (blk < 2 * G.nx_blocks) {
+      if (j > ny) return;  // V at i = 1, nxg-1, nxg
+      const int kv = X::ks_uv(g, k);
+      T v1, vn, vn1;
+      if (j == 1) {
+        v1 = vn = vn1 = (T)0;
+      } else if (j == ny) {
+        v1 = (T)bc.V_top[1];
+        vn = (T)bc.V_top[nxg - 1];
+        vn1 = (T)bc.V_top[nxg];
+      } else {
+        v1 = (T)X::in_v(g, bc, j, kv, t);
+        vn = vn1 = X::out_vw(g, Vo, j, kv, cc);
+      }
+      const long long a = bidx(g, nxg - 1, j, k);
+      V[bidx(g, 1, j, k)] = v1;
+      V[a] = vn;
+      V[a + 1] = vn1;
+    } else {
+      if (k > nz) return;  // W at i = 1, nxg-1, nxg
+      const int kw = X::ks_w(g, k);
+      T w1, wn, wn1;
+      if (j == nyg) {
+        w1 = (T)bc.W_top[1];
+        wn = (T)bc.W_top[nxg - 1];
+        wn1 = (T)bc.W_top[nxg];
+      } else if (j == 1) {
+        w1 = X::wall_w(g, bc, (T)X::in_w(g, bc, 2, kw, t), 1, k);
+        const T o2 = X::out_vw(g, Wo, 2, kw, cc);
+        wn = X::wall_w(g, bc, o2, nxg - 1, k);
+        wn1 = X::wall_w(g, bc, o2, nxg, k);
+      } else {
+        w1 = (T)X::in_w(g, bc, j, kw, t);
+        wn = wn1 = X::out_vw(g, Wo, j, kw, cc);
+      }
+      const long long a = bidx(g, nxg - 1, j, k);
+      W[bidx(g, 1, j, k)] = w1;
+      W[a] = wn;
+      W[a + 1] = wn1;
+    }
+    return;
+  }
   if (blk < G.nx_blocks) {
-    // ---- x planes, thread (j, k) ----
+    // ---- x planes of U, thread (j, k) ----
     const int j = (blk % G.x_tiles) * 32 + tx + 1, k = (blk / G.x_tiles) * 8 + ty + 1;
     double q = 0.0;
     if (j <= nyg && k <= nzg) {
       const double t = sc->t, cc = rkt * sc->dt * bc.U_top[nx];
       // U at i = 1 and nx-1 (k_bc_mass sets i = nx)
-      {
-        const int ku = X::ks_uv(g, k);
-        T u1, un;
-        if (j == nyg) {
-          u1 = (T)bc.U_top[1];
-          un = (T)bc.U_top[nx - 1];
-        } else if (j == 1) {
-          u1 = X::wall_u(g, bc, (T)X::in_u(g, bc, 2, ku, t), 1, k);
-          un = X::wall_u(g, bc, X::out_u(g, Uo, 2, ku, cc), nx - 1, k);
-        } else {
-          u1 = (T)X::in_u(g, bc, j, ku, t);
-          un = X::out_u(g, Uo, j, ku, cc);
-          if (j <= nyg - 1 && k >= 2 && k <= nzg - 2) q = ((double)u1 - (double)un) * g.ay.F[j];  // (:242-246)
-        }
-        U[bidx(g, 1, j, k)] = u1;
-        U[bidx(g, nx - 1, j, k)] = un;
+      const int ku = X::ks_uv(g, k);
+      T u1, un;
+      if (j == nyg) {
+        u1 = (T)bc.U_top[1];
+        un = (T)bc.U_top[nx - 1];
+      } else if (j == 1) {
+        u1 = X::wall_u(g, bc, (T)X::in_u(g, bc, 2, ku, t), 1, k);
+        un = X::wall_u(g, bc, X::out_u(g, Uo, 2, ku, cc), nx - 1, k);
+      } else {
+        u1 = (T)X::in_u(g, bc, j, ku, t);
+        un = X::out_u(g, Uo, j, ku, cc);
+        if (j <= nyg - 1 && k >= 2 && k <= nzg - 2) q = ((double)u1 - (double)un) * g.ay.F[j];  // (:242-246)
       }
-      if (j <= ny) {  // V at i = 1, nxg-1, nxg
-        const int kv = X::ks_uv(g, k);
-        T v1, vn, vn1;
-        if (j == 1) {
-          v1 = vn = vn1 = (T)0;
-        } else if (j == ny) {
-          v1 = (T)bc.V_top[1];
-          vn = (T)bc.V_top[nxg - 1];
-          vn1 = (T)bc.V_top[nxg];
-        } else {
-          v1 = (T)X::in_v(g, bc, j, kv, t);
-          vn = vn1 = X::out_vw(g, Vo, j, kv, cc);
-        }
-        const long long a = bidx(g, nxg - 1, j, k);
-        V[bidx(g, 1, j, k)] = v1;
-        V[a] = vn;
-        V[a + 1] = vn1;
-      }
-      if (k <= nz) {  // W at i = 1, nxg-1, nxg
-        const int kw = X::ks_w(g, k);
-        T w1, wn, wn1;
-        if (j == nyg) {
-          w1 = (T)bc.W_top[1];
-          wn = (T)bc.W_top[nxg - 1];
-          wn1 = (T)bc.W_top[nxg];
-        } else if (j == 1) {
-          w1 = X::wall_w(g, bc, (T)X::in_w(g, bc, 2, kw, t), 1, k);
-          const T o2 = X::out_vw(g, Wo, 2, kw, cc);
-          wn = X::wall_w(g, bc, o2, nxg - 1, k);
-          wn1 = X::wall_w(g, bc, o2, nxg, k);
-        } else {
-          w1 = (T)X::in_w(g, bc, j, kw, t);
-          wn = wn1 = X::out_vw(g, Wo, j, kw, cc);
-        }
-        const long long a = bidx(g, nxg - 1, j, k);
-        W[bidx(g, 1, j, k)] = w1;
-        W[a] = wn;
-        W[a + 1] = wn1;
-      }
+      U[bidx(g, 1, j, k)] = u1;
+      U[bidx(g, nx - 1, j, k)] = un;
     }
     // deterministic block reduction of the x mass-flux partials (:242-246)
     __shared__ double red[256];
@@ -1470,40 +1479,56 @@ __global__ void __launch_bounds__(256) k_bc_all(Geo g, BcData bc, BcGrid G, T *_
     }
     return;
   }
-  blk -= G.nx_blocks;
+  blk -= 3 * G.nx_blocks;
   const long long P = g.plane;
   if (blk < G.nz_blocks) {
     // ---- z ghost planes of the interior columns, thread (i, j): (3) ----
     const int i = (blk % G.zi_tiles) * 32 + tx + 2, j = (blk / G.zi_tiles) * 8 + ty + 2;
     if (i > nxg - 2 || j > nyg - 1) return;
+    // sources: planes nzg-2, 2, 3 (W: nz-1, 2); targets: 1, nzg-1, nzg (W: 1, nz)
     const long long c1 = bidx(g, i, j, 1);
-    if (i <= nx - 2) {
-      U[c1] = U[c1 + (nzg - 3) * P];
-      U[c1 + (nzg - 2) * P] = U[c1 + 1 * P];
-      U[c1 + (nzg - 1) * P] = U[c1 + 2 * P];
+    const bool du = i <= nx - 2, dv = j <= ny - 1;
+    T u0 = 0, u1 = 0, u2 = 0, v0 = 0, v1 = 0, v2 = 0;
+    if (du) {
+      u0 = U[c1 + (nzg - 3) * P];
+      u1 = U[c1 + 1 * P];
+      u2 = U[c1 + 2 * P];
     }
-    if (j <= ny - 1) {
-      V[c1] = V[c1 + (nzg - 3) * P];
-      V[c1 + (nzg - 2) * P] = V[c1 + 1 * P];
-      V[c1 + (nzg - 1) * P] = V[c1 + 2 * P];
+    if (dv) {
+      v0 = V[c1 + (nzg - 3) * P];
+      v1 = V[c1 + 1 * P];
+      v2 = V[c1 + 2 * P];
     }
-    W[c1] = W[c1 + (nz - 2) * P];
-    W[c1 + (nz - 1) * P] = W[c1 + 1 * P];
+    const T w0 = W[c1 + (nz - 2) * P], w1 = W[c1 + 1 * P];
+    if (du) {
+      U[c1] = u0;
+      U[c1 + (nzg - 2) * P] = u1;
+      U[c1 + (nzg - 1) * P] = u2;
+    }
+    if (dv) {
+      V[c1] = v0;
+      V[c1 + (nzg - 2) * P] = v1;
+      V[c1 + (nzg - 1) * P] = v2;
+    }
+    W[c1] = w0;
+    W[c1 + (nz - 1) * P] = w1;
     return;
   }
   blk -= G.nz_blocks;
   // ---- top and wall rows of the interior columns, thread (i, k): (4), (5) ----
   const int i = (blk % G.yi_tiles) * 32 + tx + 2, k = (blk / G.yi_tiles) * 8 + ty + 1;
   if (i > nxg - 2 || k > nzg) return;
-  if (i <= nx - 2) {
+  const bool du = i <= nx - 2, dw = k <= nz;
+  const T u2 = du ? U[bidx(g, i, 2, X::ks_uv(g, k))] : (T)0, w2 = dw ? W[bidx(g, i, 2, X::ks_w(g, k))] : (T)0;
+  if (du) {
     U[bidx(g, i, nyg, k)] = (T)bc.U_top[i];
-    U[bidx(g, i, 1, k)] = X::wall_u(g, bc, U[bidx(g, i, 2, X::ks_uv(g, k))], i, k);
+    U[bidx(g, i, 1, k)] = X::wall_u(g, bc, u2, i, k);
   }
   V[bidx(g, i, ny, k)] = (T)bc.V_top[i];
   V[bidx(g, i, 1, k)] = (T)0;
-  if (k <= nz) {
+  if (dw) {
     W[bidx(g, i, nyg, k)] = (T)bc.W_top[i];
-    W[bidx(g, i, 1, k)] = X::wall_w(g, bc, W[bidx(g, i, 2, X::ks_w(g, k))], i, k);
+    W[bidx(g, i, 1, k)] = X::wall_w(g, bc, w2, i, k);
   }
 }
 
@@ -2065,7 +2090,7 @@ void launch_bc(const Geo &g, const BcData &bc, T *U, T *V, T *W, const T *Uo, co
   G.nz_blocks = G.zi_tiles * ((g.nyg - 2 + 7) / 8);
   G.yi_tiles = G.zi_tiles;
   G.ny_blocks = G.yi_tiles * ((g.nzg + 7) / 8);
-  k_bc_all<T><<<G.nx_blocks + G.nz_blocks + G.ny_blocks, 256, 0, st>>>(g, bc, G, U, V, W, Uo, Vo, Wo, sc, rkt,
+  k_bc_all<T><<<3 * G.nx_blocks + G.nz_blocks + G.ny_blocks, 256, 0, st>>>(g, bc, G, U, V, W, Uo, Vo, Wo, sc, rkt,
                                                                          qx_part, qy, length_y);
   k_bc_mass<T><<<dim3((g.nyg + 31) / 32, (g.nzg + 7) / 8), dim3(32, 8), 0, st>>>(g, U, sc);
 }
