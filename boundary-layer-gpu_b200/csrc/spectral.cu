@@ -716,24 +716,24 @@ __global__ void __launch_bounds__(E::max_threads, E::min_blocks) k_idct(Geo g, S
   }
 }
 
-// Inverse DCT with the two-pass FFT (FP32), the steps around the transform
+// Inverse DCT with the two-pass FFT (both precisions), the steps around the transform
 // folded into its passes: one bulk copy brings the two rows of R into the
 // line buffer; pass 1 forms its inputs Z_n = V_A + i V_B from them in
 // registers; pass 2 writes its outputs from registers straight to the box
 // positions (Z_n holds the points i = 2n, or 2N-1-2n for 2n >= N).  The
 // copy's wait is bounded: when it runs out, bit 16 of the device flag is set
 // and the line is left unwritten.
-template <int A, int B>
-__global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> pl, const float *__restrict__ R,
-                                                  float *__restrict__ p, int *__restrict__ err) {
-  using E = TwoPassX<A, B>;
+template <int A, int B, typename T = float>
+__global__ void __launch_bounds__(TwoPassX<A, B, T>::max_threads, TwoPassX<A, B, T>::min_blocks)
+    k_idct2(Geo g, Spec s, FftPlan<T> pl, const T *__restrict__ R, T *__restrict__ p, int *__restrict__ err) {
+  using E = TwoPassX<A, B, T>;
   using namespace tma;
   constexpr int N = E::N, SB = E::SB, LINE = E::LINE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  float2 *tw = reinterpret_cast<float2 *>(smem_raw);
-  float2 *post = tw + N;
-  float2 *buf = post + N + (size_t)warp * LINE;
+  T2<T> *tw = reinterpret_cast<T2<T> *>(smem_raw);
+  T2<T> *post = tw + N;
+  T2<T> *buf = post + N + (size_t)warp * LINE;
   uint64_t *bar = reinterpret_cast<uint64_t *>(
       reinterpret_cast<unsigned char *>(post + N + (size_t)nw * LINE) + 4 * ((N + 3) / 4 * 4)) + warp;
   E::fill(tw, pl, threadIdx.x, blockDim.x);
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> 
     mbar_init(bar, 1);
     mbar_init_fence();
     // rows q and q+1 (rx apart) as one block, the length rounded up to 16 bytes
-    const uint32_t bytes = 4u * (uint32_t)((hb ? s.rx : 0) + ((N + 3) & ~3));
+    const uint32_t bytes = (uint32_t)sizeof(T) * (uint32_t)((hb ? s.rx : 0) + ((N + 3) & ~3));
     mbar_expect_tx(bar, bytes);
     bulk_load(buf, R + (long long)q * s.rx, bytes, bar);
   }
@@ -758,25 +758,25 @@ __global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> 
     }
     return;
   }
-  const float *ra = reinterpret_cast<const float *>(buf);
-  const float *rb = ra + s.rx;
+  const T *ra = reinterpret_cast<const T *>(buf);
+  const T *rb = ra + s.rx;
   {
     // pass 1 (lane n2 < B): Z_n for n = B n1 + n2, V_n = exp(+i pi n/2N) (X_n - i X_{N-n})
-    float2 x[A];
+    T2<T> x[A];
     if (lane < B) {
 #pragma unroll
       for (int n1 = 0; n1 < A; ++n1) {
         const int n = B * n1 + lane;
-        const float xa = ra[n], xan = n ? ra[N - n] : 0.f;
-        const float xb = hb ? rb[n] : 0.f, xbn = (hb && n) ? rb[N - n] : 0.f;
-        const float2 e = make_float2(post[n].x, -post[n].y);
-        const float2 va = cmul<float>(e, make_float2(xa, -xan));
-        const float2 vb = cmul<float>(e, make_float2(xb, -xbn));
-        x[n1] = make_float2(va.x - vb.y, va.y + vb.x);
+        const T xa = ra[n], xan = n ? ra[N - n] : (T)0;
+        const T xb = hb ? rb[n] : (T)0, xbn = (hb && n) ? rb[N - n] : (T)0;
+        const T2<T> e = mk<T>(post[n].x, -post[n].y);
+        const T2<T> va = cmul<T>(e, mk<T>(xa, -xan));
+        const T2<T> vb = cmul<T>(e, mk<T>(xb, -xbn));
+        x[n1] = mk<T>(va.x - vb.y, va.y + vb.x);
       }
       dft_reg<A, true>(x);
 #pragma unroll
-      for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<float, true>(x[k1], tw[k1 * B + lane]);
+      for (int k1 = 1; k1 < A; ++k1) x[k1] = twm<T, true>(x[k1], tw[k1 * B + lane]);
     }
     __syncwarp();  // every read of the raw rows is done
     if (lane < B) {
@@ -786,11 +786,11 @@ __global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> 
     __syncwarp();
   }
   if (lane < A) {
-    float2 y[B];
+    T2<T> y[B];
 #pragma unroll
     for (int n2 = 0; n2 < B; ++n2) y[n2] = buf[lane * SB + n2];
     dft_reg<B, true>(y);
-    const float inv = 1.0f / (float)N;
+    const T inv = (T)1 / (T)N;
     const int ba = q / s.M, ka = q - ba * s.M;
     const int bb = hb ? (q + 1) / s.M : ba, kb = hb ? (q + 1) - bb * s.M : ka;
     const long long ca = bidx(g, 2, ba + 2, ka + 2), cb = bidx(g, 2, bb + 2, kb + 2);
@@ -799,7 +799,7 @@ __global__ void __launch_bounds__(256, 3) k_idct2(Geo g, Spec s, FftPlan<float> 
     for (int k2 = 0; k2 < B; ++k2) {
       const int n = lane + A * k2;
       const int ip = 2 * n < N ? 2 * n : 2 * N - 1 - 2 * n;
-      const float va = y[k2].x * inv, vb = y[k2].y * inv;
+      const T va = y[k2].x * inv, vb = y[k2].y * inv;
       p[ca + ip] = va;
       if (ka == 0) p[ca + ip + zsh] = va;
       if (hb) {
@@ -1556,12 +1556,12 @@ void launch_div_dct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *
   }
 }
 
-template <int A, int B>
-static void launch_idct2(const Geo &g, const Spec &s, const FftPlan<float> &pl, const float *R, float *p, int nw,
-                         size_t sm, int grid, int *err, cudaStream_t st) {
-  cudaFuncSetAttribute(k_idct2<A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  cudaFuncSetAttribute(k_idct2<A, B>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  k_idct2<A, B><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p, err);
+template <int A, int B, typename T>
+static void launch_idct2(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, T *p, int nw, size_t sm,
+                         int grid, int *err, cudaStream_t st) {
+  cudaFuncSetAttribute(k_idct2<A, B, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_idct2<A, B, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  k_idct2<A, B, T><<<grid, 32 * nw, sm, st>>>(g, s, pl, R, p, err);
 }
 
 // the two rows of the bulk copy fit one line buffer of the two-pass kernel
@@ -1578,15 +1578,16 @@ void launch_idct(const Geo &g, const Spec &s, const FftPlan<T> &pl, const T *R, 
   const size_t sm = dct_smem_bytes(s.N, sizeof(T), nw, split);
   const int ncl = (s.NM * s.M + 1) / 2;
   const int grid = (ncl + nw - 1) / nw;
+  const bool fused = idct2_fits(s, split) && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
   if constexpr (sizeof(T) == 8) {
+    if (split == 29 && fused) return launch_idct2<29, 28, T>(g, s, pl, R, p, nw, sm, grid, err, st);
     if (split == 29) return launch_idct_e<T, TwoPassX<29, 28, T>>(g, s, pl, R, p, nw, sm, grid, st);
   }
   if constexpr (sizeof(T) == 4) {
-    const bool fused = idct2_fits(s, split) && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
-    if (split == 29 && fused) return launch_idct2<29, 28>(g, s, pl, R, p, nw, sm, grid, err, st);
-    if (split == 17 && fused) return launch_idct2<17, 30>(g, s, pl, R, p, nw, sm, grid, err, st);
-    if (split == 19 && fused) return launch_idct2<19, 10>(g, s, pl, R, p, nw, sm, grid, err, st);
-    if (split == 14 && fused) return launch_idct2<14, 9>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 29 && fused) return launch_idct2<29, 28, T>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 17 && fused) return launch_idct2<17, 30, T>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 19 && fused) return launch_idct2<19, 10, T>(g, s, pl, R, p, nw, sm, grid, err, st);
+    if (split == 14 && fused) return launch_idct2<14, 9, T>(g, s, pl, R, p, nw, sm, grid, err, st);
     if (split == 29) return launch_idct_e<T, TwoPassX<29, 28>>(g, s, pl, R, p, nw, sm, grid, st);
     if (split == 17) return launch_idct_e<T, TwoPassX<17, 30>>(g, s, pl, R, p, nw, sm, grid, st);
     if (split == 19) return launch_idct_e<T, TwoPassX<19, 10>>(g, s, pl, R, p, nw, sm, grid, st);

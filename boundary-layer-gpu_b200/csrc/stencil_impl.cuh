@@ -1624,6 +1624,83 @@ __global__ void __launch_bounds__(256) k_dt_reduce(Geo g, const T *__restrict__ 
   }
 }
 
+// The FP64 reduction with two consecutive points per thread (16-byte loads;
+// the box rows are 16-byte aligned at i = 2) and the k loop unrolled.  For
+// w the quotient C_k/|w_k| is formed only where it can raise the maximum:
+// a_k = |w_k| rC_k is within 3e-16 of |w_k|/C_k, so a point whose a_k
+// exceeds the smallest a seen so far by more than 1e-12 (relative) has a
+// quotient below that point's, and the maximum of the formed quotients is
+// the maximum of all of them, to the bit.
+template <typename T>  // double
+__global__ void __launch_bounds__(256) k_dt_reduce2(Geo g, const T *__restrict__ U, const T *__restrict__ V,
+                                                    const T *__restrict__ W, Scalars *__restrict__ sc, int kchunk,
+                                                    double cfl, double dtvis, int save_time) {
+  const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  double mu = 0.0, mv = 0.0, mw = 0.0;
+  if (i0 <= g.nxg - 1 && j <= g.nyg - 1) {
+    const int k0 = blockIdx.z * kchunk + 2;
+    const int k1 = min(k0 + kchunk - 1, g.nzg - 1);
+    double au[2] = {INFINITY, INFINITY}, av[2] = {INFINITY, INFINITY}, bw[2] = {INFINITY, INFINITY};
+    double qw[2] = {0.0, 0.0};
+    const double2 *u2 = reinterpret_cast<const double2 *>(U + bidx(g, i0, j, k0));
+    const double2 *v2 = reinterpret_cast<const double2 *>(V + bidx(g, i0, j, k0));
+    const double2 *w2 = reinterpret_cast<const double2 *>(W + bidx(g, i0, j, k0));
+    const long long ps = g.plane / 2;
+#pragma unroll 4
+    for (int k = k0; k <= k1; ++k) {
+      const long long o = (long long)(k - k0) * ps;
+      const double2 u = __ldg(u2 + o), v = __ldg(v2 + o), w = __ldg(w2 + o);
+      const double rc = g.az.rC[k];
+      const double uu[2] = {u.x, u.y}, vv[2] = {v.x, v.y}, ww[2] = {w.x, w.y};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        au[e] = fmin(au[e], fabs(uu[e]));
+        av[e] = fmin(av[e], fabs(vv[e]));
+        const double a = fabs(ww[e]) * rc;
+        if (a <= bw[e] * (1.0 + 1e-12)) {
+          qw[e] = fmax(qw[e], g.az.C[k] / fabs(ww[e]));
+          bw[e] = fmin(bw[e], a);
+        }
+      }
+    }
+    if (k1 >= k0) {
+      const double cv = g.ay.C[j];
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        if (i0 + e <= g.nxg - 1) {
+          mu = fmax(mu, g.ax.C[i0 + e] / au[e]);
+          mv = fmax(mv, cv / av[e]);
+          mw = fmax(mw, qw[e]);
+        }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+  }
+  __shared__ double red[3][8];
+  const int wid = (threadIdx.y * blockDim.x + threadIdx.x) >> 5, nwarp = (blockDim.x * blockDim.y) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][wid] = mu;
+    red[1][wid] = mv;
+    red[2][wid] = mw;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int w = 1; w < nwarp; ++w) {
+      mu = fmax(mu, red[0][w]);
+      mv = fmax(mv, red[1][w]);
+      mw = fmax(mw, red[2][w]);
+    }
+    atomicMax(&sc->lmax[0], (unsigned long long)__double_as_longlong(mu));
+    atomicMax(&sc->lmax[1], (unsigned long long)__double_as_longlong(mv));
+    atomicMax(&sc->lmax[2], (unsigned long long)__double_as_longlong(mw));
+    dt_finish_last(sc, cfl, dtvis, save_time);
+  }
+}
+
 // The same reduction for the mixed form with four consecutive points per
 // thread (16-byte loads; the box rows are 16-byte aligned at i = 2) and the
 // k loop unrolled, so that a thread keeps a dozen loads in flight.
@@ -2099,13 +2176,17 @@ template <typename T>
 void launch_dt(const Geo &g, const T *U, const T *V, const T *W, Scalars *sc, double cfl, double dtvis,
                bool save_time, cudaStream_t st) {
   const int kchunk = 32;
-  const bool vec = sizeof(T) == 4 && (g.px & 3) == 0 &&
+  // 16-byte vectors: rows of 4 floats / 2 doubles from i = 2 (element i + 2 of a row)
+  const bool vec = (g.px & (sizeof(T) == 4 ? 3 : 1)) == 0 &&
                    ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(W)) &
                     15) == 0;
-  if constexpr (sizeof(T) == 4) {
-    if (vec) {
+  if (vec) {
+    if constexpr (sizeof(T) == 4) {
       dim3 grid = vol_grid((g.nxg - 2 + 3) / 4, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
       k_dt_reduce4<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis, save_time ? 1 : 0);
+    } else {
+      dim3 grid = vol_grid((g.nxg - 2 + 1) / 2, g.nyg - 2, g.nzg - 2, kchunk), block(32, 8);
+      k_dt_reduce2<T><<<grid, block, 0, st>>>(g, U, V, W, sc, kchunk, cfl, dtvis, save_time ? 1 : 0);
     }
   }
   if (!vec) {

@@ -143,6 +143,31 @@ def test_compute_dt_exact(gpu, grid):
     s.close()
 
 
+@pytest.mark.parametrize("comp", [0, 1, 2])
+@pytest.mark.parametrize("grid", GRIDS)
+def test_compute_dt_exact_each_component(gpu, grid, comp):
+    """dt set by the convective bound of one velocity component: the other
+    two are zero at one interior point (their bounds infinite) and the
+    chosen one is shifted by 50, so that its bound is below the viscous
+    one; the oracle's dt to the last bit in each case."""
+    c = noisy_laminar(*grid, seed=9 + comp, amp=0.3)
+    F = [c.U, c.V, c.W]
+    for q in range(3):
+        F[q] = np.array(F[q], order="F")
+        if q == comp:
+            F[q] += 50.0
+        else:
+            F[q][3, 3, 3] = 0.0
+    c.U, c.V, c.W = F
+    c.cfl = 0.37
+    s = cases.solver_for(c)
+    o = oracle.oracle_for(c)
+    dt = o.compute_dt()
+    assert 0 < dt < 0.37 * 3.0 / 50.0
+    assert s.compute_dt() == dt
+    s.close()
+
+
 @pytest.mark.parametrize("grid", GRIDS)
 def test_compute_dt_mixed(gpu, grid):
     """The mixed form's compute_dt (four points per thread, 16-byte loads)
