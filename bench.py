@@ -374,7 +374,7 @@ def run_transition(args, dev):
 def run_closure(args, dev):
     """The learned wall-stress closure: trained on the turbulent DNS recipe's
     own wall samples (814 x 257 x 193, 12 snapshots of the row at h = 0.1
-    delta99 after 300 steps, 2 more held out), judged on the held-out states
+    delta99 after 300 steps, 2 more held out), assessed on the held-out states
     against the resolved wall stress beside the equilibrium law of the wall,
     then both as the wall condition of the 512 x 96 x 256 wall-modelled LES."""
     from blgpu import wallmodel, WallNet

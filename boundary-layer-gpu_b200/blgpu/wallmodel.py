@@ -163,7 +163,7 @@ def holdout_errors(net, holdout, tau_eq):
 
 
 def config4_case(retheta=2000.0, nx=512, ny=96, nz=256, seed=5, dt=0.04):
-    """The wall-modelled LES grid of the closure's judge: 512 x 96 x 256 over
+    """The wall-modelled LES grid the closure is assessed on: 512 x 96 x 256 over
     64 x 2 x 16 delta99, nearly uniform y (dy = delta/48), so h = 0.1 delta is
     the sixth row and the first cell centre sits at y+ ~ 7 (Re_theta 2000),
     far from resolving the wall gradient.  Fixed dt = 0.04 delta99/U_inf

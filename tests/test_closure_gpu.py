@@ -1,5 +1,5 @@
 """The learned wall-stress closure trained on the turbulent DNS recipe's own
-data and judged against the equilibrium law of the wall
+data and assessed against the equilibrium law of the wall
 (wallmodel.f90:1951-1985, Newton_solver.f90:13-79).
 
 Data: the 814 x 257 x 193 turbulent box (10 % divergence-free noise, Lund
