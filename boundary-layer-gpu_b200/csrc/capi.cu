@@ -1079,10 +1079,12 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
-  const bool tiled = ctx->have_tmaps && (ctx->tiles.thomas == 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
+  const bool tiled =
+      ctx->have_tmaps && (ctx->tiles.thomas >= 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
   if (tiled)
     launch_thomas_tile<T>(s, ctx->tmaps, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
-                          &ctx->sc->err, ctx->wait_limit, ctx->st);
+                          &ctx->sc->err, ctx->wait_limit, ctx->tiles.thomas == 3 || ctx->tiles.thomas == 0,
+                          ctx->st);
   else
     launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
                      ctx->st);
@@ -1710,7 +1712,7 @@ static int tiles_check(blgpu_ctx *ctx, const Tiles &t) {
   }
   if (t.zdft < 0 || t.zdft > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: zdft %d not in {0,1,2,3}", t.zdft);
   if (t.rhs_pts < 0 || t.rhs_pts > 4) return set_err(ctx, BLGPU_EINVAL, "tiles: rhs_pts %d not in {0,...,4}", t.rhs_pts);
-  if (t.thomas < 0 || t.thomas > 2) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,1,2}", t.thomas);
+  if (t.thomas < 0 || t.thomas > 3) return set_err(ctx, BLGPU_EINVAL, "tiles: thomas %d not in {0,...,3}", t.thomas);
   return BLGPU_OK;
 }
 
@@ -1826,7 +1828,7 @@ int blgpu_autotune(blgpu_ctx *ctx, int steps, double *ms_default, double *ms_bes
       {4, 8},                                                                  // proj_by
       {1, 2, 3},                                                               // zdft
       {1, 2, 4},                                                               // rhs_pts
-      {1, 2},                                                                  // thomas
+      {1, 2, 3},                                                               // thomas
       {0, 4, 8, 12, 16},                                                       // idct_nw
       {1, 2}};                                                                 // xfft
   auto measure = [&](const Tiles &t, double *ms) -> int {

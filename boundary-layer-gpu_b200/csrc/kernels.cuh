@@ -27,7 +27,8 @@ struct Tiles {
   int rhs_pts;  // FP32 DNS RHS: 1 one point per thread, 2 two points, 3 two points packed in FP32x2
                 // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2);
                 // FP64 DNS: 1 one point with global loads, 4 one point TMA-fed, 0 or 2 two points
-  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (0: tiles in FP64, ring in FP32)
+  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows, 3 the tiles with each mode's
+                // rows split over lanes (0: 3 in FP64, the ring in FP32)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
   int xfft;     // x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N; FP64: N = 812)
 };
@@ -208,10 +209,11 @@ struct ThomasMaps {  // CUtensorMap bytes of C and of the pivots
 template <typename T>
 bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out);
 // err: device flag, bit 4 set when a tile copy missed its wait limit;
-// wait_limit: mbarrier polls before giving up (< 0: the built-in limit)
+// wait_limit: mbarrier polls before giving up (< 0: the built-in limit);
+// scan: each mode's rows split over the lanes left by the tile's modes
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
-                        int klow, int *err, int wait_limit, cudaStream_t st);
+                        int klow, int *err, int wait_limit, bool scan, cudaStream_t st);
 // inverse pivots piv[b][kz][kx] of the y-solve (grid only; once per grid)
 void launch_thomas_factors(const Spec &s, double *piv, const double *dd, const double *dl, const double *du,
                            const double *kxx, const double *kzz, cudaStream_t st);

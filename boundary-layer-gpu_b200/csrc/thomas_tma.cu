@@ -45,7 +45,118 @@ inline size_t thomas_tile_smem(int NM) {
   return tile_c_bytes<T>(NM) + tile_p_bytes<T>(NM) + 2 * (size_t)NM * sizeof(double) + sizeof(uint64_t);
 }
 
+// The solve of one tile in shared memory with each mode's NM rows split
+// over P = 32 / MT lanes (lane = kk MT + m: a row's modes are one 128-byte
+// run, read without bank conflicts).  Both recurrences are first-order and
+// linear,
+//   g_b = r_b - w_b g_{b-1} (w_b = dl_b piv_{b-1}),  x_b = (g_b - du_b x_{b+1}) piv_b,
+// so lane kk runs them over its rows [kk Le, kk Le + Le) from a zero start,
+// keeping the product of its multipliers (-w_b forward, beta_b = -du_b piv_b
+// backward); an inclusive shuffle scan of these affine maps over kk gives
+// each lane the value entering its rows, and a second pass adds the product
+// times that value.  The sums are those of the serial sweeps, reassociated
+// across the P segments.
 template <typename T>
+__device__ __forceinline__ void thomas_scan_tile(T2t<T> *Ct, const double *Pt, const double *dls,
+                                                 const double *dus, int NM, int kx0, int N, int lane) {
+  constexpr int MT = ThomasTile<T>::MT, P = 32 / MT;
+  constexpr unsigned FULL = 0xffffffffu;
+  typedef T2t<T> V2;
+  const int m = lane % MT, kk = lane / MT;
+  const bool act = kx0 + m < N;
+  const int Le = (NM + P - 1) / P, s0 = kk * Le;
+  const int nr = act ? max(0, min(Le, NM - s0)) : 0;
+  V2 *c = Ct + (size_t)s0 * MT + m;
+  const double *p = Pt + (size_t)s0 * MT + m;
+  // forward from g = 0 at the segment's start
+  double gx = 0.0, gy = 0.0, h = 1.0;
+  for (int u = 0; u < nr; ++u) {
+    const int b = s0 + u;
+    const V2 cv = c[u * MT];
+    double rx = (double)cv.x, ry = (double)cv.y;
+    double w = 0.0;
+    if (b > 0) {
+      w = dls[b] * p[(u - 1) * MT];  // l_b / d'_{b-1}
+      rx = rx - w * gx;
+      ry = ry - w * gy;
+    }
+    h = -w * h;
+    gx = rx;
+    gy = ry;
+    c[u * MT] = mk2<T>((T)rx, (T)ry);
+  }
+  double A = h, Cx = gx, Cy = gy;
+#pragma unroll
+  for (int off = 1; off < P; off <<= 1) {
+    const double a2 = __shfl_up_sync(FULL, A, off * MT);
+    const double x2 = __shfl_up_sync(FULL, Cx, off * MT), y2 = __shfl_up_sync(FULL, Cy, off * MT);
+    if (kk >= off) {
+      Cx = Cx + A * x2;
+      Cy = Cy + A * y2;
+      A = A * a2;
+    }
+  }
+  double ix = __shfl_up_sync(FULL, Cx, MT), iy = __shfl_up_sync(FULL, Cy, MT);
+  if (kk == 0) ix = iy = 0.0;
+  h = 1.0;
+  for (int u = 0; u < nr; ++u) {
+    const int b = s0 + u;
+    const double w = b > 0 ? dls[b] * p[(u - 1) * MT] : 0.0;
+    h = -w * h;
+    const V2 cv = c[u * MT];
+    c[u * MT] = mk2<T>((T)((double)cv.x + h * ix), (T)((double)cv.y + h * iy));
+  }
+  // backward from x = 0 above the segment's top row
+  double xx = 0.0, xy = 0.0, kp = 1.0;
+  for (int u = nr - 1; u >= 0; --u) {
+    const int b = s0 + u;
+    const V2 cv = c[u * MT];
+    const double pv = p[u * MT];
+    double beta = 0.0;
+    if (b == NM - 1) {
+      xx = (double)cv.x * pv;
+      xy = (double)cv.y * pv;
+    } else {
+      xx = ((double)cv.x - dus[b] * xx) * pv;
+      xy = ((double)cv.y - dus[b] * xy) * pv;
+      beta = -dus[b] * pv;
+    }
+    kp = beta * kp;
+    c[u * MT] = mk2<T>((T)xx, (T)xy);
+  }
+  A = kp;
+  Cx = xx;
+  Cy = xy;
+#pragma unroll
+  for (int off = 1; off < P; off <<= 1) {
+    const double a2 = __shfl_down_sync(FULL, A, off * MT);
+    const double x2 = __shfl_down_sync(FULL, Cx, off * MT), y2 = __shfl_down_sync(FULL, Cy, off * MT);
+    if (kk + off < P) {
+      Cx = Cx + A * x2;
+      Cy = Cy + A * y2;
+      A = A * a2;
+    }
+  }
+  ix = __shfl_down_sync(FULL, Cx, MT);
+  iy = __shfl_down_sync(FULL, Cy, MT);
+  if (kk == P - 1) ix = iy = 0.0;
+  kp = 1.0;
+  for (int u = nr - 1; u >= 0; --u) {
+    const int b = s0 + u;
+    const double beta = b == NM - 1 ? 0.0 : -dus[b] * p[u * MT];
+    kp = beta * kp;
+    const V2 cv = c[u * MT];
+    c[u * MT] = mk2<T>((T)((double)cv.x + kp * ix), (T)((double)cv.y + kp * iy));
+  }
+}
+
+// SCAN: the rows of a mode split over P = 32 / MT lanes (FP32 2, FP64 4;
+// lane = kk MT + m), each lane running both recurrences over its segment
+// of the tile from a zero start with the product of its multipliers, the
+// segments joined by shuffle scans of those affine maps (see
+// thomas_scan_tile), so that every lane of the warp works and the serial
+// chains are P times shorter.
+template <typename T, bool SCAN>
 __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUtensorMap mapC,
                                                     const __grid_constant__ CUtensorMap mapP, Spec s,
                                                     const double *__restrict__ dl, const double *__restrict__ du,
@@ -85,6 +196,9 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
     }
     return;
   }
+  if (SCAN && !(H0 && kz == 0 && kx0 < klow)) {
+    thomas_scan_tile<T>(Ct, Pt, dls, dus, NM, kx0, s.N, lane);
+  } else {
   const int kx = kx0 + lane;
   if (lane < MT && kx < s.N) {
     V2 *c = Ct + lane;
@@ -143,6 +257,7 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
       }
     }
   }
+  }
   fence_async_shared();  // the sweeps' shared-memory writes before the TMA store reads them
   __syncwarp();
   if (lane == 0) {
@@ -194,22 +309,28 @@ bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out) {
 
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
-                        int klow, int *err, int wait_limit, cudaStream_t st) {
+                        int klow, int *err, int wait_limit, bool scan, cudaStream_t st) {
   constexpr int MT = ThomasTile<T>::MT;
   const size_t sm = thomas_tile_smem<T>(s.NM);
-  cudaFuncSetAttribute(k_thomas_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   CUtensorMap mc, mp;
   memcpy(&mc, maps.c, sizeof mc);
   memcpy(&mp, maps.p, sizeof mp);
   dim3 grid((s.N + MT - 1) / MT, s.MH);
-  k_thomas_tile<T><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wait_limit < 0 ? WAIT_LIMIT : wait_limit);
+  const int wl = wait_limit < 0 ? WAIT_LIMIT : wait_limit;
+  if (scan) {
+    cudaFuncSetAttribute(k_thomas_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_thomas_tile<T, true><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+  } else {
+    cudaFuncSetAttribute(k_thomas_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_thomas_tile<T, false><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+  }
 }
 
 template bool thomas_maps<float>(const Spec &, void *, double *, ThomasMaps *);
 template bool thomas_maps<double>(const Spec &, void *, double *, ThomasMaps *);
 template void launch_thomas_tile<float>(const Spec &, const ThomasMaps &, const double *, const double *, double *,
-                                        int, int *, int, cudaStream_t);
+                                        int, int *, int, bool, cudaStream_t);
 template void launch_thomas_tile<double>(const Spec &, const ThomasMaps &, const double *, const double *, double *,
-                                         int, int *, int, cudaStream_t);
+                                         int, int *, int, bool, cudaStream_t);
 
 }  // namespace blgpu

@@ -258,14 +258,17 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * 8; FP64 DNS, all bit-identical: 1 = one point, global loads, 4 = one point,
  * TMA-fed planes, 2 = two points in a register window),
  * thomas (y-solve: 1 = register ring,
- * 2 = TMA-fed tiles where ny-1 <= 256), idct_nw (lines per CTA of the
+ * 2 = TMA-fed tiles where ny-1 <= 256, one lane per mode, 3 = the same
+ * tiles with each mode's rows split over the warp's spare lanes; the
+ * built-in choice is 3 in FP64 and 1 in the mixed form), idct_nw (lines per CTA of the
  * inverse DCT), xfft (x transforms: 1 = Stockham mixed-radix FFT in shared
  * memory, any N; 2 = two-pass register FFT, built for N = nx-2 = 812
  * (29 x 28; both precisions), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9)
  * (mixed form));
  * 0 = the built-in choice.
- * Values not passed keep their current setting.  All but zdft, rhs_pts and
- * xfft leave results unchanged; those change them at FP32 rounding level.  No counterpart in the
+ * Values not passed keep their current setting.  All but zdft, rhs_pts,
+ * xfft and thomas 3 leave results unchanged; those change them at rounding
+ * level.  No counterpart in the
  * reference (its OpenACC loops take compiler-chosen gangs). */
 int blgpu_set_tiles(blgpu_ctx *ctx, const int *tiles, int n);
 int blgpu_get_tiles(const blgpu_ctx *ctx, int *tiles, int n);

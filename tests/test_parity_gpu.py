@@ -276,3 +276,44 @@ def test_tiled_y_solve_matches_ring(gpu, precision, grid):
         s.close()
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+# NM = ny-1 of 16, 32, 8, 64 (the ensemble boxes), 256 (the headline box)
+# and 100 (a last segment with fewer rows)
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+@pytest.mark.parametrize("grid", [(60, 17, 15), (131, 33, 24), (37, 9, 24), (66, 65, 20), (50, 257, 12),
+                                  (34, 101, 14)])
+def test_tile_scan_y_solve_matches_ring(gpu, precision, grid):
+    """The tiled y-solve with each mode's rows split over the tile's spare
+    lanes (shuffle scans of the two linear recurrences) against the register
+    ring: the same sums reassociated, so FP64 agrees to rounding and the
+    mixed form to its FP32 storage of the intermediate rows."""
+    c = noisy_laminar(*grid, seed=11, cfl=-2e-3)
+    out = []
+    for thomas in (1, 3):
+        s = cases.solver_for(c, precision=precision)
+        s.set_tiles(thomas=thomas)
+        assert s.tiles()["thomas"] == thomas
+        s.apply_boundary_conditions(1)
+        s.compute_projection_step(1)
+        out.append((s.download_state()[:3], s.rhs_p()))
+        s.close()
+    tol_p, tol_u = (1e-12, 1e-14) if precision == FP64 else (2e-5, 1e-6)
+    assert rel(out[1][1], out[0][1]) < tol_p, rel(out[1][1], out[0][1])
+    for a, b in zip(out[1][0], out[0][0]):
+        assert rel(a, b) < tol_u, rel(a, b)
+
+
+def test_tile_scan_y_solve_oracle_steps(gpu):
+    """Five FP64 RK3 steps with the tile-scan y-solve against the oracle."""
+    c = noisy_laminar(60, 17, 15, seed=12, amp=1e-3, cfl=-2e-3)
+    s = cases.solver_for(c)
+    s.set_tiles(thomas=3)
+    o = oracle.oracle_for(c)
+    for _ in range(5):
+        s.time_step()
+        o.step()
+    for a, b in zip(s.download_state()[:3], o.state()[:3]):
+        assert rel(a, b) < REL10
+    assert s.check_divergence() < 1e-12
+    s.close()
