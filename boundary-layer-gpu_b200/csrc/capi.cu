@@ -1079,12 +1079,12 @@ static void enq_projection(blgpu_ctx *ctx, int b, int rk_step) {
   ph_end(ctx, 1);
   const double *sp = ctx->d_spec;
   ph_begin(ctx, PH_THOMAS);
-  const bool tiled =
-      ctx->have_tmaps && (ctx->tiles.thomas >= 2 || (ctx->tiles.thomas == 0 && ctx->fp64));
+  // tiles where their tensor maps exist (NM <= 256): rows split over the CTA
+  // (thomas 0 or 3) or one thread per mode (2); else the register ring
+  const bool tiled = ctx->have_tmaps && ctx->tiles.thomas != 1;
   if (tiled)
     launch_thomas_tile<T>(s, ctx->tmaps, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
-                          &ctx->sc->err, ctx->wait_limit, ctx->tiles.thomas == 3 || ctx->tiles.thomas == 0,
-                          ctx->st);
+                          &ctx->sc->err, ctx->wait_limit, ctx->tiles.thomas != 2, ctx->st);
   else
     launch_thomas<T>(s, (T2 *)ctx->C, ctx->piv, sp + s.NM, sp + 2 * s.NM, mixed ? ctx->kz0h : nullptr, ctx->klow,
                      ctx->st);

@@ -27,8 +27,8 @@ struct Tiles {
   int rhs_pts;  // FP32 DNS RHS: 1 one point per thread, 2 two points, 3 two points packed in FP32x2
                 // instructions, 4 the same fed by TMA (0: 4 where its tensor maps exist, else 2);
                 // FP64 DNS: 1 one point with global loads, 4 one point TMA-fed, 0 or 2 two points
-  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows, 3 the tiles with each mode's
-                // rows split over lanes (0: 3 in FP64, the ring in FP32)
+  int thomas;   // y-solve: 1 register ring, 2 TMA tiles where the box allows (one thread per mode), 3 the
+                // tiles with each mode's rows split over 16 threads (0: 3 where the tiles exist, else 1)
   int idct_nw;  // complex lines (warps) per CTA of the inverse DCT, as dct_nw (0: built-in)
   int xfft;     // x transforms: 1 Stockham, 2 two-pass registers (0: two-pass where built for N; FP64: N = 812)
 };
@@ -210,7 +210,7 @@ template <typename T>
 bool thomas_maps(const Spec &s, void *C, double *piv, ThomasMaps *out);
 // err: device flag, bit 4 set when a tile copy missed its wait limit;
 // wait_limit: mbarrier polls before giving up (< 0: the built-in limit);
-// scan: each mode's rows split over the lanes left by the tile's modes
+// scan: each mode's rows split over 16 threads (k_thomas_tile_scan)
 template <typename T>
 void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl, const double *du, double *H0,
                         int klow, int *err, int wait_limit, bool scan, cudaStream_t st);

@@ -44,119 +44,13 @@ template <typename T>
 inline size_t thomas_tile_smem(int NM) {
   return tile_c_bytes<T>(NM) + tile_p_bytes<T>(NM) + 2 * (size_t)NM * sizeof(double) + sizeof(uint64_t);
 }
-
-// The solve of one tile in shared memory with each mode's NM rows split
-// over P = 32 / MT lanes (lane = kk MT + m: a row's modes are one 128-byte
-// run, read without bank conflicts).  Both recurrences are first-order and
-// linear,
-//   g_b = r_b - w_b g_{b-1} (w_b = dl_b piv_{b-1}),  x_b = (g_b - du_b x_{b+1}) piv_b,
-// so lane kk runs them over its rows [kk Le, kk Le + Le) from a zero start,
-// keeping the product of its multipliers (-w_b forward, beta_b = -du_b piv_b
-// backward); an inclusive shuffle scan of these affine maps over kk gives
-// each lane the value entering its rows, and a second pass adds the product
-// times that value.  The sums are those of the serial sweeps, reassociated
-// across the P segments.
-template <typename T>
-__device__ __forceinline__ void thomas_scan_tile(T2t<T> *Ct, const double *Pt, const double *dls,
-                                                 const double *dus, int NM, int kx0, int N, int lane) {
-  constexpr int MT = ThomasTile<T>::MT, P = 32 / MT;
-  constexpr unsigned FULL = 0xffffffffu;
-  typedef T2t<T> V2;
-  const int m = lane % MT, kk = lane / MT;
-  const bool act = kx0 + m < N;
-  const int Le = (NM + P - 1) / P, s0 = kk * Le;
-  const int nr = act ? max(0, min(Le, NM - s0)) : 0;
-  V2 *c = Ct + (size_t)s0 * MT + m;
-  const double *p = Pt + (size_t)s0 * MT + m;
-  // forward from g = 0 at the segment's start
-  double gx = 0.0, gy = 0.0, h = 1.0;
-  for (int u = 0; u < nr; ++u) {
-    const int b = s0 + u;
-    const V2 cv = c[u * MT];
-    double rx = (double)cv.x, ry = (double)cv.y;
-    double w = 0.0;
-    if (b > 0) {
-      w = dls[b] * p[(u - 1) * MT];  // l_b / d'_{b-1}
-      rx = rx - w * gx;
-      ry = ry - w * gy;
-    }
-    h = -w * h;
-    gx = rx;
-    gy = ry;
-    c[u * MT] = mk2<T>((T)rx, (T)ry);
-  }
-  double A = h, Cx = gx, Cy = gy;
-#pragma unroll
-  for (int off = 1; off < P; off <<= 1) {
-    const double a2 = __shfl_up_sync(FULL, A, off * MT);
-    const double x2 = __shfl_up_sync(FULL, Cx, off * MT), y2 = __shfl_up_sync(FULL, Cy, off * MT);
-    if (kk >= off) {
-      Cx = Cx + A * x2;
-      Cy = Cy + A * y2;
-      A = A * a2;
-    }
-  }
-  double ix = __shfl_up_sync(FULL, Cx, MT), iy = __shfl_up_sync(FULL, Cy, MT);
-  if (kk == 0) ix = iy = 0.0;
-  h = 1.0;
-  for (int u = 0; u < nr; ++u) {
-    const int b = s0 + u;
-    const double w = b > 0 ? dls[b] * p[(u - 1) * MT] : 0.0;
-    h = -w * h;
-    const V2 cv = c[u * MT];
-    c[u * MT] = mk2<T>((T)((double)cv.x + h * ix), (T)((double)cv.y + h * iy));
-  }
-  // backward from x = 0 above the segment's top row
-  double xx = 0.0, xy = 0.0, kp = 1.0;
-  for (int u = nr - 1; u >= 0; --u) {
-    const int b = s0 + u;
-    const V2 cv = c[u * MT];
-    const double pv = p[u * MT];
-    double beta = 0.0;
-    if (b == NM - 1) {
-      xx = (double)cv.x * pv;
-      xy = (double)cv.y * pv;
-    } else {
-      xx = ((double)cv.x - dus[b] * xx) * pv;
-      xy = ((double)cv.y - dus[b] * xy) * pv;
-      beta = -dus[b] * pv;
-    }
-    kp = beta * kp;
-    c[u * MT] = mk2<T>((T)xx, (T)xy);
-  }
-  A = kp;
-  Cx = xx;
-  Cy = xy;
-#pragma unroll
-  for (int off = 1; off < P; off <<= 1) {
-    const double a2 = __shfl_down_sync(FULL, A, off * MT);
-    const double x2 = __shfl_down_sync(FULL, Cx, off * MT), y2 = __shfl_down_sync(FULL, Cy, off * MT);
-    if (kk + off < P) {
-      Cx = Cx + A * x2;
-      Cy = Cy + A * y2;
-      A = A * a2;
-    }
-  }
-  ix = __shfl_down_sync(FULL, Cx, MT);
-  iy = __shfl_down_sync(FULL, Cy, MT);
-  if (kk == P - 1) ix = iy = 0.0;
-  kp = 1.0;
-  for (int u = nr - 1; u >= 0; --u) {
-    const int b = s0 + u;
-    const double beta = b == NM - 1 ? 0.0 : -dus[b] * p[u * MT];
-    kp = beta * kp;
-    const V2 cv = c[u * MT];
-    c[u * MT] = mk2<T>((T)((double)cv.x + kp * ix), (T)((double)cv.y + kp * iy));
-  }
+// the same plus the segments' maps (three doubles per thread)
+template <typename T, int NT>
+inline size_t tile_scan_smem(int NM) {
+  return thomas_tile_smem<T>(NM) + 3 * (size_t)NT * sizeof(double);
 }
 
-// SCAN: the rows of a mode split over P = 32 / MT lanes (FP32 2, FP64 4;
-// lane = kk MT + m), each lane running both recurrences over its segment
-// of the tile from a zero start with the product of its multipliers, the
-// segments joined by shuffle scans of those affine maps (see
-// thomas_scan_tile), so that every lane of the warp works and the serial
-// chains are P times shorter.
-template <typename T, bool SCAN>
+template <typename T>
 __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUtensorMap mapC,
                                                     const __grid_constant__ CUtensorMap mapP, Spec s,
                                                     const double *__restrict__ dl, const double *__restrict__ du,
@@ -196,9 +90,6 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
     }
     return;
   }
-  if (SCAN && !(H0 && kz == 0 && kx0 < klow)) {
-    thomas_scan_tile<T>(Ct, Pt, dls, dus, NM, kx0, s.N, lane);
-  } else {
   const int kx = kx0 + lane;
   if (lane < MT && kx < s.N) {
     V2 *c = Ct + lane;
@@ -257,10 +148,207 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
       }
     }
   }
-  }
   fence_async_shared();  // the sweeps' shared-memory writes before the TMA store reads them
   __syncwarp();
   if (lane == 0) {
+    store_3d(&mapC, Ct, 2 * kx0, kz, 0);
+    store_commit_and_wait_read();
+  }
+}
+
+// The same tile solve with each mode's NM rows split into P = NT / MT
+// segments: thread t takes mode m = t % MT and the rows [kk Le, kk Le + Le)
+// of it, kk = t / MT (a half- or quarter-warp reads one row's MT modes, one
+// 128-byte run, without bank conflicts).  Both recurrences are first-order
+// and linear,
+//   g_b = r_b - w_b g_{b-1} (w_b = dl_b piv_{b-1}),  x_b = (g_b - du_b x_{b+1}) piv_b,
+// so a segment runs them over its rows from a zero start, keeping the
+// product of its multipliers (-w_b forward, beta_b = -du_b piv_b backward):
+// its rows are then affine in the value entering it.  The segments' maps
+// meet in shared memory, each thread composes those of the segments before
+// (forward) or after (backward) its own into its entering value, and a
+// second pass over its rows adds the product times that value.  The sums
+// are those of the serial sweeps, reassociated across the segments; the
+// serial chains are P times shorter and every thread of the CTA works.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_thomas_tile_scan(const __grid_constant__ CUtensorMap mapC,
+                                                         const __grid_constant__ CUtensorMap mapP, Spec s,
+                                                         const double *__restrict__ dl, const double *__restrict__ du,
+                                                         double *__restrict__ H0, int klow, int *__restrict__ err,
+                                                         int wait_limit) {
+  constexpr int MT = ThomasTile<T>::MT, P = NT / MT;
+  typedef T2t<T> V2;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int NM = s.NM;
+  V2 *Ct = reinterpret_cast<V2 *>(smem_raw);                                   // [NM][MT]
+  double *Pt = reinterpret_cast<double *>(smem_raw + tile_c_bytes<T>(NM));     // [NM][MT]
+  double *dls = reinterpret_cast<double *>(smem_raw + tile_c_bytes<T>(NM) + tile_p_bytes<T>(NM));  // [NM]
+  double *dus = dls + NM;                                                                          // [NM]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(dus + NM);
+  double *mA = reinterpret_cast<double *>(bar + 1), *mX = mA + NT, *mY = mX + NT;  // segment maps [kk][m]
+  const int kx0 = blockIdx.x * MT, kz = blockIdx.y, tid = threadIdx.x;
+  const uint32_t bytes = (uint32_t)((size_t)NM * MT * (2 * sizeof(T) + sizeof(double)));
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+    mbar_expect_tx(bar, bytes);
+    load_3d(Ct, &mapC, 2 * kx0, kz, 0, bar);
+    load_3d(Pt, &mapP, kx0, kz, 0, bar);
+  }
+  for (int b = tid; b < NM; b += NT) {
+    dls[b] = dl[b];
+    dus[b] = du[b];
+  }
+  __syncthreads();
+  // wait_limit polls; after giving up, thread 0 drains with the normal limit,
+  // so no copy into this CTA's shared memory is in flight when it leaves
+  const bool ok = mbar_wait(bar, 0, wait_limit);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) {
+      atomicOr(err, 4);
+      mbar_wait(bar, 0);
+    }
+    return;
+  }
+  const int m = tid % MT, kk = tid / MT;
+  if (H0 && kz == 0 && kx0 < klow) {
+    // the mixed form's box-scale modes (and any other mode of their tile):
+    // serial sweeps, one thread per mode
+    const int kx = kx0 + tid;
+    if (tid < MT && kx < s.N) {
+      V2 *c = Ct + tid;
+      const double *p = Pt + tid;
+      if (kx < klow) {
+        double *Hd = H0 + kx;
+        double g = 0.0, rprev = 0.0;
+        for (int b = 0; b < NM; ++b) {
+          double r = (double)c[b * MT].x;
+          if (b > 0) r = r - (dls[b] * rprev) * g;
+          rprev = p[b * MT];
+          g = r;
+          Hd[(long long)b * klow] = r;
+        }
+        double x = 0.0;
+        for (int b = NM - 1; b >= 0; --b) {
+          const double h = Hd[(long long)b * klow];
+          x = (b == NM - 1) ? h * p[b * MT] : (h - dus[b] * x) * p[b * MT];
+          Hd[(long long)b * klow] = x;
+          c[b * MT] = mk2<T>((T)0, (T)0);
+        }
+      } else {
+        double gx = 0.0, gy = 0.0, rprev = 0.0;
+        for (int b = 0; b < NM; ++b) {
+          const V2 cv = c[b * MT];
+          double rx = (double)cv.x, ry = (double)cv.y;
+          if (b > 0) {
+            const double w = dls[b] * rprev;
+            rx = rx - w * gx;
+            ry = ry - w * gy;
+          }
+          rprev = p[b * MT];
+          gx = rx;
+          gy = ry;
+          c[b * MT] = mk2<T>((T)rx, (T)ry);
+        }
+        double xx = 0.0, xy = 0.0;
+        for (int b = NM - 1; b >= 0; --b) {
+          const V2 cv = c[b * MT];
+          const double pv = p[b * MT];
+          if (b == NM - 1) {
+            xx = (double)cv.x * pv;
+            xy = (double)cv.y * pv;
+          } else {
+            xx = ((double)cv.x - dus[b] * xx) * pv;
+            xy = ((double)cv.y - dus[b] * xy) * pv;
+          }
+          c[b * MT] = mk2<T>((T)xx, (T)xy);
+        }
+      }
+    }
+  } else {
+    const bool act = kx0 + m < s.N;
+    const int Le = (NM + P - 1) / P, s0 = kk * Le;
+    const int nr = act ? max(0, min(Le, NM - s0)) : 0;
+    V2 *c = Ct + (size_t)s0 * MT + m;
+    const double *p = Pt + (size_t)s0 * MT + m;
+    // forward from g = 0 at the segment's start
+    double gx = 0.0, gy = 0.0, h = 1.0;
+    for (int u = 0; u < nr; ++u) {
+      const int b = s0 + u;
+      const V2 cv = c[u * MT];
+      double rx = (double)cv.x, ry = (double)cv.y;
+      double w = 0.0;
+      if (b > 0) {
+        w = dls[b] * p[(u - 1) * MT];  // l_b / d'_{b-1}
+        rx = rx - w * gx;
+        ry = ry - w * gy;
+      }
+      h = -w * h;
+      gx = rx;
+      gy = ry;
+      c[u * MT] = mk2<T>((T)rx, (T)ry);
+    }
+    mA[tid] = h;
+    mX[tid] = gx;
+    mY[tid] = gy;
+    __syncthreads();
+    // the value entering the segment: the maps of segments 0 .. kk-1 applied to 0
+    double ix = 0.0, iy = 0.0;
+    for (int q = 0; q < kk; ++q) {
+      const int o = q * MT + m;
+      ix = mX[o] + mA[o] * ix;
+      iy = mY[o] + mA[o] * iy;
+    }
+    h = 1.0;
+    for (int u = 0; u < nr; ++u) {
+      const int b = s0 + u;
+      const double w = b > 0 ? dls[b] * p[(u - 1) * MT] : 0.0;
+      h = -w * h;
+      const V2 cv = c[u * MT];
+      c[u * MT] = mk2<T>((T)((double)cv.x + h * ix), (T)((double)cv.y + h * iy));
+    }
+    // backward from x = 0 above the segment's top row
+    double xx = 0.0, xy = 0.0, kp = 1.0;
+    for (int u = nr - 1; u >= 0; --u) {
+      const int b = s0 + u;
+      const V2 cv = c[u * MT];
+      const double pv = p[u * MT];
+      double beta = 0.0;
+      if (b == NM - 1) {
+        xx = (double)cv.x * pv;
+        xy = (double)cv.y * pv;
+      } else {
+        xx = ((double)cv.x - dus[b] * xx) * pv;
+        xy = ((double)cv.y - dus[b] * xy) * pv;
+        beta = -dus[b] * pv;
+      }
+      kp = beta * kp;
+      c[u * MT] = mk2<T>((T)xx, (T)xy);
+    }
+    __syncthreads();  // every thread has read the forward maps
+    mA[tid] = kp;
+    mX[tid] = xx;
+    mY[tid] = xy;
+    __syncthreads();
+    // the value above the segment: the maps of segments P-1 .. kk+1 applied to 0
+    ix = iy = 0.0;
+    for (int q = P - 1; q > kk; --q) {
+      const int o = q * MT + m;
+      ix = mX[o] + mA[o] * ix;
+      iy = mY[o] + mA[o] * iy;
+    }
+    kp = 1.0;
+    for (int u = nr - 1; u >= 0; --u) {
+      const int b = s0 + u;
+      const double beta = b == NM - 1 ? 0.0 : -dus[b] * p[u * MT];
+      kp = beta * kp;
+      const V2 cv = c[u * MT];
+      c[u * MT] = mk2<T>((T)((double)cv.x + kp * ix), (T)((double)cv.y + kp * iy));
+    }
+  }
+  fence_async_shared();  // the solves' shared-memory writes before the TMA store reads them
+  __syncthreads();
+  if (tid == 0) {
     store_3d(&mapC, Ct, 2 * kx0, kz, 0);
     store_commit_and_wait_read();
   }
@@ -318,11 +406,16 @@ void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl,
   dim3 grid((s.N + MT - 1) / MT, s.MH);
   const int wl = wait_limit < 0 ? WAIT_LIMIT : wait_limit;
   if (scan) {
-    cudaFuncSetAttribute(k_thomas_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_thomas_tile<T, true><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+    // 16 segments of each mode's rows: 256 threads in FP32, 128 in FP64
+    // (at 814 x 257 x 193: FP32 y-solve 0.78 / 0.55 / 0.46 / 0.58 ms per step
+    // with 4 / 8 / 16 / 32 segments, FP64 0.63 / 0.59 / 0.68 with 8 / 16 / 32)
+    constexpr int NT = 16 * MT;
+    const size_t smw = tile_scan_smem<T, NT>(s.NM);
+    cudaFuncSetAttribute(k_thomas_tile_scan<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+    k_thomas_tile_scan<T, NT><<<grid, NT, smw, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
   } else {
-    cudaFuncSetAttribute(k_thomas_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_thomas_tile<T, false><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+    cudaFuncSetAttribute(k_thomas_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_thomas_tile<T><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
   }
 }
 

@@ -258,9 +258,9 @@ int blgpu_check_divergence_noalloc(const double *U, const double *V, const doubl
  * 8; FP64 DNS, all bit-identical: 1 = one point, global loads, 4 = one point,
  * TMA-fed planes, 2 = two points in a register window),
  * thomas (y-solve: 1 = register ring,
- * 2 = TMA-fed tiles where ny-1 <= 256, one lane per mode, 3 = the same
- * tiles with each mode's rows split over the warp's spare lanes; the
- * built-in choice is 3 in FP64 and 1 in the mixed form), idct_nw (lines per CTA of the
+ * 2 = TMA-fed tiles where ny-1 <= 256, one thread per mode, 3 = the same
+ * tiles with each mode's rows split over 16 threads; the built-in choice
+ * is 3 where ny-1 <= 256, else 1), idct_nw (lines per CTA of the
  * inverse DCT), xfft (x transforms: 1 = Stockham mixed-radix FFT in shared
  * memory, any N; 2 = two-pass register FFT, built for N = nx-2 = 812
  * (29 x 28; both precisions), 510 (17 x 30), 190 (19 x 10) and 126 (14 x 9)

@@ -86,8 +86,9 @@ def test_autotune_restores_state_and_keeps_results(gpu):
     assert same(before, states([s]))
     ref = cases.solver_for(c, precision=MIXED)
     ref.advance(2)  # the built-in tiles, as s before tuning
-    # the z-transform, RHS-form and x-transform choices are the knobs that move roundings
-    ref.set_tiles(zdft=s.tiles()["zdft"], rhs_pts=s.tiles()["rhs_pts"], xfft=s.tiles()["xfft"])
+    # the z-transform, RHS-form, x-transform and y-solve choices are the knobs that move roundings
+    ref.set_tiles(zdft=s.tiles()["zdft"], rhs_pts=s.tiles()["rhs_pts"], xfft=s.tiles()["xfft"],
+                  thomas=s.tiles()["thomas"])
     s.advance(3)
     ref.advance(3)
     assert same(states([ref]), states([s]))

@@ -50,17 +50,18 @@ def test_streamed_upload_reports_non_finite_at_sync(gpu):
     s.close()
 
 
-def test_y_solve_wait_limit_reports_and_recovers(gpu):
-    """The tiled y-solve's mbarrier wait given zero polls: every tile's wait
-    gives up at once, the CTAs drain their copies (normal limit) and leave,
-    the step reports BLGPU_EDEVICE through the device flag; with the limit
-    restored and the state uploaded again the context steps exactly as a
-    fresh one."""
+@pytest.mark.parametrize("thomas", [2, 3])
+def test_y_solve_wait_limit_reports_and_recovers(gpu, thomas):
+    """The tiled y-solve's mbarrier wait given zero polls (one lane per mode,
+    and the rows split over the lanes): every tile's wait gives up at once,
+    the CTAs drain their copies (normal limit) and leave, the step reports
+    BLGPU_EDEVICE through the device flag; with the limit restored and the
+    state uploaded again the context steps exactly as a fresh one."""
     c = _case()
     c.cfl = -1e-3
     s = cases.solver_for(c, precision=FP64)
-    assert s.tiles()["thomas"] in (0, 2)
-    s.set_tiles(thomas=2)
+    assert s.tiles()["thomas"] == 0
+    s.set_tiles(thomas=thomas)
     s.set_wait_limit(0)
     s.time_step()
     with pytest.raises(BlgpuError, match="y-solve"):
@@ -71,7 +72,7 @@ def test_y_solve_wait_limit_reports_and_recovers(gpu):
     s.set_dt(1e-3)
     s.advance(2)
     r = cases.solver_for(c, precision=FP64)
-    r.set_tiles(thomas=2)
+    r.set_tiles(thomas=thomas)
     r.advance(2)
     for a, b in zip(s.download_state()[:3], r.download_state()[:3]):
         assert np.array_equal(a, b)
@@ -87,7 +88,7 @@ def test_rhs_plane_wait_limit_reports_and_recovers(gpu):
     c = _case()
     c.cfl = -1e-3
     s = cases.solver_for(c, precision=MIXED)
-    s.set_tiles(rhs_pts=4)
+    s.set_tiles(rhs_pts=4, thomas=1)  # the register-ring y-solve waits on no mbarrier
     s.set_wait_limit(0)
     s.time_step()
     with pytest.raises(BlgpuError, match="RHS"):
@@ -98,7 +99,7 @@ def test_rhs_plane_wait_limit_reports_and_recovers(gpu):
     s.set_dt(1e-3)
     s.advance(2)
     r = cases.solver_for(c, precision=MIXED)
-    r.set_tiles(rhs_pts=4)
+    r.set_tiles(rhs_pts=4, thomas=1)
     r.advance(2)
     for a, b in zip(s.download_state()[:3], r.download_state()[:3]):
         assert np.array_equal(a, b)
