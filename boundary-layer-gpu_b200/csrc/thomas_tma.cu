@@ -170,8 +170,10 @@ __global__ void __launch_bounds__(32) k_thomas_tile(const __grid_constant__ CUte
 // second pass over its rows adds the product times that value.  The sums
 // are those of the serial sweeps, reassociated across the segments; the
 // serial chains are P times shorter and every thread of the CTA works.
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_thomas_tile_scan(const __grid_constant__ CUtensorMap mapC,
+// REG: the segment's rows stay in FP64 registers from one read of the tile
+// to the final write; otherwise each pass reads and writes the tile.
+template <typename T, int NT, bool REG>
+__global__ void __launch_bounds__(NT, 512 / NT) k_thomas_tile_scan(const __grid_constant__ CUtensorMap mapC,
                                                          const __grid_constant__ CUtensorMap mapP, Spec s,
                                                          const double *__restrict__ dl, const double *__restrict__ du,
                                                          double *__restrict__ H0, int klow, int *__restrict__ err,
@@ -263,6 +265,106 @@ __global__ void __launch_bounds__(NT) k_thomas_tile_scan(const __grid_constant__
           }
           c[b * MT] = mk2<T>((T)xx, (T)xy);
         }
+      }
+    }
+  } else if (REG) {
+    // the segment's rows in FP64 registers from one read of the tile to the
+    // final write (LMAX = 16 rows: NM <= 256 over 16 segments)
+    constexpr int LMAX = 16;
+    const bool act = kx0 + m < s.N;
+    const int Le = (NM + P - 1) / P, s0 = kk * Le;
+    const int nr = act ? max(0, min(Le, NM - s0)) : 0;
+    V2 *c = Ct + (size_t)s0 * MT + m;
+    const double *p = Pt + (size_t)s0 * MT + m;
+    double vx[LMAX], vy[LMAX], pv[LMAX + 1];  // pv[u] = piv[s0 + u - 1]
+    pv[0] = (nr > 0 && s0 > 0) ? p[-MT] : 0.0;
+#pragma unroll
+    for (int u = 0; u < LMAX; ++u) {
+      if (u < nr) {
+        const V2 cv = c[u * MT];
+        vx[u] = (double)cv.x;
+        vy[u] = (double)cv.y;
+        pv[u + 1] = p[u * MT];
+      } else {
+        vx[u] = vy[u] = pv[u + 1] = 0.0;
+      }
+    }
+    double gx = 0.0, gy = 0.0, h = 1.0;
+#pragma unroll
+    for (int u = 0; u < LMAX; ++u) {
+      if (u < nr) {
+        const int b = s0 + u;
+        double w = 0.0;
+        if (b > 0) {
+          w = dls[b] * pv[u];
+          vx[u] = vx[u] - w * gx;
+          vy[u] = vy[u] - w * gy;
+        }
+        h = -w * h;
+        gx = vx[u];
+        gy = vy[u];
+      }
+    }
+    mA[tid] = h;
+    mX[tid] = gx;
+    mY[tid] = gy;
+    __syncthreads();
+    double ix = 0.0, iy = 0.0;
+    for (int q = 0; q < kk; ++q) {
+      const int o = q * MT + m;
+      ix = mX[o] + mA[o] * ix;
+      iy = mY[o] + mA[o] * iy;
+    }
+    h = 1.0;
+#pragma unroll
+    for (int u = 0; u < LMAX; ++u) {
+      if (u < nr) {
+        const int b = s0 + u;
+        const double w = b > 0 ? dls[b] * pv[u] : 0.0;
+        h = -w * h;
+        vx[u] = vx[u] + h * ix;
+        vy[u] = vy[u] + h * iy;
+      }
+    }
+    double xx = 0.0, xy = 0.0, kp = 1.0;
+#pragma unroll
+    for (int u = LMAX - 1; u >= 0; --u) {
+      if (u < nr) {
+        const int b = s0 + u;
+        const double q = pv[u + 1];
+        double beta = 0.0;
+        if (b == NM - 1) {
+          xx = vx[u] * q;
+          xy = vy[u] * q;
+        } else {
+          xx = (vx[u] - dus[b] * xx) * q;
+          xy = (vy[u] - dus[b] * xy) * q;
+          beta = -dus[b] * q;
+        }
+        kp = beta * kp;
+        vx[u] = xx;
+        vy[u] = xy;
+      }
+    }
+    __syncthreads();  // every thread has read the forward maps
+    mA[tid] = kp;
+    mX[tid] = xx;
+    mY[tid] = xy;
+    __syncthreads();
+    ix = iy = 0.0;
+    for (int q = P - 1; q > kk; --q) {
+      const int o = q * MT + m;
+      ix = mX[o] + mA[o] * ix;
+      iy = mY[o] + mA[o] * iy;
+    }
+    kp = 1.0;
+#pragma unroll
+    for (int u = LMAX - 1; u >= 0; --u) {
+      if (u < nr) {
+        const int b = s0 + u;
+        const double beta = b == NM - 1 ? 0.0 : -dus[b] * pv[u + 1];
+        kp = beta * kp;
+        c[u * MT] = mk2<T>((T)(vx[u] + kp * ix), (T)(vy[u] + kp * iy));
       }
     }
   } else {
@@ -411,8 +513,16 @@ void launch_thomas_tile(const Spec &s, const ThomasMaps &maps, const double *dl,
     // with 4 / 8 / 16 / 32 segments, FP64 0.63 / 0.59 / 0.68 with 8 / 16 / 32)
     constexpr int NT = 16 * MT;
     const size_t smw = tile_scan_smem<T, NT>(s.NM);
-    cudaFuncSetAttribute(k_thomas_tile_scan<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
-    k_thomas_tile_scan<T, NT><<<grid, NT, smw, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+    // FP64: each segment's rows in registers (0.59 -> 0.50 ms per step at
+    // 814 x 257 x 193); FP32: in the tile (0.44 against 0.52 ms per step
+    // in registers, at two CTAs per SM)
+    if (sizeof(T) == 8) {
+      cudaFuncSetAttribute(k_thomas_tile_scan<T, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+      k_thomas_tile_scan<T, NT, true><<<grid, NT, smw, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+    } else {
+      cudaFuncSetAttribute(k_thomas_tile_scan<T, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+      k_thomas_tile_scan<T, NT, false><<<grid, NT, smw, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
+    }
   } else {
     cudaFuncSetAttribute(k_thomas_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_thomas_tile<T><<<grid, 32, sm, st>>>(mc, mp, s, dl, du, H0, klow, err, wl);
