@@ -100,6 +100,18 @@ def write_rescaling(path, Umean, Vmean):
     check_io(load().blgpu_write_rescaling(str(path).encode(), len(um), len(vm), _p(um), _p(vm)))
 
 
+def read_inflow_profile(path, ny=None):
+    """inflow_file of inflow flags 2 and 5: (U_inlet at the ny+1 centres,
+    V_inlet at the ny faces); ny (the grid's) defaults to the file's."""
+    lib = load()
+    n = ctypes.c_int()
+    check_io(lib.blgpu_read_inflow_profile_info(str(path).encode(), ctypes.byref(n)))
+    ny = n.value if ny is None else int(ny)
+    U, V = np.zeros(ny + 1), np.zeros(ny)
+    check_io(lib.blgpu_read_inflow_profile(str(path).encode(), ny, _p(U), _p(V)))
+    return U, V
+
+
 def snapshot_name(fileout, step):
     buf = ctypes.create_string_buffer(4096)
     check_io(load().blgpu_snapshot_name(str(fileout).encode(), int(step), buf, 4096))

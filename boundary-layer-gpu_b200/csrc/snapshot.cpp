@@ -501,6 +501,58 @@ int blgpu_read_rescaling(const char *path, int nyg, int ny, double *Umean, doubl
   return BLGPU_OK;
 }
 
+// Inflow profile of inflow flags 2 and 5 (boundary_conditions.f90:1405-1413,
+// 1550-1558): a stream file holding ny (int32), U_inlet (ny+1 doubles, at
+// the centres yg) and V_inlet (ny doubles, at the faces y).  The reference
+// reads it in the byte order its runtime is set to (the GPU build exports
+// F_UFMTENDIAN=big); the files it ships are of both orders, so the size
+// record tells them apart.  The file's ny must equal the grid's, as there.
+static int inflow_open(const char *path, File &F, int32_t *n, bool *swap) {
+  F.f = fopen(path, "rb");
+  if (!F.f) return io_err(BLGPU_EINVAL, "%s: cannot open (%s)", path, strerror(errno));
+  if (!rd(F.f, n, 4)) return io_err(BLGPU_EINVAL, "%s: truncated", path);
+  if (fseek(F.f, 0, SEEK_END) != 0) return io_err(BLGPU_EINVAL, "%s: cannot seek", path);
+  const long size = ftell(F.f);
+  if (fseek(F.f, 4, SEEK_SET) != 0) return io_err(BLGPU_EINVAL, "%s: cannot seek", path);
+  // the order whose ny makes the file 4 + 8 (2 ny + 1) bytes long
+  const auto fits = [size](int32_t v) { return v > 0 && v < (1 << 24) && size == 4 + 8 * (2L * v + 1); };
+  *swap = false;
+  if (!fits(*n)) {
+    if (!fits(bswap32(*n))) return io_err(BLGPU_EINVAL, "%s: not an inflow profile (%ld bytes)", path, size);
+    *n = bswap32(*n);
+    *swap = true;
+  }
+  return BLGPU_OK;
+}
+
+int blgpu_read_inflow_profile_info(const char *path, int *ny) {
+  if (!path || !ny) return io_err(BLGPU_EINVAL, "blgpu_read_inflow_profile_info: null argument");
+  File F;
+  int32_t n;
+  bool swap;
+  int rc = inflow_open(path, F, &n, &swap);
+  if (rc) return rc;
+  *ny = n;
+  return BLGPU_OK;
+}
+
+int blgpu_read_inflow_profile(const char *path, int ny, double *U_inlet, double *V_inlet) {
+  if (!path || !U_inlet || !V_inlet) return io_err(BLGPU_EINVAL, "blgpu_read_inflow_profile: null argument");
+  File F;
+  int32_t n;
+  bool swap;
+  int rc = inflow_open(path, F, &n, &swap);
+  if (rc) return rc;
+  if (n != ny) return io_err(BLGPU_EINVAL, "Profile doesnt match dimensions %d %d", n, ny);
+  if (!rd(F.f, U_inlet, (size_t)(ny + 1) * 8) || !rd(F.f, V_inlet, (size_t)ny * 8))
+    return io_err(BLGPU_EINVAL, "%s: truncated", path);
+  if (swap) {
+    for (int j = 0; j <= ny; ++j) U_inlet[j] = bswapd(U_inlet[j]);
+    for (int j = 0; j < ny; ++j) V_inlet[j] = bswapd(V_inlet[j]);
+  }
+  return BLGPU_OK;
+}
+
 int blgpu_write_rescaling(const char *path, int nyg, int ny, const double *Umean, const double *Vmean) {
   if (!path || !Umean || !Vmean) return io_err(BLGPU_EINVAL, "blgpu_write_rescaling: null argument");
   File F;

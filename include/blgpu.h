@@ -418,6 +418,14 @@ int blgpu_write_snapshot(const char *path, int nx, int ny, int nz, double t, dou
  * reads big-endian, input_output.f90:445,671) */
 int blgpu_read_rescaling(const char *path, int nyg, int ny, double *Umean, double *Vmean);
 int blgpu_write_rescaling(const char *path, int nyg, int ny, const double *Umean, const double *Vmean);
+/* inflow_file of inflow flags 2 and 5 (boundary_conditions.f90:1405-1413,
+ * 1550-1558; written by the reference's generate_inflow scripts): ny
+ * (int32), U_inlet(ny+1) at the centres yg, V_inlet(ny) at the faces y,
+ * in either byte order (told apart by the file size); the _info call
+ * returns the file's ny, the read refuses a ny other than the grid's
+ * ("Profile doesnt match dimensions"). */
+int blgpu_read_inflow_profile_info(const char *path, int *ny);
+int blgpu_read_inflow_profile(const char *path, int ny, double *U_inlet, double *V_inlet);
 /* fileout.%08d (input_output.f90:516-518) */
 int blgpu_snapshot_name(const char *fileout, int step, char *name, int cap);
 /* output_data (input_output.f90:496-680) for a context: downloads the state,

@@ -5,6 +5,10 @@ as the first argument).  Reads, never executes, the reference's data files:
   - laminar_test/blasius_solution.dat  (Blasius table, eta/f/f' rows)
   - transition_test/temporal_modes_inlet.dat (binary TS inflow modes: the
     header and a checksum of the payload are kept)
+  - laminar_test/Mean_profile_Retheta1100_ny32_Ly0.40.dat and
+    tests/Mean_profile_Retheta1100_ny192_Ly0.60.dat (inflow profiles of
+    inflow flags 2 and 5: ny, U_inlet(ny+1), V_inlet(ny); decoded here with
+    numpy in the byte order that makes the file size match)
 and writes small JSON fixtures the CPU tests compare against.
 """
 import hashlib
@@ -43,6 +47,23 @@ def main(ref):
                "zmode": zm.tolist(), "tmode": tm.tolist(),
                "q_abs_sum": [float(np.abs(q[i * nq:(i + 1) * nq]).sum()) for i in range(6)]},
               open(os.path.join(out, "temporal_modes_ref.json"), "w"), indent=1)
+
+
+    profs = []
+    for rel in ("laminar_test/Mean_profile_Retheta1100_ny32_Ly0.40.dat",
+                "tests/Mean_profile_Retheta1100_ny192_Ly0.60.dat"):
+        raw = open(os.path.join(ref, rel), "rb").read()
+        for order in ("<", ">"):
+            ny = struct.unpack(order + "i", raw[:4])[0]
+            if 0 < ny < 1 << 24 and len(raw) == 4 + 8 * (2 * ny + 1):
+                break
+        else:
+            raise ValueError(rel + ": not an inflow profile")
+        d = np.frombuffer(raw, order + "f8", 2 * ny + 1, 4)
+        profs.append({"source": rel, "bytes": len(raw), "sha256": hashlib.sha256(raw).hexdigest(),
+                      "order": "little" if order == "<" else "big", "ny": ny,
+                      "U_inlet": d[:ny + 1].tolist(), "V_inlet": d[ny + 1:].tolist()})
+    json.dump(profs, open(os.path.join(out, "inflow_profiles_ref.json"), "w"), indent=0)
 
 
 if __name__ == "__main__":

@@ -204,3 +204,58 @@ def test_params_les_flag_maps_to_config(tmp_path):
     dynamic model with the coefficient averaged in z)."""
     p = files.read_params(write_turbb(tmp_path / "l.turbb", "inflow_file = a\nLES = 2\n"))
     assert p["LES"] == 2 and p["config"]["les_model"] == 2
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "inflow_profiles_ref.json")
+
+
+def _write_profile(path, ny, U, V, order):
+    with open(path, "wb") as f:
+        f.write(struct.pack(order + "i", ny))
+        f.write(np.asarray(U, dtype=order + "f8").tobytes())
+        f.write(np.asarray(V, dtype=order + "f8").tobytes())
+    return str(path)
+
+
+def test_inflow_profiles_of_the_reference(tmp_path):
+    """inflow_file of inflow flags 2 and 5 (boundary_conditions.f90:1405-1413,
+    1550-1558): the reference's two profile files, one little- and one
+    big-endian (tests/golden/inflow_profiles_ref.json, decoded from them by
+    make_golden.py), written back in their byte order and read through the C
+    ABI to the bit; the file's ny must equal the grid's."""
+    import json
+    profs = json.load(open(GOLDEN))
+    assert {p["order"] for p in profs} == {"little", "big"}
+    for p in profs:
+        ny = p["ny"]
+        f = _write_profile(tmp_path / os.path.basename(p["source"]), ny, p["U_inlet"], p["V_inlet"],
+                           "<" if p["order"] == "little" else ">")
+        assert os.path.getsize(f) == p["bytes"]
+        U, V = files.read_inflow_profile(f)
+        assert U.shape == (ny + 1,) and V.shape == (ny,)
+        assert np.array_equal(U, np.array(p["U_inlet"])) and np.array_equal(V, np.array(p["V_inlet"]))
+        U2, V2 = files.read_inflow_profile(f, ny)
+        assert np.array_equal(U, U2) and np.array_equal(V, V2)
+        with pytest.raises(BlgpuError, match="Profile doesnt match dimensions"):
+            files.read_inflow_profile(f, ny + 1)
+
+
+def test_inflow_profile_errors(tmp_path):
+    f = _write_profile(tmp_path / "short.dat", 8, np.ones(9), np.ones(7), "<")  # one V value missing
+    with pytest.raises(BlgpuError, match="not an inflow profile"):
+        files.read_inflow_profile(f)
+    with pytest.raises(BlgpuError, match="cannot open"):
+        files.read_inflow_profile(str(tmp_path / "absent.dat"))
+
+
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="BLGPU_REFERENCE_DIR not set")
+def test_inflow_profile_files_in_the_reference_tree():
+    """The profiles read straight from the reference tree equal the golden
+    fixture (which pins the fixture to the files)."""
+    import hashlib
+    import json
+    for p in json.load(open(GOLDEN)):
+        path = os.path.join(REF, p["source"])
+        assert hashlib.sha256(open(path, "rb").read()).hexdigest() == p["sha256"]
+        U, V = files.read_inflow_profile(path)
+        assert np.array_equal(U, np.array(p["U_inlet"])) and np.array_equal(V, np.array(p["V_inlet"]))
