@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <strings.h>
 #include <string>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -157,8 +158,8 @@ struct Reader {
 };
 
 // ---------------------------------------------------------------------------
-// binary helpers (stream access, native little-endian, as the reference's
-// unformatted stream files on x86)
+// binary helpers (stream access, as the reference's unformatted stream
+// files: native little-endian on x86, or big-endian, below)
 // ---------------------------------------------------------------------------
 struct File {
   FILE *f = nullptr;
@@ -183,35 +184,82 @@ double bswapd(double v) {
   return v;
 }
 
+// Byte order of the unformatted files.  The reference's GPU build runs with
+// F_UFMTENDIAN=big (its Makefile exports it), so its snapshots, Lund means
+// and inflow profiles are big-endian there and native (little-endian) in
+// the CPU build; readers here take either order, writers follow the same
+// variable: "big" makes every file big-endian (a unit list after ':' is
+// not modelled and leaves the native order).
+bool out_swapped() {
+  const char *e = getenv("F_UFMTENDIAN");
+  return e && strncasecmp(e, "big", 3) == 0 && e[3] == '\0';
+}
+void swap_n(int32_t *v, size_t n) {
+  for (size_t i = 0; i < n; ++i) v[i] = bswap32(v[i]);
+}
+void swap_n(double *v, size_t n) {
+  for (size_t i = 0; i < n; ++i) v[i] = bswapd(v[i]);
+}
+bool rd_i(FILE *f, int32_t *v, size_t n, bool sw) {
+  if (!rd(f, v, n * 4)) return false;
+  if (sw) swap_n(v, n);
+  return true;
+}
+bool rd_d(FILE *f, double *v, size_t n, bool sw) {
+  if (!rd(f, v, n * 8)) return false;
+  if (sw) swap_n(v, n);
+  return true;
+}
+bool wr_i(FILE *f, const int32_t *v, size_t n, bool sw) {
+  if (!sw) return wr(f, v, n * 4);
+  std::vector<int32_t> t(v, v + n);
+  swap_n(t.data(), n);
+  return wr(f, t.data(), n * 4);
+}
+bool wr_d(FILE *f, const double *v, size_t n, bool sw) {
+  if (!sw) return wr(f, v, n * 8);
+  const size_t chunk = 1 << 16;
+  std::vector<double> t(n < chunk ? n : chunk);
+  for (size_t i = 0; i < n; i += chunk) {
+    const size_t m = n - i < chunk ? n - i : chunk;
+    memcpy(t.data(), v + i, m * 8);
+    swap_n(t.data(), m);
+    if (!wr(f, t.data(), m * 8)) return false;
+  }
+  return true;
+}
+
 struct Layout {
   long long header = 0;                // bytes before the U size record
   int n[3][3] = {};                    // U, V, W dims from their size records
   int planes[5] = {};                  // planes stored of U, V, W, nu_t, P
   bool has_tail = false;               // nu_t and P present
+  bool swap = false;                   // big-endian file
 };
 
 // the snapshot's header (metadata and mesh) into h and, if non-null, x/y/z
-int read_header(FILE *f, blgpu_snapshot_info *h, double *x, double *y, double *z, long long *pos) {
+int read_header(FILE *f, bool sw, blgpu_snapshot_info *h, double *x, double *y, double *z, long long *pos) {
   double tn[2];
   int32_t a;
-  if (!rd(f, tn, 16) || !rd(f, &a, 4)) return io_err(BLGPU_EINVAL, "snapshot: truncated header");
+  if (fseek(f, 0, SEEK_SET) != 0 || !rd_d(f, tn, 2, sw) || !rd_i(f, &a, 1, sw))
+    return io_err(BLGPU_EINVAL, "snapshot: truncated header");
   h->t = tn[0];
   h->nu = tn[1];
   h->step = -1;
   if (a == -73) {  // magic number, then the step, then nx
     int32_t st;
-    if (!rd(f, &st, 4) || !rd(f, &a, 4)) return io_err(BLGPU_EINVAL, "snapshot: truncated header");
+    if (!rd_i(f, &st, 1, sw) || !rd_i(f, &a, 1, sw)) return io_err(BLGPU_EINVAL, "snapshot: truncated header");
     h->step = st;
   }
   int32_t n[6];
   n[0] = a;
   double *dst[6] = {x, y, z, nullptr, nullptr, nullptr};
   for (int q = 0; q < 6; ++q) {
-    if (q > 0 && !rd(f, &n[q], 4)) return io_err(BLGPU_EINVAL, "snapshot: truncated mesh record %d", q);
+    if (q > 0 && !rd_i(f, &n[q], 1, sw)) return io_err(BLGPU_EINVAL, "snapshot: truncated mesh record %d", q);
     if (n[q] < 2 || n[q] > (1 << 24)) return io_err(BLGPU_EINVAL, "snapshot: mesh record %d has size %d", q, n[q]);
     const size_t bytes = (size_t)n[q] * 8;
     if (dst[q]) {
-      if (!rd(f, dst[q], bytes)) return io_err(BLGPU_EINVAL, "snapshot: truncated mesh record %d", q);
+      if (!rd_d(f, dst[q], (size_t)n[q], sw)) return io_err(BLGPU_EINVAL, "snapshot: truncated mesh record %d", q);
     } else if (fseek(f, (long)bytes, SEEK_CUR) != 0) {
       return io_err(BLGPU_EINVAL, "snapshot: truncated mesh record %d", q);
     }
@@ -259,7 +307,7 @@ int layout(FILE *f, const blgpu_snapshot_info &h, long long pos, Layout &L) {
   long long at = pos;
   for (int q = 0; q < 3; ++q) {
     int32_t r[3];
-    if (fseek(f, (long)at, SEEK_SET) != 0 || !rd(f, r, 12)) return io_err(BLGPU_EINVAL, "snapshot: truncated");
+    if (fseek(f, (long)at, SEEK_SET) != 0 || !rd_i(f, r, 3, L.swap)) return io_err(BLGPU_EINVAL, "snapshot: truncated");
     if (r[0] != dims[q][0] || r[1] != dims[q][1] || r[2] != dims[q][2])
       return io_err(BLGPU_EINVAL, "snapshot: field %d size record %d %d %d, expected %lld %lld %lld", q, r[0], r[1],
                     r[2], dims[q][0], dims[q][1], dims[q][2]);
@@ -269,27 +317,54 @@ int layout(FILE *f, const blgpu_snapshot_info &h, long long pos, Layout &L) {
   return BLGPU_OK;
 }
 
+// the header and the layout in the byte order that fits the file: native
+// first, then swapped (a wrong order gives implausible sizes)
+int header_and_layout(FILE *f, blgpu_snapshot_info *h, double *x, double *y, double *z, long long *pos, Layout &L) {
+  std::string native_err;
+  for (int sw = 0; sw < 2; ++sw) {
+    // sizes first (the mesh skipped): the caller's arrays are filled only
+    // once the order is known
+    blgpu_snapshot_info hh = *h;
+    long long p = 0;
+    int rc = read_header(f, sw != 0, &hh, nullptr, nullptr, nullptr, &p);
+    if (!rc) {
+      Layout LL;
+      LL.swap = sw != 0;
+      rc = layout(f, hh, p, LL);
+      if (!rc && (x || y || z)) rc = read_header(f, sw != 0, &hh, x, y, z, &p);
+      if (!rc) {
+        *h = hh;
+        *pos = p;
+        L = LL;
+        return BLGPU_OK;
+      }
+    }
+    if (!sw) native_err = g_io_error;
+  }
+  return io_err(BLGPU_EINVAL, "%s", native_err.c_str());
+}
+
 // one field: size record then `planes` planes of n1 x n2; a plane left out
 // (k = n3) is filled as the z-periodic boundary pass fills it
 // (boundary_conditions.f90:204-216): plane 3 for centred fields, 2 for W.
-int read_field(FILE *f, long long n1, long long n2, long long n3, long long planes, bool w_face, double *dst) {
+int read_field(FILE *f, long long n1, long long n2, long long n3, long long planes, bool w_face, bool sw, double *dst) {
   if (fseek(f, 12, SEEK_CUR) != 0) return io_err(BLGPU_EINVAL, "snapshot: truncated field");
   const size_t pl = (size_t)(n1 * n2);
   if (!dst) {
     if (fseek(f, (long)(pl * planes * 8), SEEK_CUR) != 0) return io_err(BLGPU_EINVAL, "snapshot: truncated field");
     return BLGPU_OK;
   }
-  if (!rd(f, dst, pl * planes * 8)) return io_err(BLGPU_EINVAL, "snapshot: truncated field data");
+  if (!rd_d(f, dst, pl * planes, sw)) return io_err(BLGPU_EINVAL, "snapshot: truncated field data");
   if (planes < n3) memcpy(dst + pl * (n3 - 1), dst + pl * (w_face ? 1 : 2), pl * 8);
   return BLGPU_OK;
 }
 
-int write_field(FILE *f, int n1, int n2, int n3, int planes, const double *src) {
+int write_field(FILE *f, int n1, int n2, int n3, int planes, bool sw, const double *src) {
   const int32_t r[3] = {n1, n2, n3};
-  if (!wr(f, r, 12)) return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
-  const size_t bytes = (size_t)n1 * n2 * planes * 8;
+  if (!wr_i(f, r, 3, sw)) return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
   if (src) {
-    if (!wr(f, src, bytes)) return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
+    if (!wr_d(f, src, (size_t)n1 * n2 * planes, sw))
+      return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
   } else {
     std::vector<double> zero((size_t)n1 * n2, 0.0);
     for (int k = 0; k < planes; ++k)
@@ -404,10 +479,8 @@ int blgpu_snapshot_info_read(const char *path, blgpu_snapshot_info *h) {
   F.f = fopen(path, "rb");
   if (!F.f) return io_err(BLGPU_EINVAL, "snapshot %s: cannot open (%s)", path, strerror(errno));
   long long pos = 0;
-  int rc = read_header(F.f, h, nullptr, nullptr, nullptr, &pos);
-  if (rc) return rc;
   Layout L;
-  rc = layout(F.f, *h, pos, L);
+  int rc = header_and_layout(F.f, h, nullptr, nullptr, nullptr, &pos, L);
   if (rc) return rc;
   h->full_planes = (L.planes[0] == h->nz + 1) ? 1 : 0;
   h->has_nu_t_p = L.has_tail ? 1 : 0;
@@ -421,20 +494,19 @@ int blgpu_read_snapshot(const char *path, blgpu_snapshot_info *h, double *x, dou
   F.f = fopen(path, "rb");
   if (!F.f) return io_err(BLGPU_EINVAL, "snapshot %s: cannot open (%s)", path, strerror(errno));
   long long pos = 0;
-  int rc = read_header(F.f, h, x, y, z, &pos);
-  if (rc) return rc;
   Layout L;
-  if ((rc = layout(F.f, *h, pos, L))) return rc;
+  int rc = header_and_layout(F.f, h, x, y, z, &pos, L);
+  if (rc) return rc;
   h->full_planes = (L.planes[0] == h->nz + 1) ? 1 : 0;
   h->has_nu_t_p = L.has_tail ? 1 : 0;
   const long long nx = h->nx, ny = h->ny, nz = h->nz, nxg = nx + 1, nyg = ny + 1, nzg = nz + 1;
   if (fseek(F.f, (long)pos, SEEK_SET) != 0) return io_err(BLGPU_EINVAL, "snapshot: cannot seek");
-  if ((rc = read_field(F.f, nx, nyg, nzg, L.planes[0], false, U))) return rc;
-  if ((rc = read_field(F.f, nxg, ny, nzg, L.planes[1], false, V))) return rc;
-  if ((rc = read_field(F.f, nxg, nyg, nz, L.planes[2], true, W))) return rc;
+  if ((rc = read_field(F.f, nx, nyg, nzg, L.planes[0], false, L.swap, U))) return rc;
+  if ((rc = read_field(F.f, nxg, ny, nzg, L.planes[1], false, L.swap, V))) return rc;
+  if ((rc = read_field(F.f, nxg, nyg, nz, L.planes[2], true, L.swap, W))) return rc;
   if (L.has_tail) {
-    if ((rc = read_field(F.f, nxg, nyg, nzg, L.planes[3], false, nu_t))) return rc;
-    if ((rc = read_field(F.f, nxg, nyg, nzg, L.planes[4], false, P))) return rc;
+    if ((rc = read_field(F.f, nxg, nyg, nzg, L.planes[3], false, L.swap, nu_t))) return rc;
+    if ((rc = read_field(F.f, nxg, nyg, nzg, L.planes[4], false, L.swap, P))) return rc;
   } else {
     if (nu_t) memset(nu_t, 0, (size_t)(nxg * nyg * nzg) * 8);
     if (P) memset(P, 0, (size_t)(nxg * nyg * nzg) * 8);
@@ -451,29 +523,31 @@ int blgpu_write_snapshot(const char *path, int nx, int ny, int nz, double t, dou
   F.f = fopen(path, "wb");
   if (!F.f) return io_err(BLGPU_EINVAL, "snapshot %s: cannot create (%s)", path, strerror(errno));
   FILE *f = F.f;
+  const bool sw = out_swapped();
   const int nxg = nx + 1, nyg = ny + 1, nzg = nz + 1;
   const double tn[2] = {t, nu};
   const int32_t magic[2] = {-73, step};
-  if (!wr(f, tn, 16) || !wr(f, magic, 8)) return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
+  if (!wr_d(f, tn, 2, sw) || !wr_i(f, magic, 2, sw))
+    return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
   // faces, then centres xm(i) = (x(i)+x(i+1))/2 (initialization.f90:181-189)
   const double *fc[3] = {x, y, z};
   const int nf[3] = {nx, ny, nz};
   for (int q = 0; q < 3; ++q) {
     const int32_t n = nf[q];
-    if (!wr(f, &n, 4) || !wr(f, fc[q], (size_t)n * 8)) return io_err(BLGPU_EINVAL, "snapshot: write failed");
+    if (!wr_i(f, &n, 1, sw) || !wr_d(f, fc[q], (size_t)n, sw)) return io_err(BLGPU_EINVAL, "snapshot: write failed");
   }
   for (int q = 0; q < 3; ++q) {
     const int32_t n = nf[q] - 1;
     std::vector<double> m((size_t)n);
     for (int i = 0; i < n; ++i) m[i] = 0.5 * (fc[q][i] + fc[q][i + 1]);
-    if (!wr(f, &n, 4) || !wr(f, m.data(), (size_t)n * 8)) return io_err(BLGPU_EINVAL, "snapshot: write failed");
+    if (!wr_i(f, &n, 1, sw) || !wr_d(f, m.data(), (size_t)n, sw)) return io_err(BLGPU_EINVAL, "snapshot: write failed");
   }
   int rc;
-  if ((rc = write_field(f, nx, nyg, nzg, nzg - 1, U))) return rc;
-  if ((rc = write_field(f, nxg, ny, nzg, nzg - 1, V))) return rc;
-  if ((rc = write_field(f, nxg, nyg, nz, nz - 1, W))) return rc;
-  if ((rc = write_field(f, nxg, nyg, nzg, nzg - 1, nu_t))) return rc;
-  if ((rc = write_field(f, nxg, nyg, nzg, nzg, P))) return rc;
+  if ((rc = write_field(f, nx, nyg, nzg, nzg - 1, sw, U))) return rc;
+  if ((rc = write_field(f, nxg, ny, nzg, nzg - 1, sw, V))) return rc;
+  if ((rc = write_field(f, nxg, nyg, nz, nz - 1, sw, W))) return rc;
+  if ((rc = write_field(f, nxg, nyg, nzg, nzg - 1, sw, nu_t))) return rc;
+  if ((rc = write_field(f, nxg, nyg, nzg, nzg, sw, P))) return rc;
   if (fflush(f) != 0) return io_err(BLGPU_EINVAL, "snapshot: write failed (%s)", strerror(errno));
   return BLGPU_OK;
 }
@@ -559,7 +633,8 @@ int blgpu_write_rescaling(const char *path, int nyg, int ny, const double *Umean
   F.f = fopen(path, "wb");
   if (!F.f) return io_err(BLGPU_EINVAL, "%s: cannot create (%s)", path, strerror(errno));
   const int32_t n = nyg;
-  if (!wr(F.f, &n, 4) || !wr(F.f, Umean, (size_t)nyg * 8) || !wr(F.f, Vmean, (size_t)ny * 8))
+  const bool sw = out_swapped();
+  if (!wr_i(F.f, &n, 1, sw) || !wr_d(F.f, Umean, (size_t)nyg, sw) || !wr_d(F.f, Vmean, (size_t)ny, sw))
     return io_err(BLGPU_EINVAL, "%s: write failed (%s)", path, strerror(errno));
   return BLGPU_OK;
 }

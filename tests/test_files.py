@@ -136,15 +136,15 @@ def test_snapshot_layout_and_round_trip(tmp_path):
     assert np.array_equal(s["P"], P)
 
 
-def write_full(path, t, nu, step, x, y, z, fields, magic=True, tail=True):
+def write_full(path, t, nu, step, x, y, z, fields, magic=True, tail=True, order="<"):
     with open(path, "wb") as f:
-        f.write(struct.pack("dd", t, nu))
+        f.write(struct.pack(order + "dd", t, nu))
         if magic:
-            f.write(struct.pack("ii", -73, step))
+            f.write(struct.pack(order + "ii", -73, step))
         for a in (x, y, z, 0.5 * (x[:-1] + x[1:]), 0.5 * (y[:-1] + y[1:]), 0.5 * (z[:-1] + z[1:])):
-            f.write(struct.pack("i", len(a)) + np.asarray(a, "<f8").tobytes())
+            f.write(struct.pack(order + "i", len(a)) + np.asarray(a, order + "f8").tobytes())
         for a in (fields if tail else fields[:3]):
-            f.write(struct.pack("iii", *a.shape) + np.asarray(a, "<f8").tobytes(order="F"))
+            f.write(struct.pack(order + "iii", *a.shape) + np.asarray(a, order + "f8").tobytes(order="F"))
 
 
 def test_snapshot_full_layout_and_older_files(tmp_path):
@@ -259,3 +259,50 @@ def test_inflow_profile_files_in_the_reference_tree():
         assert hashlib.sha256(open(path, "rb").read()).hexdigest() == p["sha256"]
         U, V = files.read_inflow_profile(path)
         assert np.array_equal(U, np.array(p["U_inlet"])) and np.array_equal(V, np.array(p["V_inlet"]))
+
+
+def test_snapshot_big_endian_files(tmp_path):
+    """The reference's GPU build runs with F_UFMTENDIAN=big (its Makefile
+    exports it), so its snapshots are big-endian: read in either order, the
+    order told by which one gives a consistent header and layout (sizes
+    such as nx = 512 look plausible in both orders; the layout decides)."""
+    for nx, ny, nz in ((8, 6, 7), (512, 3, 3)):
+        x, y, z, U, V, W, nt, P = box(nx, ny, nz, 5)
+        for magic, tail in ((True, True), (False, False)):
+            path = tmp_path / ("be_%d_%d" % (nx, magic))
+            write_full(path, 0.75, 3e-5, 11, x, y, z, [U, V, W, nt, P], magic=magic, tail=tail, order=">")
+            s = files.read_snapshot(path)
+            assert s["t"] == 0.75 and s["step"] == (11 if magic else -1) and s["full_planes"] == 1
+            assert np.array_equal(s["x"], x) and np.array_equal(s["z"], z)
+            for k, a in (zip(("U", "V", "W", "nu_t", "P"), (U, V, W, nt, P)) if tail else
+                         zip(("U", "V", "W"), (U, V, W))):
+                assert np.array_equal(s[k], a)
+
+
+def test_writers_follow_F_UFMTENDIAN(tmp_path, monkeypatch):
+    """F_UFMTENDIAN=big makes the snapshot and Lund-means writers big-endian,
+    as the NVHPC runtime does for the reference's files; the readers take
+    the result back to the bit; a unit list leaves the native order."""
+    nx, ny, nz = 9, 7, 6
+    x, y, z, U, V, W, nt, P = box(nx, ny, nz, 6)
+    files.write_snapshot(tmp_path / "le", 1.5, 1e-5, 3, x, y, z, U, V, W, nt, P)
+    monkeypatch.setenv("F_UFMTENDIAN", "big")
+    files.write_snapshot(tmp_path / "be", 1.5, 1e-5, 3, x, y, z, U, V, W, nt, P)
+    um, vm = np.linspace(0.0, 1.0, ny + 1), np.linspace(-1.0, 0.0, ny)
+    files.write_rescaling(tmp_path / "mbe", um, vm)
+    monkeypatch.setenv("F_UFMTENDIAN", "big:10,11")
+    files.write_rescaling(tmp_path / "mle", um, vm)
+    monkeypatch.delenv("F_UFMTENDIAN")
+    le, be = (tmp_path / "le").read_bytes(), (tmp_path / "be").read_bytes()
+    assert len(le) == len(be) and le != be
+    assert struct.unpack(">2d2i", be[:24]) == (1.5, 1e-5, -73, 3)
+    a, b = files.read_snapshot(tmp_path / "le"), files.read_snapshot(tmp_path / "be")
+    for k in ("x", "y", "z", "U", "V", "W", "nu_t", "P"):
+        assert np.array_equal(a[k], b[k])
+    assert (tmp_path / "mbe").read_bytes() == struct.pack(">i", ny + 1) + um.astype(">f8").tobytes() + \
+        vm.astype(">f8").tobytes()
+    assert (tmp_path / "mle").read_bytes() == struct.pack("<i", ny + 1) + um.astype("<f8").tobytes() + \
+        vm.astype("<f8").tobytes()
+    for f in ("mbe", "mle"):
+        c, d = files.read_rescaling(tmp_path / f, ny)
+        assert np.array_equal(c, um) and np.array_equal(d, vm)
