@@ -720,39 +720,62 @@ int blgpu_read_input_data(blgpu_ctx *ctx, const char *filein, int *step) {
 // ---------------------------------------------------------------------------
 // Temporal inflow modes (the inflow_flag = 1 branch of
 // compute_blasius_solution_for_bc, boundary_conditions.f90:1652-1797).  The
-// file is a native-order stream: ny_inlet, n, m (int32), beta, omega (f64),
+// file is a stream (native order, or big-endian as the GPU build's runtime
+// reads it, told apart by the sizes): ny_inlet, n, m (int32), beta, omega (f64),
 // ymesh(ny_inlet), zmode(n), tmode(m), then qu_r, qu_i, qv_r, qv_i, qw_r,
 // qw_i, each (ny_inlet, n, m) in Fortran order.
 // ---------------------------------------------------------------------------
-int blgpu_read_temporal_modes_info(const char *path, blgpu_modes_info *h) {
-  if (!path || !h) return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes_info: null argument");
+// the header in the byte order whose sizes fit the file (native first)
+static int modes_header(const char *path, blgpu_modes_info *h, bool *swap) {
   FILE *f = fopen(path, "rb");
   if (!f) return io_err(BLGPU_EINVAL, "cannot open %s: %s", path, strerror(errno));
-  int32_t iv[3];
-  double dv[2];
-  const bool ok = rd(f, iv, sizeof iv) && rd(f, dv, sizeof dv);
+  int32_t iv0[3];
+  double dv0[2];
+  const bool ok = rd(f, iv0, sizeof iv0) && rd(f, dv0, sizeof dv0);
   fseek(f, 0, SEEK_END);
   const long long size = ftell(f);
   fclose(f);
   if (!ok) return io_err(BLGPU_EINVAL, "%s: short header", path);
-  if (iv[0] < 2 || iv[1] < 1 || iv[2] < 1 || iv[0] > (1 << 24) || iv[1] > 4096 || iv[2] > 4096)
-    return io_err(BLGPU_EINVAL, "%s: implausible sizes ny_inlet %d, n %d, m %d", path, iv[0], iv[1], iv[2]);
-  const long long nq = (long long)iv[0] * iv[1] * iv[2];
-  const long long want = 12 + 16 + 8LL * (iv[0] + iv[1] + iv[2]) + 6 * 8 * nq;
-  if (size != want)
-    return io_err(BLGPU_EINVAL, "%s: %lld bytes, the header's sizes need %lld", path, size, want);
-  h->ny_inlet = iv[0];
-  h->n_modes = iv[1];
-  h->m_modes = iv[2];
-  h->beta = dv[0];
-  h->omega = dv[1];
-  return BLGPU_OK;
+  for (int sw = 0; sw < 2; ++sw) {
+    int32_t iv[3] = {iv0[0], iv0[1], iv0[2]};
+    double dv[2] = {dv0[0], dv0[1]};
+    if (sw) {
+      swap_n(iv, 3);
+      swap_n(dv, 2);
+    }
+    if (iv[0] < 2 || iv[1] < 1 || iv[2] < 1 || iv[0] > (1 << 24) || iv[1] > 4096 || iv[2] > 4096) {
+      if (!sw) io_err(BLGPU_EINVAL, "%s: implausible sizes ny_inlet %d, n %d, m %d", path, iv[0], iv[1], iv[2]);
+      continue;
+    }
+    const long long nq = (long long)iv[0] * iv[1] * iv[2];
+    const long long want = 12 + 16 + 8LL * (iv[0] + iv[1] + iv[2]) + 6 * 8 * nq;
+    if (size != want) {
+      if (!sw) io_err(BLGPU_EINVAL, "%s: %lld bytes, the header's sizes need %lld", path, size, want);
+      continue;
+    }
+    h->ny_inlet = iv[0];
+    h->n_modes = iv[1];
+    h->m_modes = iv[2];
+    h->beta = dv[0];
+    h->omega = dv[1];
+    *swap = sw != 0;
+    return BLGPU_OK;
+  }
+  return BLGPU_EINVAL;  // the native order's message stands
+}
+
+int blgpu_read_temporal_modes_info(const char *path, blgpu_modes_info *h) {
+  if (!path || !h) return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes_info: null argument");
+  bool swap = false;
+  return modes_header(path, h, &swap);
 }
 
 int blgpu_read_temporal_modes(const char *path, int ny, const double *y, double *zmode, double *tmode, double *qu,
                               double *qv, double *qw, double *ymesh) {
+  if (!path) return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes: null argument");
   blgpu_modes_info h{};
-  int rc = blgpu_read_temporal_modes_info(path, &h);
+  bool swap = false;
+  int rc = modes_header(path, &h, &swap);
   if (rc) return rc;
   if (!y || ny < 3 || !zmode || !tmode || !qu || !qv || !qw)
     return io_err(BLGPU_EINVAL, "blgpu_read_temporal_modes: bad argument");
@@ -764,8 +787,8 @@ int blgpu_read_temporal_modes(const char *path, int ny, const double *y, double 
   FILE *f = fopen(path, "rb");
   if (!f) return io_err(BLGPU_EINVAL, "cannot open %s: %s", path, strerror(errno));
   fseek(f, 28, SEEK_SET);
-  const bool ok = rd(f, ym.data(), 8 * nyi) && rd(f, zm.data(), 8 * n) && rd(f, tm.data(), 8 * m) &&
-                  rd(f, q.data(), 8 * 6 * nq);
+  const bool ok = rd_d(f, ym.data(), nyi, swap) && rd_d(f, zm.data(), n, swap) && rd_d(f, tm.data(), m, swap) &&
+                  rd_d(f, q.data(), 6 * nq, swap);
   fclose(f);
   if (!ok) return io_err(BLGPU_EINVAL, "%s: short read", path);
   for (int a = 0; a < n; ++a) zmode[a] = h.beta * zm[a];   // zmode_inlet = beta_inlet*zmode_inlet

@@ -18,16 +18,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.environ.get("BLGPU_REFERENCE_DIR", "")
 
 
-def write_modes(path, ym, zm, tm, beta, omega, qu, qv, qw):
+def write_modes(path, ym, zm, tm, beta, omega, qu, qv, qw, order="<"):
     ny, n, m = qu.shape
     with open(path, "wb") as f:
-        f.write(struct.pack("<3i", ny, n, m))
-        f.write(struct.pack("<2d", beta, omega))
+        f.write(struct.pack(order + "3i", ny, n, m))
+        f.write(struct.pack(order + "2d", beta, omega))
         for a in (ym, zm, tm):
-            f.write(np.asarray(a, "<f8").tobytes())
+            f.write(np.asarray(a, order + "f8").tobytes())
         for q in (qu, qv, qw):
-            f.write(np.asfortranarray(q.real).ravel(order="F").astype("<f8").tobytes())
-            f.write(np.asfortranarray(q.imag).ravel(order="F").astype("<f8").tobytes())
+            f.write(np.asfortranarray(q.real).ravel(order="F").astype(order + "f8").tobytes())
+            f.write(np.asfortranarray(q.imag).ravel(order="F").astype(order + "f8").tobytes())
 
 
 def centres_ghost(y):
@@ -54,14 +54,16 @@ def interp_np(ym, q, tgt):
     return out
 
 
-def test_synthetic_modes_file(tmp_path):
+@pytest.mark.parametrize("order", ["<", ">"])
+def test_synthetic_modes_file(tmp_path, order):
+    """Native and big-endian files (the GPU build's runtime reads big-endian)."""
     rng = np.random.default_rng(5)
     nyi, n, m = 40, 3, 2
     ym = np.concatenate([[0.0], np.cumsum(rng.uniform(0.01, 0.05, nyi - 1))])
     zm, tm = np.array([0.0, 1.0, -1.0]), np.array([1.0, 2.0])
     q = [rng.standard_normal((nyi, n, m)) + 1j * rng.standard_normal((nyi, n, m)) for _ in range(3)]
     p = tmp_path / "modes.dat"
-    write_modes(p, ym, zm, tm, 2.5, 0.3, *q)
+    write_modes(p, ym, zm, tm, 2.5, 0.3, *q, order=order)
     y = np.linspace(0.0, ym[-1] * 1.3, 23)  # rows past the mesh end read zero
     r = files.read_temporal_modes(p, y)
     assert r["info"] == dict(ny_inlet=nyi, n_modes=n, m_modes=m, beta=2.5, omega=0.3)
