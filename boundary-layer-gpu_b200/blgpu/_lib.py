@@ -146,6 +146,10 @@ _SIGS = {
     "blgpu_read_rescaling": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p]),
     "blgpu_write_rescaling": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p]),
     "blgpu_read_inflow_profile_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "blgpu_write_statistics": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p,
+                                              c_double_p, c_double_p]),
+    "blgpu_output_statistics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "blgpu_read_inflow_profile": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, c_double_p, c_double_p]),
     "blgpu_snapshot_name": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "blgpu_output_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),

@@ -8,6 +8,9 @@ write_rescaling   <snapshot>.mean.rescaling Lund means (input_output.f90:440-458
 snapshot_name     fileout.%08d
 read_temporal_modes  the binary temporal inflow-mode file of the transition case
                   (compute_blasius_solution_for_bc, boundary_conditions.f90:1652-1797)
+read_inflow_profile  the inflow_file of inflow flags 2 and 5 (boundary_conditions.f90:1405, 1550)
+write_statistics,
+read_statistics   <fileout>.<step>.stats.txt (output_statistics, input_output.f90:685-746)
 """
 import ctypes
 
@@ -110,6 +113,35 @@ def read_inflow_profile(path, ny=None):
     U, V = np.zeros(ny + 1), np.zeros(ny)
     check_io(lib.blgpu_read_inflow_profile(str(path).encode(), ny, _p(U), _p(V)))
     return U, V
+
+
+def write_statistics(path, t, nu, nz, istep, Cf, x, y, means):
+    """means: the nine (nx, ny) arrays of Solver.statistics, in its order
+    (Umean, Vmean, Wmean, U2mean, V2mean, W2mean, UVmean, Pmean, P2mean)."""
+    Cf, x, y = (np.ascontiguousarray(a, dtype=np.float64) for a in (Cf, x, y))
+    nx, ny = len(x), len(y)
+    m = np.asarray(means, dtype=np.float64)
+    assert m.shape == (9, nx, ny)
+    buf = np.ascontiguousarray(np.stack([np.asfortranarray(a).ravel(order="F") for a in m]))
+    check_io(load().blgpu_write_statistics(str(path).encode(), float(t), float(nu), nx, ny, int(nz), int(istep),
+                                           _p(Cf), _p(x), _p(y), _p(buf)))
+
+
+def read_statistics(path):
+    """The text of a stats file back as arrays: header (t, nu, nx, ny, nz,
+    istep), Cf, x, y and the eight (nx, ny) arrays the file holds."""
+    lines = open(path).read().splitlines()
+    h = lines[0][1:]
+    t, nu = float(h[0:15]), float(h[15:30])
+    nx, ny, nz, istep = (int(h[30 + 8 * q:38 + 8 * q]) for q in range(4))
+    def num(f):  # a field that did not fit its width reads as NaN
+        return np.nan if f.strip().startswith("*") else float(f)
+
+    row = lambda s: np.array([num(s[15 * q:15 * q + 15]) for q in range(len(s) // 15)])
+    Cf, x, y = row(lines[1]), row(lines[2]), row(lines[3])
+    arrays = [np.array([row(lines[4 + q * nx + i]) for i in range(nx)]) for q in range(8)]
+    names = ("Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "Pmean", "P2mean")
+    return dict(t=t, nu=nu, nx=nx, ny=ny, nz=nz, istep=istep, Cf=Cf, x=x, y=y, **dict(zip(names, arrays)))
 
 
 def snapshot_name(fileout, step):

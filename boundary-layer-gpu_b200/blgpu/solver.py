@@ -155,6 +155,11 @@ class Solver:
         fileout.restart to it and, with rescaling, the Lund means file."""
         _lib.check_io(self.lib.blgpu_output_data(self.ctx, str(fileout).encode(), int(step), int(bool(rescaling))))
 
+    def output_statistics(self, fileout, istep, nstep_init=0):
+        """output_statistics: the device statistics written to
+        fileout.<istep+nstep_init>.stats.txt in the reference's text layout."""
+        _lib.check_io(self.lib.blgpu_output_statistics(self.ctx, str(fileout).encode(), int(istep), int(nstep_init)))
+
     def read_input_data(self, filein):
         """read_input_data: grid (replaces the current one), U, V, W and t
         from a snapshot; returns the file's step (-1 when absent)."""

@@ -686,6 +686,88 @@ int blgpu_output_data(blgpu_ctx *ctx, const char *fileout, int step, int rescali
   return BLGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// output_statistics (input_output.f90:685-746): the text file
+// <fileout>.<istep+nstep_init, 8 digits>.stats.txt holding, in Fortran list
+// formats, '%', t, nu (F15.8), nx, ny, nz, istep (I8); Cf and x (nx values,
+// F15.8, one record each); y (ny values); then Umean, Vmean, Wmean, U2mean,
+// V2mean, W2mean, Pmean, P2mean as nx records of ny values.
+// ---------------------------------------------------------------------------
+namespace {
+// Fortran Fw.d: right-justified in w columns, w asterisks when it does not
+// fit; NaN and infinities as the gfortran runtime spells them
+void put_f(std::string &out, double v, int w = 15, int d = 8) {
+  char b[64];
+  int n;
+  if (v != v) n = snprintf(b, sizeof b, "%*s", w, "NaN");
+  else if (v == INFINITY || v == -INFINITY) n = snprintf(b, sizeof b, "%*s", w, v > 0 ? "Infinity" : "-Infinity");
+  else n = snprintf(b, sizeof b, "%*.*f", w, d, v);
+  if (n > w) out.append((size_t)w, '*');
+  else out.append(b, (size_t)n);
+}
+void put_i(std::string &out, long long v, int w = 8) {
+  char b[64];
+  const int n = snprintf(b, sizeof b, "%*lld", w, v);
+  if (n > w) out.append((size_t)w, '*');
+  else out.append(b, (size_t)n);
+}
+}  // namespace
+
+int blgpu_write_statistics(const char *path, double t, double nu, int nx, int ny, int nz, int istep,
+                           const double *Cf, const double *x, const double *y, const double *means) {
+  if (!path || !Cf || !x || !y || !means) return io_err(BLGPU_EINVAL, "blgpu_write_statistics: null argument");
+  if (nx < 1 || ny < 1) return io_err(BLGPU_EINVAL, "blgpu_write_statistics: box %d x %d", nx, ny);
+  std::string out;
+  out.reserve((size_t)(nx + 2) * (ny + 2) * 15 * 8 / 7);
+  out += '%';
+  put_f(out, t);
+  put_f(out, nu);
+  put_i(out, nx);
+  put_i(out, ny);
+  put_i(out, nz);
+  put_i(out, istep);
+  out += '\n';
+  for (int i = 0; i < nx; ++i) put_f(out, Cf[i]);
+  out += '\n';
+  for (int i = 0; i < nx; ++i) put_f(out, x[i]);
+  out += '\n';
+  for (int j = 0; j < ny; ++j) put_f(out, y[j]);
+  out += '\n';
+  // means: Umean, Vmean, Wmean, U2mean, V2mean, W2mean, UVmean, Pmean, P2mean,
+  // each (nx, ny) in Fortran order; the file leaves UVmean out
+  const long long plane = (long long)nx * ny;
+  for (int q : {0, 1, 2, 3, 4, 5, 7, 8}) {
+    const double *a = means + q * plane;
+    for (int i = 0; i < nx; ++i) {
+      for (int j = 0; j < ny; ++j) put_f(out, a[i + (long long)nx * j]);
+      out += '\n';
+    }
+  }
+  File F;
+  F.f = fopen(path, "w");
+  if (!F.f) return io_err(BLGPU_EINVAL, "%s: cannot create (%s)", path, strerror(errno));
+  if (!wr(F.f, out.data(), out.size()) || fflush(F.f) != 0)
+    return io_err(BLGPU_EINVAL, "%s: write failed (%s)", path, strerror(errno));
+  return BLGPU_OK;
+}
+
+int blgpu_output_statistics(blgpu_ctx *ctx, const char *fileout, int istep, int nstep_init) {
+  if (!ctx || !fileout) return io_err(BLGPU_EINVAL, "blgpu_output_statistics: null argument");
+  int nx, ny, nz;
+  double nu, t, dt;
+  if (blgpu_box(ctx, &nx, &ny, &nz, &nu) || blgpu_get_time(ctx, &t, &dt))
+    return io_err(BLGPU_ESTATE, "%s", blgpu_last_error(ctx));
+  std::vector<double> means((size_t)9 * nx * ny), Cf((size_t)nx), x((size_t)nx), y((size_t)ny), z((size_t)nz);
+  int rc = blgpu_statistics(ctx, means.data(), nullptr, Cf.data(), nullptr, nullptr);
+  if (!rc) rc = blgpu_get_grid(ctx, x.data(), y.data(), z.data());
+  if (rc) return io_err(rc, "%s", blgpu_last_error(ctx));
+  char name[4096];
+  if ((rc = blgpu_snapshot_name(fileout, istep + nstep_init, name, sizeof name))) return rc;
+  const std::string fn = std::string(name) + ".stats.txt";
+  make_parent(fn);
+  return blgpu_write_statistics(fn.c_str(), t, nu, nx, ny, nz, istep, Cf.data(), x.data(), y.data(), means.data());
+}
+
 int blgpu_read_input_data(blgpu_ctx *ctx, const char *filein, int *step) {
   if (!ctx || !filein) return io_err(BLGPU_EINVAL, "blgpu_read_input_data: null argument");
   int nx, ny, nz;

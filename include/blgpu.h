@@ -426,6 +426,17 @@ int blgpu_write_rescaling(const char *path, int nyg, int ny, const double *Umean
  * ("Profile doesnt match dimensions"). */
 int blgpu_read_inflow_profile_info(const char *path, int *ny);
 int blgpu_read_inflow_profile(const char *path, int ny, double *U_inlet, double *V_inlet);
+/* output_statistics (input_output.f90:685-746): <name>.stats.txt in the
+ * reference's text layout ('%', t, nu as F15.8; nx, ny, nz, istep as I8;
+ * Cf and x as one record of nx F15.8 values; y as one of ny; then Umean,
+ * Vmean, Wmean, U2mean, V2mean, W2mean, Pmean, P2mean as nx records of ny).
+ * means: the nine (nx,ny) arrays of blgpu_statistics, in its order.  The
+ * context form computes the statistics on the device and names the file
+ * fileout.<istep+nstep_init, 8 digits>.stats.txt, with istep in the header,
+ * as the reference does. */
+int blgpu_write_statistics(const char *path, double t, double nu, int nx, int ny, int nz, int istep,
+                           const double *Cf, const double *x, const double *y, const double *means);
+int blgpu_output_statistics(blgpu_ctx *ctx, const char *fileout, int istep, int nstep_init);
 /* fileout.%08d (input_output.f90:516-518) */
 int blgpu_snapshot_name(const char *fileout, int step, char *name, int cap);
 /* output_data (input_output.f90:496-680) for a context: downloads the state,

@@ -306,3 +306,30 @@ def test_writers_follow_F_UFMTENDIAN(tmp_path, monkeypatch):
     for f in ("mbe", "mle"):
         c, d = files.read_rescaling(tmp_path / f, ny)
         assert np.array_equal(c, um) and np.array_equal(d, vm)
+
+
+def test_statistics_text_layout(tmp_path):
+    """output_statistics (input_output.f90:685-746): '%' and t, nu in F15.8,
+    nx, ny, nz, istep in I8; Cf, x, y one record each; then the eight means
+    as nx records of ny F15.8 values (UVmean is not written)."""
+    rng = np.random.default_rng(8)
+    nx, ny = 5, 4
+    x, y = np.linspace(0.0, 2.0, nx), np.linspace(0.0, 1.0, ny)
+    Cf = rng.uniform(-1e-3, 5e-3, nx)
+    Cf[1], Cf[2], Cf[3] = 1.0e7, np.nan, -0.0
+    means = rng.standard_normal((9, nx, ny))
+    p = tmp_path / "s.stats.txt"
+    files.write_statistics(p, 1.5, 1e-5, 6, 7, Cf, x, y, means)
+    lines = p.read_text().splitlines()
+    assert lines[0] == "%     1.50000000     0.00001000       5       4       6       7"
+    assert len(lines) == 4 + 8 * nx
+    assert lines[1][15:30] == "*" * 15 and lines[1][30:45] == " " * 12 + "NaN"
+    assert lines[1][45:60] == "    -0.00000000"
+    assert all(len(l) == 15 * nx for l in lines[1:3]) and len(lines[3]) == 15 * ny
+    assert all(len(l) == 15 * ny for l in lines[4:])
+    s = files.read_statistics(p)
+    assert (s["t"], s["nu"], s["nx"], s["ny"], s["nz"], s["istep"]) == (1.5, 1e-5, 5, 4, 6, 7)
+    assert np.array_equal(s["x"], np.round(x, 8)) and np.array_equal(s["y"], np.round(y, 8))
+    for q, name in zip((0, 1, 2, 3, 4, 5, 7, 8),
+                       ("Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "Pmean", "P2mean")):
+        assert np.abs(s[name] - means[q]).max() <= 5.01e-9, name

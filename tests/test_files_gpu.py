@@ -54,3 +54,24 @@ def test_unknown_les_model_refused(gpu):
     for les in (4, -2):
         with pytest.raises(BlgpuError, match="unknown LES model"):
             Solver(34, 17, 12, 1e-3, -0.01, les_model=les)
+
+
+def test_output_statistics(gpu, tmp_path):
+    """output_statistics for a context: the device statistics in the
+    reference's text layout, named with istep + nstep_init and headed with
+    istep; every value equals compute_statistics' to the file's 8 decimals."""
+    c = cases.laminar_case(nx=34, ny=17, nz=12)
+    s = cases.solver_for(c)
+    s.advance(2)
+    st = s.compute_statistics()
+    out = str(tmp_path / "stats" / "BL")
+    s.output_statistics(out, 5, nstep_init=10)
+    r = files.read_statistics(files.snapshot_name(out, 15) + ".stats.txt")
+    assert (r["nx"], r["ny"], r["nz"], r["istep"]) == (34, 17, 12, 5)
+    assert abs(r["t"] - s.time()[0]) <= 5.01e-9 and r["nu"] == round(c.nu, 8)
+    assert np.abs(r["x"] - s.x).max() <= 5.01e-9 and np.abs(r["y"] - s.y).max() <= 5.01e-9
+    assert np.abs(r["Cf"] - st["Cf"]).max() <= 5.01e-9
+    for name in ("Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "Pmean", "P2mean"):
+        assert r[name].shape == (34, 17)
+        assert np.abs(r[name] - st[name]).max() <= 5.01e-9 * max(1.0, np.abs(st[name]).max()), name
+    s.close()
